@@ -1,0 +1,147 @@
+"""ctypes mirror of include/patchstereo.h and the loader of libpatchstereo.so.
+
+The loader fails loudly when the library is missing: there is no CPU fallback for the engine.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import pathlib
+
+HERE = pathlib.Path(__file__).resolve().parent
+ENGINE_PATH = HERE / "libpatchstereo.so"
+SYNTH_PATH = HERE / "libps_synth.so"
+
+PS_OK, PS_EINVAL, PS_ECUDA, PS_ENODEV, PS_ECOMPILE, PS_ETIMEOUT, PS_EFAULT, PS_ENOMEM, PS_EBUSY = range(9)
+STATUS_NAMES = {0: "PS_OK", 1: "PS_EINVAL", 2: "PS_ECUDA", 3: "PS_ENODEV", 4: "PS_ECOMPILE", 5: "PS_ETIMEOUT",
+                6: "PS_EFAULT", 7: "PS_ENOMEM", 8: "PS_EBUSY"}
+PS_IMAGE_U8, PS_IMAGE_F32 = 0, 1
+PS_MATH_PARITY, PS_MATH_FAST = 0, 1
+PS_MAX_SOURCES = 32
+
+
+class Options(C.Structure):
+    _fields_ = [("math_mode", C.c_uint32), ("max_batch", C.c_uint32), ("batch_pixels", C.c_uint64),
+                ("checked", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class PmParams(C.Structure):
+    """PmParams (crates/dense/src/params.rs:76-124)."""
+    _fields_ = [("window_radius", C.c_int32), ("window_step", C.c_int32), ("sigma_spatial", C.c_float),
+                ("sigma_color", C.c_float), ("tau0", C.c_float), ("tau_alpha", C.c_float), ("tau1", C.c_float),
+                ("beta", C.c_float), ("n1", C.c_uint32), ("n2", C.c_uint32), ("prev_view_weight", C.c_float),
+                ("min_triangulation_angle_deg", C.c_float), ("incident_angle_sigma", C.c_float),
+                ("geom_lambda", C.c_float), ("geom_max_cost", C.c_float), ("top_k", C.c_uint32),
+                ("eps0_photometric", C.c_float), ("eps0_geometric", C.c_float), ("phi0_photometric_deg", C.c_float),
+                ("phi0_geometric_deg", C.c_float), ("eps_min", C.c_float), ("phi_min_deg", C.c_float),
+                ("weak_texture_var", C.c_float)]
+
+
+class FilterParams(C.Structure):
+    """FilterParams (crates/dense/src/params.rs:180-207)."""
+    _fields_ = [("min_ncc", C.c_float), ("min_triangulation_angle_deg", C.c_float), ("min_num_consistent", C.c_uint32),
+                ("geom_max_cost", C.c_float), ("ncc_sigma", C.c_float), ("median_filter", C.c_uint32)]
+
+
+class LevelImage(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("format", C.c_uint32), ("stride", C.c_uint32),
+                ("pixels", C.c_void_p), ("k", C.c_float * 4)]
+
+
+class PairGeometry(C.Structure):
+    _fields_ = [("r", C.c_float * 9), ("t", C.c_float * 3), ("center", C.c_float * 3)]
+
+
+class KernelView(C.Structure):
+    _fields_ = [("key", C.c_uint64), ("levels", C.POINTER(LevelImage)), ("sources", C.POINTER(C.c_uint32)),
+                ("num_sources", C.c_uint32), ("reserved", C.c_uint32), ("pairs", C.POINTER(PairGeometry)),
+                ("pairs_f64", C.POINTER(C.c_double)), ("depth_min", C.c_float), ("depth_max", C.c_float)]
+
+
+class KernelInput(C.Structure):
+    _fields_ = [("views", C.POINTER(KernelView)), ("num_views", C.c_uint32), ("num_levels", C.c_uint32),
+                ("pm", PmParams), ("filter", FilterParams), ("seed", C.c_uint64)]
+
+
+class ViewState(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("depth", C.POINTER(C.c_float)),
+                ("normal", C.POINTER(C.c_float)), ("cost", C.POINTER(C.c_float)), ("prior", C.POINTER(C.c_float))]
+
+
+class RunParams(C.Structure):
+    _fields_ = [("level", C.c_uint32), ("geometric", C.c_uint32), ("random_init", C.c_uint32),
+                ("iterations", C.c_uint32), ("run_id", C.c_uint32), ("use_prior", C.c_uint32)]
+
+
+class DepthSnapshot(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
+                ("maps", C.POINTER(C.POINTER(C.c_float)))]
+
+
+# Every exported symbol of include/patchstereo.h with (restype, argtypes).
+_P = C.c_void_p
+_U32P = C.POINTER(C.c_uint32)
+SIGNATURES = {
+    "ps_abi_version": (C.c_int, []),
+    "ps_pm_params_default": (None, [C.POINTER(PmParams)]),
+    "ps_filter_params_default": (None, [C.POINTER(FilterParams)]),
+    "ps_options_default": (None, [C.POINTER(Options)]),
+    "ps_backend_create": (C.c_int, [C.c_int, C.POINTER(Options), C.POINTER(_P)]),
+    "ps_backend_destroy": (None, [_P]),
+    "ps_backend_name": (C.c_char_p, [_P]),
+    "ps_backend_last_error": (C.c_char_p, [_P]),
+    "ps_begin": (C.c_int, [_P, C.POINTER(KernelInput), C.POINTER(_P)]),
+    "ps_end": (C.c_int, [_P]),
+    "ps_last_error": (C.c_char_p, [_P]),
+    "ps_run": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState), C.POINTER(RunParams), C.POINTER(DepthSnapshot)]),
+    "ps_evaluate": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState), C.c_uint32,
+                              C.POINTER(DepthSnapshot), C.POINTER(C.POINTER(C.c_float))]),
+    "ps_filter": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState), C.POINTER(DepthSnapshot),
+                            C.POINTER(C.POINTER(C.c_uint8))]),
+    "ps_upsample": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState), C.c_float, C.c_float,
+                              C.POINTER(ViewState)]),
+    "ps_median_filter": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState), C.POINTER(ViewState)]),
+    "ps_state_upload": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
+    "ps_state_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
+    "ps_run_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(RunParams)]),
+    "ps_snapshot_capture": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.c_uint64, C.c_uint32]),
+    "ps_filter_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_uint8))]),
+    "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
+    "ps_synchronize": (C.c_int, [_P]),
+    "ps_launch_count": (C.c_uint64, [_P]),
+}
+
+_engine = None
+
+
+def engine() -> C.CDLL:
+    """Loads libpatchstereo.so (built in-tree by cumulus3d_b200.build); raises if it is missing."""
+    global _engine
+    if _engine is None:
+        if not ENGINE_PATH.exists():
+            raise RuntimeError(f"{ENGINE_PATH} is not built; run `python -m cumulus3d_b200.build` "
+                               "(the engine has no CPU fallback)")
+        lib = C.CDLL(str(ENGINE_PATH))
+        for name, (res, args) in SIGNATURES.items():
+            f = getattr(lib, name)
+            f.restype = res
+            f.argtypes = args
+        _engine = lib
+    return _engine
+
+
+def default_pm() -> PmParams:
+    p = PmParams()
+    engine().ps_pm_params_default(C.byref(p))
+    return p
+
+
+def default_filter() -> FilterParams:
+    p = FilterParams()
+    engine().ps_filter_params_default(C.byref(p))
+    return p
+
+
+class PsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code

@@ -1,0 +1,87 @@
+// Elementary functions with a fixed operation sequence, compiled identically for the host (g++) and the
+// device (nvcc).  Every step is a correctly rounded IEEE-754 binary32 operation (add, mul, fma, rint), so the
+// CPU oracle and the parity build of the GPU kernels produce the same bits for the same argument.
+//
+// Methods (from the mathematics, not from any vendor library):
+//  * ps_expf: Cody–Waite argument reduction x = k·ln2 + r (ln2 split into a 16-bit head and a tail, both
+//    products folded with fma), then the degree-7 Taylor polynomial of e^r on |r| <= ln2/2 evaluated by Horner's
+//    rule, then scaling by 2^k through the exponent field.  Truncation error of the polynomial is below
+//    (ln2/2)^8/8! ~ 5e-9 relative; measured error is about 1 ulp.  Results below 2^-126·(e^-0.35) are flushed
+//    to +0 (arguments below -87.33); arguments above 88.0 return +inf.  All call sites in this project pass
+//    arguments <= 0.
+//  * ps_sincosf: Cody–Waite reduction by pi/2 (three-part split of pi/2 folded with fma, valid for |x| < 1e5),
+//    then Taylor polynomials of degree 9 (sin) and 10 (cos) on |r| <= pi/4 (truncation error < 2e-9), with the
+//    quadrant selecting sign and swap.
+#pragma once
+#include <stdint.h>
+#include <string.h>
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define PS_HD __host__ __device__ __forceinline__
+#else
+#define PS_HD static inline
+#endif
+
+PS_HD float ps_u2f(uint32_t u) {
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(u);
+#else
+  float f;
+  memcpy(&f, &u, sizeof f);
+  return f;
+#endif
+}
+
+PS_HD float ps_expf(float x) {
+  if (!(x == x)) return x;                        // NaN in, NaN out
+  if (x > 88.0f) return ps_u2f(0x7f800000u);      // +inf
+  if (x < -87.33f) return 0.0f;                   // below the smallest normal: flushed to zero
+  const float log2e = (float)1.4426950408889634;  // 1/ln 2
+  const float ln2_hi = (float)0.693145751953125;  // ln 2 rounded to 16 significant bits (k·ln2_hi exact)
+  const float ln2_lo = (float)1.4286068203094173e-06;  // ln 2 - ln2_hi
+  float k = rintf(x * log2e);
+  float r = fmaf(-k, ln2_hi, x);
+  r = fmaf(-k, ln2_lo, r);
+  float p = (float)(1.0 / 5040.0);
+  p = fmaf(p, r, (float)(1.0 / 720.0));
+  p = fmaf(p, r, (float)(1.0 / 120.0));
+  p = fmaf(p, r, (float)(1.0 / 24.0));
+  p = fmaf(p, r, (float)(1.0 / 6.0));
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
+  int ki = (int)k;                                // k in [-126, 127]
+  return p * ps_u2f((uint32_t)(ki + 127) << 23);
+}
+
+PS_HD void ps_sincosf(float x, float* s, float* c) {
+  const float two_over_pi = (float)0.63661977236758134;
+  const float pio2_1 = (float)1.5707963267948966;             // pi/2 rounded to binary32
+  const float pio2_2 = (float)(1.5707963267948966 - (double)(float)1.5707963267948966);
+  const float pio2_3 = (float)((1.5707963267948966 - (double)(float)1.5707963267948966) -
+                               (double)(float)(1.5707963267948966 - (double)(float)1.5707963267948966));
+  float q = rintf(x * two_over_pi);
+  float r = fmaf(-q, pio2_1, x);
+  r = fmaf(-q, pio2_2, r);
+  r = fmaf(-q, pio2_3, r);
+  float r2 = r * r;
+  float ps = (float)(1.0 / 362880.0);
+  ps = fmaf(ps, r2, (float)(-1.0 / 5040.0));
+  ps = fmaf(ps, r2, (float)(1.0 / 120.0));
+  ps = fmaf(ps, r2, (float)(-1.0 / 6.0));
+  float sn = fmaf(ps * r2, r, r);
+  float pc = (float)(-1.0 / 3628800.0);
+  pc = fmaf(pc, r2, (float)(1.0 / 40320.0));
+  pc = fmaf(pc, r2, (float)(-1.0 / 720.0));
+  pc = fmaf(pc, r2, (float)(1.0 / 24.0));
+  pc = fmaf(pc, r2, -0.5f);
+  float cs = fmaf(pc, r2, 1.0f);
+  int qi = ((int)q) & 3;
+  float so = sn, co = cs;
+  if (qi == 1) { so = cs; co = -sn; }
+  else if (qi == 2) { so = -sn; co = -cs; }
+  else if (qi == 3) { so = -cs; co = sn; }
+  *s = so;
+  *c = co;
+}

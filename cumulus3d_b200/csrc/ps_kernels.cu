@@ -1,0 +1,1095 @@
+// PatchStereo kernels for sm_100a.
+//
+// Compiled twice into libpatchstereo.so:
+//   PS_FAST=0 (namespace ps_parity): --fmad=false, IEEE division and square root, the project's own exp/sincos
+//            (ps_fmath.h) and fma only where written out.  Bitwise equal to the CPU oracle (oracle/ps_oracle.cpp),
+//            which follows the same operation sequence.
+//   PS_FAST=1 (namespace ps_fast):   --use_fast_math, hardware reciprocal / exp / rsqrt in the hot loops
+//            ("the kernel may use approximate division and exponential", crates/dense/src/kernel.rs:73-74).
+//
+// The rules are those of the reference kernel crates/cuda/src/kernels/patchmatch.cu (cited per function) and of
+// crates/dense/src/kernel.rs:36-74.  The B200 layout differs from the reference:
+//   * every image level is a normalised f32 plane with a PS_BORDER-pixel zero border, so a bilinear source tap is
+//     four unconditional loads after a clamp (no texture objects, no per-texel bounds tests);
+//   * a half-step CTA is 128 threads covering a 32 × 8 pixel tile; each warp takes 16 active columns of two
+//     adjacent rows, so reference-tile reads of the two colour phases fall into disjoint shared-memory banks;
+//   * the bilateral window weights of a pixel are computed once per half step and cached in shared memory (one
+//     slot per thread and tap) and reused by all 9·N + 6·a NCC evaluations of that pixel;
+//   * launches are flattened over the tiles of all views of a batch (no idle CTAs for ragged batches); the batch
+//     table travels in the kernel parameters.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "ps_fmath.h"
+#include "ps_types.h"
+
+#ifndef PS_FAST
+#define PS_FAST 0
+#endif
+#if PS_FAST
+#define PS_NS ps_fast
+#else
+#define PS_NS ps_parity
+#endif
+
+typedef unsigned long long u64;
+
+namespace PS_NS {
+
+// ------------------------------------------------------------------------------------------- math policy
+__device__ __forceinline__ float m_rcp(float x) {
+#if PS_FAST
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+#else
+  return 1.0f / x;
+#endif
+}
+__device__ __forceinline__ float m_exp(float x) {
+#if PS_FAST
+  return __expf(x);
+#else
+  return ps_expf(x);
+#endif
+}
+__device__ __forceinline__ void m_sincos(float x, float* s, float* c) {
+#if PS_FAST
+  __sincosf(x, s, c);
+#else
+  ps_sincosf(x, s, c);
+#endif
+}
+__device__ __forceinline__ float m_rsqrt(float x) {
+#if PS_FAST
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+
+// ------------------------------------------------------------------------------------------- RNG (patchmatch.cu:112-125)
+__device__ __forceinline__ u64 mix64(u64 z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ float rnd(u64& s) {
+  s += 0x9e3779b97f4a7c15ULL;
+  u64 z = mix64(s);
+  return ((float)(z >> 40) + 1.0f) * (1.0f / 16777216.0f);
+}
+__device__ __forceinline__ u64 rng_state(u64 seed, u64 key, int level, int run, int t, int half, u64 pixel) {
+  u64 tag = ((u64)level << 48) ^ ((u64)run << 32) ^ ((u64)t << 16) ^ (u64)half;
+  return mix64(seed ^ mix64(key ^ mix64(tag)) ^ pixel);
+}
+
+// ------------------------------------------------------------------------------------------- vectors (patchmatch.cu:128-133)
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+  return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 nrm3(float3 a) {
+  float l = m_rsqrt(fmaxf(dot3(a, a), 1e-30f));
+  return make_float3(a.x * l, a.y * l, a.z * l);
+}
+// patchmatch.cu:386
+__device__ __forceinline__ float3 pixel_ray(const PsLevel& R, int x, int y) {
+  return make_float3(((float)x - R.cx) / R.fx, ((float)y - R.cy) / R.fy, 1.0f);
+}
+
+// ------------------------------------------------------------------------------------------- source sample (patchmatch.cu:169-192)
+// Bilinear value at (u, v), integer-centre convention, 0 outside the image.  The clamp to [-2, w] × [-2, h] keeps
+// both taps of an out-of-image footprint inside the zero border, which reproduces the reference's "0 outside"
+// without per-texel tests.
+__device__ __forceinline__ float src_sample(const float* __restrict__ img, int pitch, float wf, float hf, float u,
+                                            float v) {
+  float xf = floorf(u), yf = floorf(v);
+  float ax = u - xf, ay = v - yf;
+  float xc = fminf(fmaxf(xf, -2.0f), wf);
+  float yc = fminf(fmaxf(yf, -2.0f), hf);
+  const float* p = img + (int)yc * pitch + (int)xc;
+  float p00 = __ldg(p), p10 = __ldg(p + 1), p01 = __ldg(p + pitch), p11 = __ldg(p + pitch + 1);
+  float top = fmaf(ax, p10 - p00, p00);
+  float bot = fmaf(ax, p11 - p01, p01);
+  return fmaf(ay, bot - top, top);
+}
+
+// ------------------------------------------------------------------------------------------- reference window
+struct RefStats {
+  float ic, W, mu, var;
+};
+
+// Tile-resident reference window of one pixel: t points at the pixel inside the shared tile (row pitch tw); wc is
+// the thread's weight-cache slot (stride NT floats between taps).
+struct RefWin {
+  const float* t;
+  int tw;
+  float* wc;
+};
+
+// ref_stats (patchmatch.cu:199-223).  Weights w_k = exp(-(dx²+dy²)/(2σs²) - (Ic-Ik)²/(2σc²)); 0 outside the image.
+template <int WR, int WS, bool CW, int NT>
+__device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) {
+  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
+  const int wn = (2 * wr) / ws + 1;
+  RefStats s;
+  s.ic = rw.t[0];
+  float W = 0.f, S = 0.f, SS = 0.f;
+#pragma unroll 1
+  for (int a = 0; a < wn; ++a) {
+    const int dy = -wr + a * ws;
+    const float* trow = rw.t + dy * rw.tw;
+    auto tap = [&](int b) {
+      const int dx = -wr + b * ws;
+      float ik = trow[dx];
+      float d = s.ic - ik;
+      float w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
+      if (CW) rw.wc[(a * wn + b) * NT] = w;
+      float wi = w * ik;
+      W = W + w;
+      S = S + wi;
+      SS = fmaf(wi, ik, SS);
+    };
+    if constexpr (WR != 0) {
+#pragma unroll
+      for (int b = 0; b < (2 * WR) / WS + 1; ++b) tap(b);
+    } else {
+#pragma unroll 1
+      for (int b = 0; b < wn; ++b) tap(b);
+    }
+  }
+  s.W = W;
+  s.mu = S / W;
+  s.var = SS / W - s.mu * s.mu;
+  return s;
+}
+
+// Plane-induced homography H = A + b (nᵀK⁻¹)/δ (patchmatch.cu:225-242).
+__device__ __forceinline__ bool homography(const PsLevel& R, const PsLPair& L, float x, float y, float4 h, float* H) {
+  float ifx = 1.0f / R.fx, ify = 1.0f / R.fy;
+  float3 n = make_float3(h.x, h.y, h.z);
+  float3 ray = make_float3((x - R.cx) * ifx, (y - R.cy) * ify, 1.0f);
+  float delta = h.w * dot3(n, ray);
+  if (!(delta < -1e-12f)) return false;
+  float id = 1.0f / delta;
+  float u0 = n.x * ifx, u1 = n.y * ify;
+  float u2 = n.z - u0 * R.cx - u1 * R.cy;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    float br = L.b[r] * id;
+    H[r * 3 + 0] = L.A[r * 3 + 0] + br * u0;
+    H[r * 3 + 1] = L.A[r * 3 + 1] + br * u1;
+    H[r * 3 + 2] = L.A[r * 3 + 2] + br * u2;
+  }
+  return true;
+}
+
+// Cost 1 - ρ of the bilateral-weighted NCC (patchmatch.cu:245-290); 2 on failure.
+// Parity operation sequence per tap (dx, dy), with sx = x+dx, sy = y+dy:
+//   zz = fma(H6, sx, fma(H7, sy, H8)); if zz > 1e-8: s = sample(fma(H0,sx,fma(H1,sy,H2))·(1/zz), fma(H3,sx,fma(H4,sy,H5))·(1/zz))
+//   ws = w·s; Ss += ws; SSs = fma(ws, s, SSs); IS = fma(ws, Ik, IS)
+template <int WR, int WS, bool CW, int NT>
+__device__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S, const float* H,
+                          int x, int y) {
+  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
+  const int wn = (2 * wr) / ws + 1;
+  const float fx = (float)x, fy = (float)y;
+  float z = fmaf(H[6], fx, fmaf(H[7], fy, H[8]));
+  if (!(z > 1e-8f)) return 2.0f;
+  float iz = m_rcp(z);
+  float u = fmaf(H[0], fx, fmaf(H[1], fy, H[2])) * iz;
+  float v = fmaf(H[3], fx, fmaf(H[4], fy, H[5])) * iz;
+  const float wf = (float)S.w, hf = (float)S.h;
+  if (!(u >= 0.f && v >= 0.f && u <= wf - 1.0f && v <= hf - 1.0f)) return 2.0f;
+  if (rs.var < 1e-5f) return 2.0f;
+  const float* __restrict__ img = S.img;
+  const int pitch = S.pitch;
+  float Ss = 0.f, SSs = 0.f, IS = 0.f;
+#pragma unroll 1
+  for (int a = 0; a < wn; ++a) {
+    const int dy = -wr + a * ws;
+    const float sy = fy + (float)dy;
+    const float rx = fmaf(H[1], sy, H[2]);
+    const float ry = fmaf(H[4], sy, H[5]);
+    const float rz = fmaf(H[7], sy, H[8]);
+    const float* trow = rw.t + dy * rw.tw;
+    const float* wrow = rw.wc + a * wn * NT;
+    auto tap = [&](int b) {
+      const int dx = -wr + b * ws;
+      const float sx = fx + (float)dx;
+      const float ik = trow[dx];
+      float w;
+      if (CW) {
+        w = wrow[b * NT];
+      } else {
+        float d = rs.ic - ik;
+        w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
+      }
+      const float zz = fmaf(H[6], sx, rz);
+      float sv = 0.f;
+      if (zz > 1e-8f) {
+        const float izz = m_rcp(zz);
+        sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+      }
+      const float wsv = w * sv;
+      Ss = Ss + wsv;
+      SSs = fmaf(wsv, sv, SSs);
+      IS = fmaf(wsv, ik, IS);
+    };
+    if constexpr (WR != 0) {
+#pragma unroll
+      for (int b = 0; b < (2 * WR) / WS + 1; ++b) tap(b);
+    } else {
+#pragma unroll 1
+      for (int b = 0; b < wn; ++b) tap(b);
+    }
+  }
+  float iW = 1.0f / rs.W;
+  float mus = Ss * iW;
+  float vars = SSs * iW - mus * mus;
+  if (vars < 1e-5f) return 2.0f;
+  float cov = IS * iW - rs.mu * mus;
+#if PS_FAST
+  float c = 1.0f - cov * rsqrtf(rs.var * vars);
+#else
+  float c = 1.0f - cov / sqrtf(rs.var * vars);
+#endif
+  return fminf(fmaxf(c, 0.0f), 2.0f);
+}
+
+// Forward/backward reprojection error through the source snapshot (patchmatch.cu:292-314); INF on failure.
+#define PS_INF_ERR 1e30f
+__device__ float geo_error(const PsRun& P, const PsLevel& R, const PsLevel& S, const PsPair& pr, int x, int y,
+                           float d) {
+  long long off = P.snap_off[pr.src];
+  if (off < 0) return PS_INF_ERR;
+  float3 X = make_float3(((float)x - R.cx) / R.fx * d, ((float)y - R.cy) / R.fy * d, d);
+  float xj = pr.r[0] * X.x + pr.r[1] * X.y + pr.r[2] * X.z + pr.t[0];
+  float yj = pr.r[3] * X.x + pr.r[4] * X.y + pr.r[5] * X.z + pr.t[1];
+  float zj = pr.r[6] * X.x + pr.r[7] * X.y + pr.r[8] * X.z + pr.t[2];
+  if (!(zj > 1e-8f)) return PS_INF_ERR;
+  float u = S.fx * xj / zj + S.cx, v = S.fy * yj / zj + S.cy;
+  float uf = floorf(u + 0.5f), vf = floorf(v + 0.5f);
+  if (!(uf >= 0.f && vf >= 0.f && uf < (float)S.w && vf < (float)S.h)) return PS_INF_ERR;
+  float dj = __ldg(P.snap + off + (long long)vf * S.w + (long long)uf);
+  if (!(dj > 0.f)) return PS_INF_ERR;
+  float3 Yj = make_float3((u - S.cx) / S.fx * dj, (v - S.cy) / S.fy * dj, dj);
+  float3 q = make_float3(Yj.x - pr.t[0], Yj.y - pr.t[1], Yj.z - pr.t[2]);
+  float Yx = pr.r[0] * q.x + pr.r[3] * q.y + pr.r[6] * q.z;
+  float Yy = pr.r[1] * q.x + pr.r[4] * q.y + pr.r[7] * q.z;
+  float Yz = pr.r[2] * q.x + pr.r[5] * q.y + pr.r[8] * q.z;
+  if (!(Yz > 1e-8f)) return PS_INF_ERR;
+  float cx = R.fx * Yx / Yz + R.cx - (float)x, cy = R.fy * Yy / Yz + R.cy - (float)y;
+  return sqrtf(cx * cx + cy * cy);
+}
+
+// (photometric cost, truncated geometric error) of one hypothesis × one source (patchmatch.cu:316-324).
+template <int WR, int WS, bool CW, int NT>
+__device__ __forceinline__ float pair_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& R,
+                                           const PsLevel& S, const PsPair& pr, const PsLPair& lp, int x, int y,
+                                           float4 h, float* geo) {
+  float H[9];
+  float c = 2.0f;
+  if (homography(R, lp, (float)x, (float)y, h, H)) c = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y);
+  if (P.geometric) *geo = fminf(geo_error(P, R, S, pr, x, y, h.w), P.gmax);
+  return c;
+}
+
+// Random normal toward the camera (patchmatch.cu:348-361), random depth (:363-366), perturbed normal (:368-384).
+__device__ float3 random_normal(u64& st, float3 ray) {
+  float3 n = make_float3(0.f, 0.f, -1.f);
+  for (int k = 0; k < 64; ++k) {
+    float v1 = 2.f * rnd(st) - 1.f, v2 = 2.f * rnd(st) - 1.f;
+    float s = v1 * v1 + v2 * v2;
+    if (s < 1.f && s > 0.f) {
+      float r = 2.f * sqrtf(1.f - s);
+      n = make_float3(v1 * r, v2 * r, 1.f - 2.f * s);
+      break;
+    }
+  }
+  if (dot3(n, ray) > 0.f) n = make_float3(-n.x, -n.y, -n.z);
+  return n;
+}
+__device__ __forceinline__ float random_depth(u64& st, float dmin, float dmax) {
+  float a = 1.f / dmax, b = 1.f / dmin;
+  return 1.f / (a + rnd(st) * (b - a));
+}
+__device__ float3 perturb_normal(u64& st, float3 n, float3 ray, float phi) {
+  float3 a = random_normal(st, make_float3(0.f, 0.f, 0.f));
+  float3 ax = cross3(a, n);
+  float l2 = dot3(ax, ax);
+  float ang = rnd(st) * phi;
+  if (l2 < 1e-12f) return n;
+  ax = nrm3(ax);
+  float3 bn = cross3(ax, n);
+  for (int k = 0; k < 4; ++k) {
+    float sa, ca;
+    m_sincos(ang, &sa, &ca);
+    float3 m = make_float3(n.x * ca + bn.x * sa, n.y * ca + bn.y * sa, n.z * ca + bn.z * sa);
+    if (dot3(m, ray) < 0.f) return nrm3(m);
+    ang *= 0.5f;
+  }
+  return n;
+}
+
+// Triangulation × incidence × resolution prior (patchmatch.cu:388-422).
+__device__ float view_prior(const PsRun& P, const PsLevel& R, const PsPair& pr, const float* H, bool hok, int x, int y,
+                            float4 h, int wr) {
+  if (!hok) return 0.f;
+  float3 ray = pixel_ray(R, x, y);
+  float3 X = make_float3(ray.x * h.w, ray.y * h.w, h.w);
+  float3 S = make_float3(pr.c[0] - X.x, pr.c[1] - X.y, pr.c[2] - X.z);
+  float ls = sqrtf(dot3(S, S)), lx = sqrtf(dot3(X, X));
+  if (ls <= 0.f || lx <= 0.f) return 0.f;
+  float cost = -dot3(S, X) / (ls * lx);
+  float tri = 1.f;
+  if (cost > P.cos_tri_min) {
+    float s = 1.f - (1.f - cost) / (1.f - P.cos_tri_min);
+    tri = fminf(fmaxf(1.f - s * s, 0.f), 1.f);
+  }
+  float cphi = dot3(S, make_float3(h.x, h.y, h.z)) / ls;
+  float xi = 1.f - fmaxf(0.f, cphi);
+  float inc = m_exp(-xi * xi * P.inv2inc);
+  float r = (float)wr;
+  float cxs[4] = {x - r, x - r, x + r, x + r};
+  float cys[4] = {y - r, y + r, y + r, y - r};
+  float px[4], py[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float z = H[6] * cxs[k] + H[7] * cys[k] + H[8];
+    if (!(z > 1e-8f)) return 0.f;
+    px[k] = (H[0] * cxs[k] + H[1] * cys[k] + H[2]) / z;
+    py[k] = (H[3] * cxs[k] + H[4] * cys[k] + H[5]) / z;
+  }
+  float area = 0.f;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) area += px[k] * py[(k + 1) & 3] - px[(k + 1) & 3] * py[k];
+  area = 0.5f * fabsf(area);
+  float aref = (2.f * r + 1.f) * (2.f * r + 1.f);
+  if (!(area > 0.f)) return 0.f;
+  float res = fminf(area / aref, aref / area);
+  return tri * inc * res;
+}
+
+// Propagation offsets of the 8 regions in order (patchmatch.cu:424-436, :480-490): regions 0-3 are the V shapes
+// (0,-1),(±1,-2),(±2,-3),(±3,-4) rotated up→right→down→left by (dx,dy)→(-dy,dx); regions 4-7 the bands
+// (0,-3),(0,-5),…,(0,-23) with the same rotations.  Every offset has odd |dx|+|dy| (opposite colour).
+__constant__ int2 c_prop[72];
+
+__device__ __forceinline__ int find_item(const PsRun& P, int cta) {
+  int lo = 0, hi = P.nitems - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    if (P.items[mid].tile0 <= cta) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// ================================================================================ half step (patchmatch.cu:439-657)
+template <int WR, int WS, bool CW>
+__global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_HALF_NT;
+  extern __shared__ float sm[];
+  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
+  const int wn = (2 * wr) / ws + 1;
+  const int TW = PS_HALF_PW + 2 * wr, TH = PS_HALF_PH + 2 * wr;
+  float* tile = sm;
+  float* wcache = sm + ((TW * TH + 31) & ~31);
+  float* wvs = wcache + (CW ? wn * wn * NT : 0);
+
+  const int ii = find_item(P, blockIdx.x);
+  const PsItem& it = P.items[ii];
+  const int w = it.w, h = it.h;
+  const int tiles_x = (w + PS_HALF_PW - 1) / PS_HALF_PW;
+  const int tl = blockIdx.x - it.tile0;
+  const int x0 = (tl % tiles_x) * PS_HALF_PW, y0 = (tl / tiles_x) * PS_HALF_PH;
+  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
+  {
+    const int ox = x0 - wr, oy = y0 - wr;
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+      int tx = i % TW, ty = i / TW;
+      int gx = ox + tx, gy = oy + ty;
+      tile[i] = (gx >= 0 && gy >= 0 && gx < w && gy < h) ? R.img[gy * R.pitch + gx] : 0.f;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row = 2 * warp + (lane >> 4), col = lane & 15;
+  const int y = y0 + row;
+  const int x = x0 + 2 * col + ((y + P.color) & 1);
+  if (x >= w || y >= h) return;
+
+  RefWin rw;
+  rw.t = tile + (row + wr) * TW + (x - x0 + wr);
+  rw.tw = TW;
+  rw.wc = wcache + threadIdx.x;
+  float* wv = wvs + threadIdx.x;
+
+  const PsView& vd = P.views[it.view];
+  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
+  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
+  const int nsrc = vd.nsrc;
+  const long long base = it.off;
+  const int pix = y * w + x;
+  float4* pl = P.plane + base;
+  const float* co = P.cost + base;
+  const float3 ray = pixel_ray(R, x, y);
+
+  // 1. Candidates: current + 8 regions.
+  float4 hyp[9];
+  hyp[0] = pl[pix];
+#pragma unroll 1
+  for (int r = 0; r < 8; ++r) {
+    const int k0 = r < 4 ? r * 7 : 28 + (r - 4) * 11;
+    const int cnt = r < 4 ? 7 : 11;
+    float best = 1e30f;
+    int bq = -1, bx = 0, by = 0;
+    for (int k = 0; k < cnt; ++k) {
+      const int2 o = c_prop[k0 + k];
+      const int qx = x + o.x, qy = y + o.y;
+      if (qx < 0 || qy < 0 || qx >= w || qy >= h) continue;
+      const float c = co[qy * w + qx];
+      if (c < best) {
+        best = c;
+        bq = qy * w + qx;
+        bx = qx;
+        by = qy;
+      }
+    }
+    hyp[1 + r] = hyp[0];
+    if (bq >= 0) {
+      const float4 q = pl[bq];
+      const float3 n = make_float3(q.x, q.y, q.z);
+      const float3 rq = pixel_ray(R, bx, by);
+      const float den = dot3(n, ray);
+      if (den < -1e-6f && q.w > 0.f) {
+        const float d = q.w * dot3(n, rq) / den;
+        if (d > 0.f && isfinite(d)) hyp[1 + r] = make_float4(n.x, n.y, n.z, d);
+      }
+    }
+  }
+
+  // 2. View traversal: voting, weighting, aggregation.
+  const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
+  const int vprev = P.bview[base + pix];
+  float num[9], numf[9];
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    num[i] = 0.f;
+    numf[i] = 0.f;
+  }
+  float den = 0.f, wbest = 0.f, denf = 0.f;
+  int vbest = 255;
+#pragma unroll 1
+  for (int j = 0; j < nsrc; ++j) {
+    const PsPair& pr = prs[j];
+    const PsLPair lp = lps[j];
+    const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
+    float m[9], gg[9];
+    float prior;
+    wv[j * NT] = 0.f;
+    {
+      float H[9];
+      const bool ok = homography(R, lp, (float)x, (float)y, hyp[0], H);
+      prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
+      if (!(prior > 0.f)) continue;
+      m[0] = ok ? ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y) : 2.f;
+      gg[0] = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[0].w), P.gmax) : 0.f;
+    }
+#pragma unroll 1
+    for (int i = 1; i < 9; ++i) {
+      float H[9];
+      const bool ok = homography(R, lp, (float)x, (float)y, hyp[i], H);
+      const float mi = ok ? ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y) : 2.f;
+      const float gi = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[i].w), P.gmax) : 0.f;
+#pragma unroll
+      for (int q = 1; q < 9; ++q)
+        if (q == i) {
+          m[q] = mi;
+          gg[q] = gi;
+        }
+    }
+    int good = 0, bad = 0;
+    float conf = 0.f;
+#pragma unroll
+    for (int i = 1; i < 9; ++i) {
+      if (m[i] < P.tau_good) {
+        good++;
+        conf += m_exp(-m[i] * m[i] * P.inv2beta2);
+      }
+      if (m[i] > P.tau_bad) bad++;
+    }
+    const bool adopt = good > P.n1 && bad < P.n2;
+    const bool isprev = j == vprev;
+    const float wp = adopt ? (isprev ? 2.f : 1.f) * conf / (float)good : (isprev ? P.prev_w : 0.f);
+    const float w2 = wp * prior;
+    wv[j * NT] = w2 > 0.f ? w2 : -prior;
+#pragma unroll
+    for (int i = 0; i < 9; ++i) numf[i] += prior * (m[i] + P.lambda * gg[i]);
+    denf += prior;
+    if (w2 > 0.f) {
+#pragma unroll
+      for (int i = 0; i < 9; ++i) num[i] += w2 * (m[i] + P.lambda * gg[i]);
+      den += w2;
+      if (w2 > wbest) {
+        wbest = w2;
+        vbest = j;
+      }
+    }
+  }
+  float agg[9];
+  int bi9 = 0;
+  if (den > 0.f) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = num[i] / den;
+  } else if (denf > 0.f) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = numf[i] / denf;
+    for (int j = 0; j < nsrc; ++j) wv[j * NT] = -wv[j * NT];
+    den = denf;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = 2.f;
+  }
+  float bagg = agg[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i)
+    if (agg[i] < bagg) {
+      bagg = agg[i];
+      bi9 = i;
+    }
+  float4 best = hyp[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i)
+    if (i == bi9) best = hyp[i];
+  float bcost = bagg;
+
+  // 3. Refinement, 6 hypotheses (patchmatch.cu:596-628), then 4. the coarse-scale candidate (:629-653).
+  u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, P.t, P.color, (u64)pix);
+  const float d_r = random_depth(st, vd.dmin, vd.dmax);
+  const float3 n_r = random_normal(st, ray);
+  const float uu = 2.f * rnd(st) - 1.f;
+  const float inv = best.w > 0.f ? (1.f / best.w) * (1.f + uu * P.eps) : -1.f;
+  const float d_p = inv > 0.f ? 1.f / inv : d_r;
+  if (!(best.w > 0.f)) best.w = d_r;
+  const float3 n0 = make_float3(best.x, best.y, best.z);
+  const float3 n_p = perturb_normal(st, n0, ray, P.phi);
+  const float bw = best.w;
+  bool has_prior = false;
+  float4 qprior = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (P.use_prior && rs.var < P.weak_var) {
+    qprior = P.prior[base + pix];
+    has_prior = qprior.w > 0.f && dot3(make_float3(qprior.x, qprior.y, qprior.z), ray) < 0.f;
+  }
+  const int ncand = has_prior ? 7 : 6;
+#pragma unroll 1
+  for (int c = 0; c < ncand; ++c) {
+    float4 cd;
+    switch (c) {
+      case 0: cd = make_float4(n0.x, n0.y, n0.z, d_r); break;
+      case 1: cd = make_float4(n_r.x, n_r.y, n_r.z, bw); break;
+      case 2: cd = make_float4(n_r.x, n_r.y, n_r.z, d_r); break;
+      case 3: cd = make_float4(n0.x, n0.y, n0.z, d_p); break;
+      case 4: cd = make_float4(n_p.x, n_p.y, n_p.z, bw); break;
+      case 5: cd = make_float4(n_p.x, n_p.y, n_p.z, d_p); break;
+      default: cd = qprior; break;
+    }
+    float cc;
+    if (den > 0.f) {
+      float nm = 0.f;
+#pragma unroll 1
+      for (int j = 0; j < nsrc; ++j) {
+        const float wj = wv[j * NT];
+        if (!(wj > 0.f)) continue;
+        const PsPair& pr = prs[j];
+        const PsLPair lp = lps[j];
+        const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
+        float g = 0.f;
+        const float mm = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, cd, &g);
+        nm += wj * (mm + P.lambda * g);
+      }
+      cc = nm / den;
+    } else {
+      cc = 2.f;
+    }
+    if (cc < bcost) {
+      bcost = cc;
+      best = cd;
+    }
+  }
+  pl[pix] = best;
+  P.cost[base + pix] = bcost;
+  P.bview[base + pix] = (unsigned char)vbest;
+}
+
+// ================================================================================ run start / evaluate (patchmatch.cu:661-692)
+// Top-K mean cost (patchmatch.cu:327-345).
+template <int WR, int WS, bool CW, int NT>
+__device__ float topk_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& R, const PsPair* prs,
+                           const PsLPair* lps, int nsrc, int x, int y, float4 h) {
+  float b0 = 1e30f, b1 = 1e30f, b2 = 1e30f;
+#pragma unroll 1
+  for (int j = 0; j < nsrc; ++j) {
+    const PsPair& pr = prs[j];
+    const PsLPair lp = lps[j];
+    const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
+    float g = 0.f;
+    float c = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, h, &g);
+    if (P.geometric) c += P.lambda * g;
+    if (c < b0) {
+      b2 = b1;
+      b1 = b0;
+      b0 = c;
+    } else if (c < b1) {
+      b2 = b1;
+      b1 = c;
+    } else if (c < b2) {
+      b2 = c;
+    }
+  }
+  const int k = min(P.topk, nsrc);
+  float s = b0;
+  if (k >= 2) s += b1;
+  if (k >= 3) s += b2;
+  return k > 0 ? s / (float)k : 2.0f;
+}
+
+// Loads the 32 × 4 reference tile of an evaluate/filter CTA; returns false for threads outside the image.
+struct EvalCtx {
+  int x, y, w, h;
+  const PsItem* it;
+  PsLevel R;
+};
+__device__ __forceinline__ bool eval_tile(const PsRun& P, float* tile, int wr, EvalCtx& e) {
+  const int ii = find_item(P, blockIdx.x);
+  const PsItem& it = P.items[ii];
+  e.it = &it;
+  e.w = it.w;
+  e.h = it.h;
+  const int tiles_x = (it.w + PS_EVAL_PW - 1) / PS_EVAL_PW;
+  const int tl = blockIdx.x - it.tile0;
+  const int x0 = (tl % tiles_x) * PS_EVAL_PW, y0 = (tl / tiles_x) * PS_EVAL_PH;
+  e.R = P.lv[it.view * P.nlevels + P.level];
+  const int TW = PS_EVAL_PW + 2 * wr, TH = PS_EVAL_PH + 2 * wr;
+  const int ox = x0 - wr, oy = y0 - wr;
+  for (int i = threadIdx.x; i < TW * TH; i += PS_EVAL_NT) {
+    int tx = i % TW, ty = i / TW;
+    int gx = ox + tx, gy = oy + ty;
+    tile[i] = (gx >= 0 && gy >= 0 && gx < it.w && gy < it.h) ? e.R.img[gy * e.R.pitch + gx] : 0.f;
+  }
+  __syncthreads();
+  e.x = x0 + (threadIdx.x & 31);
+  e.y = y0 + (threadIdx.x >> 5);
+  return e.x < it.w && e.y < it.h;
+}
+
+template <int WR, int WS, bool CW>
+__global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_EVAL_NT;
+  extern __shared__ float sm[];
+  const int wr = WR ? WR : P.wr;
+  const int TW = PS_EVAL_PW + 2 * wr, TH = PS_EVAL_PH + 2 * wr;
+  EvalCtx e;
+  if (!eval_tile(P, sm, wr, e)) return;
+  const int x = e.x, y = e.y;
+  RefWin rw;
+  {
+    const int tiles_x = (e.w + PS_EVAL_PW - 1) / PS_EVAL_PW;
+    const int tl = blockIdx.x - e.it->tile0;
+    const int x0 = (tl % tiles_x) * PS_EVAL_PW, y0 = (tl / tiles_x) * PS_EVAL_PH;
+    rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
+  }
+  rw.tw = TW;
+  rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
+  const PsItem& it = *e.it;
+  const PsView& vd = P.views[it.view];
+  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
+  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
+  const int pix = y * e.w + x;
+  const long long base = it.off;
+  const float3 ray = pixel_ray(e.R, x, y);
+  float4 h = P.plane[base + pix];
+  if (P.mode == 1 && P.random_init) {
+    u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, 0xFFFF, 0, (u64)pix);
+    const float d = random_depth(st, vd.dmin, vd.dmax);
+    const float3 n = random_normal(st, ray);
+    h = make_float4(n.x, n.y, n.z, d);
+    P.plane[base + pix] = h;
+  }
+  float c = 2.f;
+  if (h.w > 0.f) {
+    const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
+    c = topk_cost<WR, WS, CW, NT>(P, rw, rs, e.R, prs, lps, vd.nsrc, x, y, h);
+  }
+  P.cost[base + pix] = c;
+  if (P.mode == 1) P.bview[base + pix] = 255;
+}
+
+// ================================================================================ final readout (patchmatch.cu:695-737)
+template <int WR, int WS, bool CW>
+__global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_EVAL_NT;
+  extern __shared__ float sm[];
+  const int wr = WR ? WR : P.wr;
+  const int TW = PS_EVAL_PW + 2 * wr, TH = PS_EVAL_PH + 2 * wr;
+  EvalCtx e;
+  if (!eval_tile(P, sm, wr, e)) return;
+  const int x = e.x, y = e.y;
+  const PsItem& it = *e.it;
+  RefWin rw;
+  {
+    const int tiles_x = (e.w + PS_EVAL_PW - 1) / PS_EVAL_PW;
+    const int tl = blockIdx.x - it.tile0;
+    const int x0 = (tl % tiles_x) * PS_EVAL_PW, y0 = (tl / tiles_x) * PS_EVAL_PH;
+    rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
+  }
+  rw.tw = TW;
+  rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
+  const PsView& vd = P.views[it.view];
+  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
+  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
+  const int pix = y * e.w + x;
+  const long long base = it.off;
+  const float4 h = P.plane[base + pix];
+  int count = 0;
+  if (h.w > 0.f) {
+    const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
+    const float3 ray = pixel_ray(e.R, x, y);
+    const float3 X = make_float3(ray.x * h.w, ray.y * h.w, h.w);
+    const float lx = sqrtf(dot3(X, X));
+#pragma unroll 1
+    for (int j = 0; j < vd.nsrc; ++j) {
+      const PsPair& pr = prs[j];
+      const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
+      const float3 Sv = make_float3(pr.c[0] - X.x, pr.c[1] - X.y, pr.c[2] - X.z);
+      const float ls = sqrtf(dot3(Sv, Sv));
+      if (!(ls > 0.f)) continue;
+      const float cost = -dot3(Sv, X) / (ls * lx);
+      if (cost > P.cos_filter_tri) continue;
+      const float cphi = dot3(Sv, make_float3(h.x, h.y, h.z)) / ls;
+      if (cphi <= 0.f) continue;
+      float H[9];
+      const PsLPair lp = lps[j];
+      if (!homography(e.R, lp, (float)x, (float)y, h, H)) continue;
+      const float m = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y);
+      const float ee = P.ncc_norm * m_exp(-m * m * P.inv2ncc);
+      if (ee / (ee + 0.5f) < P.q_min) continue;
+      if (geo_error(P, e.R, S, pr, x, y, h.w) > P.filter_gmax) continue;
+      count++;
+    }
+  }
+  P.count[base + pix] = (unsigned char)min(count, 255);
+}
+
+// Simple kernels: CTA of 32 × 8 threads, tiles flattened like the others.
+struct SimpleCtx {
+  int x, y;
+  const PsItem* it;
+};
+__device__ __forceinline__ bool simple_px(const PsRun& P, SimpleCtx& c) {
+  const int ii = find_item(P, blockIdx.x);
+  const PsItem& it = P.items[ii];
+  const int tiles_x = (it.w + PS_SIMPLE_BX - 1) / PS_SIMPLE_BX;
+  const int tl = blockIdx.x - it.tile0;
+  c.x = (tl % tiles_x) * PS_SIMPLE_BX + (int)threadIdx.x;
+  c.y = (tl / tiles_x) * PS_SIMPLE_BY + (int)threadIdx.y;
+  c.it = &it;
+  return c.x < it.w && c.y < it.h;
+}
+
+// ================================================================================ joint bilateral upsampling (patchmatch.cu:741-801)
+// Input: level-1 planes at P.prior + item.aux; output: level planes (cost reset to 2).
+__global__ void __launch_bounds__(256) k_upsample(const __grid_constant__ PsRun P) {
+  SimpleCtx c;
+  if (!simple_px(P, c)) return;
+  const PsItem& it = *c.it;
+  const int x = c.x, y = c.y;
+  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
+  const PsLevel L = P.lv[it.view * P.nlevels + P.level - 1];
+  const float4* low = P.prior + it.aux;
+  const float3 rp = pixel_ray(R, x, y);
+  const float ip = R.img[y * R.pitch + x];
+  const float px = ((float)x - 0.5f) * 0.5f, py = ((float)y - 0.5f) * 0.5f;
+  const int qx0 = (int)roundf(px), qy0 = (int)roundf(py);
+  float sw = 0.f, sd = 0.f;
+  float3 sn = make_float3(0.f, 0.f, 0.f);
+  float nd = 1e30f, ndep = 0.f;
+  float3 nn = make_float3(0.f, 0.f, 0.f);
+  for (int qy = qy0 - 2; qy <= qy0 + 2; ++qy) {
+    if (qy < 0 || qy >= L.h) continue;
+    for (int qx = qx0 - 2; qx <= qx0 + 2; ++qx) {
+      if (qx < 0 || qx >= L.w) continue;
+      const float4 q = low[qy * L.w + qx];
+      if (!(q.w > 0.f)) continue;
+      const float3 n = make_float3(q.x, q.y, q.z);
+      const float den = dot3(n, rp);
+      if (!(den < -1e-6f)) continue;
+      const float d = q.w * dot3(n, pixel_ray(L, qx, qy)) / den;
+      if (!(d > 0.f) || !isfinite(d)) continue;
+      const float ds = ((float)qx - px) * ((float)qx - px) + ((float)qy - py) * ((float)qy - py);
+      if (ds < nd) {
+        nd = ds;
+        ndep = d;
+        nn = n;
+      }
+      const float iq = L.img[qy * L.pitch + qx];
+      const float wgt = m_exp(-ds * P.up_inv2s - (ip - iq) * (ip - iq) * P.up_inv2c);
+      sw += wgt;
+      sd += wgt * d;
+      sn.x += wgt * n.x;
+      sn.y += wgt * n.y;
+      sn.z += wgt * n.z;
+    }
+  }
+  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  float d = 0.f;
+  float3 n = make_float3(0.f, 0.f, 0.f);
+  bool ok = false;
+  if (sw > 1e-12f) {
+    d = sd / sw;
+    n = sn;
+    ok = true;
+  } else if (nd < 1e29f) {
+    d = ndep;
+    n = nn;
+    ok = true;
+  }
+  if (ok && dot3(n, n) > 1e-24f) {
+    n = nrm3(n);
+    if (dot3(n, rp) >= 0.f) n = make_float3(-n.x, -n.y, -n.z);
+    out = make_float4(n.x, n.y, n.z, d);
+  }
+  P.plane[it.off + y * it.w + x] = out;
+  P.cost[it.off + y * it.w + x] = 2.f;
+}
+
+// ================================================================================ 5×5 median plane filter (patchmatch.cu:805-849)
+// Input: planes at P.prior + item.aux (same level); output: P.plane at item.off.
+__global__ void __launch_bounds__(256) k_median(const __grid_constant__ PsRun P) {
+  SimpleCtx c;
+  if (!simple_px(P, c)) return;
+  const PsItem& it = *c.it;
+  const int x = c.x, y = c.y, w = it.w, h = it.h;
+  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
+  const float4* in = P.prior + it.aux;
+  const float4 self = in[y * w + x];
+  if (!(self.w > 0.f)) {
+    P.plane[it.off + y * w + x] = self;
+    return;
+  }
+  const float3 rp = pixel_ray(R, x, y);
+  float ds[25];
+  int qs[25];
+  int cnt = 0;
+  for (int qy = max(y - 2, 0); qy < min(y + 3, h); ++qy) {
+    for (int qx = max(x - 2, 0); qx < min(x + 3, w); ++qx) {
+      const float4 q = in[qy * w + qx];
+      if (!(q.w > 0.f)) continue;
+      const float3 n = make_float3(q.x, q.y, q.z);
+      const float den = dot3(n, rp);
+      if (!(den < -1e-6f)) continue;
+      const float d = q.w * dot3(n, pixel_ray(R, qx, qy)) / den;
+      if (!(d > 0.f) || !isfinite(d)) continue;
+      const int qi = qy * w + qx;
+      int k = cnt++;
+      while (k > 0 && (ds[k - 1] > d || (ds[k - 1] == d && qs[k - 1] > qi))) {
+        ds[k] = ds[k - 1];
+        qs[k] = qs[k - 1];
+        --k;
+      }
+      ds[k] = d;
+      qs[k] = qi;
+    }
+  }
+  float4 out = self;
+  if (cnt > 0) {
+    const int m = (cnt - 1) / 2;
+    const float4 q = in[qs[m]];
+    out = make_float4(q.x, q.y, q.z, ds[m]);
+  }
+  P.plane[it.off + y * w + x] = out;
+}
+
+// ================================================================================ helpers
+// Snapshot capture: depth channel of the resident planes into the snapshot buffer (item.aux = snapshot offset).
+__global__ void __launch_bounds__(256) k_snapshot(const __grid_constant__ PsRun P, float* snap) {
+  SimpleCtx c;
+  if (!simple_px(P, c)) return;
+  const PsItem& it = *c.it;
+  const int pix = c.y * it.w + c.x;
+  snap[it.aux + pix] = P.plane[it.off + pix].w;
+}
+
+// Readout threshold (crates/dense/src/densify.rs:441-454): depth/normal zeroed where count < need.
+__global__ void __launch_bounds__(256) k_readout(const __grid_constant__ PsRun P, float4* out) {
+  SimpleCtx c;
+  if (!simple_px(P, c)) return;
+  const PsItem& it = *c.it;
+  const int pix = c.y * it.w + c.x;
+  const int nsrc = P.views[it.view].nsrc;
+  int need = min(P.need_min, nsrc);
+  if (need < 1) need = 1;
+  const float4 q = P.plane[it.off + pix];
+  const bool keep = q.w > 0.f && (int)P.count[it.off + pix] >= need;
+  out[it.off + pix] = keep ? q : make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// FP64 homography setup A = K_j R K^-1, b = K_j t for every (view, level, source) (crates/cuda/src/patchmatch.rs:132-151).
+// One thread per (view, level, source); r/t come from pairs_f64 when given (15 doubles per source), else from the
+// f32 pair table.
+__global__ void k_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64, const int* has64,
+                               PsLPair* out, int nviews, int nlevels) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= nviews * nlevels * PS_MAXSRC) return;
+  const int j = idx % PS_MAXSRC;
+  const int l = (idx / PS_MAXSRC) % nlevels;
+  const int v = idx / (PS_MAXSRC * nlevels);
+  const PsPair& pr = pairs[v * PS_MAXSRC + j];
+  PsLPair o;
+  for (int k = 0; k < 9; ++k) o.A[k] = 0.f;
+  for (int k = 0; k < 3; ++k) o.b[k] = 0.f;
+  if (pr.src >= 0) {
+    const PsLevel& R = lv[v * nlevels + l];
+    const PsLevel& J = lv[pr.src * nlevels + l];
+    double r[9], t[3];
+    if (has64[v]) {
+      const double* p = pairs64 + ((size_t)v * PS_MAXSRC + j) * 15;
+      for (int k = 0; k < 9; ++k) r[k] = p[k];
+      for (int k = 0; k < 3; ++k) t[k] = p[9 + k];
+    } else {
+      for (int k = 0; k < 9; ++k) r[k] = (double)pr.r[k];
+      for (int k = 0; k < 3; ++k) t[k] = (double)pr.t[k];
+    }
+    const double fx = R.fx, fy = R.fy, cx = R.cx, cy = R.cy;
+    const double kinv[3][3] = {{1.0 / fx, 0.0, -cx / fx}, {0.0, 1.0 / fy, -cy / fy}, {0.0, 0.0, 1.0}};
+    const double kj[3][3] = {{(double)J.fx, 0.0, (double)J.cx}, {0.0, (double)J.fy, (double)J.cy}, {0.0, 0.0, 1.0}};
+    double kr[3][3];
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) kr[i][k] = kj[i][0] * r[0 * 3 + k] + kj[i][1] * r[1 * 3 + k] + kj[i][2] * r[2 * 3 + k];
+    for (int i = 0; i < 3; ++i)
+      for (int k = 0; k < 3; ++k) o.A[i * 3 + k] = (float)(kr[i][0] * kinv[0][k] + kr[i][1] * kinv[1][k] + kr[i][2] * kinv[2][k]);
+    for (int i = 0; i < 3; ++i) o.b[i] = (float)(kj[i][0] * t[0] + kj[i][1] * t[1] + kj[i][2] * t[2]);
+  }
+  out[idx] = o;
+}
+
+// ================================================================================ launchers
+#define PS_SPECS(X) X(5, 1) X(6, 1) X(5, 2) X(3, 1)
+
+static int g_prop_ready = 0;
+
+static cudaError_t init_constants() {
+  if (g_prop_ready) return cudaSuccess;
+  int2 h[72];
+  const int V[7][2] = {{0, -1}, {-1, -2}, {1, -2}, {-2, -3}, {2, -3}, {-3, -4}, {3, -4}};
+  int n = 0;
+  for (int r = 0; r < 8; ++r) {
+    const int dir = r & 3;
+    const bool strip = r >= 4;
+    const int cnt = strip ? 11 : 7;
+    for (int k = 0; k < cnt; ++k) {
+      int dx = strip ? 0 : V[k][0], dy = strip ? -(3 + 2 * k) : V[k][1];
+      for (int q = 0; q < dir; ++q) {
+        int t = dx;
+        dx = -dy;
+        dy = t;
+      }
+      h[n++] = make_int2(dx, dy);
+    }
+  }
+  cudaError_t e = cudaMemcpyToSymbol(c_prop, h, sizeof h);
+  if (e == cudaSuccess) g_prop_ready = 1;
+  return e;
+}
+
+size_t half_smem(int wr, int ws, bool cw, int maxsrc) {
+  const int wn = (2 * wr) / ws + 1;
+  const int TW = PS_HALF_PW + 2 * wr, TH = PS_HALF_PH + 2 * wr;
+  size_t f = ((TW * TH + 31) & ~31) + (cw ? (size_t)wn * wn * PS_HALF_NT : 0) + (size_t)maxsrc * PS_HALF_NT;
+  return f * sizeof(float);
+}
+size_t eval_smem(int wr, int ws, bool cw) {
+  const int wn = (2 * wr) / ws + 1;
+  const int TW = PS_EVAL_PW + 2 * wr, TH = PS_EVAL_PH + 2 * wr;
+  size_t f = ((TW * TH + 31) & ~31) + (cw ? (size_t)wn * wn * PS_EVAL_NT : 0);
+  return f * sizeof(float);
+}
+
+// Whether the weight cache fits (<= 200 KB of shared memory per CTA with the largest source count).
+static bool use_cache(int wr, int ws) { return half_smem(wr, ws, true, PS_MAXSRC) <= 200 * 1024; }
+
+template <typename K>
+static cudaError_t launch(K kern, int ncta, int nt, size_t smem, cudaStream_t st, const PsRun& P) {
+  static_assert(sizeof(PsRun) < 32000, "kernel parameter block too large");
+  if (ncta <= 0) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  kern<<<ncta, nt, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_half(const PsRun& P, cudaStream_t st) {
+  cudaError_t e = init_constants();
+  if (e != cudaSuccess) return e;
+  const bool cw = use_cache(P.wr, P.ws);
+  const size_t smem = half_smem(P.wr, P.ws, cw, P.maxsrc);
+#define PS_CASE(a, b) \
+  if (P.wr == a && P.ws == b) return launch(k_half<a, b, true>, P.ntiles, PS_HALF_NT, smem, st, P);
+  PS_SPECS(PS_CASE)
+#undef PS_CASE
+  if (cw) return launch(k_half<0, 1, true>, P.ntiles, PS_HALF_NT, smem, st, P);
+  return launch(k_half<0, 1, false>, P.ntiles, PS_HALF_NT, smem, st, P);
+}
+
+cudaError_t launch_eval(const PsRun& P, cudaStream_t st) {
+  const bool cw = use_cache(P.wr, P.ws);
+  const size_t smem = eval_smem(P.wr, P.ws, cw);
+#define PS_CASE(a, b) \
+  if (P.wr == a && P.ws == b) return launch(k_eval<a, b, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  PS_SPECS(PS_CASE)
+#undef PS_CASE
+  if (cw) return launch(k_eval<0, 1, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  return launch(k_eval<0, 1, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+}
+
+cudaError_t launch_filter(const PsRun& P, cudaStream_t st) {
+  const bool cw = use_cache(P.wr, P.ws);
+  const size_t smem = eval_smem(P.wr, P.ws, cw);
+#define PS_CASE(a, b) \
+  if (P.wr == a && P.ws == b) return launch(k_filter<a, b, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  PS_SPECS(PS_CASE)
+#undef PS_CASE
+  if (cw) return launch(k_filter<0, 1, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  return launch(k_filter<0, 1, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+}
+
+cudaError_t launch_upsample(const PsRun& P, cudaStream_t st) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_upsample<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P);
+  return cudaGetLastError();
+}
+cudaError_t launch_median(const PsRun& P, cudaStream_t st) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_median<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P);
+  return cudaGetLastError();
+}
+cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_snapshot<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, snap);
+  return cudaGetLastError();
+}
+cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_readout<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64, const int* has64,
+                                PsLPair* out, int nviews, int nlevels, cudaStream_t st) {
+  const int n = nviews * nlevels * PS_MAXSRC;
+  if (n <= 0) return cudaSuccess;
+  k_setup_lpairs<<<(n + 127) / 128, 128, 0, st>>>(lv, pairs, pairs64, has64, out, nviews, nlevels);
+  return cudaGetLastError();
+}
+
+}  // namespace PS_NS

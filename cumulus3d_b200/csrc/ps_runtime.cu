@@ -1,0 +1,947 @@
+// Host runtime of the B200 PatchStereo engine and its C ABI (include/patchstereo.h).
+//
+// It plays the role of the reference's CUDA session (crates/cuda/src/patchmatch.rs:285-1009): one session per
+// backend, one stream per session, every image of every level resident in HBM for the session's lifetime.  The
+// B200 design differs in these points:
+//   * images are uploaded once as normalised f32 planes with a zero border (no CUDA arrays / texture objects);
+//   * per-pixel state lives in per-level "slots" (plane float4, cost, best view, count, prior) that persist across
+//     calls, so the host-state calls (ps_run, ps_evaluate, …) are thin wrappers over resident ones and a caller that
+//     keeps everything on the device (ps_run_resident, ps_snapshot_capture, ps_filter_resident) never copies states;
+//   * the FP64 homography setup A = K_j R K^-1, b = K_j t runs on the device once per session;
+//   * the batch table rides in the kernel parameters, tiles of all views of a batch are flattened into one grid.
+#include <cuda_runtime.h>
+#include <omp.h>
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/patchstereo.h"
+#include "ps_consts.h"
+#include "ps_types.h"
+
+#define PS_DECLARE_LAUNCHERS(NS)                                                                           \
+  namespace NS {                                                                                           \
+  cudaError_t launch_half(const PsRun& P, cudaStream_t st);                                                \
+  cudaError_t launch_eval(const PsRun& P, cudaStream_t st);                                                \
+  cudaError_t launch_filter(const PsRun& P, cudaStream_t st);                                              \
+  cudaError_t launch_upsample(const PsRun& P, cudaStream_t st);                                            \
+  cudaError_t launch_median(const PsRun& P, cudaStream_t st);                                              \
+  cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
+  cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
+  cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
+                                  const int* has64, PsLPair* out, int nviews, int nlevels, cudaStream_t st); \
+  }
+PS_DECLARE_LAUNCHERS(ps_parity)
+PS_DECLARE_LAUNCHERS(ps_fast)
+
+namespace {
+
+struct Launchers {
+  cudaError_t (*half)(const PsRun&, cudaStream_t);
+  cudaError_t (*eval)(const PsRun&, cudaStream_t);
+  cudaError_t (*filter)(const PsRun&, cudaStream_t);
+  cudaError_t (*upsample)(const PsRun&, cudaStream_t);
+  cudaError_t (*median)(const PsRun&, cudaStream_t);
+  cudaError_t (*snapshot)(const PsRun&, float*, cudaStream_t);
+  cudaError_t (*readout)(const PsRun&, float4*, cudaStream_t);
+};
+const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
+                           ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
+                           ps_parity::launch_readout};
+const Launchers kFast = {ps_fast::launch_half,     ps_fast::launch_eval,   ps_fast::launch_filter,
+                         ps_fast::launch_upsample, ps_fast::launch_median, ps_fast::launch_snapshot,
+                         ps_fast::launch_readout};
+
+struct PsError {
+  int code;
+  std::string msg;
+};
+
+inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// Per-level resident state of every view.
+struct Slot {
+  bool ready = false;
+  std::vector<long long> off;  // per view pixel offset
+  long long total = 0;
+  float4* plane = nullptr;
+  float4* aux = nullptr;    // second plane buffer (median input, readout output)
+  float4* prior = nullptr;  // coarse-scale candidates
+  float* cost = nullptr;
+  unsigned char* bview = nullptr;
+  unsigned char* count = nullptr;
+  std::vector<char> prior_valid;
+};
+
+}  // namespace
+
+struct ps_backend {
+  int device = 0;
+  ps_options opts{};
+  std::string name;
+  std::string err;
+  std::mutex mu;
+  bool busy = false;
+};
+
+struct ps_session {
+  ps_backend* be = nullptr;
+  std::string err;
+  cudaStream_t st = nullptr;
+  const Launchers* L = &kParity;
+  int nv = 0, nl = 0;
+  ps_pm_params pm{};
+  ps_filter_params fl{};
+  uint64_t seed = 0;
+  PsConsts cs{};
+  std::vector<int> w, h;  // per (view, level)
+  std::vector<int> nsrc;
+  std::vector<std::vector<int>> sources;
+  // device tables
+  float* img = nullptr;
+  PsLevel* lv = nullptr;
+  PsPair* pairs = nullptr;
+  PsLPair* lpairs = nullptr;
+  PsView* views = nullptr;
+  double* pairs64 = nullptr;
+  int* has64 = nullptr;
+  std::vector<Slot> slots;
+  // snapshot
+  float* snap = nullptr;
+  size_t snap_cap = 0;
+  long long* snap_off = nullptr;
+  int snap_level = -1;
+  bool snap_valid = false;
+  uint64_t snap_id = 0;
+  // pinned staging
+  void* pin = nullptr;
+  size_t pin_cap = 0;
+  uint64_t launches = 0;
+  size_t img_bytes = 0;
+
+  int W(int v, int l) const { return w[v * nl + l]; }
+  int H(int v, int l) const { return h[v * nl + l]; }
+};
+
+namespace {
+
+void fail(int code, const std::string& m) { throw PsError{code, m}; }
+void cuda_ok(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(e == cudaErrorMemoryAllocation ? PS_ENOMEM : PS_ECUDA,
+         std::string("CUDA: ") + what + ": " + cudaGetErrorString(e));
+  }
+}
+
+template <typename F>
+int guard(ps_session* s, F&& f) {
+  if (!s) return PS_EINVAL;
+  try {
+    cuda_ok(cudaSetDevice(s->be->device), "cudaSetDevice");
+    f();
+    s->err.clear();
+    return PS_OK;
+  } catch (const PsError& e) {
+    s->err = e.msg;
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    s->err = "host allocation failed";
+    return PS_ENOMEM;
+  } catch (...) {
+    s->err = "unexpected internal error";
+    return PS_EINVAL;
+  }
+}
+
+template <typename T>
+T* dalloc(size_t n) {
+  void* p = nullptr;
+  cuda_ok(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  return (T*)p;
+}
+
+void* pinned(ps_session* s, size_t bytes) {
+  if (bytes > s->pin_cap) {
+    if (s->pin) cudaFreeHost(s->pin);
+    s->pin = nullptr;
+    s->pin_cap = 0;
+    size_t cap = round_up(bytes + bytes / 4, 1 << 20);
+    cuda_ok(cudaMallocHost(&s->pin, cap), "cudaMallocHost");
+    s->pin_cap = cap;
+  }
+  return s->pin;
+}
+
+void check_views(ps_session* s, const uint32_t* views, size_t n) {
+  if (n > 0 && !views) fail(PS_EINVAL, "views is NULL");
+  for (size_t i = 0; i < n; ++i)
+    if (views[i] >= (uint32_t)s->nv) fail(PS_EINVAL, "view index " + std::to_string(views[i]) + " out of range");
+}
+
+Slot& slot(ps_session* s, int level) {
+  if (level < 0 || level >= s->nl) fail(PS_EINVAL, "level " + std::to_string(level) + " out of range");
+  Slot& sl = s->slots[level];
+  if (!sl.ready) {
+    sl.off.assign(s->nv, 0);
+    long long tot = 0;
+    for (int v = 0; v < s->nv; ++v) {
+      sl.off[v] = tot;
+      tot += (long long)s->W(v, level) * s->H(v, level);
+    }
+    sl.total = tot;
+    sl.plane = dalloc<float4>(tot);
+    sl.aux = dalloc<float4>(tot);
+    sl.prior = dalloc<float4>(tot);
+    sl.cost = dalloc<float>(tot);
+    sl.bview = dalloc<unsigned char>(tot);
+    sl.count = dalloc<unsigned char>(tot);
+    cuda_ok(cudaMemsetAsync(sl.plane, 0, std::max<long long>(tot, 1) * sizeof(float4), s->st), "memset");
+    cuda_ok(cudaMemsetAsync(sl.bview, 255, std::max<long long>(tot, 1), s->st), "memset");
+    sl.prior_valid.assign(s->nv, 0);
+    sl.ready = true;
+  }
+  return sl;
+}
+
+// Splits a view list into launches of at most max_batch views and batch_pixels pixels (cf. Session::batches,
+// crates/cuda/src/patchmatch.rs:607-625).
+std::vector<std::pair<size_t, size_t>> batches(ps_session* s, const uint32_t* views, size_t n, int level) {
+  std::vector<std::pair<size_t, size_t>> out;
+  const size_t maxb = std::min<size_t>(s->be->opts.max_batch ? s->be->opts.max_batch : 64, PS_MAX_ITEMS);
+  const uint64_t budget = s->be->opts.batch_pixels;
+  size_t start = 0;
+  uint64_t pix = 0;
+  for (size_t i = 0; i < n; ++i) {
+    uint64_t p = (uint64_t)s->W(views[i], level) * s->H(views[i], level);
+    if (i > start && ((budget && pix + p > budget) || i - start >= maxb)) {
+      out.push_back({start, i});
+      start = i;
+      pix = 0;
+    }
+    pix += p;
+  }
+  if (start < n) out.push_back({start, n});
+  return out;
+}
+
+PsRun base_params(ps_session* s, int level) {
+  PsRun P;
+  memset(&P, 0, sizeof P);
+  P.seed = s->seed;
+  P.lv = s->lv;
+  P.pairs = s->pairs;
+  P.lpairs = s->lpairs;
+  P.views = s->views;
+  P.snap = s->snap;
+  P.snap_off = s->snap_off;
+  Slot& sl = slot(s, level);
+  P.plane = sl.plane;
+  P.cost = sl.cost;
+  P.bview = sl.bview;
+  P.count = sl.count;
+  P.prior = sl.prior;
+  P.nlevels = s->nl;
+  P.level = level;
+  P.topk = s->cs.topk;
+  P.wr = s->pm.window_radius;
+  P.ws = s->pm.window_step;
+  P.tau_bad = s->cs.tau_bad;
+  P.inv2beta2 = s->cs.inv2beta2;
+  P.prev_w = s->cs.prev_w;
+  P.n1 = s->cs.n1;
+  P.n2 = s->cs.n2;
+  P.inv2s = s->cs.inv2s;
+  P.inv2c = s->cs.inv2c;
+  P.cos_tri_min = s->cs.cos_tri_min;
+  P.inv2inc = s->cs.inv2inc;
+  P.lambda = s->cs.lambda;
+  P.gmax = s->cs.gmax;
+  P.cos_filter_tri = s->cs.cos_filter_tri;
+  P.q_min = s->cs.q_min;
+  P.ncc_norm = s->cs.ncc_norm;
+  P.inv2ncc = s->cs.inv2ncc;
+  P.filter_gmax = s->cs.filter_gmax;
+  P.weak_var = s->cs.weak_var;
+  P.need_min = (int)s->fl.min_num_consistent;
+  return P;
+}
+
+// Fills the item table for views[a..b) with tiles of pw × ph pixels; aux_level >= 0 stores that level's slot offset
+// in item.aux.
+void set_items(ps_session* s, PsRun& P, const uint32_t* views, size_t a, size_t b, int level, int pw, int ph,
+               int aux_level = -1, const std::vector<long long>* aux_off = nullptr) {
+  Slot& sl = s->slots[level];
+  int tiles = 0, maxsrc = 1;
+  P.nitems = (int)(b - a);
+  for (size_t i = a; i < b; ++i) {
+    const int v = (int)views[i];
+    PsItem& it = P.items[i - a];
+    it.view = v;
+    it.w = s->W(v, level);
+    it.h = s->H(v, level);
+    it.off = sl.off[v];
+    it.aux = aux_off ? (*aux_off)[v] : (aux_level >= 0 ? s->slots[aux_level].off[v] : 0);
+    it.tile0 = tiles;
+    tiles += ((it.w + pw - 1) / pw) * ((it.h + ph - 1) / ph);
+    maxsrc = std::max(maxsrc, s->nsrc[v]);
+  }
+  P.ntiles = tiles;
+  P.maxsrc = maxsrc;
+}
+
+void launched(ps_session* s, cudaError_t e, const char* what) {
+  cuda_ok(e, what);
+  s->launches++;
+}
+
+void sync(ps_session* s) { cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize"); }
+
+// ---- state packing (host) -------------------------------------------------------------------------------------
+void check_state(ps_session* s, int v, int level, const ps_view_state& st) {
+  if ((int)st.width != s->W(v, level) || (int)st.height != s->H(v, level))
+    fail(PS_EINVAL, "state size " + std::to_string(st.width) + "x" + std::to_string(st.height) + " != level " +
+                        std::to_string(s->W(v, level)) + "x" + std::to_string(s->H(v, level)));
+}
+
+// Uploads depth/normal (as planes) and optionally prior of views[a..b) into the level slot.
+void upload_planes(ps_session* s, const uint32_t* views, size_t a, size_t b, const ps_view_state* states,
+                   int level, bool with_prior, float4* dst_base = nullptr) {
+  Slot& sl = slot(s, level);
+  size_t total = 0;
+  for (size_t i = a; i < b; ++i) total += (size_t)states[i].width * states[i].height;
+  float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * sizeof(float4) * (with_prior ? 2 : 1));
+  size_t o = 0;
+  std::vector<size_t> so;
+  for (size_t i = a; i < b; ++i) {
+    const ps_view_state& st = states[i];
+    check_state(s, (int)views[i], level, st);
+    if (!st.depth || !st.normal) fail(PS_EINVAL, "state depth/normal is NULL");
+    so.push_back(o);
+    const long long n = (long long)st.width * st.height;
+    float4* q = stage + o;
+#pragma omp parallel for schedule(static) if (n > 65536)
+    for (long long p = 0; p < n; ++p) q[p] = make_float4(st.normal[3 * p], st.normal[3 * p + 1], st.normal[3 * p + 2], st.depth[p]);
+    o += (size_t)n;
+  }
+  float4* dst = dst_base ? dst_base : sl.plane;
+  for (size_t i = a; i < b; ++i) {
+    const size_t n = (size_t)states[i].width * states[i].height;
+    cuda_ok(cudaMemcpyAsync(dst + sl.off[views[i]], stage + so[i - a], n * sizeof(float4), cudaMemcpyHostToDevice,
+                            s->st),
+            "upload planes");
+  }
+  if (with_prior) {
+    float4* pst = stage + total;
+    size_t po = 0;
+    for (size_t i = a; i < b; ++i) {
+      const ps_view_state& st = states[i];
+      const size_t n = (size_t)st.width * st.height;
+      if (st.prior) {
+        memcpy(pst + po, st.prior, n * sizeof(float4));
+        cuda_ok(cudaMemcpyAsync(sl.prior + sl.off[views[i]], pst + po, n * sizeof(float4), cudaMemcpyHostToDevice,
+                                s->st),
+                "upload prior");
+        sl.prior_valid[views[i]] = 1;
+      } else {
+        sl.prior_valid[views[i]] = 0;
+      }
+      po += n;
+    }
+  }
+  sync(s);  // the staging buffer is reused by the next call
+}
+
+// Downloads planes (from `src` or the slot planes) and/or costs into host states.
+void download_states(ps_session* s, const uint32_t* views, size_t a, size_t b, ps_view_state* states, int level,
+                     bool planes, bool costs, const float4* src = nullptr) {
+  Slot& sl = slot(s, level);
+  size_t total = 0;
+  for (size_t i = a; i < b; ++i) total += (size_t)s->W(views[i], level) * s->H(views[i], level);
+  float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * (sizeof(float4) + sizeof(float)));
+  float* cst = (float*)(stage + total);
+  size_t o = 0;
+  std::vector<size_t> so;
+  for (size_t i = a; i < b; ++i) {
+    const int v = (int)views[i];
+    check_state(s, v, level, states[i]);
+    const size_t n = (size_t)s->W(v, level) * s->H(v, level);
+    so.push_back(o);
+    if (planes)
+      cuda_ok(cudaMemcpyAsync(stage + o, (src ? src : sl.plane) + sl.off[v], n * sizeof(float4),
+                              cudaMemcpyDeviceToHost, s->st),
+              "download planes");
+    if (costs)
+      cuda_ok(cudaMemcpyAsync(cst + o, sl.cost + sl.off[v], n * sizeof(float), cudaMemcpyDeviceToHost, s->st),
+              "download cost");
+    o += n;
+  }
+  sync(s);
+  for (size_t i = a; i < b; ++i) {
+    ps_view_state& st = states[i];
+    const long long n = (long long)st.width * st.height;
+    const float4* q = stage + so[i - a];
+    if (planes) {
+      if (!st.depth || !st.normal) fail(PS_EINVAL, "state depth/normal is NULL");
+#pragma omp parallel for schedule(static) if (n > 65536)
+      for (long long p = 0; p < n; ++p) {
+        st.normal[3 * p] = q[p].x;
+        st.normal[3 * p + 1] = q[p].y;
+        st.normal[3 * p + 2] = q[p].z;
+        st.depth[p] = q[p].w;
+      }
+    }
+    if (costs) {
+      if (!st.cost) fail(PS_EINVAL, "state cost is NULL");
+      memcpy(st.cost, cst + so[i - a], n * sizeof(float));
+    }
+  }
+}
+
+// Uploads a host snapshot (re-uploaded only when its id or level changes, cf. Session::ensure_snapshot,
+// crates/cuda/src/patchmatch.rs:573-604).
+void ensure_snapshot(ps_session* s, const ps_depth_snapshot* snap) {
+  if (!snap) fail(PS_EINVAL, "a geometric run needs a snapshot");
+  if (snap->level >= (uint32_t)s->nl) fail(PS_EINVAL, "snapshot level out of range");
+  if (s->snap_valid && s->snap_id == snap->id && s->snap_level == (int)snap->level) return;
+  const int l = (int)snap->level;
+  std::vector<long long> offs(s->nv, -1);
+  size_t total = 0;
+  for (int v = 0; v < s->nv; ++v) {
+    if ((uint32_t)v < snap->num_maps && snap->maps && snap->maps[v]) {
+      offs[v] = (long long)total;
+      total += (size_t)s->W(v, l) * s->H(v, l);
+    }
+  }
+  if (total > s->snap_cap) {
+    if (s->snap) cudaFree(s->snap);
+    s->snap = nullptr;
+    s->snap_cap = 0;
+    s->snap = dalloc<float>(total);
+    s->snap_cap = total;
+  }
+  for (int v = 0; v < s->nv; ++v)
+    if (offs[v] >= 0)
+      cuda_ok(cudaMemcpyAsync(s->snap + offs[v], snap->maps[v], (size_t)s->W(v, l) * s->H(v, l) * sizeof(float),
+                              cudaMemcpyHostToDevice, s->st),
+              "upload snapshot");
+  cuda_ok(cudaMemcpyAsync(s->snap_off, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
+          "upload snapshot offsets");
+  sync(s);
+  s->snap_valid = true;
+  s->snap_id = snap->id;
+  s->snap_level = l;
+}
+
+// Eval (mode 1) + iterations × two colours on the resident slot of views[a..b).
+void run_batch(ps_session* s, const uint32_t* views, size_t a, size_t b, const ps_run_params* p, bool use_prior) {
+  PsRun P = base_params(s, (int)p->level);
+  P.geometric = p->geometric ? 1 : 0;
+  P.run_id = (int)p->run_id;
+  P.random_init = p->random_init ? 1 : 0;
+  P.use_prior = use_prior ? 1 : 0;
+  P.mode = 1;
+  set_items(s, P, views, a, b, (int)p->level, PS_EVAL_PW, PS_EVAL_PH);
+  launched(s, s->L->eval(P, s->st), "evaluate kernel");
+  PsRun H = P;
+  set_items(s, H, views, a, b, (int)p->level, PS_HALF_PW, PS_HALF_PH);
+  for (uint32_t t = 0; t < p->iterations; ++t) {
+    H.t = (int)t;
+    ps_iter_consts(&s->pm, P.geometric, (int)t, &H.tau_good, &H.eps, &H.phi);
+    for (int color = 0; color < 2; ++color) {
+      H.color = color;
+      launched(s, s->L->half(H, s->st), "half-step kernel");
+    }
+  }
+}
+
+void require_snapshot_level(ps_session* s, int level) {
+  if (!s->snap_valid) fail(PS_EINVAL, "a geometric run needs a snapshot");
+  if (s->snap_level != level) fail(PS_EINVAL, "snapshot level differs from the run level");
+}
+
+}  // namespace
+
+// ================================================================================================ C ABI
+extern "C" {
+
+int ps_abi_version(void) { return PS_ABI_VERSION; }
+void ps_pm_params_default(ps_pm_params* out) {
+  if (out) ps_default_pm(out);
+}
+void ps_filter_params_default(ps_filter_params* out) {
+  if (out) ps_default_filter(out);
+}
+void ps_options_default(ps_options* out) {
+  if (!out) return;
+  memset(out, 0, sizeof *out);
+  out->math_mode = PS_MATH_PARITY;
+  out->max_batch = 64;
+  out->batch_pixels = 0;
+}
+
+int ps_backend_create(int device, const ps_options* opts, ps_backend** out) {
+  if (!out) return PS_EINVAL;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  if (device < 0 || device >= n) return PS_ENODEV;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PS_ENODEV;
+  if (prop.major != 10) return PS_ENODEV;  // the kernels are built for sm_100a only
+  ps_backend* be = new (std::nothrow) ps_backend();
+  if (!be) return PS_ENOMEM;
+  be->device = device;
+  ps_options_default(&be->opts);
+  if (opts) be->opts = *opts;
+  if (be->opts.math_mode > PS_MATH_FAST || be->opts.checked) {
+    delete be;
+    return PS_EINVAL;
+  }
+  be->name = std::string("b200(") + prop.name + (be->opts.math_mode == PS_MATH_FAST ? ", fast)" : ", parity)");
+  *out = be;
+  return PS_OK;
+}
+
+void ps_backend_destroy(ps_backend* be) { delete be; }
+const char* ps_backend_name(const ps_backend* be) { return be ? be->name.c_str() : ""; }
+const char* ps_backend_last_error(const ps_backend* be) { return be ? be->err.c_str() : "backend is NULL"; }
+const char* ps_last_error(const ps_session* s) { return s ? s->err.c_str() : "session is NULL"; }
+uint64_t ps_launch_count(const ps_session* s) { return s ? s->launches : 0; }
+
+int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
+  if (!be || !in || !out) return PS_EINVAL;
+  *out = nullptr;
+  {
+    std::lock_guard<std::mutex> g(be->mu);
+    if (be->busy) {
+      be->err = "the backend already has an open session";
+      return PS_EBUSY;
+    }
+    be->busy = true;
+  }
+  ps_session* s = new (std::nothrow) ps_session();
+  if (!s) {
+    std::lock_guard<std::mutex> g(be->mu);
+    be->busy = false;
+    return PS_ENOMEM;
+  }
+  s->be = be;
+  int rc = guard(s, [&] {
+    const ps_pm_params& pm = in->pm;
+    if (pm.window_radius < 1 || pm.window_radius > 20 || pm.window_step < 1 || pm.window_step > 2)
+      fail(PS_EINVAL, "window radius " + std::to_string(pm.window_radius) + " (1..=20), step " +
+                          std::to_string(pm.window_step) + " (1|2)");
+    if (in->num_levels < 1) fail(PS_EINVAL, "num_levels must be >= 1");
+    if (in->num_views > 0 && !in->views) fail(PS_EINVAL, "views is NULL");
+    s->nv = (int)in->num_views;
+    s->nl = (int)in->num_levels;
+    s->pm = pm;
+    s->fl = in->filter;
+    s->seed = in->seed;
+    s->cs = ps_session_consts(&s->pm, &s->fl);
+    s->L = be->opts.math_mode == PS_MATH_FAST ? &kFast : &kParity;
+    s->w.assign(s->nv * s->nl, 0);
+    s->h.assign(s->nv * s->nl, 0);
+    s->nsrc.assign(s->nv, 0);
+    s->sources.assign(s->nv, {});
+    // validation (crates/cuda/src/patchmatch.rs:292-294, :366-371)
+    size_t total = 0;
+    std::vector<size_t> offs(s->nv * s->nl), pitches(s->nv * s->nl);
+    for (int v = 0; v < s->nv; ++v) {
+      const ps_kernel_view& kv = in->views[v];
+      if (!kv.levels) fail(PS_EINVAL, "view " + std::to_string(v) + ": levels is NULL");
+      if (kv.num_sources > PS_MAX_SOURCES)
+        fail(PS_EINVAL, "view " + std::to_string(v) + ": " + std::to_string(kv.num_sources) + " sources > 32");
+      if (kv.num_sources > 0 && (!kv.sources || !kv.pairs))
+        fail(PS_EINVAL, "view " + std::to_string(v) + ": sources/pairs is NULL");
+      for (uint32_t j = 0; j < kv.num_sources; ++j)
+        if (kv.sources[j] >= in->num_views) fail(PS_EINVAL, "view " + std::to_string(v) + ": source out of range");
+      s->nsrc[v] = (int)kv.num_sources;
+      s->sources[v].assign(kv.sources, kv.sources + kv.num_sources);
+      for (int l = 0; l < s->nl; ++l) {
+        const ps_level_image& li = kv.levels[l];
+        if (li.width < 1 || li.height < 1 || !li.pixels || li.format > PS_IMAGE_F32)
+          fail(PS_EINVAL, "view " + std::to_string(v) + " level " + std::to_string(l) + ": bad image");
+        if (li.width > (1u << 15) || li.height > (1u << 15)) fail(PS_EINVAL, "image larger than 32768 pixels");
+        if (!(li.k[0] != 0.0f) || !(li.k[1] != 0.0f)) fail(PS_EINVAL, "focal length is zero");
+        s->w[v * s->nl + l] = (int)li.width;
+        s->h[v * s->nl + l] = (int)li.height;
+        const size_t pitch = round_up(li.width + 2 * PS_BORDER, 32);
+        total = round_up(total, 32);
+        offs[v * s->nl + l] = total;
+        pitches[v * s->nl + l] = pitch;
+        total += pitch * (li.height + 2 * PS_BORDER);
+      }
+    }
+    cuda_ok(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "cudaStreamCreate");
+    // images: normalised f32 planes with a zero border
+    std::vector<float> host(std::max<size_t>(total, 1), 0.0f);
+    std::vector<PsLevel> lvh(s->nv * s->nl);
+    s->img = dalloc<float>(total);
+    s->img_bytes = total * sizeof(float);
+    for (int v = 0; v < s->nv; ++v)
+      for (int l = 0; l < s->nl; ++l) {
+        const ps_level_image& li = in->views[v].levels[l];
+        const size_t pitch = pitches[v * s->nl + l];
+        float* dst = host.data() + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
+        const size_t stride = li.stride ? li.stride : li.width;
+        for (uint32_t y = 0; y < li.height; ++y) {
+          if (li.format == PS_IMAGE_U8) {
+            const uint8_t* src = (const uint8_t*)li.pixels + y * stride;
+            for (uint32_t x = 0; x < li.width; ++x) dst[y * pitch + x] = (float)src[x] * (1.0f / 255.0f);
+          } else {
+            const float* src = (const float*)li.pixels + y * stride;
+            memcpy(dst + y * pitch, src, li.width * sizeof(float));
+          }
+        }
+        PsLevel& L = lvh[v * s->nl + l];
+        L.img = s->img + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
+        L.w = (int)li.width;
+        L.h = (int)li.height;
+        L.pitch = (int)pitch;
+        L.pad = 0;
+        L.fx = li.k[0];
+        L.fy = li.k[1];
+        L.cx = li.k[2];
+        L.cy = li.k[3];
+      }
+    cuda_ok(cudaMemcpyAsync(s->img, host.data(), total * sizeof(float), cudaMemcpyHostToDevice, s->st), "upload images");
+    s->lv = dalloc<PsLevel>(lvh.size());
+    cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
+    // pairs, views, FP64 pair tables
+    std::vector<PsPair> prh((size_t)std::max(s->nv, 1) * PS_MAXSRC);
+    std::vector<double> p64((size_t)std::max(s->nv, 1) * PS_MAXSRC * 15, 0.0);
+    std::vector<int> has64(std::max(s->nv, 1), 0);
+    std::vector<PsView> vdh(std::max(s->nv, 1));
+    for (auto& p : prh) {
+      memset(&p, 0, sizeof p);
+      p.src = -1;
+    }
+    for (int v = 0; v < s->nv; ++v) {
+      const ps_kernel_view& kv = in->views[v];
+      for (uint32_t j = 0; j < kv.num_sources; ++j) {
+        PsPair& p = prh[v * PS_MAXSRC + j];
+        memcpy(p.r, kv.pairs[j].r, sizeof p.r);
+        memcpy(p.t, kv.pairs[j].t, sizeof p.t);
+        memcpy(p.c, kv.pairs[j].center, sizeof p.c);
+        p.src = (int)kv.sources[j];
+        if (kv.pairs_f64) memcpy(&p64[((size_t)v * PS_MAXSRC + j) * 15], kv.pairs_f64 + (size_t)j * 15, 15 * sizeof(double));
+      }
+      has64[v] = kv.pairs_f64 ? 1 : 0;
+      vdh[v].key = kv.key;
+      vdh[v].dmin = kv.depth_min;
+      vdh[v].dmax = kv.depth_max;
+      vdh[v].nsrc = (int)kv.num_sources;
+      vdh[v].pad = 0;
+    }
+    s->pairs = dalloc<PsPair>(prh.size());
+    s->views = dalloc<PsView>(vdh.size());
+    s->pairs64 = dalloc<double>(p64.size());
+    s->has64 = dalloc<int>(has64.size());
+    s->lpairs = dalloc<PsLPair>((size_t)std::max(s->nv, 1) * s->nl * PS_MAXSRC);
+    cuda_ok(cudaMemcpyAsync(s->pairs, prh.data(), prh.size() * sizeof(PsPair), cudaMemcpyHostToDevice, s->st), "upload pairs");
+    cuda_ok(cudaMemcpyAsync(s->views, vdh.data(), vdh.size() * sizeof(PsView), cudaMemcpyHostToDevice, s->st), "upload views");
+    cuda_ok(cudaMemcpyAsync(s->pairs64, p64.data(), p64.size() * sizeof(double), cudaMemcpyHostToDevice, s->st), "upload pairs64");
+    cuda_ok(cudaMemcpyAsync(s->has64, has64.data(), has64.size() * sizeof(int), cudaMemcpyHostToDevice, s->st), "upload has64");
+    launched(s, ps_parity::launch_setup_lpairs(s->lv, s->pairs, s->pairs64, s->has64, s->lpairs, s->nv, s->nl, s->st),
+             "homography setup kernel");
+    s->snap_off = dalloc<long long>(std::max(s->nv, 1));
+    std::vector<long long> none(std::max(s->nv, 1), -1);
+    cuda_ok(cudaMemcpyAsync(s->snap_off, none.data(), none.size() * sizeof(long long), cudaMemcpyHostToDevice, s->st), "upload");
+    s->snap = dalloc<float>(1);
+    s->snap_cap = 1;
+    s->slots.assign(s->nl, Slot());
+    sync(s);
+  });
+  if (rc != PS_OK) {
+    be->err = s->err;
+    ps_end(s);
+    return rc;
+  }
+  *out = s;
+  return PS_OK;
+}
+
+int ps_end(ps_session* s) {
+  if (!s) return PS_EINVAL;
+  if (s->be) cudaSetDevice(s->be->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  for (Slot& sl : s->slots) {
+    cudaFree(sl.plane);
+    cudaFree(sl.aux);
+    cudaFree(sl.prior);
+    cudaFree(sl.cost);
+    cudaFree(sl.bview);
+    cudaFree(sl.count);
+  }
+  cudaFree(s->img);
+  cudaFree(s->lv);
+  cudaFree(s->pairs);
+  cudaFree(s->lpairs);
+  cudaFree(s->views);
+  cudaFree(s->pairs64);
+  cudaFree(s->has64);
+  cudaFree(s->snap);
+  cudaFree(s->snap_off);
+  if (s->pin) cudaFreeHost(s->pin);
+  if (s->st) cudaStreamDestroy(s->st);
+  cudaGetLastError();
+  if (s->be) {
+    std::lock_guard<std::mutex> g(s->be->mu);
+    s->be->busy = false;
+  }
+  delete s;
+  return PS_OK;
+}
+
+int ps_state_upload(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* states) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && !states) fail(PS_EINVAL, "states is NULL");
+    upload_planes(s, views, 0, n, states, (int)level, true);
+    Slot& sl = slot(s, (int)level);
+    // costs too
+    for (size_t i = 0; i < n; ++i)
+      if (states[i].cost)
+        cuda_ok(cudaMemcpyAsync(sl.cost + sl.off[views[i]], states[i].cost,
+                                (size_t)states[i].width * states[i].height * sizeof(float), cudaMemcpyHostToDevice, s->st),
+                "upload cost");
+    sync(s);
+  });
+}
+
+int ps_state_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* states) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && !states) fail(PS_EINVAL, "states is NULL");
+    download_states(s, views, 0, n, states, (int)level, true, true);
+  });
+}
+
+int ps_run_resident(ps_session* s, const uint32_t* views, size_t n, const ps_run_params* p) {
+  return guard(s, [&] {
+    if (!p) fail(PS_EINVAL, "params is NULL");
+    check_views(s, views, n);
+    Slot& sl = slot(s, (int)p->level);
+    if (p->geometric) require_snapshot_level(s, (int)p->level);
+    for (auto [a, b] : batches(s, views, n, (int)p->level)) {
+      bool up = p->use_prior != 0;
+      for (size_t i = a; i < b; ++i) up = up && sl.prior_valid[views[i]];
+      run_batch(s, views, a, b, p, up);
+    }
+  });
+}
+
+int ps_run(ps_session* s, const uint32_t* views, size_t n, ps_view_state* states, const ps_run_params* p,
+           const ps_depth_snapshot* snapshot) {
+  return guard(s, [&] {
+    if (!p) fail(PS_EINVAL, "params is NULL");
+    check_views(s, views, n);
+    if (n && !states) fail(PS_EINVAL, "states is NULL");
+    if (p->geometric) ensure_snapshot(s, snapshot);
+    if (p->geometric && s->snap_level != (int)p->level) fail(PS_EINVAL, "snapshot level differs from the run level");
+    const int level = (int)p->level;
+    Slot& sl = slot(s, level);
+    for (auto [a, b] : batches(s, views, n, level)) {
+      for (size_t i = a; i < b; ++i) check_state(s, (int)views[i], level, states[i]);
+      bool all_prior = true;
+      for (size_t i = a; i < b; ++i) all_prior = all_prior && states[i].prior != nullptr;
+      if (!p->random_init || (p->use_prior && all_prior)) {
+        if (!p->random_init) upload_planes(s, views, a, b, states, level, p->use_prior && all_prior);
+        else {
+          // prior only: upload it without touching the planes
+          for (size_t i = a; i < b; ++i) {
+            const size_t np = (size_t)states[i].width * states[i].height;
+            cuda_ok(cudaMemcpyAsync(sl.prior + sl.off[views[i]], states[i].prior, np * sizeof(float4),
+                                    cudaMemcpyHostToDevice, s->st),
+                    "upload prior");
+            sl.prior_valid[views[i]] = 1;
+          }
+          sync(s);
+        }
+      }
+      run_batch(s, views, a, b, p, p->use_prior && all_prior);
+      download_states(s, views, a, b, states, level, true, true);
+    }
+  });
+}
+
+int ps_evaluate(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* states,
+                uint32_t geometric, const ps_depth_snapshot* snapshot, float* const* out_cost) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && (!states || !out_cost)) fail(PS_EINVAL, "states/out_cost is NULL");
+    if (geometric) {
+      ensure_snapshot(s, snapshot);
+      if (s->snap_level != (int)level) fail(PS_EINVAL, "snapshot level differs from the evaluation level");
+    }
+    Slot& sl = slot(s, (int)level);
+    for (auto [a, b] : batches(s, views, n, (int)level)) {
+      upload_planes(s, views, a, b, states, (int)level, false);
+      PsRun P = base_params(s, (int)level);
+      P.geometric = geometric ? 1 : 0;
+      P.mode = 0;
+      set_items(s, P, views, a, b, (int)level, PS_EVAL_PW, PS_EVAL_PH);
+      launched(s, s->L->eval(P, s->st), "evaluate kernel");
+      for (size_t i = a; i < b; ++i) {
+        if (!out_cost[i]) fail(PS_EINVAL, "out_cost entry is NULL");
+        cuda_ok(cudaMemcpyAsync(out_cost[i], sl.cost + sl.off[views[i]],
+                                (size_t)s->W(views[i], level) * s->H(views[i], level) * sizeof(float),
+                                cudaMemcpyDeviceToHost, s->st),
+                "download cost");
+      }
+      sync(s);
+    }
+  });
+}
+
+int ps_filter(ps_session* s, const uint32_t* views, size_t n, const ps_view_state* states,
+              const ps_depth_snapshot* snapshot, uint8_t* const* out_counts) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && (!states || !out_counts)) fail(PS_EINVAL, "states/out_counts is NULL");
+    ensure_snapshot(s, snapshot);
+    const int level = s->snap_level;
+    Slot& sl = slot(s, level);
+    for (auto [a, b] : batches(s, views, n, level)) {
+      upload_planes(s, views, a, b, states, level, false);
+      PsRun P = base_params(s, level);
+      P.geometric = 1;
+      set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
+      launched(s, s->L->filter(P, s->st), "filter kernel");
+      for (size_t i = a; i < b; ++i) {
+        if (!out_counts[i]) fail(PS_EINVAL, "out_counts entry is NULL");
+        cuda_ok(cudaMemcpyAsync(out_counts[i], sl.count + sl.off[views[i]],
+                                (size_t)s->W(views[i], level) * s->H(views[i], level), cudaMemcpyDeviceToHost, s->st),
+                "download counts");
+      }
+      sync(s);
+    }
+  });
+}
+
+int ps_upsample(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* low,
+                float sigma_s, float sigma_c, ps_view_state* out) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (level < 1 || level >= (uint32_t)s->nl) fail(PS_EINVAL, "upsample level must be in 1..num_levels-1");
+    if (n && (!low || !out)) fail(PS_EINVAL, "low/out is NULL");
+    for (auto [a, b] : batches(s, views, n, (int)level)) {
+      upload_planes(s, views, a, b, low, (int)level - 1, false);
+      PsRun P = base_params(s, (int)level);
+      P.prior = s->slots[level - 1].plane;
+      P.up_inv2s = 1.0f / (2.0f * sigma_s * sigma_s);
+      P.up_inv2c = 1.0f / (2.0f * sigma_c * sigma_c);
+      set_items(s, P, views, a, b, (int)level, PS_SIMPLE_BX, PS_SIMPLE_BY, (int)level - 1);
+      launched(s, s->L->upsample(P, s->st), "upsample kernel");
+      download_states(s, views, a, b, out, (int)level, true, true);
+    }
+  });
+}
+
+int ps_median_filter(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* in,
+                     ps_view_state* out) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && (!in || !out)) fail(PS_EINVAL, "in/out is NULL");
+    Slot& sl = slot(s, (int)level);
+    for (auto [a, b] : batches(s, views, n, (int)level)) {
+      upload_planes(s, views, a, b, in, (int)level, false, sl.aux);
+      PsRun P = base_params(s, (int)level);
+      P.prior = sl.aux;
+      set_items(s, P, views, a, b, (int)level, PS_SIMPLE_BX, PS_SIMPLE_BY, (int)level);
+      launched(s, s->L->median(P, s->st), "median kernel");
+      download_states(s, views, a, b, out, (int)level, true, false);
+      for (size_t i = a; i < b; ++i)
+        if (out[i].cost && in[i].cost && out[i].cost != in[i].cost)
+          memcpy(out[i].cost, in[i].cost, (size_t)in[i].width * in[i].height * sizeof(float));
+    }
+  });
+}
+
+int ps_snapshot_capture(ps_session* s, uint32_t level, const uint32_t* views, size_t n, uint64_t id,
+                        uint32_t keep_others) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    Slot& sl = slot(s, (int)level);
+    if ((size_t)sl.total > s->snap_cap) {
+      if (keep_others) fail(PS_EINVAL, "keep_others needs a snapshot buffer of this level");
+      if (s->snap) cudaFree(s->snap);
+      s->snap = nullptr;
+      s->snap_cap = 0;
+      s->snap = dalloc<float>(sl.total);
+      s->snap_cap = sl.total;
+    }
+    std::vector<long long> offs(s->nv, -1);
+    if (keep_others && s->snap_valid && s->snap_level == (int)level) {
+      cuda_ok(cudaMemcpyAsync(offs.data(), s->snap_off, s->nv * sizeof(long long), cudaMemcpyDeviceToHost, s->st), "read offsets");
+      sync(s);
+      // resident captures always use the slot layout
+      for (int v = 0; v < s->nv; ++v)
+        if (offs[v] >= 0 && offs[v] != sl.off[v]) fail(PS_EINVAL, "keep_others needs a resident snapshot");
+    }
+    for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
+    for (auto [a, b] : batches(s, views, n, (int)level)) {
+      PsRun P = base_params(s, (int)level);
+      set_items(s, P, views, a, b, (int)level, PS_SIMPLE_BX, PS_SIMPLE_BY, (int)level);
+      launched(s, s->L->snapshot(P, s->snap, s->st), "snapshot kernel");
+    }
+    cuda_ok(cudaMemcpyAsync(s->snap_off, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st), "upload offsets");
+    sync(s);
+    s->snap_valid = true;
+    s->snap_level = (int)level;
+    s->snap_id = id;
+  });
+}
+
+int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* const* out_counts) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (!s->snap_valid) fail(PS_EINVAL, "filter needs a snapshot");
+    const int level = s->snap_level;
+    Slot& sl = slot(s, level);
+    for (auto [a, b] : batches(s, views, n, level)) {
+      PsRun P = base_params(s, level);
+      P.geometric = 1;
+      set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
+      launched(s, s->L->filter(P, s->st), "filter kernel");
+      if (out_counts) {
+        for (size_t i = a; i < b; ++i)
+          if (out_counts[i])
+            cuda_ok(cudaMemcpyAsync(out_counts[i], sl.count + sl.off[views[i]],
+                                    (size_t)s->W(views[i], level) * s->H(views[i], level), cudaMemcpyDeviceToHost, s->st),
+                    "download counts");
+      }
+    }
+    if (out_counts) sync(s);
+  });
+}
+
+int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_state* out) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (!s->snap_valid) fail(PS_EINVAL, "readout needs the filter's snapshot level");
+    const int level = s->snap_level;
+    Slot& sl = slot(s, level);
+    for (auto [a, b] : batches(s, views, n, level)) {
+      PsRun P = base_params(s, level);
+      set_items(s, P, views, a, b, level, PS_SIMPLE_BX, PS_SIMPLE_BY);
+      launched(s, s->L->readout(P, sl.aux, s->st), "readout kernel");
+      if (out) download_states(s, views, a, b, out, level, true, true, sl.aux);
+    }
+  });
+}
+
+int ps_synchronize(ps_session* s) {
+  return guard(s, [&] { sync(s); });
+}
+
+}  // extern "C"

@@ -1,0 +1,89 @@
+// Device-side descriptor tables of the PatchStereo engine (plain structs shared by the kernels and the host
+// runtime).  They play the role of the reference's LevelDesc / PairRec / LevelPair / ViewDesc / BatchItem / KParams
+// (crates/cuda/src/kernels/patchmatch.cu:52-109), laid out for this engine: images are normalised f32 planes with a
+// zero border instead of texture objects, and the batch table travels inside the kernel parameters.
+#pragma once
+#include <stdint.h>
+
+#define PS_MAXSRC 32
+#define PS_MAX_ITEMS 64  // views per launch (reference max_batch default, crates/cuda/src/patchmatch.rs:76)
+#define PS_BORDER 2      // zero border (pixels) around every image plane: bilinear taps never need bounds checks
+
+// Half-step CTA: 128 threads, 4 warps; a warp covers 16 active columns × 2 rows of a 32 × 8 pixel tile.
+#define PS_HALF_NT 128
+#define PS_HALF_PW 32
+#define PS_HALF_PH 8
+// Evaluate / filter CTA: 128 threads covering 32 × 4 pixels (a warp is one row).
+#define PS_EVAL_NT 128
+#define PS_EVAL_PW 32
+#define PS_EVAL_PH 4
+// Simple per-pixel kernels (upsample, median, readout, snapshot): 32 × 8 threads.
+#define PS_SIMPLE_BX 32
+#define PS_SIMPLE_BY 8
+
+// One (view, level) image plane.
+struct PsLevel {
+  const float* img;  // pixel (0,0) of a plane with PS_BORDER zero rows/columns on every side
+  int w, h, pitch;   // pitch in floats
+  int pad;
+  float fx, fy, cx, cy;
+};
+
+// Reference -> source relative geometry (PairGeometry) plus the source view index.
+struct PsPair {
+  float r[9];
+  float t[3];
+  float c[3];
+  int src;
+};
+
+// Constant part of the plane-induced homography at one level: A = K_j R K^-1, b = K_j t.
+struct PsLPair {
+  float A[9];
+  float b[3];
+};
+
+struct PsView {
+  unsigned long long key;
+  float dmin, dmax;
+  int nsrc, pad;
+};
+
+// One view of a launch.  `off` indexes the per-pixel state arrays of the view's level slot; `aux` is the offset of
+// the view's low-level planes for upsampling; `tile0` is the first CTA of this item (prefix sum over items).
+struct PsItem {
+  long long off;
+  long long aux;
+  int view, w, h, tile0;
+};
+
+// Launch parameters (kernel parameter space, so the batch table needs no device allocation).
+struct PsRun {
+  unsigned long long seed;
+  const PsLevel* lv;
+  const PsPair* pairs;
+  const PsLPair* lpairs;
+  const PsView* views;
+  const float* snap;
+  const long long* snap_off;
+  float4* plane;
+  float* cost;
+  unsigned char* bview;
+  unsigned char* count;
+  const float4* prior;  // coarse-scale candidates (run) or low-level planes (upsample) or input planes (median)
+  int nlevels, level, geometric, run_id;
+  int t, color, random_init, topk;
+  int use_prior, nitems, ntiles, maxsrc;
+  int wr, ws;  // runtime window for the generic kernels
+  float tau_good, tau_bad, inv2beta2, prev_w;
+  int n1, n2;
+  float inv2s, inv2c;
+  float cos_tri_min, inv2inc, lambda, gmax;
+  float eps, phi;
+  float cos_filter_tri, q_min, ncc_norm, inv2ncc;
+  float filter_gmax, weak_var;
+  float up_inv2s, up_inv2c;  // joint bilateral upsampling constants
+  int need_min;              // readout threshold: min_num_consistent
+  int mode;                  // evaluate: 1 = run start (init + cost + clear best view), 0 = cost only
+  PsItem items[PS_MAX_ITEMS];
+};

@@ -1,0 +1,237 @@
+"""Seeded synthetic aerial workloads for the PatchStereo engine.
+
+The workloads stand in for real imagery (no dataset is named): terrain heightfields with value-noise albedo, rendered
+by ``csrc/ps_synth.cpp`` through camera formations:
+
+* ``workload_small``  — small scenes for parity tests (the oracle finishes in seconds);
+* ``workload_c1``     — 640×480, 3-camera formation at 30 m, 40° off nadir, 10 m baseline, σ=0.01 noise, each view a
+                        reference with the other two as sources, depth 25–60 m, 11×11 window, 5 iterations;
+* ``workload_c2``     — same generator at 1920×1080, 3 cameras × 8 positions 5 m apart along the track (24 views),
+                        4 nearest sources, 13×13 window, 6 photometric iterations + a geometric-consistency round
+                        + the filter;
+* ``workload_c3``     — 64 reference views of mixed sizes from 4 terrains, 2–8 sources each;
+* ``workload_c5``     — 3840×2160, 3 × 16 positions, terrain + box structures of 3–15 m.
+
+Geometry helpers restate ``pair_geometry`` (crates/dense/src/densify.rs:183-205, FP64) and the FNV-1a view key
+(crates/dense/src/math.rs:31-39, used at crates/dense/src/densify.rs:301).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _lib
+from .patchstereo import KernelInput, KernelView, LevelImage, PairGeometry
+
+
+class _SynthScene(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("relief", C.c_double), ("wavelength", C.c_double), ("cell", C.c_double),
+                ("x0", C.c_double), ("y0", C.c_double), ("x1", C.c_double), ("y1", C.c_double),
+                ("noise_sigma", C.c_double), ("num_boxes", C.c_int), ("box_hmin", C.c_double),
+                ("box_hmax", C.c_double), ("box_smin", C.c_double), ("box_smax", C.c_double),
+                ("albedo_scale", C.c_double)]
+
+
+_synth = None
+
+
+def _synth_lib():
+    global _synth
+    if _synth is None:
+        if not _lib.SYNTH_PATH.exists():
+            raise RuntimeError(f"{_lib.SYNTH_PATH} is not built; run `python -m cumulus3d_b200.build`")
+        _synth = C.CDLL(str(_lib.SYNTH_PATH))
+        _synth.synth_render.restype = C.c_int
+        _synth.synth_render.argtypes = [C.POINTER(_SynthScene), C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_void_p]
+    return _synth
+
+
+def fnv1a(b: bytes) -> int:
+    """hash_bytes (crates/dense/src/math.rs:31-39)."""
+    h = 0xCBF29CE484222325
+    for x in b:
+        h ^= x
+        h = (h * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+@dataclass
+class Camera:
+    name: str
+    k: Tuple[float, float, float, float]  # fx, fy, cx, cy (integer-centre convention)
+    r: np.ndarray  # world -> camera rotation (3×3, float64)
+    t: np.ndarray  # world -> camera translation
+    width: int
+    height: int
+
+    @property
+    def center(self) -> np.ndarray:
+        return -self.r.T @ self.t
+
+
+def formation(width: int, height: int, positions: int, *, baseline: float = 10.0, spacing: float = 5.0,
+              altitude: float = 30.0, pitch_deg: float = 40.0, hfov_deg: float = 60.0, cams_per_row: int = 3,
+              prefix: str = "view", y0: float = 0.0) -> List[Camera]:
+    """Cameras side by side (cross-track, `baseline` apart) at `altitude`, optical axis `pitch_deg` off nadir toward
+    the track direction (+y); `positions` formation stations `spacing` apart along +y."""
+    f = (width / 2.0) / math.tan(math.radians(hfov_deg) / 2.0)
+    k = (f, f, (width - 1) / 2.0, (height - 1) / 2.0)
+    p = math.radians(pitch_deg)
+    zc = np.array([0.0, math.sin(p), -math.cos(p)])
+    xc = np.array([1.0, 0.0, 0.0])
+    yc = np.cross(zc, xc)
+    r = np.stack([xc, yc, zc])
+    cams = []
+    for s in range(positions):
+        for c in range(cams_per_row):
+            ctr = np.array([(c - (cams_per_row - 1) / 2.0) * baseline, y0 + s * spacing, altitude])
+            cams.append(Camera(f"{prefix}_p{s:02d}_c{c}.png", k, r.copy(), -r @ ctr, width, height))
+    return cams
+
+
+def _extent(cams: Sequence[Camera], zmin: float = -1.0) -> Tuple[float, float, float, float]:
+    pts = []
+    for cam in cams:
+        fx, fy, cx, cy = cam.k
+        for (u, v) in [(0, 0), (cam.width - 1, 0), (0, cam.height - 1), (cam.width - 1, cam.height - 1)]:
+            d = cam.r.T @ np.array([(u - cx) / fx, (v - cy) / fy, 1.0])
+            c = cam.center
+            t = (c[2] - zmin) / max(-d[2], 1e-6)
+            pts.append(c + t * d)
+            pts.append(c)
+    pts = np.array(pts)
+    return pts[:, 0].min() - 5, pts[:, 1].min() - 5, pts[:, 0].max() + 5, pts[:, 1].max() + 5
+
+
+def render(cams: Sequence[Camera], seed: int, *, relief: float = 8.0, wavelength: float = 24.0, cell: float = 0.1,
+           noise_sigma: float = 0.01, boxes: int = 0, box_h: Tuple[float, float] = (3.0, 15.0),
+           box_s: Tuple[float, float] = (4.0, 12.0), with_gt: bool = True):
+    """Renders every camera (all must share width/height).  Returns images (n, h, w) f32 and, with `with_gt`,
+    ground-truth depth (n, h, w) and normals (n, h, w, 3)."""
+    w, h = cams[0].width, cams[0].height
+    assert all(c.width == w and c.height == h for c in cams)
+    x0, y0, x1, y1 = _extent(cams)
+    sc = _SynthScene(seed, relief, wavelength, cell, x0, y0, x1, y1, noise_sigma, boxes, box_h[0], box_h[1],
+                     box_s[0], box_s[1], 1.0)
+    n = len(cams)
+    cam = np.zeros((n, 16), np.float64)
+    for i, c in enumerate(cams):
+        cam[i, :4] = c.k
+        cam[i, 4:13] = c.r.ravel()
+        cam[i, 13:] = c.t
+    img = np.empty((n, h, w), np.float32)
+    dep = np.empty((n, h, w), np.float32) if with_gt else None
+    nrm = np.empty((n, h, w, 3), np.float32) if with_gt else None
+    rc = _synth_lib().synth_render(C.byref(sc), cam.ctypes.data_as(C.POINTER(C.c_double)), n, w, h, img.ctypes.data,
+                                   dep.ctypes.data if with_gt else None, nrm.ctypes.data if with_gt else None)
+    if rc != 0:
+        raise RuntimeError("synth_render failed")
+    return img, dep, nrm
+
+
+def pair_geometry(ref: Camera, src: Camera) -> np.ndarray:
+    """Reference -> source relative geometry in FP64 (crates/dense/src/densify.rs:183-205): R = R_s R_rᵀ,
+    t = t_s - R t_r, centre = -Rᵀ t.  Returns 15 doubles (r[9], t[3], center[3])."""
+    rr = src.r @ ref.r.T
+    t = src.t - rr @ ref.t
+    c = -(rr.T @ t)
+    return np.concatenate([rr.ravel(), t, c])
+
+
+def nearest_sources(cams: Sequence[Camera], k: int) -> List[List[int]]:
+    """The k nearest other cameras by centre distance (ties by index)."""
+    ctr = np.array([c.center for c in cams])
+    out = []
+    for i in range(len(cams)):
+        d = np.linalg.norm(ctr - ctr[i], axis=1)
+        order = sorted((float(d[j]), j) for j in range(len(cams)) if j != i)
+        out.append([j for _, j in order[:k]])
+    return out
+
+
+def kernel_input(cams: Sequence[Camera], images: Sequence[np.ndarray], sources: Sequence[Sequence[int]],
+                 depth_range: Tuple[float, float], *, window_radius: int, window_step: int = 1, seed: int = 0x005EED0FDE75,
+                 fast_filter: bool = True, ranges: Optional[Sequence[Tuple[float, float]]] = None) -> KernelInput:
+    """Single-level KernelInput: each view's f32 image, its sources with f32 pairs (and the FP64 pairs)."""
+    views = []
+    for i, cam in enumerate(cams):
+        p64 = np.stack([pair_geometry(cam, cams[j]) for j in sources[i]]) if sources[i] else np.zeros((0, 15))
+        pairs = [PairGeometry(p[:9].astype(np.float32), p[9:12].astype(np.float32), p[12:15].astype(np.float32))
+                 for p in p64]
+        dr = ranges[i] if ranges is not None else depth_range
+        views.append(KernelView(fnv1a(cam.name.encode()), [LevelImage(images[i], cam.k)], list(sources[i]), pairs,
+                                float(dr[0]), float(dr[1]), p64))
+    pm = _lib.default_pm()
+    pm.window_radius = window_radius
+    pm.window_step = window_step
+    fl = _lib.default_filter()
+    if fast_filter:  # fast-profile filter tuning (crates/dense/src/params.rs:452-459)
+        fl.min_ncc, fl.geom_max_cost, fl.min_num_consistent, fl.median_filter = 0.2, 0.5, 3, 0
+    return KernelInput(views, 1, pm, fl, seed)
+
+
+@dataclass
+class Workload:
+    name: str
+    cams: List[Camera]
+    images: np.ndarray
+    gt_depth: Optional[np.ndarray]
+    gt_normal: Optional[np.ndarray]
+    input: KernelInput
+    photometric_iters: int
+    geometric_rounds: int
+    geometric_iters: int
+
+    @property
+    def views(self) -> List[int]:
+        return list(range(len(self.cams)))
+
+    def pixels(self) -> int:
+        return sum(c.width * c.height for c in self.cams)
+
+    def iterations(self) -> int:
+        return self.photometric_iters + self.geometric_rounds * self.geometric_iters
+
+
+def workload_small(width: int = 96, height: int = 72, views: int = 3, window_radius: int = 3, window_step: int = 1,
+                   seed: int = 7, iters: int = 2, geo_rounds: int = 0, geo_iters: int = 1, sources: int = 2,
+                   positions: int = 1) -> Workload:
+    """A small scene the oracle finishes in seconds (same generator, lower resolution)."""
+    cams = formation(width, height, positions, prefix=f"small{seed}")[: max(views, 2)]
+    img, dep, nrm = render(cams, seed)
+    src = nearest_sources(cams, min(sources, len(cams) - 1))
+    inp = kernel_input(cams, list(img), src, (25.0, 60.0), window_radius=window_radius, window_step=window_step)
+    return Workload("small", cams, img, dep, nrm, inp, iters, geo_rounds, geo_iters)
+
+
+def workload_c1(seed: int = 1) -> Workload:
+    cams = formation(640, 480, 1, prefix="c1")
+    img, dep, nrm = render(cams, seed)
+    src = [[j for j in range(3) if j != i] for i in range(3)]
+    inp = kernel_input(cams, list(img), src, (25.0, 60.0), window_radius=5, window_step=1)
+    return Workload("c1_640x480_3views_w11_5it", cams, img, dep, nrm, inp, 5, 0, 0)
+
+
+def workload_c2(seed: int = 2, with_gt: bool = True, views: Optional[int] = None) -> Workload:
+    cams = formation(1920, 1080, 8, prefix="c2")
+    if views is not None:
+        cams = cams[:views]
+    img, dep, nrm = render(cams, seed, with_gt=with_gt)
+    src = nearest_sources(cams, 4)
+    inp = kernel_input(cams, list(img), src, (25.0, 60.0), window_radius=6, window_step=1)
+    return Workload("c2_1920x1080_24views_w13_6it_geo", cams, img, dep, nrm, inp, 6, 1, 2)
+
+
+def workload_c5(seed: int = 5, views: Optional[int] = None, with_gt: bool = False) -> Workload:
+    cams = formation(3840, 2160, 16, prefix="c5")
+    if views is not None:
+        cams = cams[:views]
+    img, dep, nrm = render(cams, seed, boxes=40, with_gt=with_gt)
+    src = nearest_sources(cams, 5)
+    inp = kernel_input(cams, list(img), src, (20.0, 60.0), window_radius=6, window_step=1)
+    return Workload("c5_3840x2160_48views_boxes", cams, img, dep, nrm, inp, 2, 1, 1)

@@ -1,0 +1,245 @@
+/*
+ * patchstereo.h — C ABI of the B200 PatchStereo depth-map engine (libpatchstereo.so).
+ *
+ * The engine is a drop-in for the PatchMatch backend that cumulus3d-dense drives through cumulus3d-cuda.  Each
+ * entry point below replaces one method of the reference's Rust traits; the reference file:line is given beside it
+ * (paths inside the cumulus3d project):
+ *
+ *   trait PatchMatchBackend  crates/dense/src/kernel.rs:240-245   (impl CudaPatchMatch crates/cuda/src/patchmatch.rs:285-298)
+ *   trait PatchMatchSession  crates/dense/src/kernel.rs:192-237   (impl Session crates/cuda/src/patchmatch.rs:751-869)
+ *
+ * Conventions (same as the reference, crates/dense/src/kernel.rs:36-74): an integer pixel index is the pixel
+ * centre; ray(x,y) = ((x-cx)/fx, (y-cy)/fy, 1); depth is camera z; normals are unit vectors in reference-camera
+ * coordinates with n·ray < 0.  Level 0 is the coarsest scale.
+ *
+ * All pointers are borrowed: the caller owns them and they only need to stay valid for the duration of the call
+ * (ps_begin copies every image and geometry table to the device).  No call allocates memory the caller must free.
+ * Every entry point returns a ps_status; the message of the last failure is available from ps_last_error /
+ * ps_backend_last_error.  No C++ exception crosses this boundary.
+ *
+ * Threading: a backend serialises sessions (one open session per backend at a time, as the reference's mutex in
+ * crates/cuda/src/patchmatch.rs:96-97).  A session owns one CUDA stream and is not thread-safe.  Blocking calls
+ * return after their results are in host memory.
+ */
+#ifndef PATCHSTEREO_H
+#define PATCHSTEREO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS_MAX_SOURCES 32 /* crates/cuda/src/kernels/patchmatch.cu:40 (MAXSRC) */
+#define PS_ABI_VERSION 1
+
+/* Status codes.  Maps the reference's error kinds: Error::InvalidArgument -> PS_EINVAL,
+ * Error::Invariant("CUDA: …") -> PS_ECUDA (crates/cuda/src/patchmatch.rs:234-236),
+ * GpuError::NotAvailable -> PS_ENODEV (crates/cuda/src/device.rs:190-201). */
+typedef enum ps_status {
+  PS_OK = 0,
+  PS_EINVAL = 1,   /* bad argument, size or parameter */
+  PS_ECUDA = 2,    /* CUDA runtime / driver failure */
+  PS_ENODEV = 3,   /* no usable sm_100 device */
+  PS_ECOMPILE = 4, /* unused: kernels are compiled ahead of time for sm_100a */
+  PS_ETIMEOUT = 5, /* a bounded device-side wait gave up */
+  PS_EFAULT = 6,   /* a checked build detected an out-of-bounds index */
+  PS_ENOMEM = 7,   /* device or pinned allocation failed */
+  PS_EBUSY = 8     /* the backend already has an open session */
+} ps_status;
+
+typedef enum ps_image_format {
+  PS_IMAGE_U8 = 0,  /* 8-bit gray, value/255 (crates/dense/src/kernel.rs:87-88, patchmatch.cu:141) */
+  PS_IMAGE_F32 = 1  /* 32-bit float gray, used as is (intended range [0,1]) */
+} ps_image_format;
+
+typedef enum ps_math_mode {
+  PS_MATH_PARITY = 0, /* IEEE division/sqrt, the project's own exp/sincos, explicit fma: bitwise equal to the oracle */
+  PS_MATH_FAST = 1    /* hardware approximate reciprocal/exp/rsqrt (the reference's "speed first" numerics) */
+} ps_math_mode;
+
+/* Backend options (cf. CudaPatchMatchOptions, crates/cuda/src/patchmatch.rs:56-81). */
+typedef struct ps_options {
+  uint32_t math_mode;    /* ps_math_mode */
+  uint32_t max_batch;    /* views per launch; 0 = 64 (reference default) */
+  uint64_t batch_pixels; /* pixel budget per launch; 0 = unbounded (HBM holds every view of a job) */
+  uint32_t checked;      /* reserved (bounds-checked build); must be 0 */
+  uint32_t reserved;
+} ps_options;
+
+/* PmParams (crates/dense/src/params.rs:76-124, defaults :126-154). */
+typedef struct ps_pm_params {
+  int32_t window_radius;
+  int32_t window_step;
+  float sigma_spatial; /* <= 0: window radius (PmParams::sigma_s, params.rs:158-164) */
+  float sigma_color;
+  float tau0;
+  float tau_alpha;
+  float tau1;
+  float beta;
+  uint32_t n1;
+  uint32_t n2;
+  float prev_view_weight;
+  float min_triangulation_angle_deg;
+  float incident_angle_sigma;
+  float geom_lambda;
+  float geom_max_cost;
+  uint32_t top_k;
+  float eps0_photometric;
+  float eps0_geometric;
+  float phi0_photometric_deg;
+  float phi0_geometric_deg;
+  float eps_min;
+  float phi_min_deg;
+  float weak_texture_var;
+} ps_pm_params;
+
+/* FilterParams (crates/dense/src/params.rs:180-207). */
+typedef struct ps_filter_params {
+  float min_ncc;
+  float min_triangulation_angle_deg;
+  uint32_t min_num_consistent;
+  float geom_max_cost;
+  float ncc_sigma;
+  uint32_t median_filter;
+} ps_filter_params;
+
+/* LevelImage (crates/dense/src/kernel.rs:80-91), with a pixel format added for float inputs. */
+typedef struct ps_level_image {
+  uint32_t width;
+  uint32_t height;
+  uint32_t format;    /* ps_image_format */
+  uint32_t stride;    /* elements per row; 0 = width */
+  const void* pixels; /* row-major */
+  float k[4];         /* fx, fy, cx, cy (integer-centre convention) */
+} ps_level_image;
+
+/* PairGeometry (crates/dense/src/kernel.rs:93-103), same repr(C) layout. */
+typedef struct ps_pair_geometry {
+  float r[9];      /* reference -> source rotation, row-major */
+  float t[3];      /* reference -> source translation */
+  float center[3]; /* source centre in reference-camera coordinates */
+} ps_pair_geometry;
+
+/* KernelView (crates/dense/src/kernel.rs:105-120). */
+typedef struct ps_kernel_view {
+  uint64_t key;                   /* RNG key, FNV-1a of the image name (crates/dense/src/math.rs:31-39) */
+  const ps_level_image* levels;   /* num_levels entries, 0 = coarsest */
+  const uint32_t* sources;        /* num_sources view indices (<= PS_MAX_SOURCES) */
+  uint32_t num_sources;
+  uint32_t reserved;
+  const ps_pair_geometry* pairs;  /* num_sources entries */
+  const double* pairs_f64;        /* optional: num_sources × 15 doubles (r[9], t[3], center[3]); when given, the
+                                     homography setup A = K_j R K^-1, b = K_j t runs from these in FP64 */
+  float depth_min;
+  float depth_max;
+} ps_kernel_view;
+
+/* KernelInput (crates/dense/src/kernel.rs:122-135). */
+typedef struct ps_kernel_input {
+  const ps_kernel_view* views;
+  uint32_t num_views;
+  uint32_t num_levels;
+  ps_pm_params pm;
+  ps_filter_params filter;
+  uint64_t seed;
+} ps_kernel_input;
+
+/* ViewState (crates/dense/src/kernel.rs:137-160): caller-owned arrays, updated in place by ps_run. */
+typedef struct ps_view_state {
+  uint32_t width;
+  uint32_t height;
+  float* depth;       /* w*h */
+  float* normal;      /* 3*w*h, xyz interleaved */
+  float* cost;        /* w*h */
+  const float* prior; /* 4*w*h (nx,ny,nz,d) or NULL (= empty) */
+} ps_view_state;
+
+/* RunParams (crates/dense/src/kernel.rs:173-189). */
+typedef struct ps_run_params {
+  uint32_t level;
+  uint32_t geometric;
+  uint32_t random_init;
+  uint32_t iterations;
+  uint32_t run_id;
+  uint32_t use_prior;
+} ps_run_params;
+
+/* DepthSnapshot (crates/dense/src/kernel.rs:162-171): maps[v] is the depth map of view v at `level`
+ * (width*height floats) or NULL when absent.  Equal id implies equal content. */
+typedef struct ps_depth_snapshot {
+  uint64_t id;
+  uint32_t level;
+  uint32_t num_maps;
+  const float* const* maps;
+} ps_depth_snapshot;
+
+typedef struct ps_backend ps_backend;
+typedef struct ps_session ps_session;
+
+/* ---- defaults and diagnostics ------------------------------------------------------------------------------ */
+int ps_abi_version(void);
+void ps_pm_params_default(ps_pm_params* out);         /* PmParams::default, crates/dense/src/params.rs:126-154 */
+void ps_filter_params_default(ps_filter_params* out); /* FilterParams::default, crates/dense/src/params.rs:196-207 */
+void ps_options_default(ps_options* out);             /* CudaPatchMatchOptions::default, patchmatch.rs:71-81 */
+
+/* ---- PatchMatchBackend ------------------------------------------------------------------------------------- */
+/* CudaPatchMatch::new / try_default (crates/cuda/src/patchmatch.rs:238-246). */
+int ps_backend_create(int device, const ps_options* opts, ps_backend** out);
+void ps_backend_destroy(ps_backend* be);
+/* PatchMatchBackend::name (crates/dense/src/kernel.rs:241-242); the string lives as long as the backend. */
+const char* ps_backend_name(const ps_backend* be);
+const char* ps_backend_last_error(const ps_backend* be);
+/* PatchMatchBackend::begin (crates/dense/src/kernel.rs:243-244; crates/cuda/src/patchmatch.rs:289-297, Session::new
+ * :355-547): validates, uploads every level of every view, builds the FP64 homography tables. */
+int ps_begin(ps_backend* be, const ps_kernel_input* input, ps_session** out);
+/* Drop for Session (crates/cuda/src/patchmatch.rs:992-1009): frees the device state, releases the backend. */
+int ps_end(ps_session* s);
+const char* ps_last_error(const ps_session* s);
+
+/* ---- PatchMatchSession ------------------------------------------------------------------------------------- */
+/* PatchMatchSession::run (crates/dense/src/kernel.rs:193-194; crates/cuda/src/patchmatch.rs:752-799).  A geometric
+ * run requires a snapshot. */
+int ps_run(ps_session* s, const uint32_t* views, size_t n, ps_view_state* states, const ps_run_params* p,
+           const ps_depth_snapshot* snapshot);
+/* PatchMatchSession::evaluate (crates/dense/src/kernel.rs:195-203; patchmatch.rs:801-824): out_cost[i] receives
+ * w*h floats for views[i]. */
+int ps_evaluate(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* states,
+                uint32_t geometric, const ps_depth_snapshot* snapshot, float* const* out_cost);
+/* PatchMatchSession::filter (crates/dense/src/kernel.rs:204-207; patchmatch.rs:842-868): out_counts[i] receives
+ * w*h bytes. */
+int ps_filter(ps_session* s, const uint32_t* views, size_t n, const ps_view_state* states,
+              const ps_depth_snapshot* snapshot, uint8_t* const* out_counts);
+/* PatchMatchSession::upsample (crates/dense/src/kernel.rs:208-232; patchmatch.rs:826-836, :931-960): low[i] is at
+ * level-1, out[i] (caller-allocated depth/normal/cost at `level`) receives the upsampled planes, cost = 2. */
+int ps_upsample(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* low,
+                float sigma_s, float sigma_c, ps_view_state* out);
+/* PatchMatchSession::median_filter (crates/dense/src/kernel.rs:233-236; patchmatch.rs:838-840, :962-989). */
+int ps_median_filter(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* in,
+                     ps_view_state* out);
+
+/* ---- device-resident extension (no reference counterpart: the reference re-uploads states per call) --------
+ * The session keeps one state slot per (view, level) in HBM.  These calls let a caller run the whole schedule
+ * without host round trips; ps_run/ps_evaluate/ps_filter above are implemented on top of them. */
+int ps_state_upload(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_view_state* states);
+int ps_state_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* states);
+int ps_run_resident(ps_session* s, const uint32_t* views, size_t n, const ps_run_params* p);
+/* Copies the resident depth of `views` at `level` into the session's snapshot buffer (other views become absent
+ * unless `keep_others`). */
+int ps_snapshot_capture(ps_session* s, uint32_t level, const uint32_t* views, size_t n, uint64_t id,
+                        uint32_t keep_others);
+/* Filter on the resident states against the resident snapshot; out_counts may be NULL (counts stay on device and
+ * ps_readout_resident applies the threshold). */
+int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* const* out_counts);
+/* Readout threshold of crates/dense/src/densify.rs:441-454 on device: depth and normal are zeroed where
+ * count < max(1, min(min_num_consistent, nsrc)); writes the result into out (host) when given. */
+int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_state* out);
+int ps_synchronize(ps_session* s);
+/* Number of kernel launches this session issued so far (for launch accounting). */
+uint64_t ps_launch_count(const ps_session* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PATCHSTEREO_H */

@@ -1,0 +1,135 @@
+"""ctypes wrapper of the CPU oracle (oracle/_build/libps_oracle.so).  TEST INFRASTRUCTURE ONLY.
+
+Used by tests/, __graft_entry__.smoke() (as the checker) and bench.py's CPU-baseline / reference legs.  The engine
+(cumulus3d_b200) never imports this module.  The entry points take the same C structs as include/patchstereo.h so a
+test feeds identical inputs to the engine and to the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import pathlib
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from cumulus3d_b200 import _lib
+from cumulus3d_b200.patchstereo import (CInput, DepthSnapshot, KernelInput, RunParams, ViewState, _views, c_snapshot,
+                                        c_states)
+
+PATH = pathlib.Path(__file__).resolve().parent / "_build" / "libps_oracle.so"
+_o = None
+
+_SV = C.POINTER(_lib.ViewState)
+_KI = C.POINTER(_lib.KernelInput)
+_U32P = C.POINTER(C.c_uint32)
+_SNAP = C.POINTER(_lib.DepthSnapshot)
+
+
+def lib() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not PATH.exists():
+            raise RuntimeError(f"{PATH} is not built; run `make -C oracle`")
+        o = C.CDLL(str(PATH))
+        sig = {
+            "oracle_run": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP, C.c_int]),
+            "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
+                                          C.POINTER(C.POINTER(C.c_float)), C.c_int]),
+            "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
+            "oracle_upsample": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_float, C.c_float, _SV, C.c_int]),
+            "oracle_median": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, _SV, C.c_int]),
+            "oracle_reeval_f64": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
+                                            C.POINTER(C.POINTER(C.c_double)), C.c_int]),
+            "oracle_mix64": (C.c_uint64, [C.c_uint64]),
+            "oracle_rng_state": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                              C.c_uint64]),
+            "oracle_rng_next": (C.c_float, [C.POINTER(C.c_uint64)]),
+            "oracle_hash_bytes": (C.c_uint64, [C.c_char_p, C.c_size_t]),
+            "oracle_erf": (C.c_double, [C.c_double]),
+            "oracle_emission_norm": (C.c_double, [C.c_double]),
+            "oracle_emission": (C.c_double, [C.c_double, C.c_double]),
+            "oracle_visibility_probability": (C.c_double, [C.c_double, C.c_double]),
+            "oracle_triangulation_prior": (C.c_double, [C.c_double, C.c_double]),
+            "oracle_incident_prior": (C.c_double, [C.c_double, C.c_double]),
+            "oracle_resolution_prior": (C.c_double, [C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double]),
+            "oracle_plane_transfer": (C.c_int, [C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                                C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+            "oracle_num_levels": (C.c_size_t, [C.c_size_t, C.c_size_t, C.c_size_t]),
+            "oracle_pyramid_step": (None, [C.c_void_p, C.c_size_t, C.c_size_t, C.POINTER(C.c_double), C.c_void_p,
+                                           C.POINTER(C.c_double)]),
+            "oracle_expf": (C.c_float, [C.c_float]),
+            "oracle_sincosf": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        }
+        for n, (r, a) in sig.items():
+            f = getattr(o, n)
+            f.restype, f.argtypes = r, a
+        _o = o
+    return _o
+
+
+def _threads(threads: Optional[int]) -> int:
+    return int(threads) if threads else (os.cpu_count() or 1)
+
+
+def _chk(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with status {rc}")
+
+
+def run(inp: KernelInput, views: Sequence[int], states: List[ViewState], p: RunParams,
+        snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None) -> None:
+    """PatchMatchSession::run restated on the CPU (states updated in place)."""
+    ci, keep = CInput(inp), []
+    rp = p.c()
+    _chk(lib().oracle_run(C.byref(ci.c), _views(views), len(views), c_states(states, keep), C.byref(rp),
+                          c_snapshot(snapshot, keep), _threads(threads)), "run")
+
+
+def evaluate(inp: KernelInput, level: int, views: Sequence[int], states: List[ViewState], geometric: bool = False,
+             snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None) -> List[np.ndarray]:
+    ci, keep = CInput(inp), []
+    outs = [np.empty((s.height, s.width), np.float32) for s in states]
+    op = (C.POINTER(C.c_float) * max(len(outs), 1))(*[o.ctypes.data_as(C.POINTER(C.c_float)) for o in outs])
+    _chk(lib().oracle_evaluate(C.byref(ci.c), level, _views(views), len(views), c_states(states, keep), int(geometric),
+                               c_snapshot(snapshot, keep), op, _threads(threads)), "evaluate")
+    return outs
+
+
+def filter(inp: KernelInput, views: Sequence[int], states: List[ViewState], snapshot: DepthSnapshot,
+           threads: Optional[int] = None) -> List[np.ndarray]:
+    ci, keep = CInput(inp), []
+    outs = [np.empty((s.height, s.width), np.uint8) for s in states]
+    op = (C.POINTER(C.c_uint8) * max(len(outs), 1))(*[o.ctypes.data_as(C.POINTER(C.c_uint8)) for o in outs])
+    _chk(lib().oracle_filter(C.byref(ci.c), _views(views), len(views), c_states(states, keep),
+                             c_snapshot(snapshot, keep), op, _threads(threads)), "filter")
+    return outs
+
+
+def upsample(inp: KernelInput, level: int, views: Sequence[int], low: List[ViewState], sigma_s: float, sigma_c: float,
+             threads: Optional[int] = None) -> List[ViewState]:
+    ci, keep = CInput(inp), []
+    outs = [ViewState.new(inp.views[v].levels[level].width, inp.views[v].levels[level].height) for v in views]
+    _chk(lib().oracle_upsample(C.byref(ci.c), level, _views(views), len(views), c_states(low, keep), sigma_s, sigma_c,
+                               c_states(outs, keep), _threads(threads)), "upsample")
+    return outs
+
+
+def median(inp: KernelInput, level: int, views: Sequence[int], states: List[ViewState],
+           threads: Optional[int] = None) -> List[ViewState]:
+    ci, keep = CInput(inp), []
+    outs = [ViewState.new(s.width, s.height) for s in states]
+    _chk(lib().oracle_median(C.byref(ci.c), level, _views(views), len(views), c_states(states, keep),
+                             c_states(outs, keep), _threads(threads)), "median")
+    return outs
+
+
+def reeval_f64(inp: KernelInput, level: int, views: Sequence[int], states: List[ViewState], geometric: bool = False,
+               snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None) -> List[np.ndarray]:
+    """FP64 re-evaluation of the top-K cost of the given hypotheses."""
+    ci, keep = CInput(inp), []
+    outs = [np.empty((s.height, s.width), np.float64) for s in states]
+    op = (C.POINTER(C.c_double) * max(len(outs), 1))(*[o.ctypes.data_as(C.POINTER(C.c_double)) for o in outs])
+    _chk(lib().oracle_reeval_f64(C.byref(ci.c), level, _views(views), len(views), c_states(states, keep),
+                                 int(geometric), c_snapshot(snapshot, keep), op, _threads(threads)), "reeval")
+    return outs

@@ -1,0 +1,1131 @@
+// ps_oracle.cpp — CPU oracle for the PatchStereo hot path.  TEST INFRASTRUCTURE ONLY: it is loaded by tests/,
+// by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker; the engine never calls it.
+//
+// What it restates.  The reference ships no CPU PatchStereo ("This crate has no CPU backend",
+// crates/dense/README.md:231-232); its only implementation is the CUDA kernel file
+// crates/cuda/src/kernels/patchmatch.cu with the host constants of crates/cuda/src/patchmatch.rs.  This file
+// restates that kernel function by function (citations per function), in the reference's own structure: one pixel
+// at a time, the reference window read from the image with "0 outside", window weights recomputed per tap, and the
+// CPU twins of crates/dense/src/math.rs and crates/dense/src/upsample.rs for the known-answer tests.
+//
+// Parity pinning.  The reference has no golden PatchStereo outputs (no CPU path, no stored depth maps), so the
+// depth-map results are "parity unpinned" against the reference itself.  What IS pinned: the RNG
+// (kernel.rs:247-259), FNV-1a (math.rs:31-39), erf / emission / priors / plane transfer (the known answers of
+// math.rs:156-213), pyramid levels, intrinsics and the JBU/median plane reproduction (upsample.rs:262-308); see
+// tests/test_oracle_kat.py and tests/golden/.
+//
+// Numerics contract (shared with the engine's parity build).  Compiled with -ffp-contract=off: every operation is a
+// correctly rounded binary32 (or binary64) operation in the order written; fused multiply-adds appear only where
+// written as fma(); division and square root are IEEE; exp and sincos are the functions of ps_fmath.h.  The places
+// where the reference leaves the choice to the compiler (contraction, __expf, rsqrtf, hardware bilinear) are fixed
+// as follows, identically in the engine: bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
+// fma(ay, bot-top, top) on values already divided by 255; tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
+// the two numerators); window accumulation Ss += w·s, SSs = fma(w·s, s, SSs), IS = fma(w·s, Ik, IS); reference
+// statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); rsqrt(a) = 1/sqrt(a); ρ = cov / sqrt(var_r·var_s).
+//
+// Mode "f64" re-evaluates costs of given hypotheses with every step in binary64 (exp, sqrt, division exact to
+// double rounding) and the homography built from FP64 geometry — the FP64 CPU re-evaluation of the precision rule.
+#include <math.h>
+#include <omp.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "../cumulus3d_b200/csrc/ps_consts.h"
+#include "../cumulus3d_b200/csrc/ps_fmath.h"
+#include "../include/patchstereo.h"
+
+namespace {
+
+typedef unsigned long long u64;
+
+// ------------------------------------------------------------------------- scalar policy (binary32 / binary64)
+inline float fm(float a, float b, float c) { return fmaf(a, b, c); }
+inline double fm(double a, double b, double c) { return fma(a, b, c); }
+inline float ex(float x) { return ps_expf(x); }
+inline double ex(double x) { return exp(x); }
+inline float fl(float x) { return floorf(x); }
+inline double fl(double x) { return floor(x); }
+inline float mn(float a, float b) { return fminf(a, b); }
+inline double mn(double a, double b) { return fmin(a, b); }
+inline float mx(float a, float b) { return fmaxf(a, b); }
+inline double mx(double a, double b) { return fmax(a, b); }
+inline float sq(float a) { return sqrtf(a); }
+inline double sq(double a) { return sqrt(a); }
+
+template <class T>
+struct V3 {
+  T x, y, z;
+};
+template <class T>
+inline T dot3(V3<T> a, V3<T> b) {
+  return a.x * b.x + a.y * b.y + a.z * b.z;
+}
+template <class T>
+inline V3<T> cross3(V3<T> a, V3<T> b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+template <class T>
+inline V3<T> nrm3(V3<T> a) {
+  T l = (T)1 / sq(mx(dot3(a, a), (T)1e-30f));
+  return {a.x * l, a.y * l, a.z * l};
+}
+struct P4 {
+  float x, y, z, w;  // normal, depth
+};
+
+// ------------------------------------------------------------------------- RNG (patchmatch.cu:112-125, kernel.rs:247-259)
+inline u64 mix64(u64 z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+inline float rnd(u64& s) {
+  s += 0x9e3779b97f4a7c15ULL;
+  u64 z = mix64(s);
+  return ((float)(z >> 40) + 1.0f) * (1.0f / 16777216.0f);
+}
+inline u64 rng_state(u64 seed, u64 key, int level, int run, int t, int half, u64 pixel) {
+  u64 tag = ((u64)level << 48) ^ ((u64)run << 32) ^ ((u64)t << 16) ^ (u64)half;
+  return mix64(seed ^ mix64(key ^ mix64(tag)) ^ pixel);
+}
+
+// ------------------------------------------------------------------------- scene
+struct Img {
+  int w = 0, h = 0;
+  std::vector<float> px;  // value/255 for u8 input, as is for f32 input
+  float fx = 1, fy = 1, cx = 0, cy = 0;
+  // RefGlobal::at (patchmatch.cu:139-142): 0 outside.
+  float at(int x, int y) const {
+    if (x < 0 || y < 0 || x >= w || y >= h) return 0.0f;
+    return px[(size_t)y * w + x];
+  }
+};
+struct Pair {
+  float r[9], t[3], c[3];
+  int src;
+  double r64[9], t64[3];
+};
+struct LPair {
+  float A[9], b[3];
+  double A64[9], b64[3];
+};
+struct View {
+  u64 key;
+  float dmin, dmax;
+  std::vector<Img> lv;
+  std::vector<Pair> pairs;
+  std::vector<LPair> lp;  // [level][src]
+};
+struct Scene {
+  int nl = 0;
+  std::vector<View> v;
+  ps_pm_params pm;
+  ps_filter_params fp;
+  u64 seed;
+  PsConsts cs;
+  int wr, ws, wn;
+  const Img& L(int view, int level) const { return v[view].lv[level]; }
+};
+
+// A = K_j R K^-1, b = K_j t in binary64 (crates/cuda/src/patchmatch.rs:132-151), then rounded to binary32.
+void level_pair(const float* kr, const float* kj, const double* r, const double* t, LPair& o) {
+  const double fx = kr[0], fy = kr[1], cx = kr[2], cy = kr[3];
+  const double kinv[3][3] = {{1.0 / fx, 0.0, -cx / fx}, {0.0, 1.0 / fy, -cy / fy}, {0.0, 0.0, 1.0}};
+  const double km[3][3] = {{(double)kj[0], 0.0, (double)kj[2]}, {0.0, (double)kj[1], (double)kj[3]}, {0.0, 0.0, 1.0}};
+  double krm[3][3];
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) krm[i][k] = km[i][0] * r[0 * 3 + k] + km[i][1] * r[1 * 3 + k] + km[i][2] * r[2 * 3 + k];
+  for (int i = 0; i < 3; ++i)
+    for (int k = 0; k < 3; ++k) {
+      o.A64[i * 3 + k] = krm[i][0] * kinv[0][k] + krm[i][1] * kinv[1][k] + krm[i][2] * kinv[2][k];
+      o.A[i * 3 + k] = (float)o.A64[i * 3 + k];
+    }
+  for (int i = 0; i < 3; ++i) {
+    o.b64[i] = km[i][0] * t[0] + km[i][1] * t[1] + km[i][2] * t[2];
+    o.b[i] = (float)o.b64[i];
+  }
+}
+
+bool load_scene(const ps_kernel_input* in, Scene& sc) {
+  if (!in || in->num_levels < 1) return false;
+  sc.nl = (int)in->num_levels;
+  sc.pm = in->pm;
+  sc.fp = in->filter;
+  sc.seed = in->seed;
+  sc.cs = ps_session_consts(&sc.pm, &sc.fp);
+  sc.wr = sc.pm.window_radius;
+  sc.ws = sc.pm.window_step;
+  sc.wn = (2 * sc.wr) / sc.ws + 1;
+  sc.v.resize(in->num_views);
+  for (uint32_t i = 0; i < in->num_views; ++i) {
+    const ps_kernel_view& kv = in->views[i];
+    View& v = sc.v[i];
+    v.key = kv.key;
+    v.dmin = kv.depth_min;
+    v.dmax = kv.depth_max;
+    v.lv.resize(sc.nl);
+    for (int l = 0; l < sc.nl; ++l) {
+      const ps_level_image& li = kv.levels[l];
+      Img& im = v.lv[l];
+      im.w = (int)li.width;
+      im.h = (int)li.height;
+      im.fx = li.k[0];
+      im.fy = li.k[1];
+      im.cx = li.k[2];
+      im.cy = li.k[3];
+      im.px.resize((size_t)im.w * im.h);
+      const size_t stride = li.stride ? li.stride : li.width;
+      for (int y = 0; y < im.h; ++y)
+        for (int x = 0; x < im.w; ++x)
+          im.px[(size_t)y * im.w + x] = li.format == PS_IMAGE_U8
+                                            ? (float)((const uint8_t*)li.pixels)[y * stride + x] * (1.0f / 255.0f)
+                                            : ((const float*)li.pixels)[y * stride + x];
+    }
+    v.pairs.resize(kv.num_sources);
+    for (uint32_t j = 0; j < kv.num_sources; ++j) {
+      Pair& p = v.pairs[j];
+      memcpy(p.r, kv.pairs[j].r, sizeof p.r);
+      memcpy(p.t, kv.pairs[j].t, sizeof p.t);
+      memcpy(p.c, kv.pairs[j].center, sizeof p.c);
+      p.src = (int)kv.sources[j];
+      for (int k = 0; k < 9; ++k) p.r64[k] = kv.pairs_f64 ? kv.pairs_f64[j * 15 + k] : (double)p.r[k];
+      for (int k = 0; k < 3; ++k) p.t64[k] = kv.pairs_f64 ? kv.pairs_f64[j * 15 + 9 + k] : (double)p.t[k];
+    }
+  }
+  for (uint32_t i = 0; i < in->num_views; ++i) {
+    View& v = sc.v[i];
+    v.lp.resize((size_t)sc.nl * v.pairs.size());
+    for (int l = 0; l < sc.nl; ++l)
+      for (size_t j = 0; j < v.pairs.size(); ++j) {
+        const ps_level_image& a = in->views[i].levels[l];
+        const ps_level_image& b = in->views[v.pairs[j].src].levels[l];
+        level_pair(a.k, b.k, v.pairs[j].r64, v.pairs[j].t64, v.lp[l * v.pairs.size() + j]);
+      }
+  }
+  return true;
+}
+
+// ------------------------------------------------------------------------- per-pixel restatement
+struct Run {
+  const Scene* sc;
+  int view, level;
+  int geometric, run_id, t, color, topk, use_prior;
+  float tau_good, eps, phi;
+  const std::vector<std::vector<float>>* snap;  // per view (empty = absent)
+};
+
+template <class T>
+struct RS {
+  T ic, W, mu, var;
+};
+
+// Source sample, integer-centre convention, 0 outside (patchmatch.cu:169-192, software path).
+template <class T>
+T sample(const Img& S, T u, T v) {
+  T xf = fl(u), yf = fl(v);
+  T ax = u - xf, ay = v - yf;
+  // integer footprint; the clamp only guards the conversion and keeps out-of-image footprints out of the image
+  const int x0 = (int)mn(mx(xf, (T)-2), (T)S.w), y0 = (int)mn(mx(yf, (T)-2), (T)S.h);
+  T p00 = (T)S.at(x0, y0), p10 = (T)S.at(x0 + 1, y0), p01 = (T)S.at(x0, y0 + 1), p11 = (T)S.at(x0 + 1, y0 + 1);
+  T top = fm(ax, p10 - p00, p00);
+  T bot = fm(ax, p11 - p01, p01);
+  return fm(ay, bot - top, top);
+}
+
+// ref_stats (patchmatch.cu:199-223).
+template <class T>
+RS<T> ref_stats(const Scene& sc, const Img& R, int x, int y) {
+  RS<T> s;
+  s.ic = (T)R.at(x, y);
+  T W = 0, S = 0, SS = 0;
+  const T inv2s = (T)sc.cs.inv2s, inv2c = (T)sc.cs.inv2c;
+  for (int a = 0; a < sc.wn; ++a) {
+    int dy = -sc.wr + a * sc.ws;
+    for (int b = 0; b < sc.wn; ++b) {
+      int dx = -sc.wr + b * sc.ws;
+      T ik = (T)R.at(x + dx, y + dy);
+      T d = s.ic - ik;
+      T w = ex(-(T)(dx * dx + dy * dy) * inv2s - d * d * inv2c);
+      T wi = w * ik;
+      W = W + w;
+      S = S + wi;
+      SS = fm(wi, ik, SS);
+    }
+  }
+  s.W = W;
+  s.mu = S / W;
+  s.var = SS / W - s.mu * s.mu;
+  return s;
+}
+
+// Homography (patchmatch.cu:225-242).
+template <class T>
+bool homography(const Img& R, const LPair& L, T x, T y, const P4& h, T* H) {
+  T ifx = (T)1 / (T)R.fx, ify = (T)1 / (T)R.fy;
+  V3<T> n = {(T)h.x, (T)h.y, (T)h.z};
+  V3<T> ray = {(x - (T)R.cx) * ifx, (y - (T)R.cy) * ify, (T)1};
+  T delta = (T)h.w * dot3(n, ray);
+  if (!(delta < (T)-1e-12f)) return false;
+  T id = (T)1 / delta;
+  T u0 = n.x * ifx, u1 = n.y * ify;
+  T u2 = n.z - u0 * (T)R.cx - u1 * (T)R.cy;
+  const bool d64 = sizeof(T) == 8;
+  for (int r = 0; r < 3; ++r) {
+    T br = (d64 ? (T)L.b64[r] : (T)L.b[r]) * id;
+    H[r * 3 + 0] = (d64 ? (T)L.A64[r * 3 + 0] : (T)L.A[r * 3 + 0]) + br * u0;
+    H[r * 3 + 1] = (d64 ? (T)L.A64[r * 3 + 1] : (T)L.A[r * 3 + 1]) + br * u1;
+    H[r * 3 + 2] = (d64 ? (T)L.A64[r * 3 + 2] : (T)L.A[r * 3 + 2]) + br * u2;
+  }
+  return true;
+}
+
+// NCC cost (patchmatch.cu:245-290), weights recomputed per tap as the reference's global-memory path does.
+template <class T>
+T ncc_cost(const Scene& sc, const Img& R, const RS<T>& rs, const Img& S, const T* H, int x, int y) {
+  T fx = (T)x, fy = (T)y;
+  T z = fm(H[6], fx, fm(H[7], fy, H[8]));
+  if (!(z > (T)1e-8f)) return 2;
+  T iz = (T)1 / z;
+  T u = fm(H[0], fx, fm(H[1], fy, H[2])) * iz, v = fm(H[3], fx, fm(H[4], fy, H[5])) * iz;
+  if (!(u >= 0 && v >= 0 && u <= (T)S.w - (T)1 && v <= (T)S.h - (T)1)) return 2;
+  if (rs.var < (T)1e-5f) return 2;
+  const T inv2s = (T)sc.cs.inv2s, inv2c = (T)sc.cs.inv2c;
+  T Ss = 0, SSs = 0, IS = 0;
+  for (int a = 0; a < sc.wn; ++a) {
+    int dy = -sc.wr + a * sc.ws;
+    T sy = fy + (T)dy;
+    for (int b = 0; b < sc.wn; ++b) {
+      int dx = -sc.wr + b * sc.ws;
+      T sx = fx + (T)dx;
+      T ik = (T)R.at(x + dx, y + dy);
+      T d = rs.ic - ik;
+      T w = ex(-(T)(dx * dx + dy * dy) * inv2s - d * d * inv2c);
+      T zz = fm(H[6], sx, fm(H[7], sy, H[8]));
+      T sv = 0;
+      if (zz > (T)1e-8f) {
+        T izz = (T)1 / zz;
+        sv = sample<T>(S, fm(H[0], sx, fm(H[1], sy, H[2])) * izz, fm(H[3], sx, fm(H[4], sy, H[5])) * izz);
+      }
+      T wsv = w * sv;
+      Ss = Ss + wsv;
+      SSs = fm(wsv, sv, SSs);
+      IS = fm(wsv, ik, IS);
+    }
+  }
+  T iW = (T)1 / rs.W;
+  T mus = Ss * iW;
+  T vars = SSs * iW - mus * mus;
+  if (vars < (T)1e-5f) return 2;
+  T cov = IS * iW - rs.mu * mus;
+  T c = (T)1 - cov / sq(rs.var * vars);
+  return mn(mx(c, (T)0), (T)2);
+}
+
+// Forward/backward reprojection error (patchmatch.cu:292-314).
+const float INF_ERR = 1e30f;
+template <class T>
+T geo_error(const Run& r, const Img& R, const Img& S, const Pair& pr, int x, int y, T d) {
+  const std::vector<float>& sm = (*r.snap)[pr.src];
+  if (sm.empty()) return (T)INF_ERR;
+  const bool d64 = sizeof(T) == 8;
+  auto rr = [&](int k) { return d64 ? (T)pr.r64[k] : (T)pr.r[k]; };
+  auto tt = [&](int k) { return d64 ? (T)pr.t64[k] : (T)pr.t[k]; };
+  V3<T> X = {((T)x - (T)R.cx) / (T)R.fx * d, ((T)y - (T)R.cy) / (T)R.fy * d, d};
+  T xj = rr(0) * X.x + rr(1) * X.y + rr(2) * X.z + tt(0);
+  T yj = rr(3) * X.x + rr(4) * X.y + rr(5) * X.z + tt(1);
+  T zj = rr(6) * X.x + rr(7) * X.y + rr(8) * X.z + tt(2);
+  if (!(zj > (T)1e-8f)) return (T)INF_ERR;
+  T u = (T)S.fx * xj / zj + (T)S.cx, v = (T)S.fy * yj / zj + (T)S.cy;
+  T uf = fl(u + (T)0.5f), vf = fl(v + (T)0.5f);
+  if (!(uf >= 0 && vf >= 0 && uf < (T)S.w && vf < (T)S.h)) return (T)INF_ERR;
+  T dj = (T)sm[(size_t)vf * S.w + (size_t)uf];
+  if (!(dj > 0)) return (T)INF_ERR;
+  V3<T> Yj = {(u - (T)S.cx) / (T)S.fx * dj, (v - (T)S.cy) / (T)S.fy * dj, dj};
+  V3<T> q = {Yj.x - tt(0), Yj.y - tt(1), Yj.z - tt(2)};
+  T Yx = rr(0) * q.x + rr(3) * q.y + rr(6) * q.z;
+  T Yy = rr(1) * q.x + rr(4) * q.y + rr(7) * q.z;
+  T Yz = rr(2) * q.x + rr(5) * q.y + rr(8) * q.z;
+  if (!(Yz > (T)1e-8f)) return (T)INF_ERR;
+  T cx = (T)R.fx * Yx / Yz + (T)R.cx - (T)x, cy = (T)R.fy * Yy / Yz + (T)R.cy - (T)y;
+  return sq(cx * cx + cy * cy);
+}
+
+template <class T>
+T pair_cost(const Run& r, const Img& R, const RS<T>& rs, int j, int x, int y, const P4& h, T* geo) {
+  const Scene& sc = *r.sc;
+  const View& vw = sc.v[r.view];
+  const Pair& pr = vw.pairs[j];
+  const Img& S = sc.L(pr.src, r.level);
+  const LPair& lp = vw.lp[(size_t)r.level * vw.pairs.size() + j];
+  T H[9];
+  T c = 2;
+  if (homography<T>(R, lp, (T)x, (T)y, h, H)) c = ncc_cost<T>(sc, R, rs, S, H, x, y);
+  if (r.geometric) *geo = mn(geo_error<T>(r, R, S, pr, x, y, (T)h.w), (T)sc.cs.gmax);
+  return c;
+}
+
+// topk_cost (patchmatch.cu:327-345).
+template <class T>
+T topk_cost(const Run& r, const Img& R, const RS<T>& rs, int x, int y, const P4& h) {
+  const View& vw = r.sc->v[r.view];
+  T b0 = (T)1e30f, b1 = (T)1e30f, b2 = (T)1e30f;
+  const int nsrc = (int)vw.pairs.size();
+  for (int j = 0; j < nsrc; ++j) {
+    T g = 0;
+    T c = pair_cost<T>(r, R, rs, j, x, y, h, &g);
+    if (r.geometric) c += (T)r.sc->cs.lambda * g;
+    if (c < b0) {
+      b2 = b1;
+      b1 = b0;
+      b0 = c;
+    } else if (c < b1) {
+      b2 = b1;
+      b1 = c;
+    } else if (c < b2) {
+      b2 = c;
+    }
+  }
+  int k = std::min(r.topk, nsrc);
+  T s = b0;
+  if (k >= 2) s += b1;
+  if (k >= 3) s += b2;
+  return k > 0 ? s / (T)k : (T)2;
+}
+
+V3<float> pixel_ray(const Img& R, int x, int y) { return {((float)x - R.cx) / R.fx, ((float)y - R.cy) / R.fy, 1.0f}; }
+
+// random_normal / random_depth / perturb_normal (patchmatch.cu:348-384).
+V3<float> random_normal(u64& st, V3<float> ray) {
+  V3<float> n = {0.f, 0.f, -1.f};
+  for (int k = 0; k < 64; ++k) {
+    float v1 = 2.f * rnd(st) - 1.f, v2 = 2.f * rnd(st) - 1.f;
+    float s = v1 * v1 + v2 * v2;
+    if (s < 1.f && s > 0.f) {
+      float r = 2.f * sqrtf(1.f - s);
+      n = {v1 * r, v2 * r, 1.f - 2.f * s};
+      break;
+    }
+  }
+  if (dot3(n, ray) > 0.f) n = {-n.x, -n.y, -n.z};
+  return n;
+}
+float random_depth(u64& st, float dmin, float dmax) {
+  float a = 1.f / dmax, b = 1.f / dmin;
+  return 1.f / (a + rnd(st) * (b - a));
+}
+V3<float> perturb_normal(u64& st, V3<float> n, V3<float> ray, float phi) {
+  V3<float> a = random_normal(st, {0.f, 0.f, 0.f});
+  V3<float> ax = cross3(a, n);
+  float l2 = dot3(ax, ax);
+  float ang = rnd(st) * phi;
+  if (l2 < 1e-12f) return n;
+  ax = nrm3(ax);
+  V3<float> bn = cross3(ax, n);
+  for (int k = 0; k < 4; ++k) {
+    float sa, ca;
+    ps_sincosf(ang, &sa, &ca);
+    V3<float> m = {n.x * ca + bn.x * sa, n.y * ca + bn.y * sa, n.z * ca + bn.z * sa};
+    if (dot3(m, ray) < 0.f) return nrm3(m);
+    ang *= 0.5f;
+  }
+  return n;
+}
+
+// view_prior (patchmatch.cu:388-422).
+float view_prior(const Scene& sc, const Img& R, const Pair& pr, const float* H, bool hok, int x, int y, const P4& h) {
+  if (!hok) return 0.f;
+  V3<float> ray = pixel_ray(R, x, y);
+  V3<float> X = {ray.x * h.w, ray.y * h.w, h.w};
+  V3<float> S = {pr.c[0] - X.x, pr.c[1] - X.y, pr.c[2] - X.z};
+  float ls = sqrtf(dot3(S, S)), lx = sqrtf(dot3(X, X));
+  if (ls <= 0.f || lx <= 0.f) return 0.f;
+  float cost = -dot3(S, X) / (ls * lx);
+  float tri = 1.f;
+  if (cost > sc.cs.cos_tri_min) {
+    float s = 1.f - (1.f - cost) / (1.f - sc.cs.cos_tri_min);
+    tri = fminf(fmaxf(1.f - s * s, 0.f), 1.f);
+  }
+  float cphi = dot3(S, V3<float>{h.x, h.y, h.z}) / ls;
+  float xi = 1.f - fmaxf(0.f, cphi);
+  float inc = ps_expf(-xi * xi * sc.cs.inv2inc);
+  float r = (float)sc.wr;
+  float cxs[4] = {x - r, x - r, x + r, x + r};
+  float cys[4] = {y - r, y + r, y + r, y - r};
+  float px[4], py[4];
+  for (int k = 0; k < 4; ++k) {
+    float z = H[6] * cxs[k] + H[7] * cys[k] + H[8];
+    if (!(z > 1e-8f)) return 0.f;
+    px[k] = (H[0] * cxs[k] + H[1] * cys[k] + H[2]) / z;
+    py[k] = (H[3] * cxs[k] + H[4] * cys[k] + H[5]) / z;
+  }
+  float area = 0.f;
+  for (int k = 0; k < 4; ++k) area += px[k] * py[(k + 1) & 3] - px[(k + 1) & 3] * py[k];
+  area = 0.5f * fabsf(area);
+  float aref = (2.f * r + 1.f) * (2.f * r + 1.f);
+  if (!(area > 0.f)) return 0.f;
+  float res = fminf(area / aref, aref / area);
+  return tri * inc * res;
+}
+
+// Region offsets for the "up" direction (patchmatch.cu:425) and the 90° rotation (:427-436).
+const int V_OFF[7][2] = {{0, -1}, {-1, -2}, {1, -2}, {-2, -3}, {2, -3}, {-3, -4}, {3, -4}};
+void rot_dir(int dir, int dx, int dy, int& ox, int& oy) {
+  ox = dx;
+  oy = dy;
+  for (int k = 0; k < dir; ++k) {
+    int t = ox;
+    ox = -oy;
+    oy = t;
+  }
+}
+
+struct State {
+  int w, h;
+  std::vector<P4> plane;
+  std::vector<float> cost;
+  std::vector<uint8_t> bview;
+  std::vector<P4> prior;
+};
+
+// One red-black half step of one pixel (patchmatch.cu:439-657).  Reads opposite-colour neighbours only.
+void half_pixel(const Run& r, State& st, int x, int y) {
+  const Scene& sc = *r.sc;
+  const View& vd = sc.v[r.view];
+  const Img& R = sc.L(r.view, r.level);
+  const int w = st.w, h = st.h;
+  const int pix = y * w + x;
+  const V3<float> ray = pixel_ray(R, x, y);
+  P4 hyp[9];
+  hyp[0] = st.plane[pix];
+  for (int rg = 0; rg < 8; ++rg) {
+    int dir = rg & 3;
+    bool strip = rg >= 4;
+    int cnt = strip ? 11 : 7;
+    float best = 1e30f;
+    int bq = -1, bx = 0, by = 0;
+    for (int k = 0; k < cnt; ++k) {
+      int dx, dy;
+      if (strip) rot_dir(dir, 0, -(3 + 2 * k), dx, dy);
+      else rot_dir(dir, V_OFF[k][0], V_OFF[k][1], dx, dy);
+      int qx = x + dx, qy = y + dy;
+      if (qx < 0 || qy < 0 || qx >= w || qy >= h) continue;
+      float c = st.cost[qy * w + qx];
+      if (c < best) {
+        best = c;
+        bq = qy * w + qx;
+        bx = qx;
+        by = qy;
+      }
+    }
+    hyp[1 + rg] = hyp[0];
+    if (bq >= 0) {
+      P4 q = st.plane[bq];
+      V3<float> n = {q.x, q.y, q.z};
+      V3<float> rq = pixel_ray(R, bx, by);
+      float den = dot3(n, ray);
+      if (den < -1e-6f && q.w > 0.f) {
+        float d = q.w * dot3(n, rq) / den;
+        if (d > 0.f && std::isfinite(d)) hyp[1 + rg] = {n.x, n.y, n.z, d};
+      }
+    }
+  }
+  const RS<float> rs = ref_stats<float>(sc, R, x, y);
+  const int vprev = st.bview[pix];
+  const int nsrc = (int)vd.pairs.size();
+  float num[9] = {0}, numf[9] = {0};
+  float den = 0.f, wbest = 0.f, denf = 0.f;
+  int vbest = 255;
+  float wv[PS_MAX_SOURCES];
+  for (int j = 0; j < nsrc; ++j) {
+    const Pair& pr = vd.pairs[j];
+    const Img& S = sc.L(pr.src, r.level);
+    const LPair& lp = vd.lp[(size_t)r.level * nsrc + j];
+    float m[9], gg[9];
+    float prior;
+    {
+      float H[9];
+      bool ok = homography<float>(R, lp, (float)x, (float)y, hyp[0], H);
+      prior = view_prior(sc, R, pr, H, ok, x, y, hyp[0]);
+      wv[j] = 0.f;
+      if (!(prior > 0.f)) continue;
+      m[0] = ok ? ncc_cost<float>(sc, R, rs, S, H, x, y) : 2.f;
+      gg[0] = r.geometric ? fminf(geo_error<float>(r, R, S, pr, x, y, hyp[0].w), sc.cs.gmax) : 0.f;
+    }
+    for (int i = 1; i < 9; ++i) {
+      float H[9];
+      bool ok = homography<float>(R, lp, (float)x, (float)y, hyp[i], H);
+      m[i] = ok ? ncc_cost<float>(sc, R, rs, S, H, x, y) : 2.f;
+      gg[i] = r.geometric ? fminf(geo_error<float>(r, R, S, pr, x, y, hyp[i].w), sc.cs.gmax) : 0.f;
+    }
+    int good = 0, bad = 0;
+    float conf = 0.f;
+    for (int i = 1; i < 9; ++i) {
+      if (m[i] < r.tau_good) {
+        good++;
+        conf += ps_expf(-m[i] * m[i] * sc.cs.inv2beta2);
+      }
+      if (m[i] > sc.cs.tau_bad) bad++;
+    }
+    bool adopt = good > sc.cs.n1 && bad < sc.cs.n2;
+    bool isprev = j == vprev;
+    float wp = adopt ? (isprev ? 2.f : 1.f) * conf / (float)good : (isprev ? sc.cs.prev_w : 0.f);
+    float w2 = wp * prior;
+    wv[j] = w2 > 0.f ? w2 : -prior;
+    for (int i = 0; i < 9; ++i) numf[i] += prior * (m[i] + sc.cs.lambda * gg[i]);
+    denf += prior;
+    if (w2 > 0.f) {
+      for (int i = 0; i < 9; ++i) num[i] += w2 * (m[i] + sc.cs.lambda * gg[i]);
+      den += w2;
+      if (w2 > wbest) {
+        wbest = w2;
+        vbest = j;
+      }
+    }
+  }
+  float agg[9];
+  int bi9 = 0;
+  if (den > 0.f) {
+    for (int i = 0; i < 9; ++i) agg[i] = num[i] / den;
+    for (int i = 1; i < 9; ++i)
+      if (agg[i] < agg[bi9]) bi9 = i;
+  } else if (denf > 0.f) {
+    for (int i = 0; i < 9; ++i) agg[i] = numf[i] / denf;
+    for (int i = 1; i < 9; ++i)
+      if (agg[i] < agg[bi9]) bi9 = i;
+    for (int j = 0; j < nsrc; ++j) wv[j] = -wv[j];
+    den = denf;
+  } else {
+    for (int i = 0; i < 9; ++i) agg[i] = 2.f;
+  }
+  P4 best = hyp[bi9];
+  float bcost = agg[bi9];
+  u64 s = rng_state(sc.seed, vd.key, r.level, r.run_id, r.t, r.color, (u64)pix);
+  float d_r = random_depth(s, vd.dmin, vd.dmax);
+  V3<float> n_r = random_normal(s, ray);
+  float u = 2.f * rnd(s) - 1.f;
+  float inv = best.w > 0.f ? (1.f / best.w) * (1.f + u * r.eps) : -1.f;
+  float d_p = inv > 0.f ? 1.f / inv : d_r;
+  if (!(best.w > 0.f)) best.w = d_r;
+  V3<float> n0 = {best.x, best.y, best.z};
+  V3<float> n_p = perturb_normal(s, n0, ray, r.phi);
+  P4 cand[6] = {{n0.x, n0.y, n0.z, d_r},        {n_r.x, n_r.y, n_r.z, best.w}, {n_r.x, n_r.y, n_r.z, d_r},
+                {n0.x, n0.y, n0.z, d_p},        {n_p.x, n_p.y, n_p.z, best.w}, {n_p.x, n_p.y, n_p.z, d_p}};
+  auto weighted = [&](const P4& c) {
+    if (!(den > 0.f)) return 2.f;
+    float nm = 0.f;
+    for (int j = 0; j < nsrc; ++j) {
+      if (!(wv[j] > 0.f)) continue;
+      float g = 0.f;
+      float mm = pair_cost<float>(r, R, rs, j, x, y, c, &g);
+      nm += wv[j] * (mm + sc.cs.lambda * g);
+    }
+    return nm / den;
+  };
+  for (int c = 0; c < 6; ++c) {
+    float cc = weighted(cand[c]);
+    if (cc < bcost) {
+      bcost = cc;
+      best = cand[c];
+    }
+  }
+  if (r.use_prior && rs.var < sc.cs.weak_var) {
+    P4 q = st.prior[pix];
+    if (q.w > 0.f && dot3(V3<float>{q.x, q.y, q.z}, ray) < 0.f) {
+      float cc = weighted(q);
+      if (cc < bcost) {
+        bcost = cc;
+        best = q;
+      }
+    }
+  }
+  st.plane[pix] = best;
+  st.cost[pix] = bcost;
+  st.bview[pix] = (uint8_t)vbest;
+}
+
+// pm_eval (patchmatch.cu:661-692).
+void eval_pixel(const Run& r, State& st, int x, int y, int mode, int random_init) {
+  const Scene& sc = *r.sc;
+  const View& vd = sc.v[r.view];
+  const Img& R = sc.L(r.view, r.level);
+  const int pix = y * st.w + x;
+  V3<float> ray = pixel_ray(R, x, y);
+  P4 h = st.plane[pix];
+  if (mode == 1 && random_init) {
+    u64 s = rng_state(sc.seed, vd.key, r.level, r.run_id, 0xFFFF, 0, (u64)pix);
+    float d = random_depth(s, vd.dmin, vd.dmax);
+    V3<float> n = random_normal(s, ray);
+    h = {n.x, n.y, n.z, d};
+    st.plane[pix] = h;
+  }
+  float c = 2.f;
+  if (h.w > 0.f) {
+    RS<float> rs = ref_stats<float>(sc, R, x, y);
+    c = topk_cost<float>(r, R, rs, x, y, h);
+  }
+  st.cost[pix] = c;
+  if (mode == 1) st.bview[pix] = 255;
+}
+
+// pm_filter (patchmatch.cu:695-737).
+int filter_pixel(const Run& r, const State& st, int x, int y) {
+  const Scene& sc = *r.sc;
+  const View& vd = sc.v[r.view];
+  const Img& R = sc.L(r.view, r.level);
+  const int pix = y * st.w + x;
+  P4 h = st.plane[pix];
+  int count = 0;
+  if (h.w > 0.f) {
+    RS<float> rs = ref_stats<float>(sc, R, x, y);
+    V3<float> ray = pixel_ray(R, x, y);
+    V3<float> X = {ray.x * h.w, ray.y * h.w, h.w};
+    float lx = sqrtf(dot3(X, X));
+    const int nsrc = (int)vd.pairs.size();
+    for (int j = 0; j < nsrc; ++j) {
+      const Pair& pr = vd.pairs[j];
+      const Img& S = sc.L(pr.src, r.level);
+      V3<float> Sv = {pr.c[0] - X.x, pr.c[1] - X.y, pr.c[2] - X.z};
+      float ls = sqrtf(dot3(Sv, Sv));
+      if (!(ls > 0.f)) continue;
+      float cost = -dot3(Sv, X) / (ls * lx);
+      if (cost > sc.cs.cos_filter_tri) continue;
+      float cphi = dot3(Sv, V3<float>{h.x, h.y, h.z}) / ls;
+      if (cphi <= 0.f) continue;
+      float H[9];
+      if (!homography<float>(R, vd.lp[(size_t)r.level * nsrc + j], (float)x, (float)y, h, H)) continue;
+      float m = ncc_cost<float>(sc, R, rs, S, H, x, y);
+      float e = sc.cs.ncc_norm * ps_expf(-m * m * sc.cs.inv2ncc);
+      if (e / (e + 0.5f) < sc.cs.q_min) continue;
+      if (geo_error<float>(r, R, S, pr, x, y, h.w) > sc.cs.filter_gmax) continue;
+      count++;
+    }
+  }
+  return std::min(count, 255);
+}
+
+void to_state(const ps_view_state& vs, State& st, bool planes) {
+  st.w = (int)vs.width;
+  st.h = (int)vs.height;
+  const size_t n = (size_t)st.w * st.h;
+  st.plane.assign(n, P4{0, 0, 0, 0});
+  st.cost.assign(n, 2.0f);
+  st.bview.assign(n, 255);
+  if (planes)
+    for (size_t p = 0; p < n; ++p) st.plane[p] = {vs.normal[3 * p], vs.normal[3 * p + 1], vs.normal[3 * p + 2], vs.depth[p]};
+  if (vs.prior) {
+    st.prior.resize(n);
+    memcpy(st.prior.data(), vs.prior, n * sizeof(P4));
+  }
+}
+void from_state(const State& st, ps_view_state& vs) {
+  const size_t n = (size_t)st.w * st.h;
+  for (size_t p = 0; p < n; ++p) {
+    vs.normal[3 * p] = st.plane[p].x;
+    vs.normal[3 * p + 1] = st.plane[p].y;
+    vs.normal[3 * p + 2] = st.plane[p].z;
+    vs.depth[p] = st.plane[p].w;
+    vs.cost[p] = st.cost[p];
+  }
+}
+
+std::vector<std::vector<float>> snapshot_maps(const Scene& sc, const ps_depth_snapshot* snap) {
+  std::vector<std::vector<float>> m(sc.v.size());
+  if (!snap) return m;
+  for (size_t v = 0; v < sc.v.size(); ++v)
+    if (v < snap->num_maps && snap->maps && snap->maps[v]) {
+      const Img& L = sc.L((int)v, (int)snap->level);
+      m[v].assign(snap->maps[v], snap->maps[v] + (size_t)L.w * L.h);
+    }
+  return m;
+}
+
+int set_threads(int threads) {
+  if (threads > 0) omp_set_num_threads(threads);
+  return 0;
+}
+
+}  // namespace
+
+// ================================================================================================ C entry points
+extern "C" {
+
+// PatchMatchSession::run restated (crates/cuda/src/patchmatch.rs:752-799): per view, run start (evaluate mode 1)
+// then `iterations` × (colour 0, colour 1) half steps.
+int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
+               const ps_run_params* p, const ps_depth_snapshot* snap, int threads) {
+  Scene sc;
+  if (!load_scene(in, sc) || !p) return PS_EINVAL;
+  if (p->geometric && !snap) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<std::vector<float>> maps = snapshot_maps(sc, snap);
+  for (size_t i = 0; i < n; ++i) {
+    State st;
+    to_state(states[i], st, !p->random_init);
+    Run r;
+    r.sc = &sc;
+    r.view = (int)views[i];
+    r.level = (int)p->level;
+    r.geometric = p->geometric;
+    r.run_id = (int)p->run_id;
+    r.topk = sc.cs.topk;
+    r.use_prior = p->use_prior && states[i].prior ? 1 : 0;
+    r.snap = &maps;
+    r.t = 0;
+    r.color = 0;
+    r.tau_good = r.eps = r.phi = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < st.h; ++y)
+      for (int x = 0; x < st.w; ++x) eval_pixel(r, st, x, y, 1, p->random_init);
+    for (uint32_t t = 0; t < p->iterations; ++t) {
+      r.t = (int)t;
+      ps_iter_consts(&sc.pm, p->geometric, (int)t, &r.tau_good, &r.eps, &r.phi);
+      for (int color = 0; color < 2; ++color) {
+        r.color = color;
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int y = 0; y < st.h; ++y)
+          for (int x = ((y + color) & 1); x < st.w; x += 2) half_pixel(r, st, x, y);
+      }
+    }
+    from_state(st, states[i]);
+  }
+  return PS_OK;
+}
+
+int oracle_evaluate(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,
+                    const ps_view_state* states, uint32_t geometric, const ps_depth_snapshot* snap, float* const* out,
+                    int threads) {
+  Scene sc;
+  if (!load_scene(in, sc)) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<std::vector<float>> maps = snapshot_maps(sc, snap);
+  for (size_t i = 0; i < n; ++i) {
+    State st;
+    to_state(states[i], st, true);
+    Run r{};
+    r.sc = &sc;
+    r.view = (int)views[i];
+    r.level = (int)level;
+    r.geometric = geometric;
+    r.topk = sc.cs.topk;
+    r.snap = &maps;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < st.h; ++y)
+      for (int x = 0; x < st.w; ++x) eval_pixel(r, st, x, y, 0, 0);
+    memcpy(out[i], st.cost.data(), st.cost.size() * sizeof(float));
+  }
+  return PS_OK;
+}
+
+int oracle_filter(const ps_kernel_input* in, const uint32_t* views, size_t n, const ps_view_state* states,
+                  const ps_depth_snapshot* snap, uint8_t* const* out, int threads) {
+  Scene sc;
+  if (!load_scene(in, sc) || !snap) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<std::vector<float>> maps = snapshot_maps(sc, snap);
+  for (size_t i = 0; i < n; ++i) {
+    State st;
+    to_state(states[i], st, true);
+    Run r{};
+    r.sc = &sc;
+    r.view = (int)views[i];
+    r.level = (int)snap->level;
+    r.geometric = 1;
+    r.topk = sc.cs.topk;
+    r.snap = &maps;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < st.h; ++y)
+      for (int x = 0; x < st.w; ++x) out[i][y * st.w + x] = (uint8_t)filter_pixel(r, st, x, y);
+  }
+  return PS_OK;
+}
+
+// pm_upsample (patchmatch.cu:741-801), binary32.
+int oracle_upsample(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,
+                    const ps_view_state* low, float sigma_s, float sigma_c, ps_view_state* out, int threads) {
+  Scene sc;
+  if (!load_scene(in, sc) || level < 1) return PS_EINVAL;
+  set_threads(threads);
+  const float inv2s = 1.0f / (2.0f * sigma_s * sigma_s), inv2c = 1.0f / (2.0f * sigma_c * sigma_c);
+  for (size_t i = 0; i < n; ++i) {
+    const Img& R = sc.L((int)views[i], (int)level);
+    const Img& L = sc.L((int)views[i], (int)level - 1);
+    const ps_view_state& lo = low[i];
+    ps_view_state& o = out[i];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < R.h; ++y)
+      for (int x = 0; x < R.w; ++x) {
+        V3<float> rp = pixel_ray(R, x, y);
+        float ip = R.at(x, y);
+        float px = ((float)x - 0.5f) * 0.5f, py = ((float)y - 0.5f) * 0.5f;
+        int qx0 = (int)roundf(px), qy0 = (int)roundf(py);
+        float sw = 0.f, sd = 0.f;
+        V3<float> sn = {0.f, 0.f, 0.f};
+        float nd = 1e30f, ndep = 0.f;
+        V3<float> nn = {0.f, 0.f, 0.f};
+        for (int qy = qy0 - 2; qy <= qy0 + 2; ++qy) {
+          if (qy < 0 || qy >= L.h) continue;
+          for (int qx = qx0 - 2; qx <= qx0 + 2; ++qx) {
+            if (qx < 0 || qx >= L.w) continue;
+            size_t qi = (size_t)qy * L.w + qx;
+            float qw = lo.depth[qi];
+            if (!(qw > 0.f)) continue;
+            V3<float> nq = {lo.normal[3 * qi], lo.normal[3 * qi + 1], lo.normal[3 * qi + 2]};
+            float den = dot3(nq, rp);
+            if (!(den < -1e-6f)) continue;
+            float d = qw * dot3(nq, pixel_ray(L, qx, qy)) / den;
+            if (!(d > 0.f) || !std::isfinite(d)) continue;
+            float ds = ((float)qx - px) * ((float)qx - px) + ((float)qy - py) * ((float)qy - py);
+            if (ds < nd) {
+              nd = ds;
+              ndep = d;
+              nn = nq;
+            }
+            float iq = L.at(qx, qy);
+            float wgt = ps_expf(-ds * inv2s - (ip - iq) * (ip - iq) * inv2c);
+            sw += wgt;
+            sd += wgt * d;
+            sn.x += wgt * nq.x;
+            sn.y += wgt * nq.y;
+            sn.z += wgt * nq.z;
+          }
+        }
+        float d = 0.f;
+        V3<float> nr = {0.f, 0.f, 0.f};
+        bool ok = false;
+        if (sw > 1e-12f) {
+          d = sd / sw;
+          nr = sn;
+          ok = true;
+        } else if (nd < 1e29f) {
+          d = ndep;
+          nr = nn;
+          ok = true;
+        }
+        P4 res = {0.f, 0.f, 0.f, 0.f};
+        if (ok && dot3(nr, nr) > 1e-24f) {
+          nr = nrm3(nr);
+          if (dot3(nr, rp) >= 0.f) nr = {-nr.x, -nr.y, -nr.z};
+          res = {nr.x, nr.y, nr.z, d};
+        }
+        size_t p = (size_t)y * R.w + x;
+        o.normal[3 * p] = res.x;
+        o.normal[3 * p + 1] = res.y;
+        o.normal[3 * p + 2] = res.z;
+        o.depth[p] = res.w;
+        if (o.cost) o.cost[p] = 2.f;
+      }
+  }
+  return PS_OK;
+}
+
+// pm_median (patchmatch.cu:805-849), binary32.
+int oracle_median(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,
+                  const ps_view_state* inp, ps_view_state* out, int threads) {
+  Scene sc;
+  if (!load_scene(in, sc)) return PS_EINVAL;
+  set_threads(threads);
+  for (size_t i = 0; i < n; ++i) {
+    const Img& R = sc.L((int)views[i], (int)level);
+    const ps_view_state& s = inp[i];
+    ps_view_state& o = out[i];
+    const int w = R.w, h = R.h;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < h; ++y)
+      for (int x = 0; x < w; ++x) {
+        size_t p = (size_t)y * w + x;
+        P4 self = {s.normal[3 * p], s.normal[3 * p + 1], s.normal[3 * p + 2], s.depth[p]};
+        P4 res = self;
+        if (self.w > 0.f) {
+          V3<float> rp = pixel_ray(R, x, y);
+          float ds[25];
+          int qs[25];
+          int c = 0;
+          for (int qy = std::max(y - 2, 0); qy < std::min(y + 3, h); ++qy)
+            for (int qx = std::max(x - 2, 0); qx < std::min(x + 3, w); ++qx) {
+              size_t qi = (size_t)qy * w + qx;
+              float qw = s.depth[qi];
+              if (!(qw > 0.f)) continue;
+              V3<float> nq = {s.normal[3 * qi], s.normal[3 * qi + 1], s.normal[3 * qi + 2]};
+              float den = dot3(nq, rp);
+              if (!(den < -1e-6f)) continue;
+              float d = qw * dot3(nq, pixel_ray(R, qx, qy)) / den;
+              if (!(d > 0.f) || !std::isfinite(d)) continue;
+              int k = c++;
+              while (k > 0 && (ds[k - 1] > d || (ds[k - 1] == d && qs[k - 1] > (int)qi))) {
+                ds[k] = ds[k - 1];
+                qs[k] = qs[k - 1];
+                --k;
+              }
+              ds[k] = d;
+              qs[k] = (int)qi;
+            }
+          if (c > 0) {
+            int m = (c - 1) / 2;
+            res = {s.normal[3 * qs[m]], s.normal[3 * qs[m] + 1], s.normal[3 * qs[m] + 2], ds[m]};
+          }
+        }
+        o.normal[3 * p] = res.x;
+        o.normal[3 * p + 1] = res.y;
+        o.normal[3 * p + 2] = res.z;
+        o.depth[p] = res.w;
+        if (o.cost && s.cost && o.cost != s.cost) o.cost[p] = s.cost[p];
+      }
+  }
+  return PS_OK;
+}
+
+// FP64 re-evaluation of given hypotheses: top-K cost of every pixel in binary64 (geometry from FP64 pairs when
+// given).  out[i] receives w*h doubles.
+int oracle_reeval_f64(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,
+                      const ps_view_state* states, uint32_t geometric, const ps_depth_snapshot* snap,
+                      double* const* out, int threads) {
+  Scene sc;
+  if (!load_scene(in, sc)) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<std::vector<float>> maps = snapshot_maps(sc, snap);
+  for (size_t i = 0; i < n; ++i) {
+    State st;
+    to_state(states[i], st, true);
+    Run r{};
+    r.sc = &sc;
+    r.view = (int)views[i];
+    r.level = (int)level;
+    r.geometric = geometric;
+    r.topk = sc.cs.topk;
+    r.snap = &maps;
+    const Img& R = sc.L(r.view, r.level);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int y = 0; y < st.h; ++y)
+      for (int x = 0; x < st.w; ++x) {
+        P4 hh = st.plane[(size_t)y * st.w + x];
+        double c = 2.0;
+        if (hh.w > 0.f) {
+          RS<double> rs = ref_stats<double>(sc, R, x, y);
+          c = topk_cost<double>(r, R, rs, x, y, hh);
+        }
+        out[i][(size_t)y * st.w + x] = c;
+      }
+  }
+  return PS_OK;
+}
+
+// ---- known-answer entry points (crates/dense/src/math.rs, kernel.rs, upsample.rs) ----------------------------
+uint64_t oracle_mix64(uint64_t z) { return mix64(z); }
+uint64_t oracle_rng_state(uint64_t seed, uint64_t key, uint32_t level, uint32_t run, uint32_t t, uint32_t half,
+                          uint64_t pixel) {
+  return rng_state(seed, key, (int)level, (int)run, (int)t, (int)half, pixel);
+}
+float oracle_rng_next(uint64_t* state) {
+  u64 s = *state;
+  float f = rnd(s);
+  *state = s;
+  return f;
+}
+uint64_t oracle_hash_bytes(const uint8_t* b, size_t n) {
+  uint64_t h = 0xcbf29ce484222325ULL;
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 0x00000100000001b3ULL;
+  }
+  return h;
+}
+double oracle_erf(double x) { return ps_erf(x); }
+double oracle_emission_norm(double s) { return ps_emission_norm(s); }
+double oracle_emission(double c, double s) { return ps_emission(c, s); }
+double oracle_visibility_probability(double c, double s) {
+  double e = ps_emission(c, s);
+  return e / (e + 0.5);
+}
+// triangulation_prior / incident_prior / resolution_prior (math.rs:84-123)
+double oracle_triangulation_prior(double cos_theta, double min_angle_rad) {
+  double cmin = cos(min_angle_rad);
+  if (cos_theta > cmin) {
+    double s = 1.0 - (1.0 - cos_theta) / (1.0 - cmin);
+    return std::min(std::max(1.0 - s * s, 0.0), 1.0);
+  }
+  return 1.0;
+}
+double oracle_incident_prior(double cos_phi, double sigma) {
+  double x = 1.0 - std::max(cos_phi, 0.0);
+  return exp(-x * x / (2.0 * sigma * sigma));
+}
+double oracle_resolution_prior(const double* h, double x, double y, double radius) {
+  double c[4][2] = {{x - radius, y - radius}, {x - radius, y + radius}, {x + radius, y + radius}, {x + radius, y - radius}};
+  double p[4][2];
+  for (int i = 0; i < 4; ++i) {
+    double z = h[6] * c[i][0] + h[7] * c[i][1] + h[8];
+    p[i][0] = (h[0] * c[i][0] + h[1] * c[i][1] + h[2]) / z;
+    p[i][1] = (h[3] * c[i][0] + h[4] * c[i][1] + h[5]) / z;
+  }
+  double area = 0.0;
+  for (int i = 0; i < 4; ++i) area += p[i][0] * p[(i + 1) % 4][1] - p[(i + 1) % 4][0] * p[i][1];
+  double a_src = 0.5 * fabs(area), a_ref = (2.0 * radius + 1.0) * (2.0 * radius + 1.0);
+  if (a_src <= 0.0 || !std::isfinite(a_src)) return 0.0;
+  return std::min(a_src / a_ref, a_ref / a_src);
+}
+// plane_transfer (math.rs:143-154); returns 1 and writes *out when the transfer exists.
+int oracle_plane_transfer(double dq, const double* n, const double* rq, const double* rp, double* out) {
+  double num = n[0] * rq[0] + n[1] * rq[1] + n[2] * rq[2];
+  double den = n[0] * rp[0] + n[1] * rp[1] + n[2] * rp[2];
+  if (den > -1e-6) return 0;
+  double d = dq * num / den;
+  if (!(d > 0.0 && std::isfinite(d))) return 0;
+  *out = d;
+  return 1;
+}
+// num_levels (upsample.rs:35-44)
+size_t oracle_num_levels(size_t min_side, size_t max_levels, size_t min_size) {
+  size_t l = 1, s = min_side;
+  while (l < max_levels && s / 2 >= min_size) {
+    s /= 2;
+    l += 1;
+  }
+  return l;
+}
+// build_pyramid, one step (upsample.rs:46-102): blur3 (σ=0.5, clamped borders), 2×2 average, round to u8.
+// out has (w/2)*(h/2) bytes; kout receives the halved intrinsics.
+void oracle_pyramid_step(const uint8_t* src, size_t w, size_t h, const double* k, uint8_t* out, double* kout) {
+  float g0 = expf(-1.0f / (2.0f * 0.25f));
+  float g[3] = {g0, 1.0f, g0};
+  float s = g[0] + g[1] + g[2];
+  for (float& x : g) x /= s;
+  std::vector<float> cur(w * h), tmp(w * h), b(w * h);
+  for (size_t i = 0; i < w * h; ++i) cur[i] = (float)src[i];
+  for (size_t y = 0; y < h; ++y)
+    for (size_t x = 0; x < w; ++x) {
+      float a = 0.0f;
+      for (int kk = 0; kk < 3; ++kk) {
+        long xx = std::min(std::max((long)x + kk - 1, 0L), (long)w - 1);
+        a += g[kk] * cur[y * w + xx];
+      }
+      tmp[y * w + x] = a;
+    }
+  for (size_t y = 0; y < h; ++y)
+    for (size_t x = 0; x < w; ++x) {
+      float a = 0.0f;
+      for (int kk = 0; kk < 3; ++kk) {
+        long yy = std::min(std::max((long)y + kk - 1, 0L), (long)h - 1);
+        a += g[kk] * tmp[yy * w + x];
+      }
+      b[y * w + x] = a;
+    }
+  size_t nw = w / 2, nh = h / 2;
+  for (size_t y = 0; y < nh; ++y)
+    for (size_t x = 0; x < nw; ++x) {
+      size_t i = 2 * y * w + 2 * x;
+      float v = 0.25f * (b[i] + b[i + 1] + b[i + w] + b[i + w + 1]);
+      out[y * nw + x] = (uint8_t)std::min(std::max(roundf(v), 0.0f), 255.0f);
+    }
+  kout[0] = k[0] * 0.5;
+  kout[1] = k[1] * 0.5;
+  kout[2] = (k[2] + 0.5) * 0.5 - 0.5;
+  kout[3] = (k[3] + 0.5) * 0.5 - 0.5;
+}
+float oracle_expf(float x) { return ps_expf(x); }
+void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
+
+}  // extern "C"

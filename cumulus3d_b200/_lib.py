@@ -21,7 +21,11 @@ PS_MAX_SOURCES = 32
 
 class Options(C.Structure):
     _fields_ = [("math_mode", C.c_uint32), ("max_batch", C.c_uint32), ("batch_pixels", C.c_uint64),
-                ("checked", C.c_uint32), ("reserved", C.c_uint32)]
+                ("checked", C.c_uint32), ("tuning", C.c_uint32)]
+
+
+PS_TUNE_NO_WEIGHT_CACHE, PS_TUNE_TEX_GATHER, PS_TUNE_ONE_LANE = 0x1, 0x2, 0x4
+PS_KERNEL_HALF, PS_KERNEL_EVAL, PS_KERNEL_FILTER, PS_KERNEL_OTHER = range(4)
 
 
 class PmParams(C.Structure):
@@ -108,6 +112,12 @@ SIGNATURES = {
     "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_synchronize": (C.c_int, [_P]),
     "ps_launch_count": (C.c_uint64, [_P]),
+    "ps_session_stream": (C.c_void_p, [_P]),
+    "ps_set_profiling": (C.c_int, [_P, C.c_uint32]),
+    "ps_kernel_stats": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
+                                  C.POINTER(C.c_uint64)]),
+    "ps_reset_stats": (C.c_int, [_P]),
+    "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
 }
 
 _engine = None

@@ -10,7 +10,8 @@
 // The rules are those of the reference kernel crates/cuda/src/kernels/patchmatch.cu (cited per function) and of
 // crates/dense/src/kernel.rs:36-74.  The B200 layout differs from the reference:
 //   * every image level is a normalised f32 plane with a PS_BORDER-pixel zero border, so a bilinear source tap is
-//     four unconditional loads after a clamp (no texture objects, no per-texel bounds tests);
+//     four unconditional loads after a clamp (no per-texel bounds tests); optionally (PS_TUNE_TEX_GATHER) a gather
+//     through a border-addressed texture fetches the same four texels with one instruction;
 //   * a half-step CTA is 128 threads covering a 32 × 8 pixel tile; each warp takes 16 active columns of two
 //     adjacent rows, so reference-tile reads of the two colour phases fall into disjoint shared-memory banks;
 //   * the bilateral window weights of a pixel are computed once per half step and cached in shared memory (one
@@ -42,7 +43,7 @@ __device__ __forceinline__ float m_rcp(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 #else
-  return 1.0f / x;
+  return __frcp_rn(x);  // correctly rounded, i.e. the same bits as 1.0f / x
 #endif
 }
 __device__ __forceinline__ float m_exp(float x) {
@@ -101,14 +102,31 @@ __device__ __forceinline__ float3 pixel_ray(const PsLevel& R, int x, int y) {
 // Bilinear value at (u, v), integer-centre convention, 0 outside the image.  The clamp to [-2, w] × [-2, h] keeps
 // both taps of an out-of-image footprint inside the zero border, which reproduces the reference's "0 outside"
 // without per-texel tests.
+__device__ __forceinline__ int f2i_exact(float v) {
+  // v is an integer in [-2^22, 2^22]: adding 1.5·2^23 puts it in the low mantissa bits (one FADD instead of the
+  // quarter-rate F2I conversion).
+  return __float_as_int(v + 12582912.0f) - 0x4B400000;
+}
 __device__ __forceinline__ float src_sample(const float* __restrict__ img, int pitch, float wf, float hf, float u,
                                             float v) {
   float xf = floorf(u), yf = floorf(v);
   float ax = u - xf, ay = v - yf;
   float xc = fminf(fmaxf(xf, -2.0f), wf);
   float yc = fminf(fmaxf(yf, -2.0f), hf);
-  const float* p = img + (int)yc * pitch + (int)xc;
+  const float* p = img + f2i_exact(yc) * pitch + f2i_exact(xc);
   float p00 = __ldg(p), p10 = __ldg(p + 1), p01 = __ldg(p + pitch), p11 = __ldg(p + pitch + 1);
+  float top = fmaf(ax, p10 - p00, p00);
+  float bot = fmaf(ax, p11 - p01, p01);
+  return fmaf(ay, bot - top, top);
+}
+// Same sample through the texture unit: one gather at the exact integer corner (x0+1, y0+1) of the 2×2 footprint
+// returns its four texels (border addressing gives 0 outside the image); the bilinear arithmetic is unchanged, so
+// the result has the same bits as src_sample.  Gather order: (T[x0,y1], T[x1,y1], T[x1,y0], T[x0,y0]).
+__device__ __forceinline__ float src_sample_tex(unsigned long long tex, float u, float v) {
+  float xf = floorf(u), yf = floorf(v);
+  float ax = u - xf, ay = v - yf;
+  const float4 q = tex2Dgather<float4>((cudaTextureObject_t)tex, xf + 1.0f, yf + 1.0f, 0);
+  const float p00 = q.w, p10 = q.z, p01 = q.x, p11 = q.y;
   float top = fmaf(ax, p10 - p00, p00);
   float bot = fmaf(ax, p11 - p01, p01);
   return fmaf(ay, bot - top, top);
@@ -120,35 +138,53 @@ struct RefStats {
 };
 
 // Tile-resident reference window of one pixel: t points at the pixel inside the shared tile (row pitch tw); wc is
-// the thread's weight-cache slot (stride NT floats between taps).
+// the thread's weight-cache slot (stride NT floats between taps).  Window sums are split by row parity: even rows
+// (a = 0, 2, …) and odd rows (a = 1, 3, …) accumulate separately, in ascending row order, and the NCC uses
+// even + odd.  With G = 2 lanes per pixel, lane g sums the rows of parity g and the two partial sums meet through
+// one shuffle (pmask = the pair's lanes); with G = 1 one thread keeps both partial sums.
 struct RefWin {
   const float* t;
   int tw;
   float* wc;
+  int g;
+  unsigned pmask;
 };
 
+// Row-parity partial sums -> total (even + odd; IEEE addition is commutative, so both lanes get the same bits).
+template <int G>
+__device__ __forceinline__ float pair_total(const RefWin& rw, const float* part) {
+  if constexpr (G == 1) {
+    return part[0] + part[1];
+  } else {
+    const float other = __shfl_xor_sync(rw.pmask, part[0], 1);
+    return part[0] + other;
+  }
+}
+
 // ref_stats (patchmatch.cu:199-223).  Weights w_k = exp(-(dx²+dy²)/(2σs²) - (Ic-Ik)²/(2σc²)); 0 outside the image.
-template <int WR, int WS, bool CW, int NT>
+template <int WR, int WS, bool CW, int NT, int G = 1>
 __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) {
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
   RefStats s;
   s.ic = rw.t[0];
-  float W = 0.f, S = 0.f, SS = 0.f;
+  float W[2] = {0.f, 0.f}, S[2] = {0.f, 0.f}, SS[2] = {0.f, 0.f};
 #pragma unroll 1
-  for (int a = 0; a < wn; ++a) {
+  for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
     const int dy = -wr + a * ws;
+    const int pa = G == 2 ? 0 : (a & 1);
     const float* trow = rw.t + dy * rw.tw;
+    float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
     auto tap = [&](int b) {
       const int dx = -wr + b * ws;
       float ik = trow[dx];
       float d = s.ic - ik;
       float w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
-      if (CW) rw.wc[(a * wn + b) * NT] = w;
+      if (CW) wrow[b * NT] = w;
       float wi = w * ik;
-      W = W + w;
-      S = S + wi;
-      SS = fmaf(wi, ik, SS);
+      W[pa] = W[pa] + w;
+      S[pa] = S[pa] + wi;
+      SS[pa] = fmaf(wi, ik, SS[pa]);
     };
     if constexpr (WR != 0) {
 #pragma unroll
@@ -158,9 +194,10 @@ __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) 
       for (int b = 0; b < wn; ++b) tap(b);
     }
   }
-  s.W = W;
-  s.mu = S / W;
-  s.var = SS / W - s.mu * s.mu;
+  s.W = pair_total<G>(rw, W);
+  const float St = pair_total<G>(rw, S), SSt = pair_total<G>(rw, SS);
+  s.mu = St / s.W;
+  s.var = SSt / s.W - s.mu * s.mu;
   return s;
 }
 
@@ -188,9 +225,9 @@ __device__ __forceinline__ bool homography(const PsLevel& R, const PsLPair& L, f
 // Parity operation sequence per tap (dx, dy), with sx = x+dx, sy = y+dy:
 //   zz = fma(H6, sx, fma(H7, sy, H8)); if zz > 1e-8: s = sample(fma(H0,sx,fma(H1,sy,H2))·(1/zz), fma(H3,sx,fma(H4,sy,H5))·(1/zz))
 //   ws = w·s; Ss += ws; SSs = fma(ws, s, SSs); IS = fma(ws, Ik, IS)
-template <int WR, int WS, bool CW, int NT>
-__device__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S, const float* H,
-                          int x, int y) {
+template <int WR, int WS, bool CW, int NT, bool TEX = false, int G = 1>
+__device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
+                                          const float* H, int x, int y, int& nwin) {
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
   const float fx = (float)x, fy = (float)y;
@@ -202,18 +239,21 @@ __device__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, 
   const float wf = (float)S.w, hf = (float)S.h;
   if (!(u >= 0.f && v >= 0.f && u <= wf - 1.0f && v <= hf - 1.0f)) return 2.0f;
   if (rs.var < 1e-5f) return 2.0f;
+  nwin++;
   const float* __restrict__ img = S.img;
+  const unsigned long long tex = S.tex;
   const int pitch = S.pitch;
-  float Ss = 0.f, SSs = 0.f, IS = 0.f;
+  float Ss[2] = {0.f, 0.f}, SSs[2] = {0.f, 0.f}, IS[2] = {0.f, 0.f};
 #pragma unroll 1
-  for (int a = 0; a < wn; ++a) {
+  for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
     const int dy = -wr + a * ws;
+    const int pa = G == 2 ? 0 : (a & 1);
     const float sy = fy + (float)dy;
     const float rx = fmaf(H[1], sy, H[2]);
     const float ry = fmaf(H[4], sy, H[5]);
     const float rz = fmaf(H[7], sy, H[8]);
     const float* trow = rw.t + dy * rw.tw;
-    const float* wrow = rw.wc + a * wn * NT;
+    const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
     auto tap = [&](int b) {
       const int dx = -wr + b * ws;
       const float sx = fx + (float)dx;
@@ -229,12 +269,13 @@ __device__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, 
       float sv = 0.f;
       if (zz > 1e-8f) {
         const float izz = m_rcp(zz);
-        sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+        if constexpr (TEX) sv = src_sample_tex(tex, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+        else sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
       }
       const float wsv = w * sv;
-      Ss = Ss + wsv;
-      SSs = fmaf(wsv, sv, SSs);
-      IS = fmaf(wsv, ik, IS);
+      Ss[pa] = Ss[pa] + wsv;
+      SSs[pa] = fmaf(wsv, sv, SSs[pa]);
+      IS[pa] = fmaf(wsv, ik, IS[pa]);
     };
     if constexpr (WR != 0) {
 #pragma unroll
@@ -244,11 +285,12 @@ __device__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, 
       for (int b = 0; b < wn; ++b) tap(b);
     }
   }
+  const float Sst = pair_total<G>(rw, Ss), SSst = pair_total<G>(rw, SSs), ISt = pair_total<G>(rw, IS);
   float iW = 1.0f / rs.W;
-  float mus = Ss * iW;
-  float vars = SSs * iW - mus * mus;
+  float mus = Sst * iW;
+  float vars = SSst * iW - mus * mus;
   if (vars < 1e-5f) return 2.0f;
-  float cov = IS * iW - rs.mu * mus;
+  float cov = ISt * iW - rs.mu * mus;
 #if PS_FAST
   float c = 1.0f - cov * rsqrtf(rs.var * vars);
 #else
@@ -284,13 +326,13 @@ __device__ float geo_error(const PsRun& P, const PsLevel& R, const PsLevel& S, c
 }
 
 // (photometric cost, truncated geometric error) of one hypothesis × one source (patchmatch.cu:316-324).
-template <int WR, int WS, bool CW, int NT>
+template <int WR, int WS, bool CW, int NT, bool TEX = false, int G = 1>
 __device__ __forceinline__ float pair_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& R,
                                            const PsLevel& S, const PsPair& pr, const PsLPair& lp, int x, int y,
-                                           float4 h, float* geo) {
+                                           float4 h, float* geo, int& nwin) {
   float H[9];
   float c = 2.0f;
-  if (homography(R, lp, (float)x, (float)y, h, H)) c = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y);
+  if (homography(R, lp, (float)x, (float)y, h, H)) c = ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin);
   if (P.geometric) *geo = fminf(geo_error(P, R, S, pr, x, y, h.w), P.gmax);
   return c;
 }
@@ -387,23 +429,42 @@ __device__ __forceinline__ int find_item(const PsRun& P, int cta) {
 }
 
 // ================================================================================ half step (patchmatch.cu:439-657)
-template <int WR, int WS, bool CW>
-__global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ PsRun P) {
+// Warp-aggregated add of the per-thread NCC window count (threads that already returned do not take part).
+__device__ __forceinline__ void count_windows(const PsRun& P, int nwin) {
+  if (!P.ncc_count) return;
+  const unsigned m = __activemask();
+  const unsigned s = __reduce_add_sync(m, (unsigned)nwin);
+  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s) atomicAdd(P.ncc_count, (unsigned long long)s);
+}
+
+// Half-step tile geometry for G lanes per pixel: G = 1 -> 32 × 8 pixels (a warp = 16 active columns × 2 rows);
+// G = 2 -> 16 × 8 pixels (a warp = 8 active columns × 2 rows × 2 lanes).  The shared tile's row pitch is padded so
+// that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.
+__host__ __device__ constexpr int half_pw(int G) { return G == 2 ? PS_HALF2_PW : PS_HALF_PW; }
+__host__ __device__ constexpr int half_tw(int G, int wr) {
+  return G == 2 ? (((PS_HALF2_PW + 2 * wr) + 15) / 32) * 32 + 16 : PS_HALF_PW + 2 * wr;
+}
+
+// G = 1: two CTAs per SM with the weight cache (~90 KB each for a 13×13 window), four without it.
+// G = 2: the two lanes of a pixel split the window rows, so each thread caches half the weights: four CTAs per SM.
+template <int WR, int WS, bool CW, bool TEX, int G>
+__global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_HALF_NT;
+  constexpr int PW = half_pw(G);
   extern __shared__ float sm[];
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
-  const int TW = PS_HALF_PW + 2 * wr, TH = PS_HALF_PH + 2 * wr;
+  const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
   float* tile = sm;
   float* wcache = sm + ((TW * TH + 31) & ~31);
-  float* wvs = wcache + (CW ? wn * wn * NT : 0);
+  float* wvs = wcache + (CW ? ((wn + G - 1) / G) * wn * NT : 0);
 
   const int ii = find_item(P, blockIdx.x);
   const PsItem& it = P.items[ii];
   const int w = it.w, h = it.h;
-  const int tiles_x = (w + PS_HALF_PW - 1) / PS_HALF_PW;
+  const int tiles_x = (w + PW - 1) / PW;
   const int tl = blockIdx.x - it.tile0;
-  const int x0 = (tl % tiles_x) * PS_HALF_PW, y0 = (tl / tiles_x) * PS_HALF_PH;
+  const int x0 = (tl % tiles_x) * PW, y0 = (tl / tiles_x) * PS_HALF_PH;
   const PsLevel R = P.lv[it.view * P.nlevels + P.level];
   {
     const int ox = x0 - wr, oy = y0 - wr;
@@ -415,15 +476,18 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ 
   }
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int row = 2 * warp + (lane >> 4), col = lane & 15;
+  const int gl = G == 2 ? (lane & 1) : 0;
+  const int row = 2 * warp + (lane >> 4), col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
   const int y = y0 + row;
   const int x = x0 + 2 * col + ((y + P.color) & 1);
-  if (x >= w || y >= h) return;
+  if (x >= w || y >= h) return;  // both lanes of a pixel leave together
 
   RefWin rw;
   rw.t = tile + (row + wr) * TW + (x - x0 + wr);
   rw.tw = TW;
   rw.wc = wcache + threadIdx.x;
+  rw.g = gl;
+  rw.pmask = G == 2 ? (3u << (lane & ~1)) : 0u;
   float* wv = wvs + threadIdx.x;
 
   const PsView& vd = P.views[it.view];
@@ -471,7 +535,8 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ 
   }
 
   // 2. View traversal: voting, weighting, aggregation.
-  const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
+  int nwin = 0;
+  const RefStats rs = ref_stats<WR, WS, CW, NT, G>(P, rw);
   const int vprev = P.bview[base + pix];
   float num[9], numf[9];
 #pragma unroll
@@ -494,14 +559,14 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ 
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[0], H);
       prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
       if (!(prior > 0.f)) continue;
-      m[0] = ok ? ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y) : 2.f;
+      m[0] = ok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.f;
       gg[0] = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[0].w), P.gmax) : 0.f;
     }
 #pragma unroll 1
     for (int i = 1; i < 9; ++i) {
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[i], H);
-      const float mi = ok ? ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y) : 2.f;
+      const float mi = ok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.f;
       const float gi = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[i].w), P.gmax) : 0.f;
 #pragma unroll
       for (int q = 1; q < 9; ++q)
@@ -606,7 +671,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ 
         const PsLPair lp = lps[j];
         const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
         float g = 0.f;
-        const float mm = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, cd, &g);
+        const float mm = pair_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, R, S, pr, lp, x, y, cd, &g, nwin);
         nm += wj * (mm + P.lambda * g);
       }
       cc = nm / den;
@@ -618,16 +683,19 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half(const __grid_constant__ 
       best = cd;
     }
   }
-  pl[pix] = best;
-  P.cost[base + pix] = bcost;
-  P.bview[base + pix] = (unsigned char)vbest;
+  if (gl == 0) {
+    pl[pix] = best;
+    P.cost[base + pix] = bcost;
+    P.bview[base + pix] = (unsigned char)vbest;
+  }
+  count_windows(P, gl == 0 ? nwin : 0);
 }
 
 // ================================================================================ run start / evaluate (patchmatch.cu:661-692)
 // Top-K mean cost (patchmatch.cu:327-345).
 template <int WR, int WS, bool CW, int NT>
 __device__ float topk_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& R, const PsPair* prs,
-                           const PsLPair* lps, int nsrc, int x, int y, float4 h) {
+                           const PsLPair* lps, int nsrc, int x, int y, float4 h, int& nwin) {
   float b0 = 1e30f, b1 = 1e30f, b2 = 1e30f;
 #pragma unroll 1
   for (int j = 0; j < nsrc; ++j) {
@@ -635,7 +703,7 @@ __device__ float topk_cost(const PsRun& P, const RefWin& rw, const RefStats& rs,
     const PsLPair lp = lps[j];
     const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
     float g = 0.f;
-    float c = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, h, &g);
+    float c = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, h, &g, nwin);
     if (P.geometric) c += P.lambda * g;
     if (c < b0) {
       b2 = b1;
@@ -718,12 +786,14 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
     P.plane[base + pix] = h;
   }
   float c = 2.f;
+  int nwin = 0;
   if (h.w > 0.f) {
     const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
-    c = topk_cost<WR, WS, CW, NT>(P, rw, rs, e.R, prs, lps, vd.nsrc, x, y, h);
+    c = topk_cost<WR, WS, CW, NT>(P, rw, rs, e.R, prs, lps, vd.nsrc, x, y, h, nwin);
   }
   P.cost[base + pix] = c;
   if (P.mode == 1) P.bview[base + pix] = 255;
+  count_windows(P, nwin);
 }
 
 // ================================================================================ final readout (patchmatch.cu:695-737)
@@ -753,6 +823,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant_
   const long long base = it.off;
   const float4 h = P.plane[base + pix];
   int count = 0;
+  int nwin = 0;
   if (h.w > 0.f) {
     const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
     const float3 ray = pixel_ray(e.R, x, y);
@@ -772,7 +843,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant_
       float H[9];
       const PsLPair lp = lps[j];
       if (!homography(e.R, lp, (float)x, (float)y, h, H)) continue;
-      const float m = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y);
+      const float m = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y, nwin);
       const float ee = P.ncc_norm * m_exp(-m * m * P.inv2ncc);
       if (ee / (ee + 0.5f) < P.q_min) continue;
       if (geo_error(P, e.R, S, pr, x, y, h.w) > P.filter_gmax) continue;
@@ -780,6 +851,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant_
     }
   }
   P.count[base + pix] = (unsigned char)min(count, 255);
+  count_windows(P, nwin);
 }
 
 // Simple kernels: CTA of 32 × 8 threads, tiles flattened like the others.
@@ -974,6 +1046,24 @@ __global__ void k_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const dou
   out[idx] = o;
 }
 
+// FP32 throughput probe: 8 independent FFMA chains per thread, register resident.
+__global__ void __launch_bounds__(256) k_fp32_probe(float* out, int iters, float a, float b) {
+  float v[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) v[k] = (float)(threadIdx.x + k);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+#pragma unroll
+      for (int k = 0; k < 8; ++k) v[k] = fmaf(v[k], a, b);
+    }
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += v[k];
+  if (s == 12345.678f) out[blockIdx.x] = s;  // keeps the loop alive
+}
+
 // ================================================================================ launchers
 #define PS_SPECS(X) X(5, 1) X(6, 1) X(5, 2) X(3, 1)
 
@@ -1003,10 +1093,11 @@ static cudaError_t init_constants() {
   return e;
 }
 
-size_t half_smem(int wr, int ws, bool cw, int maxsrc) {
+size_t half_smem(int wr, int ws, bool cw, int maxsrc, int G) {
   const int wn = (2 * wr) / ws + 1;
-  const int TW = PS_HALF_PW + 2 * wr, TH = PS_HALF_PH + 2 * wr;
-  size_t f = ((TW * TH + 31) & ~31) + (cw ? (size_t)wn * wn * PS_HALF_NT : 0) + (size_t)maxsrc * PS_HALF_NT;
+  const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
+  size_t f = ((TW * TH + 31) & ~31) + (cw ? (size_t)((wn + G - 1) / G) * wn * PS_HALF_NT : 0) +
+             (size_t)maxsrc * PS_HALF_NT;
   return f * sizeof(float);
 }
 size_t eval_smem(int wr, int ws, bool cw) {
@@ -1017,7 +1108,7 @@ size_t eval_smem(int wr, int ws, bool cw) {
 }
 
 // Whether the weight cache fits (<= 200 KB of shared memory per CTA with the largest source count).
-static bool use_cache(int wr, int ws) { return half_smem(wr, ws, true, PS_MAXSRC) <= 200 * 1024; }
+static bool use_cache(int wr, int ws) { return half_smem(wr, ws, true, PS_MAXSRC, 1) <= 200 * 1024; }
 
 template <typename K>
 static cudaError_t launch(K kern, int ncta, int nt, size_t smem, cudaStream_t st, const PsRun& P) {
@@ -1029,17 +1120,30 @@ static cudaError_t launch(K kern, int ncta, int nt, size_t smem, cudaStream_t st
   return cudaGetLastError();
 }
 
-cudaError_t launch_half(const PsRun& P, cudaStream_t st) {
+// Lanes per pixel of the half-step kernel for a tuning word (PS_TUNE_ONE_LANE selects 1, default 2).
+int half_lanes(unsigned tuning) { return (tuning & 0x4u) ? 1 : 2; }
+
+template <int A, int B, int G>
+static cudaError_t launch_half_g(const PsRun& P, bool cw, bool tex, size_t smem, cudaStream_t st) {
+  if (cw) return tex ? launch(k_half<A, B, true, true, G>, P.ntiles, PS_HALF_NT, smem, st, P)
+                     : launch(k_half<A, B, true, false, G>, P.ntiles, PS_HALF_NT, smem, st, P);
+  return tex ? launch(k_half<A, B, false, true, G>, P.ntiles, PS_HALF_NT, smem, st, P)
+             : launch(k_half<A, B, false, false, G>, P.ntiles, PS_HALF_NT, smem, st, P);
+}
+
+cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st) {
   cudaError_t e = init_constants();
   if (e != cudaSuccess) return e;
-  const bool cw = use_cache(P.wr, P.ws);
-  const size_t smem = half_smem(P.wr, P.ws, cw, P.maxsrc);
-#define PS_CASE(a, b) \
-  if (P.wr == a && P.ws == b) return launch(k_half<a, b, true>, P.ntiles, PS_HALF_NT, smem, st, P);
+  const bool cw = use_cache(P.wr, P.ws) && !(tuning & 0x1u);
+  const bool tex = (tuning & 0x2u) != 0;
+  const int G = half_lanes(tuning);
+  const size_t smem = half_smem(P.wr, P.ws, cw, P.maxsrc, G);
+#define PS_CASE(a, b)                                                                \
+  if (P.wr == a && P.ws == b)                                                        \
+    return G == 2 ? launch_half_g<a, b, 2>(P, cw, tex, smem, st) : launch_half_g<a, b, 1>(P, cw, tex, smem, st);
   PS_SPECS(PS_CASE)
 #undef PS_CASE
-  if (cw) return launch(k_half<0, 1, true>, P.ntiles, PS_HALF_NT, smem, st, P);
-  return launch(k_half<0, 1, false>, P.ntiles, PS_HALF_NT, smem, st, P);
+  return G == 2 ? launch_half_g<0, 1, 2>(P, cw, tex, smem, st) : launch_half_g<0, 1, 1>(P, cw, tex, smem, st);
 }
 
 cudaError_t launch_eval(const PsRun& P, cudaStream_t st) {
@@ -1082,6 +1186,10 @@ cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st) {
 cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st) {
   if (P.ntiles <= 0) return cudaSuccess;
   k_readout<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, out);
+  return cudaGetLastError();
+}
+cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st) {
+  k_fp32_probe<<<blocks, 256, 0, st>>>(out, iters, 0.999999f, 1e-7f);
   return cudaGetLastError();
 }
 cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64, const int* has64,

@@ -25,13 +25,15 @@
 
 #define PS_DECLARE_LAUNCHERS(NS)                                                                           \
   namespace NS {                                                                                           \
-  cudaError_t launch_half(const PsRun& P, cudaStream_t st);                                                \
+  cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st);                               \
+  int half_lanes(unsigned tuning);                                                                         \
   cudaError_t launch_eval(const PsRun& P, cudaStream_t st);                                                \
   cudaError_t launch_filter(const PsRun& P, cudaStream_t st);                                              \
   cudaError_t launch_upsample(const PsRun& P, cudaStream_t st);                                            \
   cudaError_t launch_median(const PsRun& P, cudaStream_t st);                                              \
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
   cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
+  cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
                                   const int* has64, PsLPair* out, int nviews, int nlevels, cudaStream_t st); \
   }
@@ -41,20 +43,21 @@ PS_DECLARE_LAUNCHERS(ps_fast)
 namespace {
 
 struct Launchers {
-  cudaError_t (*half)(const PsRun&, cudaStream_t);
+  cudaError_t (*half)(const PsRun&, unsigned, cudaStream_t);
   cudaError_t (*eval)(const PsRun&, cudaStream_t);
   cudaError_t (*filter)(const PsRun&, cudaStream_t);
   cudaError_t (*upsample)(const PsRun&, cudaStream_t);
   cudaError_t (*median)(const PsRun&, cudaStream_t);
   cudaError_t (*snapshot)(const PsRun&, float*, cudaStream_t);
   cudaError_t (*readout)(const PsRun&, float4*, cudaStream_t);
+  int (*half_lanes)(unsigned);
 };
 const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
                            ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
-                           ps_parity::launch_readout};
+                           ps_parity::launch_readout,  ps_parity::half_lanes};
 const Launchers kFast = {ps_fast::launch_half,     ps_fast::launch_eval,   ps_fast::launch_filter,
                          ps_fast::launch_upsample, ps_fast::launch_median, ps_fast::launch_snapshot,
-                         ps_fast::launch_readout};
+                         ps_fast::launch_readout,  ps_fast::half_lanes};
 
 struct PsError {
   int code;
@@ -122,6 +125,19 @@ struct ps_session {
   size_t pin_cap = 0;
   uint64_t launches = 0;
   size_t img_bytes = 0;
+  std::vector<cudaArray_t> arrays;       // texture arrays (PS_TUNE_TEX_GATHER)
+  std::vector<cudaTextureObject_t> texs;
+  unsigned tuning = 0;
+  // profiling
+  bool profiling = false;
+  unsigned long long* counters = nullptr;  // NCC windows per kernel kind (device)
+  struct Pending {
+    int kind;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  double kind_ms[PS_KERNEL_KINDS] = {0, 0, 0, 0};
+  uint64_t kind_launches[PS_KERNEL_KINDS] = {0, 0, 0, 0};
 
   int W(int v, int l) const { return w[v * nl + l]; }
   int H(int v, int l) const { return h[v * nl + l]; }
@@ -299,6 +315,39 @@ void launched(ps_session* s, cudaError_t e, const char* what) {
   s->launches++;
 }
 
+// Brackets one launch with CUDA events (profiling on) and points the NCC-window counter at its kind.
+template <typename F>
+void timed_launch(ps_session* s, int kind, PsRun& P, F&& f, const char* what) {
+  if (!s->profiling) {
+    P.ncc_count = nullptr;
+    launched(s, f(P), what);
+    return;
+  }
+  P.ncc_count = s->counters + kind;
+  ps_session::Pending pd;
+  pd.kind = kind;
+  cuda_ok(cudaEventCreate(&pd.a), "cudaEventCreate");
+  cuda_ok(cudaEventCreate(&pd.b), "cudaEventCreate");
+  cuda_ok(cudaEventRecord(pd.a, s->st), "cudaEventRecord");
+  launched(s, f(P), what);
+  cuda_ok(cudaEventRecord(pd.b, s->st), "cudaEventRecord");
+  s->pending.push_back(pd);
+  s->kind_launches[kind]++;
+}
+
+void collect_events(ps_session* s) {
+  if (s->pending.empty()) return;
+  cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize");
+  for (auto& pd : s->pending) {
+    float ms = 0.f;
+    cuda_ok(cudaEventElapsedTime(&ms, pd.a, pd.b), "cudaEventElapsedTime");
+    s->kind_ms[pd.kind] += ms;
+    cudaEventDestroy(pd.a);
+    cudaEventDestroy(pd.b);
+  }
+  s->pending.clear();
+}
+
 void sync(ps_session* s) { cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize"); }
 
 // ---- state packing (host) -------------------------------------------------------------------------------------
@@ -446,15 +495,17 @@ void run_batch(ps_session* s, const uint32_t* views, size_t a, size_t b, const p
   P.use_prior = use_prior ? 1 : 0;
   P.mode = 1;
   set_items(s, P, views, a, b, (int)p->level, PS_EVAL_PW, PS_EVAL_PH);
-  launched(s, s->L->eval(P, s->st), "evaluate kernel");
+  timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
   PsRun H = P;
-  set_items(s, H, views, a, b, (int)p->level, PS_HALF_PW, PS_HALF_PH);
+  set_items(s, H, views, a, b, (int)p->level, s->L->half_lanes(s->tuning) == 2 ? PS_HALF2_PW : PS_HALF_PW,
+            PS_HALF_PH);
   for (uint32_t t = 0; t < p->iterations; ++t) {
     H.t = (int)t;
     ps_iter_consts(&s->pm, P.geometric, (int)t, &H.tau_good, &H.eps, &H.phi);
     for (int color = 0; color < 2; ++color) {
       H.color = color;
-      launched(s, s->L->half(H, s->st), "half-step kernel");
+      timed_launch(s, PS_KERNEL_HALF, H, [&](const PsRun& q) { return s->L->half(q, s->tuning, s->st); },
+                   "half-step kernel");
     }
   }
 }
@@ -501,7 +552,7 @@ int ps_backend_create(int device, const ps_options* opts, ps_backend** out) {
   be->device = device;
   ps_options_default(&be->opts);
   if (opts) be->opts = *opts;
-  if (be->opts.math_mode > PS_MATH_FAST || be->opts.checked) {
+  if (be->opts.math_mode > PS_MATH_FAST || be->opts.checked || (be->opts.tuning & ~PS_TUNE_VALID_MASK)) {
     delete be;
     return PS_EINVAL;
   }
@@ -548,6 +599,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     s->seed = in->seed;
     s->cs = ps_session_consts(&s->pm, &s->fl);
     s->L = be->opts.math_mode == PS_MATH_FAST ? &kFast : &kParity;
+    s->tuning = be->opts.tuning;
     s->w.assign(s->nv * s->nl, 0);
     s->h.assign(s->nv * s->nl, 0);
     s->nsrc.assign(s->nv, 0);
@@ -604,6 +656,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
         }
         PsLevel& L = lvh[v * s->nl + l];
         L.img = s->img + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
+        L.tex = 0;
         L.w = (int)li.width;
         L.h = (int)li.height;
         L.pitch = (int)pitch;
@@ -614,6 +667,36 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
         L.cy = li.k[3];
       }
     cuda_ok(cudaMemcpyAsync(s->img, host.data(), total * sizeof(float), cudaMemcpyHostToDevice, s->st), "upload images");
+    if (s->tuning & PS_TUNE_TEX_GATHER) {
+      // one gather-capable CUDA array + border-addressed point texture per (view, level), filled from the plane
+      const cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+      for (int v = 0; v < s->nv; ++v)
+        for (int l = 0; l < s->nl; ++l) {
+          PsLevel& L = lvh[v * s->nl + l];
+          cudaArray_t arr = nullptr;
+          cuda_ok(cudaMallocArray(&arr, &cd, L.w, L.h, cudaArrayTextureGather), "cudaMallocArray");
+          s->arrays.push_back(arr);
+          cuda_ok(cudaMemcpy2DToArrayAsync(arr, 0, 0, L.img, L.pitch * sizeof(float), L.w * sizeof(float), L.h,
+                                           cudaMemcpyDeviceToDevice, s->st),
+                  "copy texture array");
+          cudaResourceDesc rd;
+          memset(&rd, 0, sizeof rd);
+          rd.resType = cudaResourceTypeArray;
+          rd.res.array.array = arr;
+          cudaTextureDesc td;
+          memset(&td, 0, sizeof td);
+          td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
+          td.filterMode = cudaFilterModePoint;
+          td.readMode = cudaReadModeElementType;
+          td.normalizedCoords = 0;
+          cudaTextureObject_t t = 0;
+          cuda_ok(cudaCreateTextureObject(&t, &rd, &td, nullptr), "cudaCreateTextureObject");
+          s->texs.push_back(t);
+          L.tex = (unsigned long long)t;
+        }
+    }
+    s->counters = dalloc<unsigned long long>(PS_KERNEL_KINDS);
+    cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     s->lv = dalloc<PsLevel>(lvh.size());
     cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
     // pairs, views, FP64 pair tables
@@ -691,6 +774,13 @@ int ps_end(ps_session* s) {
   cudaFree(s->has64);
   cudaFree(s->snap);
   cudaFree(s->snap_off);
+  for (cudaTextureObject_t t : s->texs) cudaDestroyTextureObject(t);
+  for (cudaArray_t a : s->arrays) cudaFreeArray(a);
+  cudaFree(s->counters);
+  for (auto& pd : s->pending) {
+    cudaEventDestroy(pd.a);
+    cudaEventDestroy(pd.b);
+  }
   if (s->pin) cudaFreeHost(s->pin);
   if (s->st) cudaStreamDestroy(s->st);
   cudaGetLastError();
@@ -790,7 +880,7 @@ int ps_evaluate(ps_session* s, uint32_t level, const uint32_t* views, size_t n, 
       P.geometric = geometric ? 1 : 0;
       P.mode = 0;
       set_items(s, P, views, a, b, (int)level, PS_EVAL_PW, PS_EVAL_PH);
-      launched(s, s->L->eval(P, s->st), "evaluate kernel");
+      timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
       for (size_t i = a; i < b; ++i) {
         if (!out_cost[i]) fail(PS_EINVAL, "out_cost entry is NULL");
         cuda_ok(cudaMemcpyAsync(out_cost[i], sl.cost + sl.off[views[i]],
@@ -816,7 +906,7 @@ int ps_filter(ps_session* s, const uint32_t* views, size_t n, const ps_view_stat
       PsRun P = base_params(s, level);
       P.geometric = 1;
       set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
-      launched(s, s->L->filter(P, s->st), "filter kernel");
+      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
       for (size_t i = a; i < b; ++i) {
         if (!out_counts[i]) fail(PS_EINVAL, "out_counts entry is NULL");
         cuda_ok(cudaMemcpyAsync(out_counts[i], sl.count + sl.off[views[i]],
@@ -912,7 +1002,7 @@ int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* 
       PsRun P = base_params(s, level);
       P.geometric = 1;
       set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
-      launched(s, s->L->filter(P, s->st), "filter kernel");
+      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
       if (out_counts) {
         for (size_t i = a; i < b; ++i)
           if (out_counts[i])
@@ -942,6 +1032,76 @@ int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_
 
 int ps_synchronize(ps_session* s) {
   return guard(s, [&] { sync(s); });
+}
+
+void* ps_session_stream(const ps_session* s) { return s ? (void*)s->st : nullptr; }
+
+int ps_set_profiling(ps_session* s, uint32_t enable) {
+  return guard(s, [&] {
+    collect_events(s);
+    s->profiling = enable != 0;
+  });
+}
+
+int ps_kernel_stats(ps_session* s, uint32_t kind, double* total_ms, uint64_t* launches, uint64_t* ncc_windows) {
+  return guard(s, [&] {
+    if (kind >= PS_KERNEL_KINDS) fail(PS_EINVAL, "kernel kind out of range");
+    collect_events(s);
+    unsigned long long c[PS_KERNEL_KINDS];
+    cuda_ok(cudaMemcpyAsync(c, s->counters, sizeof c, cudaMemcpyDeviceToHost, s->st), "read counters");
+    sync(s);
+    if (total_ms) *total_ms = s->kind_ms[kind];
+    if (launches) *launches = s->kind_launches[kind];
+    if (ncc_windows) *ncc_windows = c[kind];
+  });
+}
+
+int ps_reset_stats(ps_session* s) {
+  return guard(s, [&] {
+    collect_events(s);
+    for (int k = 0; k < PS_KERNEL_KINDS; ++k) {
+      s->kind_ms[k] = 0;
+      s->kind_launches[k] = 0;
+    }
+    cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
+    sync(s);
+  });
+}
+
+int ps_measure_fp32_peak(int device, double* tflops) {
+  if (!tflops) return PS_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return PS_ENODEV;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PS_ENODEV;
+  float* out = nullptr;
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) return PS_ECUDA;
+  const int blocks = prop.multiProcessorCount * 8, iters = 2048;
+  int rc = PS_OK;
+  cudaEvent_t a, b;
+  if (cudaMalloc(&out, blocks * sizeof(float)) != cudaSuccess) rc = PS_ENOMEM;
+  if (rc == PS_OK) {
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4 && rc == PS_OK; ++rep) {
+      cudaEventRecord(a, st);
+      if (ps_parity::launch_fp32_probe(out, blocks, iters, st) != cudaSuccess) rc = PS_ECUDA;
+      cudaEventRecord(b, st);
+      if (cudaEventSynchronize(b) != cudaSuccess) rc = PS_ECUDA;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, a, b);
+      if (rep > 0 && ms < best) best = ms;  // first launch is warm-up
+    }
+    const double flop = 2.0 * 8 * 16 * (double)iters * blocks * 256;
+    *tflops = flop / (best * 1e-3) / 1e12;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  cudaFree(out);
+  cudaStreamDestroy(st);
+  cudaGetLastError();
+  return rc;
 }
 
 }  // extern "C"

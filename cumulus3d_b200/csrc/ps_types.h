@@ -12,6 +12,7 @@
 // Half-step CTA: 128 threads, 4 warps; a warp covers 16 active columns × 2 rows of a 32 × 8 pixel tile.
 #define PS_HALF_NT 128
 #define PS_HALF_PW 32
+#define PS_HALF2_PW 16  // two lanes per pixel: a warp = 8 active columns × 2 rows × 2 lanes
 #define PS_HALF_PH 8
 // Evaluate / filter CTA: 128 threads covering 32 × 4 pixels (a warp is one row).
 #define PS_EVAL_NT 128
@@ -23,8 +24,9 @@
 
 // One (view, level) image plane.
 struct PsLevel {
-  const float* img;  // pixel (0,0) of a plane with PS_BORDER zero rows/columns on every side
-  int w, h, pitch;   // pitch in floats
+  const float* img;    // pixel (0,0) of a plane with PS_BORDER zero rows/columns on every side
+  unsigned long long tex;  // border-addressed point texture of the same plane (cudaTextureObject_t), 0 if not built
+  int w, h, pitch;         // pitch in floats
   int pad;
   float fx, fy, cx, cy;
 };
@@ -85,5 +87,6 @@ struct PsRun {
   float up_inv2s, up_inv2c;  // joint bilateral upsampling constants
   int need_min;              // readout threshold: min_num_consistent
   int mode;                  // evaluate: 1 = run start (init + cost + clear best view), 0 = cost only
+  unsigned long long* ncc_count;  // when set, kernels add the number of NCC window evaluations they performed
   PsItem items[PS_MAX_ITEMS];
 };

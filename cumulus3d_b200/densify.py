@@ -1,0 +1,197 @@
+"""Depth-map driver over a PatchMatch session: the schedule of ``compute_depth_maps``
+(crates/dense/src/densify.rs:212-498) for callers of this engine.
+
+* :func:`compute_depth_maps` — the reference's multi-scale flow through the host-state session API (run at the coarsest
+  level from random init; per finer level: upsample → evaluate → restorer run → evaluate → per-pixel restorer choice;
+  geometric rounds against snapshots; final median filter / filter / readout threshold).
+* :func:`schedule_resident` — the same single-level schedule entirely on the device (states, snapshots, filter and
+  readout stay in HBM), used by the benchmark's device-resident leg.
+* :func:`build_pyramid`, :func:`num_levels`, :func:`readout` — host helpers restating upsample.rs:35-102 and
+  densify.rs:441-454.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from .patchstereo import DepthSnapshot, KernelInput, LevelImage, PatchMatchSession, RunParams, ViewState
+
+
+@dataclass
+class Schedule:
+    """LevelSchedule (crates/dense/src/params.rs:62-73) plus the multi-scale constants of DensifyOptions."""
+    photometric_iters: int = 6
+    restorer_random_init: bool = False
+    geometric_rounds: int = 2
+    geometric_iters: int = 2
+    photometric_iters_upper: int = 3  # fast profile: 6 at level 0, 3 above (params.rs:496-503)
+    jbu_sigma_spatial: float = 1.0
+    jbu_sigma_color: float = 0.04
+    restorer_threshold: float = 0.1
+
+    def at(self, level: int) -> "Schedule":
+        s = Schedule(**self.__dict__)
+        if level > 0:
+            s.photometric_iters = self.photometric_iters_upper
+        return s
+
+
+def num_levels(min_side: int, max_levels: int, min_size: int) -> int:
+    """upsample.rs:35-44."""
+    l, s = 1, min_side
+    while l < max_levels and s // 2 >= min_size:
+        s //= 2
+        l += 1
+    return l
+
+
+def build_pyramid(gray: np.ndarray, k: Sequence[float], levels: int) -> List[LevelImage]:
+    """u8 pyramid (upsample.rs:46-102): separable 3-tap Gaussian (σ = 0.5, clamped borders), 2×2 average, rounding
+    to u8; f ← f/2, c ← (c + 0.5)/2 − 0.5.  Returns level 0 = coarsest."""
+    g0 = np.float32(np.exp(np.float32(-1.0) / np.float32(2.0 * 0.25)))
+    g = np.array([g0, 1.0, g0], np.float32)
+    g = g / g.sum(dtype=np.float32)
+    out = [LevelImage(np.ascontiguousarray(gray), tuple(float(x) for x in k))]
+    cur = gray.astype(np.float32)
+    kk = [float(x) for x in k]
+    for _ in range(1, levels):
+        h, w = cur.shape
+        xp = np.pad(cur, ((0, 0), (1, 1)), mode="edge")
+        tmp = g[0] * xp[:, :-2] + g[1] * xp[:, 1:-1] + g[2] * xp[:, 2:]
+        yp = np.pad(tmp, ((1, 1), (0, 0)), mode="edge")
+        b = g[0] * yp[:-2] + g[1] * yp[1:-1] + g[2] * yp[2:]
+        nh, nw = h // 2, w // 2
+        b = b[: 2 * nh, : 2 * nw]
+        nxt = np.float32(0.25) * (b[0::2, 0::2] + b[0::2, 1::2] + b[1::2, 0::2] + b[1::2, 1::2])
+        q = np.clip(np.round(nxt), 0, 255).astype(np.uint8)
+        kk = [kk[0] * 0.5, kk[1] * 0.5, (kk[2] + 0.5) * 0.5 - 0.5, (kk[3] + 0.5) * 0.5 - 0.5]
+        out.append(LevelImage(q, tuple(kk)))
+        cur = q.astype(np.float32)
+    out.reverse()
+    return out
+
+
+def readout(states: Sequence[ViewState], counts: Sequence[np.ndarray], nsrc: Sequence[int],
+            min_num_consistent: int) -> List[ViewState]:
+    """Readout threshold (densify.rs:441-454): depth/normal zeroed where count < max(1, min(min_num_consistent, nsrc))."""
+    out = []
+    for s, c, n in zip(states, counts, nsrc):
+        need = max(1, min(min_num_consistent, n))
+        keep = (s.depth > 0) & (c >= need)
+        r = s.copy()
+        r.depth[~keep] = 0.0
+        r.normal[~keep] = 0.0
+        out.append(r)
+    return out
+
+
+def compute_depth_maps(session: PatchMatchSession, inp: KernelInput, views: Sequence[int],
+                       sch: Schedule = Schedule(), weak_texture_prior: bool = False):
+    """The multi-scale schedule of compute_depth_maps (densify.rs:350-454) for `views`.  Returns (raw states at the
+    top level, filtered states, filter counts)."""
+    nl = inp.num_levels
+    top = nl - 1
+    run_id = 0
+    snap_id = 0
+
+    def next_run():
+        nonlocal run_id
+        run_id += 1
+        return run_id
+
+    def snapshot(level, states):
+        nonlocal snap_id
+        snap_id += 1
+        maps: List[Optional[np.ndarray]] = [None] * len(inp.views)
+        for v, s in zip(views, states):
+            maps[v] = s.depth.copy()
+        return DepthSnapshot(snap_id, level, maps)
+
+    def size(v, l):
+        li = inp.views[v].levels[l]
+        return li.width, li.height
+
+    states: List[ViewState] = []
+    for level in range(nl):
+        s = sch.at(level)
+        use_prior = level > 0 and inp.pm.weak_texture_var > 0.0 and weak_texture_prior
+        if level == 0:
+            states = [ViewState.new(*size(v, 0)) for v in views]
+            session.run(views, states, RunParams(level, False, True, s.photometric_iters, next_run(), False))
+        else:
+            up = session.upsample(inp, level, views, states, s.jbu_sigma_spatial, s.jbu_sigma_color)
+            if use_prior:
+                for u in up:
+                    u.prior = np.ascontiguousarray(u.planes())
+            c_init = session.evaluate(level, views, up, False, None)
+            if s.restorer_random_init:
+                photo = [ViewState.new(u.width, u.height) for u in up]
+                for p, u in zip(photo, up):
+                    p.prior = u.prior
+            else:
+                photo = [u.copy() for u in up]
+            session.run(views, photo, RunParams(level, False, s.restorer_random_init, s.photometric_iters, next_run(),
+                                                use_prior))
+            c_photo = session.evaluate(level, views, photo, False, None)
+            new = []
+            for u, ph, ci, cp in zip(up, photo, c_init, c_photo):
+                take = (u.depth <= 0.0) | ((ci - cp) > s.restorer_threshold)
+                u.depth[take] = ph.depth[take]
+                u.normal[take] = ph.normal[take]
+                new.append(u)
+            states = new
+        for _ in range(s.geometric_rounds):
+            snap = snapshot(level, states)
+            session.run(views, states, RunParams(level, True, False, s.geometric_iters, next_run(), use_prior), snap)
+    for st in states:
+        st.prior = None
+    if inp.filter.median_filter:
+        states = session.median_filter(inp, top, views, states)
+    snap = snapshot(top, states)
+    counts = session.filter(views, states, snap)
+    nsrc = [len(inp.views[v].sources) for v in views]
+    return states, readout(states, counts, nsrc, inp.filter.min_num_consistent), counts
+
+
+def schedule_host(session: PatchMatchSession, inp: KernelInput, views: Sequence[int], photometric_iters: int,
+                  geometric_rounds: int, geometric_iters: int):
+    """Single-level schedule through the host-state API (every call copies states in and out, as the reference's
+    session does).  Returns (raw states, filtered states, counts)."""
+    level = 0
+    states = [ViewState.new(inp.views[v].levels[0].width, inp.views[v].levels[0].height) for v in views]
+    run_id = 1
+    session.run(views, states, RunParams(level, False, True, photometric_iters, run_id))
+    snap_id = 0
+    for _ in range(geometric_rounds):
+        snap_id += 1
+        run_id += 1
+        maps: List[Optional[np.ndarray]] = [None] * len(inp.views)
+        for v, s in zip(views, states):
+            maps[v] = s.depth
+        session.run(views, states, RunParams(level, True, False, geometric_iters, run_id),
+                    DepthSnapshot(snap_id, level, maps))
+    snap_id += 1
+    maps = [None] * len(inp.views)
+    for v, s in zip(views, states):
+        maps[v] = s.depth
+    counts = session.filter(views, states, DepthSnapshot(snap_id, level, maps))
+    nsrc = [len(inp.views[v].sources) for v in views]
+    return states, readout(states, counts, nsrc, inp.filter.min_num_consistent), counts
+
+
+def schedule_resident(session: PatchMatchSession, views: Sequence[int], photometric_iters: int, geometric_rounds: int,
+                      geometric_iters: int, level: int = 0, snap_base: int = 1_000_000) -> None:
+    """Single-level schedule with every state on the device: photometric run from random init, geometric rounds against
+    device-captured snapshots, filter, readout threshold.  Results stay resident (download with session.download /
+    readout_resident)."""
+    run_id = 1
+    session.run_resident(views, RunParams(level, False, True, photometric_iters, run_id))
+    for r in range(geometric_rounds):
+        run_id += 1
+        session.snapshot_capture(level, views, snap_base + 2 * r)
+        session.run_resident(views, RunParams(level, True, False, geometric_iters, run_id))
+    session.snapshot_capture(level, views, snap_base + 2 * geometric_rounds + 1)
+    session.filter_resident(views, download=False)
+    session.readout_resident(views, download=False)

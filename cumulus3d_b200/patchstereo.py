@@ -207,16 +207,28 @@ def _views(views: Sequence[int]):
     return (C.c_uint32 * max(len(views), 1))(*views)
 
 
+def measure_fp32_peak(device: int = 0) -> float:
+    """Measured FP32 FFMA throughput of the device in TFLOP/s."""
+    t = C.c_double()
+    rc = _lib.engine().ps_measure_fp32_peak(device, C.byref(t))
+    if rc != _lib.PS_OK:
+        raise PsError(rc, "fp32 probe failed")
+    return t.value
+
+
 class PatchMatchBackend:
     """CudaPatchMatch equivalent (crates/cuda/src/patchmatch.rs:91-298) on one B200."""
 
-    def __init__(self, device: int = 0, math: str = "parity", max_batch: int = 64, batch_pixels: int = 0):
+    def __init__(self, device: int = 0, math: str = "parity", max_batch: int = 64, batch_pixels: int = 0,
+                 tuning: int = 0):
         self.lib = _lib.engine()
         o = _lib.Options()
         self.lib.ps_options_default(C.byref(o))
         o.math_mode = {"parity": _lib.PS_MATH_PARITY, "fast": _lib.PS_MATH_FAST}[math]
         o.max_batch = max_batch
         o.batch_pixels = batch_pixels
+        o.tuning = tuning
+        self.device = device
         h = C.c_void_p()
         rc = self.lib.ps_backend_create(device, C.byref(o), C.byref(h))
         if rc != _lib.PS_OK:
@@ -354,6 +366,20 @@ class PatchMatchSession:
 
     def launch_count(self) -> int:
         return int(self.lib.ps_launch_count(self.h))
+
+    def stream(self) -> int:
+        return int(self.lib.ps_session_stream(self.h) or 0)
+
+    def set_profiling(self, on: bool = True) -> None:
+        self._check(self.lib.ps_set_profiling(self.h, int(on)))
+
+    def kernel_stats(self, kind: int) -> dict:
+        ms, n, w = C.c_double(), C.c_uint64(), C.c_uint64()
+        self._check(self.lib.ps_kernel_stats(self.h, kind, C.byref(ms), C.byref(n), C.byref(w)))
+        return {"ms": ms.value, "launches": n.value, "ncc_windows": w.value}
+
+    def reset_stats(self) -> None:
+        self._check(self.lib.ps_reset_stats(self.h))
 
     def close(self) -> None:
         if self.h:

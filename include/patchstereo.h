@@ -65,8 +65,14 @@ typedef struct ps_options {
   uint32_t max_batch;    /* views per launch; 0 = 64 (reference default) */
   uint64_t batch_pixels; /* pixel budget per launch; 0 = unbounded (HBM holds every view of a job) */
   uint32_t checked;      /* reserved (bounds-checked build); must be 0 */
-  uint32_t reserved;
+  uint32_t tuning;       /* half-step kernel variant, PS_TUNE_* flags; 0 = defaults (the autotuner sets these) */
 } ps_options;
+
+/* Half-step kernel variants (same results bit for bit; only speed differs). */
+#define PS_TUNE_NO_WEIGHT_CACHE 0x1u /* recompute window weights per tap (more CTAs per SM, more exp work) */
+#define PS_TUNE_TEX_GATHER 0x2u      /* fetch each bilinear 2×2 footprint with one texture gather (same bits) */
+#define PS_TUNE_ONE_LANE 0x4u        /* one thread per pixel (default: two lanes per pixel split the window rows) */
+#define PS_TUNE_VALID_MASK 0x7u
 
 /* PmParams (crates/dense/src/params.rs:76-124, defaults :126-154). */
 typedef struct ps_pm_params {
@@ -238,6 +244,24 @@ int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_
 int ps_synchronize(ps_session* s);
 /* Number of kernel launches this session issued so far (for launch accounting). */
 uint64_t ps_launch_count(const ps_session* s);
+/* The session's CUDA stream (a cudaStream_t), for callers that record their own events on it. */
+void* ps_session_stream(const ps_session* s);
+
+/* ---- measurement (no reference counterpart; replaces CUMULUS3D_CUDA_TRACE, crates/cuda/src/patchmatch.rs:780-797) */
+typedef enum ps_kernel_kind {
+  PS_KERNEL_HALF = 0,
+  PS_KERNEL_EVAL = 1,
+  PS_KERNEL_FILTER = 2,
+  PS_KERNEL_OTHER = 3,
+  PS_KERNEL_KINDS = 4
+} ps_kernel_kind;
+/* With profiling on, every launch is bracketed by CUDA events on the session stream and half-step / evaluate /
+ * filter launches count the NCC window evaluations they perform (each is (2R/step+1)^2 taps). */
+int ps_set_profiling(ps_session* s, uint32_t enable);
+int ps_kernel_stats(ps_session* s, uint32_t kind, double* total_ms, uint64_t* launches, uint64_t* ncc_windows);
+int ps_reset_stats(ps_session* s);
+/* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 FLOP) from a register-resident FFMA loop. */
+int ps_measure_fp32_peak(int device, double* tflops);
 
 #ifdef __cplusplus
 }

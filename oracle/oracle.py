@@ -34,6 +34,8 @@ def lib() -> C.CDLL:
         o = C.CDLL(str(PATH))
         sig = {
             "oracle_run": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP, C.c_int]),
+            "oracle_run_rows": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP, C.c_int,
+                                          C.c_int, C.c_int]),
             "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int]),
             "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
@@ -78,12 +80,14 @@ def _chk(rc: int, what: str):
 
 
 def run(inp: KernelInput, views: Sequence[int], states: List[ViewState], p: RunParams,
-        snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None) -> None:
-    """PatchMatchSession::run restated on the CPU (states updated in place)."""
+        snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None, rows=None) -> None:
+    """PatchMatchSession::run restated on the CPU (states updated in place).  `rows` = (y0, y1) restricts the
+    work to a band of rows (timing samples only)."""
     ci, keep = CInput(inp), []
     rp = p.c()
-    _chk(lib().oracle_run(C.byref(ci.c), _views(views), len(views), c_states(states, keep), C.byref(rp),
-                          c_snapshot(snapshot, keep), _threads(threads)), "run")
+    y0, y1 = rows if rows is not None else (0, 0)
+    _chk(lib().oracle_run_rows(C.byref(ci.c), _views(views), len(views), c_states(states, keep), C.byref(rp),
+                               c_snapshot(snapshot, keep), _threads(threads), y0, y1), "run")
 
 
 def evaluate(inp: KernelInput, level: int, views: Sequence[int], states: List[ViewState], geometric: bool = False,

@@ -21,7 +21,9 @@
 // as follows, identically in the engine: bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
 // fma(ay, bot-top, top) on values already divided by 255; tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
 // the two numerators); window accumulation Ss += w·s, SSs = fma(w·s, s, SSs), IS = fma(w·s, Ik, IS); reference
-// statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); rsqrt(a) = 1/sqrt(a); ρ = cov / sqrt(var_r·var_s).
+// statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); every window sum (W, S, SS, Ss, SSs, IS) is kept as two partial
+// sums by row parity — even rows and odd rows, each in ascending row and column order — and the total is
+// even + odd; rsqrt(a) = 1/sqrt(a); ρ = cov / sqrt(var_r·var_s).
 //
 // Mode "f64" re-evaluates costs of given hypotheses with every step in binary64 (exp, sqrt, division exact to
 // double rounding) and the homography built from FP64 geometry — the FP64 CPU re-evaluation of the precision rule.
@@ -236,29 +238,32 @@ T sample(const Img& S, T u, T v) {
   return fm(ay, bot - top, top);
 }
 
-// ref_stats (patchmatch.cu:199-223).
+// ref_stats (patchmatch.cu:199-223), window sums split by row parity (even rows and odd rows accumulate
+// separately in ascending row order; total = even + odd).
 template <class T>
 RS<T> ref_stats(const Scene& sc, const Img& R, int x, int y) {
   RS<T> s;
   s.ic = (T)R.at(x, y);
-  T W = 0, S = 0, SS = 0;
+  T W[2] = {0, 0}, S[2] = {0, 0}, SS[2] = {0, 0};
   const T inv2s = (T)sc.cs.inv2s, inv2c = (T)sc.cs.inv2c;
   for (int a = 0; a < sc.wn; ++a) {
     int dy = -sc.wr + a * sc.ws;
+    const int p = a & 1;
     for (int b = 0; b < sc.wn; ++b) {
       int dx = -sc.wr + b * sc.ws;
       T ik = (T)R.at(x + dx, y + dy);
       T d = s.ic - ik;
       T w = ex(-(T)(dx * dx + dy * dy) * inv2s - d * d * inv2c);
       T wi = w * ik;
-      W = W + w;
-      S = S + wi;
-      SS = fm(wi, ik, SS);
+      W[p] = W[p] + w;
+      S[p] = S[p] + wi;
+      SS[p] = fm(wi, ik, SS[p]);
     }
   }
-  s.W = W;
-  s.mu = S / W;
-  s.var = SS / W - s.mu * s.mu;
+  s.W = W[0] + W[1];
+  const T St = S[0] + S[1], SSt = SS[0] + SS[1];
+  s.mu = St / s.W;
+  s.var = SSt / s.W - s.mu * s.mu;
   return s;
 }
 
@@ -294,9 +299,10 @@ T ncc_cost(const Scene& sc, const Img& R, const RS<T>& rs, const Img& S, const T
   if (!(u >= 0 && v >= 0 && u <= (T)S.w - (T)1 && v <= (T)S.h - (T)1)) return 2;
   if (rs.var < (T)1e-5f) return 2;
   const T inv2s = (T)sc.cs.inv2s, inv2c = (T)sc.cs.inv2c;
-  T Ss = 0, SSs = 0, IS = 0;
+  T Ss[2] = {0, 0}, SSs[2] = {0, 0}, IS[2] = {0, 0};
   for (int a = 0; a < sc.wn; ++a) {
     int dy = -sc.wr + a * sc.ws;
+    const int p = a & 1;
     T sy = fy + (T)dy;
     for (int b = 0; b < sc.wn; ++b) {
       int dx = -sc.wr + b * sc.ws;
@@ -311,16 +317,17 @@ T ncc_cost(const Scene& sc, const Img& R, const RS<T>& rs, const Img& S, const T
         sv = sample<T>(S, fm(H[0], sx, fm(H[1], sy, H[2])) * izz, fm(H[3], sx, fm(H[4], sy, H[5])) * izz);
       }
       T wsv = w * sv;
-      Ss = Ss + wsv;
-      SSs = fm(wsv, sv, SSs);
-      IS = fm(wsv, ik, IS);
+      Ss[p] = Ss[p] + wsv;
+      SSs[p] = fm(wsv, sv, SSs[p]);
+      IS[p] = fm(wsv, ik, IS[p]);
     }
   }
+  const T Sst = Ss[0] + Ss[1], SSst = SSs[0] + SSs[1], ISt = IS[0] + IS[1];
   T iW = (T)1 / rs.W;
-  T mus = Ss * iW;
-  T vars = SSs * iW - mus * mus;
+  T mus = Sst * iW;
+  T vars = SSst * iW - mus * mus;
   if (vars < (T)1e-5f) return 2;
-  T cov = IS * iW - rs.mu * mus;
+  T cov = ISt * iW - rs.mu * mus;
   T c = (T)1 - cov / sq(rs.var * vars);
   return mn(mx(c, (T)0), (T)2);
 }
@@ -755,8 +762,10 @@ extern "C" {
 
 // PatchMatchSession::run restated (crates/cuda/src/patchmatch.rs:752-799): per view, run start (evaluate mode 1)
 // then `iterations` × (colour 0, colour 1) half steps.
-int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
-               const ps_run_params* p, const ps_depth_snapshot* snap, int threads) {
+// Rows [y0, y1) only (y1 <= 0: all rows): the timing sample of the CPU baseline runs a band of rows, whose cost is
+// proportional to its pixel count; parity tests always run every row.
+int oracle_run_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
+                    const ps_run_params* p, const ps_depth_snapshot* snap, int threads, int y0, int y1) {
   Scene sc;
   if (!load_scene(in, sc) || !p) return PS_EINVAL;
   if (p->geometric && !snap) return PS_EINVAL;
@@ -777,8 +786,9 @@ int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_vi
     r.t = 0;
     r.color = 0;
     r.tau_good = r.eps = r.phi = 0;
+    const int ya = std::max(y0, 0), yb = y1 > 0 ? std::min(y1, st.h) : st.h;
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int y = 0; y < st.h; ++y)
+    for (int y = ya; y < yb; ++y)
       for (int x = 0; x < st.w; ++x) eval_pixel(r, st, x, y, 1, p->random_init);
     for (uint32_t t = 0; t < p->iterations; ++t) {
       r.t = (int)t;
@@ -786,13 +796,18 @@ int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_vi
       for (int color = 0; color < 2; ++color) {
         r.color = color;
 #pragma omp parallel for schedule(dynamic, 1)
-        for (int y = 0; y < st.h; ++y)
+        for (int y = ya; y < yb; ++y)
           for (int x = ((y + color) & 1); x < st.w; x += 2) half_pixel(r, st, x, y);
       }
     }
     from_state(st, states[i]);
   }
   return PS_OK;
+}
+
+int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
+               const ps_run_params* p, const ps_depth_snapshot* snap, int threads) {
+  return oracle_run_rows(in, views, n, states, p, snap, threads, 0, 0);
 }
 
 int oracle_evaluate(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,

@@ -139,3 +139,19 @@ def test_bit_reproducible(backend):
         s.run(wl.views, b, p)
     for x, y in zip(a, b):
         _assert_same(x, y, "rerun")
+
+
+@pytest.mark.parametrize("tuning", [1, 2, 3, 4, 5, 6, 7])
+def test_half_step_variants_bitwise_equal(tuning):
+    """Every half-step kernel variant (weight cache off, texture gather, one lane per pixel) gives the oracle's bits."""
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    wl = scenes.workload_small(72, 56, window_radius=6, seed=13)
+    p = RunParams(0, False, True, 2, 1)
+    gpu, cpu = _states(wl), _states(wl)
+    be = PatchMatchBackend(0, math="parity", tuning=tuning)
+    with be.begin(wl.input) as s:
+        s.run(wl.views, gpu, p)
+    be.close()
+    oracle.run(wl.input, wl.views, cpu, p)
+    for i in range(len(gpu)):
+        _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning}")

@@ -125,6 +125,11 @@ def bench_ours(args, rank, world, local):
     wl = scenes.workload_c2(seed=2 + (0 if shard_job else rank), with_gt=False, views=args.views)
     mine = shard(len(wl.cams), rank, world) if shard_job else list(range(len(wl.cams)))
     wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
+    tuned = None
+    if args.tuning < 0:  # autotune the half-step variant on a prefix of this job's views (outside the timed region)
+        from cumulus3d_b200.autotune import tune
+        tuned = tune(wl.input, local, args.math, views=mine)
+        args.tuning = tuned["tuning"]
     be = PatchMatchBackend(local, math=args.math, tuning=args.tuning)
     fp32_peak = measure_fp32_peak(local)
     sess = be.begin(wl.input)
@@ -199,6 +204,7 @@ def bench_ours(args, rank, world, local):
         "config": {"workload": wl.name, "views": views_total, "width": 1920, "height": 1080, "window": f"{wn}x{wn}",
                    "sources": 4, "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x"
                    f"{wl.geometric_iters} geometric", "math": args.math, "tuning": args.tuning,
+                   "autotune": None if tuned is None else {"half_ms": tuned["ms"], "cached": tuned["cached"]},
                    "l2": "inputs larger than L2 (24 f32 images + 1.2 GB of resident per-pixel state)",
                    "parallelism": (f"one job's views sharded over {world} ranks" if shard_job else
                                    f"{world} independent job(s), one per GPU")},
@@ -342,7 +348,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--math", default="parity", choices=["parity", "fast"])
-    ap.add_argument("--tuning", type=int, default=0)
+    ap.add_argument("--tuning", type=int, default=-1, help="half-step variant (PS_TUNE_* flags); -1 = autotune")
     ap.add_argument("--shard-job", action="store_true", help="shard one job's views over the ranks (strong scaling)")
     ap.add_argument("--views", type=int, default=None,
                     help="first N views of the workload only (small profiling cases, not a bench line)")

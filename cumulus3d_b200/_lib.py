@@ -108,6 +108,8 @@ SIGNATURES = {
     "ps_state_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_run_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(RunParams)]),
     "ps_snapshot_capture": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.c_uint64, C.c_uint32]),
+    "ps_snapshot_buffer": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_void_p), C.POINTER(C.c_uint64)]),
+    "ps_snapshot_mark": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.c_uint64]),
     "ps_filter_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_uint8))]),
     "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_synchronize": (C.c_int, [_P]),

@@ -1,0 +1,76 @@
+"""Autotuner for the half-step kernel variant.
+
+All variants of the half-step kernel produce the same bits, so the choice only affects speed:
+
+* lanes per pixel: one thread per pixel, or two lanes that split the window rows;
+* window-weight cache: on or off;
+* source sampling: loads from the bordered plane, or a texture gather.
+
+The tuner times each candidate on a prefix of the caller's own views (a photometric run of one red-black iteration,
+kernel time from the session's CUDA events) and returns the fastest tuning word.  Results are cached in a JSON file
+keyed by (GPU name, window radius, window step, math mode, image size class).
+"""
+from __future__ import annotations
+
+import json
+import os
+import pathlib
+from typing import Dict, Optional, Sequence
+
+from . import _lib
+from .patchstereo import KernelInput, PatchMatchBackend, RunParams
+
+CANDIDATES = (0, 2, 3, 4, 6, 7)  # see PS_TUNE_* in include/patchstereo.h
+DEFAULT_CACHE = pathlib.Path(os.environ.get("PS_AUTOTUNE_CACHE",
+                                            pathlib.Path(__file__).resolve().parent / "_autotune_cache.json"))
+
+
+def _key(gpu: str, inp: KernelInput, math: str) -> str:
+    lv = inp.views[0].levels[-1]
+    mp = lv.width * lv.height / 1e6
+    size = "S" if mp < 0.5 else ("M" if mp < 4 else "L")
+    return f"{gpu}|r{inp.pm.window_radius}|s{inp.pm.window_step}|{math}|{size}"
+
+
+def _load(path: pathlib.Path) -> Dict[str, dict]:
+    try:
+        return json.loads(path.read_text())
+    except Exception:
+        return {}
+
+
+def tune(inp: KernelInput, device: int = 0, math: str = "parity", views: Optional[Sequence[int]] = None,
+         candidates: Sequence[int] = CANDIDATES, cache: Optional[pathlib.Path] = DEFAULT_CACHE,
+         max_views: int = 4, force: bool = False) -> dict:
+    """Returns {"tuning": t, "ms": {t: half-step ms}, "cached": bool}."""
+    probe = PatchMatchBackend(device, math=math)
+    gpu = probe.name()
+    probe.close()
+    key = _key(gpu, inp, math)
+    if cache is not None and not force:
+        hit = _load(cache).get(key)
+        if hit:
+            return dict(hit, cached=True)
+    vs = list(views if views is not None else range(len(inp.views)))[:max_views]
+    times = {}
+    for t in candidates:
+        be = PatchMatchBackend(device, math=math, tuning=t)
+        with be.begin(inp) as s:
+            p = RunParams(inp.num_levels - 1, False, True, 1, 1)
+            s.run_resident(vs, p)  # warm-up (module load, texture setup)
+            s.synchronize()
+            s.set_profiling(True)
+            s.reset_stats()
+            s.run_resident(vs, p)
+            times[t] = s.kernel_stats(_lib.PS_KERNEL_HALF)["ms"]
+        be.close()
+    best = min(times, key=times.get)
+    res = {"tuning": best, "ms": {str(k): round(v, 3) for k, v in times.items()}, "key": key}
+    if cache is not None:
+        data = _load(cache)
+        data[key] = res
+        try:
+            cache.write_text(json.dumps(data, indent=1))
+        except OSError:
+            pass
+    return dict(res, cached=False)

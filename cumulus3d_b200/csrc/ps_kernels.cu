@@ -43,7 +43,7 @@ __device__ __forceinline__ float m_rcp(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 #else
-  return __frcp_rn(x);  // correctly rounded, i.e. the same bits as 1.0f / x
+  return ps_rcpf(x);  // branch-free Newton reciprocal (ps_fmath.h), the same bits as the oracle
 #endif
 }
 __device__ __forceinline__ float m_exp(float x) {
@@ -265,13 +265,15 @@ __device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, cons
         float d = rs.ic - ik;
         w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
       }
+      // Branch-free tap: behind the source camera (zz <= 1e-8) the sample is 0; the reciprocal is replaced by 0 there
+      // so the (discarded) fetch coordinates stay finite, and every tap's fetch can be issued ahead of its use.
       const float zz = fmaf(H[6], sx, rz);
-      float sv = 0.f;
-      if (zz > 1e-8f) {
-        const float izz = m_rcp(zz);
-        if constexpr (TEX) sv = src_sample_tex(tex, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
-        else sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
-      }
+      const bool front = zz > 1e-8f;
+      const float izz = front ? m_rcp(zz) : 0.0f;
+      float sv;
+      if constexpr (TEX) sv = src_sample_tex(tex, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+      else sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+      sv = front ? sv : 0.0f;
       const float wsv = w * sv;
       Ss[pa] = Ss[pa] + wsv;
       SSs[pa] = fmaf(wsv, sv, SSs[pa]);

@@ -992,6 +992,50 @@ int ps_snapshot_capture(ps_session* s, uint32_t level, const uint32_t* views, si
   });
 }
 
+int ps_snapshot_buffer(ps_session* s, uint32_t level, float** device_ptr, uint64_t* offsets) {
+  return guard(s, [&] {
+    Slot& sl = slot(s, (int)level);
+    if ((size_t)sl.total > s->snap_cap || s->snap_level != (int)level) {
+      // (re)lay the buffer out like the level's slots; nothing is present yet
+      if ((size_t)sl.total > s->snap_cap) {
+        if (s->snap) cudaFree(s->snap);
+        s->snap = nullptr;
+        s->snap_cap = 0;
+        s->snap = dalloc<float>(sl.total);
+        s->snap_cap = sl.total;
+      }
+      std::vector<long long> none(s->nv, -1);
+      cuda_ok(cudaMemcpyAsync(s->snap_off, none.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
+              "upload offsets");
+      sync(s);
+      s->snap_level = (int)level;
+      s->snap_valid = false;
+    }
+    if (device_ptr) *device_ptr = s->snap;
+    if (offsets)
+      for (int v = 0; v < s->nv; ++v) offsets[v] = (uint64_t)sl.off[v];
+  });
+}
+
+int ps_snapshot_mark(ps_session* s, uint32_t level, const uint32_t* views, size_t n, uint64_t id) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    Slot& sl = slot(s, (int)level);
+    if (s->snap_level != (int)level || (size_t)sl.total > s->snap_cap)
+      fail(PS_EINVAL, "call ps_snapshot_buffer for this level first");
+    std::vector<long long> offs(s->nv, -1);
+    cuda_ok(cudaMemcpyAsync(offs.data(), s->snap_off, s->nv * sizeof(long long), cudaMemcpyDeviceToHost, s->st),
+            "read offsets");
+    sync(s);
+    for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
+    cuda_ok(cudaMemcpyAsync(s->snap_off, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
+            "upload offsets");
+    sync(s);
+    s->snap_valid = true;
+    s->snap_id = id;
+  });
+}
+
 int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* const* out_counts) {
   return guard(s, [&] {
     check_views(s, views, n);

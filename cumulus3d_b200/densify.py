@@ -65,7 +65,8 @@ def build_pyramid(gray: np.ndarray, k: Sequence[float], levels: int) -> List[Lev
         nh, nw = h // 2, w // 2
         b = b[: 2 * nh, : 2 * nw]
         nxt = np.float32(0.25) * (b[0::2, 0::2] + b[0::2, 1::2] + b[1::2, 0::2] + b[1::2, 1::2])
-        q = np.clip(np.round(nxt), 0, 255).astype(np.uint8)
+        fl = np.floor(nxt)  # values are >= 0: round half away from zero = floor + (frac >= 0.5), exact in binary32
+        q = np.clip(fl + (nxt - fl >= np.float32(0.5)), 0, 255).astype(np.uint8)
         kk = [kk[0] * 0.5, kk[1] * 0.5, (kk[2] + 0.5) * 0.5 - 0.5, (kk[3] + 0.5) * 0.5 - 0.5]
         out.append(LevelImage(q, tuple(kk)))
         cur = q.astype(np.float32)

@@ -336,6 +336,16 @@ class PatchMatchSession:
     def snapshot_capture(self, level: int, views: Sequence[int], snap_id: int, keep_others: bool = False) -> None:
         self._check(self.lib.ps_snapshot_capture(self.h, level, _views(views), len(views), snap_id, int(keep_others)))
 
+    def snapshot_buffer(self, level: int):
+        """(device pointer, per-view offsets in floats) of the level's snapshot buffer."""
+        ptr = C.c_void_p()
+        offs = (C.c_uint64 * max(len(self.input.views), 1))()
+        self._check(self.lib.ps_snapshot_buffer(self.h, level, C.byref(ptr), offs))
+        return int(ptr.value or 0), [int(offs[i]) for i in range(len(self.input.views))]
+
+    def snapshot_mark(self, level: int, views: Sequence[int], snap_id: int) -> None:
+        self._check(self.lib.ps_snapshot_mark(self.h, level, _views(views), len(views), snap_id))
+
     def filter_resident(self, views: Sequence[int], download: bool = True) -> Optional[List[np.ndarray]]:
         if not download:
             self._check(self.lib.ps_filter_resident(self.h, _views(views), len(views), None))

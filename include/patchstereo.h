@@ -235,6 +235,14 @@ int ps_run_resident(ps_session* s, const uint32_t* views, size_t n, const ps_run
  * unless `keep_others`). */
 int ps_snapshot_capture(ps_session* s, uint32_t level, const uint32_t* views, size_t n, uint64_t id,
                         uint32_t keep_others);
+/* The snapshot buffer of `level` in device memory (allocated on first use), laid out like the level's state slots:
+ * offsets[v] (num_views entries, in floats) is where view v's w*h depth map lives.  A multi-GPU caller writes the
+ * maps of views owned by other ranks there (e.g. NCCL broadcast into this GPU's own memory) and then declares them
+ * with ps_snapshot_mark. */
+int ps_snapshot_buffer(ps_session* s, uint32_t level, float** device_ptr, uint64_t* offsets);
+/* Declares the maps of `views` present in the snapshot buffer of `level` (content written by the caller) and sets
+ * the snapshot id; views not listed keep their current presence. */
+int ps_snapshot_mark(ps_session* s, uint32_t level, const uint32_t* views, size_t n, uint64_t id);
 /* Filter on the resident states against the resident snapshot; out_counts may be NULL (counts stay on device and
  * ps_readout_resident applies the threshold). */
 int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* const* out_counts);

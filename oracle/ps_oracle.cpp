@@ -17,8 +17,9 @@
 // Numerics contract (shared with the engine's parity build).  Compiled with -ffp-contract=off: every operation is a
 // correctly rounded binary32 (or binary64) operation in the order written; fused multiply-adds appear only where
 // written as fma(); division and square root are IEEE; exp and sincos are the functions of ps_fmath.h.  The places
-// where the reference leaves the choice to the compiler (contraction, __expf, rsqrtf, hardware bilinear) are fixed
-// as follows, identically in the engine: bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
+// where the reference leaves the choice to the compiler (contraction, __expf, rsqrtf, the approximate division of
+// its fast-math build, hardware bilinear) are fixed as follows, identically in the engine: the projective
+// reciprocal 1/z of the NCC (centre and taps) is ps_rcpf (Newton, <= 0.5006 ulp); bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
 // fma(ay, bot-top, top) on values already divided by 255; tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
 // the two numerators); window accumulation Ss += w·s, SSs = fma(w·s, s, SSs), IS = fma(w·s, Ik, IS); reference
 // statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); every window sum (W, S, SS, Ss, SSs, IS) is kept as two partial
@@ -56,6 +57,10 @@ inline double mn(double a, double b) { return fmin(a, b); }
 inline float mx(float a, float b) { return fmaxf(a, b); }
 inline double mx(double a, double b) { return fmax(a, b); }
 inline float sq(float a) { return sqrtf(a); }
+// Tap reciprocal: binary32 uses the branch-free Newton reciprocal of ps_fmath.h (the engine's parity sequence);
+// binary64 divides.
+inline float rc(float a) { return ps_rcpf(a); }
+inline double rc(double a) { return 1.0 / a; }
 inline double sq(double a) { return sqrt(a); }
 
 template <class T>
@@ -294,7 +299,7 @@ T ncc_cost(const Scene& sc, const Img& R, const RS<T>& rs, const Img& S, const T
   T fx = (T)x, fy = (T)y;
   T z = fm(H[6], fx, fm(H[7], fy, H[8]));
   if (!(z > (T)1e-8f)) return 2;
-  T iz = (T)1 / z;
+  T iz = rc(z);
   T u = fm(H[0], fx, fm(H[1], fy, H[2])) * iz, v = fm(H[3], fx, fm(H[4], fy, H[5])) * iz;
   if (!(u >= 0 && v >= 0 && u <= (T)S.w - (T)1 && v <= (T)S.h - (T)1)) return 2;
   if (rs.var < (T)1e-5f) return 2;
@@ -313,7 +318,7 @@ T ncc_cost(const Scene& sc, const Img& R, const RS<T>& rs, const Img& S, const T
       T zz = fm(H[6], sx, fm(H[7], sy, H[8]));
       T sv = 0;
       if (zz > (T)1e-8f) {
-        T izz = (T)1 / zz;
+        T izz = rc(zz);
         sv = sample<T>(S, fm(H[0], sx, fm(H[1], sy, H[2])) * izz, fm(H[3], sx, fm(H[4], sy, H[5])) * izz);
       }
       T wsv = w * sv;

@@ -1,0 +1,108 @@
+"""The C ABI library (CPU only: no compute calls).
+
+* libpatchstereo.so loads and exports every function declared in include/patchstereo.h;
+* the ctypes mirror has the same struct sizes and field offsets as a C compilation of the header;
+* without a GPU, backend creation fails with PS_ENODEV (no CPU fallback exists);
+* parameter defaults equal the reference's PmParams::default / FilterParams::default
+  (crates/dense/src/params.rs:126-154, :196-207).
+"""
+import ctypes as C
+import os
+import re
+import subprocess
+import tempfile
+
+import pytest
+
+from cumulus3d_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "patchstereo.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"^\s*(?:const\s+)?[\w\s\*]+?\b(ps_\w+)\s*\(", src, flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(str(_lib.ENGINE_PATH))
+    names = declared_functions()
+    assert len(names) >= 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    # the ctypes table covers the same set
+    assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+
+
+STRUCTS = {
+    "ps_options": _lib.Options, "ps_pm_params": _lib.PmParams, "ps_filter_params": _lib.FilterParams,
+    "ps_level_image": _lib.LevelImage, "ps_pair_geometry": _lib.PairGeometry, "ps_kernel_view": _lib.KernelView,
+    "ps_kernel_input": _lib.KernelInput, "ps_view_state": _lib.ViewState, "ps_run_params": _lib.RunParams,
+    "ps_depth_snapshot": _lib.DepthSnapshot,
+}
+
+
+def test_struct_layout_matches_c():
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in STRUCTS.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    with tempfile.TemporaryDirectory() as d:
+        c = os.path.join(d, "layout.c")
+        exe = os.path.join(d, "layout")
+        open(c, "w").write("\n".join(lines))
+        subprocess.run(["gcc", "-std=c99", "-o", exe, c], check=True)
+        out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = dict(l.rsplit(" ", 1) for l in out if l)
+    for cname, py in STRUCTS.items():
+        assert int(got[f"{cname} size"]) == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(py, fname).offset, f"{cname}.{fname}"
+
+
+def test_no_gpu_means_enodev():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = _lib.engine()
+    h = C.c_void_p()
+    rc = lib.ps_backend_create(0, None, C.byref(h))
+    assert rc == _lib.PS_ENODEV and not h.value
+    from cumulus3d_b200.patchstereo import PatchMatchBackend, PsError
+    with pytest.raises(PsError) as e:
+        PatchMatchBackend(0)
+    assert e.value.code == _lib.PS_ENODEV
+
+
+def test_null_arguments_rejected_without_device():
+    lib = _lib.engine()
+    assert lib.ps_backend_create(0, None, None) == _lib.PS_EINVAL
+    assert lib.ps_begin(None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_end(None) == _lib.PS_EINVAL
+    assert lib.ps_run(None, None, 0, None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_last_error(None) == b"session is NULL"
+    assert lib.ps_abi_version() == 1
+
+
+def test_defaults_match_reference():
+    pm = _lib.default_pm()
+    assert (pm.window_radius, pm.window_step, pm.sigma_spatial, pm.top_k, pm.n1, pm.n2) == (5, 2, -1.0, 3, 2, 3)
+    for name, want in [("sigma_color", 0.2), ("tau0", 0.8), ("tau_alpha", 90.0), ("tau1", 1.2), ("beta", 0.3),
+                       ("prev_view_weight", 0.2), ("min_triangulation_angle_deg", 1.0), ("incident_angle_sigma", 0.9),
+                       ("geom_lambda", 0.2), ("geom_max_cost", 3.0), ("eps0_photometric", 0.2),
+                       ("eps0_geometric", 0.05), ("phi0_photometric_deg", 30.0), ("phi0_geometric_deg", 10.0),
+                       ("eps_min", 0.005), ("phi_min_deg", 1.0), ("weak_texture_var", 0.0)]:
+        assert abs(getattr(pm, name) - want) < 1e-7, name
+    fl = _lib.default_filter()
+    assert (fl.min_num_consistent, fl.median_filter) == (2, 1)
+    for name, want in [("min_ncc", 0.1), ("min_triangulation_angle_deg", 3.0), ("geom_max_cost", 1.0),
+                       ("ncc_sigma", 0.6)]:
+        assert abs(getattr(fl, name) - want) < 1e-7, name
+    o = _lib.Options()
+    _lib.engine().ps_options_default(C.byref(o))
+    assert (o.math_mode, o.max_batch, o.batch_pixels, o.checked, o.tuning) == (0, 64, 0, 0, 0)

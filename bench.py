@@ -111,6 +111,18 @@ def shard(n_views: int, rank: int, world: int):
     return list(range(start, start + base + (1 if rank < extra else 0)))
 
 
+def make_workload(args, rank: int, shard_job: bool):
+    """The benchmark workload: c2 (drone scale, the metric's configuration; default), c1 (640×480, 3 views) or c3
+    (64 views of mixed sizes from 4 terrains, 2-8 sources each)."""
+    from cumulus3d_b200 import scenes
+    seed_shift = 0 if shard_job else rank
+    if args.workload == "c1":
+        return scenes.workload_c1(seed=1 + seed_shift)
+    if args.workload == "c3":
+        return scenes.workload_c3(seed=3 + seed_shift)
+    return scenes.workload_c2(seed=2 + seed_shift, with_gt=False, views=args.views)
+
+
 def bench_ours(args, rank, world, local):
     import torch
     from cumulus3d_b200 import _lib, densify, scenes
@@ -122,7 +134,7 @@ def bench_ours(args, rank, world, local):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     shard_job = world > 1 and args.shard_job
-    wl = scenes.workload_c2(seed=2 + (0 if shard_job else rank), with_gt=False, views=args.views)
+    wl = make_workload(args, rank, shard_job)
     mine = shard(len(wl.cams), rank, world) if shard_job else list(range(len(wl.cams)))
     wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
     tuned = None
@@ -201,8 +213,10 @@ def bench_ours(args, rank, world, local):
         "unit": "views/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "strong" if shard_job else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain renderer, no dataset)",
-        "config": {"workload": wl.name, "views": views_total, "width": 1920, "height": 1080, "window": f"{wn}x{wn}",
-                   "sources": 4, "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x"
+        "config": {"workload": wl.name, "views": views_total, "sizes": sorted({f"{c.width}x{c.height}" for c in wl.cams}),
+                   "window": f"{wn}x{wn}", "sources": sorted({len(v.sources) for v in wl.input.views}),
+                   "megapixels_per_job": round(wl.pixels() / 1e6, 2),
+                   "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x"
                    f"{wl.geometric_iters} geometric", "math": args.math, "tuning": args.tuning,
                    "autotune": None if tuned is None else {"half_ms": tuned["ms"], "cached": tuned["cached"]},
                    "l2": "inputs larger than L2 (24 f32 images + 1.2 GB of resident per-pixel state)",
@@ -350,6 +364,8 @@ def main():
     ap.add_argument("--math", default="parity", choices=["parity", "fast"])
     ap.add_argument("--tuning", type=int, default=-1, help="half-step variant (PS_TUNE_* flags); -1 = autotune")
     ap.add_argument("--shard-job", action="store_true", help="shard one job's views over the ranks (strong scaling)")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3"],
+                    help="c2 = the metric's drone-scale configuration (default); c1/c3 = the other configurations")
     ap.add_argument("--views", type=int, default=None,
                     help="first N views of the workload only (small profiling cases, not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")

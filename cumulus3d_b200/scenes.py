@@ -110,12 +110,13 @@ def _extent(cams: Sequence[Camera], zmin: float = -1.0) -> Tuple[float, float, f
 
 def render(cams: Sequence[Camera], seed: int, *, relief: float = 8.0, wavelength: float = 24.0, cell: float = 0.1,
            noise_sigma: float = 0.01, boxes: int = 0, box_h: Tuple[float, float] = (3.0, 15.0),
-           box_s: Tuple[float, float] = (4.0, 12.0), with_gt: bool = True):
+           box_s: Tuple[float, float] = (4.0, 12.0), with_gt: bool = True,
+           extent: Optional[Tuple[float, float, float, float]] = None):
     """Renders every camera (all must share width/height).  Returns images (n, h, w) f32 and, with `with_gt`,
     ground-truth depth (n, h, w) and normals (n, h, w, 3)."""
     w, h = cams[0].width, cams[0].height
     assert all(c.width == w and c.height == h for c in cams)
-    x0, y0, x1, y1 = _extent(cams)
+    x0, y0, x1, y1 = extent if extent is not None else _extent(cams)
     sc = _SynthScene(seed, relief, wavelength, cell, x0, y0, x1, y1, noise_sigma, boxes, box_h[0], box_h[1],
                      box_s[0], box_s[1], 1.0)
     n = len(cams)
@@ -225,6 +226,45 @@ def workload_c2(seed: int = 2, with_gt: bool = True, views: Optional[int] = None
     src = nearest_sources(cams, 4)
     inp = kernel_input(cams, list(img), src, (25.0, 60.0), window_radius=6, window_step=1)
     return Workload("c2_1920x1080_24views_w13_6it_geo", cams, img, dep, nrm, inp, 6, 1, 2)
+
+
+C3_SIZES = ((960, 540), (1280, 720), (1920, 1080), (2048, 1536))
+
+
+def workload_c3(seed: int = 3, scenes_n: int = 4, per_scene: int = 16, with_gt: bool = False,
+                sizes=C3_SIZES) -> Workload:
+    """Batched uneven workload: `scenes_n` seeded terrains × `per_scene` reference views; every view's size is drawn
+    uniformly from `sizes`, its source count uniformly from 2..8 (nearest cameras of its own scene), depth range
+    20-80 m.  Cameras of one scene fly a 4-wide formation; all views run in one session."""
+    rng = np.random.default_rng(seed)
+    cams_all: List[Camera] = []
+    images: List[np.ndarray] = []
+    sources: List[List[int]] = []
+    gts = []
+    for sc in range(scenes_n):
+        base = formation(1920, 1080, per_scene // 4, cams_per_row=4, prefix=f"c3s{sc}", spacing=6.0)
+        picks = rng.integers(0, len(sizes), per_scene)
+        cams = []
+        for cam, k in zip(base, picks):
+            w, h = sizes[k]
+            f = (w / 2.0) / math.tan(math.radians(60.0) / 2.0)
+            cams.append(Camera(cam.name, (f, f, (w - 1) / 2.0, (h - 1) / 2.0), cam.r, cam.t, w, h))
+        ext = _extent(cams)
+        imgs: List[Optional[np.ndarray]] = [None] * len(cams)
+        for (w, h) in sorted({(c.width, c.height) for c in cams}):
+            idx = [i for i, c in enumerate(cams) if (c.width, c.height) == (w, h)]
+            img, dep, _ = render([cams[i] for i in idx], seed * 100 + sc, with_gt=with_gt, extent=ext)
+            for j, i in enumerate(idx):
+                imgs[i] = img[j]
+        off = len(cams_all)
+        near = nearest_sources(cams, len(cams) - 1)
+        for i in range(len(cams)):
+            k = int(rng.integers(2, 9))
+            sources.append([off + j for j in near[i][:k]])
+        cams_all += cams
+        images += imgs
+    inp = kernel_input(cams_all, images, sources, (20.0, 80.0), window_radius=6, window_step=1)
+    return Workload("c3_64views_mixed_sizes_2to8_sources", cams_all, None, None, None, inp, 6, 1, 2)
 
 
 def workload_c5(seed: int = 5, views: Optional[int] = None, with_gt: bool = False) -> Workload:

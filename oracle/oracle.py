@@ -137,3 +137,29 @@ def reeval_f64(inp: KernelInput, level: int, views: Sequence[int], states: List[
     _chk(lib().oracle_reeval_f64(C.byref(ci.c), level, _views(views), len(views), c_states(states, keep),
                                  int(geometric), c_snapshot(snapshot, keep), op, _threads(threads)), "reeval")
     return outs
+
+
+class OracleSession:
+    """The oracle behind the PatchMatchSession interface, so a driver (e.g. densify.compute_depth_maps) runs the
+    same schedule on the CPU restatement as on the engine."""
+
+    def __init__(self, inp: KernelInput, threads: Optional[int] = None):
+        self.input, self.threads = inp, threads
+
+    def run(self, views, states, p, snapshot=None):
+        run(self.input, views, states, p, snapshot, self.threads)
+
+    def evaluate(self, level, views, states, geometric=False, snapshot=None):
+        return evaluate(self.input, level, views, states, geometric, snapshot, self.threads)
+
+    def filter(self, views, states, snapshot):
+        return filter(self.input, views, states, snapshot, self.threads)
+
+    def upsample(self, inp, level, views, low, sigma_s, sigma_c):
+        return upsample(self.input, level, views, low, sigma_s, sigma_c, self.threads)
+
+    def median_filter(self, inp, level, views, states):
+        outs = median(self.input, level, views, states, self.threads)
+        for o, s in zip(outs, states):
+            o.cost[...] = s.cost
+        return outs

@@ -1,0 +1,40 @@
+"""The multi-scale driver (compute_depth_maps schedule) on the engine equals the same schedule on the oracle."""
+import numpy as np
+import pytest
+
+from cumulus3d_b200 import densify, scenes
+from cumulus3d_b200.patchstereo import KernelInput
+from oracle.oracle import OracleSession
+
+pytestmark = pytest.mark.gpu
+
+
+def _pyramid_input(wl, levels=3, weak_var=0.0, median=True):
+    views = []
+    for v, cam in zip(wl.input.views, wl.cams):
+        g = np.clip(np.round(v.levels[0].pixels * 255.0), 0, 255).astype(np.uint8)  # 8-bit gray, as the reference
+        v.levels = densify.build_pyramid(g, cam.k, levels)
+        views.append(v)
+    inp = KernelInput(views, levels, wl.input.pm, wl.input.filter, wl.input.seed)
+    inp.pm.weak_texture_var = weak_var
+    inp.filter.median_filter = int(median)
+    return inp
+
+
+@pytest.mark.parametrize("weak_var", [0.0, 0.002])
+def test_multiscale_schedule_bitwise_equal(backend, weak_var):
+    wl = scenes.workload_small(128, 96, views=3, window_radius=3, seed=17)
+    inp = _pyramid_input(wl, 3, weak_var)
+    sch = densify.Schedule(photometric_iters=2, photometric_iters_upper=1, geometric_rounds=1, geometric_iters=1)
+    with backend.begin(inp) as s:
+        g_raw, g_fin, g_cnt = densify.compute_depth_maps(s, inp, [0, 1, 2], sch, weak_texture_prior=weak_var > 0)
+    c_raw, c_fin, c_cnt = densify.compute_depth_maps(OracleSession(inp), inp, [0, 1, 2], sch,
+                                                     weak_texture_prior=weak_var > 0)
+    for a, b in zip(g_raw, c_raw):
+        np.testing.assert_array_equal(a.depth, b.depth)
+        np.testing.assert_array_equal(a.normal, b.normal)
+    for a, b in zip(g_cnt, c_cnt):
+        np.testing.assert_array_equal(a, b)
+    for a, b in zip(g_fin, c_fin):
+        np.testing.assert_array_equal(a.depth, b.depth)
+    assert sum(float((f.depth > 0).mean()) for f in g_fin) > 0.3

@@ -152,8 +152,9 @@ def bench_ours(args, rank, world, local):
         exchange = SnapshotExchange(sess, wl.input, world, rank, shard)
 
     def step():
-        if exchange is None:
-            densify.schedule_resident(sess, mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters)
+        if exchange is None:  # one CUDA-graph launch per step (captured during the first warm-up step)
+            sess.schedule_resident(mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters,
+                                   graph=not args.no_graph)
         else:
             exchange.schedule(mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters)
 
@@ -164,10 +165,10 @@ def bench_ours(args, rank, world, local):
             dist.barrier()
         sess.synchronize()
 
+    sess.set_profiling(True)  # before warm-up, so the captured graph carries the per-launch timing events
     for _ in range(args.warmup):
         step()
     barrier()
-    sess.set_profiling(True)
     sess.reset_stats()
     launches0 = sess.launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -369,6 +370,7 @@ def main():
     ap.add_argument("--views", type=int, default=None,
                     help="first N views of the workload only (small profiling cases, not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="issue the schedule's launches directly (no CUDA graph)")
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

@@ -76,6 +76,11 @@ class RunParams(C.Structure):
                 ("iterations", C.c_uint32), ("run_id", C.c_uint32), ("use_prior", C.c_uint32)]
 
 
+class Schedule(C.Structure):
+    _fields_ = [("level", C.c_uint32), ("photometric_iters", C.c_uint32), ("geometric_rounds", C.c_uint32),
+                ("geometric_iters", C.c_uint32), ("run_id_base", C.c_uint32), ("use_graph", C.c_uint32)]
+
+
 class DepthSnapshot(C.Structure):
     _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
                 ("maps", C.POINTER(C.POINTER(C.c_float)))]
@@ -112,6 +117,7 @@ SIGNATURES = {
     "ps_snapshot_mark": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.c_uint64]),
     "ps_filter_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_uint8))]),
     "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
+    "ps_schedule_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(Schedule)]),
     "ps_synchronize": (C.c_int, [_P]),
     "ps_launch_count": (C.c_uint64, [_P]),
     "ps_session_stream": (C.c_void_p, [_P]),

@@ -1190,6 +1190,9 @@ cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st) {
   k_readout<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, out);
   return cudaGetLastError();
 }
+// Module constants (propagation offsets); called at session begin, outside any stream capture.
+cudaError_t prepare() { return init_constants(); }
+
 cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st) {
   k_fp32_probe<<<blocks, 256, 0, st>>>(out, iters, 0.999999f, 1e-7f);
   return cudaGetLastError();

@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -34,6 +35,7 @@
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
   cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
   cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
+  cudaError_t prepare();                                                                                   \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
                                   const int* has64, PsLPair* out, int nviews, int nlevels, cudaStream_t st); \
   }
@@ -134,10 +136,20 @@ struct ps_session {
   struct Pending {
     int kind;
     cudaEvent_t a, b;
+    bool persistent;  // owned by a captured graph (re-recorded on every replay)
   };
   std::vector<Pending> pending;
   double kind_ms[PS_KERNEL_KINDS] = {0, 0, 0, 0};
   uint64_t kind_launches[PS_KERNEL_KINDS] = {0, 0, 0, 0};
+  bool capturing = false;  // a stream capture of this session's stream is in progress
+  // captured single-level schedules (ps_schedule_resident)
+  struct GraphEntry {
+    cudaGraphExec_t exec = nullptr;  // captured schedule (nullptr: direct launches)
+    long long* offsets = nullptr;    // snapshot offset table of the schedule's view set (device)
+    uint64_t per_replay = 0;         // kernels per replay
+    std::vector<Pending> events;     // per-launch event nodes captured with profiling on
+  };
+  std::map<std::string, GraphEntry> graphs;
 
   int W(int v, int l) const { return w[v * nl + l]; }
   int H(int v, int l) const { return h[v * nl + l]; }
@@ -326,11 +338,15 @@ void timed_launch(ps_session* s, int kind, PsRun& P, F&& f, const char* what) {
   P.ncc_count = s->counters + kind;
   ps_session::Pending pd;
   pd.kind = kind;
+  pd.persistent = false;
   cuda_ok(cudaEventCreate(&pd.a), "cudaEventCreate");
   cuda_ok(cudaEventCreate(&pd.b), "cudaEventCreate");
-  cuda_ok(cudaEventRecord(pd.a, s->st), "cudaEventRecord");
+  // inside a stream capture the records must be external event nodes (re-recorded on each replay), not the
+  // capture-internal dependencies a plain cudaEventRecord expresses
+  const unsigned flags = s->capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+  cuda_ok(cudaEventRecordWithFlags(pd.a, s->st, flags), "cudaEventRecord");
   launched(s, f(P), what);
-  cuda_ok(cudaEventRecord(pd.b, s->st), "cudaEventRecord");
+  cuda_ok(cudaEventRecordWithFlags(pd.b, s->st, flags), "cudaEventRecord");
   s->pending.push_back(pd);
   s->kind_launches[kind]++;
 }
@@ -342,8 +358,10 @@ void collect_events(ps_session* s) {
     float ms = 0.f;
     cuda_ok(cudaEventElapsedTime(&ms, pd.a, pd.b), "cudaEventElapsedTime");
     s->kind_ms[pd.kind] += ms;
-    cudaEventDestroy(pd.a);
-    cudaEventDestroy(pd.b);
+    if (!pd.persistent) {
+      cudaEventDestroy(pd.a);
+      cudaEventDestroy(pd.b);
+    }
   }
   s->pending.clear();
 }
@@ -634,6 +652,9 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
       }
     }
     cuda_ok(cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking), "cudaStreamCreate");
+    // module constants are set here, outside any stream capture (their copy is synchronous)
+    cuda_ok(ps_parity::prepare(), "module constants");
+    cuda_ok(ps_fast::prepare(), "module constants");
     // images: normalised f32 planes with a zero border
     std::vector<float> host(std::max<size_t>(total, 1), 0.0f);
     std::vector<PsLevel> lvh(s->nv * s->nl);
@@ -778,8 +799,17 @@ int ps_end(ps_session* s) {
   for (cudaArray_t a : s->arrays) cudaFreeArray(a);
   cudaFree(s->counters);
   for (auto& pd : s->pending) {
+    if (pd.persistent) continue;  // destroyed with their graph below
     cudaEventDestroy(pd.a);
     cudaEventDestroy(pd.b);
+  }
+  for (auto& kv : s->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    cudaFree(kv.second.offsets);
+    for (auto& pd : kv.second.events) {
+      cudaEventDestroy(pd.a);
+      cudaEventDestroy(pd.b);
+    }
   }
   if (s->pin) cudaFreeHost(s->pin);
   if (s->st) cudaStreamDestroy(s->st);
@@ -1071,6 +1101,138 @@ int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_
       launched(s, s->L->readout(P, sl.aux, s->st), "readout kernel");
       if (out) download_states(s, views, a, b, out, level, true, true, sl.aux);
     }
+  });
+}
+
+namespace {
+
+// Snapshot of `views` at `level` captured on the device: depth of the resident planes into the snapshot buffer (slot
+// layout) and the offset table copied from a device array prepared for this view set.  No host synchronisation.
+void enqueue_snapshot(ps_session* s, const uint32_t* views, size_t n, int level, const long long* offsets_dev) {
+  for (auto [a, b] : batches(s, views, n, level)) {
+    PsRun P = base_params(s, level);
+    set_items(s, P, views, a, b, level, PS_SIMPLE_BX, PS_SIMPLE_BY, level);
+    launched(s, s->L->snapshot(P, s->snap, s->st), "snapshot kernel");
+  }
+  cuda_ok(cudaMemcpyAsync(s->snap_off, offsets_dev, s->nv * sizeof(long long), cudaMemcpyDeviceToDevice, s->st),
+          "snapshot offsets");
+}
+
+// The launches of one single-level schedule, in the order of densify.schedule_resident.
+void enqueue_schedule(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch,
+                      const long long* offsets_dev) {
+  const int level = (int)sch->level;
+  Slot& sl = slot(s, level);
+  ps_run_params p{sch->level, 0, 1, sch->photometric_iters, sch->run_id_base, 0};
+  for (auto [a, b] : batches(s, views, n, level)) run_batch(s, views, a, b, &p, false);
+  for (uint32_t r = 0; r < sch->geometric_rounds; ++r) {
+    enqueue_snapshot(s, views, n, level, offsets_dev);
+    ps_run_params g{sch->level, 1, 0, sch->geometric_iters, sch->run_id_base + 1 + r, 0};
+    for (auto [a, b] : batches(s, views, n, level)) run_batch(s, views, a, b, &g, false);
+  }
+  enqueue_snapshot(s, views, n, level, offsets_dev);
+  for (auto [a, b] : batches(s, views, n, level)) {
+    PsRun P = base_params(s, level);
+    P.geometric = 1;
+    set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
+    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+    PsRun Q = base_params(s, level);
+    set_items(s, Q, views, a, b, level, PS_SIMPLE_BX, PS_SIMPLE_BY);
+    launched(s, s->L->readout(Q, sl.aux, s->st), "readout kernel");
+  }
+}
+
+}  // namespace
+
+int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch) {
+  return guard(s, [&] {
+    if (!sch) fail(PS_EINVAL, "schedule is NULL");
+    check_views(s, views, n);
+    const int level = (int)sch->level;
+    Slot& sl = slot(s, level);
+    // the snapshot buffer in the slot layout, allocated outside any capture
+    if ((size_t)sl.total > s->snap_cap) {
+      if (s->snap) cudaFree(s->snap);
+      s->snap = nullptr;
+      s->snap_cap = 0;
+      s->snap = dalloc<float>(sl.total);
+      s->snap_cap = sl.total;
+    }
+    std::string key = std::to_string(level) + ":" + std::to_string(sch->photometric_iters) + ":" +
+                      std::to_string(sch->geometric_rounds) + ":" + std::to_string(sch->geometric_iters) + ":" +
+                      std::to_string(sch->run_id_base) + ":" + std::to_string(sch->use_graph) + ":" +
+                      std::to_string(s->profiling) + ":";
+    for (size_t i = 0; i < n; ++i) key += std::to_string(views[i]) + ",";
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+      ps_session::GraphEntry ge;
+      std::vector<long long> offs(s->nv, -1);
+      for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
+      ge.offsets = dalloc<long long>(s->nv);
+      cuda_ok(cudaMemcpyAsync(ge.offsets, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
+              "upload offsets");
+      sync(s);
+      if (sch->use_graph) {
+        // capture once: the launches the direct path issues, recorded into a graph; with profiling on, the per-launch
+        // events become event-record nodes that every replay re-records
+        collect_events(s);
+        const uint64_t before = s->launches;
+        uint64_t kl[PS_KERNEL_KINDS];
+        for (int k = 0; k < PS_KERNEL_KINDS; ++k) kl[k] = s->kind_launches[k];
+        cudaGraph_t g = nullptr;
+        cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        s->capturing = true;
+        try {
+          enqueue_schedule(s, views, n, sch, ge.offsets);
+          s->capturing = false;
+        } catch (...) {
+          s->capturing = false;
+          cudaStreamEndCapture(s->st, &g);
+          if (g) cudaGraphDestroy(g);
+          s->launches = before;
+          for (auto& pd : s->pending) {
+            cudaEventDestroy(pd.a);
+            cudaEventDestroy(pd.b);
+          }
+          s->pending.clear();
+          cudaFree(ge.offsets);
+          throw;
+        }
+        ge.per_replay = s->launches - before;
+        s->launches = before;
+        for (int k = 0; k < PS_KERNEL_KINDS; ++k) s->kind_launches[k] = kl[k];
+        ge.events = s->pending;
+        for (auto& pd : ge.events) pd.persistent = true;
+        s->pending.clear();
+        cudaError_t e = cudaStreamEndCapture(s->st, &g);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, g, 0);
+        if (g) cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+          cudaFree(ge.offsets);
+          for (auto& pd : ge.events) {
+            cudaEventDestroy(pd.a);
+            cudaEventDestroy(pd.b);
+          }
+        }
+        cuda_ok(e, "graph capture");
+      }
+      it = s->graphs.emplace(key, ge).first;
+    }
+    ps_session::GraphEntry& ge = it->second;
+    if (ge.exec) {
+      if (!ge.events.empty()) collect_events(s);  // the previous replay's event nodes are re-recorded by this one
+      cuda_ok(cudaGraphLaunch(ge.exec, s->st), "cudaGraphLaunch");
+      s->launches += ge.per_replay;
+      for (auto& pd : ge.events) {
+        s->pending.push_back(pd);
+        s->kind_launches[pd.kind]++;
+      }
+    } else {
+      enqueue_schedule(s, views, n, sch, ge.offsets);
+    }
+    s->snap_valid = true;
+    s->snap_level = level;
+    s->snap_id = 0x5c4ed000ull + sch->run_id_base;
   });
 }
 

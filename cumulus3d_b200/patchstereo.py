@@ -371,6 +371,12 @@ class PatchMatchSession:
         self._check(self.lib.ps_readout_resident(self.h, _views(views), len(views), c_states(outs, keep)))
         return outs
 
+    def schedule_resident(self, views: Sequence[int], photometric_iters: int, geometric_rounds: int,
+                          geometric_iters: int, level: int = 0, run_id_base: int = 1, graph: bool = True) -> None:
+        """The whole single-level schedule on resident states (asynchronous); with `graph`, one CUDA-graph launch."""
+        sch = _lib.Schedule(level, photometric_iters, geometric_rounds, geometric_iters, run_id_base, int(graph))
+        self._check(self.lib.ps_schedule_resident(self.h, _views(views), len(views), C.byref(sch)))
+
     def synchronize(self) -> None:
         self._check(self.lib.ps_synchronize(self.h))
 

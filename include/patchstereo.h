@@ -249,6 +249,21 @@ int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* 
 /* Readout threshold of crates/dense/src/densify.rs:441-454 on device: depth and normal are zeroed where
  * count < max(1, min(min_num_consistent, nsrc)); writes the result into out (host) when given. */
 int ps_readout_resident(ps_session* s, const uint32_t* views, size_t n, ps_view_state* out);
+/* A whole single-level schedule on resident states: photometric run (random init), `geometric_rounds` geometric runs
+ * each against a snapshot of `views` captured on the device, the filter against a final snapshot and the readout
+ * threshold (results stay resident).  With `use_graph`, the sequence is captured once into a CUDA graph per
+ * (views, schedule, profiling flag) and replayed with one cudaGraphLaunch per call: no host synchronisation and no
+ * host copies inside.  Asynchronous: returns after enqueueing; ps_synchronize waits.  No reference counterpart (the
+ * reference drives every run from the host, crates/dense/src/densify.rs:351-439). */
+typedef struct ps_schedule {
+  uint32_t level;
+  uint32_t photometric_iters;
+  uint32_t geometric_rounds;
+  uint32_t geometric_iters;
+  uint32_t run_id_base; /* run ids run_id_base, run_id_base+1, … (RNG keys) */
+  uint32_t use_graph;
+} ps_schedule;
+int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch);
 int ps_synchronize(ps_session* s);
 /* Number of kernel launches this session issued so far (for launch accounting). */
 uint64_t ps_launch_count(const ps_session* s);

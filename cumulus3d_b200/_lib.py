@@ -17,6 +17,7 @@ STATUS_NAMES = {0: "PS_OK", 1: "PS_EINVAL", 2: "PS_ECUDA", 3: "PS_ENODEV", 4: "P
 PS_IMAGE_U8, PS_IMAGE_F32 = 0, 1
 PS_MATH_PARITY, PS_MATH_FAST = 0, 1
 PS_MAX_SOURCES = 32
+PS_NOALLOC_MAX_PIXELS = 1 << 21  # capacity of the allocation-free median filter's static device array
 
 
 class Options(C.Structure):
@@ -118,6 +119,8 @@ SIGNATURES = {
     "ps_filter_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_uint8))]),
     "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_schedule_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(Schedule)]),
+    "ps_median_filter_inplace_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32,
+                                                    C.POINTER(C.c_float), C.c_void_p]),
     "ps_synchronize": (C.c_int, [_P]),
     "ps_launch_count": (C.c_uint64, [_P]),
     "ps_session_stream": (C.c_void_p, [_P]),

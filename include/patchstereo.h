@@ -270,6 +270,21 @@ uint64_t ps_launch_count(const ps_session* s);
 /* The session's CUDA stream (a cudaStream_t), for callers that record their own events on it. */
 void* ps_session_stream(const ps_session* s);
 
+/* ---- allocation-free median filter (no counterpart in the reference) ---------------------------------------
+ * For callers that own device buffers but may not allocate device memory (a host framework's memory pool owns every
+ * allocation, a fixed budget forbids growth after start-up, or a real-time loop must not allocate).  Filters the
+ * caller's planes in place: `planes` is device memory, 16-byte aligned, width*height float4 (nx, ny, nz, d), and
+ * k = fx, fy, cx, cy of the image.  Same rule and same bits as ps_median_filter.  Instead of a session buffer, the
+ * input copy lives in a static device array of PS_NOALLOC_MAX_PIXELS planes (32 MiB, reserved on every GPU that
+ * loads the library until exit); larger images are rejected with PS_EINVAL.  No cudaMalloc or cudaFree is called.
+ * All calls on a device share that array and it keeps the last call's contents (a call reads only what it copied,
+ * so nothing needs clearing); calls that overlap on the GPU race on it.  The first call on a device looks up the
+ * array's address with that device current; make it before any stream capture.  Asynchronous on `stream`
+ * (a cudaStream_t, NULL = default stream). */
+#define PS_NOALLOC_MAX_PIXELS (1u << 21)
+int ps_median_filter_inplace_noalloc(int device, float* planes, uint32_t width, uint32_t height, const float* k,
+                                     void* stream);
+
 /* ---- measurement (no reference counterpart; replaces CUMULUS3D_CUDA_TRACE, crates/cuda/src/patchmatch.rs:780-797) */
 typedef enum ps_kernel_kind {
   PS_KERNEL_HALF = 0,

@@ -18,6 +18,8 @@ PS_IMAGE_U8, PS_IMAGE_F32 = 0, 1
 PS_MATH_PARITY, PS_MATH_FAST = 0, 1
 PS_MAX_SOURCES = 32
 PS_NOALLOC_MAX_PIXELS = 1 << 21  # capacity of the allocation-free median filter's static device array
+PS_INIT_RANDOM, PS_INIT_PROPOSAL = 1, 2  # ps_run_params.random_init / ps_schedule.init
+PS_SWEEP_PLANES, PS_NET_CH_IN, PS_NET_CH_OUT = 32, 48, 8
 
 
 class Options(C.Structure):
@@ -26,7 +28,8 @@ class Options(C.Structure):
 
 
 PS_TUNE_NO_WEIGHT_CACHE, PS_TUNE_TEX_GATHER, PS_TUNE_ONE_LANE = 0x1, 0x2, 0x4
-PS_KERNEL_HALF, PS_KERNEL_EVAL, PS_KERNEL_FILTER, PS_KERNEL_OTHER = range(4)
+PS_KERNEL_HALF, PS_KERNEL_EVAL, PS_KERNEL_FILTER, PS_KERNEL_OTHER, PS_KERNEL_SWEEP, PS_KERNEL_NET = range(6)
+PS_KERNEL_KINDS = 6
 
 
 class PmParams(C.Structure):
@@ -79,7 +82,8 @@ class RunParams(C.Structure):
 
 class Schedule(C.Structure):
     _fields_ = [("level", C.c_uint32), ("photometric_iters", C.c_uint32), ("geometric_rounds", C.c_uint32),
-                ("geometric_iters", C.c_uint32), ("run_id_base", C.c_uint32), ("use_graph", C.c_uint32)]
+                ("geometric_iters", C.c_uint32), ("run_id_base", C.c_uint32), ("use_graph", C.c_uint32),
+                ("init", C.c_uint32)]
 
 
 class DepthSnapshot(C.Structure):
@@ -129,6 +133,24 @@ SIGNATURES = {
                                   C.POINTER(C.c_uint64)]),
     "ps_reset_stats": (C.c_int, [_P]),
     "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    # learned proposal
+    "ps_net_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),
+    "ps_net_destroy": (None, [_P]),
+    "ps_net_last_error": (C.c_char_p, [_P]),
+    "ps_net_num_params": (C.c_uint64, [_P]),
+    "ps_net_step": (C.c_uint32, [_P]),
+    "ps_net_get_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "ps_net_set_params": (C.c_int, [_P, C.POINTER(C.c_float)]),
+    "ps_net_forward": (C.c_int, [_P, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p]),
+    "ps_net_train_step": (C.c_int, [_P, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                                    C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "ps_net_conv_check": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
+                                    C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "ps_sweep_volume": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "ps_propose": (C.c_int, [_P, _P, C.c_uint32, _U32P, C.c_size_t, C.c_float, C.POINTER(C.c_uint64)]),
+    "ps_proposal_upload": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_float))]),
+    "ps_proposal_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_float)),
+                                       C.POINTER(C.POINTER(C.c_float))]),
 }
 
 _engine = None

@@ -51,6 +51,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> pathlib.Path:
         ("k_fast.o", CSRC / "ps_kernels.cu", FAST),
         ("runtime.o", CSRC / "ps_runtime.cu", ["-Xcompiler", "-fopenmp"]),
         ("noalloc.o", CSRC / "ps_noalloc.cu", PARITY),
+        ("cnn.o", CSRC / "ps_cnn.cu", []),
     ]
     for name, src, flags in specs:
         out = OBJ / name

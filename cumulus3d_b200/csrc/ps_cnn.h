@@ -1,0 +1,19 @@
+// Internal interface between the proposal network (ps_cnn.cu) and the session runtime (ps_runtime.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+struct ps_net;
+
+namespace ps_cnn {
+// Network forward of `B` inputs of H × W pixels (bf16 NHWC, 48 channels, device) into `out` (f32 NHWC, 8 channels,
+// device), enqueued on `st`.  H and W are multiples of 8.  Returns a ps_status; on failure *err holds the message.
+int forward_on_stream(ps_net* net, const void* in, int B, int H, int W, float* out, cudaStream_t st, std::string* err);
+// Head output -> proposal planes and confidences of an H × W view whose network rows hold Wp pixels; k = fx fy cx cy.
+// Adds the number of proposed pixels to *count when count is not null.
+cudaError_t launch_decode(const float* o, int Wp, int H, int W, float4* planes, float* conf, float inv_near,
+                          float inv_far, float thr, const float* k, unsigned long long* count, cudaStream_t st);
+// Kernel launches of one forward pass.
+constexpr int kForwardLaunches = 21;
+}  // namespace ps_cnn

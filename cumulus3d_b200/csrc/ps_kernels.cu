@@ -18,6 +18,7 @@
 //     slot per thread and tap) and reused by all 9·N + 6·a NCC evaluations of that pixel;
 //   * launches are flattened over the tiles of all views of a batch (no idle CTAs for ragged batches); the batch
 //     table travels in the kernel parameters.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "ps_fmath.h"
@@ -785,6 +786,10 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
     const float d = random_depth(st, vd.dmin, vd.dmax);
     const float3 n = random_normal(st, ray);
     h = make_float4(n.x, n.y, n.z, d);
+    if (P.proposal) {  // learned init: a proposed plane (d > 0) replaces the random draw; elsewhere the draw stays
+      const float4 q = P.proposal[base + pix];
+      if (q.w > 0.f) h = q;
+    }
     P.plane[base + pix] = h;
   }
   float c = 2.f;
@@ -795,6 +800,64 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
   }
   P.cost[base + pix] = c;
   if (P.mode == 1) P.bview[base + pix] = 255;
+  count_windows(P, nwin);
+}
+
+// ================================================================================ plane sweep (learned proposal input)
+// Cost volume of one view for the proposal network (no reference counterpart).  PS_SWEEP_PLANES fronto-parallel
+// planes n = (0, 0, -1) at inverse depths i_k = 1/dmax + (2k+1)/64 · (1/dmin - 1/dmax) (bin centres); the cost of a
+// plane is the mean over the first min(2, nsrc) sources of the NCC cost 1 - ρ (the same window statistics, homography
+// and NCC as the half step, window radius wr and step P.sweep_ws), 2 where the homography fails.  Output per pixel,
+// bf16 (round to nearest even): [image, cost_0 … cost_31, 0 × 15] at netin[(y · netin_pitch + x) · 48].
+__device__ __forceinline__ unsigned short bf16_bits(float v) {
+  const __nv_bfloat16 b = __float2bfloat16_rn(v);
+  return *reinterpret_cast<const unsigned short*>(&b);
+}
+
+template <int WR, int WS>
+__global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_EVAL_NT;
+  extern __shared__ float sm[];
+  const int wr = WR ? WR : P.wr;
+  const int TW = PS_EVAL_PW + 2 * wr, TH = PS_EVAL_PH + 2 * wr;
+  EvalCtx e;
+  if (!eval_tile(P, sm, wr, e)) return;
+  const int x = e.x, y = e.y;
+  RefWin rw;
+  {
+    const int tiles_x = (e.w + PS_EVAL_PW - 1) / PS_EVAL_PW;
+    const int tl = blockIdx.x - e.it->tile0;
+    const int x0 = (tl % tiles_x) * PS_EVAL_PW, y0 = (tl / tiles_x) * PS_EVAL_PH;
+    rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
+  }
+  rw.tw = TW;
+  rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
+  const PsView& vd = P.views[e.it->view];
+  const PsLPair* lps = P.lpairs + ((size_t)e.it->view * P.nlevels + P.level) * PS_MAXSRC;
+  const PsPair* prs = P.pairs + (size_t)e.it->view * PS_MAXSRC;
+  const int nuse = min(vd.nsrc, 2);
+  const RefStats rs = ref_stats<WR, WS, true, NT>(P, rw);
+  const float inear = 1.0f / vd.dmin, ifar = 1.0f / vd.dmax;
+  unsigned short* out = P.netin + ((long long)y * P.netin_pitch + x) * PS_NET_CH_IN;
+  out[0] = bf16_bits(rw.t[0]);
+  int nwin = 0;
+#pragma unroll 1
+  for (int k = 0; k < PS_SWEEP_PLANES; ++k) {
+    const float id = fmaf((float)(2 * k + 1) * (1.0f / 64.0f), inear - ifar, ifar);
+    const float4 h = make_float4(0.0f, 0.0f, -1.0f, 1.0f / id);
+    float c = 0.0f;
+#pragma unroll 1
+    for (int j = 0; j < nuse; ++j) {
+      const PsLevel S = P.lv[prs[j].src * P.nlevels + P.level];
+      float H[9];
+      c += homography(e.R, lps[j], (float)x, (float)y, h, H) ? ncc_cost<WR, WS, true, NT>(P, rw, rs, S, H, x, y, nwin)
+                                                             : 2.0f;
+    }
+    c = nuse == 2 ? c * 0.5f : (nuse == 1 ? c : 2.0f);
+    out[1 + k] = bf16_bits(c);
+  }
+#pragma unroll
+  for (int k = 1 + PS_SWEEP_PLANES; k < PS_NET_CH_IN; ++k) out[k] = 0;
   count_windows(P, nwin);
 }
 
@@ -1190,6 +1253,17 @@ cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st) {
   k_readout<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, out);
   return cudaGetLastError();
 }
+size_t sweep_smem(int wr, int ws) { return eval_smem(wr, ws, true); }
+
+cudaError_t launch_sweep(const PsRun& P, cudaStream_t st) {
+  const size_t smem = sweep_smem(P.wr, P.sweep_ws);
+  if (P.wr == 6 && P.sweep_ws == 2) return launch(k_sweep<6, 2>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  if (P.wr == 5 && P.sweep_ws == 2) return launch(k_sweep<5, 2>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  PsRun Q = P;
+  Q.ws = P.sweep_ws;  // the generic kernel reads the window step from the parameters
+  return launch(k_sweep<0, 1>, Q.ntiles, PS_EVAL_NT, smem, st, Q);
+}
+
 // Module constants (propagation offsets); called at session begin, outside any stream capture.
 cudaError_t prepare() { return init_constants(); }
 

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/patchstereo.h"
+#include "ps_cnn.h"
 #include "ps_consts.h"
 #include "ps_types.h"
 
@@ -34,6 +35,7 @@
   cudaError_t launch_median(const PsRun& P, cudaStream_t st);                                              \
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
   cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
+  cudaError_t launch_sweep(const PsRun& P, cudaStream_t st);                                               \
   cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
   cudaError_t prepare();                                                                                   \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
@@ -53,13 +55,14 @@ struct Launchers {
   cudaError_t (*snapshot)(const PsRun&, float*, cudaStream_t);
   cudaError_t (*readout)(const PsRun&, float4*, cudaStream_t);
   int (*half_lanes)(unsigned);
+  cudaError_t (*sweep)(const PsRun&, cudaStream_t);
 };
 const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
                            ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
-                           ps_parity::launch_readout,  ps_parity::half_lanes};
+                           ps_parity::launch_readout,  ps_parity::half_lanes,    ps_parity::launch_sweep};
 const Launchers kFast = {ps_fast::launch_half,     ps_fast::launch_eval,   ps_fast::launch_filter,
                          ps_fast::launch_upsample, ps_fast::launch_median, ps_fast::launch_snapshot,
-                         ps_fast::launch_readout,  ps_fast::half_lanes};
+                         ps_fast::launch_readout,  ps_fast::half_lanes,    ps_fast::launch_sweep};
 
 struct PsError {
   int code;
@@ -80,6 +83,9 @@ struct Slot {
   unsigned char* bview = nullptr;
   unsigned char* count = nullptr;
   std::vector<char> prior_valid;
+  float4* proposal = nullptr;  // learned proposals (allocated by the first proposal call of the level)
+  float* pconf = nullptr;      // their confidences
+  std::vector<char> proposal_valid;
 };
 
 }  // namespace
@@ -106,6 +112,14 @@ struct ps_session {
   std::vector<int> w, h;  // per (view, level)
   std::vector<int> nsrc;
   std::vector<std::vector<int>> sources;
+  std::vector<PsLevel> lvh;  // host copies of the level and view tables
+  std::vector<PsView> vdh;
+  // learned proposal buffers (network input / output of one view, grown on demand)
+  unsigned short* netin = nullptr;
+  size_t netin_cap = 0;
+  float* netout = nullptr;
+  size_t netout_cap = 0;
+  unsigned long long* pcount = nullptr;
   // device tables
   float* img = nullptr;
   PsLevel* lv = nullptr;
@@ -139,8 +153,8 @@ struct ps_session {
     bool persistent;  // owned by a captured graph (re-recorded on every replay)
   };
   std::vector<Pending> pending;
-  double kind_ms[PS_KERNEL_KINDS] = {0, 0, 0, 0};
-  uint64_t kind_launches[PS_KERNEL_KINDS] = {0, 0, 0, 0};
+  double kind_ms[PS_KERNEL_KINDS] = {};
+  uint64_t kind_launches[PS_KERNEL_KINDS] = {};
   bool capturing = false;  // a stream capture of this session's stream is in progress
   // captured single-level schedules (ps_schedule_resident)
   struct GraphEntry {
@@ -512,6 +526,13 @@ void run_batch(ps_session* s, const uint32_t* views, size_t a, size_t b, const p
   P.random_init = p->random_init ? 1 : 0;
   P.use_prior = use_prior ? 1 : 0;
   P.mode = 1;
+  if (p->random_init == PS_INIT_PROPOSAL) {
+    Slot& sl = s->slots[p->level];
+    for (size_t i = a; i < b; ++i)
+      if (!sl.proposal || !sl.proposal_valid[views[i]])
+        fail(PS_EINVAL, "view " + std::to_string(views[i]) + " has no proposal at level " + std::to_string(p->level));
+    P.proposal = sl.proposal;
+  }
   set_items(s, P, views, a, b, (int)p->level, PS_EVAL_PW, PS_EVAL_PH);
   timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
   PsRun H = P;
@@ -718,6 +739,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     }
     s->counters = dalloc<unsigned long long>(PS_KERNEL_KINDS);
     cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
+    s->lvh = lvh;
     s->lv = dalloc<PsLevel>(lvh.size());
     cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
     // pairs, views, FP64 pair tables
@@ -746,6 +768,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
       vdh[v].nsrc = (int)kv.num_sources;
       vdh[v].pad = 0;
     }
+    s->vdh = vdh;
     s->pairs = dalloc<PsPair>(prh.size());
     s->views = dalloc<PsView>(vdh.size());
     s->pairs64 = dalloc<double>(p64.size());
@@ -785,7 +808,12 @@ int ps_end(ps_session* s) {
     cudaFree(sl.cost);
     cudaFree(sl.bview);
     cudaFree(sl.count);
+    cudaFree(sl.proposal);
+    cudaFree(sl.pconf);
   }
+  cudaFree(s->netin);
+  cudaFree(s->netout);
+  cudaFree(s->pcount);
   cudaFree(s->img);
   cudaFree(s->lv);
   cudaFree(s->pairs);
@@ -849,6 +877,7 @@ int ps_state_download(ps_session* s, uint32_t level, const uint32_t* views, size
 int ps_run_resident(ps_session* s, const uint32_t* views, size_t n, const ps_run_params* p) {
   return guard(s, [&] {
     if (!p) fail(PS_EINVAL, "params is NULL");
+    if (p->random_init > PS_INIT_PROPOSAL) fail(PS_EINVAL, "random_init must be 0, 1 or 2");
     check_views(s, views, n);
     Slot& sl = slot(s, (int)p->level);
     if (p->geometric) require_snapshot_level(s, (int)p->level);
@@ -864,6 +893,7 @@ int ps_run(ps_session* s, const uint32_t* views, size_t n, ps_view_state* states
            const ps_depth_snapshot* snapshot) {
   return guard(s, [&] {
     if (!p) fail(PS_EINVAL, "params is NULL");
+    if (p->random_init > PS_INIT_PROPOSAL) fail(PS_EINVAL, "random_init must be 0, 1 or 2");
     check_views(s, views, n);
     if (n && !states) fail(PS_EINVAL, "states is NULL");
     if (p->geometric) ensure_snapshot(s, snapshot);
@@ -1123,7 +1153,8 @@ void enqueue_schedule(ps_session* s, const uint32_t* views, size_t n, const ps_s
                       const long long* offsets_dev) {
   const int level = (int)sch->level;
   Slot& sl = slot(s, level);
-  ps_run_params p{sch->level, 0, 1, sch->photometric_iters, sch->run_id_base, 0};
+  ps_run_params p{sch->level, 0, sch->init == PS_INIT_PROPOSAL ? PS_INIT_PROPOSAL : PS_INIT_RANDOM,
+                  sch->photometric_iters, sch->run_id_base, 0};
   for (auto [a, b] : batches(s, views, n, level)) run_batch(s, views, a, b, &p, false);
   for (uint32_t r = 0; r < sch->geometric_rounds; ++r) {
     enqueue_snapshot(s, views, n, level, offsets_dev);
@@ -1147,6 +1178,7 @@ void enqueue_schedule(ps_session* s, const uint32_t* views, size_t n, const ps_s
 int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch) {
   return guard(s, [&] {
     if (!sch) fail(PS_EINVAL, "schedule is NULL");
+    if (sch->init > PS_INIT_PROPOSAL) fail(PS_EINVAL, "schedule init must be PS_INIT_RANDOM or PS_INIT_PROPOSAL");
     check_views(s, views, n);
     const int level = (int)sch->level;
     Slot& sl = slot(s, level);
@@ -1161,7 +1193,7 @@ int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const p
     std::string key = std::to_string(level) + ":" + std::to_string(sch->photometric_iters) + ":" +
                       std::to_string(sch->geometric_rounds) + ":" + std::to_string(sch->geometric_iters) + ":" +
                       std::to_string(sch->run_id_base) + ":" + std::to_string(sch->use_graph) + ":" +
-                      std::to_string(s->profiling) + ":";
+                      std::to_string(s->profiling) + ":" + std::to_string(sch->init == PS_INIT_PROPOSAL) + ":";
     for (size_t i = 0; i < n; ++i) key += std::to_string(views[i]) + ",";
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
@@ -1233,6 +1265,161 @@ int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const p
     s->snap_valid = true;
     s->snap_level = level;
     s->snap_id = 0x5c4ed000ull + sch->run_id_base;
+  });
+}
+
+// ---- learned proposal ------------------------------------------------------------------------------------------
+extern "C++" {
+namespace {
+
+void ensure_proposals(ps_session* s, Slot& sl) {
+  if (sl.proposal) return;
+  sl.proposal = dalloc<float4>(sl.total);
+  sl.pconf = dalloc<float>(sl.total);
+  cuda_ok(cudaMemsetAsync(sl.proposal, 0, std::max<long long>(sl.total, 1) * sizeof(float4), s->st), "memset");
+  cuda_ok(cudaMemsetAsync(sl.pconf, 0, std::max<long long>(sl.total, 1) * sizeof(float), s->st), "memset");
+  sl.proposal_valid.assign(s->nv, 0);
+}
+
+void enqueue_sweep(ps_session* s, int level, uint32_t view, unsigned short* out, int row_pixels) {
+  PsRun P = base_params(s, level);
+  P.netin = out;
+  P.netin_pitch = row_pixels;
+  P.sweep_ws = 2;
+  set_items(s, P, &view, 0, 1, level, PS_EVAL_PW, PS_EVAL_PH);
+  timed_launch(s, PS_KERNEL_SWEEP, P, [&](const PsRun& q) { return s->L->sweep(q, s->st); }, "sweep kernel");
+}
+
+template <typename T>
+void grow(ps_session* s, T*& buf, size_t& cap, size_t elems) {
+  if (elems <= cap) return;
+  sync(s);  // the previous user of the buffer has finished
+  cudaFree(buf);
+  buf = nullptr;
+  cap = 0;
+  buf = dalloc<T>(elems);
+  cap = elems;
+}
+
+}  // namespace
+}  // extern "C++"
+
+int ps_sweep_volume(ps_session* s, uint32_t level, uint32_t view, void* out, uint32_t row_pixels) {
+  return guard(s, [&] {
+    check_views(s, &view, 1);
+    if (!out) fail(PS_EINVAL, "out is NULL");
+    slot(s, (int)level);
+    if ((int)row_pixels < s->W((int)view, (int)level)) fail(PS_EINVAL, "row_pixels is smaller than the view width");
+    if ((uintptr_t)out % 16) fail(PS_EINVAL, "out must be 16-byte aligned");
+    enqueue_sweep(s, (int)level, view, (unsigned short*)out, (int)row_pixels);
+  });
+}
+
+int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views, size_t n, float conf_threshold,
+               uint64_t* proposed) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (!net) fail(PS_EINVAL, "net is NULL");
+    if (!(conf_threshold >= 0.f && conf_threshold <= 1.f)) fail(PS_EINVAL, "conf_threshold must be in [0, 1]");
+    const int l = (int)level;
+    Slot& sl = slot(s, l);
+    ensure_proposals(s, sl);
+    size_t in_need = 1, out_need = 1;
+    for (size_t i = 0; i < n; ++i) {
+      const size_t hp = round_up(s->H(views[i], l), 8), wp = round_up(s->W(views[i], l), 8);
+      in_need = std::max(in_need, hp * wp * PS_NET_CH_IN);
+      out_need = std::max(out_need, hp * wp * PS_NET_CH_OUT);
+    }
+    grow(s, s->netin, s->netin_cap, in_need);
+    grow(s, s->netout, s->netout_cap, out_need);
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(1);
+    cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
+    for (size_t i = 0; i < n; ++i) {
+      const uint32_t v = views[i];
+      const int w = s->W(v, l), h = s->H(v, l);
+      const int hp = (int)round_up(h, 8), wp = (int)round_up(w, 8);
+      if (hp != h || wp != w)
+        cuda_ok(cudaMemsetAsync(s->netin, 0, (size_t)hp * wp * PS_NET_CH_IN * 2, s->st), "memset");
+      enqueue_sweep(s, l, v, s->netin, wp);
+      ps_session::Pending pd{};
+      if (s->profiling) {
+        cuda_ok(cudaEventCreate(&pd.a), "cudaEventCreate");
+        cuda_ok(cudaEventCreate(&pd.b), "cudaEventCreate");
+        cuda_ok(cudaEventRecord(pd.a, s->st), "cudaEventRecord");
+      }
+      std::string err;
+      const int rc = ps_cnn::forward_on_stream(net, s->netin, 1, hp, wp, s->netout, s->st, &err);
+      if (rc != PS_OK) {
+        if (s->profiling) {
+          cudaEventDestroy(pd.a);
+          cudaEventDestroy(pd.b);
+        }
+        fail(rc, "proposal network: " + err);
+      }
+      const PsLevel& L = s->lvh[v * s->nl + l];
+      const float k[4] = {L.fx, L.fy, L.cx, L.cy};
+      const PsView& vd = s->vdh[v];
+      cuda_ok(ps_cnn::launch_decode(s->netout, wp, h, w, sl.proposal + sl.off[v], sl.pconf + sl.off[v],
+                                    1.0f / vd.dmin, 1.0f / vd.dmax, conf_threshold, k, s->pcount, s->st),
+              "decode kernel");
+      s->launches += ps_cnn::kForwardLaunches + 1;
+      if (s->profiling) {
+        cuda_ok(cudaEventRecord(pd.b, s->st), "cudaEventRecord");
+        pd.kind = PS_KERNEL_NET;
+        pd.persistent = false;
+        s->pending.push_back(pd);
+        s->kind_launches[PS_KERNEL_NET]++;
+      }
+      sl.proposal_valid[v] = 1;
+    }
+    if (proposed) {
+      unsigned long long c = 0;
+      cuda_ok(cudaMemcpyAsync(&c, s->pcount, sizeof c, cudaMemcpyDeviceToHost, s->st), "read proposal count");
+      sync(s);
+      *proposed = c;
+    }
+  });
+}
+
+int ps_proposal_upload(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const float* const* planes) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && !planes) fail(PS_EINVAL, "planes is NULL");
+    Slot& sl = slot(s, (int)level);
+    ensure_proposals(s, sl);
+    for (size_t i = 0; i < n; ++i) {
+      if (!planes[i]) fail(PS_EINVAL, "planes[i] is NULL");
+      const size_t np = (size_t)s->W(views[i], (int)level) * s->H(views[i], (int)level);
+      cuda_ok(cudaMemcpyAsync(sl.proposal + sl.off[views[i]], planes[i], np * sizeof(float4), cudaMemcpyHostToDevice,
+                              s->st),
+              "upload proposal");
+    }
+    sync(s);
+    for (size_t i = 0; i < n; ++i) sl.proposal_valid[views[i]] = 1;
+  });
+}
+
+int ps_proposal_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, float* const* planes,
+                         float* const* conf) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && !planes) fail(PS_EINVAL, "planes is NULL");
+    Slot& sl = slot(s, (int)level);
+    for (size_t i = 0; i < n; ++i)
+      if (!sl.proposal || !sl.proposal_valid[views[i]])
+        fail(PS_EINVAL, "view " + std::to_string(views[i]) + " has no proposal");
+    for (size_t i = 0; i < n; ++i) {
+      const size_t np = (size_t)s->W(views[i], (int)level) * s->H(views[i], (int)level);
+      if (!planes[i]) fail(PS_EINVAL, "planes[i] is NULL");
+      cuda_ok(cudaMemcpyAsync(planes[i], sl.proposal + sl.off[views[i]], np * sizeof(float4), cudaMemcpyDeviceToHost,
+                              s->st),
+              "download proposal");
+      if (conf && conf[i])
+        cuda_ok(cudaMemcpyAsync(conf[i], sl.pconf + sl.off[views[i]], np * sizeof(float), cudaMemcpyDeviceToHost,
+                                s->st),
+                "download confidence");
+    }
+    sync(s);
   });
 }
 

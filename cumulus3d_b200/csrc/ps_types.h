@@ -21,6 +21,14 @@
 // Simple per-pixel kernels (upsample, median, readout, snapshot): 32 × 8 threads.
 #define PS_SIMPLE_BX 32
 #define PS_SIMPLE_BY 8
+// Learned proposal: network input channels (image, PS_SWEEP_PLANES sweep costs, zero padding to a multiple of 16);
+// the same values as the C ABI header.
+#ifndef PS_SWEEP_PLANES
+#define PS_SWEEP_PLANES 32
+#endif
+#ifndef PS_NET_CH_IN
+#define PS_NET_CH_IN 48
+#endif
 
 // One (view, level) image plane.
 struct PsLevel {
@@ -88,5 +96,9 @@ struct PsRun {
   int need_min;              // readout threshold: min_num_consistent
   int mode;                  // evaluate: 1 = run start (init + cost + clear best view), 0 = cost only
   unsigned long long* ncc_count;  // when set, kernels add the number of NCC window evaluations they performed
+  const float4* proposal;  // run start with random init: planes with d > 0 replace the random draw (learned init)
+  unsigned short* netin;   // plane sweep: bf16 network input [rows][netin_pitch][PS_NET_CH_IN] of the run's one view
+  int netin_pitch;         // pixels per row of netin
+  int sweep_ws;            // plane sweep: window step
   PsItem items[PS_MAX_ITEMS];
 };

@@ -105,10 +105,10 @@ class ViewState:
 
 @dataclass
 class RunParams:
-    """RunParams (kernel.rs:173-189)."""
+    """RunParams (kernel.rs:173-189).  random_init: False / True, or PS_INIT_PROPOSAL (2) for the learned init."""
     level: int
     geometric: bool
-    random_init: bool
+    random_init: int
     iterations: int
     run_id: int
     use_prior: bool = False
@@ -372,10 +372,43 @@ class PatchMatchSession:
         return outs
 
     def schedule_resident(self, views: Sequence[int], photometric_iters: int, geometric_rounds: int,
-                          geometric_iters: int, level: int = 0, run_id_base: int = 1, graph: bool = True) -> None:
-        """The whole single-level schedule on resident states (asynchronous); with `graph`, one CUDA-graph launch."""
-        sch = _lib.Schedule(level, photometric_iters, geometric_rounds, geometric_iters, run_id_base, int(graph))
+                          geometric_iters: int, level: int = 0, run_id_base: int = 1, graph: bool = True,
+                          proposal: bool = False) -> None:
+        """The whole single-level schedule on resident states (asynchronous); with `graph`, one CUDA-graph launch.
+        With `proposal`, the photometric run starts from the stored proposals (PS_INIT_PROPOSAL)."""
+        sch = _lib.Schedule(level, photometric_iters, geometric_rounds, geometric_iters, run_id_base, int(graph),
+                            _lib.PS_INIT_PROPOSAL if proposal else _lib.PS_INIT_RANDOM)
         self._check(self.lib.ps_schedule_resident(self.h, _views(views), len(views), C.byref(sch)))
+
+    # ---- learned proposal (no reference counterpart) ----------------------------------------------------------
+    def sweep_volume(self, level: int, view: int, out_ptr: int, row_pixels: int) -> None:
+        """Writes the view's network input (bf16 NHWC, 48 channels) to device memory at `out_ptr` (asynchronous on
+        the session stream)."""
+        self._check(self.lib.ps_sweep_volume(self.h, level, view, C.c_void_p(out_ptr), row_pixels))
+
+    def propose(self, net, level: int, views: Sequence[int], conf_threshold: float = 0.5,
+                count: bool = True) -> Optional[int]:
+        """Sweep + network + decode into the session's proposal store; returns the number of proposed pixels."""
+        n = C.c_uint64()
+        self._check(self.lib.ps_propose(self.h, net.h, level, _views(views), len(views), conf_threshold,
+                                        C.byref(n) if count else None))
+        return int(n.value) if count else None
+
+    def proposal_upload(self, level: int, views: Sequence[int], planes: Sequence[np.ndarray]) -> None:
+        arrs = [np.ascontiguousarray(a, np.float32) for a in planes]
+        pp = (C.POINTER(C.c_float) * max(len(arrs), 1))(*[a.ctypes.data_as(C.POINTER(C.c_float)) for a in arrs])
+        self._check(self.lib.ps_proposal_upload(self.h, level, _views(views), len(views), pp))
+
+    def proposal_download(self, level: int, views: Sequence[int]):
+        """Stored proposals: list of ((h, w, 4) planes, (h, w) confidences)."""
+        outs = []
+        for v in views:
+            w, h = self._size(v, level)
+            outs.append((np.empty((h, w, 4), np.float32), np.empty((h, w), np.float32)))
+        pp = (C.POINTER(C.c_float) * max(len(outs), 1))(*[o[0].ctypes.data_as(C.POINTER(C.c_float)) for o in outs])
+        cp = (C.POINTER(C.c_float) * max(len(outs), 1))(*[o[1].ctypes.data_as(C.POINTER(C.c_float)) for o in outs])
+        self._check(self.lib.ps_proposal_download(self.h, level, _views(views), len(views), pp, cp))
+        return outs
 
     def synchronize(self) -> None:
         self._check(self.lib.ps_synchronize(self.h))

@@ -32,7 +32,7 @@ extern "C" {
 #endif
 
 #define PS_MAX_SOURCES 32 /* crates/cuda/src/kernels/patchmatch.cu:40 (MAXSRC) */
-#define PS_ABI_VERSION 1
+#define PS_ABI_VERSION 2
 
 /* Status codes.  Maps the reference's error kinds: Error::InvalidArgument -> PS_EINVAL,
  * Error::Invariant("CUDA: …") -> PS_ECUDA (crates/cuda/src/patchmatch.rs:234-236),
@@ -162,7 +162,11 @@ typedef struct ps_view_state {
   const float* prior; /* 4*w*h (nx,ny,nz,d) or NULL (= empty) */
 } ps_view_state;
 
-/* RunParams (crates/dense/src/kernel.rs:173-189). */
+/* RunParams (crates/dense/src/kernel.rs:173-189).  random_init: 0 = keep the states' planes, PS_INIT_RANDOM = seeded
+ * random planes (the reference's `true`), PS_INIT_PROPOSAL = the session's learned proposal where one exists and the
+ * same random draw elsewhere (no reference counterpart; see ps_propose). */
+#define PS_INIT_RANDOM 1u
+#define PS_INIT_PROPOSAL 2u
 typedef struct ps_run_params {
   uint32_t level;
   uint32_t geometric;
@@ -262,6 +266,7 @@ typedef struct ps_schedule {
   uint32_t geometric_iters;
   uint32_t run_id_base; /* run ids run_id_base, run_id_base+1, … (RNG keys) */
   uint32_t use_graph;
+  uint32_t init; /* initialisation of the photometric run: PS_INIT_RANDOM or PS_INIT_PROPOSAL */
 } ps_schedule;
 int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch);
 int ps_synchronize(ps_session* s);
@@ -285,13 +290,70 @@ void* ps_session_stream(const ps_session* s);
 int ps_median_filter_inplace_noalloc(int device, float* planes, uint32_t width, uint32_t height, const float* k,
                                      void* stream);
 
+/* ---- learned proposal (no counterpart in the reference) -----------------------------------------------------
+ * A BF16 encoder-decoder network predicts an initial plane and a confidence per pixel from the reference image and a
+ * plane-sweep cost volume.  A run start with random_init = PS_INIT_PROPOSAL takes the proposed plane where the
+ * confidence reached the threshold and the ordinary random draw everywhere else, so plain random initialisation is
+ * the per-pixel fallback.
+ * Network tensors are NHWC in device memory with height and width multiples of 8: input bf16 (raw bits)
+ * [batch][height][width][PS_NET_CH_IN] = (image, PS_SWEEP_PLANES sweep costs, zeros); output f32
+ * [batch][height][width][PS_NET_CH_OUT] = (logit of t = (1/d - 1/dmax) / (1/dmin - 1/dmax), normal xyz (not unit),
+ * logit of the confidence, 3 unused).  Parameters: 12 convolutions 3×3 in the order e0a e0b e1a e1b e2a e2b e3a e3b d2
+ * d1 d0 head with (cin, cout) = (48,32) (32,32) (32,64) (64,64) (64,96) (96,96) (96,128) (128,128) (224,96) (160,64)
+ * (96,32) (32,8); each stores W [cout][9][cin] (tap = 3·(dy+1) + (dx+1)) then b [cout], f32.  A net is not
+ * thread-safe. */
+#define PS_SWEEP_PLANES 32
+#define PS_NET_CH_IN 48
+#define PS_NET_CH_OUT 8
+typedef struct ps_net ps_net;
+/* Seeded He-uniform initialisation on `device`. */
+int ps_net_create(int device, uint64_t seed, ps_net** out);
+void ps_net_destroy(ps_net* net);
+const char* ps_net_last_error(const ps_net* net);
+uint64_t ps_net_num_params(const ps_net* net);
+uint32_t ps_net_step(const ps_net* net); /* AdamW steps taken */
+int ps_net_get_params(ps_net* net, float* host);       /* num_params floats */
+int ps_net_set_params(ps_net* net, const float* host); /* also resets nothing of the optimiser state */
+/* Forward on device buffers, enqueued on `stream` (a cudaStream_t; NULL = the net's own stream, then blocking). */
+int ps_net_forward(ps_net* net, const void* input, uint32_t batch, uint32_t height, uint32_t width, float* out,
+                   void* stream);
+/* One AdamW step (β = 0.9, 0.999, ε = 1e-8; weight decay on weights only) on device buffers: labels f32
+ * [batch][height][width][6] = (t*, normal xyz, valid, depth d*).  Loss per valid pixel |σ(o0) - t*| + (1 - n̂·n*) +
+ * 0.5·BCE(σ(o4), |d - d*| < 0.01·d*), averaged.  lr = 0 computes the loss and gradients only.  grad_out (host,
+ * num_params floats, may be NULL) receives the gradients.  Blocking. */
+int ps_net_train_step(ps_net* net, const void* input, const float* labels, uint32_t batch, uint32_t height,
+                      uint32_t width, float depth_min, float depth_max, float lr, float weight_decay, float* loss,
+                      float* grad_out);
+/* One 3×3 convolution (no bias) on host buffers through the network's kernels, for gradient checks: y = conv(x, w),
+ * dx = conv(dy, flipped wᵀ), dw = Σ dy ⊗ im2col(x).  x, dy: bf16 bits NHWC; w f32 [cout][9][cin] (rounded to bf16);
+ * cin and cout multiples of 8. */
+int ps_net_conv_check(int device, const uint16_t* x, const float* w, const uint16_t* dy, uint32_t batch,
+                      uint32_t height, uint32_t width, uint32_t cin, uint32_t cout, float* y, float* dx, float* dw);
+/* Network input of one view at `level` into device memory `out` (rows of `row_pixels` >= width pixels; the caller
+ * zeroes any padding): the image and PS_SWEEP_PLANES fronto-parallel plane-sweep NCC costs (inverse depths at bin
+ * centres between 1/dmax and 1/dmin; mean over the first two sources; window radius as the session's, step 2).
+ * Asynchronous on the session stream. */
+int ps_sweep_volume(ps_session* s, uint32_t level, uint32_t view, void* out, uint32_t row_pixels);
+/* Sweep + network + decode for `views` at `level`: stores each view's proposal (planes with d = 0 where the
+ * confidence is below conf_threshold) in the session for a later PS_INIT_PROPOSAL run start.  `proposed` (may be
+ * NULL; then asynchronous) receives the number of proposed pixels. */
+int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views, size_t n, float conf_threshold,
+               uint64_t* proposed);
+/* Caller-supplied proposals (host, 4·w·h floats (nx, ny, nz, d), d <= 0 = none) and read-back of the stored ones
+ * (conf may be NULL). */
+int ps_proposal_upload(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const float* const* planes);
+int ps_proposal_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, float* const* planes,
+                         float* const* conf);
+
 /* ---- measurement (no reference counterpart; replaces CUMULUS3D_CUDA_TRACE, crates/cuda/src/patchmatch.rs:780-797) */
 typedef enum ps_kernel_kind {
   PS_KERNEL_HALF = 0,
   PS_KERNEL_EVAL = 1,
   PS_KERNEL_FILTER = 2,
   PS_KERNEL_OTHER = 3,
-  PS_KERNEL_KINDS = 4
+  PS_KERNEL_SWEEP = 4, /* plane sweep of the learned proposal */
+  PS_KERNEL_NET = 5,   /* proposal network forward + decode (one event pair per view) */
+  PS_KERNEL_KINDS = 6
 } ps_kernel_kind;
 /* With profiling on, every launch is bracketed by CUDA events on the session stream and half-step / evaluate /
  * filter launches count the NCC window evaluations they perform (each is (2R/step+1)^2 taps). */

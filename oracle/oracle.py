@@ -36,6 +36,9 @@ def lib() -> C.CDLL:
             "oracle_run": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP, C.c_int]),
             "oracle_run_rows": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP, C.c_int,
                                           C.c_int, C.c_int]),
+            "oracle_run_init": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP,
+                                          C.POINTER(C.POINTER(C.c_float)), C.c_int, C.c_int, C.c_int]),
+            "oracle_sweep": (C.c_int, [_KI, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]),
             "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int]),
             "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
@@ -80,14 +83,31 @@ def _chk(rc: int, what: str):
 
 
 def run(inp: KernelInput, views: Sequence[int], states: List[ViewState], p: RunParams,
-        snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None, rows=None) -> None:
+        snapshot: Optional[DepthSnapshot] = None, threads: Optional[int] = None, rows=None,
+        proposals: Optional[Sequence[np.ndarray]] = None) -> None:
     """PatchMatchSession::run restated on the CPU (states updated in place).  `rows` = (y0, y1) restricts the
-    work to a band of rows (timing samples only)."""
+    work to a band of rows (timing samples only).  With random_init = PS_INIT_PROPOSAL, `proposals[i]` (h, w, 4)
+    f32 planes replace the random draw where d > 0 (the engine's learned init)."""
     ci, keep = CInput(inp), []
     rp = p.c()
     y0, y1 = rows if rows is not None else (0, 0)
-    _chk(lib().oracle_run_rows(C.byref(ci.c), _views(views), len(views), c_states(states, keep), C.byref(rp),
-                               c_snapshot(snapshot, keep), _threads(threads), y0, y1), "run")
+    pp = None
+    if proposals is not None:
+        arrs = [np.ascontiguousarray(a, np.float32) for a in proposals]
+        keep.append(arrs)
+        pp = (C.POINTER(C.c_float) * max(len(arrs), 1))(*[a.ctypes.data_as(C.POINTER(C.c_float)) for a in arrs])
+    _chk(lib().oracle_run_init(C.byref(ci.c), _views(views), len(views), c_states(states, keep), C.byref(rp),
+                               c_snapshot(snapshot, keep), pp, _threads(threads), y0, y1), "run")
+
+
+def sweep(inp: KernelInput, level: int, view: int, threads: Optional[int] = None) -> np.ndarray:
+    """The plane-sweep network input of one view: (h, w, 48) uint16 bf16 bits (image, 32 costs, zeros)."""
+    ci = CInput(inp)
+    lv = inp.views[view].levels[level]
+    h, w = lv.pixels.shape[:2]
+    out = np.zeros((h, w, _lib.PS_NET_CH_IN), np.uint16)
+    _chk(lib().oracle_sweep(C.byref(ci.c), level, view, out.ctypes.data, w, _threads(threads)), "sweep")
+    return out
 
 
 def evaluate(inp: KernelInput, level: int, views: Sequence[int], states: List[ViewState], geometric: bool = False,

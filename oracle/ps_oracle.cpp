@@ -223,6 +223,7 @@ struct Run {
   int geometric, run_id, t, color, topk, use_prior;
   float tau_good, eps, phi;
   const std::vector<std::vector<float>>* snap;  // per view (empty = absent)
+  const float* proposal = nullptr;  // learned init: 4 floats per pixel, d > 0 replaces the random draw
 };
 
 template <class T>
@@ -672,6 +673,10 @@ void eval_pixel(const Run& r, State& st, int x, int y, int mode, int random_init
     float d = random_depth(s, vd.dmin, vd.dmax);
     V3<float> n = random_normal(s, ray);
     h = {n.x, n.y, n.z, d};
+    if (r.proposal && r.proposal[4 * pix + 3] > 0.f) {
+      const float* q = r.proposal + 4 * pix;
+      h = {q[0], q[1], q[2], q[3]};
+    }
     st.plane[pix] = h;
   }
   float c = 2.f;
@@ -769,8 +774,9 @@ extern "C" {
 // then `iterations` × (colour 0, colour 1) half steps.
 // Rows [y0, y1) only (y1 <= 0: all rows): the timing sample of the CPU baseline runs a band of rows, whose cost is
 // proportional to its pixel count; parity tests always run every row.
-int oracle_run_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
-                    const ps_run_params* p, const ps_depth_snapshot* snap, int threads, int y0, int y1) {
+int oracle_run_init(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
+                    const ps_run_params* p, const ps_depth_snapshot* snap, const float* const* proposals, int threads,
+                    int y0, int y1) {
   Scene sc;
   if (!load_scene(in, sc) || !p) return PS_EINVAL;
   if (p->geometric && !snap) return PS_EINVAL;
@@ -791,6 +797,7 @@ int oracle_run_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, 
     r.t = 0;
     r.color = 0;
     r.tau_good = r.eps = r.phi = 0;
+    r.proposal = (p->random_init == PS_INIT_PROPOSAL && proposals) ? proposals[i] : nullptr;
     const int ya = std::max(y0, 0), yb = y1 > 0 ? std::min(y1, st.h) : st.h;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int y = ya; y < yb; ++y)
@@ -810,9 +817,61 @@ int oracle_run_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, 
   return PS_OK;
 }
 
+int oracle_run_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
+                    const ps_run_params* p, const ps_depth_snapshot* snap, int threads, int y0, int y1) {
+  return oracle_run_init(in, views, n, states, p, snap, nullptr, threads, y0, y1);
+}
+
 int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_view_state* states,
                const ps_run_params* p, const ps_depth_snapshot* snap, int threads) {
   return oracle_run_rows(in, views, n, states, p, snap, threads, 0, 0);
+}
+
+// Plane-sweep network input of one view (the engine's ps_sweep_volume; no reference counterpart): per pixel, bf16
+// bits of [image, 32 costs, 15 zeros] where cost k is the mean over the first min(2, nsrc) sources of the NCC cost of
+// the fronto-parallel plane (0, 0, -1, 1/i_k), i_k = fma((2k+1)/64, 1/dmin - 1/dmax, 1/dmax), window radius as the
+// session's and step 2 (2 where the homography fails).  Rows of `row_pixels` pixels.
+int oracle_sweep(const ps_kernel_input* in, uint32_t level, uint32_t view, uint16_t* out, uint32_t row_pixels,
+                 int threads) {
+  Scene sc;
+  if (!load_scene(in, sc) || view >= sc.v.size() || (int)level >= sc.nl || !out) return PS_EINVAL;
+  sc.ws = 2;
+  sc.wn = (2 * sc.wr) / sc.ws + 1;
+  set_threads(threads);
+  const View& vd = sc.v[view];
+  const Img& R = sc.L((int)view, (int)level);
+  if ((int)row_pixels < R.w) return PS_EINVAL;
+  const int nsrc = (int)vd.pairs.size(), nuse = std::min(nsrc, 2);
+  const float inear = 1.0f / vd.dmin, ifar = 1.0f / vd.dmax;
+  auto bf16 = [](float v) -> uint16_t {  // round to nearest even (finite values)
+    uint32_t u;
+    memcpy(&u, &v, 4);
+    u += 0x7FFFu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+  };
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int y = 0; y < R.h; ++y)
+    for (int x = 0; x < R.w; ++x) {
+      uint16_t* o = out + ((size_t)y * row_pixels + x) * PS_NET_CH_IN;
+      const RS<float> rs = ref_stats<float>(sc, R, x, y);
+      o[0] = bf16(R.at(x, y));
+      for (int k = 0; k < PS_SWEEP_PLANES; ++k) {
+        const float id = std::fma((float)(2 * k + 1) * (1.0f / 64.0f), inear - ifar, ifar);
+        const P4 h = {0.0f, 0.0f, -1.0f, 1.0f / id};
+        float c = 0.0f;
+        for (int j = 0; j < nuse; ++j) {
+          const Img& S = sc.L(vd.pairs[j].src, (int)level);
+          float H[9];
+          c += homography<float>(R, vd.lp[(size_t)level * nsrc + j], (float)x, (float)y, h, H)
+                   ? ncc_cost<float>(sc, R, rs, S, H, x, y)
+                   : 2.0f;
+        }
+        c = nuse == 2 ? c * 0.5f : (nuse == 1 ? c : 2.0f);
+        o[1 + k] = bf16(c);
+      }
+      for (int k = 1 + PS_SWEEP_PLANES; k < PS_NET_CH_IN; ++k) o[k] = 0;
+    }
+  return PS_OK;
 }
 
 int oracle_evaluate(const ps_kernel_input* in, uint32_t level, const uint32_t* views, size_t n,

@@ -41,7 +41,7 @@ STRUCTS = {
     "ps_options": _lib.Options, "ps_pm_params": _lib.PmParams, "ps_filter_params": _lib.FilterParams,
     "ps_level_image": _lib.LevelImage, "ps_pair_geometry": _lib.PairGeometry, "ps_kernel_view": _lib.KernelView,
     "ps_kernel_input": _lib.KernelInput, "ps_view_state": _lib.ViewState, "ps_run_params": _lib.RunParams,
-    "ps_depth_snapshot": _lib.DepthSnapshot,
+    "ps_depth_snapshot": _lib.DepthSnapshot, "ps_schedule": _lib.Schedule,
 }
 
 
@@ -86,7 +86,15 @@ def test_null_arguments_rejected_without_device():
     assert lib.ps_end(None) == _lib.PS_EINVAL
     assert lib.ps_run(None, None, 0, None, None, None) == _lib.PS_EINVAL
     assert lib.ps_last_error(None) == b"session is NULL"
-    assert lib.ps_abi_version() == 1
+    assert lib.ps_abi_version() == 2
+    # learned-proposal entry points
+    assert lib.ps_net_create(0, 1, None) == _lib.PS_EINVAL
+    assert lib.ps_net_num_params(None) == 0
+    assert lib.ps_net_last_error(None) == b"net is NULL"
+    assert lib.ps_net_forward(None, None, 1, 8, 8, None, None) == _lib.PS_EINVAL
+    assert lib.ps_net_train_step(None, None, None, 1, 8, 8, 25.0, 60.0, 0.0, 0.0, None, None) == _lib.PS_EINVAL
+    assert lib.ps_sweep_volume(None, 0, 0, None, 0) == _lib.PS_EINVAL
+    assert lib.ps_propose(None, None, 0, None, 0, 0.5, None) == _lib.PS_EINVAL
 
 
 def test_defaults_match_reference():

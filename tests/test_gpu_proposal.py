@@ -1,0 +1,205 @@
+"""Learned proposal on the GPU: network kernels against the FP64 oracle, the plane sweep and the proposal-gated run
+start bit for bit against the CPU oracle, the random-init fallback, the propose pipeline and training.
+
+Tolerances: the sweep and every PatchStereo run are integer-exact (zero tolerance, parity build).  The network runs in
+BF16 with FP32 accumulation: a single convolution is compared with FP64 at 1e-5 of the output's max magnitude (1e-4
+for the weight gradient, a sum over all pixels); whole-network gradients at 3 % relative L2 per layer against an
+oracle that rounds to bf16 where the GPU stores bf16.
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import cnn_oracle as O
+from oracle import oracle
+from cumulus3d_b200 import _lib, proposal, scenes
+from cumulus3d_b200.patchstereo import PatchMatchBackend, RunParams, ViewState
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16(rng, shape, lo=-1.0, hi=1.0):
+    return O.bf16_bits(rng.uniform(lo, hi, shape))
+
+
+@pytest.mark.parametrize("shape", [(2, 9, 13, 48, 32), (1, 8, 8, 32, 8), (1, 12, 20, 224, 96), (3, 5, 7, 16, 64)])
+def test_conv_kernels_match_fp64(shape):
+    b, h, w, ci, co = shape
+    rng = np.random.default_rng(sum(shape))
+    x = _bf16(rng, (b, h, w, ci))
+    dy = _bf16(rng, (b, h, w, co))
+    wt = rng.uniform(-0.3, 0.3, (co, 9, ci)).astype(np.float32)
+    y, dx, dw = proposal.conv_check(x, wt, dy)
+    xf, dyf, wf = O.from_bf16_bits(x), O.from_bf16_bits(dy), O.bf16_round(wt)
+    y_ref = O.conv(xf, wf)
+    dx_ref, dw_ref, _ = O.conv_grads(xf, wf, dyf)
+    assert np.abs(y - y_ref).max() <= 1e-5 * np.abs(y_ref).max()
+    assert np.abs(dx - dx_ref).max() <= 1e-5 * np.abs(dx_ref).max()
+    assert np.abs(dw - dw_ref).max() <= 1e-4 * np.abs(dw_ref).max()
+
+
+def _labels(rng, b, h, w, dr=(25.0, 60.0)):
+    lab = np.zeros((b, h, w, 6), np.float32)
+    lab[..., 0] = rng.uniform(0, 1, (b, h, w))
+    n = rng.normal(size=(b, h, w, 3))
+    lab[..., 1:4] = n / np.linalg.norm(n, axis=-1, keepdims=True)
+    lab[..., 4] = rng.random((b, h, w)) < 0.8
+    d = 1.0 / (1.0 / dr[1] + lab[..., 0] * (1.0 / dr[0] - 1.0 / dr[1]))
+    lab[..., 5] = d * (1 + rng.normal(0, 0.01, (b, h, w)))
+    lab[lab[..., 4] == 0] = 0
+    return lab
+
+
+def test_network_gradients_match_fp64_oracle():
+    rng = np.random.default_rng(7)
+    b, h, w = 2, 16, 24
+    xb = O.bf16_bits(np.concatenate([rng.uniform(0, 1, (b, h, w, 33)), np.zeros((b, h, w, 15))], axis=-1))
+    lab = _labels(rng, b, h, w)
+    net = proposal.ProposalNet(0, seed=3)
+    x_t = torch.from_numpy(xb.view(np.int16)).cuda()
+    lab_t = torch.from_numpy(lab).cuda()
+    loss, g = net.train_step(x_t, lab_t, (25.0, 60.0), lr=0.0, grads=True)
+    params = net.get_params()
+    out = torch.empty((b, h, w, 8), dtype=torch.float32, device="cuda")
+    net.forward(x_t, out)
+    torch.cuda.synchronize()
+    a = O.forward(O.split(params), O.from_bf16_bits(xb), bf16=True)
+    np.testing.assert_allclose(out.cpu().numpy(), a["o"], rtol=0, atol=2e-2 * np.abs(a["o"]).max())
+    loss_ref, g_o = O.loss_and_grad(a["o"], lab.astype(np.float64), (25.0, 60.0))
+    assert abs(loss - loss_ref) <= 1e-3 * abs(loss_ref)
+    g_ref = O.backward(O.split(params), a, g_o, bf16=True)
+    o = 0
+    for (ci, co), name in zip(proposal.LAYERS, proposal.LAYER_NAMES):
+        n = co * 9 * ci + co
+        gg, rr = g[o:o + n], g_ref[o:o + n]
+        rel = np.linalg.norm(gg - rr) / max(np.linalg.norm(rr), 1e-30)
+        assert rel < 3e-2, (name, rel)
+        o += n
+    cos = float(g @ g_ref / (np.linalg.norm(g) * np.linalg.norm(g_ref)))
+    assert cos > 0.999
+    net.close()
+
+
+@pytest.mark.parametrize("wr,size", [(3, (64, 48)), (6, (80, 64))])
+def test_sweep_bitwise_vs_oracle(wr, size):
+    wl = scenes.workload_small(size[0], size[1], views=3, window_radius=wr, seed=11)
+    be = PatchMatchBackend(0, math="parity")
+    w, h = size
+    with be.begin(wl.input) as s:
+        for v in range(3):
+            buf = torch.zeros((h, w, 48), dtype=torch.int16, device="cuda")
+            s.sweep_volume(0, v, buf.data_ptr(), w)
+            s.synchronize()
+            got = buf.cpu().numpy().view(np.uint16)
+            want = oracle.sweep(wl.input, 0, v)
+            np.testing.assert_array_equal(got, want)
+    be.close()
+
+
+def _proposals(wl, seed, keep=0.5):
+    rng = np.random.default_rng(seed)
+    out = []
+    for v, cam in enumerate(wl.cams):
+        p = np.zeros((cam.height, cam.width, 4), np.float32)
+        n = wl.gt_normal[v].astype(np.float32)
+        fx, fy, cx, cy = cam.k
+        ys, xs = np.mgrid[0:cam.height, 0:cam.width]
+        ray = np.stack([(xs - cx) / fx, (ys - cy) / fy, np.ones_like(xs, dtype=np.float64)], -1)
+        n = np.where(((n * ray).sum(-1) > 0)[..., None], -n, n)  # facing the camera
+        p[..., :3] = n
+        p[..., 3] = wl.gt_depth[v] * (1 + rng.normal(0, 0.003, wl.gt_depth[v].shape))
+        p[rng.random((cam.height, cam.width)) > keep] = 0.0
+        out.append(p)
+    return out
+
+
+def test_proposal_init_bitwise_vs_oracle():
+    wl = scenes.workload_small(96, 64, views=3, window_radius=3, seed=5)
+    props = _proposals(wl, 1)
+    views = [0, 1, 2]
+    be = PatchMatchBackend(0, math="parity")
+    st = [ViewState.new(c.width, c.height) for c in wl.cams]
+    with be.begin(wl.input) as s:
+        s.proposal_upload(0, views, props)
+        s.run(views, st, RunParams(0, False, _lib.PS_INIT_PROPOSAL, 2, 1))
+    be.close()
+    ref = [ViewState.new(c.width, c.height) for c in wl.cams]
+    oracle.run(wl.input, views, ref, RunParams(0, False, _lib.PS_INIT_PROPOSAL, 2, 1), proposals=props)
+    for a, b in zip(st, ref):
+        np.testing.assert_array_equal(a.depth, b.depth)
+        np.testing.assert_array_equal(a.normal, b.normal)
+        np.testing.assert_array_equal(a.cost, b.cost)
+
+
+def test_empty_proposal_falls_back_to_random_init_bitwise():
+    """Where no plane is proposed the run start draws exactly the plain random hypothesis."""
+    wl = scenes.workload_small(96, 64, views=3, window_radius=3, seed=6)
+    views = [0, 1, 2]
+    empty = [np.zeros((c.height, c.width, 4), np.float32) for c in wl.cams]
+    be = PatchMatchBackend(0, math="parity")
+    a = [ViewState.new(c.width, c.height) for c in wl.cams]
+    b = [ViewState.new(c.width, c.height) for c in wl.cams]
+    with be.begin(wl.input) as s:
+        s.run(views, a, RunParams(0, False, True, 2, 1))
+        s.proposal_upload(0, views, empty)
+        s.run(views, b, RunParams(0, False, _lib.PS_INIT_PROPOSAL, 2, 1))
+        with pytest.raises(_lib.PsError):  # level without proposals
+            s.run_resident([0], RunParams(0, False, 3, 1, 1))
+    be.close()
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x.depth, y.depth)
+        np.testing.assert_array_equal(x.normal, y.normal)
+
+
+def test_propose_pipeline_and_learned_run_vs_oracle():
+    """ps_propose = sweep -> network -> decode (checked against the same steps done separately), and the schedule's
+    learned run start from those proposals equals the oracle's run from the same proposals bit for bit."""
+    wl = scenes.workload_small(100, 60, views=3, window_radius=3, seed=9)  # sizes not multiples of 8: padded input
+    views = [0, 1, 2]
+    net = proposal.ProposalNet(0, seed=5)
+    be = PatchMatchBackend(0, math="parity")
+    st = [ViewState.new(c.width, c.height) for c in wl.cams]
+    with be.begin(wl.input) as s:
+        n_all = s.propose(net, 0, views, conf_threshold=0.0)
+        props = s.proposal_download(0, views)
+        assert n_all == sum(int((p[..., 3] > 0).sum()) for p, _ in props)
+        assert n_all > 0.5 * sum(c.width * c.height for c in wl.cams)
+        # the same steps by hand for view 1: sweep into a padded buffer, forward, decode on the host
+        w, h = wl.cams[1].width, wl.cams[1].height
+        hp, wp = (h + 7) // 8 * 8, (w + 7) // 8 * 8
+        xin = torch.zeros((1, hp, wp, 48), dtype=torch.int16, device="cuda")
+        s.sweep_volume(0, 1, xin.data_ptr(), wp)
+        s.synchronize()
+        out = torch.empty((1, hp, wp, 8), dtype=torch.float32, device="cuda")
+        net.forward(xin, out)
+        torch.cuda.synchronize()
+        o = out.cpu().numpy()[0, :h, :w].astype(np.float64)
+        conf = 1 / (1 + np.exp(-o[..., 4]))
+        np.testing.assert_allclose(props[1][1], conf, rtol=0, atol=1e-5)
+        t = 1 / (1 + np.exp(-o[..., 0]))
+        d = 1 / (1 / 60.0 + t * (1 / 25.0 - 1 / 60.0))
+        m = props[1][0][..., 3] > 0
+        np.testing.assert_allclose(props[1][0][..., 3][m], d[m], rtol=1e-5)
+        assert s.propose(net, 0, views, conf_threshold=1.0) == 0
+        # learned schedule run start from the stored proposals (threshold 0.5)
+        s.propose(net, 0, views, conf_threshold=0.5)
+        props = [p for p, _ in s.proposal_download(0, views)]
+        s.run(views, st, RunParams(0, False, _lib.PS_INIT_PROPOSAL, 1, 1))
+    be.close()
+    net.close()
+    ref = [ViewState.new(c.width, c.height) for c in wl.cams]
+    oracle.run(wl.input, views, ref, RunParams(0, False, _lib.PS_INIT_PROPOSAL, 1, 1), proposals=props)
+    for a, b in zip(st, ref):
+        np.testing.assert_array_equal(a.depth, b.depth)
+        np.testing.assert_array_equal(a.normal, b.normal)
+
+
+def test_training_reduces_loss():
+    data = proposal.make_training_set(n_scenes=12, seed=500, crop=64, group=12, log=None)
+    assert data.valid_fraction > 0.2
+    net = proposal.ProposalNet(0, seed=2)
+    losses = proposal.train(net, data, steps=60, batch=4, lr=1e-3, log=None)
+    assert all(np.isfinite(losses))
+    assert np.mean(losses[-5:]) < 0.85 * np.mean(losses[:5]), (losses[:5], losses[-5:])
+    assert net.step == 60
+    net.close()

@@ -234,6 +234,8 @@ def bench_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    if not args.no_learned and not shard_job:
+        res["learned"] = learned_leg(args, wl, sess, stream, mine, value, ms_step, barrier, local)
     sess.close()
     # ---- e2e through the host-buffer C ABI (session begin uploads the images) ----
     if not args.no_e2e:
@@ -248,6 +250,105 @@ def bench_ours(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return res
+
+
+def net_flop_per_pixel():
+    """Multiply-adds ×2 of one forward pass per full-resolution pixel (level l holds 4^-l of the pixels)."""
+    from cumulus3d_b200.proposal import LAYERS
+    level = (0, 0, 1, 1, 2, 2, 3, 3, 2, 1, 0, 0)
+    return sum(2 * 9 * ci * co / 4 ** lv for (ci, co), lv in zip(LAYERS, level))
+
+
+def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, local):
+    """The learned-init schedule on the same resident session: ps_propose (plane sweep + proposal network + decode)
+    then the schedule with `--learned-iters` photometric iterations from the proposals (random init where the
+    confidence is below 0.5), the same geometric round, filter and readout.  Timed like the plain step; accuracy is
+    the agreement of the final filtered depth with the plain schedule's (within 1 % depth on the pixels the plain
+    result keeps), next to the plain schedule's agreement with itself under another RNG seed and to a plain schedule
+    shortened to the same iteration count."""
+    import torch
+    from cumulus3d_b200 import _lib, proposal
+
+    net = proposal.ProposalNet(local, weights=proposal.DEFAULT_WEIGHTS)
+    k = args.learned_iters
+    plain_depth = np.stack([o.depth for o in sess.readout_resident(mine)])  # the last plain step's result
+
+    def depth():
+        return np.stack([o.depth for o in sess.readout_resident(mine)])
+
+    def timed(fn, warm, steps):
+        for _ in range(warm):
+            fn()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        sess.synchronize()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def learned_step():
+        sess.propose(net, 0, mine, proposal.CONF_THRESHOLD, count=False)
+        sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters, graph=not args.no_graph,
+                               proposal=True)
+
+    sess.set_profiling(True)  # per-launch events for the sweep and network shares
+    sess.reset_stats()
+    ms_learned = timed(learned_step, args.warmup, args.steps)
+    net_stats = sess.kernel_stats(_lib.PS_KERNEL_NET)
+    sweep_stats = sess.kernel_stats(_lib.PS_KERNEL_SWEEP)
+    sess.set_profiling(False)
+    learned_depth = depth()
+    ms_short = timed(lambda: sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters,
+                                                     graph=not args.no_graph), 1, 2)
+    short_depth = depth()
+    sess.schedule_resident(mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters, run_id_base=101,
+                           graph=False)
+    seed_depth = depth()
+    ref_valid = plain_depth > 0
+
+    def agree(d):
+        return round(float((np.abs(d - plain_depth) <= 0.01 * plain_depth)[ref_valid].mean()), 4)
+
+    steps_total = args.warmup + args.steps
+    net_ms = net_stats["ms"] / max(net_stats["launches"], 1)
+    px = wl.cams[mine[0]].width * wl.cams[mine[0]].height
+    pad_px = ((wl.cams[mine[0]].height + 7) // 8 * 8) * ((wl.cams[mine[0]].width + 7) // 8 * 8)
+    flop = net_flop_per_pixel() * pad_px
+    peaks = _peaks()
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    achieved = flop / (net_ms / 1e3) / 1e12 if net_ms > 0 else float("nan")
+    net.close()
+    n = len(mine)
+    return {
+        "schedule": f"propose (plane sweep + network + decode) + {k} photometric from the proposal + "
+                    f"{wl.geometric_rounds}x{wl.geometric_iters} geometric + filter",
+        "value": round(n / (ms_learned / 1e3), 3), "unit": "views/s", "ms_per_step": round(ms_learned, 2),
+        "vs_plain": round(ms_step_ratio(plain_ms, ms_learned), 3),
+        "propose_ms_per_view": round((net_stats["ms"] + sweep_stats["ms"]) / max(net_stats["launches"], 1), 3),
+        "sweep_ms_per_view": round(sweep_stats["ms"] / max(sweep_stats["launches"], 1), 3),
+        "net_ms_per_view": round(net_ms, 3),
+        "accuracy": {"agree_with_plain": agree(learned_depth), "plain_other_seed": agree(seed_depth),
+                     "coverage": round(float((learned_depth > 0).mean()), 4),
+                     "coverage_plain": round(float(ref_valid.mean()), 4),
+                     "definition": "fraction of the plain schedule's valid pixels whose final depth is within 1 % "
+                                   "of it; the plain schedule rerun with another RNG seed sets the floor"},
+        "plain_same_iterations": {"value": round(n / (ms_short / 1e3), 3), "ms_per_step": round(ms_short, 2),
+                                  "agree_with_plain": agree(short_depth),
+                                  "coverage": round(float((short_depth > 0).mean()), 4)},
+        "net_roofline": {"bound": "tensor", "kernel": "proposal network forward (12 conv layers, mma.sync bf16)",
+                         "achieved": round(achieved, 2), "peak": bf16_peak, "unit": "TFLOP/s",
+                         "frac": round(achieved / bf16_peak, 4), "peak_source": "MEASURED_PEAKS.json bf16_tflops "
+                         "(measured)" if "bf16_tflops" in peaks else "fallback 1590",
+                         "flop_per_view": round(flop / 1e9, 1), "unit_flop": "GFLOP"},
+        "timed_steps": args.steps, "warmup": args.warmup, "steps_total": steps_total,
+    }
+
+
+def ms_step_ratio(plain_ms, other_ms):
+    return plain_ms / other_ms
 
 
 def e2e_leg(args, wl, be, mine, world, rank, local, multi, views_total):
@@ -372,6 +473,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="issue the schedule's launches directly (no CUDA graph)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-init schedule")
+    ap.add_argument("--learned-iters", type=int, default=3,
+                    help="photometric iterations of the learned-init schedule")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

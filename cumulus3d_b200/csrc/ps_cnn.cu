@@ -452,8 +452,8 @@ struct Net {
   bf16* wb = nullptr;  // BF16 copy of the parameters (the forward pass reads weights from here, biases from w)
   bf16* wt = nullptr;  // flipped weights of one layer (data gradient)
   int step = 0;
-  cudaStream_t st = nullptr;     // the net's own stream (training, host-buffer calls)
-  cudaStream_t last = nullptr;   // stream of the last call that used the workspace
+  cudaStream_t st = nullptr;     // the net's own stream (training, calls without a stream)
+  cudaEvent_t ws_done = nullptr; // recorded after every use of the workspace, on the stream of that use
   size_t ws_bytes = 0;
   char* ws = nullptr;            // activation (and gradient) workspace
   float* stats = nullptr;        // loss sum, valid count (loss kernel), valid count (count kernel)
@@ -502,8 +502,10 @@ struct Acts {
       *g_p1, *g_a0;
 };
 
-// Carves the workspace into the buffers of one pass (x and o only when the caller does not supply them); grows it
-// after the previous user's work has finished.
+// Carves the workspace into the buffers of one pass on stream `st` (x and o only when the caller does not supply
+// them).  The pass is ordered after the previous use of the workspace (possibly on another stream) through the
+// ws_done event; growing the workspace waits for that use to finish on the host.  The caller records ws_done on `st`
+// after its last launch (end_use).
 void carve(Net& n, int B, int H, int W, Acts* A, bool grads, bool own_io, cudaStream_t st) {
   const long long P0 = (long long)B * H * W, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
   struct Item {
@@ -558,20 +560,22 @@ void carve(Net& n, int B, int H, int W, Acts* A, bool grads, bool own_io, cudaSt
   size_t total = 0;
   for (auto& i : it) total += (i.bytes + 255) & ~(size_t)255;
   if (total > n.ws_bytes) {
-    if (n.last) ck(cudaStreamSynchronize(n.last), "sync before workspace growth");
+    ck(cudaEventSynchronize(n.ws_done), "wait for the workspace");
     if (n.ws) cudaFree(n.ws);
     n.ws = nullptr;
     n.ws_bytes = 0;
     ck(cudaMalloc(&n.ws, total), "cudaMalloc workspace");
     n.ws_bytes = total;
   }
-  n.last = st;
+  ck(cudaStreamWaitEvent(st, n.ws_done, 0), "order after the previous workspace use");
   size_t o = 0;
   for (auto& i : it) {
     *i.p = n.ws + o;
     o += (i.bytes + 255) & ~(size_t)255;
   }
 }
+
+void end_use(Net& n, cudaStream_t st) { ck(cudaEventRecord(n.ws_done, st), "record workspace use"); }
 
 void conv_launch(const ConvArgs& a, cudaStream_t st) {
   const long long M = (long long)a.B * a.H * a.W;
@@ -765,6 +769,7 @@ int forward_on_stream(ps_net* pn, const void* in, int B, int H, int W, float* ou
     a.x = (bf16*)in;
     a.o = out;
     forward(n, a, B, H, W, st);
+    end_use(n, st);
   });
   if (rc != PS_OK && err) *err = n.err;
   return rc;
@@ -805,6 +810,7 @@ int ps_net_create(int device, uint64_t seed, ps_net** out) {
     }
     n.nparam = off;
     ck(cudaStreamCreateWithFlags(&n.st, cudaStreamNonBlocking), "cudaStreamCreate");
+    ck(cudaEventCreateWithFlags(&n.ws_done, cudaEventDisableTiming), "cudaEventCreate");
     ck(cudaMalloc(&n.w, off * 4), "cudaMalloc");
     ck(cudaMalloc(&n.g, off * 4), "cudaMalloc");
     ck(cudaMalloc(&n.m, off * 4), "cudaMalloc");
@@ -841,7 +847,7 @@ void ps_net_destroy(ps_net* pn) {
   Net& n = pn->n;
   if (cudaSetDevice(n.device) == cudaSuccess) {
     if (n.st) cudaStreamSynchronize(n.st);
-    if (n.last && n.last != n.st) cudaStreamSynchronize(n.last);
+    if (n.ws_done) cudaEventSynchronize(n.ws_done);  // a use on a caller's stream (that stream may be gone by now)
     cudaFree(n.w);
     cudaFree(n.g);
     cudaFree(n.m);
@@ -851,6 +857,7 @@ void ps_net_destroy(ps_net* pn) {
     cudaFree(n.ws);
     cudaFree(n.stats);
     if (n.st) cudaStreamDestroy(n.st);
+    if (n.ws_done) cudaEventDestroy(n.ws_done);
   }
   cudaGetLastError();
   delete pn;
@@ -872,7 +879,7 @@ int ps_net_set_params(ps_net* pn, const float* host) {
   if (!pn || !host) return PS_EINVAL;
   return guard(pn->n, [&] {
     ck(cudaStreamSynchronize(pn->n.st), "sync");
-    if (pn->n.last) ck(cudaStreamSynchronize(pn->n.last), "sync");
+    ck(cudaEventSynchronize(pn->n.ws_done), "sync");  // parameters are read by passes on callers' streams too
     upload_params(pn->n, host);
   });
 }
@@ -898,6 +905,7 @@ int ps_net_train_step(ps_net* pn, const void* input, const float* labels, uint32
     k_loss<<<blocks(P0), 256, 0, st>>>(a.o, labels, a.g_o, n.stats, P0, 1.f, 1.f / depth_min, 1.f / depth_max);
     k_scale_grad<<<blocks(P0 * 8), 256, 0, st>>>(a.g_o, P0 * 8, n.stats + 2);
     backward(n, a, B, H, W, st);
+    end_use(n, st);
     ck(cudaFreeAsync(a.o, st), "cudaFreeAsync");
     if (grad_out) ck(cudaMemcpyAsync(grad_out, n.g, n.nparam * 4, cudaMemcpyDeviceToHost, st), "gradients");
     if (lr > 0.f) {
@@ -931,6 +939,7 @@ int ps_net_forward(ps_net* pn, const void* input, uint32_t B, uint32_t H, uint32
     a.x = (bf16*)input;
     a.o = out;
     forward(n, a, B, H, W, st);
+    end_use(n, st);
     if (!stream) ck(cudaStreamSynchronize(st), "sync");
   });
 }

@@ -260,6 +260,7 @@ def make_training_set(n_scenes: int = 300, seed: int = 1000, crop: int = 256, de
 
     dev = torch.device("cuda", device)
     xs = torch.empty((n_scenes, crop, crop, _lib.PS_NET_CH_IN), dtype=torch.int16, device=dev)
+    torch.cuda.synchronize(dev)  # the session stream that fills xs does not wait for torch's stream
     labs = np.zeros((n_scenes, crop, crop, 6), np.float32)
     t_render = t_label = 0.0
     be = PatchMatchBackend(device, math="parity")

@@ -86,6 +86,25 @@ class Schedule(C.Structure):
                 ("init", C.c_uint32)]
 
 
+class PostParams(C.Structure):
+    """PostParams (crates/dense/src/postproc.rs:41-74), speckle removal part."""
+    _fields_ = [("remove_speckles", C.c_uint32), ("speckle_rel_depth", C.c_float), ("speckle_min_area_frac", C.c_double),
+                ("speckle_keep_cost", C.c_float)]
+
+
+class FusionParams(C.Structure):
+    """FusionParams of consistency fusion (crates/dense/src/params.rs:286-351)."""
+    _fields_ = [("min_consistent_views", C.c_uint32), ("consistency_num_images", C.c_uint32), ("mark_used", C.c_uint32),
+                ("mark_radius", C.c_uint32), ("inverse_variance", C.c_uint32), ("reserved", C.c_uint32),
+                ("sigma_px0", C.c_double), ("sigma_px_slope", C.c_double), ("max_reproj_error", C.c_double),
+                ("max_depth_error", C.c_double), ("max_normal_error_deg", C.c_double)]
+
+
+class FusionView(C.Structure):
+    _fields_ = [("k", C.c_double * 4), ("r", C.c_double * 9), ("t", C.c_double * 3), ("baseline", C.c_double),
+                ("image_id", C.c_uint32), ("num_overlap", C.c_uint32), ("overlap", C.POINTER(C.c_uint32))]
+
+
 class DepthSnapshot(C.Structure):
     _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
                 ("maps", C.POINTER(C.POINTER(C.c_float)))]
@@ -133,6 +152,17 @@ SIGNATURES = {
                                   C.POINTER(C.c_uint64)]),
     "ps_reset_stats": (C.c_int, [_P]),
     "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    # post-processing, fusion, output
+    "ps_post_params_default": (None, [C.POINTER(PostParams)]),
+    "ps_fusion_params_default": (None, [C.POINTER(FusionParams)]),
+    "ps_postprocess_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(PostParams),
+                                          C.POINTER(C.c_uint64)]),
+    "ps_readout_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
+    "ps_fuse_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView), C.POINTER(FusionParams),
+                                   C.POINTER(C.c_uint64)]),
+    "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_uint32]),
+    "ps_write_ply": (C.c_int, [C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     # learned proposal
     "ps_net_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),
     "ps_net_destroy": (None, [_P]),

@@ -52,6 +52,8 @@ def build_engine(force: bool = False, verbose: bool = False) -> pathlib.Path:
         ("runtime.o", CSRC / "ps_runtime.cu", ["-Xcompiler", "-fopenmp"]),
         ("noalloc.o", CSRC / "ps_noalloc.cu", PARITY),
         ("cnn.o", CSRC / "ps_cnn.cu", []),
+        ("post.o", CSRC / "ps_post.cu", PARITY),
+        ("io.o", CSRC / "ps_io.cpp", []),
     ]
     for name, src, flags in specs:
         out = OBJ / name

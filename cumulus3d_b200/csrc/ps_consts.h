@@ -15,6 +15,9 @@ struct PsConsts {
   float cos_filter_tri, q_min, ncc_norm, inv2ncc, filter_gmax, weak_var;
 };
 
+// Rust's f64::to_radians: x * (PI / 180) with the quotient taken in binary64.
+static inline double ps_to_radians_f64(double deg) { return deg * (3.14159265358979323846 / 180.0); }
+
 // Rust's f32::to_radians: x * (PI_f32 / 180) with the quotient taken in binary32.
 static inline float ps_to_radians_f32(float deg) {
   const float pi = 3.14159265358979323846f;

@@ -1,0 +1,351 @@
+// Post-processing of resident depth maps: speckle removal and consistency fusion.
+//
+//   * Speckle removal restates remove_speckles (crates/dense/src/postproc.rs:77-129): 4-connected components of valid
+//     pixels, two neighbours joined when |d_j - d_i| <= rel·min(d_i, d_j); a component smaller than
+//     ceil(w·h·min_area_frac) whose lower median cost (sorted costs[len/2]) exceeds keep_cost is erased.  The
+//     reference grows components by depth-first search from the first pixel in row-major order; the components of this
+//     symmetric relation do not depend on the order, so the GPU labels them with a lock-free union-find (roots hook to
+//     the smaller index, so each label is the component's first pixel) and finds the lower median of each small
+//     component exactly by bisection over an order-preserving integer key of the f32 costs.
+//   * Consistency fusion restates fuse_consistency with residual handling "none" (crates/dense/src/fusion.rs:219-459):
+//     views in the caller's order, every reference pixel of a view evaluated independently in FP64 (projection,
+//     back-projection, reprojection error, normal agreement, inverse-variance weighted means).  Within one view the
+//     evaluation reads only marks that earlier views wrote and writes marks of other views, so one kernel launch per
+//     view reproduces the reference's result exactly; points are appended in any order and carry the reference's
+//     point key, so sorting by key restores the reference's order (views ascending, row-major within a view).
+//
+// This file is compiled with the parity flags (no contraction, IEEE division and square root): the FP64 operation
+// sequence matches the CPU oracle's restatement operation by operation.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "ps_post.h"
+
+namespace ps_post {
+
+// ------------------------------------------------------------------------------------------- speckles
+__device__ __forceinline__ int item_of(const SpkArgs& A, int cta) {
+  int lo = 0, hi = A.nitems - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (A.items[mid].tile0 <= cta) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+struct Px {
+  int x, y, g;  // pixel and its slot index
+  const SpkItem* it;
+};
+
+__device__ __forceinline__ bool spk_px(const SpkArgs& A, Px& p) {
+  const int ii = item_of(A, blockIdx.x);
+  const SpkItem& it = A.items[ii];
+  const int tiles_x = (it.w + 31) / 32;
+  const int tl = blockIdx.x - it.tile0;
+  p.x = (tl % tiles_x) * 32 + threadIdx.x;
+  p.y = (tl / tiles_x) * 8 + threadIdx.y;
+  p.it = &it;
+  if (p.x >= it.w || p.y >= it.h) return false;
+  p.g = (int)(it.off + (long long)p.y * it.w + p.x);
+  return true;
+}
+
+// Order-preserving key of an f32 (IEEE total order): keys compare like the floats (−0 before +0).
+__device__ __forceinline__ unsigned fkey(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float funkey(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7FFFFFFFu) : ~k);
+}
+
+__device__ __forceinline__ int find_root(const int* parent, int x) {
+  int p;
+  while ((p = __ldcg(parent + x)) != x) x = p;  // L2 reads: parents change during the union pass
+  return x;
+}
+
+// Joins the components of a and b: the larger root is hooked under the smaller with a compare-and-swap; a failed swap
+// means the root got a (smaller) parent meanwhile, so the loop continues from it.  Each retry strictly lowers `a`.
+__device__ void unite(int* parent, int a, int b) {
+  while (true) {
+    a = find_root(parent, a);
+    b = find_root(parent, b);
+    if (a == b) return;
+    if (a < b) {
+      const int t = a;
+      a = b;
+      b = t;
+    }
+    const int old = atomicCAS(parent + a, a, b);
+    if (old == a) return;
+    a = old;
+  }
+}
+
+__device__ __forceinline__ bool joined(float di, float dj, float rel) {
+  return dj > 0.f && fabsf(dj - di) <= rel * fminf(di, dj);
+}
+
+__global__ void k_spk_init(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  A.parent[p.g] = A.plane[p.g].w > 0.f ? p.g : -1;
+  A.size[p.g] = 0;
+  A.cnt[p.g] = 0;
+}
+
+__global__ void k_spk_union(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  const float di = A.plane[p.g].w;
+  if (!(di > 0.f)) return;
+  if (p.x + 1 < p.it->w && joined(di, A.plane[p.g + 1].w, A.rel)) unite(A.parent, p.g, p.g + 1);
+  if (p.y + 1 < p.it->h && joined(di, A.plane[p.g + p.it->w].w, A.rel)) unite(A.parent, p.g, p.g + p.it->w);
+}
+
+__global__ void k_spk_flatten(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  if (A.parent[p.g] < 0) return;
+  const int r = find_root(A.parent, p.g);
+  A.parent[p.g] = r;
+  atomicAdd(A.size + r, 1);
+}
+
+// Small components: bisection state [lo, hi] over cost keys for the lower median (the (size/2)-th smallest key).
+__global__ void k_spk_bisect_init(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  if (A.parent[p.g] != p.g || A.size[p.g] >= p.it->min_area) return;
+  A.lo[p.g] = 0u;
+  A.hi[p.g] = 0xFFFFFFFFu;
+}
+
+__global__ void k_spk_count(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  const int r = A.parent[p.g];
+  if (r < 0 || A.size[r] >= p.it->min_area) return;
+  const unsigned lo = A.lo[r], hi = A.hi[r];
+  const unsigned mid = lo + (hi - lo) / 2u;
+  if (fkey(A.cost[p.g]) <= mid) atomicAdd(A.cnt + r, 1u);
+}
+
+__global__ void k_spk_step(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  if (A.parent[p.g] != p.g || A.size[p.g] >= p.it->min_area) return;
+  const unsigned lo = A.lo[p.g], hi = A.hi[p.g];
+  const unsigned mid = lo + (hi - lo) / 2u;
+  const unsigned k = (unsigned)A.size[p.g] / 2u;
+  if (A.cnt[p.g] >= k + 1u) A.hi[p.g] = mid;
+  else A.lo[p.g] = mid + 1u;
+  A.cnt[p.g] = 0u;
+}
+
+__global__ void k_spk_erase(SpkArgs A) {
+  Px p;
+  if (!spk_px(A, p)) return;
+  const int r = A.parent[p.g];
+  if (r < 0 || A.size[r] >= p.it->min_area) return;
+  if (funkey(A.lo[r]) > A.keep) {
+    A.plane[p.g] = make_float4(0.f, 0.f, 0.f, 0.f);
+    atomicAdd(A.removed, 1ull);
+  }
+}
+
+__global__ void k_count_valid(SpkArgs A) {
+  Px p;
+  const bool ok = spk_px(A, p) && A.plane[p.g].w > 0.f;
+  const unsigned m = __ballot_sync(0xffffffffu, ok);
+  if (threadIdx.x == 0 && m) atomicAdd(A.valid, (unsigned long long)__popc(m));
+}
+
+cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st) {
+  if (ntiles <= 0) return cudaSuccess;
+  k_count_valid<<<ntiles, dim3(32, 8), 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* launches) {
+  if (ntiles <= 0) return cudaSuccess;
+  const dim3 b(32, 8);
+  k_spk_init<<<ntiles, b, 0, st>>>(A);
+  k_spk_union<<<ntiles, b, 0, st>>>(A);
+  k_spk_flatten<<<ntiles, b, 0, st>>>(A);
+  k_spk_bisect_init<<<ntiles, b, 0, st>>>(A);
+  for (int i = 0; i < 32; ++i) {  // 32 halvings of the 2^32 key range leave lo == hi
+    k_spk_count<<<ntiles, b, 0, st>>>(A);
+    k_spk_step<<<ntiles, b, 0, st>>>(A);
+  }
+  k_spk_erase<<<ntiles, b, 0, st>>>(A);
+  *launches += 5 + 64;
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------- fusion
+struct Hit {
+  int o, q;
+};
+
+// camera -> world of pixel (col, row) at depth d: X = Rᵀ (c - t), c = ((col-cx)/fx·d, (row-cy)/fy·d, d)
+__device__ __forceinline__ void backproject(const FuseView& c, double col, double row, double d, double* X) {
+  const double cc[3] = {(col - c.k[2]) / c.k[0] * d, (row - c.k[3]) / c.k[1] * d, d};
+  const double p[3] = {cc[0] - c.t[0], cc[1] - c.t[1], cc[2] - c.t[2]};
+  const double* r = c.r;
+  X[0] = r[0] * p[0] + r[3] * p[1] + r[6] * p[2];
+  X[1] = r[1] * p[0] + r[4] * p[1] + r[7] * p[2];
+  X[2] = r[2] * p[0] + r[5] * p[1] + r[8] * p[2];
+}
+
+__device__ __forceinline__ bool project(const FuseView& c, const double* x, double* u, double* v, double* z) {
+  const double* r = c.r;
+  const double cz = r[6] * x[0] + r[7] * x[1] + r[8] * x[2] + c.t[2];
+  if (cz <= 0.0) return false;
+  const double cx = r[0] * x[0] + r[1] * x[1] + r[2] * x[2] + c.t[0];
+  const double cy = r[3] * x[0] + r[4] * x[1] + r[5] * x[2] + c.t[1];
+  *u = c.k[0] * cx / cz + c.k[2];
+  *v = c.k[1] * cy / cz + c.k[3];
+  *z = cz;
+  return true;
+}
+
+__device__ __forceinline__ void normal_world(const FuseView& c, float4 q, double* n) {
+  const double m[3] = {(double)q.x, (double)q.y, (double)q.z};
+  const double* r = c.r;
+  n[0] = r[0] * m[0] + r[3] * m[1] + r[6] * m[2];
+  n[1] = r[1] * m[0] + r[4] * m[1] + r[7] * m[2];
+  n[2] = r[2] * m[0] + r[5] * m[1] + r[8] * m[2];
+}
+
+// inv_var (crates/dense/src/fusion.rs:86-95): 1/σ_d² with σ_d = d²·σ_px/(f·b), σ_px = σ0 + slope·clamp(cost, 0, 2).
+__device__ __forceinline__ double inv_var(const FuseArgs& A, const FuseView& c, double d, float cost) {
+  if (!A.inverse_variance || !(c.baseline > 0.0)) return 1.0;
+  const double spx = A.sigma0 + A.slope * (double)fminf(fmaxf(cost, 0.0f), 2.0f);
+  const double sd = d * d * spx / (c.k[0] * c.baseline);
+  return 1.0 / fmax(sd * sd, 1e-300);
+}
+
+// Gray u8 colour of an image plane value (the reference uses the view's colour image; these images are gray).
+__device__ __forceinline__ double gray_u8(const FuseView& c, int col, int row) {
+  const int x = min(col, c.w - 1), y = min(row, c.h - 1);
+  const float v = c.img[(long long)y * c.pitch + x] * 255.0f;
+  return (double)(unsigned char)fminf(fmaxf(rintf(v), 0.0f), 255.0f);
+}
+
+__global__ void __launch_bounds__(256) k_fuse(FuseArgs A) {
+  const FuseView& cv = A.views[A.v];
+  const int col = blockIdx.x * 32 + threadIdx.x, row = blockIdx.y * 8 + threadIdx.y;
+  if (col >= cv.w || row >= cv.h) return;
+  const long long pix = (long long)row * cv.w + col;
+  const float4 q = A.plane[cv.off + pix];
+  if (!(q.w > 0.0f)) return;
+  if (A.mark_used && A.marks[cv.off + pix] != 0) return;
+  const double d = (double)q.w;
+  double x[3], nw[3];
+  backproject(cv, (double)col, (double)row, d, x);
+  normal_world(cv, q, nw);
+  const double w0 = inv_var(A, cv, d, A.cost[cv.off + pix]);
+  double sw = w0;
+  double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
+  double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
+  const double c0 = gray_u8(cv, col, row);
+  double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
+  Hit hits[PS_FUSE_MAX_OVERLAP];
+  int nh = 0;
+  for (int i = 0; i < cv.nov; ++i) {
+    const int o = cv.ov[i];
+    const FuseView& oc = A.views[o];
+    double u, vv, z;
+    if (!project(oc, x, &u, &vv, &z)) continue;
+    const double cu = floor(u + 0.5), rv = floor(vv + 0.5);
+    if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
+    const int opix = (int)rv * oc.w + (int)cu;
+    const float4 oq = A.plane[oc.off + opix];
+    const double od = (double)oq.w;
+    if (od <= 0.0 || fabs(z - od) / od > A.depth_tol) continue;
+    double xo[3];
+    backproject(oc, cu, rv, od, xo);
+    double bu, bv, bz;
+    if (!project(cv, xo, &bu, &bv, &bz)) continue;
+    const double eu = bu - (double)col, ev = bv - (double)row;
+    if (eu * eu + ev * ev > A.r2) continue;
+    double no[3];
+    normal_world(oc, oq, no);
+    if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < A.cos_n) continue;
+    const double co = gray_u8(oc, (int)cu, (int)rv);
+    const double wo = inv_var(A, oc, od, A.cost[oc.off + opix]);
+    sw += wo;
+    for (int k = 0; k < 3; ++k) {
+      sx[k] += wo * xo[k];
+      sn[k] += wo * no[k];
+      sc[k] += wo * co;
+    }
+    hits[nh].o = o;
+    hits[nh].q = opix;
+    nh++;
+  }
+  if (nh < A.min_views) return;
+  const double m = sw;
+  const double l = sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+  if (l < 1.1920928955078125e-07) return;  // f32::EPSILON
+  if (A.mark_used) {
+    for (int i = 0; i < nh; ++i) {
+      const FuseView& oc = A.views[hits[i].o];
+      if (A.mark_radius == 0) {
+        A.marks[oc.off + hits[i].q] = 1;
+        continue;
+      }
+      // marks within the radius whose depth agrees with the hit (crates/dense/src/fusion.rs:363-388)
+      const int cx0 = hits[i].q % oc.w, cy0 = hits[i].q / oc.w, r = A.mark_radius;
+      const double d0 = (double)A.plane[oc.off + hits[i].q].w;
+      for (int yy = max(cy0 - r, 0); yy <= min(cy0 + r, oc.h - 1); ++yy)
+        for (int xx = max(cx0 - r, 0); xx <= min(cx0 + r, oc.w - 1); ++xx) {
+          const long long qq = (long long)yy * oc.w + xx;
+          const double dq = (double)A.plane[oc.off + qq].w;
+          if (dq > 0.0 && fabs(dq - d0) <= A.depth_tol * d0) A.marks[oc.off + qq] = 1;
+        }
+    }
+  }
+  const unsigned long long slot = atomicAdd(A.count, 1ull);
+  if (slot >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
+  A.pos[3 * slot + 0] = (float)(sx[0] / m);
+  A.pos[3 * slot + 1] = (float)(sx[1] / m);
+  A.pos[3 * slot + 2] = (float)(sx[2] / m);
+  A.nrm[3 * slot + 0] = (float)(sn[0] / l);
+  A.nrm[3 * slot + 1] = (float)(sn[1] / l);
+  A.nrm[3 * slot + 2] = (float)(sn[2] / l);
+  for (int k = 0; k < 3; ++k) A.col[3 * slot + k] = (unsigned char)round(sc[k] / m);
+  A.key[slot] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
+                (unsigned long long)(col & 0xffff);
+  // visibility: sorted, de-duplicated {v} ∪ hit views
+  unsigned short* vis = A.vis + slot * A.vis_stride;
+  int nv = 0;
+  vis[nv++] = (unsigned short)A.v;
+  for (int i = 0; i < nh; ++i) {
+    const unsigned short o = (unsigned short)hits[i].o;
+    int j = nv;
+    bool dup = false;
+    for (int k = 0; k < nv; ++k) dup = dup || vis[k] == o;
+    if (dup) continue;
+    while (j > 0 && vis[j - 1] > o) {
+      vis[j] = vis[j - 1];
+      --j;
+    }
+    vis[j] = o;
+    nv++;
+  }
+  A.nvis[slot] = (unsigned char)nv;
+}
+
+cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st) {
+  const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+  k_fuse<<<g, b, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+}  // namespace ps_post

@@ -1,0 +1,69 @@
+// Device-side tables of the post-processing kernels (ps_post.cu) shared with the session runtime.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ps_types.h"
+
+#define PS_FUSE_MAX_OVERLAP 32  // overlap views checked per reference pixel (consistency_num_images is at most this)
+
+namespace ps_post {
+
+// One view of a speckle launch: slot offset, size, first CTA, minimum component area ceil(w·h·frac).
+struct SpkItem {
+  long long off;
+  int w, h, tile0, min_area;
+};
+
+struct SpkArgs {
+  float4* plane;       // readout planes (nx, ny, nz, d), erased in place
+  const float* cost;   // final matching costs
+  int* parent;         // union-find parent per slot pixel (-1 = invalid)
+  int* size;           // component size per root
+  unsigned* lo;        // bisection bounds per small root (order-preserving cost keys)
+  unsigned* hi;
+  unsigned* cnt;
+  unsigned long long* removed;
+  unsigned long long* valid;  // k_count_valid: valid pixels of the items
+  float rel, keep;
+  int nitems;
+  SpkItem items[PS_MAX_ITEMS];
+};
+
+// Camera and depth map of one view for fusion: world -> camera x_c = R x_w + t (R row-major), intrinsics k.
+struct FuseView {
+  double k[4];
+  double r[9];
+  double t[3];
+  double baseline;       // representative baseline (median source-centre distance), 0 = unweighted
+  const float* img;      // image plane (for the gray colour), row pitch `pitch` floats
+  long long off;         // slot offset of the view's depth map
+  int w, h, pitch;
+  unsigned image_id;
+  int nov;               // overlap views to check, in order
+  int ov[PS_FUSE_MAX_OVERLAP];
+};
+
+struct FuseArgs {
+  const FuseView* views;  // device table indexed by session view
+  int v;                  // reference view of this launch
+  const float4* plane;    // readout planes of the level (slot layout)
+  const float* cost;
+  unsigned char* marks;   // "used" marks per slot pixel
+  int min_views, mark_used, mark_radius, inverse_variance;
+  double sigma0, slope, depth_tol, cos_n, r2;
+  float* pos;
+  float* nrm;
+  unsigned char* col;
+  unsigned long long* key;
+  unsigned char* nvis;
+  unsigned short* vis;    // vis_stride entries per point (sorted contributing views)
+  int vis_stride;
+  unsigned long long* count;
+  unsigned long long capacity;
+};
+
+cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* launches);
+cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
+cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);
+
+}  // namespace ps_post

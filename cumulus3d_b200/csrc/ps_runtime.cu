@@ -23,6 +23,7 @@
 #include "../../include/patchstereo.h"
 #include "ps_cnn.h"
 #include "ps_consts.h"
+#include "ps_post.h"
 #include "ps_types.h"
 
 #define PS_DECLARE_LAUNCHERS(NS)                                                                           \
@@ -86,6 +87,33 @@ struct Slot {
   float4* proposal = nullptr;  // learned proposals (allocated by the first proposal call of the level)
   float* pconf = nullptr;      // their confidences
   std::vector<char> proposal_valid;
+  int* spk = nullptr;          // speckle removal: parent, size, lo, hi, cnt per pixel (5 ints each, lazily)
+  unsigned char* marks = nullptr;  // fusion "used" marks
+};
+
+// Fused point cloud of the last ps_fuse_resident call (device).
+struct FusedCloud {
+  unsigned long long cap = 0, count = 0;
+  int vis_stride = 0;
+  float* pos = nullptr;
+  float* nrm = nullptr;
+  unsigned char* col = nullptr;
+  unsigned long long* key = nullptr;
+  unsigned char* nvis = nullptr;
+  unsigned short* vis = nullptr;
+  unsigned long long* counter = nullptr;
+  ps_post::FuseView* views = nullptr;
+  void release() {
+    cudaFree(pos);
+    cudaFree(nrm);
+    cudaFree(col);
+    cudaFree(key);
+    cudaFree(nvis);
+    cudaFree(vis);
+    *this = FusedCloud{counter, views};
+  }
+  FusedCloud() = default;
+  FusedCloud(unsigned long long* c, ps_post::FuseView* v) : counter(c), views(v) {}
 };
 
 }  // namespace
@@ -120,6 +148,7 @@ struct ps_session {
   float* netout = nullptr;
   size_t netout_cap = 0;
   unsigned long long* pcount = nullptr;
+  FusedCloud fused;
   // device tables
   float* img = nullptr;
   PsLevel* lv = nullptr;
@@ -810,7 +839,12 @@ int ps_end(ps_session* s) {
     cudaFree(sl.count);
     cudaFree(sl.proposal);
     cudaFree(sl.pconf);
+    cudaFree(sl.spk);
+    cudaFree(sl.marks);
   }
+  s->fused.release();
+  cudaFree(s->fused.counter);
+  cudaFree(s->fused.views);
   cudaFree(s->netin);
   cudaFree(s->netout);
   cudaFree(s->pcount);
@@ -1420,6 +1454,257 @@ int ps_proposal_download(ps_session* s, uint32_t level, const uint32_t* views, s
                 "download confidence");
     }
     sync(s);
+  });
+}
+
+int ps_readout_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* out) {
+  return guard(s, [&] {
+    check_views(s, views, n);
+    if (n && !out) fail(PS_EINVAL, "out is NULL");
+    Slot& sl = slot(s, (int)level);
+    for (auto [a, b] : batches(s, views, n, (int)level)) download_states(s, views, a, b, out, (int)level, true, true, sl.aux);
+  });
+}
+
+// ---- post-processing and fusion --------------------------------------------------------------------------------
+extern "C++" {
+namespace {
+
+// Item table of a speckle / count launch over views[a..b) at `level` (32 × 8 pixel tiles).
+int spk_items(ps_session* s, ps_post::SpkArgs& A, const uint32_t* views, size_t a, size_t b, int level, double frac) {
+  Slot& sl = s->slots[level];
+  int tiles = 0;
+  A.nitems = (int)(b - a);
+  for (size_t i = a; i < b; ++i) {
+    const int v = (int)views[i];
+    ps_post::SpkItem& it = A.items[i - a];
+    it.off = sl.off[v];
+    it.w = s->W(v, level);
+    it.h = s->H(v, level);
+    it.tile0 = tiles;
+    it.min_area = (int)std::ceil((double)it.w * it.h * frac);
+    tiles += ((it.w + 31) / 32) * ((it.h + 7) / 8);
+  }
+  return tiles;
+}
+
+}  // namespace
+}  // extern "C++"
+
+void ps_post_params_default(ps_post_params* out) {
+  if (!out) return;
+  out->remove_speckles = 1;
+  out->speckle_rel_depth = 0.02f;
+  out->speckle_min_area_frac = 2e-4;
+  out->speckle_keep_cost = 0.2f;
+}
+
+void ps_fusion_params_default(ps_fusion_params* out) {
+  if (!out) return;
+  memset(out, 0, sizeof *out);
+  out->min_consistent_views = 5;
+  out->consistency_num_images = 12;
+  out->mark_used = 1;
+  out->mark_radius = 0;
+  out->inverse_variance = 1;
+  out->sigma_px0 = 0.25;
+  out->sigma_px_slope = 1.0;
+  out->max_reproj_error = 2.0;
+  out->max_depth_error = 0.01;
+  out->max_normal_error_deg = 10.0;
+}
+
+int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
+                            uint64_t* removed) {
+  return guard(s, [&] {
+    if (!p) fail(PS_EINVAL, "params is NULL");
+    check_views(s, views, n);
+    Slot& sl = slot(s, (int)level);
+    if (removed) *removed = 0;
+    if (!p->remove_speckles || n == 0) return;
+    if (!sl.spk) sl.spk = dalloc<int>((size_t)std::max<long long>(sl.total, 1) * 5);
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(1);
+    cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
+    const size_t T = (size_t)std::max<long long>(sl.total, 1);
+    for (auto [a, b] : batches(s, views, n, (int)level)) {
+      ps_post::SpkArgs A;
+      memset(&A, 0, sizeof A);
+      A.plane = sl.aux;
+      A.cost = sl.cost;
+      A.parent = sl.spk;
+      A.size = sl.spk + T;
+      A.lo = (unsigned*)(sl.spk + 2 * T);
+      A.hi = (unsigned*)(sl.spk + 3 * T);
+      A.cnt = (unsigned*)(sl.spk + 4 * T);
+      A.removed = s->pcount;
+      A.rel = p->speckle_rel_depth;
+      A.keep = p->speckle_keep_cost;
+      const int tiles = spk_items(s, A, views, a, b, (int)level, p->speckle_min_area_frac);
+      bool any = false;
+      for (int i = 0; i < A.nitems; ++i) any = any || A.items[i].min_area > 1;
+      if (!any) continue;  // the reference returns early when the minimum area is <= 1
+      for (int i = 0; i < A.nitems; ++i)
+        if (A.items[i].min_area <= 1) A.items[i].min_area = 0;  // no component is small
+      int nl = 0;
+      cuda_ok(ps_post::launch_speckles(A, tiles, s->st, &nl), "speckle kernels");
+      s->launches += nl;
+    }
+    if (removed) {
+      unsigned long long c = 0;
+      cuda_ok(cudaMemcpyAsync(&c, s->pcount, sizeof c, cudaMemcpyDeviceToHost, s->st), "read count");
+      sync(s);
+      *removed = c;
+    }
+  });
+}
+
+int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
+                     const ps_fusion_params* p, uint64_t* num_points) {
+  return guard(s, [&] {
+    if (!p || (n && !cams)) fail(PS_EINVAL, "params or cams is NULL");
+    check_views(s, views, n);
+    if (s->nv > 65535) fail(PS_EINVAL, "fusion supports at most 65535 views");
+    if (p->consistency_num_images > PS_FUSE_MAX_OVERLAP)
+      fail(PS_EINVAL, "consistency_num_images > " + std::to_string(PS_FUSE_MAX_OVERLAP));
+    const int l = (int)level;
+    Slot& sl = slot(s, l);
+    std::vector<char> used(s->nv, 0);
+    for (size_t i = 0; i < n; ++i) used[views[i]] = 1;
+    // camera table (indexed by session view); overlap lists filtered to used views and truncated
+    std::vector<ps_post::FuseView> fv(s->nv);
+    for (int v = 0; v < s->nv; ++v) {
+      ps_post::FuseView& f = fv[v];
+      memset(&f, 0, sizeof f);
+      f.off = sl.off[v];
+      f.w = s->W(v, l);
+      f.h = s->H(v, l);
+      const PsLevel& L = s->lvh[v * s->nl + l];
+      f.img = L.img;
+      f.pitch = L.pitch;
+      if (!used[v]) continue;
+      const ps_fusion_view& c = cams[v];
+      memcpy(f.k, c.k, sizeof f.k);
+      memcpy(f.r, c.r, sizeof f.r);
+      memcpy(f.t, c.t, sizeof f.t);
+      f.baseline = c.baseline;
+      f.image_id = c.image_id;
+      if (c.num_overlap && !c.overlap) fail(PS_EINVAL, "overlap is NULL");
+      for (uint32_t j = 0; j < c.num_overlap && f.nov < (int)p->consistency_num_images; ++j) {
+        const uint32_t o = c.overlap[j];
+        if (o >= (uint32_t)s->nv) fail(PS_EINVAL, "overlap view out of range");
+        if (used[o] && (int)o != v) f.ov[f.nov++] = (int)o;
+      }
+    }
+    FusedCloud& fc = s->fused;
+    if (!fc.counter) fc.counter = dalloc<unsigned long long>(1);
+    if (!fc.views) fc.views = dalloc<ps_post::FuseView>(std::max(s->nv, 1));
+    cuda_ok(cudaMemcpyAsync(fc.views, fv.data(), fv.size() * sizeof(ps_post::FuseView), cudaMemcpyHostToDevice, s->st),
+            "upload fusion views");
+    // capacity: valid pixels of the fused views
+    cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
+    for (auto [a, b] : batches(s, views, n, l)) {
+      ps_post::SpkArgs A;
+      memset(&A, 0, sizeof A);
+      A.plane = sl.aux;
+      A.valid = fc.counter;
+      const int tiles = spk_items(s, A, views, a, b, l, 0.0);
+      cuda_ok(ps_post::launch_count_valid(A, tiles, s->st), "count kernel");
+      s->launches++;
+    }
+    unsigned long long valid = 0;
+    cuda_ok(cudaMemcpyAsync(&valid, fc.counter, sizeof valid, cudaMemcpyDeviceToHost, s->st), "read count");
+    sync(s);
+    const int stride = (int)p->consistency_num_images + 1;
+    if (valid > fc.cap || stride != fc.vis_stride) {
+      fc.release();
+      const size_t c = std::max<unsigned long long>(valid, 1);
+      fc.pos = dalloc<float>(3 * c);
+      fc.nrm = dalloc<float>(3 * c);
+      fc.col = dalloc<unsigned char>(3 * c);
+      fc.key = dalloc<unsigned long long>(c);
+      fc.nvis = dalloc<unsigned char>(c);
+      fc.vis = dalloc<unsigned short>(c * stride);
+      fc.cap = c;
+      fc.vis_stride = stride;
+    }
+    if (!sl.marks) sl.marks = dalloc<unsigned char>(std::max<long long>(sl.total, 1));
+    cuda_ok(cudaMemsetAsync(sl.marks, 0, std::max<long long>(sl.total, 1), s->st), "memset");
+    cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
+    ps_post::FuseArgs A;
+    memset(&A, 0, sizeof A);
+    A.views = fc.views;
+    A.plane = sl.aux;
+    A.cost = sl.cost;
+    A.marks = sl.marks;
+    A.min_views = (int)p->min_consistent_views;
+    A.mark_used = p->mark_used ? 1 : 0;
+    A.mark_radius = (int)p->mark_radius;
+    A.inverse_variance = p->inverse_variance ? 1 : 0;
+    A.sigma0 = p->sigma_px0;
+    A.slope = p->sigma_px_slope;
+    A.depth_tol = p->max_depth_error;
+    A.cos_n = std::cos(ps_to_radians_f64(p->max_normal_error_deg));
+    A.r2 = p->max_reproj_error * p->max_reproj_error;
+    A.pos = fc.pos;
+    A.nrm = fc.nrm;
+    A.col = fc.col;
+    A.key = fc.key;
+    A.nvis = fc.nvis;
+    A.vis = fc.vis;
+    A.vis_stride = stride;
+    A.count = fc.counter;
+    A.capacity = fc.cap;
+    std::vector<uint32_t> order(views, views + n);
+    std::sort(order.begin(), order.end());  // the reference walks views in index order
+    order.erase(std::unique(order.begin(), order.end()), order.end());
+    for (uint32_t v : order) {
+      A.v = (int)v;
+      cuda_ok(ps_post::launch_fuse(A, s->W(v, l), s->H(v, l), s->st), "fusion kernel");
+      s->launches++;
+    }
+    unsigned long long cnt = 0;
+    cuda_ok(cudaMemcpyAsync(&cnt, fc.counter, sizeof cnt, cudaMemcpyDeviceToHost, s->st), "read count");
+    sync(s);
+    fc.count = std::min(cnt, fc.cap);
+    if (num_points) *num_points = fc.count;
+  });
+}
+
+int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
+                    uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride) {
+  return guard(s, [&] {
+    FusedCloud& fc = s->fused;
+    const size_t n = fc.count;
+    if (capacity < n) fail(PS_EINVAL, "capacity " + std::to_string(capacity) + " < " + std::to_string(n) + " points");
+    if (vis && (int)vis_stride < fc.vis_stride) fail(PS_EINVAL, "vis_stride too small");
+    std::vector<float> p(3 * n), q(3 * n);
+    std::vector<unsigned char> c(3 * n), nv(n);
+    std::vector<unsigned long long> k(n);
+    std::vector<unsigned short> vv((size_t)n * std::max(fc.vis_stride, 1));
+    if (n) {
+      cuda_ok(cudaMemcpyAsync(p.data(), fc.pos, 12 * n, cudaMemcpyDeviceToHost, s->st), "download");
+      cuda_ok(cudaMemcpyAsync(q.data(), fc.nrm, 12 * n, cudaMemcpyDeviceToHost, s->st), "download");
+      cuda_ok(cudaMemcpyAsync(c.data(), fc.col, 3 * n, cudaMemcpyDeviceToHost, s->st), "download");
+      cuda_ok(cudaMemcpyAsync(k.data(), fc.key, 8 * n, cudaMemcpyDeviceToHost, s->st), "download");
+      cuda_ok(cudaMemcpyAsync(nv.data(), fc.nvis, n, cudaMemcpyDeviceToHost, s->st), "download");
+      cuda_ok(cudaMemcpyAsync(vv.data(), fc.vis, 2 * n * fc.vis_stride, cudaMemcpyDeviceToHost, s->st), "download");
+    }
+    sync(s);
+    // points in the reference's order: ascending key (view, row, column)
+    std::vector<size_t> idx(n);
+    for (size_t i = 0; i < n; ++i) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
+    for (size_t j = 0; j < n; ++j) {
+      const size_t i = idx[j];
+      if (positions) memcpy(positions + 3 * j, &p[3 * i], 12);
+      if (normals) memcpy(normals + 3 * j, &q[3 * i], 12);
+      if (colors) memcpy(colors + 3 * j, &c[3 * i], 3);
+      if (keys) keys[j] = k[i];
+      if (vis_counts) vis_counts[j] = nv[i];
+      if (vis)
+        for (int t = 0; t < (int)vis_stride; ++t)
+          vis[(size_t)j * vis_stride + t] = t < fc.vis_stride && t < nv[i] ? vv[i * fc.vis_stride + t] : 0;
+    }
   });
 }
 

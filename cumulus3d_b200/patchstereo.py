@@ -380,6 +380,46 @@ class PatchMatchSession:
                             _lib.PS_INIT_PROPOSAL if proposal else _lib.PS_INIT_RANDOM)
         self._check(self.lib.ps_schedule_resident(self.h, _views(views), len(views), C.byref(sch)))
 
+    # ---- post-processing and fusion ----------------------------------------------------------------------------
+    def postprocess_resident(self, level: int, views: Sequence[int], post=None, count: bool = True) -> Optional[int]:
+        """Speckle removal on the readout planes (PostParams; defaults of the reference when `post` is None)."""
+        from .fusion import default_post
+        p = post if post is not None else default_post()
+        n = C.c_uint64()
+        self._check(self.lib.ps_postprocess_resident(self.h, level, _views(views), len(views), C.byref(p),
+                                                     C.byref(n) if count else None))
+        return int(n.value) if count else None
+
+    def readout_download(self, level: int, views: Sequence[int]) -> List[ViewState]:
+        """The current readout planes (after post-processing) and costs, without recomputing the readout."""
+        out = [ViewState.new(*self._size(v, level)) for v in views]
+        keep = []
+        self._check(self.lib.ps_readout_download(self.h, level, _views(views), len(views), c_states(out, keep)))
+        return out
+
+    def fuse_resident(self, level: int, views: Sequence[int], cams, params=None) -> int:
+        """Consistency fusion of the readout planes of `views`; `cams` is a fusion.FusionCams of every view."""
+        from .fusion import default_fusion
+        p = params if params is not None else default_fusion()
+        n = C.c_uint64()
+        self._check(self.lib.ps_fuse_resident(self.h, level, _views(views), len(views), cams.table, C.byref(p),
+                                              C.byref(n)))
+        self._fused = (int(n.value), int(p.consistency_num_images) + 1)
+        return int(n.value)
+
+    def fused_points(self):
+        from .fusion import FusedCloud
+        n, stride = getattr(self, "_fused", (0, 1))
+        pos = np.empty((n, 3), np.float32)
+        nrm = np.empty((n, 3), np.float32)
+        col = np.empty((n, 3), np.uint8)
+        key = np.empty(n, np.uint64)
+        nv = np.empty(n, np.uint8)
+        vis = np.empty((n, stride), np.uint16)
+        self._check(self.lib.ps_fused_points(self.h, n, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data,
+                                             key.ctypes.data, nv.ctypes.data, vis.ctypes.data, stride))
+        return FusedCloud(pos, nrm, col, key, nv, vis)
+
     # ---- learned proposal (no reference counterpart) ----------------------------------------------------------
     def sweep_volume(self, level: int, view: int, out_ptr: int, row_pixels: int) -> None:
         """Writes the view's network input (bf16 NHWC, 48 channels) to device memory at `out_ptr` (asynchronous on

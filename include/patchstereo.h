@@ -345,6 +345,67 @@ int ps_proposal_upload(ps_session* s, uint32_t level, const uint32_t* views, siz
 int ps_proposal_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, float* const* planes,
                          float* const* conf);
 
+/* ---- post-processing and fusion of resident depth maps -------------------------------------------------------
+ * PostParams (crates/dense/src/postproc.rs:41-74): speckle removal only (fill_holes is off by default there and is
+ * not provided).  remove_speckles (postproc.rs:77-129) runs on the readout planes of `level` in place: 4-connected
+ * components (|d_j - d_i| <= rel·min(d_i, d_j)) smaller than ceil(w·h·min_area_frac) whose lower median cost exceeds
+ * keep_cost are erased.  Asynchronous unless `removed` is given (then it receives the erased pixel count). */
+typedef struct ps_post_params {
+  uint32_t remove_speckles;     /* true */
+  float speckle_rel_depth;      /* 0.02 */
+  double speckle_min_area_frac; /* 2e-4 */
+  float speckle_keep_cost;      /* 0.2 */
+} ps_post_params;
+void ps_post_params_default(ps_post_params* out);
+int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
+                            uint64_t* removed);
+/* Downloads the current readout planes (after any post-processing) and final costs of `views` at `level` without
+ * recomputing the readout. */
+int ps_readout_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* out);
+/* FusionParams of consistency fusion (crates/dense/src/params.rs:286-351; residual handling "none"). */
+typedef struct ps_fusion_params {
+  uint32_t min_consistent_views;   /* 5 */
+  uint32_t consistency_num_images; /* 12 (at most 32) */
+  uint32_t mark_used;              /* true */
+  uint32_t mark_radius;            /* 0 */
+  uint32_t inverse_variance;       /* true */
+  uint32_t reserved;
+  double sigma_px0;                /* 0.25 */
+  double sigma_px_slope;           /* 1.0 */
+  double max_reproj_error;         /* 2.0 px */
+  double max_depth_error;          /* 0.01 relative */
+  double max_normal_error_deg;     /* 10 */
+} ps_fusion_params;
+void ps_fusion_params_default(ps_fusion_params* out);
+/* Camera of one view for fusion (DenseView, crates/dense/src/scene.rs): world -> camera x_c = R x_w + t with R
+ * row-major, intrinsics k = fx, fy, cx, cy, the representative baseline (median distance to its source centres,
+ * crates/dense/src/densify.rs:260-275; 0 = no inverse-variance weight), the point-key image id and the overlap list
+ * (views to check, in order; crates/dense/src/densify.rs:519). */
+typedef struct ps_fusion_view {
+  double k[4];
+  double r[9];
+  double t[3];
+  double baseline;
+  uint32_t image_id;
+  uint32_t num_overlap;
+  const uint32_t* overlap;
+} ps_fusion_view;
+/* Consistency fusion (crates/dense/src/fusion.rs:219-459) of the readout planes and final costs of `views` at
+ * `level`; cams[v] for every session view v (only the listed views are used).  Views are fused in index order.  The
+ * point cloud stays in the session; num_points receives its size.  Colours are the gray image value as u8. */
+int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
+                     const ps_fusion_params* p, uint64_t* num_points);
+/* The fused points in the reference's order (ascending point key (image_id << 32) | (row << 16) | col): positions
+ * and normals 3 floats, colours 3 bytes, keys, the number of contributing views and their indices (ascending,
+ * vis_stride >= consistency_num_images + 1 entries per point).  Any output may be NULL. */
+int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
+                    uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride);
+
+/* DenseOutput::write_ply (crates/dense/src/densify.rs:143-153; crates/core/src/io/ply.rs:82-140, layout
+ * XyzNormalRgb): binary little-endian PLY "x y z [nx ny nz] red green blue" (float / uchar), 27 bytes per point with
+ * normals.  normals and colors may be NULL (colour 255 then). */
+int ps_write_ply(const char* path, uint64_t n, const float* positions, const float* normals, const uint8_t* colors);
+
 /* ---- measurement (no reference counterpart; replaces CUMULUS3D_CUDA_TRACE, crates/cuda/src/patchmatch.rs:780-797) */
 typedef enum ps_kernel_kind {
   PS_KERNEL_HALF = 0,

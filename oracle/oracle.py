@@ -39,6 +39,14 @@ def lib() -> C.CDLL:
             "oracle_run_init": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int, C.c_int, C.c_int]),
             "oracle_sweep": (C.c_int, [_KI, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]),
+            "oracle_remove_speckles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
+                                                 C.c_double, C.c_float, C.POINTER(C.c_uint64)]),
+            "oracle_fuse": (C.c_int, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
+                                      C.POINTER(C.c_uint32), C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                      C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p,
+                                      C.POINTER(_lib.FusionParams), C.c_int, C.c_uint64, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                      C.POINTER(C.c_uint64)]),
             "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int]),
             "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
@@ -183,3 +191,44 @@ class OracleSession:
         for o, s in zip(outs, states):
             o.cost[...] = s.cost
         return outs
+
+
+def remove_speckles(depth: np.ndarray, normal: np.ndarray, cost: np.ndarray, post) -> int:
+    """remove_speckles restated (depth (h, w), normal (h, w, 3) updated in place); returns the erased pixel count."""
+    assert depth.dtype == np.float32 and normal.dtype == np.float32 and depth.flags.c_contiguous
+    h, w = depth.shape
+    c = np.ascontiguousarray(cost, np.float32)
+    n = C.c_uint64()
+    _chk(lib().oracle_remove_speckles(depth.ctypes.data, normal.ctypes.data, c.ctypes.data, w, h,
+                                      post.speckle_rel_depth, post.speckle_min_area_frac, post.speckle_keep_cost,
+                                      C.byref(n)), "remove_speckles")
+    return int(n.value)
+
+
+def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[int] = None):
+    """Consistency fusion restated.  cams: fusion.FusionCams of all views; depths/normals/costs/images per view (the
+    images as the engine stores them: f32, u8 inputs divided by 255 in binary32); only `views` are used.  Returns a
+    fusion.FusedCloud in the reference's point order."""
+    from cumulus3d_b200.fusion import FusedCloud
+    nv = len(depths)
+    ws = (C.c_uint32 * nv)(*[d.shape[1] for d in depths])
+    hs = (C.c_uint32 * nv)(*[d.shape[0] for d in depths])
+    keep = [np.ascontiguousarray(a, np.float32) for a in list(depths) + list(normals) + list(costs) + list(images)]
+    ptr = lambda arrs: (C.c_void_p * nv)(*[a.ctypes.data for a in arrs])
+    dp, np_, cp, ip = (ptr(keep[i * nv:(i + 1) * nv]) for i in range(4))
+    used = np.zeros(nv, np.uint8)
+    used[list(views)] = 1
+    cap = int(sum(int((d > 0).sum()) for d in depths)) + 1
+    stride = int(params.consistency_num_images) + 1
+    pos = np.empty((cap, 3), np.float32)
+    nrm = np.empty((cap, 3), np.float32)
+    col = np.empty((cap, 3), np.uint8)
+    key = np.empty(cap, np.uint64)
+    vc = np.empty(cap, np.uint8)
+    vis = np.empty((cap, stride), np.uint16)
+    n = C.c_uint64()
+    _chk(lib().oracle_fuse(nv, cams.table, ws, hs, dp, np_, cp, ip, used.ctypes.data, C.byref(params),
+                           _threads(threads), cap, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data, key.ctypes.data,
+                           vc.ctypes.data, vis.ctypes.data, stride, C.byref(n)), "fuse")
+    k = int(n.value)
+    return FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])

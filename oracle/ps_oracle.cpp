@@ -1207,4 +1207,252 @@ void oracle_pyramid_step(const uint8_t* src, size_t w, size_t h, const double* k
 float oracle_expf(float x) { return ps_expf(x); }
 void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
 
+
+// ================================================================================================ post-processing
+// remove_speckles (crates/dense/src/postproc.rs:77-129): depth-first growth from every unlabelled valid pixel in
+// row-major order over 4-neighbours with |d_j - d_i| <= rel·min(d_i, d_j); a component smaller than
+// ceil(w·h·frac) whose lower median cost (costs sorted by total order, element len/2) exceeds keep is erased
+// (depth 0, normal 0).  normal: 3 floats per pixel.
+int oracle_remove_speckles(float* depth, float* normal, const float* cost, uint32_t w, uint32_t h, float rel,
+                           double frac, float keep, uint64_t* removed) {
+  if (!depth || !normal || !cost) return PS_EINVAL;
+  const size_t n = (size_t)w * h;
+  const size_t min_area = (size_t)std::ceil((double)n * frac);
+  if (removed) *removed = 0;
+  if (min_area <= 1) return PS_OK;
+  std::vector<uint32_t> label(n, UINT32_MAX);
+  std::vector<size_t> stack, comp;
+  std::vector<float> costs;
+  uint64_t erased = 0;
+  auto total_less = [](float a, float b) {  // f32::total_cmp
+    int32_t ia, ib;
+    memcpy(&ia, &a, 4);
+    memcpy(&ib, &b, 4);
+    ia ^= (int32_t)((uint32_t)(ia >> 31) >> 1);
+    ib ^= (int32_t)((uint32_t)(ib >> 31) >> 1);
+    return ia < ib;
+  };
+  for (size_t start = 0; start < n; ++start) {
+    if (depth[start] <= 0.0f || label[start] != UINT32_MAX) continue;
+    comp.clear();
+    stack.push_back(start);
+    label[start] = (uint32_t)start;
+    while (!stack.empty()) {
+      const size_t i = stack.back();
+      stack.pop_back();
+      comp.push_back(i);
+      const size_t x = i % w, y = i / w;
+      const float di = depth[i];
+      size_t nb[4] = {SIZE_MAX, SIZE_MAX, SIZE_MAX, SIZE_MAX};
+      if (x > 0) nb[0] = i - 1;
+      if (x + 1 < w) nb[1] = i + 1;
+      if (y > 0) nb[2] = i - w;
+      if (y + 1 < h) nb[3] = i + w;
+      for (size_t j : nb) {
+        if (j == SIZE_MAX || label[j] != UINT32_MAX || depth[j] <= 0.0f) continue;
+        if (std::fabs(depth[j] - di) <= rel * std::min(di, depth[j])) {
+          label[j] = (uint32_t)start;
+          stack.push_back(j);
+        }
+      }
+    }
+    if (comp.size() < min_area) {
+      costs.clear();
+      for (size_t i : comp) costs.push_back(cost[i]);
+      std::sort(costs.begin(), costs.end(), total_less);
+      if (costs[costs.size() / 2] > keep) {
+        for (size_t i : comp) {
+          depth[i] = 0.0f;
+          normal[3 * i] = normal[3 * i + 1] = normal[3 * i + 2] = 0.0f;
+        }
+        erased += comp.size();
+      }
+    }
+  }
+  if (removed) *removed = erased;
+  return PS_OK;
+}
+
+// Consistency fusion (crates/dense/src/fusion.rs:219-459, residual handling "none", colour = gray u8 of `img`).
+// Views in index order (used[v] != 0); within a view every pixel is evaluated independently (rows in parallel, the
+// result does not depend on it).  Points are written in the reference's order into caller buffers of `capacity`
+// points; vis holds vis_stride entries per point.  Returns the point count in *count.
+namespace {
+struct FCam {
+  double k[4], r[9], t[3], baseline;
+  int w, h;
+};
+void f_backproject(const FCam& c, double col, double row, double d, double* X) {
+  const double cc[3] = {(col - c.k[2]) / c.k[0] * d, (row - c.k[3]) / c.k[1] * d, d};
+  const double p[3] = {cc[0] - c.t[0], cc[1] - c.t[1], cc[2] - c.t[2]};
+  X[0] = c.r[0] * p[0] + c.r[3] * p[1] + c.r[6] * p[2];
+  X[1] = c.r[1] * p[0] + c.r[4] * p[1] + c.r[7] * p[2];
+  X[2] = c.r[2] * p[0] + c.r[5] * p[1] + c.r[8] * p[2];
+}
+bool f_project(const FCam& c, const double* x, double* u, double* v, double* z) {
+  const double cz = c.r[6] * x[0] + c.r[7] * x[1] + c.r[8] * x[2] + c.t[2];
+  if (cz <= 0.0) return false;
+  const double cx = c.r[0] * x[0] + c.r[1] * x[1] + c.r[2] * x[2] + c.t[0];
+  const double cy = c.r[3] * x[0] + c.r[4] * x[1] + c.r[5] * x[2] + c.t[1];
+  *u = c.k[0] * cx / cz + c.k[2];
+  *v = c.k[1] * cy / cz + c.k[3];
+  *z = cz;
+  return true;
+}
+void f_normal(const FCam& c, const float* n3, double* n) {
+  const double m[3] = {(double)n3[0], (double)n3[1], (double)n3[2]};
+  n[0] = c.r[0] * m[0] + c.r[3] * m[1] + c.r[6] * m[2];
+  n[1] = c.r[1] * m[0] + c.r[4] * m[1] + c.r[7] * m[2];
+  n[2] = c.r[2] * m[0] + c.r[5] * m[1] + c.r[8] * m[2];
+}
+double f_inv_var(const ps_fusion_params& p, const FCam& c, double d, float cost) {
+  if (!p.inverse_variance || !(c.baseline > 0.0)) return 1.0;
+  const double spx = p.sigma_px0 + p.sigma_px_slope * (double)std::min(std::max(cost, 0.0f), 2.0f);
+  const double sd = d * d * spx / (c.k[0] * c.baseline);
+  return 1.0 / std::max(sd * sd, 1e-300);
+}
+double f_gray(const float* img, const FCam& c, int col, int row) {
+  const int x = std::min(col, c.w - 1), y = std::min(row, c.h - 1);
+  const float v = img[(size_t)y * c.w + x] * 255.0f;
+  return (double)(uint8_t)std::min(std::max(std::nearbyint(v), 0.0f), 255.0f);
+}
+struct FPoint {
+  float pos[3], nrm[3];
+  uint8_t col[3];
+  uint64_t key;
+  std::vector<uint16_t> vis;
+};
+}  // namespace
+
+int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* widths, const uint32_t* heights,
+                const float* const* depth, const float* const* normal, const float* const* cost,
+                const float* const* img, const uint8_t* used, const ps_fusion_params* p, int threads,
+                uint64_t capacity, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
+                uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count) {
+  if (!cams || !widths || !heights || !depth || !normal || !cost || !img || !used || !p || !count) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<FCam> fc(nviews);
+  for (uint32_t v = 0; v < nviews; ++v) {
+    memcpy(fc[v].k, cams[v].k, sizeof fc[v].k);
+    memcpy(fc[v].r, cams[v].r, sizeof fc[v].r);
+    memcpy(fc[v].t, cams[v].t, sizeof fc[v].t);
+    fc[v].baseline = cams[v].baseline;
+    fc[v].w = (int)widths[v];
+    fc[v].h = (int)heights[v];
+  }
+  std::vector<std::vector<uint8_t>> marks(nviews);
+  for (uint32_t v = 0; v < nviews; ++v)
+    if (used[v]) marks[v].assign((size_t)fc[v].w * fc[v].h, 0);
+  const double cos_n = std::cos(ps_to_radians_f64(p->max_normal_error_deg));
+  const double r2 = p->max_reproj_error * p->max_reproj_error;
+  uint64_t n_out = 0;
+  for (uint32_t v = 0; v < nviews; ++v) {
+    if (!used[v]) continue;
+    const FCam& cv = fc[v];
+    std::vector<int> ov;
+    for (uint32_t j = 0; j < cams[v].num_overlap && ov.size() < p->consistency_num_images; ++j) {
+      const uint32_t o = cams[v].overlap[j];
+      if (o < nviews && used[o] && o != v) ov.push_back((int)o);
+    }
+    std::vector<std::vector<FPoint>> rows(cv.h);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int row = 0; row < cv.h; ++row) {
+      std::vector<std::pair<int, int>> hits;
+      for (int col = 0; col < cv.w; ++col) {
+        const size_t pix = (size_t)row * cv.w + col;
+        if (depth[v][pix] <= 0.0f) continue;
+        if (p->mark_used && __atomic_load_n(&marks[v][pix], __ATOMIC_RELAXED) != 0) continue;
+        const double d = (double)depth[v][pix];
+        double x[3], nw[3];
+        f_backproject(cv, (double)col, (double)row, d, x);
+        f_normal(cv, normal[v] + 3 * pix, nw);
+        const double w0 = f_inv_var(*p, cv, d, cost[v][pix]);
+        double sw = w0;
+        double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
+        double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
+        const double c0 = f_gray(img[v], cv, col, row);
+        double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
+        hits.clear();
+        for (int o : ov) {
+          const FCam& oc = fc[o];
+          double u, vv, z;
+          if (!f_project(oc, x, &u, &vv, &z)) continue;
+          const double cu = std::floor(u + 0.5), rv = std::floor(vv + 0.5);
+          if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
+          const size_t opix = (size_t)rv * oc.w + (size_t)cu;
+          const double od = (double)depth[o][opix];
+          if (od <= 0.0 || std::fabs(z - od) / od > p->max_depth_error) continue;
+          double xo[3];
+          f_backproject(oc, cu, rv, od, xo);
+          double bu, bv, bz;
+          if (!f_project(cv, xo, &bu, &bv, &bz)) continue;
+          const double eu = bu - (double)col, ev = bv - (double)row;
+          if (eu * eu + ev * ev > r2) continue;
+          double no[3];
+          f_normal(oc, normal[o] + 3 * opix, no);
+          if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < cos_n) continue;
+          const double co = f_gray(img[o], oc, (int)cu, (int)rv);
+          const double wo = f_inv_var(*p, oc, od, cost[o][opix]);
+          sw += wo;
+          for (int k = 0; k < 3; ++k) {
+            sx[k] += wo * xo[k];
+            sn[k] += wo * no[k];
+            sc[k] += wo * co;
+          }
+          hits.push_back({o, (int)opix});
+        }
+        if (hits.size() < p->min_consistent_views) continue;
+        const double m = sw;
+        const double l = std::sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+        if (l < 1.1920928955078125e-07) continue;
+        if (p->mark_used) {
+          for (auto& hq : hits) {
+            const FCam& oc = fc[hq.first];
+            if (p->mark_radius == 0) {
+              __atomic_store_n(&marks[hq.first][hq.second], (uint8_t)1, __ATOMIC_RELAXED);
+              continue;
+            }
+            const int cx0 = hq.second % oc.w, cy0 = hq.second / oc.w, r = (int)p->mark_radius;
+            const double d0 = (double)depth[hq.first][hq.second];
+            for (int yy = std::max(cy0 - r, 0); yy <= std::min(cy0 + r, oc.h - 1); ++yy)
+              for (int xx = std::max(cx0 - r, 0); xx <= std::min(cx0 + r, oc.w - 1); ++xx) {
+                const size_t qq = (size_t)yy * oc.w + xx;
+                const double dq = (double)depth[hq.first][qq];
+                if (dq > 0.0 && std::fabs(dq - d0) <= p->max_depth_error * d0)
+                  __atomic_store_n(&marks[hq.first][qq], (uint8_t)1, __ATOMIC_RELAXED);
+              }
+          }
+        }
+        FPoint pt;
+        for (int k = 0; k < 3; ++k) {
+          pt.pos[k] = (float)(sx[k] / m);
+          pt.nrm[k] = (float)(sn[k] / l);
+          pt.col[k] = (uint8_t)std::round(sc[k] / m);
+        }
+        pt.key = ((uint64_t)cams[v].image_id << 32) | ((uint64_t)(row & 0xffff) << 16) | (uint64_t)(col & 0xffff);
+        pt.vis.push_back((uint16_t)v);
+        for (auto& hq : hits) pt.vis.push_back((uint16_t)hq.first);
+        std::sort(pt.vis.begin(), pt.vis.end());
+        pt.vis.erase(std::unique(pt.vis.begin(), pt.vis.end()), pt.vis.end());
+        rows[row].push_back(std::move(pt));
+      }
+    }
+    for (auto& r : rows)
+      for (auto& pt : r) {
+        if (n_out < capacity) {
+          if (positions) memcpy(positions + 3 * n_out, pt.pos, 12);
+          if (normals) memcpy(normals + 3 * n_out, pt.nrm, 12);
+          if (colors) memcpy(colors + 3 * n_out, pt.col, 3);
+          if (keys) keys[n_out] = pt.key;
+          if (vis_counts) vis_counts[n_out] = (uint8_t)pt.vis.size();
+          if (vis)
+            for (uint32_t t = 0; t < vis_stride; ++t) vis[n_out * vis_stride + t] = t < pt.vis.size() ? pt.vis[t] : 0;
+        }
+        n_out++;
+      }
+  }
+  *count = n_out;
+  return n_out <= capacity ? PS_OK : PS_EINVAL;
+}
+
 }  // extern "C"

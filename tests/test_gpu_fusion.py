@@ -1,0 +1,79 @@
+"""Speckle removal and consistency fusion on the GPU against the CPU oracle, bit for bit (zero tolerance: integer
+labels and comparisons, and FP64 fusion arithmetic in the same operation order on both sides)."""
+import numpy as np
+import pytest
+
+from cumulus3d_b200 import fusion, scenes
+from cumulus3d_b200.patchstereo import PatchMatchBackend
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pipeline():
+    """A short full schedule on 6 views (2 formation stations), read out on the device."""
+    wl = scenes.workload_small(160, 120, views=6, window_radius=3, seed=21, iters=2, sources=4, positions=2)
+    views = list(range(len(wl.cams)))
+    be = PatchMatchBackend(0, math="parity")
+    s = be.begin(wl.input)
+    s.schedule_resident(views, 2, 1, 1, graph=False)
+    s.synchronize()
+    yield wl, views, s
+    s.close()
+    be.close()
+
+
+def _speckles_ref(states, post):
+    out, removed = [], 0
+    for st in states:
+        d = st.depth.copy()
+        n = st.normal.copy()
+        removed += oracle.remove_speckles(d, n, st.cost, post)
+        out.append((d, n))
+    return out, removed
+
+
+@pytest.mark.parametrize("frac", [2e-4, 0.01])
+def test_speckles_bitwise_vs_oracle(pipeline, frac):
+    wl, views, s = pipeline
+    before = s.readout_resident(views)
+    post = fusion.default_post()
+    post.speckle_min_area_frac = frac
+    want, n_ref = _speckles_ref(before, post)
+    n = s.postprocess_resident(0, views, post)
+    got = s.readout_download(0, views)
+    assert n == n_ref
+    if frac == 0.01:
+        assert n > 0  # the case removes something
+    for g, (d, nn) in zip(got, want):
+        np.testing.assert_array_equal(g.depth, d)
+        np.testing.assert_array_equal(g.normal, nn)
+
+
+def test_fusion_bitwise_vs_oracle(pipeline):
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    prm = fusion.default_fusion(3)
+    n = s.fuse_resident(0, views, fc, prm)
+    got = s.fused_points()
+    want = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
+                       list(wl.images), views, prm)
+    assert n == len(want) > 0
+    np.testing.assert_array_equal(got.keys, want.keys)
+    np.testing.assert_array_equal(got.positions, want.positions)
+    np.testing.assert_array_equal(got.normals, want.normals)
+    np.testing.assert_array_equal(got.colors, want.colors)
+    np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
+    for i in range(len(want)):
+        assert got.visibility(i) == want.visibility(i)
+    # the subset without view 0 (view 0's pixels neither references nor partners)
+    n2 = s.fuse_resident(0, views[1:], fc, prm)
+    want2 = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
+                        list(wl.images), views[1:], prm)
+    assert n2 == len(want2)
+    np.testing.assert_array_equal(s.fused_points().keys, want2.keys)

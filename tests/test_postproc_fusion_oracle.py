@@ -1,0 +1,113 @@
+"""Post-processing and fusion restatements on the CPU, pinned by the reference's own tests: the speckle known answer
+of crates/dense/src/postproc.rs (tests::speckle_and_fill), the PLY layout of crates/dense/tests/host_parts.rs
+(ply_output_layout), and the fusion properties of host_parts.rs (fused ground-truth maps lie on the surface; the
+result is deterministic; a view whose depth is scaled by 2 % stops merging at the 1 % tolerance)."""
+import numpy as np
+import pytest
+
+from cumulus3d_b200 import fusion, scenes
+from oracle import oracle
+
+
+def _speckle_case():
+    w, h = 40, 30
+    d = np.full((h, w), 10.0, np.float32)
+    n = np.tile(np.float32([0, 0, -1]), (h, w, 1))
+    c = np.full((h, w), 0.5, np.float32)
+    for (x, y) in [(5, 5), (6, 5), (5, 6), (6, 6)]:
+        d[y, x] = 5.0
+    d[20:23, 20:23] = 0.0
+    p = fusion.default_post()
+    p.speckle_min_area_frac = 10.0 / (w * h)
+    return d, n, c, p
+
+
+def test_speckle_known_answer():
+    d, n, c, p = _speckle_case()
+    assert oracle.remove_speckles(d, n, c, p) == 4
+    assert d[5, 5] == 0.0 and (n[5, 5] == 0).all()
+    assert d[0, 0] == 10.0
+
+
+def test_speckle_keeps_low_cost_components_and_defaults():
+    d, n, c, p = _speckle_case()
+    c[5:7, 5:7] = 0.1  # median cost 0.1 <= keep 0.2: kept
+    assert oracle.remove_speckles(d, n, c, p) == 0
+    p = fusion.default_post()
+    assert (p.remove_speckles, round(p.speckle_rel_depth, 6), p.speckle_min_area_frac,
+            round(p.speckle_keep_cost, 6)) == (1, 0.02, 2e-4, 0.2)
+    d, n, c, _ = _speckle_case()
+    assert oracle.remove_speckles(d, n, c, p) == 0  # ceil(1200·2e-4) = 1: off
+
+
+def test_speckle_components_do_not_depend_on_scan_order():
+    rng = np.random.default_rng(3)
+    d = rng.choice([0.0, 10.0, 10.1, 13.0], size=(48, 64), p=[0.3, 0.3, 0.2, 0.2]).astype(np.float32)
+    c = rng.uniform(0, 1, d.shape).astype(np.float32)
+    p = fusion.default_post()
+    p.speckle_min_area_frac = 0.005
+    a, na = d.copy(), np.zeros(d.shape + (3,), np.float32)
+    b, nb = d[::-1, ::-1].copy(), np.zeros(d.shape + (3,), np.float32)
+    ra = oracle.remove_speckles(a, na, c, p)
+    rb = oracle.remove_speckles(b, nb, c[::-1, ::-1].copy(), p)
+    assert ra == rb > 0
+    np.testing.assert_array_equal(a, b[::-1, ::-1])
+
+
+def test_ply_layout_matches_reference(tmp_path):
+    f = tmp_path / "a.ply"
+    pos = np.float32([[1, 2, 3], [4, 5, 6]])
+    nrm = np.float32([[0, 0, 1], [0, 0, 1]])
+    col = np.uint8([[1, 2, 3], [4, 5, 6]])
+    fusion.write_ply(f, pos, nrm, col)
+    b = f.read_bytes()
+    hdr = ("ply\nformat binary_little_endian 1.0\nelement vertex 2\nproperty float x\nproperty float y\n"
+           "property float z\nproperty float nx\nproperty float ny\nproperty float nz\nproperty uchar red\n"
+           "property uchar green\nproperty uchar blue\nend_header\n").encode()
+    assert b[:len(hdr)] == hdr
+    assert len(b) - len(hdr) == 54
+    rec = np.frombuffer(b[len(hdr):], dtype=np.dtype([("p", "<f4", 3), ("n", "<f4", 3), ("c", "u1", 3)]))
+    np.testing.assert_array_equal(rec["p"], pos)
+    np.testing.assert_array_equal(rec["c"], col)
+
+
+@pytest.fixture(scope="module")
+def gt_scene():
+    wl = scenes.workload_small(160, 120, views=6, window_radius=3, seed=3, positions=2)
+    src = [list(kv.sources) for kv in wl.input.views]
+    return wl, fusion.FusionCams(wl.cams, src)
+
+
+def _fuse_gt(wl, fc, depths=None, threads=None, min_views=3):
+    d = [g.astype(np.float32) for g in (depths if depths is not None else wl.gt_depth)]
+    n = [g.astype(np.float32) for g in wl.gt_normal]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    return oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), fusion.default_fusion(min_views), threads)
+
+
+def test_fusion_of_true_maps_lies_on_surfaces(gt_scene):
+    wl, fc = gt_scene
+    cl = _fuse_gt(wl, fc)
+    assert len(cl) > 0.05 * sum(g.size for g in wl.gt_depth)
+    assert (cl.vis_counts >= 4).all()  # reference + at least 3 agreeing views
+    keys = cl.keys.astype(np.int64)
+    assert (np.diff(keys) > 0).all()  # reference order: ascending keys
+    err = []
+    for i in range(0, len(cl), 37):
+        v, row, col = int(keys[i] >> 32), int((keys[i] >> 16) & 0xFFFF), int(keys[i] & 0xFFFF)
+        pc = wl.cams[v].r @ cl.positions[i].astype(np.float64) + wl.cams[v].t
+        err.append(abs(pc[2] - wl.gt_depth[v][row, col]) / wl.gt_depth[v][row, col])
+    assert np.max(err) < 0.01 and np.median(err) < 0.002
+    again = _fuse_gt(wl, fc, threads=1)
+    np.testing.assert_array_equal(again.keys, cl.keys)
+    np.testing.assert_array_equal(again.positions, cl.positions)
+
+
+def test_fusion_depth_tolerance(gt_scene):
+    wl, fc = gt_scene
+    base = _fuse_gt(wl, fc)
+    scaled = [g.copy() for g in wl.gt_depth]
+    scaled[2] = scaled[2] * 1.02
+    sc = _fuse_gt(wl, fc, scaled)
+    merged = lambda cl: int(sum(1 for i in range(len(cl)) if 2 in cl.visibility(i) and cl.vis_counts[i] > 1))
+    assert merged(sc) * 50 < merged(base)

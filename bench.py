@@ -120,6 +120,8 @@ def make_workload(args, rank: int, shard_job: bool):
         return scenes.workload_c1(seed=1 + seed_shift)
     if args.workload == "c3":
         return scenes.workload_c3(seed=3 + seed_shift)
+    if args.workload == "c5":
+        return scenes.workload_c5(seed=5 + seed_shift, views=args.views)
     return scenes.workload_c2(seed=2 + seed_shift, with_gt=False, views=args.views)
 
 
@@ -234,8 +236,19 @@ def bench_ours(args, rank, world, local):
         "gpu_launches": int(launches),
         "clocks": clk.summary(),
     }
+    hbm = [hbm_used(local)]
+    if not shard_job:
+        res["fusion"] = fusion_stage(args, wl, sess, mine, check=rank == 0 and not args.no_check)
+        hbm.append(hbm_used(local))
+        if rank == 0 and not args.no_check:
+            res["fp64_reeval"] = fp64_check(wl, sess, mine)
     if not args.no_learned and not shard_job:
         res["learned"] = learned_leg(args, wl, sess, stream, mine, value, ms_step, barrier, local)
+        res["learned"]["fused_vs_plain"] = round(res["learned"]["fused_points"] / max(res["fusion"]["points"], 1), 4)
+        hbm.append(hbm_used(local))
+    if args.latency or args.workload == "c5":
+        res["latency"] = view_latency(wl, sess, stream, mine)
+    res["hbm_high_water_gb"] = round(max(hbm) / 1e9, 2)
     sess.close()
     # ---- e2e through the host-buffer C ABI (session begin uploads the images) ----
     if not args.no_e2e:
@@ -250,6 +263,80 @@ def bench_ours(args, rank, world, local):
         dist.barrier()
         dist.destroy_process_group()
     return res
+
+
+def hbm_used(device):
+    """Device memory in use (all allocations on the GPU, from cudaMemGetInfo)."""
+    import torch
+    free, total = torch.cuda.mem_get_info(device)
+    return total - free
+
+
+def fp64_check(wl, sess, mine):
+    """FP64 re-evaluation of the final hypotheses of the first view: the engine's FP32 top-K photometric cost of the
+    post-processed planes (ps_evaluate) against the oracle's binary64 restatement of the same cost."""
+    from cumulus3d_b200.patchstereo import ViewState
+    from oracle import oracle
+    v = mine[0]
+    st = sess.readout_download(0, [v])
+    f32 = sess.evaluate(0, [v], st)[0].astype(np.float64)
+    t0 = time.perf_counter()
+    f64 = oracle.reeval_f64(wl.input, 0, [v], st)[0]
+    dt = time.perf_counter() - t0
+    m = st[0].depth > 0
+    e = np.abs(f32 - f64)[m]
+    return {"view": v, "pixels": int(m.sum()), "max_abs_cost_err": float(e.max()) if e.size else None,
+            "mean_abs_cost_err": float(e.mean()) if e.size else None,
+            "p99_abs_cost_err": float(np.percentile(e, 99)) if e.size else None,
+            "frac_err_above_1e-3": float((e > 1e-3).mean()) if e.size else None, "oracle_s": round(dt, 2),
+            "what": "top-K photometric cost (1 - NCC) of the final planes: FP32 engine vs FP64 CPU re-evaluation"}
+
+
+def view_latency(wl, sess, stream, mine):
+    """Latency of one view's photometric run alone on the GPU (run start + the workload's photometric iterations),
+    CUDA-event timed per view: p50 / p99 over the job's views.  (In the batched schedule every view completes with the
+    job.)"""
+    import torch
+    from cumulus3d_b200.patchstereo import RunParams
+    ms = []
+    for v in mine:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sess.run_resident([v], RunParams(0, False, True, wl.photometric_iters, 1))
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return {"p50_ms": round(float(np.percentile(ms, 50)), 2), "p99_ms": round(float(np.percentile(ms, 99)), 2),
+            "views": len(ms), "what": f"one view, run start + {wl.photometric_iters} photometric iterations"}
+
+
+def fusion_stage(args, wl, sess, mine, check=True, label="plain"):
+    """Readout -> speckle removal -> consistency fusion (min 3 agreeing views) on the resident maps of the last step;
+    with `check`, the CPU oracle fuses the same maps and must give the same point count."""
+    import torch
+    from cumulus3d_b200 import fusion
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    prm = fusion.default_fusion(3)
+    sess.readout_resident(mine, download=False)
+    sess.synchronize()
+    t0 = time.perf_counter()
+    removed = sess.postprocess_resident(0, mine)
+    n = sess.fuse_resident(0, mine, fc, prm)
+    dt = time.perf_counter() - t0
+    out = {"points": n, "speckle_pixels_removed": removed, "ms": round(dt * 1e3, 2),
+           "params": "speckles (rel 0.02, area 2e-4, keep 0.2); consistency fusion min 3 views, 12 overlap views, "
+                     "1 % depth, 2 px, 10 deg, inverse-variance weights"}
+    if check:
+        from oracle import oracle
+        st = sess.readout_download(0, mine)
+        t1 = time.perf_counter()
+        imgs = [kv.levels[0].pixels for kv in wl.input.views]  # f32 planes, as the engine stores them
+        ref = oracle.fuse(fc, [x.depth for x in st], [x.normal for x in st], [x.cost for x in st], imgs, mine, prm)
+        out["oracle_points"] = len(ref)
+        out["oracle_s"] = round(time.perf_counter() - t1, 2)
+        out["oracle_cores"] = os.cpu_count() or 1
+    return out
 
 
 def net_flop_per_pixel():
@@ -301,6 +388,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     sweep_stats = sess.kernel_stats(_lib.PS_KERNEL_SWEEP)
     sess.set_profiling(False)
     learned_depth = depth()
+    learned_fused = fusion_stage(args, wl, sess, mine, check=False)["points"]
     ms_short = timed(lambda: sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters,
                                                      graph=not args.no_graph), 1, 2)
     short_depth = depth()
@@ -335,6 +423,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
                      "coverage_plain": round(float(ref_valid.mean()), 4),
                      "definition": "fraction of the plain schedule's valid pixels whose final depth is within 1 % "
                                    "of it; the plain schedule rerun with another RNG seed sets the floor"},
+        "fused_points": learned_fused,
         "plain_same_iterations": {"value": round(n / (ms_short / 1e3), 3), "ms_per_step": round(ms_short, 2),
                                   "agree_with_plain": agree(short_depth),
                                   "coverage": round(float((short_depth > 0).mean()), 4)},
@@ -466,13 +555,16 @@ def main():
     ap.add_argument("--math", default="parity", choices=["parity", "fast"])
     ap.add_argument("--tuning", type=int, default=-1, help="half-step variant (PS_TUNE_* flags); -1 = autotune")
     ap.add_argument("--shard-job", action="store_true", help="shard one job's views over the ranks (strong scaling)")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3"],
-                    help="c2 = the metric's drone-scale configuration (default); c1/c3 = the other configurations")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c1", "c3", "c5"],
+                    help="c2 = the metric's drone-scale configuration (default); c1/c3/c5 = the other configurations")
+    ap.add_argument("--latency", action="store_true", help="per-view latency p50/p99 (always on for c5)")
     ap.add_argument("--views", type=int, default=None,
                     help="first N views of the workload only (small profiling cases, not a bench line)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="issue the schedule's launches directly (no CUDA graph)")
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-check", action="store_true",
+                    help="skip the CPU oracle checks (fused point count, FP64 re-evaluation)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-init schedule")
     ap.add_argument("--learned-iters", type=int, default=3,
                     help="photometric iterations of the learned-init schedule")

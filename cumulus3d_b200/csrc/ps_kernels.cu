@@ -814,7 +814,7 @@ __device__ __forceinline__ unsigned short bf16_bits(float v) {
   return *reinterpret_cast<const unsigned short*>(&b);
 }
 
-template <int WR, int WS>
+template <int WR, int WS, bool TEX>
 __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_EVAL_NT;
   extern __shared__ float sm[];
@@ -850,8 +850,9 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__
     for (int j = 0; j < nuse; ++j) {
       const PsLevel S = P.lv[prs[j].src * P.nlevels + P.level];
       float H[9];
-      c += homography(e.R, lps[j], (float)x, (float)y, h, H) ? ncc_cost<WR, WS, true, NT>(P, rw, rs, S, H, x, y, nwin)
-                                                             : 2.0f;
+      c += homography(e.R, lps[j], (float)x, (float)y, h, H)
+               ? ncc_cost<WR, WS, true, NT, TEX>(P, rw, rs, S, H, x, y, nwin)
+               : 2.0f;
     }
     c = nuse == 2 ? c * 0.5f : (nuse == 1 ? c : 2.0f);
     out[1 + k] = bf16_bits(c);
@@ -1255,13 +1256,19 @@ cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st) {
 }
 size_t sweep_smem(int wr, int ws) { return eval_smem(wr, ws, true); }
 
-cudaError_t launch_sweep(const PsRun& P, cudaStream_t st) {
+// `tex`: sample sources through their texture objects (tex2Dgather; same bits as the software bilinear).
+cudaError_t launch_sweep(const PsRun& P, bool tex, cudaStream_t st) {
   const size_t smem = sweep_smem(P.wr, P.sweep_ws);
-  if (P.wr == 6 && P.sweep_ws == 2) return launch(k_sweep<6, 2>, P.ntiles, PS_EVAL_NT, smem, st, P);
-  if (P.wr == 5 && P.sweep_ws == 2) return launch(k_sweep<5, 2>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  if (P.wr == 6 && P.sweep_ws == 2)
+    return tex ? launch(k_sweep<6, 2, true>, P.ntiles, PS_EVAL_NT, smem, st, P)
+               : launch(k_sweep<6, 2, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  if (P.wr == 5 && P.sweep_ws == 2)
+    return tex ? launch(k_sweep<5, 2, true>, P.ntiles, PS_EVAL_NT, smem, st, P)
+               : launch(k_sweep<5, 2, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
   PsRun Q = P;
   Q.ws = P.sweep_ws;  // the generic kernel reads the window step from the parameters
-  return launch(k_sweep<0, 1>, Q.ntiles, PS_EVAL_NT, smem, st, Q);
+  return tex ? launch(k_sweep<0, 1, true>, Q.ntiles, PS_EVAL_NT, smem, st, Q)
+             : launch(k_sweep<0, 1, false>, Q.ntiles, PS_EVAL_NT, smem, st, Q);
 }
 
 // Module constants (propagation offsets); called at session begin, outside any stream capture.

@@ -36,7 +36,7 @@
   cudaError_t launch_median(const PsRun& P, cudaStream_t st);                                              \
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
   cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
-  cudaError_t launch_sweep(const PsRun& P, cudaStream_t st);                                               \
+  cudaError_t launch_sweep(const PsRun& P, bool tex, cudaStream_t st);                                     \
   cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
   cudaError_t prepare();                                                                                   \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
@@ -56,7 +56,7 @@ struct Launchers {
   cudaError_t (*snapshot)(const PsRun&, float*, cudaStream_t);
   cudaError_t (*readout)(const PsRun&, float4*, cudaStream_t);
   int (*half_lanes)(unsigned);
-  cudaError_t (*sweep)(const PsRun&, cudaStream_t);
+  cudaError_t (*sweep)(const PsRun&, bool, cudaStream_t);
 };
 const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
                            ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
@@ -1321,7 +1321,8 @@ void enqueue_sweep(ps_session* s, int level, uint32_t view, unsigned short* out,
   P.netin_pitch = row_pixels;
   P.sweep_ws = 2;
   set_items(s, P, &view, 0, 1, level, PS_EVAL_PW, PS_EVAL_PH);
-  timed_launch(s, PS_KERNEL_SWEEP, P, [&](const PsRun& q) { return s->L->sweep(q, s->st); }, "sweep kernel");
+  const bool tex = (s->tuning & PS_TUNE_TEX_GATHER) != 0;  // the session built texture objects for its planes
+  timed_launch(s, PS_KERNEL_SWEEP, P, [&](const PsRun& q) { return s->L->sweep(q, tex, s->st); }, "sweep kernel");
 }
 
 template <typename T>

@@ -95,10 +95,11 @@ def test_network_gradients_match_fp64_oracle():
     assert cos > 0.999, report
 
 
-@pytest.mark.parametrize("wr,size", [(3, (64, 48)), (6, (80, 64))])
-def test_sweep_bitwise_vs_oracle(wr, size):
+@pytest.mark.parametrize("wr,size,tuning", [(3, (64, 48), 0), (6, (80, 64), 0), (6, (80, 64), 6), (3, (64, 48), 2)])
+def test_sweep_bitwise_vs_oracle(wr, size, tuning):
+    """Software bilinear (tuning 0) and texture-gather sampling (tuning with PS_TUNE_TEX_GATHER) give the same bits."""
     wl = scenes.workload_small(size[0], size[1], views=3, window_radius=wr, seed=11)
-    be = PatchMatchBackend(0, math="parity")
+    be = PatchMatchBackend(0, math="parity", tuning=tuning)
     w, h = size
     with be.begin(wl.input) as s:
         for v in range(3):

@@ -31,10 +31,10 @@ typedef __nv_bfloat16 bf16;
 
 namespace ps_cnn {
 
-// ------------------------------------------------------------------------------------------- conv forward (implicit GEMM)
-// C[p][co] = sum_{tap, ci} X[p shifted by tap][ci] * W[co][tap][ci];  M = pixels, N = Cout, K = 9·Cin.
-// CTA: 128 threads, tile 64 pixels × 64 output channels, K in chunks of 16 channels of one tap; warps 2×2, each
-// 32×32 = 2 (m16) × 4 (n8) mma tiles.
+// ------------------------------------------------------------------------------------------- tensor-core tiles
+// Convolution as an implicit GEMM: C[p][co] = sum_{tap, ci} X[p shifted by tap][ci] * W[co][tap][ci] (M = pixels,
+// N = cout, K = 9·cin) on mma.sync m16n8k16 (bf16 operands, f32 accumulators).  Weight-gradient tile (k_conv_wgrad):
+// 128 threads, 64 × 64 outputs, K in chunks of 16 pixels; warps 2 × 2, each 32 × 32 = 2 (m16) × 4 (n8) fragments.
 constexpr int CM = 64, CN = 64, CK = 16, CPAD = 8;
 
 __device__ __forceinline__ void mma_bf16(float* d, const uint32_t* a, const uint32_t* b) {
@@ -55,95 +55,140 @@ struct ConvArgs {
   int relu;
 };
 
-__global__ void __launch_bounds__(128) k_conv_fwd(ConvArgs a) {
-  __shared__ __align__(16) bf16 As[CM][CK + CPAD];
-  __shared__ __align__(16) bf16 Bs[CN][CK + CPAD];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int wm = warp >> 1, wn = warp & 1;
-  const long long M = (long long)a.B * a.H * a.W;
-  const long long m0 = (long long)blockIdx.x * CM;
-  const int n0 = blockIdx.y * CN;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) acc[i][j][k] = 0.f;
-  // the pixel this thread loads for A (two threads per pixel, 8 channels each)
-  const int lr = tid >> 1, lc = (tid & 1) * 8;
-  const long long lp = m0 + lr;
-  int ln = 0, ly = 0, lx = 0;
-  const bool lvalid = lp < M;
-  if (lvalid) {
-    ln = (int)(lp / ((long long)a.H * a.W));
-    const int rem = (int)(lp - (long long)ln * a.H * a.W);
-    ly = rem / a.W;
-    lx = rem - ly * a.W;
-  }
-  const int kchunks = (a.cin + CK - 1) / CK;  // cin is a multiple of 8: the last chunk may be half empty
-  for (int tap = 0; tap < 9; ++tap) {
-    const int dy = tap / 3 - 1, dx = tap % 3 - 1;
-    const int sy = ly + dy, sx = lx + dx;
-    const bool inb = lvalid && sy >= 0 && sy < a.H && sx >= 0 && sx < a.W;
-    const bf16* xrow = a.x + (((long long)ln * a.H + sy) * a.W + sx) * a.cin_stride + a.cin_off;
-    for (int kc = 0; kc < kchunks; ++kc) {
-      // A: 64 pixels × 16 channels
-      const bool kin = kc * CK + lc < a.cin;
-      uint4 va = make_uint4(0, 0, 0, 0);
-      if (inb && kin) va = *(const uint4*)(xrow + kc * CK + lc);
-      *(uint4*)&As[lr][lc] = va;
-      // B: 64 output channels × 16 k
-      {
-        const int co = n0 + lr;
-        uint4 vb = make_uint4(0, 0, 0, 0);
-        if (co < a.cout && kin) vb = *(const uint4*)(a.w + ((long long)co * 9 + tap) * a.cin + kc * CK + lc);
-        *(uint4*)&Bs[lr][lc] = vb;
-      }
-      __syncthreads();
-      const int g = lane >> 2, t = lane & 3;
-      uint32_t af[2][4], bfr[4][2];
-#pragma unroll
-      for (int i = 0; i < 2; ++i) {
-        const int r = wm * 32 + i * 16 + g;
-        af[i][0] = *(const uint32_t*)&As[r][t * 2];
-        af[i][1] = *(const uint32_t*)&As[r + 8][t * 2];
-        af[i][2] = *(const uint32_t*)&As[r][t * 2 + 8];
-        af[i][3] = *(const uint32_t*)&As[r + 8][t * 2 + 8];
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) {
-        const int c = wn * 32 + j * 8 + g;
-        bfr[j][0] = *(const uint32_t*)&Bs[c][t * 2];
-        bfr[j][1] = *(const uint32_t*)&Bs[c][t * 2 + 8];
-      }
-#pragma unroll
-      for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bfr[j]);
-      __syncthreads();
+
+// ------------------------------------------------------------------------------------------- conv forward, halo-tiled
+// The production convolution.  A CTA (8 warps) computes an 8 × 16 pixel output tile for BN output channels.  For each
+// chunk of 32 input channels it stages, with cp.async into a double buffer, the (8+2) × (16+2) halo of the input tile
+// and the chunk's weights for all 9 taps; every tap then reads its shifted A operand from the same halo copy.  Warp w
+// owns output row w of the tile (16 pixels = one m16 fragment) × BN columns; fragments come from shared memory through
+// ldmatrix (rows padded to 80 bytes, so the 8 row addresses of a matrix hit distinct banks).  Out-of-image halo pixels
+// and input channels beyond cin are zero-filled by the copy itself (source size 0).
+constexpr int HT_H = 8, HT_W = 16, HALO_W = HT_W + 2, HALO_PX = (HT_H + 2) * HALO_W;
+constexpr int KC = 32, KCP = 40;  // channels per stage, padded row length (bf16)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t* r, const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t* r, const void* p) {
+  asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];\n" : "=r"(r[0]), "=r"(r[1]) : "r"(smem_u32(p)));
+}
+
+template <int BN>
+constexpr size_t conv2_smem() {
+  return (size_t)2 * (HALO_PX * KCP + 9 * BN * KCP) * sizeof(bf16);
+}
+
+template <int BN>
+__global__ void __launch_bounds__(256) k_conv2(ConvArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  bf16* halo = reinterpret_cast<bf16*>(smraw);  // [2][HALO_PX][KCP]
+  bf16* wsm = halo + 2 * HALO_PX * KCP;         // [2][9][BN][KCP]
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tiles_x = (a.W + HT_W - 1) / HT_W, tiles_y = (a.H + HT_H - 1) / HT_H;
+  int t = blockIdx.x;
+  const int b = t / (tiles_x * tiles_y);
+  t -= b * tiles_x * tiles_y;
+  const int ty0 = (t / tiles_x) * HT_H, tx0 = (t % tiles_x) * HT_W;
+  const int n0 = blockIdx.y * BN;
+  const int nchunks = (a.cin + KC - 1) / KC;
+
+  auto load_stage = [&](int stage, int kc) {
+    const int c0 = kc * KC;
+    for (int i = tid; i < HALO_PX * 4; i += 256) {
+      const int px = i >> 2, seg = i & 3;
+      const int hy = px / HALO_W, hx = px - hy * HALO_W;
+      const int gy = ty0 + hy - 1, gx = tx0 + hx - 1, ch = c0 + seg * 8;
+      const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && ch < a.cin;
+      const bf16* src = ok ? a.x + (((long long)b * a.H + gy) * a.W + gx) * a.cin_stride + a.cin_off + ch : a.x;
+      cp_async16(halo + ((size_t)stage * HALO_PX + px) * KCP + seg * 8, src, ok ? 16 : 0);
     }
-  }
-  // epilogue
-  const int g = lane >> 2, t = lane & 3;
+    for (int i = tid; i < 9 * BN * 4; i += 256) {
+      const int seg = i & 3, r = i >> 2;
+      const int n = r % BN, tap = r / BN;
+      const int co = n0 + n, ch = c0 + seg * 8;
+      const bool ok = co < a.cout && ch < a.cin;
+      const bf16* src = ok ? a.w + ((long long)co * 9 + tap) * a.cin + ch : a.w;
+      cp_async16(wsm + (((size_t)stage * 9 + tap) * BN + n) * KCP + seg * 8, src, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+
+  float acc[BN / 8][4];
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+  for (int j = 0; j < BN / 8; ++j)
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long long p = m0 + wm * 32 + i * 16 + g + h * 8;
-      if (p >= M) continue;
+    for (int e = 0; e < 4; ++e) acc[j][e] = 0.f;
+
+  load_stage(0, 0);
+  for (int kc = 0; kc < nchunks; ++kc) {
+    if (kc + 1 < nchunks) {
+      load_stage((kc + 1) & 1, kc + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const int st = kc & 1;
+    const bf16* hs = halo + (size_t)st * HALO_PX * KCP;
+    const bf16* ws = wsm + (size_t)st * 9 * BN * KCP;
 #pragma unroll
-      for (int j = 0; j < 4; ++j)
+    for (int tap = 0; tap < 9; ++tap) {
+      const int dy = tap / 3, dx = tap - dy * 3;
 #pragma unroll
-        for (int e = 0; e < 2; ++e) {
-          const int co = n0 + wn * 32 + j * 8 + t * 2 + e;
-          if (co >= a.cout) continue;
-          float v = acc[i][j][h * 2 + e] + (a.bias ? a.bias[co] : 0.f);
-          if (a.relu) v = fmaxf(v, 0.f);
-          if (a.y) a.y[p * a.cout + co] = __float2bfloat16(v);
-          if (a.yf) a.yf[p * a.cout + co] = v;
+      for (int ks = 0; ks < 2; ++ks) {
+        uint32_t af[4];
+        ldsm_x4(af, hs + ((warp + dy) * HALO_W + (lane & 15) + dx) * KCP + ks * 16 + (lane >> 4) * 8);
+        const bf16* wt = ws + (size_t)tap * BN * KCP + ks * 16 + ((lane >> 3) & 1) * 8;
+#pragma unroll
+        for (int j = 0; j < BN / 8; j += 2) {
+          if (j + 1 < BN / 8) {
+            uint32_t bq[4];
+            ldsm_x4(bq, wt + (j * 8 + (lane >> 4) * 8 + (lane & 7)) * KCP);
+            mma_bf16(acc[j], af, bq);
+            mma_bf16(acc[j + 1], af, bq + 2);
+          } else {
+            uint32_t bq[2];
+            ldsm_x2(bq, wt + (j * 8 + (lane & 7)) * KCP);
+            mma_bf16(acc[j], af, bq);
+          }
         }
+      }
     }
+    __syncthreads();  // every warp is done with this stage before the next prefetch overwrites it
+  }
+  // epilogue: rows g and g+8 of the m16 fragment are output columns tx0+g and tx0+g+8 of tile row `warp`
+  const int g = lane >> 2, tq = lane & 3, oy = ty0 + warp;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int ox = tx0 + g + h * 8;
+    if (oy >= a.H || ox >= a.W) continue;
+    const long long p = ((long long)b * a.H + oy) * a.W + ox;
+#pragma unroll
+    for (int j = 0; j < BN / 8; ++j) {
+      const int co = n0 + j * 8 + tq * 2;  // cout is a multiple of 8: co + 1 < cout whenever co < cout
+      if (co >= a.cout) continue;
+      float v0 = acc[j][h * 2] + (a.bias ? a.bias[co] : 0.f);
+      float v1 = acc[j][h * 2 + 1] + (a.bias ? a.bias[co + 1] : 0.f);
+      if (a.relu) {
+        v0 = fmaxf(v0, 0.f);
+        v1 = fmaxf(v1, 0.f);
+      }
+      if (a.y) *reinterpret_cast<__nv_bfloat162*>(a.y + p * a.cout + co) = __floats2bfloat162_rn(v0, v1);
+      if (a.yf) *reinterpret_cast<float2*>(a.yf + p * a.cout + co) = make_float2(v0, v1);
+    }
+  }
 }
 
 // ------------------------------------------------------------------------------------------- conv weight gradient
@@ -577,10 +622,32 @@ void carve(Net& n, int B, int H, int W, Acts* A, bool grads, bool own_io, cudaSt
 
 void end_use(Net& n, cudaStream_t st) { ck(cudaEventRecord(n.ws_done, st), "record workspace use"); }
 
+template <int BN>
+void conv2_launch(const ConvArgs& a, cudaStream_t st) {
+  constexpr size_t smem = conv2_smem<BN>();
+  // opt-in to more than 48 KB of dynamic shared memory (per device; cheap, so on every launch)
+  ck(cudaFuncSetAttribute(k_conv2<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "conv smem");
+  const long long tiles = (long long)a.B * ((a.H + HT_H - 1) / HT_H) * ((a.W + HT_W - 1) / HT_W);
+  dim3 g((unsigned)tiles, (unsigned)((a.cout + BN - 1) / BN));
+  k_conv2<BN><<<g, 256, smem, st>>>(a);
+}
+
+// Output-channel tile matched to cout (cout > 128 in two tiles: 224 -> 112, 160 -> 80).
 void conv_launch(const ConvArgs& a, cudaStream_t st) {
-  const long long M = (long long)a.B * a.H * a.W;
-  dim3 g((unsigned)((M + CM - 1) / CM), (unsigned)((a.cout + CN - 1) / CN));
-  k_conv_fwd<<<g, 128, 0, st>>>(a);
+  switch (a.cout) {
+    case 8: return conv2_launch<8>(a, st);
+    case 16: return conv2_launch<16>(a, st);
+    case 32: return conv2_launch<32>(a, st);
+    case 48: return conv2_launch<48>(a, st);
+    case 64: return conv2_launch<64>(a, st);
+    case 96: return conv2_launch<96>(a, st);
+    case 128: return conv2_launch<128>(a, st);
+    case 160: return conv2_launch<80>(a, st);
+    case 224: return conv2_launch<112>(a, st);
+    default: break;
+  }
+  if (a.cout % 32 == 0) return conv2_launch<32>(a, st);
+  return conv2_launch<8>(a, st);
 }
 
 // Layer li on x (channel stride xs), bias + optional ReLU; bf16 and/or f32 output.

@@ -53,6 +53,11 @@ struct ConvArgs {
   float* yf;       // [B][H][W][cout] (f32 output) or null
   int B, H, W, cin, cin_stride, cin_off, cout;
   int relu;
+  // Virtual "upsample + concatenate" input (k_conv2 only; x2 == null: off): input channels [0, split) are x at half
+  // resolution [B][H/2][W/2][cin_stride] read at (y/2, x/2) (nearest 2× upsampling), channels [split, cin) are
+  // x2 [B][H][W][x2_stride] (the skip connection).  split is a multiple of 8.
+  const bf16* x2;
+  int split, x2_stride;
 };
 
 
@@ -111,7 +116,15 @@ __global__ void __launch_bounds__(256) k_conv2(ConvArgs a) {
       const int hy = px / HALO_W, hx = px - hy * HALO_W;
       const int gy = ty0 + hy - 1, gx = tx0 + hx - 1, ch = c0 + seg * 8;
       const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && ch < a.cin;
-      const bf16* src = ok ? a.x + (((long long)b * a.H + gy) * a.W + gx) * a.cin_stride + a.cin_off + ch : a.x;
+      const bf16* src = a.x;
+      if (ok) {
+        if (!a.x2)
+          src = a.x + (((long long)b * a.H + gy) * a.W + gx) * a.cin_stride + a.cin_off + ch;
+        else if (ch < a.split)
+          src = a.x + (((long long)b * (a.H >> 1) + (gy >> 1)) * (a.W >> 1) + (gx >> 1)) * a.cin_stride + ch;
+        else
+          src = a.x2 + (((long long)b * a.H + gy) * a.W + gx) * a.x2_stride + (ch - a.split);
+      }
       cp_async16(halo + ((size_t)stage * HALO_PX + px) * KCP + seg * 8, src, ok ? 16 : 0);
     }
     for (int i = tid; i < 9 * BN * 4; i += 256) {
@@ -314,17 +327,25 @@ __global__ void k_bias_grad(const bf16* dy, float* db, long long P, int C) {
 }
 
 // 2×2 average pooling (NHWC) and its gradient.
+// One thread per 8 channels of an output pixel (16-byte loads and store; C is a multiple of 8).
 __global__ void k_pool_fwd(const bf16* x, bf16* y, int B, int H, int W, int C) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int h = H / 2, w = W / 2;
-  if (i >= (long long)B * h * w * C) return;
-  const int c = i % C;
-  const long long p = i / C;
+  const int h = H / 2, w = W / 2, C8 = C / 8;
+  if (i >= (long long)B * h * w * C8) return;
+  const int c = (int)(i % C8) * 8;
+  const long long p = i / C8;
   const int xx = p % w, yy = (p / w) % h, b = (int)(p / ((long long)w * h));
   const long long base = (((long long)b * H + 2 * yy) * W + 2 * xx) * C + c;
-  const float s = __bfloat162float(x[base]) + __bfloat162float(x[base + C]) + __bfloat162float(x[base + (long long)W * C]) +
-                  __bfloat162float(x[base + (long long)W * C + C]);
-  y[i] = __float2bfloat16(0.25f * s);
+  const uint4 q[4] = {*(const uint4*)(x + base), *(const uint4*)(x + base + C), *(const uint4*)(x + base + (long long)W * C),
+                      *(const uint4*)(x + base + (long long)W * C + C)};
+  const bf16* e[4] = {(const bf16*)&q[0], (const bf16*)&q[1], (const bf16*)&q[2], (const bf16*)&q[3]};
+  uint4 o;
+  bf16* r = (bf16*)&o;
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    r[k] = __float2bfloat16(0.25f * (__bfloat162float(e[0][k]) + __bfloat162float(e[1][k]) + __bfloat162float(e[2][k]) +
+                                     __bfloat162float(e[3][k])));
+  *(uint4*)(y + p * C + c) = o;
 }
 // dX (full res, C channels) = dY/4 broadcast; `accumulate` adds to dX.
 __global__ void k_pool_bwd(const bf16* dy, bf16* dx, int B, int H, int W, int C, int accumulate) {
@@ -576,11 +597,11 @@ void carve(Net& n, int B, int H, int W, Acts* A, bool grads, bool own_io, cudaSt
   add(&a.p3, P3 * 96, 2);
   add(&a.a3, P3 * 128, 2);
   add(&a.b3, P3 * 128, 2);
-  add(&a.c2, P2 * 224, 2);
+  if (grads) add(&a.c2, P2 * 224, 2);
   add(&a.d2, P2 * 96, 2);
-  add(&a.c1, P1 * 160, 2);
+  if (grads) add(&a.c1, P1 * 160, 2);
   add(&a.d1, P1 * 64, 2);
-  add(&a.c0, P0 * 96, 2);
+  if (grads) add(&a.c0, P0 * 96, 2);
   add(&a.d0, P0 * 32, 2);
   if (grads) {
     add(&a.g_o, P0 * 8, 2);
@@ -653,7 +674,7 @@ void conv_launch(const ConvArgs& a, cudaStream_t st) {
 // Layer li on x (channel stride xs), bias + optional ReLU; bf16 and/or f32 output.
 void conv(Net& n, cudaStream_t st, int li, const bf16* x, int xs, bf16* y, float* yf, int B, int H, int W, int relu) {
   const Layer& l = n.L[li];
-  ConvArgs a;
+  ConvArgs a{};
   a.x = x;
   a.w = n.wb + l.off;
   a.bias = n.w + l.off + l.nw();
@@ -670,29 +691,58 @@ void conv(Net& n, cudaStream_t st, int li, const bf16* x, int xs, bf16* y, float
   conv_launch(a, st);
 }
 
+// Layer li reading the virtual concatenation [up2(lo) (clo channels), skip (cskip channels)].
+void conv_cat(Net& n, cudaStream_t st, int li, const bf16* lo, int clo, const bf16* skip, int cskip, bf16* y, int B,
+              int H, int W) {
+  const Layer& l = n.L[li];
+  ConvArgs a{};
+  memset(&a, 0, sizeof a);
+  a.x = lo;
+  a.w = n.wb + l.off;
+  a.bias = n.w + l.off + l.nw();
+  a.y = y;
+  a.B = B;
+  a.H = H;
+  a.W = W;
+  a.cin = l.cin;
+  a.cin_stride = clo;
+  a.cout = l.cout;
+  a.relu = 1;
+  a.x2 = skip;
+  a.split = clo;
+  a.x2_stride = cskip;
+  conv_launch(a, st);
+}
+
 void forward(Net& n, const Acts& a, int B, int H, int W, cudaStream_t st) {
   const long long P0 = (long long)B * H * W, P1 = P0 / 4, P2 = P0 / 16, P3 = P0 / 64;
   const int H1 = H / 2, W1 = W / 2, H2 = H / 4, W2 = W / 4, H3 = H / 8, W3 = W / 8;
   conv(n, st, E0A, a.x, 48, a.a0, nullptr, B, H, W, 1);
   conv(n, st, E0B, a.a0, 32, a.s0, nullptr, B, H, W, 1);
-  k_pool_fwd<<<blocks(P1 * 32), 256, 0, st>>>(a.s0, a.p1, B, H, W, 32);
+  k_pool_fwd<<<blocks(P1 * 4), 256, 0, st>>>(a.s0, a.p1, B, H, W, 32);
   conv(n, st, E1A, a.p1, 32, a.a1, nullptr, B, H1, W1, 1);
   conv(n, st, E1B, a.a1, 64, a.s1, nullptr, B, H1, W1, 1);
-  k_pool_fwd<<<blocks(P2 * 64), 256, 0, st>>>(a.s1, a.p2, B, H1, W1, 64);
+  k_pool_fwd<<<blocks(P2 * 8), 256, 0, st>>>(a.s1, a.p2, B, H1, W1, 64);
   conv(n, st, E2A, a.p2, 64, a.a2, nullptr, B, H2, W2, 1);
   conv(n, st, E2B, a.a2, 96, a.s2, nullptr, B, H2, W2, 1);
-  k_pool_fwd<<<blocks(P3 * 96), 256, 0, st>>>(a.s2, a.p3, B, H2, W2, 96);
+  k_pool_fwd<<<blocks(P3 * 12), 256, 0, st>>>(a.s2, a.p3, B, H2, W2, 96);
   conv(n, st, E3A, a.p3, 96, a.a3, nullptr, B, H3, W3, 1);
   conv(n, st, E3B, a.a3, 128, a.b3, nullptr, B, H3, W3, 1);
-  k_up_fwd<<<blocks(P2 * 128), 256, 0, st>>>(a.b3, a.c2, B, H2, W2, 128, 224);
-  k_copy_ch<<<blocks(P2 * 96), 256, 0, st>>>(a.s2, 96, 0, a.c2, 224, 128, 96, P2, 0);
-  conv(n, st, D2, a.c2, 224, a.d2, nullptr, B, H2, W2, 1);
-  k_up_fwd<<<blocks(P1 * 96), 256, 0, st>>>(a.d2, a.c1, B, H1, W1, 96, 160);
-  k_copy_ch<<<blocks(P1 * 64), 256, 0, st>>>(a.s1, 64, 0, a.c1, 160, 96, 64, P1, 0);
-  conv(n, st, D1, a.c1, 160, a.d1, nullptr, B, H1, W1, 1);
-  k_up_fwd<<<blocks(P0 * 64), 256, 0, st>>>(a.d1, a.c0, B, H, W, 64, 96);
-  k_copy_ch<<<blocks(P0 * 32), 256, 0, st>>>(a.s0, 32, 0, a.c0, 96, 64, 32, P0, 0);
-  conv(n, st, D0, a.c0, 96, a.d0, nullptr, B, H, W, 1);
+  if (a.c2) {  // training: the concatenations are materialised (the backward pass reads them)
+    k_up_fwd<<<blocks(P2 * 128), 256, 0, st>>>(a.b3, a.c2, B, H2, W2, 128, 224);
+    k_copy_ch<<<blocks(P2 * 96), 256, 0, st>>>(a.s2, 96, 0, a.c2, 224, 128, 96, P2, 0);
+    conv(n, st, D2, a.c2, 224, a.d2, nullptr, B, H2, W2, 1);
+    k_up_fwd<<<blocks(P1 * 96), 256, 0, st>>>(a.d2, a.c1, B, H1, W1, 96, 160);
+    k_copy_ch<<<blocks(P1 * 64), 256, 0, st>>>(a.s1, 64, 0, a.c1, 160, 96, 64, P1, 0);
+    conv(n, st, D1, a.c1, 160, a.d1, nullptr, B, H1, W1, 1);
+    k_up_fwd<<<blocks(P0 * 64), 256, 0, st>>>(a.d1, a.c0, B, H, W, 64, 96);
+    k_copy_ch<<<blocks(P0 * 32), 256, 0, st>>>(a.s0, 32, 0, a.c0, 96, 64, 32, P0, 0);
+    conv(n, st, D0, a.c0, 96, a.d0, nullptr, B, H, W, 1);
+  } else {  // inference: upsampling and concatenation happen in the convolution's input loader
+    conv_cat(n, st, D2, a.b3, 128, a.s2, 96, a.d2, B, H2, W2);
+    conv_cat(n, st, D1, a.d2, 96, a.s1, 64, a.d1, B, H1, W1);
+    conv_cat(n, st, D0, a.d1, 64, a.s0, 32, a.d0, B, H, W);
+  }
   conv(n, st, HEAD, a.d0, 32, nullptr, a.o, B, H, W, 0);
   ck(cudaGetLastError(), "network forward");
 }
@@ -720,7 +770,7 @@ void conv_bwd(Net& n, cudaStream_t st, int li, const bf16* dy, const bf16* x, in
   k_bias_grad<<<256, 256 / l.cout * l.cout, 0, st>>>(dy, n.g + l.off + l.nw(), P, l.cout);
   if (dx) {
     k_flip_weights<<<blocks((long long)l.nw()), 256, 0, st>>>(n.wb + l.off, n.wt, l.cout, l.cin);
-    ConvArgs a;
+    ConvArgs a{};
     a.x = dy;
     a.w = n.wt;
     a.bias = nullptr;
@@ -1048,7 +1098,7 @@ int ps_net_conv_check(int device, const uint16_t* x, const float* w, const uint1
     ck(cudaMemcpy(b.dy, dy, P * cout * 2, cudaMemcpyHostToDevice), "upload");
     ck(cudaMemcpy(b.wb, hw.data(), nw * 2, cudaMemcpyHostToDevice), "upload");
     ck(cudaMemset(b.dw, 0, nw * 4), "cudaMemset");
-    ConvArgs a;
+    ConvArgs a{};
     a.x = b.x;
     a.w = b.wb;
     a.bias = nullptr;

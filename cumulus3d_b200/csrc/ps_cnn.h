@@ -14,6 +14,7 @@ int forward_on_stream(ps_net* net, const void* in, int B, int H, int W, float* o
 // Adds the number of proposed pixels to *count when count is not null.
 cudaError_t launch_decode(const float* o, int Wp, int H, int W, float4* planes, float* conf, float inv_near,
                           float inv_far, float thr, const float* k, unsigned long long* count, cudaStream_t st);
-// Kernel launches of one forward pass.
-constexpr int kForwardLaunches = 21;
+// Kernel launches of one inference forward pass (12 convolutions, 3 poolings; upsampling and concatenation are
+// fused into the convolutions' input loads).
+constexpr int kForwardLaunches = 15;
 }  // namespace ps_cnn

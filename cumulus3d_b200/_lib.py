@@ -105,6 +105,13 @@ class FusionView(C.Structure):
                 ("image_id", C.c_uint32), ("num_overlap", C.c_uint32), ("overlap", C.POINTER(C.c_uint32))]
 
 
+class MultiscaleSchedule(C.Structure):
+    _fields_ = [("photometric_iters", C.c_uint32), ("photometric_iters_upper", C.c_uint32),
+                ("geometric_rounds", C.c_uint32), ("geometric_iters", C.c_uint32), ("jbu_sigma_spatial", C.c_float),
+                ("jbu_sigma_color", C.c_float), ("restorer_threshold", C.c_float), ("weak_texture_prior", C.c_uint32),
+                ("run_id_base", C.c_uint32), ("use_graph", C.c_uint32)]
+
+
 class DepthSnapshot(C.Structure):
     _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
                 ("maps", C.POINTER(C.POINTER(C.c_float)))]
@@ -142,6 +149,8 @@ SIGNATURES = {
     "ps_filter_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_uint8))]),
     "ps_readout_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_schedule_resident": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(Schedule)]),
+    "ps_multiscale_schedule_default": (None, [C.POINTER(MultiscaleSchedule)]),
+    "ps_schedule_multiscale": (C.c_int, [_P, _U32P, C.c_size_t, C.POINTER(MultiscaleSchedule)]),
     "ps_median_filter_inplace_noalloc": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32,
                                                     C.POINTER(C.c_float), C.c_void_p]),
     "ps_synchronize": (C.c_int, [_P]),

@@ -1271,6 +1271,25 @@ cudaError_t launch_sweep(const PsRun& P, bool tex, cudaStream_t st) {
              : launch(k_sweep<0, 1, false>, Q.ntiles, PS_EVAL_NT, smem, st, Q);
 }
 
+// Per-pixel restorer choice of the multi-scale driver (the host driver's `take` rule): the restorer run's plane stays
+// where the upsampled plane is invalid (d <= 0) or its evaluated cost exceeds the restorer's by more than `thr`;
+// everywhere else the upsampled plane is restored.
+__global__ void __launch_bounds__(256) k_restore(const __grid_constant__ PsRun P, const float4* up, const float* cinit,
+                                                 float thr) {
+  SimpleCtx c;
+  if (!simple_px(P, c)) return;
+  const long long g = c.it->off + (long long)c.y * c.it->w + c.x;
+  const float4 u = up[g];
+  const bool take = u.w <= 0.0f || (cinit[g] - P.cost[g]) > thr;
+  if (!take) P.plane[g] = u;
+}
+
+cudaError_t launch_restore(const PsRun& P, const float4* up, const float* cinit, float thr, cudaStream_t st) {
+  if (P.ntiles <= 0) return cudaSuccess;
+  k_restore<<<P.ntiles, dim3(PS_SIMPLE_BX, PS_SIMPLE_BY), 0, st>>>(P, up, cinit, thr);
+  return cudaGetLastError();
+}
+
 // Module constants (propagation offsets); called at session begin, outside any stream capture.
 cudaError_t prepare() { return init_constants(); }
 

@@ -37,6 +37,7 @@
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
   cudaError_t launch_readout(const PsRun& P, float4* out, cudaStream_t st);                                \
   cudaError_t launch_sweep(const PsRun& P, bool tex, cudaStream_t st);                                     \
+  cudaError_t launch_restore(const PsRun& P, const float4* up, const float* cinit, float thr, cudaStream_t st); \
   cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
   cudaError_t prepare();                                                                                   \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
@@ -57,13 +58,16 @@ struct Launchers {
   cudaError_t (*readout)(const PsRun&, float4*, cudaStream_t);
   int (*half_lanes)(unsigned);
   cudaError_t (*sweep)(const PsRun&, bool, cudaStream_t);
+  cudaError_t (*restore)(const PsRun&, const float4*, const float*, float, cudaStream_t);
 };
 const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
                            ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
-                           ps_parity::launch_readout,  ps_parity::half_lanes,    ps_parity::launch_sweep};
+                           ps_parity::launch_readout,  ps_parity::half_lanes,    ps_parity::launch_sweep,
+                           ps_parity::launch_restore};
 const Launchers kFast = {ps_fast::launch_half,     ps_fast::launch_eval,   ps_fast::launch_filter,
                          ps_fast::launch_upsample, ps_fast::launch_median, ps_fast::launch_snapshot,
-                         ps_fast::launch_readout,  ps_fast::half_lanes,    ps_fast::launch_sweep};
+                         ps_fast::launch_readout,  ps_fast::half_lanes,    ps_fast::launch_sweep,
+                         ps_fast::launch_restore};
 
 struct PsError {
   int code;
@@ -89,6 +93,7 @@ struct Slot {
   std::vector<char> proposal_valid;
   int* spk = nullptr;          // speckle removal: parent, size, lo, hi, cnt per pixel (5 ints each, lazily)
   unsigned char* marks = nullptr;  // fusion "used" marks
+  float* cinit = nullptr;          // multi-scale driver: cost of the upsampled planes
 };
 
 // Fused point cloud of the last ps_fuse_resident call (device).
@@ -191,6 +196,7 @@ struct ps_session {
     long long* offsets = nullptr;    // snapshot offset table of the schedule's view set (device)
     uint64_t per_replay = 0;         // kernels per replay
     std::vector<Pending> events;     // per-launch event nodes captured with profiling on
+    std::vector<long long*> level_offsets;  // multi-scale schedules: snapshot offset table per level (device)
   };
   std::map<std::string, GraphEntry> graphs;
 
@@ -411,6 +417,32 @@ void collect_events(ps_session* s) {
 
 void sync(ps_session* s) { cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize"); }
 
+// Destroys every captured schedule graph: they hold device addresses of a buffer about to be replaced.
+void drop_graphs(ps_session* s) {
+  if (s->graphs.empty()) return;
+  collect_events(s);  // finishes the stream and releases the replays' pending events
+  for (auto& kv : s->graphs) {
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    cudaFree(kv.second.offsets);
+    for (long long* o : kv.second.level_offsets) cudaFree(o);
+    for (auto& pd : kv.second.events) {
+      cudaEventDestroy(pd.a);
+      cudaEventDestroy(pd.b);
+    }
+  }
+  s->graphs.clear();
+}
+
+// Grows the snapshot buffer to `total` floats (captured graphs are dropped first).
+void realloc_snapshot(ps_session* s, size_t total) {
+  drop_graphs(s);
+  if (s->snap) cudaFree(s->snap);
+  s->snap = nullptr;
+  s->snap_cap = 0;
+  s->snap = dalloc<float>(std::max<size_t>(total, 1));
+  s->snap_cap = total;
+}
+
 // ---- state packing (host) -------------------------------------------------------------------------------------
 void check_state(ps_session* s, int v, int level, const ps_view_state& st) {
   if ((int)st.width != s->W(v, level) || (int)st.height != s->H(v, level))
@@ -528,11 +560,7 @@ void ensure_snapshot(ps_session* s, const ps_depth_snapshot* snap) {
     }
   }
   if (total > s->snap_cap) {
-    if (s->snap) cudaFree(s->snap);
-    s->snap = nullptr;
-    s->snap_cap = 0;
-    s->snap = dalloc<float>(total);
-    s->snap_cap = total;
+    realloc_snapshot(s, total);
   }
   for (int v = 0; v < s->nv; ++v)
     if (offs[v] >= 0)
@@ -841,6 +869,7 @@ int ps_end(ps_session* s) {
     cudaFree(sl.pconf);
     cudaFree(sl.spk);
     cudaFree(sl.marks);
+    cudaFree(sl.cinit);
   }
   s->fused.release();
   cudaFree(s->fused.counter);
@@ -868,6 +897,7 @@ int ps_end(ps_session* s) {
   for (auto& kv : s->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
     cudaFree(kv.second.offsets);
+    for (long long* o : kv.second.level_offsets) cudaFree(o);
     for (auto& pd : kv.second.events) {
       cudaEventDestroy(pd.a);
       cudaEventDestroy(pd.b);
@@ -1058,11 +1088,7 @@ int ps_snapshot_capture(ps_session* s, uint32_t level, const uint32_t* views, si
     Slot& sl = slot(s, (int)level);
     if ((size_t)sl.total > s->snap_cap) {
       if (keep_others) fail(PS_EINVAL, "keep_others needs a snapshot buffer of this level");
-      if (s->snap) cudaFree(s->snap);
-      s->snap = nullptr;
-      s->snap_cap = 0;
-      s->snap = dalloc<float>(sl.total);
-      s->snap_cap = sl.total;
+      realloc_snapshot(s, sl.total);
     }
     std::vector<long long> offs(s->nv, -1);
     if (keep_others && s->snap_valid && s->snap_level == (int)level) {
@@ -1092,11 +1118,7 @@ int ps_snapshot_buffer(ps_session* s, uint32_t level, float** device_ptr, uint64
     if ((size_t)sl.total > s->snap_cap || s->snap_level != (int)level) {
       // (re)lay the buffer out like the level's slots; nothing is present yet
       if ((size_t)sl.total > s->snap_cap) {
-        if (s->snap) cudaFree(s->snap);
-        s->snap = nullptr;
-        s->snap_cap = 0;
-        s->snap = dalloc<float>(sl.total);
-        s->snap_cap = sl.total;
+        realloc_snapshot(s, sl.total);
       }
       std::vector<long long> none(s->nv, -1);
       cuda_ok(cudaMemcpyAsync(s->snap_off, none.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
@@ -1209,6 +1231,183 @@ void enqueue_schedule(ps_session* s, const uint32_t* views, size_t n, const ps_s
 
 }  // namespace
 
+extern "C++" {
+namespace {
+
+// The launches of the multi-scale driver (densify.compute_depth_maps with the restorer's default: no random init):
+// coarsest level from random init; every finer level upsampled (joint bilateral), evaluated, refined by a restorer
+// run from the upsampled planes, evaluated again and merged per pixel (k_restore); geometric rounds at every level
+// against snapshots captured on the device; at the top level the median filter (when the filter parameters ask for
+// it), the final snapshot, the filter and the readout.  Run ids count up from run_id_base like the host driver's.
+void enqueue_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps_multiscale_schedule* m,
+                        const std::vector<long long*>& offs) {
+  uint32_t run_id = m->run_id_base;
+  const int top = s->nl - 1;
+  for (int l = 0; l < s->nl; ++l) {
+    Slot& sl = slot(s, l);
+    const uint32_t iters = l == 0 ? m->photometric_iters : m->photometric_iters_upper;
+    const bool use_prior = l > 0 && m->weak_texture_prior && s->pm.weak_texture_var > 0.0f;
+    if (l == 0) {
+      ps_run_params p{0, 0, PS_INIT_RANDOM, iters, run_id++, 0};
+      for (auto [a, b] : batches(s, views, n, 0)) run_batch(s, views, a, b, &p, false);
+    } else {
+      for (auto [a, b] : batches(s, views, n, l)) {
+        PsRun U = base_params(s, l);
+        U.prior = s->slots[l - 1].plane;
+        U.up_inv2s = 1.0f / (2.0f * m->jbu_sigma_spatial * m->jbu_sigma_spatial);
+        U.up_inv2c = 1.0f / (2.0f * m->jbu_sigma_color * m->jbu_sigma_color);
+        set_items(s, U, views, a, b, l, PS_SIMPLE_BX, PS_SIMPLE_BY, l - 1);
+        launched(s, s->L->upsample(U, s->st), "upsample kernel");
+        PsRun E = base_params(s, l);  // c_init: top-K photometric cost of the upsampled planes
+        set_items(s, E, views, a, b, l, PS_EVAL_PW, PS_EVAL_PH);
+        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+      }
+      for (size_t i = 0; i < n; ++i) {  // keep the upsampled planes and their cost
+        const size_t np = (size_t)s->W(views[i], l) * s->H(views[i], l), o = (size_t)sl.off[views[i]];
+        cuda_ok(cudaMemcpyAsync(sl.aux + o, sl.plane + o, np * sizeof(float4), cudaMemcpyDeviceToDevice, s->st), "copy");
+        cuda_ok(cudaMemcpyAsync(sl.cinit + o, sl.cost + o, np * sizeof(float), cudaMemcpyDeviceToDevice, s->st), "copy");
+        if (use_prior)
+          cuda_ok(cudaMemcpyAsync(sl.prior + o, sl.plane + o, np * sizeof(float4), cudaMemcpyDeviceToDevice, s->st),
+                  "copy");
+      }
+      ps_run_params p{(uint32_t)l, 0, 0, iters, run_id++, use_prior ? 1u : 0u};
+      for (auto [a, b] : batches(s, views, n, l)) run_batch(s, views, a, b, &p, use_prior);
+      for (auto [a, b] : batches(s, views, n, l)) {
+        PsRun E = base_params(s, l);  // c_photo
+        set_items(s, E, views, a, b, l, PS_EVAL_PW, PS_EVAL_PH);
+        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+        PsRun R = base_params(s, l);
+        set_items(s, R, views, a, b, l, PS_SIMPLE_BX, PS_SIMPLE_BY);
+        launched(s, s->L->restore(R, sl.aux, sl.cinit, m->restorer_threshold, s->st), "restore kernel");
+      }
+    }
+    for (uint32_t r = 0; r < m->geometric_rounds; ++r) {
+      enqueue_snapshot(s, views, n, l, offs[l]);
+      ps_run_params g{(uint32_t)l, 1, 0, m->geometric_iters, run_id++, use_prior ? 1u : 0u};
+      for (auto [a, b] : batches(s, views, n, l)) run_batch(s, views, a, b, &g, use_prior);
+    }
+  }
+  Slot& st = slot(s, top);
+  if (s->fl.median_filter) {
+    for (size_t i = 0; i < n; ++i) {
+      const size_t np = (size_t)s->W(views[i], top) * s->H(views[i], top), o = (size_t)st.off[views[i]];
+      cuda_ok(cudaMemcpyAsync(st.aux + o, st.plane + o, np * sizeof(float4), cudaMemcpyDeviceToDevice, s->st), "copy");
+    }
+    for (auto [a, b] : batches(s, views, n, top)) {
+      PsRun M = base_params(s, top);
+      M.prior = st.aux;
+      set_items(s, M, views, a, b, top, PS_SIMPLE_BX, PS_SIMPLE_BY, top);
+      launched(s, s->L->median(M, s->st), "median kernel");
+    }
+  }
+  enqueue_snapshot(s, views, n, top, offs[top]);
+  for (auto [a, b] : batches(s, views, n, top)) {
+    PsRun P = base_params(s, top);
+    P.geometric = 1;
+    set_items(s, P, views, a, b, top, PS_EVAL_PW, PS_EVAL_PH);
+    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+    PsRun Q = base_params(s, top);
+    set_items(s, Q, views, a, b, top, PS_SIMPLE_BX, PS_SIMPLE_BY);
+    launched(s, s->L->readout(Q, st.aux, s->st), "readout kernel");
+  }
+}
+
+// Runs `enqueue` through a CUDA graph captured once per key (use_graph) or directly; `prepare` allocates and uploads
+// what the launches need, outside any capture.
+template <typename Prep, typename Enq>
+void graph_run(ps_session* s, const std::string& key, bool use_graph, Prep&& prepare, Enq&& enqueue) {
+  auto it = s->graphs.find(key);
+  if (it == s->graphs.end()) {
+    ps_session::GraphEntry ge;
+    auto release = [&] {
+      cudaFree(ge.offsets);
+      for (long long* o : ge.level_offsets) cudaFree(o);
+    };
+    try {
+      prepare(ge);
+      sync(s);
+    } catch (...) {
+      release();
+      throw;
+    }
+    if (use_graph) {
+      // capture once: the launches the direct path issues, recorded into a graph; with profiling on, the per-launch
+      // events become event-record nodes that every replay re-records
+      collect_events(s);
+      const uint64_t before = s->launches;
+      uint64_t kl[PS_KERNEL_KINDS];
+      for (int k = 0; k < PS_KERNEL_KINDS; ++k) kl[k] = s->kind_launches[k];
+      cudaGraph_t g = nullptr;
+      cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+      s->capturing = true;
+      try {
+        enqueue(ge);
+        s->capturing = false;
+      } catch (...) {
+        s->capturing = false;
+        cudaStreamEndCapture(s->st, &g);
+        if (g) cudaGraphDestroy(g);
+        s->launches = before;
+        for (auto& pd : s->pending) {
+          cudaEventDestroy(pd.a);
+          cudaEventDestroy(pd.b);
+        }
+        s->pending.clear();
+        release();
+        throw;
+      }
+      ge.per_replay = s->launches - before;
+      s->launches = before;
+      for (int k = 0; k < PS_KERNEL_KINDS; ++k) s->kind_launches[k] = kl[k];
+      ge.events = s->pending;
+      for (auto& pd : ge.events) pd.persistent = true;
+      s->pending.clear();
+      cudaError_t e = cudaStreamEndCapture(s->st, &g);
+      if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, g, 0);
+      if (g) cudaGraphDestroy(g);
+      if (e != cudaSuccess) {
+        release();
+        for (auto& pd : ge.events) {
+          cudaEventDestroy(pd.a);
+          cudaEventDestroy(pd.b);
+        }
+      }
+      cuda_ok(e, "graph capture");
+    }
+    it = s->graphs.emplace(key, ge).first;
+  }
+  ps_session::GraphEntry& ge = it->second;
+  if (ge.exec) {
+    if (!ge.events.empty()) collect_events(s);  // the previous replay's event nodes are re-recorded by this one
+    cuda_ok(cudaGraphLaunch(ge.exec, s->st), "cudaGraphLaunch");
+    s->launches += ge.per_replay;
+    for (auto& pd : ge.events) {
+      s->pending.push_back(pd);
+      s->kind_launches[pd.kind]++;
+    }
+  } else {
+    enqueue(ge);
+  }
+}
+
+void ensure_snapshot_capacity(ps_session* s, long long total) {
+  if ((size_t)total > s->snap_cap) {
+    realloc_snapshot(s, total);  // drops captured graphs: they hold the old buffer's address
+  }
+}
+
+long long* view_offsets(ps_session* s, int level, const uint32_t* views, size_t n) {
+  Slot& sl = slot(s, level);
+  std::vector<long long> offs(s->nv, -1);
+  for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
+  long long* d = dalloc<long long>(s->nv);
+  cuda_ok(cudaMemcpyAsync(d, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st), "upload offsets");
+  return d;
+}
+
+}  // namespace
+}  // extern "C++"
+
 int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch) {
   return guard(s, [&] {
     if (!sch) fail(PS_EINVAL, "schedule is NULL");
@@ -1216,91 +1415,69 @@ int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const p
     check_views(s, views, n);
     const int level = (int)sch->level;
     Slot& sl = slot(s, level);
-    // the snapshot buffer in the slot layout, allocated outside any capture
-    if ((size_t)sl.total > s->snap_cap) {
-      if (s->snap) cudaFree(s->snap);
-      s->snap = nullptr;
-      s->snap_cap = 0;
-      s->snap = dalloc<float>(sl.total);
-      s->snap_cap = sl.total;
-    }
-    std::string key = std::to_string(level) + ":" + std::to_string(sch->photometric_iters) + ":" +
+    ensure_snapshot_capacity(s, sl.total);  // the snapshot buffer in the slot layout, allocated outside any capture
+    std::string key = "single:" + std::to_string(level) + ":" + std::to_string(sch->photometric_iters) + ":" +
                       std::to_string(sch->geometric_rounds) + ":" + std::to_string(sch->geometric_iters) + ":" +
                       std::to_string(sch->run_id_base) + ":" + std::to_string(sch->use_graph) + ":" +
                       std::to_string(s->profiling) + ":" + std::to_string(sch->init == PS_INIT_PROPOSAL) + ":";
     for (size_t i = 0; i < n; ++i) key += std::to_string(views[i]) + ",";
-    auto it = s->graphs.find(key);
-    if (it == s->graphs.end()) {
-      ps_session::GraphEntry ge;
-      std::vector<long long> offs(s->nv, -1);
-      for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
-      ge.offsets = dalloc<long long>(s->nv);
-      cuda_ok(cudaMemcpyAsync(ge.offsets, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st),
-              "upload offsets");
-      sync(s);
-      if (sch->use_graph) {
-        // capture once: the launches the direct path issues, recorded into a graph; with profiling on, the per-launch
-        // events become event-record nodes that every replay re-records
-        collect_events(s);
-        const uint64_t before = s->launches;
-        uint64_t kl[PS_KERNEL_KINDS];
-        for (int k = 0; k < PS_KERNEL_KINDS; ++k) kl[k] = s->kind_launches[k];
-        cudaGraph_t g = nullptr;
-        cuda_ok(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
-        s->capturing = true;
-        try {
-          enqueue_schedule(s, views, n, sch, ge.offsets);
-          s->capturing = false;
-        } catch (...) {
-          s->capturing = false;
-          cudaStreamEndCapture(s->st, &g);
-          if (g) cudaGraphDestroy(g);
-          s->launches = before;
-          for (auto& pd : s->pending) {
-            cudaEventDestroy(pd.a);
-            cudaEventDestroy(pd.b);
-          }
-          s->pending.clear();
-          cudaFree(ge.offsets);
-          throw;
-        }
-        ge.per_replay = s->launches - before;
-        s->launches = before;
-        for (int k = 0; k < PS_KERNEL_KINDS; ++k) s->kind_launches[k] = kl[k];
-        ge.events = s->pending;
-        for (auto& pd : ge.events) pd.persistent = true;
-        s->pending.clear();
-        cudaError_t e = cudaStreamEndCapture(s->st, &g);
-        if (e == cudaSuccess) e = cudaGraphInstantiate(&ge.exec, g, 0);
-        if (g) cudaGraphDestroy(g);
-        if (e != cudaSuccess) {
-          cudaFree(ge.offsets);
-          for (auto& pd : ge.events) {
-            cudaEventDestroy(pd.a);
-            cudaEventDestroy(pd.b);
-          }
-        }
-        cuda_ok(e, "graph capture");
-      }
-      it = s->graphs.emplace(key, ge).first;
-    }
-    ps_session::GraphEntry& ge = it->second;
-    if (ge.exec) {
-      if (!ge.events.empty()) collect_events(s);  // the previous replay's event nodes are re-recorded by this one
-      cuda_ok(cudaGraphLaunch(ge.exec, s->st), "cudaGraphLaunch");
-      s->launches += ge.per_replay;
-      for (auto& pd : ge.events) {
-        s->pending.push_back(pd);
-        s->kind_launches[pd.kind]++;
-      }
-    } else {
-      enqueue_schedule(s, views, n, sch, ge.offsets);
-    }
+    graph_run(
+        s, key, sch->use_graph != 0,
+        [&](ps_session::GraphEntry& ge) { ge.offsets = view_offsets(s, level, views, n); },
+        [&](ps_session::GraphEntry& ge) { enqueue_schedule(s, views, n, sch, ge.offsets); });
     s->snap_valid = true;
     s->snap_level = level;
     s->snap_id = 0x5c4ed000ull + sch->run_id_base;
   });
 }
+
+void ps_multiscale_schedule_default(ps_multiscale_schedule* out) {
+  if (!out) return;
+  memset(out, 0, sizeof *out);
+  out->photometric_iters = 6;
+  out->photometric_iters_upper = 3;
+  out->geometric_rounds = 2;
+  out->geometric_iters = 2;
+  out->jbu_sigma_spatial = 1.0f;
+  out->jbu_sigma_color = 0.04f;
+  out->restorer_threshold = 0.1f;
+  out->weak_texture_prior = 0;
+  out->run_id_base = 1;
+  out->use_graph = 1;
+}
+
+int ps_schedule_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps_multiscale_schedule* m) {
+  return guard(s, [&] {
+    if (!m) fail(PS_EINVAL, "schedule is NULL");
+    if (!(m->jbu_sigma_spatial > 0.f) || !(m->jbu_sigma_color > 0.f)) fail(PS_EINVAL, "JBU sigmas must be > 0");
+    check_views(s, views, n);
+    const int top = s->nl - 1;
+    for (int l = 0; l < s->nl; ++l) {  // every buffer the launches use exists before any capture
+      Slot& sl = slot(s, l);
+      if (l > 0 && !sl.cinit) sl.cinit = dalloc<float>(std::max<long long>(sl.total, 1));
+    }
+    long long maxtot = 0;
+    for (int l = 0; l < s->nl; ++l) maxtot = std::max(maxtot, s->slots[l].total);
+    ensure_snapshot_capacity(s, maxtot);
+    char buf[256];
+    snprintf(buf, sizeof buf, "multi:%u:%u:%u:%u:%a:%a:%a:%u:%u:%u:%d:", m->photometric_iters,
+             m->photometric_iters_upper, m->geometric_rounds, m->geometric_iters, m->jbu_sigma_spatial,
+             m->jbu_sigma_color, m->restorer_threshold, m->weak_texture_prior, m->run_id_base, m->use_graph,
+             (int)s->profiling);
+    std::string key = buf;
+    for (size_t i = 0; i < n; ++i) key += std::to_string(views[i]) + ",";
+    graph_run(
+        s, key, m->use_graph != 0,
+        [&](ps_session::GraphEntry& ge) {
+          for (int l = 0; l < s->nl; ++l) ge.level_offsets.push_back(view_offsets(s, l, views, n));
+        },
+        [&](ps_session::GraphEntry& ge) { enqueue_multiscale(s, views, n, m, ge.level_offsets); });
+    s->snap_valid = true;
+    s->snap_level = top;
+    s->snap_id = 0x3c4ed000ull + m->run_id_base;
+  });
+}
+
 
 // ---- learned proposal ------------------------------------------------------------------------------------------
 extern "C++" {

@@ -156,6 +156,19 @@ def compute_depth_maps(session: PatchMatchSession, inp: KernelInput, views: Sequ
     return states, readout(states, counts, nsrc, inp.filter.min_num_consistent), counts
 
 
+def compute_depth_maps_resident(session: PatchMatchSession, inp: KernelInput, views: Sequence[int],
+                                sch: Schedule = Schedule(), weak_texture_prior: bool = False,
+                                graph: bool = True) -> List[ViewState]:
+    """compute_depth_maps on the device (ps_schedule_multiscale): the same schedule, no host round trips, one graph
+    launch.  Returns the filtered states (readout) of the top level."""
+    if sch.restorer_random_init:
+        raise ValueError("the device driver implements the restorer without random init (the fast profile)")
+    session.schedule_multiscale(views, sch.photometric_iters, sch.photometric_iters_upper, sch.geometric_rounds,
+                                sch.geometric_iters, sch.jbu_sigma_spatial, sch.jbu_sigma_color,
+                                sch.restorer_threshold, weak_texture_prior, 1, graph)
+    return session.readout_download(inp.num_levels - 1, views)
+
+
 def schedule_host(session: PatchMatchSession, inp: KernelInput, views: Sequence[int], photometric_iters: int,
                   geometric_rounds: int, geometric_iters: int):
     """Single-level schedule through the host-state API (every call copies states in and out, as the reference's

@@ -420,6 +420,17 @@ class PatchMatchSession:
                                              key.ctypes.data, nv.ctypes.data, vis.ctypes.data, stride))
         return FusedCloud(pos, nrm, col, key, nv, vis)
 
+    def schedule_multiscale(self, views: Sequence[int], photometric_iters: int = 6, photometric_iters_upper: int = 3,
+                            geometric_rounds: int = 2, geometric_iters: int = 2, jbu_sigma_spatial: float = 1.0,
+                            jbu_sigma_color: float = 0.04, restorer_threshold: float = 0.1,
+                            weak_texture_prior: bool = False, run_id_base: int = 1, graph: bool = True) -> None:
+        """The multi-scale driver over every level on the device (asynchronous); results in the top level's readout
+        planes (readout_download(top, views))."""
+        m = _lib.MultiscaleSchedule(photometric_iters, photometric_iters_upper, geometric_rounds, geometric_iters,
+                                    jbu_sigma_spatial, jbu_sigma_color, restorer_threshold, int(weak_texture_prior),
+                                    run_id_base, int(graph))
+        self._check(self.lib.ps_schedule_multiscale(self.h, _views(views), len(views), C.byref(m)))
+
     # ---- learned proposal (no reference counterpart) ----------------------------------------------------------
     def sweep_volume(self, level: int, view: int, out_ptr: int, row_pixels: int) -> None:
         """Writes the view's network input (bf16 NHWC, 48 channels) to device memory at `out_ptr` (asynchronous on

@@ -269,6 +269,28 @@ typedef struct ps_schedule {
   uint32_t init; /* initialisation of the photometric run: PS_INIT_RANDOM or PS_INIT_PROPOSAL */
 } ps_schedule;
 int ps_schedule_resident(ps_session* s, const uint32_t* views, size_t n, const ps_schedule* sch);
+/* The multi-scale driver of compute_depth_maps (crates/dense/src/densify.rs:350-454, restorer without random init)
+ * on resident states over every level of the session, captured into one CUDA graph per (views, schedule, profiling
+ * flag) when use_graph: coarsest level from random init; each finer level upsampled (JBU), evaluated, refined by a
+ * restorer run from the upsampled planes, evaluated again and merged per pixel (the restorer's plane where the
+ * upsampled one is invalid or its cost exceeds the restorer's by more than restorer_threshold); geometric rounds at
+ * every level against device-captured snapshots; at the top level the median filter (when the filter parameters enable
+ * it), the filter and the readout threshold (results in the top level's readout planes).  Asynchronous.  No reference
+ * counterpart (the reference drives these steps from the host). */
+typedef struct ps_multiscale_schedule {
+  uint32_t photometric_iters;       /* coarsest level (6) */
+  uint32_t photometric_iters_upper; /* finer levels (3) */
+  uint32_t geometric_rounds;        /* per level (2) */
+  uint32_t geometric_iters;         /* (2) */
+  float jbu_sigma_spatial;          /* 1.0 */
+  float jbu_sigma_color;            /* 0.04 */
+  float restorer_threshold;         /* 0.1 */
+  uint32_t weak_texture_prior;      /* upsampled planes as the coarse prior of finer levels (0) */
+  uint32_t run_id_base;             /* 1 */
+  uint32_t use_graph;               /* 1 */
+} ps_multiscale_schedule;
+void ps_multiscale_schedule_default(ps_multiscale_schedule* out);
+int ps_schedule_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps_multiscale_schedule* m);
 int ps_synchronize(ps_session* s);
 /* Number of kernel launches this session issued so far (for launch accounting). */
 uint64_t ps_launch_count(const ps_session* s);

@@ -42,6 +42,8 @@ STRUCTS = {
     "ps_level_image": _lib.LevelImage, "ps_pair_geometry": _lib.PairGeometry, "ps_kernel_view": _lib.KernelView,
     "ps_kernel_input": _lib.KernelInput, "ps_view_state": _lib.ViewState, "ps_run_params": _lib.RunParams,
     "ps_depth_snapshot": _lib.DepthSnapshot, "ps_schedule": _lib.Schedule,
+    "ps_multiscale_schedule": _lib.MultiscaleSchedule, "ps_post_params": _lib.PostParams,
+    "ps_fusion_params": _lib.FusionParams, "ps_fusion_view": _lib.FusionView,
 }
 
 

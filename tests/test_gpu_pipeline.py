@@ -38,3 +38,22 @@ def test_multiscale_schedule_bitwise_equal(backend, weak_var):
     for a, b in zip(g_fin, c_fin):
         np.testing.assert_array_equal(a.depth, b.depth)
     assert sum(float((f.depth > 0).mean()) for f in g_fin) > 0.3
+
+
+@pytest.mark.parametrize("weak_var,graph", [(0.0, True), (0.0, False), (0.002, True)])
+def test_multiscale_on_device_equals_host_driver(backend, weak_var, graph):
+    """ps_schedule_multiscale (every level on the device, one graph launch) = the host-driven compute_depth_maps."""
+    wl = scenes.workload_small(128, 96, views=3, window_radius=3, seed=17)
+    inp = _pyramid_input(wl, 3, weak_var)
+    sch = densify.Schedule(photometric_iters=2, photometric_iters_upper=1, geometric_rounds=1, geometric_iters=1)
+    with backend.begin(inp) as s:
+        _, h_fin, _ = densify.compute_depth_maps(s, inp, [0, 1, 2], sch, weak_texture_prior=weak_var > 0)
+    with backend.begin(inp) as s:
+        d_fin = densify.compute_depth_maps_resident(s, inp, [0, 1, 2], sch, weak_texture_prior=weak_var > 0,
+                                                    graph=graph)
+        again = densify.compute_depth_maps_resident(s, inp, [0, 1, 2], sch, weak_texture_prior=weak_var > 0,
+                                                    graph=graph)  # a replay gives the same maps
+    for a, b, c in zip(d_fin, h_fin, again):
+        np.testing.assert_array_equal(a.depth, b.depth)
+        np.testing.assert_array_equal(a.normal, b.normal)
+        np.testing.assert_array_equal(a.depth, c.depth)

@@ -171,6 +171,9 @@ SIGNATURES = {
                                    C.POINTER(C.c_uint64)]),
     "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_uint32]),
+    "ps_build_pyramid": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.c_uint32,
+                                   C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                   C.POINTER(C.c_double)]),
     "ps_write_ply": (C.c_int, [C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
     # learned proposal
     "ps_net_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),

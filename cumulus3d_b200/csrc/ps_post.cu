@@ -348,4 +348,43 @@ cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st) {
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------- image pyramid
+// One level of build_pyramid (crates/dense/src/upsample.rs:46-102): separable 3-tap blur with clamped borders
+// (tmp = g0·s[x-1] + g1·s[x] + g2·s[x+1], then the same vertically on tmp, each sum left to right), 2×2 average
+// 0.25·(((b00 + b01) + b10) + b11), rounded half away from zero and clamped to u8.  One thread per output pixel
+// recomputes the 4 × 2 blurred values it needs (no contraction: the same binary32 operations as the reference).
+__device__ __forceinline__ float pyr_src(const unsigned char* in, int w, int h, int y, int x) {
+  x = min(max(x, 0), w - 1);
+  y = min(max(y, 0), h - 1);
+  return (float)in[(long long)y * w + x];
+}
+__device__ __forceinline__ float pyr_tmp(const unsigned char* in, int w, int h, int y, int x, float g0, float g1,
+                                         float g2) {
+  return (g0 * pyr_src(in, w, h, y, x - 1) + g1 * pyr_src(in, w, h, y, x)) + g2 * pyr_src(in, w, h, y, x + 1);
+}
+__device__ __forceinline__ float pyr_blur(const unsigned char* in, int w, int h, int y, int x, float g0, float g1,
+                                          float g2) {
+  const int ym = max(y - 1, 0), yp = min(y + 1, h - 1);
+  return (g0 * pyr_tmp(in, w, h, ym, x, g0, g1, g2) + g1 * pyr_tmp(in, w, h, y, x, g0, g1, g2)) +
+         g2 * pyr_tmp(in, w, h, yp, x, g0, g1, g2);
+}
+__global__ void k_pyramid(const unsigned char* in, int w, int h, unsigned char* out, float g0, float g1, float g2) {
+  const int X = blockIdx.x * blockDim.x + threadIdx.x, Y = blockIdx.y * blockDim.y + threadIdx.y;
+  const int nw = w / 2, nh = h / 2;
+  if (X >= nw || Y >= nh) return;
+  const int y = 2 * Y, x = 2 * X;
+  const float b00 = pyr_blur(in, w, h, y, x, g0, g1, g2), b01 = pyr_blur(in, w, h, y, x + 1, g0, g1, g2);
+  const float b10 = pyr_blur(in, w, h, y + 1, x, g0, g1, g2), b11 = pyr_blur(in, w, h, y + 1, x + 1, g0, g1, g2);
+  const float v = 0.25f * (((b00 + b01) + b10) + b11);
+  out[(long long)Y * nw + X] = (unsigned char)fminf(fmaxf(roundf(v), 0.0f), 255.0f);
+}
+
+cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g,
+                           cudaStream_t st) {
+  const dim3 b(32, 8), gr((w / 2 + 31) / 32, (h / 2 + 7) / 8);
+  if (w / 2 < 1 || h / 2 < 1) return cudaSuccess;
+  k_pyramid<<<gr, b, 0, st>>>(in, w, h, out, g[0], g[1], g[2]);
+  return cudaGetLastError();
+}
+
 }  // namespace ps_post

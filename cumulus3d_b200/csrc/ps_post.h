@@ -65,5 +65,6 @@ struct FuseArgs {
 cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* launches);
 cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);
+cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g, cudaStream_t st);
 
 }  // namespace ps_post

@@ -1886,6 +1886,68 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
   });
 }
 
+// build_pyramid (crates/dense/src/upsample.rs:46-102) on the GPU.  Weights g = (e^-2, 1, e^-2) / ((e^-2 + 1) + e^-2)
+// in binary32 (f32::exp of -1/(2·0.25), summed left to right), as the reference computes them.
+int ps_build_pyramid(int device, const uint8_t* gray, uint32_t width, uint32_t height, const double* k,
+                     uint32_t levels, uint8_t* const* out, uint32_t* out_w, uint32_t* out_h, double* out_k) {
+  if (!gray || !out || !out_w || !out_h || levels < 1 || width < 1 || height < 1 || levels > 16) return PS_EINVAL;
+  for (uint32_t i = 0; i < levels; ++i)
+    if (!out[i]) return PS_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  const float e = std::exp(-1.0f / (2.0f * 0.25f));
+  const float sum = (e + 1.0f) + e;
+  const float g[3] = {e / sum, 1.0f / sum, e / sum};
+  std::vector<uint32_t> w(levels), h(levels);  // finest first
+  w[0] = width;
+  h[0] = height;
+  size_t total = 0;
+  for (uint32_t i = 0; i < levels; ++i) {
+    if (i) {
+      w[i] = w[i - 1] / 2;
+      h[i] = h[i - 1] / 2;
+      if (w[i] < 1 || h[i] < 1) return PS_EINVAL;
+    }
+    total += (size_t)w[i] * h[i];
+  }
+  unsigned char* d = nullptr;
+  cudaStream_t st = nullptr;
+  int rc = PS_OK;
+  if (cudaMalloc(&d, total) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    rc = PS_ENOMEM;
+  } else {
+    size_t off = 0;
+    std::vector<size_t> offs(levels);
+    for (uint32_t i = 0; i < levels; ++i) {
+      offs[i] = off;
+      off += (size_t)w[i] * h[i];
+    }
+    cudaError_t ce = cudaMemcpyAsync(d, gray, (size_t)width * height, cudaMemcpyHostToDevice, st);
+    for (uint32_t i = 1; i < levels && ce == cudaSuccess; ++i)
+      ce = ps_post::launch_pyramid(d + offs[i - 1], (int)w[i - 1], (int)h[i - 1], d + offs[i], g, st);
+    for (uint32_t i = 0; i < levels && ce == cudaSuccess; ++i)  // out[0] = coarsest
+      ce = cudaMemcpyAsync(out[levels - 1 - i], d + offs[i], (size_t)w[i] * h[i], cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) rc = PS_ECUDA;
+  }
+  if (st) cudaStreamDestroy(st);
+  cudaFree(d);
+  cudaGetLastError();
+  double kk[4] = {k ? k[0] : 0.0, k ? k[1] : 0.0, k ? k[2] : 0.0, k ? k[3] : 0.0};
+  for (uint32_t i = 0; i < levels; ++i) {
+    out_w[levels - 1 - i] = w[i];
+    out_h[levels - 1 - i] = h[i];
+    if (out_k) memcpy(out_k + 4 * (levels - 1 - i), kk, sizeof kk);
+    kk[0] = kk[0] * 0.5;
+    kk[1] = kk[1] * 0.5;
+    kk[2] = (kk[2] + 0.5) * 0.5 - 0.5;
+    kk[3] = (kk[3] + 0.5) * 0.5 - 0.5;
+  }
+  return rc;
+}
+
 int ps_synchronize(ps_session* s) {
   return guard(s, [&] { sync(s); });
 }

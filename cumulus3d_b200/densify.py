@@ -74,6 +74,26 @@ def build_pyramid(gray: np.ndarray, k: Sequence[float], levels: int) -> List[Lev
     return out
 
 
+def build_pyramid_device(gray: np.ndarray, k: Sequence[float], levels: int, device: int = 0) -> List[LevelImage]:
+    """build_pyramid on the GPU (ps_build_pyramid): the same levels as :func:`build_pyramid`, coarsest first."""
+    import ctypes as C
+    from . import _lib
+    g = np.ascontiguousarray(gray, np.uint8)
+    h, w = g.shape
+    sizes = [(w, h)]
+    for _ in range(1, levels):
+        sizes.append((sizes[-1][0] // 2, sizes[-1][1] // 2))
+    outs = [np.empty((sh, sw), np.uint8) for (sw, sh) in reversed(sizes)]
+    op = (C.c_void_p * levels)(*[o.ctypes.data for o in outs])
+    ow, oh = (C.c_uint32 * levels)(), (C.c_uint32 * levels)()
+    kin = (C.c_double * 4)(*[float(x) for x in k])
+    ko = (C.c_double * (4 * levels))()
+    rc = _lib.engine().ps_build_pyramid(device, g.ctypes.data, w, h, kin, levels, op, ow, oh, ko)
+    if rc != _lib.PS_OK:
+        raise _lib.PsError(rc, "ps_build_pyramid failed")
+    return [LevelImage(outs[i], tuple(ko[4 * i:4 * i + 4])) for i in range(levels)]
+
+
 def readout(states: Sequence[ViewState], counts: Sequence[np.ndarray], nsrc: Sequence[int],
             min_num_consistent: int) -> List[ViewState]:
     """Readout threshold (densify.rs:441-454): depth/normal zeroed where count < max(1, min(min_num_consistent, nsrc))."""

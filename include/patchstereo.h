@@ -423,6 +423,12 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride);
 
+/* build_pyramid (crates/dense/src/upsample.rs:46-102) on the GPU: out[0] is the coarsest level, out[levels-1] the
+ * input itself; level sizes halve (floor) towards the coarse end; out_k (may be NULL) receives 4 doubles per level
+ * (f·0.5, c ← (c + 0.5)·0.5 − 0.5 per step from k).  Blocking; allocates and frees its own device memory. */
+int ps_build_pyramid(int device, const uint8_t* gray, uint32_t width, uint32_t height, const double* k,
+                     uint32_t levels, uint8_t* const* out, uint32_t* out_w, uint32_t* out_h, double* out_k);
+
 /* DenseOutput::write_ply (crates/dense/src/densify.rs:143-153; crates/core/src/io/ply.rs:82-140, layout
  * XyzNormalRgb): binary little-endian PLY "x y z [nx ny nz] red green blue" (float / uchar), 27 bytes per point with
  * normals.  normals and colors may be NULL (colour 255 then). */

@@ -57,3 +57,17 @@ def test_multiscale_on_device_equals_host_driver(backend, weak_var, graph):
         np.testing.assert_array_equal(a.depth, b.depth)
         np.testing.assert_array_equal(a.normal, b.normal)
         np.testing.assert_array_equal(a.depth, c.depth)
+
+
+@pytest.mark.parametrize("shape,levels", [((96, 128), 3), ((1080, 1920), 4), ((77, 131), 3)])
+def test_pyramid_on_device_equals_host(shape, levels):
+    """ps_build_pyramid (GPU) = build_pyramid (host restatement of upsample.rs:46-102), levels and intrinsics."""
+    rng = np.random.default_rng(shape[0])
+    gray = rng.integers(0, 256, shape, dtype=np.uint8)
+    k = (1663.0, 1663.5, (shape[1] - 1) / 2.0, (shape[0] - 1) / 2.0)
+    host = densify.build_pyramid(gray, k, levels)
+    dev = densify.build_pyramid_device(gray, k, levels)
+    assert len(host) == len(dev) == levels
+    for a, b in zip(host, dev):
+        np.testing.assert_array_equal(a.pixels, b.pixels)
+        assert tuple(a.k) == tuple(b.k)

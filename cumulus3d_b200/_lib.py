@@ -189,6 +189,7 @@ SIGNATURES = {
     "ps_net_conv_check": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ps_sweep_volume": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),
+    "ps_set_sweep_normals": (C.c_int, [_P, C.c_void_p]),
     "ps_propose": (C.c_int, [_P, _P, C.c_uint32, _U32P, C.c_size_t, C.c_float, C.POINTER(C.c_uint64)]),
     "ps_proposal_upload": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_float))]),
     "ps_proposal_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(C.POINTER(C.c_float)),

@@ -804,8 +804,9 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
 }
 
 // ================================================================================ plane sweep (learned proposal input)
-// Cost volume of one view for the proposal network (no reference counterpart).  PS_SWEEP_PLANES fronto-parallel
-// planes n = (0, 0, -1) at inverse depths i_k = 1/dmax + (2k+1)/64 · (1/dmin - 1/dmax) (bin centres); the cost of a
+// Cost volume of one view for the proposal network (no reference counterpart).  PS_SWEEP_PLANES planes with the
+// normal P.sweep_n (fronto-parallel (0, 0, -1) unless the caller set one, e.g. the world's up direction in the camera
+// frame) through inverse depths i_k = 1/dmax + (2k+1)/64 · (1/dmin - 1/dmax) (bin centres) at the pixel; the cost of a
 // plane is the mean over the first min(2, nsrc) sources of the NCC cost 1 - ρ (the same window statistics, homography
 // and NCC as the half step, window radius wr and step P.sweep_ws), 2 where the homography fails.  Output per pixel,
 // bf16 (round to nearest even): [image, cost_0 … cost_31, 0 × 15] at netin[(y · netin_pitch + x) · 48].
@@ -844,7 +845,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__
 #pragma unroll 1
   for (int k = 0; k < PS_SWEEP_PLANES; ++k) {
     const float id = fmaf((float)(2 * k + 1) * (1.0f / 64.0f), inear - ifar, ifar);
-    const float4 h = make_float4(0.0f, 0.0f, -1.0f, 1.0f / id);
+    const float4 h = make_float4(P.sweep_n[0], P.sweep_n[1], P.sweep_n[2], 1.0f / id);
     float c = 0.0f;
 #pragma unroll 1
     for (int j = 0; j < nuse; ++j) {

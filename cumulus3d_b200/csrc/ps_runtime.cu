@@ -146,6 +146,7 @@ struct ps_session {
   std::vector<int> nsrc;
   std::vector<std::vector<int>> sources;
   std::vector<PsLevel> lvh;  // host copies of the level and view tables
+  std::vector<float> sweep_n;  // plane-sweep normal per view (3 floats; fronto-parallel by default)
   std::vector<PsView> vdh;
   // learned proposal buffers (network input / output of one view, grown on demand)
   unsigned short* netin = nullptr;
@@ -826,6 +827,8 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
       vdh[v].pad = 0;
     }
     s->vdh = vdh;
+    s->sweep_n.assign(3 * (size_t)std::max(s->nv, 1), 0.0f);
+    for (int v = 0; v < s->nv; ++v) s->sweep_n[3 * v + 2] = -1.0f;
     s->pairs = dalloc<PsPair>(prh.size());
     s->views = dalloc<PsView>(vdh.size());
     s->pairs64 = dalloc<double>(p64.size());
@@ -1497,6 +1500,7 @@ void enqueue_sweep(ps_session* s, int level, uint32_t view, unsigned short* out,
   P.netin = out;
   P.netin_pitch = row_pixels;
   P.sweep_ws = 2;
+  for (int c = 0; c < 3; ++c) P.sweep_n[c] = s->sweep_n[3 * view + c];
   set_items(s, P, &view, 0, 1, level, PS_EVAL_PW, PS_EVAL_PH);
   const bool tex = (s->tuning & PS_TUNE_TEX_GATHER) != 0;  // the session built texture objects for its planes
   timed_launch(s, PS_KERNEL_SWEEP, P, [&](const PsRun& q) { return s->L->sweep(q, tex, s->st); }, "sweep kernel");
@@ -1515,6 +1519,21 @@ void grow(ps_session* s, T*& buf, size_t& cap, size_t elems) {
 
 }  // namespace
 }  // extern "C++"
+
+int ps_set_sweep_normals(ps_session* s, const float* normals) {
+  return guard(s, [&] {
+    for (int v = 0; v < s->nv; ++v) {
+      const float* n = normals ? normals + 3 * v : nullptr;
+      const float x = n ? n[0] : 0.0f, y = n ? n[1] : 0.0f, z = n ? n[2] : -1.0f;
+      const float len = std::sqrt(x * x + y * y + z * z);
+      if (!(len > 0.5f && len < 2.0f) || !(z < 0.0f)) fail(PS_EINVAL, "sweep normal of view " + std::to_string(v) +
+                                                               " must be a unit vector facing the camera (z < 0)");
+      s->sweep_n[3 * v] = x;
+      s->sweep_n[3 * v + 1] = y;
+      s->sweep_n[3 * v + 2] = z;
+    }
+  });
+}
 
 int ps_sweep_volume(ps_session* s, uint32_t level, uint32_t view, void* out, uint32_t row_pixels) {
   return guard(s, [&] {

@@ -100,5 +100,6 @@ struct PsRun {
   unsigned short* netin;   // plane sweep: bf16 network input [rows][netin_pitch][PS_NET_CH_IN] of the run's one view
   int netin_pitch;         // pixels per row of netin
   int sweep_ws;            // plane sweep: window step
+  float sweep_n[3];        // plane sweep: plane normal in the reference camera frame (n · ray < 0)
   PsItem items[PS_MAX_ITEMS];
 };

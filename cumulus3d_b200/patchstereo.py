@@ -437,6 +437,14 @@ class PatchMatchSession:
         the session stream)."""
         self._check(self.lib.ps_sweep_volume(self.h, level, view, C.c_void_p(out_ptr), row_pixels))
 
+    def set_sweep_normals(self, normals: Optional[np.ndarray]) -> None:
+        """(n_views, 3) plane-sweep normals in each camera frame, or None for fronto-parallel planes."""
+        if normals is None:
+            self._check(self.lib.ps_set_sweep_normals(self.h, None))
+            return
+        a = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+        self._check(self.lib.ps_set_sweep_normals(self.h, a.ctypes.data))
+
     def propose(self, net, level: int, views: Sequence[int], conf_threshold: float = 0.5,
                 count: bool = True) -> Optional[int]:
         """Sweep + network + decode into the session's proposal store; returns the number of proposed pixels."""

@@ -135,6 +135,17 @@ def render(cams: Sequence[Camera], seed: int, *, relief: float = 8.0, wavelength
     return img, dep, nrm
 
 
+def up_normals(cams: Sequence[Camera], up=(0.0, 0.0, 1.0)) -> np.ndarray:
+    """The world's up direction in each camera frame (R · up), turned to face the camera: (n_views, 3) f32, for the
+    plane sweep of the learned proposal (its planes then follow the ground's tilt)."""
+    out = np.zeros((len(cams), 3), np.float32)
+    for i, c in enumerate(cams):
+        n = np.asarray(c.r, np.float64) @ np.asarray(up, np.float64)
+        n = n / np.linalg.norm(n)
+        out[i] = -n if n[2] > 0 else n
+    return out
+
+
 def pair_geometry(ref: Camera, src: Camera) -> np.ndarray:
     """Reference -> source relative geometry in FP64 (crates/dense/src/densify.rs:183-205): R = R_s R_rᵀ,
     t = t_s - R t_r, centre = -Rᵀ t.  Returns 15 doubles (r[9], t[3], center[3])."""

@@ -356,6 +356,10 @@ int ps_net_conv_check(int device, const uint16_t* x, const float* w, const uint1
  * centres between 1/dmax and 1/dmin; mean over the first two sources; window radius as the session's, step 2).
  * Asynchronous on the session stream. */
 int ps_sweep_volume(ps_session* s, uint32_t level, uint32_t view, void* out, uint32_t row_pixels);
+/* Plane normal of each view's sweep in its camera frame (3 floats per session view; NULL = fronto-parallel
+ * (0, 0, -1), the default).  Aerial callers pass the world's up direction seen from the camera (R · up), so the sweep
+ * planes follow the ground's tilt.  Unit length, z < 0. */
+int ps_set_sweep_normals(ps_session* s, const float* normals);
 /* Sweep + network + decode for `views` at `level`: stores each view's proposal (planes with d = 0 where the
  * confidence is below conf_threshold) in the session for a later PS_INIT_PROPOSAL run start.  `proposed` (may be
  * NULL; then asynchronous) receives the number of proposed pixels. */

@@ -38,7 +38,7 @@ def lib() -> C.CDLL:
                                           C.c_int, C.c_int]),
             "oracle_run_init": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, C.POINTER(_lib.RunParams), _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int, C.c_int, C.c_int]),
-            "oracle_sweep": (C.c_int, [_KI, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_int]),
+            "oracle_sweep": (C.c_int, [_KI, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_int]),
             "oracle_remove_speckles": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_float,
                                                  C.c_double, C.c_float, C.POINTER(C.c_uint64)]),
             "oracle_fuse": (C.c_int, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
@@ -108,13 +108,16 @@ def run(inp: KernelInput, views: Sequence[int], states: List[ViewState], p: RunP
                                c_snapshot(snapshot, keep), pp, _threads(threads), y0, y1), "run")
 
 
-def sweep(inp: KernelInput, level: int, view: int, threads: Optional[int] = None) -> np.ndarray:
+def sweep(inp: KernelInput, level: int, view: int, threads: Optional[int] = None,
+          normal: Optional[Sequence[float]] = None) -> np.ndarray:
     """The plane-sweep network input of one view: (h, w, 48) uint16 bf16 bits (image, 32 costs, zeros)."""
     ci = CInput(inp)
     lv = inp.views[view].levels[level]
     h, w = lv.pixels.shape[:2]
     out = np.zeros((h, w, _lib.PS_NET_CH_IN), np.uint16)
-    _chk(lib().oracle_sweep(C.byref(ci.c), level, view, out.ctypes.data, w, _threads(threads)), "sweep")
+    n = None if normal is None else np.ascontiguousarray(normal, np.float32)
+    _chk(lib().oracle_sweep(C.byref(ci.c), level, view, out.ctypes.data, w, None if n is None else n.ctypes.data,
+                            _threads(threads)), "sweep")
     return out
 
 

@@ -829,10 +829,11 @@ int oracle_run(const ps_kernel_input* in, const uint32_t* views, size_t n, ps_vi
 
 // Plane-sweep network input of one view (the engine's ps_sweep_volume; no reference counterpart): per pixel, bf16
 // bits of [image, 32 costs, 15 zeros] where cost k is the mean over the first min(2, nsrc) sources of the NCC cost of
-// the fronto-parallel plane (0, 0, -1, 1/i_k), i_k = fma((2k+1)/64, 1/dmin - 1/dmax, 1/dmax), window radius as the
-// session's and step 2 (2 where the homography fails).  Rows of `row_pixels` pixels.
+// the plane (n, 1/i_k) at the pixel, n = `normal` (NULL: fronto-parallel (0, 0, -1)),
+// i_k = fma((2k+1)/64, 1/dmin - 1/dmax, 1/dmax), window radius as the session's and step 2 (2 where the homography
+// fails).  Rows of `row_pixels` pixels.
 int oracle_sweep(const ps_kernel_input* in, uint32_t level, uint32_t view, uint16_t* out, uint32_t row_pixels,
-                 int threads) {
+                 const float* normal, int threads) {
   Scene sc;
   if (!load_scene(in, sc) || view >= sc.v.size() || (int)level >= sc.nl || !out) return PS_EINVAL;
   sc.ws = 2;
@@ -857,7 +858,7 @@ int oracle_sweep(const ps_kernel_input* in, uint32_t level, uint32_t view, uint1
       o[0] = bf16(R.at(x, y));
       for (int k = 0; k < PS_SWEEP_PLANES; ++k) {
         const float id = std::fma((float)(2 * k + 1) * (1.0f / 64.0f), inear - ifar, ifar);
-        const P4 h = {0.0f, 0.0f, -1.0f, 1.0f / id};
+        const P4 h = {normal ? normal[0] : 0.0f, normal ? normal[1] : 0.0f, normal ? normal[2] : -1.0f, 1.0f / id};
         float c = 0.0f;
         for (int j = 0; j < nuse; ++j) {
           const Img& S = sc.L(vd.pairs[j].src, (int)level);

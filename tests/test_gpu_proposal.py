@@ -221,3 +221,22 @@ def test_training_reduces_loss():
     assert np.mean(losses[-5:]) < 0.85 * np.mean(losses[:5]), (losses[:5], losses[-5:])
     assert net.step == 60
     net.close()
+
+
+def test_sweep_with_ground_normals_bitwise_vs_oracle():
+    """A caller-set sweep normal (the world's up seen from each camera) reaches the kernel and matches the oracle."""
+    wl = scenes.workload_small(64, 48, views=3, window_radius=3, seed=12)
+    normals = scenes.up_normals(wl.cams)
+    be = PatchMatchBackend(0, math="parity", tuning=6)
+    with be.begin(wl.input) as s:
+        s.set_sweep_normals(normals)
+        buf = torch.zeros((48, 64, 48), dtype=torch.int16, device="cuda")
+        torch.cuda.synchronize()
+        s.sweep_volume(0, 1, buf.data_ptr(), 64)
+        s.synchronize()
+        got = buf.cpu().numpy().view(np.uint16)
+        with pytest.raises(_lib.PsError):  # a normal facing away from the camera is rejected
+            s.set_sweep_normals(-normals)
+    be.close()
+    np.testing.assert_array_equal(got, oracle.sweep(wl.input, 0, 1, normal=normals[1]))
+    assert not np.array_equal(got, oracle.sweep(wl.input, 0, 1))  # and differs from the fronto-parallel sweep

@@ -331,7 +331,9 @@ def fusion_stage(args, wl, sess, mine, check=True, label="plain"):
         from oracle import oracle
         st = sess.readout_download(0, mine)
         t1 = time.perf_counter()
-        imgs = [kv.levels[0].pixels for kv in wl.input.views]  # f32 planes, as the engine stores them
+        from cumulus3d_b200 import scenes
+        imgs = [scenes.unit_plane(kv.levels[0].pixels) if kv.levels[0].pixels.dtype == np.uint8
+                else kv.levels[0].pixels for kv in wl.input.views]  # the f32 planes the engine computes with
         ref = oracle.fuse(fc, [x.depth for x in st], [x.normal for x in st], [x.cost for x in st], imgs, mine, prm)
         out["oracle_points"] = len(ref)
         out["oracle_s"] = round(time.perf_counter() - t1, 2)

@@ -15,6 +15,10 @@ struct PsConsts {
   float cos_filter_tri, q_min, ncc_norm, inv2ncc, filter_gmax, weak_var;
 };
 
+// An 8-bit gray value as the unit-range f32 the engine computes with: the correctly rounded u/255 (the value an
+// 8-bit normalized texture fetch returns, so texture and plane sampling agree bit for bit).
+static inline float ps_u8_unit(unsigned char u) { return (float)((double)u / 255.0); }
+
 // Rust's f64::to_radians: x * (PI / 180) with the quotient taken in binary64.
 static inline double ps_to_radians_f64(double deg) { return deg * (3.14159265358979323846 / 180.0); }
 

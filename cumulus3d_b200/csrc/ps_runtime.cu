@@ -748,7 +748,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
         for (uint32_t y = 0; y < li.height; ++y) {
           if (li.format == PS_IMAGE_U8) {
             const uint8_t* src = (const uint8_t*)li.pixels + y * stride;
-            for (uint32_t x = 0; x < li.width; ++x) dst[y * pitch + x] = (float)src[x] * (1.0f / 255.0f);
+            for (uint32_t x = 0; x < li.width; ++x) dst[y * pitch + x] = ps_u8_unit(src[x]);
           } else {
             const float* src = (const float*)li.pixels + y * stride;
             memcpy(dst + y * pitch, src, li.width * sizeof(float));
@@ -768,17 +768,27 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
       }
     cuda_ok(cudaMemcpyAsync(s->img, host.data(), total * sizeof(float), cudaMemcpyHostToDevice, s->st), "upload images");
     if (s->tuning & PS_TUNE_TEX_GATHER) {
-      // one gather-capable CUDA array + border-addressed point texture per (view, level), filled from the plane
-      const cudaChannelFormatDesc cd = cudaCreateChannelDesc<float>();
+      // one gather-capable CUDA array + border-addressed point texture per (view, level).  8-bit images keep 8-bit
+      // texels read as normalized floats (the texture unit returns the correctly rounded u/255, the plane's value, for
+      // every u); f32 images are copied from the plane.
+      const cudaChannelFormatDesc cdf = cudaCreateChannelDesc<float>();
+      const cudaChannelFormatDesc cd8 = cudaCreateChannelDesc<unsigned char>();
       for (int v = 0; v < s->nv; ++v)
         for (int l = 0; l < s->nl; ++l) {
           PsLevel& L = lvh[v * s->nl + l];
+          const ps_level_image& li = in->views[v].levels[l];
+          const bool u8 = li.format == PS_IMAGE_U8;
           cudaArray_t arr = nullptr;
-          cuda_ok(cudaMallocArray(&arr, &cd, L.w, L.h, cudaArrayTextureGather), "cudaMallocArray");
+          cuda_ok(cudaMallocArray(&arr, u8 ? &cd8 : &cdf, L.w, L.h, cudaArrayTextureGather), "cudaMallocArray");
           s->arrays.push_back(arr);
-          cuda_ok(cudaMemcpy2DToArrayAsync(arr, 0, 0, L.img, L.pitch * sizeof(float), L.w * sizeof(float), L.h,
-                                           cudaMemcpyDeviceToDevice, s->st),
-                  "copy texture array");
+          if (u8)
+            cuda_ok(cudaMemcpy2DToArray(arr, 0, 0, li.pixels, li.stride ? li.stride : li.width, L.w, L.h,
+                                        cudaMemcpyHostToDevice),
+                    "copy texture array");
+          else
+            cuda_ok(cudaMemcpy2DToArrayAsync(arr, 0, 0, L.img, L.pitch * sizeof(float), L.w * sizeof(float), L.h,
+                                             cudaMemcpyDeviceToDevice, s->st),
+                    "copy texture array");
           cudaResourceDesc rd;
           memset(&rd, 0, sizeof rd);
           rd.resType = cudaResourceTypeArray;
@@ -787,7 +797,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
           memset(&td, 0, sizeof td);
           td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
           td.filterMode = cudaFilterModePoint;
-          td.readMode = cudaReadModeElementType;
+          td.readMode = u8 ? cudaReadModeNormalizedFloat : cudaReadModeElementType;
           td.normalizedCoords = 0;
           cudaTextureObject_t t = 0;
           cuda_ok(cudaCreateTextureObject(&t, &rd, &td, nullptr), "cudaCreateTextureObject");

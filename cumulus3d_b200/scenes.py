@@ -166,17 +166,31 @@ def nearest_sources(cams: Sequence[Camera], k: int) -> List[List[int]]:
     return out
 
 
+def to_gray8(img: np.ndarray) -> np.ndarray:
+    """A rendered unit-range image as the 8-bit gray the reference's LevelImage holds (crates/dense/src/kernel.rs:80-91):
+    round(255·v), clamped."""
+    return np.clip(np.round(np.asarray(img, np.float64) * 255.0), 0, 255).astype(np.uint8)
+
+
+def unit_plane(gray8: np.ndarray) -> np.ndarray:
+    """The engine's f32 plane of an 8-bit image: the correctly rounded u/255 per pixel."""
+    return (np.asarray(gray8, np.float64) / 255.0).astype(np.float32)
+
+
 def kernel_input(cams: Sequence[Camera], images: Sequence[np.ndarray], sources: Sequence[Sequence[int]],
                  depth_range: Tuple[float, float], *, window_radius: int, window_step: int = 1, seed: int = 0x005EED0FDE75,
-                 fast_filter: bool = True, ranges: Optional[Sequence[Tuple[float, float]]] = None) -> KernelInput:
-    """Single-level KernelInput: each view's f32 image, its sources with f32 pairs (and the FP64 pairs)."""
+                 fast_filter: bool = True, ranges: Optional[Sequence[Tuple[float, float]]] = None,
+                 gray8: bool = True) -> KernelInput:
+    """Single-level KernelInput: each view's image (8-bit gray by default, as the reference takes it; f32 with
+    gray8=False), its sources with f32 pairs (and the FP64 pairs)."""
     views = []
     for i, cam in enumerate(cams):
         p64 = np.stack([pair_geometry(cam, cams[j]) for j in sources[i]]) if sources[i] else np.zeros((0, 15))
         pairs = [PairGeometry(p[:9].astype(np.float32), p[9:12].astype(np.float32), p[12:15].astype(np.float32))
                  for p in p64]
         dr = ranges[i] if ranges is not None else depth_range
-        views.append(KernelView(fnv1a(cam.name.encode()), [LevelImage(images[i], cam.k)], list(sources[i]), pairs,
+        img = to_gray8(images[i]) if gray8 and np.asarray(images[i]).dtype != np.uint8 else images[i]
+        views.append(KernelView(fnv1a(cam.name.encode()), [LevelImage(img, cam.k)], list(sources[i]), pairs,
                                 float(dr[0]), float(dr[1]), p64))
     pm = _lib.default_pm()
     pm.window_radius = window_radius

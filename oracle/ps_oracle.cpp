@@ -20,7 +20,7 @@
 // where the reference leaves the choice to the compiler (contraction, __expf, rsqrtf, the approximate division of
 // its fast-math build, hardware bilinear) are fixed as follows, identically in the engine: the projective
 // reciprocal 1/z of the NCC (centre and taps) is ps_rcpf (Newton, <= 0.5006 ulp); bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
-// fma(ay, bot-top, top) on values already divided by 255; tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
+// fma(ay, bot-top, top) on unit-range values (8-bit input: the correctly rounded u/255); tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
 // the two numerators); window accumulation Ss += w·s, SSs = fma(w·s, s, SSs), IS = fma(w·s, Ik, IS); reference
 // statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); every window sum (W, S, SS, Ss, SSs, IS) is kept as two partial
 // sums by row parity — even rows and odd rows, each in ascending row and column order — and the total is
@@ -189,7 +189,7 @@ bool load_scene(const ps_kernel_input* in, Scene& sc) {
       for (int y = 0; y < im.h; ++y)
         for (int x = 0; x < im.w; ++x)
           im.px[(size_t)y * im.w + x] = li.format == PS_IMAGE_U8
-                                            ? (float)((const uint8_t*)li.pixels)[y * stride + x] * (1.0f / 255.0f)
+                                            ? ps_u8_unit(((const uint8_t*)li.pixels)[y * stride + x])
                                             : ((const float*)li.pixels)[y * stride + x];
     }
     v.pairs.resize(kv.num_sources);

@@ -62,7 +62,7 @@ def test_fusion_bitwise_vs_oracle(pipeline):
     n = s.fuse_resident(0, views, fc, prm)
     got = s.fused_points()
     want = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
-                       list(wl.images), views, prm)
+                       [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views], views, prm)
     assert n == len(want) > 0
     np.testing.assert_array_equal(got.keys, want.keys)
     np.testing.assert_array_equal(got.positions, want.positions)
@@ -74,6 +74,6 @@ def test_fusion_bitwise_vs_oracle(pipeline):
     # the subset without view 0 (view 0's pixels neither references nor partners)
     n2 = s.fuse_resident(0, views[1:], fc, prm)
     want2 = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
-                        list(wl.images), views[1:], prm)
+                        [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views], views[1:], prm)
     assert n2 == len(want2)
     np.testing.assert_array_equal(s.fused_points().keys, want2.keys)

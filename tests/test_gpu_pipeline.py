@@ -12,7 +12,8 @@ pytestmark = pytest.mark.gpu
 def _pyramid_input(wl, levels=3, weak_var=0.0, median=True):
     views = []
     for v, cam in zip(wl.input.views, wl.cams):
-        g = np.clip(np.round(v.levels[0].pixels * 255.0), 0, 255).astype(np.uint8)  # 8-bit gray, as the reference
+        px = v.levels[0].pixels  # 8-bit gray, as the reference takes it
+        g = px if px.dtype == np.uint8 else scenes.to_gray8(px)
         v.levels = densify.build_pyramid(g, cam.k, levels)
         views.append(v)
     inp = KernelInput(views, levels, wl.input.pm, wl.input.filter, wl.input.seed)

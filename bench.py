@@ -358,7 +358,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     import torch
     from cumulus3d_b200 import _lib, proposal
 
-    net = proposal.ProposalNet(local, weights=proposal.DEFAULT_WEIGHTS)
+    net = proposal.ProposalNet(local, weights=args.weights or proposal.DEFAULT_WEIGHTS)
     k = args.learned_iters
     plain_depth = np.stack([o.depth for o in sess.readout_resident(mine)])  # the last plain step's result
 
@@ -394,6 +394,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     ms_short = timed(lambda: sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters,
                                                      graph=not args.no_graph), 1, 2)
     short_depth = depth()
+    short_fused = fusion_stage(args, wl, sess, mine, check=False)["points"]
     sess.schedule_resident(mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters, run_id_base=101,
                            graph=False)
     seed_depth = depth()
@@ -427,7 +428,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
                                    "of it; the plain schedule rerun with another RNG seed sets the floor"},
         "fused_points": learned_fused,
         "plain_same_iterations": {"value": round(n / (ms_short / 1e3), 3), "ms_per_step": round(ms_short, 2),
-                                  "agree_with_plain": agree(short_depth),
+                                  "agree_with_plain": agree(short_depth), "fused_points": short_fused,
                                   "coverage": round(float((short_depth > 0).mean()), 4)},
         "net_roofline": {"bound": "tensor", "kernel": "proposal network forward (12 conv layers, mma.sync bf16)",
                          "achieved": round(achieved, 2), "peak": bf16_peak, "unit": "TFLOP/s",
@@ -568,6 +569,7 @@ def main():
     ap.add_argument("--no-check", action="store_true",
                     help="skip the CPU oracle checks (fused point count, FP64 re-evaluation)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-init schedule")
+    ap.add_argument("--weights", default=None, help="proposal network parameters (.npz; default: the committed ones)")
     ap.add_argument("--learned-iters", type=int, default=3,
                     help="photometric iterations of the learned-init schedule")
     args = ap.parse_args()

@@ -361,6 +361,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     import torch
     from cumulus3d_b200 import _lib, proposal
 
+    proposal.set_conv_path(args.conv_path)
     net = proposal.ProposalNet(local, weights=args.weights or proposal.DEFAULT_WEIGHTS)
     k = args.learned_iters
     # final depth maps of every view, flattened into one vector (views may differ in size)
@@ -573,6 +574,8 @@ def main():
                     help="skip the CPU oracle checks (fused point count, FP64 re-evaluation)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-init schedule")
     ap.add_argument("--weights", default=None, help="proposal network parameters (.npz; default: the committed ones)")
+    ap.add_argument("--conv-path", default="auto", choices=["auto", "mma", "tcgen05"],
+                    help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
     ap.add_argument("--learned-iters", type=int, default=3,
                     help="photometric iterations of the learned-init schedule")
     args = ap.parse_args()

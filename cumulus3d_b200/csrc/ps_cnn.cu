@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <new>
@@ -202,6 +203,236 @@ __global__ void __launch_bounds__(256) k_conv2(ConvArgs a) {
       if (a.yf) *reinterpret_cast<float2*>(a.yf + p * a.cout + co) = make_float2(v0, v1);
     }
   }
+}
+
+// ------------------------------------------------------------------------------------------- conv forward on tcgen05
+// Inference and training convolutions with cout = N in {32, 64, 96, 128} on the 5th-generation tensor cores.  A CTA
+// (4 warps) computes R = 4 output rows × 128 pixels × N channels; the R accumulators D_r[128 × N] (f32) sit side by side
+// in tensor memory (columns r·N .. r·N + N).  Per chunk of KCH input channels the CTA stages, with cp.async into a
+// double buffer,
+//   * the R + 2 input rows y0-1 .. y0+R over pixels x0-1 .. x0+128 in the canonical K-major layout without swizzle,
+//     [row][kgroup (8 channels)][pixel][8 channels] = 16 bytes per (pixel, kgroup): the A operand of output row r and
+//     tap (dy, dx) is input row r + dy with its start address moved by dx pixels (16 bytes), so nothing is re-laid;
+//   * the chunk's weights of the 9 taps as [tap][kgroup][n][8 channels] (the B operand, shared by the R rows).
+// One thread issues R × 9 taps × KCH/16 tcgen05.mma (M = 128, N, K = 16, bf16 -> f32) and commits them to the stage's
+// mbarrier; refilling that stage waits on it.  The epilogue reads each D_r with tcgen05.ld (warp w owns TMEM lanes
+// 32w .. 32w+31 = pixels), adds the bias, applies ReLU and stores bf16 or f32.  Every wait is bounded: on expiry the
+// kernel counts it in g_conv5_timeouts and skips the remaining work (the host reports invalid results); every CTA frees
+// its tensor memory before it exits.
+constexpr int T5_PX = 128, T5_ROWPX = T5_PX + 2;  // pixels per row segment, staged pixels per row
+constexpr long long T5_SPIN = 1ll << 20;                     // bound on mbarrier polls (a chunk takes microseconds)
+__device__ unsigned int g_conv5_timeouts = 0;
+
+template <int N>
+struct Conv5Cfg {
+  static constexpr int R = N <= 32 ? 2 : 4;      // output rows per CTA (two CTAs per SM for N = 32)
+  static constexpr int KCH = N <= 64 ? 32 : 16;  // input channels per stage
+  static constexpr int KG = KCH / 8;             // kgroups per stage
+  static constexpr size_t in_bytes = (size_t)(R + 2) * KG * T5_ROWPX * 16;
+  static constexpr size_t w_bytes = (size_t)9 * KG * N * 16;
+  static constexpr size_t smem = 2 * (in_bytes + w_bytes) + 64;
+  static constexpr int cols = R * N <= 64 ? 64 : (R * N <= 128 ? 128 : (R * N <= 256 ? 256 : 512));  // 2^k >= R·N
+};
+
+// Shared-memory matrix descriptor, K-major, no swizzle (16-byte rows in groups of 8 at `sbo`, K chunks at `lbo`).
+__device__ __forceinline__ uint64_t umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100; base offset 0, layout type 0 (no swizzle)
+  return d;
+}
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
+}
+// Waits for the completion of the phase with the given parity; false if the bound expired.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (long long i = 0; i < T5_SPIN; ++i) {
+    unsigned done;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 1) k_conv5(ConvArgs a) {
+  using Cfg = Conv5Cfg<N>;
+  constexpr int KCH = Cfg::KCH, KG = Cfg::KG, T5_R = Cfg::R;
+  extern __shared__ __align__(128) unsigned char sm5[];
+  unsigned char* in_s = sm5;                        // [2][R+2][KG][130][16 B]
+  unsigned char* w_s = sm5 + 2 * Cfg::in_bytes;     // [2][9][KG][N][16 B]
+  unsigned char* misc = w_s + 2 * Cfg::w_bytes;     // mbarriers, TMEM address, flags
+  const unsigned bar0 = smem_u32(misc), bar1 = smem_u32(misc + 8);
+  volatile unsigned* tmem_slot = reinterpret_cast<volatile unsigned*>(misc + 16);
+  volatile int* fail_flag = reinterpret_cast<volatile int*>(misc + 20);
+  volatile int* last_commit = reinterpret_cast<volatile int*>(misc + 24);  // last chunk whose MMAs were committed
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int segs = (a.W + T5_PX - 1) / T5_PX, bands = (a.H + T5_R - 1) / T5_R;
+  int t = blockIdx.x;
+  const int seg = t % segs;
+  t /= segs;
+  const int y0 = (t % bands) * T5_R, b = t / bands;
+  const int x0 = seg * T5_PX;
+  const int nchunks = (a.cin + KCH - 1) / KCH;
+
+  if (warp == 0) {  // tensor memory for the accumulators (warp-wide)
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(misc + 16)),
+                 "r"(Cfg::cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
+  }
+  if (tid == 0) {
+    mbar_init(bar0, 1);
+    mbar_init(bar1, 1);
+    *fail_flag = *(volatile unsigned*)&g_conv5_timeouts != 0;  // after any expired wait, skip all work quickly
+    *last_commit = -1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const unsigned tmem = *tmem_slot;
+
+  auto load_stage = [&](int stage, int kc) {
+    const int c0 = kc * KCH;
+    unsigned char* is = in_s + (size_t)stage * Cfg::in_bytes;
+    for (int i = tid; i < (T5_R + 2) * KG * T5_ROWPX; i += 128) {
+      const int px = i % T5_ROWPX, g = (i / T5_ROWPX) % KG, r = i / (T5_ROWPX * KG);
+      const int gy = y0 + r - 1, gx = x0 + px - 1, ch = c0 + g * 8;
+      const bool ok = gy >= 0 && gy < a.H && gx >= 0 && gx < a.W && ch < a.cin;
+      const bf16* src = a.x;
+      if (ok) {
+        if (!a.x2)
+          src = a.x + (((long long)b * a.H + gy) * a.W + gx) * a.cin_stride + a.cin_off + ch;
+        else if (ch < a.split)
+          src = a.x + (((long long)b * (a.H >> 1) + (gy >> 1)) * (a.W >> 1) + (gx >> 1)) * a.cin_stride + ch;
+        else
+          src = a.x2 + (((long long)b * a.H + gy) * a.W + gx) * a.x2_stride + (ch - a.split);
+      }
+      cp_async16(is + ((size_t)(r * KG + g) * T5_ROWPX + px) * 16, src, ok ? 16 : 0);
+    }
+    unsigned char* ws = w_s + (size_t)stage * Cfg::w_bytes;
+    for (int i = tid; i < 9 * KG * N; i += 128) {
+      const int n = i % N, g = (i / N) % KG, tap = i / (N * KG);
+      const int ch = c0 + g * 8;
+      const bool ok = n < a.cout && ch < a.cin;
+      const bf16* src = ok ? a.w + ((long long)n * 9 + tap) * a.cin + ch : a.w;
+      cp_async16(ws + ((size_t)(tap * KG + g) * N + n) * 16, src, ok ? 16 : 0);
+    }
+    cp_async_commit();
+  };
+
+  // instruction descriptor: f32 accumulator, bf16 A and B, both K-major, N, M = 128
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+  load_stage(0, 0);
+  for (int kc = 0; kc < nchunks; ++kc) {
+    const int st = kc & 1;
+    if (kc + 1 < nchunks) {
+      // the stage about to be refilled held chunk kc-1: its MMAs must have finished reading it
+      if (kc >= 1 && !*fail_flag && !mbar_wait(st ? bar0 : bar1, ((kc - 1) >> 1) & 1)) {
+        *fail_flag = 1;
+        atomicAdd(&g_conv5_timeouts, 1u);
+      }
+      load_stage((kc + 1) & 1, kc + 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // cp.async data -> tensor-core operand reads
+    __syncthreads();
+    if (tid == 0 && !*fail_flag) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+      const unsigned ib = smem_u32(in_s + (size_t)st * Cfg::in_bytes);
+      const unsigned wb = smem_u32(w_s + (size_t)st * Cfg::w_bytes);
+#pragma unroll 1
+      for (int tap = 0; tap < 9; ++tap) {
+        const int dy = tap / 3, dx = tap - dy * 3;
+#pragma unroll
+        for (int ks = 0; ks < KCH / 16; ++ks) {
+          const unsigned baddr = wb + (unsigned)(((tap * KG + 2 * ks) * N) * 16);
+          const uint64_t bd = umma_desc(baddr, N * 16, 128);
+          const unsigned acc = (kc | tap | ks) != 0;
+#pragma unroll
+          for (int r = 0; r < T5_R; ++r) {
+            const unsigned aaddr = ib + (unsigned)((((r + dy) * KG + 2 * ks) * T5_ROWPX + dx) * 16);
+            const uint64_t ad = umma_desc(aaddr, T5_ROWPX * 16, 128);
+            asm volatile(
+                "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n}\n" ::"r"(
+                    tmem + (unsigned)(r * N)),
+                "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                       st ? bar1 : bar0)
+                   : "memory");
+      *last_commit = kc;
+    }
+  }
+  // the last commit covers every MMA this CTA issued: wait for it before reading or freeing tensor memory
+  __syncthreads();
+  const int lc = *last_commit;
+  const bool failed = *fail_flag;
+  const bool done = !failed && lc >= 0 && mbar_wait((lc & 1) ? bar1 : bar0, (lc >> 1) & 1);
+  // one decision for the whole CTA: the tensor-memory loads below are warp-collective
+  const bool ok = __syncthreads_and(done ? 1 : 0) && lc == nchunks - 1;
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
+  const int px = x0 + warp * 32 + lane;
+  if (ok) {
+#pragma unroll 1
+    for (int r = 0; r < T5_R; ++r) {
+      const int y = y0 + r;
+#pragma unroll 1
+      for (int c0 = 0; c0 < N; c0 += 32) {
+        uint32_t v32[32];
+        const unsigned taddr = tmem + ((unsigned)(warp * 32) << 16) + (unsigned)(r * N + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,"
+            "%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+            : "=r"(v32[0]), "=r"(v32[1]), "=r"(v32[2]), "=r"(v32[3]), "=r"(v32[4]), "=r"(v32[5]), "=r"(v32[6]),
+              "=r"(v32[7]), "=r"(v32[8]), "=r"(v32[9]), "=r"(v32[10]), "=r"(v32[11]), "=r"(v32[12]), "=r"(v32[13]),
+              "=r"(v32[14]), "=r"(v32[15]), "=r"(v32[16]), "=r"(v32[17]), "=r"(v32[18]), "=r"(v32[19]),
+              "=r"(v32[20]), "=r"(v32[21]), "=r"(v32[22]), "=r"(v32[23]), "=r"(v32[24]), "=r"(v32[25]),
+              "=r"(v32[26]), "=r"(v32[27]), "=r"(v32[28]), "=r"(v32[29]), "=r"(v32[30]), "=r"(v32[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        if (px < a.W && y < a.H) {
+          const long long p = ((long long)b * a.H + y) * a.W + px;
+#pragma unroll
+          for (int j = 0; j < 32; j += 8) {
+            float v[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+              v[e] = __uint_as_float(v32[j + e]) + (a.bias ? a.bias[c0 + j + e] : 0.f);
+              if (a.relu) v[e] = fmaxf(v[e], 0.f);
+            }
+            if (a.y) {
+              uint4 o;
+              __nv_bfloat162* h2 = reinterpret_cast<__nv_bfloat162*>(&o);
+#pragma unroll
+              for (int e = 0; e < 4; ++e) h2[e] = __floats2bfloat162_rn(v[2 * e], v[2 * e + 1]);
+              *reinterpret_cast<uint4*>(a.y + p * a.cout + c0 + j) = o;
+            }
+            if (a.yf) {
+              float4* f = reinterpret_cast<float4*>(a.yf + p * a.cout + c0 + j);
+              f[0] = make_float4(v[0], v[1], v[2], v[3]);
+              f[1] = make_float4(v[4], v[5], v[6], v[7]);
+            }
+          }
+        }
+      }
+    }
+  }
+  if (tid == 0 && !ok && !failed) atomicAdd(&g_conv5_timeouts, 1u);
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::);
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(Cfg::cols));
 }
 
 // ------------------------------------------------------------------------------------------- conv weight gradient
@@ -653,8 +884,30 @@ void conv2_launch(const ConvArgs& a, cudaStream_t st) {
   k_conv2<BN><<<g, 256, smem, st>>>(a);
 }
 
-// Output-channel tile matched to cout (cout > 128 in two tiles: 224 -> 112, 160 -> 80).
+template <int N>
+void conv5_launch(const ConvArgs& a, cudaStream_t st) {
+  constexpr size_t smem = Conv5Cfg<N>::smem;
+  static_assert(smem <= 227 * 1024, "tcgen05 convolution tile exceeds shared memory");
+  ck(cudaFuncSetAttribute(k_conv5<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "conv smem");
+  constexpr int R = Conv5Cfg<N>::R;
+  const long long ctas = (long long)a.B * ((a.H + R - 1) / R) * ((a.W + T5_PX - 1) / T5_PX);
+  k_conv5<N><<<(unsigned)ctas, 128, smem, st>>>(a);
+}
+
+// 0: tcgen05 for cout in {64, 96, 128} (on B200 the 128 × 32 tile of cout = 32 is faster on mma.sync), 1: mma.sync
+// only, 2: tcgen05 for every cout in {32, 64, 96, 128}
+int g_conv_path = 0;
+
+// cout in {32, 64, 96, 128}: tcgen05 (k_conv5); otherwise mma.sync (k_conv2) with the output-channel tile matched to
+// cout (cout > 128 in two tiles: 224 -> 112, 160 -> 80).
 void conv_launch(const ConvArgs& a, cudaStream_t st) {
+  if (g_conv_path == 2 || (g_conv_path == 0 && a.cout >= 64)) switch (a.cout) {
+      case 32: return conv5_launch<32>(a, st);
+      case 64: return conv5_launch<64>(a, st);
+      case 96: return conv5_launch<96>(a, st);
+      case 128: return conv5_launch<128>(a, st);
+      default: break;
+    }
   switch (a.cout) {
     case 8: return conv2_launch<8>(a, st);
     case 16: return conv2_launch<16>(a, st);
@@ -981,6 +1234,34 @@ void ps_net_destroy(ps_net* pn) {
 }
 
 const char* ps_net_last_error(const ps_net* pn) { return pn ? pn->n.err.c_str() : "net is NULL"; }
+
+int ps_net_set_conv_path(int path) {
+  if (path < 0 || path > 2) return PS_EINVAL;
+  g_conv_path = path;
+  return PS_OK;
+}
+
+int ps_net_conv_timeouts(int device, uint32_t* count, int reset) {
+  if (!count) return PS_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  unsigned c = 0;
+  if (cudaMemcpyFromSymbol(&c, g_conv5_timeouts, sizeof c) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ECUDA;
+  }
+  *count = c;
+  if (reset) {
+    const unsigned z = 0;
+    if (cudaMemcpyToSymbol(g_conv5_timeouts, &z, sizeof z) != cudaSuccess) {
+      cudaGetLastError();
+      return PS_ECUDA;
+    }
+  }
+  return PS_OK;
+}
 uint64_t ps_net_num_params(const ps_net* pn) { return pn ? (uint64_t)pn->n.nparam : 0; }
 uint32_t ps_net_step(const ps_net* pn) { return pn ? (uint32_t)pn->n.step : 0; }
 

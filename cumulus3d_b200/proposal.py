@@ -134,6 +134,23 @@ class ProposalNet:
             pass
 
 
+def set_conv_path(path: str) -> None:
+    """'auto' (default: tcgen05 for cout >= 64, mma.sync otherwise), 'mma' (mma.sync only) or 'tcgen05' (tcgen05 for
+    every cout in {32, 64, 96, 128})."""
+    rc = _lib.engine().ps_net_set_conv_path({"auto": 0, "mma": 1, "tcgen05": 2}[path])
+    if rc != _lib.PS_OK:
+        raise _lib.PsError(rc, "ps_net_set_conv_path failed")
+
+
+def conv_timeouts(device: int = 0, reset: bool = False) -> int:
+    """Expired bounded waits of the tcgen05 convolution on `device` (0 when every result is valid)."""
+    c = C.c_uint32()
+    rc = _lib.engine().ps_net_conv_timeouts(device, C.byref(c), int(reset))
+    if rc != _lib.PS_OK:
+        raise _lib.PsError(rc, "ps_net_conv_timeouts failed")
+    return int(c.value)
+
+
 def conv_check(x: np.ndarray, w: np.ndarray, dy: np.ndarray, device: int = 0):
     """One convolution forward / data gradient / weight gradient through the network's kernels (host buffers).
     x (B, H, W, cin) and dy (B, H, W, cout) uint16 bf16 bits; w (cout, 9, cin) f32."""

@@ -346,6 +346,12 @@ int ps_net_forward(ps_net* net, const void* input, uint32_t batch, uint32_t heig
 int ps_net_train_step(ps_net* net, const void* input, const float* labels, uint32_t batch, uint32_t height,
                       uint32_t width, float depth_min, float depth_max, float lr, float weight_decay, float* loss,
                       float* grad_out);
+/* Convolution kernels of every net in the process: 0 (default) = tcgen05 (5th-generation tensor cores,
+ * tensor-memory accumulators) for cout in {64, 96, 128} and mma.sync otherwise; 1 = mma.sync only; 2 = tcgen05 for
+ * every cout in {32, 64, 96, 128}. */
+int ps_net_set_conv_path(int path);
+/* Bounded waits of the tcgen05 convolution that expired on `device` (its results are then invalid); reset clears. */
+int ps_net_conv_timeouts(int device, uint32_t* count, int reset);
 /* One 3×3 convolution (no bias) on host buffers through the network's kernels, for gradient checks: y = conv(x, w),
  * dx = conv(dy, flipped wᵀ), dw = Σ dy ⊗ im2col(x).  x, dy: bf16 bits NHWC; w f32 [cout][9][cin] (rounded to bf16);
  * cin and cout multiples of 8. */

@@ -22,8 +22,13 @@ def _bf16(rng, shape, lo=-1.0, hi=1.0):
     return O.bf16_bits(rng.uniform(lo, hi, shape))
 
 
-@pytest.mark.parametrize("shape", [(2, 9, 13, 48, 32), (1, 8, 8, 32, 8), (1, 12, 20, 224, 96), (3, 5, 7, 16, 64)])
-def test_conv_kernels_match_fp64(shape):
+@pytest.mark.parametrize("path", ["tcgen05", "mma"])
+@pytest.mark.parametrize("shape", [(2, 9, 13, 48, 32), (1, 8, 8, 32, 8), (1, 12, 20, 224, 96), (3, 5, 7, 16, 64),
+                                   (1, 4, 300, 128, 128)])
+def test_conv_kernels_match_fp64(shape, path):
+    """Forward (tcgen05 for cout in {32, 64, 96, 128}, else mma.sync; or mma.sync only), data and weight gradients."""
+    proposal.set_conv_path(path)
+    proposal.conv_timeouts(reset=True)
     b, h, w, ci, co = shape
     rng = np.random.default_rng(sum(shape))
     x = _bf16(rng, (b, h, w, ci))
@@ -36,6 +41,8 @@ def test_conv_kernels_match_fp64(shape):
     assert np.abs(y - y_ref).max() <= 1e-5 * np.abs(y_ref).max()
     assert np.abs(dx - dx_ref).max() <= 1e-5 * np.abs(dx_ref).max()
     assert np.abs(dw - dw_ref).max() <= 1e-4 * np.abs(dw_ref).max()
+    assert proposal.conv_timeouts() == 0
+    proposal.set_conv_path("auto")
 
 
 def _labels(rng, b, h, w, dr=(25.0, 60.0)):

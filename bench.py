@@ -434,7 +434,9 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
         "plain_same_iterations": {"value": round(n / (ms_short / 1e3), 3), "ms_per_step": round(ms_short, 2),
                                   "agree_with_plain": agree(short_depth), "fused_points": short_fused,
                                   "coverage": round(float((short_depth > 0).mean()), 4)},
-        "net_roofline": {"bound": "tensor", "kernel": "proposal network forward (12 conv layers, mma.sync bf16)",
+        "net_roofline": {"bound": "tensor", "kernel": "proposal network forward (12 conv layers, bf16; "
+                         + {"auto": "tcgen05 for 64-128 output channels, mma.sync for 32",
+                            "mma": "mma.sync only", "tcgen05": "tcgen05 only"}[args.conv_path] + ")",
                          "achieved": round(achieved, 2), "peak": bf16_peak, "unit": "TFLOP/s",
                          "frac": round(achieved / bf16_peak, 4), "peak_source": "MEASURED_PEAKS.json bf16_tflops "
                          "(measured)" if "bf16_tflops" in peaks else "fallback 1590",

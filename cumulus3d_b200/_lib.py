@@ -188,6 +188,7 @@ SIGNATURES = {
                                     C.c_float, C.c_float, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
     "ps_net_set_conv_path": (C.c_int, [C.c_int]),
     "ps_net_conv_timeouts": (C.c_int, [C.c_int, C.POINTER(C.c_uint32), C.c_int]),
+    "ps_net_test_stall_convolutions": (C.c_int, [C.c_int, C.c_int]),
     "ps_net_conv_check": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32,
                                     C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]),
     "ps_sweep_volume": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32]),

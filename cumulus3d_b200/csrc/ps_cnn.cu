@@ -220,8 +220,10 @@ __global__ void __launch_bounds__(256) k_conv2(ConvArgs a) {
 // kernel counts it in g_conv5_timeouts and skips the remaining work (the host reports invalid results); every CTA frees
 // its tensor memory before it exits.
 constexpr int T5_PX = 128, T5_ROWPX = T5_PX + 2;  // pixels per row segment, staged pixels per row
-constexpr long long T5_SPIN = 1ll << 20;                     // bound on mbarrier polls (a chunk takes microseconds)
+constexpr unsigned long long T5_WAIT_NS = 200000000ull;     // bound on one mbarrier wait (a chunk takes microseconds)
+constexpr long long T5_SPIN = 1ll << 24;                     // and on its polls
 __device__ unsigned int g_conv5_timeouts = 0;
+__device__ int g_conv5_stall = 0;  // failure test: the issuing thread commits nothing, so the bounded waits run out
 
 template <int N>
 struct Conv5Cfg {
@@ -247,9 +249,16 @@ __device__ __forceinline__ uint64_t umma_desc(unsigned addr, unsigned lbo, unsig
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count));
 }
-// Waits for the completion of the phase with the given parity; false if the bound expired.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+// Waits for the completion of the phase with the given parity; false once 200 ms (or 2^24 polls) have passed.
 __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  const unsigned long long t0 = global_ns();
   for (long long i = 0; i < T5_SPIN; ++i) {
+    if ((i & 255) == 255 && global_ns() - t0 > T5_WAIT_NS) return false;
     unsigned done;
     asm volatile(
         "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
@@ -345,7 +354,7 @@ __global__ void __launch_bounds__(128, 1) k_conv5(ConvArgs a) {
     }
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // cp.async data -> tensor-core operand reads
     __syncthreads();
-    if (tid == 0 && !*fail_flag) {
+    if (tid == 0 && !*fail_flag && !*(volatile int*)&g_conv5_stall) {
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::);
       const unsigned ib = smem_u32(in_s + (size_t)st * Cfg::in_bytes);
       const unsigned wb = smem_u32(w_s + (size_t)st * Cfg::w_bytes);
@@ -1145,6 +1154,20 @@ int forward_on_stream(ps_net* pn, const void* in, int B, int H, int W, float* ou
   return rc;
 }
 
+int conv_health(std::string* err) {
+  unsigned c = 0;
+  if (cudaMemcpyFromSymbol(&c, g_conv5_timeouts, sizeof c) != cudaSuccess) {
+    cudaGetLastError();
+    if (err) *err = "cannot read the tensor-core convolution status";
+    return PS_ECUDA;
+  }
+  if (c) {
+    if (err) *err = std::to_string(c) + " tensor-core convolution wait(s) expired: network outputs are invalid";
+    return PS_ETIMEOUT;
+  }
+  return PS_OK;
+}
+
 cudaError_t launch_decode(const float* o, int Wp, int H, int W, float4* planes, float* conf, float inv_near,
                           float inv_far, float thr, const float* k, unsigned long long* count, cudaStream_t st) {
   dim3 b(32, 8), g((W + 31) / 32, (H + 7) / 8);
@@ -1241,6 +1264,19 @@ int ps_net_set_conv_path(int path) {
   return PS_OK;
 }
 
+int ps_net_test_stall_convolutions(int device, int on) {
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  const int v = on ? 1 : 0;
+  if (cudaMemcpyToSymbol(g_conv5_stall, &v, sizeof v) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ECUDA;
+  }
+  return PS_OK;
+}
+
 int ps_net_conv_timeouts(int device, uint32_t* count, int reset) {
   if (!count) return PS_EINVAL;
   if (cudaSetDevice(device) != cudaSuccess) {
@@ -1324,6 +1360,9 @@ int ps_net_train_step(ps_net* pn, const void* input, const float* labels, uint32
     ck(cudaMemcpyAsync(sv, n.stats, 8, cudaMemcpyDeviceToHost, st), "loss");
     ck(cudaStreamSynchronize(st), "sync");
     if (loss_out) *loss_out = sv[1] > 0.f ? sv[0] / sv[1] : 0.f;
+    std::string e;
+    const int h = conv_health(&e);
+    if (h != PS_OK) throw Fail{h, e};
   });
 }
 
@@ -1338,7 +1377,12 @@ int ps_net_forward(ps_net* pn, const void* input, uint32_t B, uint32_t H, uint32
     a.o = out;
     forward(n, a, B, H, W, st);
     end_use(n, st);
-    if (!stream) ck(cudaStreamSynchronize(st), "sync");
+    if (!stream) {
+      ck(cudaStreamSynchronize(st), "sync");
+      std::string e;
+      const int h = conv_health(&e);
+      if (h != PS_OK) throw Fail{h, e};
+    }
   });
 }
 

@@ -14,6 +14,9 @@ int forward_on_stream(ps_net* net, const void* in, int B, int H, int W, float* o
 // Adds the number of proposed pixels to *count when count is not null.
 cudaError_t launch_decode(const float* o, int Wp, int H, int W, float4* planes, float* conf, float inv_near,
                           float inv_far, float thr, const float* k, unsigned long long* count, cudaStream_t st);
+// PS_ETIMEOUT (with a message) when a bounded wait of the tensor-core convolution expired on the current device since
+// the counter was last cleared: network outputs computed since then are invalid.  Reads device memory (synchronous).
+int conv_health(std::string* err);
 // Kernel launches of one inference forward pass (12 convolutions, 3 poolings; upsampling and concatenation are
 // fused into the convolutions' input loads).
 constexpr int kForwardLaunches = 15;

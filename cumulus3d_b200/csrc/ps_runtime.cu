@@ -1618,6 +1618,9 @@ int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views
       cuda_ok(cudaMemcpyAsync(&c, s->pcount, sizeof c, cudaMemcpyDeviceToHost, s->st), "read proposal count");
       sync(s);
       *proposed = c;
+      std::string e;
+      const int h = ps_cnn::conv_health(&e);
+      if (h != PS_OK) fail(h, "proposal network: " + e);
     }
   });
 }

@@ -352,6 +352,9 @@ int ps_net_train_step(ps_net* net, const void* input, const float* labels, uint3
 int ps_net_set_conv_path(int path);
 /* Bounded waits of the tcgen05 convolution that expired on `device` (its results are then invalid); reset clears. */
 int ps_net_conv_timeouts(int device, uint32_t* count, int reset);
+/* Failure test of the bounded waits (on = 1): the tensor-core convolution's issuing thread stops committing work, so
+ * its waits expire, it records the failure and returns; clear with on = 0 and reset the counter afterwards. */
+int ps_net_test_stall_convolutions(int device, int on);
 /* One 3×3 convolution (no bias) on host buffers through the network's kernels, for gradient checks: y = conv(x, w),
  * dx = conv(dy, flipped wᵀ), dw = Σ dy ⊗ im2col(x).  x, dy: bf16 bits NHWC; w f32 [cout][9][cin] (rounded to bf16);
  * cin and cout multiples of 8. */
@@ -368,7 +371,8 @@ int ps_sweep_volume(ps_session* s, uint32_t level, uint32_t view, void* out, uin
 int ps_set_sweep_normals(ps_session* s, const float* normals);
 /* Sweep + network + decode for `views` at `level`: stores each view's proposal (planes with d = 0 where the
  * confidence is below conf_threshold) in the session for a later PS_INIT_PROPOSAL run start.  `proposed` (may be
- * NULL; then asynchronous) receives the number of proposed pixels. */
+ * NULL; then asynchronous) receives the number of proposed pixels; with it the call also fails with PS_ETIMEOUT if a
+ * bounded wait of the tensor-core convolution expired (ps_net_conv_timeouts). */
 int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views, size_t n, float conf_threshold,
                uint64_t* proposed);
 /* Caller-supplied proposals (host, 4·w·h floats (nx, ny, nz, d), d <= 0 = none) and read-back of the stored ones

@@ -247,3 +247,33 @@ def test_sweep_with_ground_normals_bitwise_vs_oracle():
     be.close()
     np.testing.assert_array_equal(got, oracle.sweep(wl.input, 0, 1, normal=normals[1]))
     assert not np.array_equal(got, oracle.sweep(wl.input, 0, 1))  # and differs from the fronto-parallel sweep
+
+
+def test_tensor_core_wait_expiry_is_reported_and_recoverable():
+    """The tcgen05 convolution's bounded waits: with commits withheld (test switch) the kernel returns, counts the
+    expiry, and a blocking forward reports PS_ETIMEOUT; afterwards the same context computes correct results."""
+    lib = _lib.engine()
+    rng = np.random.default_rng(3)
+    x = _bf16(rng, (1, 4, 40, 128))  # 4 input chunks: the stage-reuse wait runs
+    dy = _bf16(rng, (1, 4, 40, 64))
+    wt = rng.uniform(-0.3, 0.3, (64, 9, 128)).astype(np.float32)
+    proposal.conv_timeouts(reset=True)
+    assert lib.ps_net_test_stall_convolutions(0, 1) == _lib.PS_OK
+    try:
+        proposal.conv_check(x, wt, dy)  # returns (results invalid) instead of hanging
+        assert proposal.conv_timeouts() > 0
+        net = proposal.ProposalNet(0, seed=4)
+        xin = torch.zeros((1, 16, 16, 48), dtype=torch.int16, device="cuda")
+        out = torch.empty((1, 16, 16, 8), dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        with pytest.raises(_lib.PsError) as e:
+            net.forward(xin, out)
+        assert e.value.code == _lib.PS_ETIMEOUT
+        net.close()
+    finally:
+        assert lib.ps_net_test_stall_convolutions(0, 0) == _lib.PS_OK
+        proposal.conv_timeouts(reset=True)
+    y, _, _ = proposal.conv_check(x, wt, dy)
+    y_ref = O.conv(O.from_bf16_bits(x), O.bf16_round(wt))
+    assert np.abs(y - y_ref).max() <= 1e-5 * np.abs(y_ref).max()
+    assert proposal.conv_timeouts() == 0

@@ -120,13 +120,22 @@ __device__ __forceinline__ float src_sample(const float* __restrict__ img, int p
   float bot = fmaf(ax, p11 - p01, p01);
   return fmaf(ay, bot - top, top);
 }
-// Same sample through the texture unit: one gather at the exact integer corner (x0+1, y0+1) of the 2×2 footprint
-// returns its four texels (border addressing gives 0 outside the image); the bilinear arithmetic is unchanged, so
-// the result has the same bits as src_sample.  Gather order: (T[x0,y1], T[x1,y1], T[x1,y0], T[x0,y0]).
+// Same sample through the texture unit: a gather at the exact integer coordinate (x0, y0) selects the footprint
+// (x0-1 .. x0, y0-1 .. y0), and the texel offset (+1, +1) of the tld4 instruction moves it onto (x0 .. x0+1,
+// y0 .. y0+1), so the four texels come back without two coordinate additions per tap (border addressing gives 0
+// outside the image).  The bilinear arithmetic is unchanged, so the result has the same bits as src_sample.
+// Gather order: (T[x0,y1], T[x1,y1], T[x1,y0], T[x0,y0]).
+__device__ __forceinline__ float4 gather_red_offset11(unsigned long long tex, float x, float y) {
+  float4 q;
+  asm("tld4.r.2d.v4.f32.f32 {%0, %1, %2, %3}, [%4, {%5, %6}], {%7, %8};"
+      : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
+      : "l"(tex), "f"(x), "f"(y), "r"(1), "r"(1));
+  return q;
+}
 __device__ __forceinline__ float src_sample_tex(unsigned long long tex, float u, float v) {
   float xf = floorf(u), yf = floorf(v);
   float ax = u - xf, ay = v - yf;
-  const float4 q = tex2Dgather<float4>((cudaTextureObject_t)tex, xf + 1.0f, yf + 1.0f, 0);
+  const float4 q = gather_red_offset11(tex, xf, yf);
   const float p00 = q.w, p10 = q.z, p01 = q.x, p11 = q.y;
   float top = fmaf(ax, p10 - p00, p00);
   float bot = fmaf(ax, p11 - p01, p01);
@@ -226,69 +235,21 @@ __device__ __forceinline__ bool homography(const PsLevel& R, const PsLPair& L, f
 // Parity operation sequence per tap (dx, dy), with sx = x+dx, sy = y+dy:
 //   zz = fma(H6, sx, fma(H7, sy, H8)); if zz > 1e-8: s = sample(fma(H0,sx,fma(H1,sy,H2))·(1/zz), fma(H3,sx,fma(H4,sy,H5))·(1/zz))
 //   ws = w·s; Ss += ws; SSs = fma(ws, s, SSs); IS = fma(ws, Ik, IS)
-template <int WR, int WS, bool CW, int NT, bool TEX = false, int G = 1>
-__device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
-                                          const float* H, int x, int y, int& nwin) {
-  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
-  const int wn = (2 * wr) / ws + 1;
-  const float fx = (float)x, fy = (float)y;
-  float z = fmaf(H[6], fx, fmaf(H[7], fy, H[8]));
-  if (!(z > 1e-8f)) return 2.0f;
-  float iz = m_rcp(z);
-  float u = fmaf(H[0], fx, fmaf(H[1], fy, H[2])) * iz;
-  float v = fmaf(H[3], fx, fmaf(H[4], fy, H[5])) * iz;
+//
+// Prologue (patchmatch.cu:251-262): the window centre must project in front of the source camera and inside the
+// image, and the reference window must have variance; otherwise the cost is 2 and no window is evaluated.
+__device__ __forceinline__ bool ncc_begin(const RefStats& rs, const PsLevel& S, const float* H, float fx, float fy) {
+  const float z = fmaf(H[6], fx, fmaf(H[7], fy, H[8]));
+  if (!(z > 1e-8f)) return false;
+  const float iz = m_rcp(z);
+  const float u = fmaf(H[0], fx, fmaf(H[1], fy, H[2])) * iz;
+  const float v = fmaf(H[3], fx, fmaf(H[4], fy, H[5])) * iz;
   const float wf = (float)S.w, hf = (float)S.h;
-  if (!(u >= 0.f && v >= 0.f && u <= wf - 1.0f && v <= hf - 1.0f)) return 2.0f;
-  if (rs.var < 1e-5f) return 2.0f;
-  nwin++;
-  const float* __restrict__ img = S.img;
-  const unsigned long long tex = S.tex;
-  const int pitch = S.pitch;
-  float Ss[2] = {0.f, 0.f}, SSs[2] = {0.f, 0.f}, IS[2] = {0.f, 0.f};
-#pragma unroll 1
-  for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
-    const int dy = -wr + a * ws;
-    const int pa = G == 2 ? 0 : (a & 1);
-    const float sy = fy + (float)dy;
-    const float rx = fmaf(H[1], sy, H[2]);
-    const float ry = fmaf(H[4], sy, H[5]);
-    const float rz = fmaf(H[7], sy, H[8]);
-    const float* trow = rw.t + dy * rw.tw;
-    const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
-    auto tap = [&](int b) {
-      const int dx = -wr + b * ws;
-      const float sx = fx + (float)dx;
-      const float ik = trow[dx];
-      float w;
-      if (CW) {
-        w = wrow[b * NT];
-      } else {
-        float d = rs.ic - ik;
-        w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
-      }
-      // Branch-free tap: behind the source camera (zz <= 1e-8) the sample is 0; the reciprocal is replaced by 0 there
-      // so the (discarded) fetch coordinates stay finite, and every tap's fetch can be issued ahead of its use.
-      const float zz = fmaf(H[6], sx, rz);
-      const bool front = zz > 1e-8f;
-      const float izz = front ? m_rcp(zz) : 0.0f;
-      float sv;
-      if constexpr (TEX) sv = src_sample_tex(tex, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
-      else sv = src_sample(img, pitch, wf, hf, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
-      sv = front ? sv : 0.0f;
-      const float wsv = w * sv;
-      Ss[pa] = Ss[pa] + wsv;
-      SSs[pa] = fmaf(wsv, sv, SSs[pa]);
-      IS[pa] = fmaf(wsv, ik, IS[pa]);
-    };
-    if constexpr (WR != 0) {
-#pragma unroll
-      for (int b = 0; b < (2 * WR) / WS + 1; ++b) tap(b);
-    } else {
-#pragma unroll 1
-      for (int b = 0; b < wn; ++b) tap(b);
-    }
-  }
-  const float Sst = pair_total<G>(rw, Ss), SSst = pair_total<G>(rw, SSs), ISt = pair_total<G>(rw, IS);
+  if (!(u >= 0.f && v >= 0.f && u <= wf - 1.0f && v <= hf - 1.0f)) return false;
+  return !(rs.var < 1e-5f);
+}
+// Epilogue (patchmatch.cu:280-289) from the window totals.
+__device__ __forceinline__ float ncc_finish(const RefStats& rs, float Sst, float SSst, float ISt) {
   float iW = 1.0f / rs.W;
   float mus = Sst * iW;
   float vars = SSst * iW - mus * mus;
@@ -300,6 +261,110 @@ __device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, cons
   float c = 1.0f - cov / sqrtf(rs.var * vars);
 #endif
   return fminf(fmaxf(c, 0.0f), 2.0f);
+}
+
+// Window sums over the taps (patchmatch.cu:263-279) and the cost; the prologue must have passed.
+//
+// A tap behind the source camera (zz <= 1e-8) samples 0.  The computed zz = fma(H6, sx, fma(H7, sy, H8)) is monotone
+// in sx for a fixed row and, through the correctly rounded inner fma, monotone in sy for a fixed column (each step is
+// a correctly rounded function of an affine expression, and rounding is monotone), so the smallest zz of the window
+// is at one of its four corner taps.  When all four are in front, every tap is, and the taps run without the
+// per-tap test and selects; otherwise a guarded loop handles each tap (the same bits either way).
+template <int WR, int WS, bool CW, int NT, bool TEX, int G>
+__device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
+                                            const float* H, int x, int y) {
+  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
+  const int wn = (2 * wr) / ws + 1;
+  const float fx = (float)x, fy = (float)y;
+  const float wf = (float)S.w, hf = (float)S.h;
+  const float* __restrict__ img = S.img;
+  const unsigned long long tex = S.tex;
+  const int pitch = S.pitch;
+  float Ss[2] = {0.f, 0.f}, SSs[2] = {0.f, 0.f}, IS[2] = {0.f, 0.f};
+  const float sx0 = fx + (float)(-wr), sx1 = fx + (float)wr;
+  const float rz0 = fmaf(H[7], fy + (float)(-wr), H[8]), rz1 = fmaf(H[7], fy + (float)wr, H[8]);
+  const bool all_front = fmaf(H[6], sx0, rz0) > 1e-8f && fmaf(H[6], sx1, rz0) > 1e-8f &&
+                         fmaf(H[6], sx0, rz1) > 1e-8f && fmaf(H[6], sx1, rz1) > 1e-8f;
+  auto sample = [&](float uf, float vf) {
+    if constexpr (TEX) return src_sample_tex(tex, uf, vf);
+    else return src_sample(img, pitch, wf, hf, uf, vf);
+  };
+  auto accumulate = [&](int pa, float w, float sv, float ik) {
+    const float wsv = w * sv;
+    Ss[pa] = Ss[pa] + wsv;
+    SSs[pa] = fmaf(wsv, sv, SSs[pa]);
+    IS[pa] = fmaf(wsv, ik, IS[pa]);
+  };
+  auto weight = [&](const float* wrow, int b, int dx, int dy, float ik) {
+    if constexpr (CW) {
+      return wrow[b * NT];
+    } else {
+      const float d = rs.ic - ik;
+      return m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
+    }
+  };
+  if (all_front) {
+#pragma unroll 1
+    for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
+      const int dy = -wr + a * ws;
+      const int pa = G == 2 ? 0 : (a & 1);
+      const float sy = fy + (float)dy;
+      const float rx = fmaf(H[1], sy, H[2]);
+      const float ry = fmaf(H[4], sy, H[5]);
+      const float rz = fmaf(H[7], sy, H[8]);
+      const float* trow = rw.t + dy * rw.tw;
+      const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+      auto tap = [&](int b) {
+        const int dx = -wr + b * ws;
+        const float sx = fx + (float)dx;
+        const float ik = trow[dx];
+        const float w = weight(wrow, b, dx, dy, ik);
+        const float izz = m_rcp(fmaf(H[6], sx, rz));
+        accumulate(pa, w, sample(fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz), ik);
+      };
+      if constexpr (WR != 0) {
+#pragma unroll
+        for (int b = 0; b < (2 * WR) / WS + 1; ++b) tap(b);
+      } else {
+#pragma unroll 1
+        for (int b = 0; b < wn; ++b) tap(b);
+      }
+    }
+  } else {
+#pragma unroll 1
+    for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
+      const int dy = -wr + a * ws;
+      const int pa = G == 2 ? 0 : (a & 1);
+      const float sy = fy + (float)dy;
+      const float rx = fmaf(H[1], sy, H[2]);
+      const float ry = fmaf(H[4], sy, H[5]);
+      const float rz = fmaf(H[7], sy, H[8]);
+      const float* trow = rw.t + dy * rw.tw;
+      const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+#pragma unroll 1
+      for (int b = 0; b < wn; ++b) {
+        const int dx = -wr + b * ws;
+        const float sx = fx + (float)dx;
+        const float ik = trow[dx];
+        const float w = weight(wrow, b, dx, dy, ik);
+        // the reciprocal is replaced by 0 behind the camera so the discarded fetch coordinates stay finite
+        const float zz = fmaf(H[6], sx, rz);
+        const bool front = zz > 1e-8f;
+        const float izz = front ? m_rcp(zz) : 0.0f;
+        const float sv = sample(fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+        accumulate(pa, w, front ? sv : 0.0f, ik);
+      }
+    }
+  }
+  return ncc_finish(rs, pair_total<G>(rw, Ss), pair_total<G>(rw, SSs), pair_total<G>(rw, IS));
+}
+
+template <int WR, int WS, bool CW, int NT, bool TEX = false, int G = 1>
+__device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
+                                          const float* H, int x, int y, int& nwin) {
+  if (!ncc_begin(rs, S, H, (float)x, (float)y)) return 2.0f;
+  nwin++;
+  return ncc_window<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y);
 }
 
 // Forward/backward reprojection error through the source snapshot (patchmatch.cu:292-314); INF on failure.
@@ -562,17 +627,15 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[0], H);
       prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
       if (!(prior > 0.f)) continue;
-      m[0] = ok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.f;
-      gg[0] = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[0].w), P.gmax) : 0.f;
     }
 #pragma unroll 1
-    for (int i = 1; i < 9; ++i) {
+    for (int i = 0; i < 9; ++i) {
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[i], H);
       const float mi = ok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.f;
       const float gi = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[i].w), P.gmax) : 0.f;
 #pragma unroll
-      for (int q = 1; q < 9; ++q)
+      for (int q = 0; q < 9; ++q)
         if (q == i) {
           m[q] = mi;
           gg[q] = gi;
@@ -651,18 +714,20 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
     has_prior = qprior.w > 0.f && dot3(make_float3(qprior.x, qprior.y, qprior.z), ray) < 0.f;
   }
   const int ncand = has_prior ? 7 : 6;
+  auto candidate = [&](int c) {
+    switch (c) {
+      case 0: return make_float4(n0.x, n0.y, n0.z, d_r);
+      case 1: return make_float4(n_r.x, n_r.y, n_r.z, bw);
+      case 2: return make_float4(n_r.x, n_r.y, n_r.z, d_r);
+      case 3: return make_float4(n0.x, n0.y, n0.z, d_p);
+      case 4: return make_float4(n_p.x, n_p.y, n_p.z, bw);
+      case 5: return make_float4(n_p.x, n_p.y, n_p.z, d_p);
+      default: return qprior;
+    }
+  };
 #pragma unroll 1
   for (int c = 0; c < ncand; ++c) {
-    float4 cd;
-    switch (c) {
-      case 0: cd = make_float4(n0.x, n0.y, n0.z, d_r); break;
-      case 1: cd = make_float4(n_r.x, n_r.y, n_r.z, bw); break;
-      case 2: cd = make_float4(n_r.x, n_r.y, n_r.z, d_r); break;
-      case 3: cd = make_float4(n0.x, n0.y, n0.z, d_p); break;
-      case 4: cd = make_float4(n_p.x, n_p.y, n_p.z, bw); break;
-      case 5: cd = make_float4(n_p.x, n_p.y, n_p.z, d_p); break;
-      default: cd = qprior; break;
-    }
+    const float4 cd = candidate(c);
     float cc;
     if (den > 0.f) {
       float nm = 0.f;

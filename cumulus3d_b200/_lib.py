@@ -161,6 +161,7 @@ SIGNATURES = {
                                   C.POINTER(C.c_uint64)]),
     "ps_reset_stats": (C.c_int, [_P]),
     "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
+    "ps_check_reciprocal": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     # post-processing, fusion, output
     "ps_post_params_default": (None, [C.POINTER(PostParams)]),
     "ps_fusion_params_default": (None, [C.POINTER(FusionParams)]),

@@ -44,7 +44,14 @@ __device__ __forceinline__ float m_rcp(float x) {
   asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
   return r;
 #else
-  return ps_rcpf(x);  // branch-free Newton reciprocal (ps_fmath.h), the same bits as the oracle
+  // Correctly rounded reciprocal (the oracle's IEEE 1/x): the hardware approximation rcp.approx (within 1 ulp)
+  // refined by one Newton-Raphson correction on the exact FMA residual e = 1 - x*r, r' = r + r*e rounded once
+  // (Markstein's FMA correction).  The result equals the round-to-nearest-even reciprocal for every x in
+  // [2^-126, 2^126), checked exhaustively over all significands by k_rcp_check (ps_check_reciprocal); the kernels
+  // only take reciprocals of projective depths above 1e-8.
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return fmaf(r, fmaf(-x, r, 1.0f), r);
 #endif
 }
 __device__ __forceinline__ float m_exp(float x) {
@@ -1178,6 +1185,20 @@ __global__ void k_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const dou
   out[idx] = o;
 }
 
+// Exhaustive check of m_rcp against the correctly rounded reciprocal (__frcp_rn): x = (1 + i/2^23)·2^e for every
+// significand i (blockIdx.x·256 + threadIdx.x < 2^23) and exponent e = e_lo + blockIdx.y.  Counts mismatches and keeps
+// the first 8 arguments that differ.
+__global__ void __launch_bounds__(256) k_rcp_check(int e_lo, unsigned long long* bad, unsigned* first) {
+  const unsigned i = blockIdx.x * 256u + threadIdx.x;
+  if (i >= (1u << 23)) return;
+  const unsigned bits = ((unsigned)(127 + e_lo + (int)blockIdx.y) << 23) | i;
+  const float x = __uint_as_float(bits);
+  if (__float_as_uint(m_rcp(x)) != __float_as_uint(__frcp_rn(x))) {
+    const unsigned long long k = atomicAdd(bad, 1ull);
+    if (k < 8) first[k] = bits;
+  }
+}
+
 // FP32 throughput probe: 8 independent FFMA chains per thread, register resident.
 __global__ void __launch_bounds__(256) k_fp32_probe(float* out, int iters, float a, float b) {
   float v[8];
@@ -1358,6 +1379,12 @@ cudaError_t launch_restore(const PsRun& P, const float4* up, const float* cinit,
 
 // Module constants (propagation offsets); called at session begin, outside any stream capture.
 cudaError_t prepare() { return init_constants(); }
+
+cudaError_t launch_rcp_check(int e_lo, int e_hi, unsigned long long* bad, unsigned* first, cudaStream_t st) {
+  if (e_lo < -126 || e_hi > 127 || e_lo > e_hi) return cudaErrorInvalidValue;
+  k_rcp_check<<<dim3((1u << 23) / 256, e_hi - e_lo + 1), 256, 0, st>>>(e_lo, bad, first);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st) {
   k_fp32_probe<<<blocks, 256, 0, st>>>(out, iters, 0.999999f, 1e-7f);

@@ -39,6 +39,7 @@
   cudaError_t launch_sweep(const PsRun& P, bool tex, cudaStream_t st);                                     \
   cudaError_t launch_restore(const PsRun& P, const float4* up, const float* cinit, float thr, cudaStream_t st); \
   cudaError_t launch_fp32_probe(float* out, int blocks, int iters, cudaStream_t st);                       \
+  cudaError_t launch_rcp_check(int e_lo, int e_hi, unsigned long long* bad, unsigned* first, cudaStream_t st); \
   cudaError_t prepare();                                                                                   \
   cudaError_t launch_setup_lpairs(const PsLevel* lv, const PsPair* pairs, const double* pairs64,           \
                                   const int* has64, PsLPair* out, int nviews, int nlevels, cudaStream_t st); \
@@ -2016,6 +2017,33 @@ int ps_reset_stats(ps_session* s) {
     cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     sync(s);
   });
+}
+
+int ps_check_reciprocal(int device, int exp_lo, int exp_hi, uint64_t* mismatches, uint32_t* first_bad) {
+  if (!mismatches || exp_lo < -126 || exp_hi > 127 || exp_lo > exp_hi) return PS_EINVAL;
+  if (cudaSetDevice(device) != cudaSuccess) return PS_ENODEV;
+  unsigned long long* bad = nullptr;
+  unsigned* first = nullptr;
+  int rc = PS_OK;
+  if (cudaMalloc(&bad, sizeof(unsigned long long)) != cudaSuccess || cudaMalloc(&first, 8 * sizeof(unsigned)) != cudaSuccess)
+    rc = PS_ENOMEM;
+  if (rc == PS_OK && (cudaMemset(bad, 0, sizeof(unsigned long long)) != cudaSuccess ||
+                      cudaMemset(first, 0, 8 * sizeof(unsigned)) != cudaSuccess))
+    rc = PS_ECUDA;
+  if (rc == PS_OK && ps_parity::launch_rcp_check(exp_lo, exp_hi, bad, first, 0) != cudaSuccess) rc = PS_ECUDA;
+  unsigned long long h = 0;
+  unsigned f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  if (rc == PS_OK && (cudaMemcpy(&h, bad, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                      cudaMemcpy(f, first, sizeof f, cudaMemcpyDeviceToHost) != cudaSuccess))
+    rc = PS_ECUDA;
+  if (rc == PS_OK) {
+    *mismatches = h;
+    if (first_bad) memcpy(first_bad, f, sizeof f);
+  }
+  cudaFree(bad);
+  cudaFree(first);
+  cudaGetLastError();
+  return rc;
 }
 
 int ps_measure_fp32_peak(int device, double* tflops) {

@@ -465,6 +465,10 @@ int ps_kernel_stats(ps_session* s, uint32_t kind, double* total_ms, uint64_t* la
 int ps_reset_stats(ps_session* s);
 /* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 FLOP) from a register-resident FFMA loop. */
 int ps_measure_fp32_peak(int device, double* tflops);
+/* Self-check of the numerics contract: compares the kernels' reciprocal with the correctly rounded reciprocal for
+ * every binary32 significand at the exponents exp_lo..exp_hi (within -126..127).  *mismatches = the number that
+ * differ; first_bad (may be NULL) receives up to 8 differing arguments as bit patterns. */
+int ps_check_reciprocal(int device, int exp_lo, int exp_hi, uint64_t* mismatches, uint32_t* first_bad);
 
 #ifdef __cplusplus
 }

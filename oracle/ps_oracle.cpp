@@ -19,7 +19,7 @@
 // written as fma(); division and square root are IEEE; exp and sincos are the functions of ps_fmath.h.  The places
 // where the reference leaves the choice to the compiler (contraction, __expf, rsqrtf, the approximate division of
 // its fast-math build, hardware bilinear) are fixed as follows, identically in the engine: the projective
-// reciprocal 1/z of the NCC (centre and taps) is ps_rcpf (Newton, <= 0.5006 ulp); bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
+// reciprocal 1/z of the NCC (centre and taps) is the correctly rounded reciprocal (IEEE division); bilinear sample top = fma(ax, p10-p00, p00), bottom likewise, value =
 // fma(ay, bot-top, top) on unit-range values (8-bit input: the correctly rounded u/255); tap projection z = fma(H6, sx, fma(H7, sy, H8)) (same for
 // the two numerators); window accumulation Ss += w·s, SSs = fma(w·s, s, SSs), IS = fma(w·s, Ik, IS); reference
 // statistics S += w·Ik, SS = fma(w·Ik, Ik, SS); every window sum (W, S, SS, Ss, SSs, IS) is kept as two partial
@@ -57,9 +57,9 @@ inline double mn(double a, double b) { return fmin(a, b); }
 inline float mx(float a, float b) { return fmaxf(a, b); }
 inline double mx(double a, double b) { return fmax(a, b); }
 inline float sq(float a) { return sqrtf(a); }
-// Tap reciprocal: binary32 uses the branch-free Newton reciprocal of ps_fmath.h (the engine's parity sequence);
-// binary64 divides.
-inline float rc(float a) { return ps_rcpf(a); }
+// Tap reciprocal: binary32 is the correctly rounded 1/a (IEEE division; the engine's parity build computes the same
+// value with a hardware approximation and one FMA correction); binary64 divides.
+inline float rc(float a) { return 1.0f / a; }
 inline double rc(double a) { return 1.0 / a; }
 inline double sq(double a) { return sqrt(a); }
 

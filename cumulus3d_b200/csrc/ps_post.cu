@@ -379,6 +379,24 @@ __global__ void k_pyramid(const unsigned char* in, int w, int h, unsigned char* 
   out[(long long)Y * nw + X] = (unsigned char)fminf(fmaxf(roundf(v), 0.0f), 255.0f);
 }
 
+// Reference planes of a session: out[y·pitch + x] = lut[in[y·w + x]] (lut = the correctly rounded u/255 of the host,
+// so the plane has the bits the oracle's plane has).
+__global__ void k_u8_plane(const unsigned char* __restrict__ in, int w, int h, const float* __restrict__ lut,
+                           float* __restrict__ out, int pitch) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)w * h) return;
+  const int y = (int)(i / w), x = (int)(i - (long long)y * w);
+  out[(long long)y * pitch + x] = lut[in[i]];
+}
+
+cudaError_t launch_u8_plane(const unsigned char* in, int w, int h, const float* lut, float* out, int pitch,
+                            cudaStream_t st) {
+  const long long n = (long long)w * h;
+  if (n <= 0) return cudaSuccess;
+  k_u8_plane<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, w, h, lut, out, pitch);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g,
                            cudaStream_t st) {
   const dim3 b(32, 8), gr((w / 2 + 31) / 32, (h / 2 + 7) / 8);

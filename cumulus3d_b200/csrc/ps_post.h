@@ -66,5 +66,8 @@ cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* 
 cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);
 cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g, cudaStream_t st);
+// 8-bit image (w × h, tight rows) -> f32 plane rows of `pitch` floats through a 256-entry table.
+cudaError_t launch_u8_plane(const unsigned char* in, int w, int h, const float* lut, float* out, int pitch,
+                            cudaStream_t st);
 
 }  // namespace ps_post

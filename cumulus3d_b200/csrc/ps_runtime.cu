@@ -109,13 +109,14 @@ struct FusedCloud {
   unsigned short* vis = nullptr;
   unsigned long long* counter = nullptr;
   ps_post::FuseView* views = nullptr;
-  void release() {
-    cudaFree(pos);
-    cudaFree(nrm);
-    cudaFree(col);
-    cudaFree(key);
-    cudaFree(nvis);
-    cudaFree(vis);
+  template <typename Free>
+  void release(Free&& free) {
+    free(pos);
+    free(nrm);
+    free(col);
+    free(key);
+    free(nvis);
+    free(vis);
     *this = FusedCloud{counter, views};
   }
   FusedCloud() = default;
@@ -131,6 +132,18 @@ struct ps_backend {
   std::string err;
   std::mutex mu;
   bool busy = false;
+  // Memory kept between sessions (one session at a time): device buffers come from this stream-ordered pool, which
+  // keeps what a session frees for the next one, and the pinned staging buffer passes from session to session.
+  cudaMemPool_t pool = nullptr;
+  void* pin = nullptr;
+  size_t pin_cap = 0;
+  // texture arrays of the previous session, reused by size and format (freeing an array can stall for a long time)
+  struct CachedArray {
+    cudaArray_t a;
+    int w, h;
+    bool u8;
+  };
+  std::vector<CachedArray> arrays;
 };
 
 struct ps_session {
@@ -178,6 +191,7 @@ struct ps_session {
   uint64_t launches = 0;
   size_t img_bytes = 0;
   std::vector<cudaArray_t> arrays;       // texture arrays (PS_TUNE_TEX_GATHER)
+  std::vector<ps_backend::CachedArray> array_keys;  // their sizes and formats, handed back to the backend at the end
   std::vector<cudaTextureObject_t> texs;
   unsigned tuning = 0;
   // profiling
@@ -237,11 +251,20 @@ int guard(ps_session* s, F&& f) {
   }
 }
 
+// Session device memory: from the backend's pool in the session stream's order (plain cudaMalloc when the device
+// offers no pool).  Every use of a buffer is on the session stream.
 template <typename T>
-T* dalloc(size_t n) {
+T* dalloc(ps_session* s, size_t n) {
   void* p = nullptr;
-  cuda_ok(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)), "cudaMalloc");
+  const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  if (s->be && s->be->pool) cuda_ok(cudaMallocFromPoolAsync(&p, bytes, s->be->pool, s->st), "cudaMallocFromPoolAsync");
+  else cuda_ok(cudaMalloc(&p, bytes), "cudaMalloc");
   return (T*)p;
+}
+void dfree(ps_session* s, void* p) {
+  if (!p) return;
+  if (s->be && s->be->pool) cudaFreeAsync(p, s->st);
+  else cudaFree(p);
 }
 
 void* pinned(ps_session* s, size_t bytes) {
@@ -273,12 +296,12 @@ Slot& slot(ps_session* s, int level) {
       tot += (long long)s->W(v, level) * s->H(v, level);
     }
     sl.total = tot;
-    sl.plane = dalloc<float4>(tot);
-    sl.aux = dalloc<float4>(tot);
-    sl.prior = dalloc<float4>(tot);
-    sl.cost = dalloc<float>(tot);
-    sl.bview = dalloc<unsigned char>(tot);
-    sl.count = dalloc<unsigned char>(tot);
+    sl.plane = dalloc<float4>(s, tot);
+    sl.aux = dalloc<float4>(s, tot);
+    sl.prior = dalloc<float4>(s, tot);
+    sl.cost = dalloc<float>(s, tot);
+    sl.bview = dalloc<unsigned char>(s, tot);
+    sl.count = dalloc<unsigned char>(s, tot);
     cuda_ok(cudaMemsetAsync(sl.plane, 0, std::max<long long>(tot, 1) * sizeof(float4), s->st), "memset");
     cuda_ok(cudaMemsetAsync(sl.bview, 255, std::max<long long>(tot, 1), s->st), "memset");
     sl.prior_valid.assign(s->nv, 0);
@@ -425,8 +448,8 @@ void drop_graphs(ps_session* s) {
   collect_events(s);  // finishes the stream and releases the replays' pending events
   for (auto& kv : s->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    cudaFree(kv.second.offsets);
-    for (long long* o : kv.second.level_offsets) cudaFree(o);
+    dfree(s, kv.second.offsets);
+    for (long long* o : kv.second.level_offsets) dfree(s, o);
     for (auto& pd : kv.second.events) {
       cudaEventDestroy(pd.a);
       cudaEventDestroy(pd.b);
@@ -438,10 +461,10 @@ void drop_graphs(ps_session* s) {
 // Grows the snapshot buffer to `total` floats (captured graphs are dropped first).
 void realloc_snapshot(ps_session* s, size_t total) {
   drop_graphs(s);
-  if (s->snap) cudaFree(s->snap);
+  if (s->snap) dfree(s, s->snap);
   s->snap = nullptr;
   s->snap_cap = 0;
-  s->snap = dalloc<float>(std::max<size_t>(total, 1));
+  s->snap = dalloc<float>(s, std::max<size_t>(total, 1));
   s->snap_cap = total;
 }
 
@@ -655,11 +678,35 @@ int ps_backend_create(int device, const ps_options* opts, ps_backend** out) {
     return PS_EINVAL;
   }
   be->name = std::string("b200(") + prop.name + (be->opts.math_mode == PS_MATH_FAST ? ", fast)" : ", parity)");
+  cudaMemPoolProps pp;
+  memset(&pp, 0, sizeof pp);
+  pp.allocType = cudaMemAllocationTypePinned;
+  pp.handleTypes = cudaMemHandleTypeNone;
+  pp.location.type = cudaMemLocationTypeDevice;
+  pp.location.id = device;
+  if (cudaMemPoolCreate(&be->pool, &pp) == cudaSuccess) {
+    uint64_t keep = UINT64_MAX;  // keep freed memory in the pool until the backend is destroyed
+    if (cudaMemPoolSetAttribute(be->pool, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+      cudaMemPoolDestroy(be->pool);
+      be->pool = nullptr;
+    }
+  } else {
+    be->pool = nullptr;
+  }
+  cudaGetLastError();
   *out = be;
   return PS_OK;
 }
 
-void ps_backend_destroy(ps_backend* be) { delete be; }
+void ps_backend_destroy(ps_backend* be) {
+  if (!be) return;
+  cudaSetDevice(be->device);
+  if (be->pin) cudaFreeHost(be->pin);
+  for (auto& c : be->arrays) cudaFreeArray(c.a);
+  if (be->pool) cudaMemPoolDestroy(be->pool);
+  cudaGetLastError();
+  delete be;
+}
 const char* ps_backend_name(const ps_backend* be) { return be ? be->name.c_str() : ""; }
 const char* ps_backend_last_error(const ps_backend* be) { return be ? be->err.c_str() : "backend is NULL"; }
 const char* ps_last_error(const ps_session* s) { return s ? s->err.c_str() : "session is NULL"; }
@@ -683,6 +730,10 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     return PS_ENOMEM;
   }
   s->be = be;
+  s->pin = be->pin;  // pinned staging kept from the backend's previous session
+  s->pin_cap = be->pin_cap;
+  be->pin = nullptr;
+  be->pin_cap = 0;
   int rc = guard(s, [&] {
     const ps_pm_params& pm = in->pm;
     if (pm.window_radius < 1 || pm.window_radius > 20 || pm.window_step < 1 || pm.window_step > 2)
@@ -735,28 +786,61 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     // module constants are set here, outside any stream capture (their copy is synchronous)
     cuda_ok(ps_parity::prepare(), "module constants");
     cuda_ok(ps_fast::prepare(), "module constants");
-    // images: normalised f32 planes with a zero border
-    std::vector<float> host(std::max<size_t>(total, 1), 0.0f);
+    // images: normalised f32 planes with a zero border.  8-bit images travel as bytes through the pinned staging
+    // buffer and are expanded on the device with a table of the correctly rounded u/255 (the oracle's plane values);
+    // f32 images are copied row by row into the bordered plane.
     std::vector<PsLevel> lvh(s->nv * s->nl);
-    s->img = dalloc<float>(total);
+    s->img = dalloc<float>(s, total);
     s->img_bytes = total * sizeof(float);
+    cuda_ok(cudaMemsetAsync(s->img, 0, std::max<size_t>(total, 1) * sizeof(float), s->st), "memset images");
+    size_t u8_total = 0;
+    std::vector<size_t> u8_off(s->nv * s->nl, 0);
+    for (int v = 0; v < s->nv; ++v)
+      for (int l = 0; l < s->nl; ++l) {
+        const ps_level_image& li = in->views[v].levels[l];
+        if (li.format != PS_IMAGE_U8) continue;
+        u8_off[v * s->nl + l] = u8_total;
+        u8_total += round_up((size_t)li.width * li.height, 16);
+      }
+    unsigned char* d8 = nullptr;  // the 8-bit images on the device, then the table
+    if (u8_total) {
+      unsigned char* stage = (unsigned char*)pinned(s, u8_total + 256 * sizeof(float));
+      float* lut = (float*)(stage + u8_total);
+      for (int u = 0; u < 256; ++u) lut[u] = ps_u8_unit((unsigned char)u);
+      std::vector<std::pair<int, int>> u8_images;
+      for (int v = 0; v < s->nv; ++v)
+        for (int l = 0; l < s->nl; ++l)
+          if (in->views[v].levels[l].format == PS_IMAGE_U8) u8_images.push_back({v, l});
+#pragma omp parallel for schedule(dynamic)
+      for (long long k = 0; k < (long long)u8_images.size(); ++k) {
+        const ps_level_image& li = in->views[u8_images[k].first].levels[u8_images[k].second];
+        unsigned char* dst = stage + u8_off[u8_images[k].first * s->nl + u8_images[k].second];
+        const size_t stride = li.stride ? li.stride : li.width;
+        for (uint32_t y = 0; y < li.height; ++y)
+          memcpy(dst + (size_t)y * li.width, (const unsigned char*)li.pixels + y * stride, li.width);
+      }
+      d8 = dalloc<unsigned char>(s, u8_total + 256 * sizeof(float));
+      cuda_ok(cudaMemcpyAsync(d8, stage, u8_total + 256 * sizeof(float), cudaMemcpyHostToDevice, s->st),
+              "upload 8-bit images");
+    }
     for (int v = 0; v < s->nv; ++v)
       for (int l = 0; l < s->nl; ++l) {
         const ps_level_image& li = in->views[v].levels[l];
         const size_t pitch = pitches[v * s->nl + l];
-        float* dst = host.data() + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
-        const size_t stride = li.stride ? li.stride : li.width;
-        for (uint32_t y = 0; y < li.height; ++y) {
-          if (li.format == PS_IMAGE_U8) {
-            const uint8_t* src = (const uint8_t*)li.pixels + y * stride;
-            for (uint32_t x = 0; x < li.width; ++x) dst[y * pitch + x] = ps_u8_unit(src[x]);
-          } else {
-            const float* src = (const float*)li.pixels + y * stride;
-            memcpy(dst + y * pitch, src, li.width * sizeof(float));
-          }
+        float* dst = s->img + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
+        if (li.format == PS_IMAGE_U8) {
+          launched(s,
+                   ps_post::launch_u8_plane(d8 + u8_off[v * s->nl + l], (int)li.width, (int)li.height,
+                                            (const float*)(d8 + u8_total), dst, (int)pitch, s->st),
+                   "image plane kernel");
+        } else {
+          const size_t stride = li.stride ? li.stride : li.width;
+          cuda_ok(cudaMemcpy2DAsync(dst, pitch * sizeof(float), li.pixels, stride * sizeof(float),
+                                    li.width * sizeof(float), li.height, cudaMemcpyHostToDevice, s->st),
+                  "upload image");
         }
         PsLevel& L = lvh[v * s->nl + l];
-        L.img = s->img + offs[v * s->nl + l] + PS_BORDER * pitch + PS_BORDER;
+        L.img = dst;
         L.tex = 0;
         L.w = (int)li.width;
         L.h = (int)li.height;
@@ -767,7 +851,6 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
         L.cx = li.k[2];
         L.cy = li.k[3];
       }
-    cuda_ok(cudaMemcpyAsync(s->img, host.data(), total * sizeof(float), cudaMemcpyHostToDevice, s->st), "upload images");
     if (s->tuning & PS_TUNE_TEX_GATHER) {
       // one gather-capable CUDA array + border-addressed point texture per (view, level).  8-bit images keep 8-bit
       // texels read as normalized floats (the texture unit returns the correctly rounded u/255, the plane's value, for
@@ -780,11 +863,20 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
           const ps_level_image& li = in->views[v].levels[l];
           const bool u8 = li.format == PS_IMAGE_U8;
           cudaArray_t arr = nullptr;
-          cuda_ok(cudaMallocArray(&arr, u8 ? &cd8 : &cdf, L.w, L.h, cudaArrayTextureGather), "cudaMallocArray");
+          auto& cache = be->arrays;
+          for (size_t k = 0; k < cache.size(); ++k)
+            if (cache[k].w == L.w && cache[k].h == L.h && cache[k].u8 == u8) {
+              arr = cache[k].a;
+              cache.erase(cache.begin() + (long)k);
+              break;
+            }
+          if (!arr)
+            cuda_ok(cudaMallocArray(&arr, u8 ? &cd8 : &cdf, L.w, L.h, cudaArrayTextureGather), "cudaMallocArray");
           s->arrays.push_back(arr);
+          s->array_keys.push_back({arr, L.w, L.h, u8});
           if (u8)
-            cuda_ok(cudaMemcpy2DToArray(arr, 0, 0, li.pixels, li.stride ? li.stride : li.width, L.w, L.h,
-                                        cudaMemcpyHostToDevice),
+            cuda_ok(cudaMemcpy2DToArrayAsync(arr, 0, 0, d8 + u8_off[v * s->nl + l], L.w, L.w, L.h,
+                                             cudaMemcpyDeviceToDevice, s->st),
                     "copy texture array");
           else
             cuda_ok(cudaMemcpy2DToArrayAsync(arr, 0, 0, L.img, L.pitch * sizeof(float), L.w * sizeof(float), L.h,
@@ -806,10 +898,14 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
           L.tex = (unsigned long long)t;
         }
     }
-    s->counters = dalloc<unsigned long long>(PS_KERNEL_KINDS);
+    if (d8) {
+      sync(s);  // the pinned staging buffer is reused by the next call
+      dfree(s, d8);
+    }
+    s->counters = dalloc<unsigned long long>(s, PS_KERNEL_KINDS);
     cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     s->lvh = lvh;
-    s->lv = dalloc<PsLevel>(lvh.size());
+    s->lv = dalloc<PsLevel>(s, lvh.size());
     cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
     // pairs, views, FP64 pair tables
     std::vector<PsPair> prh((size_t)std::max(s->nv, 1) * PS_MAXSRC);
@@ -840,21 +936,21 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     s->vdh = vdh;
     s->sweep_n.assign(3 * (size_t)std::max(s->nv, 1), 0.0f);
     for (int v = 0; v < s->nv; ++v) s->sweep_n[3 * v + 2] = -1.0f;
-    s->pairs = dalloc<PsPair>(prh.size());
-    s->views = dalloc<PsView>(vdh.size());
-    s->pairs64 = dalloc<double>(p64.size());
-    s->has64 = dalloc<int>(has64.size());
-    s->lpairs = dalloc<PsLPair>((size_t)std::max(s->nv, 1) * s->nl * PS_MAXSRC);
+    s->pairs = dalloc<PsPair>(s, prh.size());
+    s->views = dalloc<PsView>(s, vdh.size());
+    s->pairs64 = dalloc<double>(s, p64.size());
+    s->has64 = dalloc<int>(s, has64.size());
+    s->lpairs = dalloc<PsLPair>(s, (size_t)std::max(s->nv, 1) * s->nl * PS_MAXSRC);
     cuda_ok(cudaMemcpyAsync(s->pairs, prh.data(), prh.size() * sizeof(PsPair), cudaMemcpyHostToDevice, s->st), "upload pairs");
     cuda_ok(cudaMemcpyAsync(s->views, vdh.data(), vdh.size() * sizeof(PsView), cudaMemcpyHostToDevice, s->st), "upload views");
     cuda_ok(cudaMemcpyAsync(s->pairs64, p64.data(), p64.size() * sizeof(double), cudaMemcpyHostToDevice, s->st), "upload pairs64");
     cuda_ok(cudaMemcpyAsync(s->has64, has64.data(), has64.size() * sizeof(int), cudaMemcpyHostToDevice, s->st), "upload has64");
     launched(s, ps_parity::launch_setup_lpairs(s->lv, s->pairs, s->pairs64, s->has64, s->lpairs, s->nv, s->nl, s->st),
              "homography setup kernel");
-    s->snap_off = dalloc<long long>(std::max(s->nv, 1));
+    s->snap_off = dalloc<long long>(s, std::max(s->nv, 1));
     std::vector<long long> none(std::max(s->nv, 1), -1);
     cuda_ok(cudaMemcpyAsync(s->snap_off, none.data(), none.size() * sizeof(long long), cudaMemcpyHostToDevice, s->st), "upload");
-    s->snap = dalloc<float>(1);
+    s->snap = dalloc<float>(s, 1);
     s->snap_cap = 1;
     s->slots.assign(s->nl, Slot());
     sync(s);
@@ -873,36 +969,41 @@ int ps_end(ps_session* s) {
   if (s->be) cudaSetDevice(s->be->device);
   if (s->st) cudaStreamSynchronize(s->st);
   for (Slot& sl : s->slots) {
-    cudaFree(sl.plane);
-    cudaFree(sl.aux);
-    cudaFree(sl.prior);
-    cudaFree(sl.cost);
-    cudaFree(sl.bview);
-    cudaFree(sl.count);
-    cudaFree(sl.proposal);
-    cudaFree(sl.pconf);
-    cudaFree(sl.spk);
-    cudaFree(sl.marks);
-    cudaFree(sl.cinit);
+    dfree(s, sl.plane);
+    dfree(s, sl.aux);
+    dfree(s, sl.prior);
+    dfree(s, sl.cost);
+    dfree(s, sl.bview);
+    dfree(s, sl.count);
+    dfree(s, sl.proposal);
+    dfree(s, sl.pconf);
+    dfree(s, sl.spk);
+    dfree(s, sl.marks);
+    dfree(s, sl.cinit);
   }
-  s->fused.release();
-  cudaFree(s->fused.counter);
-  cudaFree(s->fused.views);
-  cudaFree(s->netin);
-  cudaFree(s->netout);
-  cudaFree(s->pcount);
-  cudaFree(s->img);
-  cudaFree(s->lv);
-  cudaFree(s->pairs);
-  cudaFree(s->lpairs);
-  cudaFree(s->views);
-  cudaFree(s->pairs64);
-  cudaFree(s->has64);
-  cudaFree(s->snap);
-  cudaFree(s->snap_off);
+  s->fused.release([s](void* q) { dfree(s, q); });
+  dfree(s, s->fused.counter);
+  dfree(s, s->fused.views);
+  dfree(s, s->netin);
+  dfree(s, s->netout);
+  dfree(s, s->pcount);
+  dfree(s, s->img);
+  dfree(s, s->lv);
+  dfree(s, s->pairs);
+  dfree(s, s->lpairs);
+  dfree(s, s->views);
+  dfree(s, s->pairs64);
+  dfree(s, s->has64);
+  dfree(s, s->snap);
+  dfree(s, s->snap_off);
   for (cudaTextureObject_t t : s->texs) cudaDestroyTextureObject(t);
-  for (cudaArray_t a : s->arrays) cudaFreeArray(a);
-  cudaFree(s->counters);
+  if (s->be) {  // arrays no session reused are freed; this session's arrays wait for the next one
+    for (auto& c : s->be->arrays) cudaFreeArray(c.a);
+    s->be->arrays = s->array_keys;
+  } else {
+    for (cudaArray_t a : s->arrays) cudaFreeArray(a);
+  }
+  dfree(s, s->counters);
   for (auto& pd : s->pending) {
     if (pd.persistent) continue;  // destroyed with their graph below
     cudaEventDestroy(pd.a);
@@ -910,14 +1011,21 @@ int ps_end(ps_session* s) {
   }
   for (auto& kv : s->graphs) {
     if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    cudaFree(kv.second.offsets);
-    for (long long* o : kv.second.level_offsets) cudaFree(o);
+    dfree(s, kv.second.offsets);
+    for (long long* o : kv.second.level_offsets) dfree(s, o);
     for (auto& pd : kv.second.events) {
       cudaEventDestroy(pd.a);
       cudaEventDestroy(pd.b);
     }
   }
-  if (s->pin) cudaFreeHost(s->pin);
+  if (s->st) cudaStreamSynchronize(s->st);  // the frees above are stream-ordered
+  if (s->be && s->pin) {
+    if (s->be->pin) cudaFreeHost(s->be->pin);
+    s->be->pin = s->pin;  // the pinned staging buffer stays with the backend for its next session
+    s->be->pin_cap = s->pin_cap;
+  } else if (s->pin) {
+    cudaFreeHost(s->pin);
+  }
   if (s->st) cudaStreamDestroy(s->st);
   cudaGetLastError();
   if (s->be) {
@@ -1334,8 +1442,8 @@ void graph_run(ps_session* s, const std::string& key, bool use_graph, Prep&& pre
   if (it == s->graphs.end()) {
     ps_session::GraphEntry ge;
     auto release = [&] {
-      cudaFree(ge.offsets);
-      for (long long* o : ge.level_offsets) cudaFree(o);
+      dfree(s, ge.offsets);
+      for (long long* o : ge.level_offsets) dfree(s, o);
     };
     try {
       prepare(ge);
@@ -1414,7 +1522,7 @@ long long* view_offsets(ps_session* s, int level, const uint32_t* views, size_t 
   Slot& sl = slot(s, level);
   std::vector<long long> offs(s->nv, -1);
   for (size_t i = 0; i < n; ++i) offs[views[i]] = sl.off[views[i]];
-  long long* d = dalloc<long long>(s->nv);
+  long long* d = dalloc<long long>(s, s->nv);
   cuda_ok(cudaMemcpyAsync(d, offs.data(), s->nv * sizeof(long long), cudaMemcpyHostToDevice, s->st), "upload offsets");
   return d;
 }
@@ -1468,7 +1576,7 @@ int ps_schedule_multiscale(ps_session* s, const uint32_t* views, size_t n, const
     const int top = s->nl - 1;
     for (int l = 0; l < s->nl; ++l) {  // every buffer the launches use exists before any capture
       Slot& sl = slot(s, l);
-      if (l > 0 && !sl.cinit) sl.cinit = dalloc<float>(std::max<long long>(sl.total, 1));
+      if (l > 0 && !sl.cinit) sl.cinit = dalloc<float>(s, std::max<long long>(sl.total, 1));
     }
     long long maxtot = 0;
     for (int l = 0; l < s->nl; ++l) maxtot = std::max(maxtot, s->slots[l].total);
@@ -1499,8 +1607,8 @@ namespace {
 
 void ensure_proposals(ps_session* s, Slot& sl) {
   if (sl.proposal) return;
-  sl.proposal = dalloc<float4>(sl.total);
-  sl.pconf = dalloc<float>(sl.total);
+  sl.proposal = dalloc<float4>(s, sl.total);
+  sl.pconf = dalloc<float>(s, sl.total);
   cuda_ok(cudaMemsetAsync(sl.proposal, 0, std::max<long long>(sl.total, 1) * sizeof(float4), s->st), "memset");
   cuda_ok(cudaMemsetAsync(sl.pconf, 0, std::max<long long>(sl.total, 1) * sizeof(float), s->st), "memset");
   sl.proposal_valid.assign(s->nv, 0);
@@ -1521,10 +1629,10 @@ template <typename T>
 void grow(ps_session* s, T*& buf, size_t& cap, size_t elems) {
   if (elems <= cap) return;
   sync(s);  // the previous user of the buffer has finished
-  cudaFree(buf);
+  dfree(s, buf);
   buf = nullptr;
   cap = 0;
-  buf = dalloc<T>(elems);
+  buf = dalloc<T>(s, elems);
   cap = elems;
 }
 
@@ -1574,7 +1682,7 @@ int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views
     }
     grow(s, s->netin, s->netin_cap, in_need);
     grow(s, s->netout, s->netout_cap, out_need);
-    if (!s->pcount) s->pcount = dalloc<unsigned long long>(1);
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 1);
     cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
     for (size_t i = 0; i < n; ++i) {
       const uint32_t v = views[i];
@@ -1733,8 +1841,8 @@ int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views
     Slot& sl = slot(s, (int)level);
     if (removed) *removed = 0;
     if (!p->remove_speckles || n == 0) return;
-    if (!sl.spk) sl.spk = dalloc<int>((size_t)std::max<long long>(sl.total, 1) * 5);
-    if (!s->pcount) s->pcount = dalloc<unsigned long long>(1);
+    if (!sl.spk) sl.spk = dalloc<int>(s, (size_t)std::max<long long>(sl.total, 1) * 5);
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 1);
     cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
     const size_t T = (size_t)std::max<long long>(sl.total, 1);
     for (auto [a, b] : batches(s, views, n, (int)level)) {
@@ -1807,8 +1915,8 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
       }
     }
     FusedCloud& fc = s->fused;
-    if (!fc.counter) fc.counter = dalloc<unsigned long long>(1);
-    if (!fc.views) fc.views = dalloc<ps_post::FuseView>(std::max(s->nv, 1));
+    if (!fc.counter) fc.counter = dalloc<unsigned long long>(s, 1);
+    if (!fc.views) fc.views = dalloc<ps_post::FuseView>(s, std::max(s->nv, 1));
     cuda_ok(cudaMemcpyAsync(fc.views, fv.data(), fv.size() * sizeof(ps_post::FuseView), cudaMemcpyHostToDevice, s->st),
             "upload fusion views");
     // capacity: valid pixels of the fused views
@@ -1827,18 +1935,18 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     sync(s);
     const int stride = (int)p->consistency_num_images + 1;
     if (valid > fc.cap || stride != fc.vis_stride) {
-      fc.release();
+      fc.release([s](void* q) { dfree(s, q); });
       const size_t c = std::max<unsigned long long>(valid, 1);
-      fc.pos = dalloc<float>(3 * c);
-      fc.nrm = dalloc<float>(3 * c);
-      fc.col = dalloc<unsigned char>(3 * c);
-      fc.key = dalloc<unsigned long long>(c);
-      fc.nvis = dalloc<unsigned char>(c);
-      fc.vis = dalloc<unsigned short>(c * stride);
+      fc.pos = dalloc<float>(s, 3 * c);
+      fc.nrm = dalloc<float>(s, 3 * c);
+      fc.col = dalloc<unsigned char>(s, 3 * c);
+      fc.key = dalloc<unsigned long long>(s, c);
+      fc.nvis = dalloc<unsigned char>(s, c);
+      fc.vis = dalloc<unsigned short>(s, c * stride);
       fc.cap = c;
       fc.vis_stride = stride;
     }
-    if (!sl.marks) sl.marks = dalloc<unsigned char>(std::max<long long>(sl.total, 1));
+    if (!sl.marks) sl.marks = dalloc<unsigned char>(s, std::max<long long>(sl.total, 1));
     cuda_ok(cudaMemsetAsync(sl.marks, 0, std::max<long long>(sl.total, 1), s->st), "memset");
     cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
     ps_post::FuseArgs A;

@@ -11,6 +11,8 @@
 """
 from __future__ import annotations
 
+import os
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 from typing import List, Optional, Sequence
 
@@ -96,16 +98,23 @@ def build_pyramid_device(gray: np.ndarray, k: Sequence[float], levels: int, devi
 
 def readout(states: Sequence[ViewState], counts: Sequence[np.ndarray], nsrc: Sequence[int],
             min_num_consistent: int) -> List[ViewState]:
-    """Readout threshold (densify.rs:441-454): depth/normal zeroed where count < max(1, min(min_num_consistent, nsrc))."""
-    out = []
-    for s, c, n in zip(states, counts, nsrc):
+    """Readout threshold (densify.rs:441-454): depth/normal zeroed where count < max(1, min(min_num_consistent, nsrc)).
+    Returns new states (the inputs are unchanged); views are processed on a thread pool (numpy releases the GIL on
+    whole-array operations)."""
+    zero = np.float32(0.0)
+
+    def one(args):
+        s, c, n = args
         need = max(1, min(min_num_consistent, n))
         keep = (s.depth > 0) & (c >= need)
-        r = s.copy()
-        r.depth[~keep] = 0.0
-        r.normal[~keep] = 0.0
-        out.append(r)
-    return out
+        return ViewState(s.width, s.height, np.where(keep, s.depth, zero), np.where(keep[..., None], s.normal, zero),
+                         s.cost.copy(), None if s.prior is None else s.prior.copy())
+
+    items = list(zip(states, counts, nsrc))
+    if len(items) < 2:
+        return [one(a) for a in items]
+    with ThreadPoolExecutor(max_workers=min(len(items), os.cpu_count() or 1)) as ex:
+        return list(ex.map(one, items))
 
 
 def compute_depth_maps(session: PatchMatchSession, inp: KernelInput, views: Sequence[int],

@@ -195,7 +195,10 @@ void ps_filter_params_default(ps_filter_params* out); /* FilterParams::default, 
 void ps_options_default(ps_options* out);             /* CudaPatchMatchOptions::default, patchmatch.rs:71-81 */
 
 /* ---- PatchMatchBackend ------------------------------------------------------------------------------------- */
-/* CudaPatchMatch::new / try_default (crates/cuda/src/patchmatch.rs:238-246). */
+/* CudaPatchMatch::new / try_default (crates/cuda/src/patchmatch.rs:238-246).  A backend runs one session at a time
+ * and keeps what its last session used for the next one: device buffers (a stream-ordered memory pool that does not
+ * release freed memory), the pinned host staging buffer and the texture arrays.  ps_backend_destroy releases them;
+ * end the backend's session first. */
 int ps_backend_create(int device, const ps_options* opts, ps_backend** out);
 void ps_backend_destroy(ps_backend* be);
 /* PatchMatchBackend::name (crates/dense/src/kernel.rs:241-242); the string lives as long as the backend. */

@@ -242,6 +242,7 @@ def bench_ours(args, rank, world, local):
         hbm.append(hbm_used(local))
         if rank == 0 and not args.no_check:
             res["fp64_reeval"] = fp64_check(wl, sess, mine)
+        res["neighbors"] = neighbors_stage(wl, sess, mine, local, check=rank == 0 and not args.no_check)
     if not args.no_learned and not shard_job:
         res["learned"] = learned_leg(args, wl, sess, stream, mine, value, ms_step, barrier, local)
         res["learned"]["fused_vs_plain"] = round(res["learned"]["fused_points"] / max(res["fusion"]["points"], 1), 4)
@@ -341,6 +342,35 @@ def fusion_stage(args, wl, sess, mine, check=True, label="plain"):
         out["oracle_points"] = len(ref)
         out["oracle_s"] = round(time.perf_counter() - t1, 2)
         out["oracle_cores"] = os.cpu_count() or 1
+    return out
+
+
+def neighbors_stage(wl, sess, mine, local, check=True):
+    """Neighbour views and depth ranges (ps_select_neighbors, NeighborOptions defaults) from sparse tracks built on the
+    final filtered depth maps of the last step (seeded pixels back-projected and seen by every view whose depth
+    agrees within 0.5 %); with `check`, the CPU oracle must give the same selections and ranges."""
+    from cumulus3d_b200 import scenes
+    from cumulus3d_b200.neighbors import NeighborParams, select_neighbors
+    st = sess.readout_download(0, mine)
+    depth = np.stack([x.depth for x in st])
+    model = scenes.sparse_model([wl.cams[v] for v in mine], depth, 20000, seed=11)
+    prm = NeighborParams()
+    select_neighbors(model, prm, local)  # warm-up (module load)
+    times = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        got = select_neighbors(model, prm, local)
+        times.append(time.perf_counter() - t0)
+    out = {"points": int(model.xyz.shape[0]), "observations": int(model.track_views.size),
+           "ms": round(sorted(times)[1] * 1e3, 2),
+           "what": "PairStats + select_all + depth_ranges on the GPU through the C ABI (host arrays in and out), "
+                   "median of 3; NeighborOptions defaults (10 views, 1 deg)"}
+    if check:
+        from oracle import oracle
+        t1 = time.perf_counter()
+        ref = oracle.select_neighbors(model, prm)
+        out["oracle_s"] = round(time.perf_counter() - t1, 2)
+        out["equal"] = bool(ref.sources == got.sources and ref.depth_ranges == got.depth_ranges)
     return out
 
 

@@ -112,6 +112,15 @@ class MultiscaleSchedule(C.Structure):
                 ("run_id_base", C.c_uint32), ("use_graph", C.c_uint32)]
 
 
+class SparseView(C.Structure):
+    _fields_ = [("r", C.c_double * 9), ("t", C.c_double * 3)]
+
+
+class NeighborParams(C.Structure):
+    _fields_ = [("num_views", C.c_uint32), ("direction_bins", C.c_uint32), ("min_triangulation_angle_deg", C.c_double),
+                ("diversity_decay", C.c_double)]
+
+
 class DepthSnapshot(C.Structure):
     _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
                 ("maps", C.POINTER(C.POINTER(C.c_float)))]
@@ -176,6 +185,10 @@ SIGNATURES = {
                                    C.POINTER(C.c_void_p), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
                                    C.POINTER(C.c_double)]),
     "ps_write_ply": (C.c_int, [C.c_char_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    # neighbour views and depth ranges
+    "ps_neighbor_params_default": (None, [C.POINTER(NeighborParams)]),
+    "ps_select_neighbors": (C.c_int, [C.c_int, C.POINTER(SparseView), C.c_uint32, _P, _P, _P, C.c_uint64,
+                                      C.POINTER(NeighborParams), _P, _P, _P, _P, _P, _P]),
     # learned proposal
     "ps_net_create": (C.c_int, [C.c_int, C.c_uint64, C.POINTER(_P)]),
     "ps_net_destroy": (None, [_P]),

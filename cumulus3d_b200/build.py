@@ -53,6 +53,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> pathlib.Path:
         ("noalloc.o", CSRC / "ps_noalloc.cu", PARITY),
         ("cnn.o", CSRC / "ps_cnn.cu", []),
         ("post.o", CSRC / "ps_post.cu", PARITY),
+        ("neighbors.o", CSRC / "ps_neighbors.cu", PARITY),
         ("io.o", CSRC / "ps_io.cpp", []),
     ]
     for name, src, flags in specs:

@@ -166,6 +166,42 @@ def nearest_sources(cams: Sequence[Camera], k: int) -> List[List[int]]:
     return out
 
 
+def sparse_model(cams: Sequence[Camera], gt_depth: np.ndarray, points_per_view: int = 4000, seed: int = 0,
+                 rel_tol: float = 0.005):
+    """Sparse points and tracks standing in for a structure-from-motion model: seeded pixels of every view
+    back-projected through its ground-truth depth, each seen by every view whose ground-truth depth at the projection
+    (nearest pixel) agrees within `rel_tol`; points seen by fewer than two views are dropped.  Tracks list their views
+    in ascending order.  Returns a neighbors.SparseModel."""
+    from .neighbors import SparseModel
+    rng = np.random.default_rng(seed)
+    pts = []
+    for i, c in enumerate(cams):
+        ys = rng.integers(0, c.height, points_per_view)
+        xs = rng.integers(0, c.width, points_per_view)
+        d = gt_depth[i][ys, xs].astype(np.float64)
+        ok = d > 0
+        ray = np.stack([(xs - c.k[2]) / c.k[0], (ys - c.k[3]) / c.k[1], np.ones(points_per_view)], -1)[ok]
+        pts.append((ray * d[ok, None] - c.t) @ c.r)  # world = Rᵀ (camera point - t)
+    X = np.concatenate(pts)
+    vis = np.zeros((len(X), len(cams)), bool)
+    for j, c in enumerate(cams):
+        P = X @ c.r.T + c.t
+        z = P[:, 2]
+        zs = np.where(z > 0, z, 1.0)
+        ui = np.rint(c.k[0] * P[:, 0] / zs + c.k[2]).astype(np.int64)
+        vi = np.rint(c.k[1] * P[:, 1] / zs + c.k[3]).astype(np.int64)
+        inside = (z > 0) & (ui >= 0) & (vi >= 0) & (ui < c.width) & (vi < c.height)
+        dg = np.zeros(len(X))
+        dg[inside] = gt_depth[j][vi[inside], ui[inside]]
+        vis[:, j] = inside & (dg > 0) & (np.abs(z - dg) <= rel_tol * dg)
+    keep = vis.sum(1) >= 2
+    vis = vis[keep]
+    off = np.zeros(len(vis) + 1, np.uint32)
+    off[1:] = np.cumsum(vis.sum(1))
+    views = np.array([np.concatenate([c.r.ravel(), c.t]) for c in cams], np.float64)
+    return SparseModel(views, np.ascontiguousarray(X[keep]), off, np.nonzero(vis)[1].astype(np.uint32))
+
+
 def to_gray8(img: np.ndarray) -> np.ndarray:
     """A rendered unit-range image as the 8-bit gray the reference's LevelImage holds (crates/dense/src/kernel.rs:80-91):
     round(255·v), clamped."""

@@ -440,6 +440,34 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride);
 
+/* ---- neighbour views and depth ranges from sparse tracks (crates/dense/src/neighbors.rs:44-186) --------------
+ * A view of the sparse model: world -> camera rotation r (row-major) and translation t (DenseView r, t). */
+typedef struct ps_sparse_view {
+  double r[9];
+  double t[3];
+} ps_sparse_view;
+/* NeighborOptions (crates/dense/src/params.rs:355-369); diversity_decay >= 1 selects plain shared-count order
+ * (PairStats::select_all), below 1 the direction-diverse greedy choice (PairStats::select_diverse, as
+ * crates/dense/src/densify.rs:224-240 chooses). */
+typedef struct ps_neighbor_params {
+  uint32_t num_views;                 /* 10: sources kept per view (1..1024) */
+  uint32_t direction_bins;            /* 8 */
+  double min_triangulation_angle_deg; /* 1.0: pairs whose 75th-percentile angle is below are skipped (0: no test) */
+  double diversity_decay;             /* 1.0 */
+} ps_neighbor_params;
+void ps_neighbor_params_default(ps_neighbor_params* out);
+/* PairStats::new + select_all / select_diverse + depth_ranges on the GPU.  Point i has position xyz[3i..3i+3) and
+ * the track track_views[track_offsets[i] .. track_offsets[i+1]) (view indices, repeats allowed and counted as the
+ * reference counts them).  Outputs: sources[v * num_views + k] for k < num_sources[v] (the rest UINT32_MAX);
+ * depth_range[2v], [2v+1] = (0.75·d1%, 1.25·d99%) of the view's positive point depths and has_range[v] = 0 when it
+ * has none.  pair_count / pair_angle75 (may be NULL; num_views² entries, index min(a,b)·n + max(a,b)) receive the
+ * shared count and the 75th-percentile triangulation angle (radians) of every pair.  At most 4096 views.  Blocking;
+ * allocates and frees its own device memory. */
+int ps_select_neighbors(int device, const ps_sparse_view* views, uint32_t num_views, const double* xyz,
+                        const uint32_t* track_offsets, const uint32_t* track_views, uint64_t num_points,
+                        const ps_neighbor_params* p, uint32_t* sources, uint32_t* num_sources, double* depth_range,
+                        uint8_t* has_range, uint32_t* pair_count, double* pair_angle75);
+
 /* build_pyramid (crates/dense/src/upsample.rs:46-102) on the GPU: out[0] is the coarsest level, out[levels-1] the
  * input itself; level sizes halve (floor) towards the coarse end; out_k (may be NULL) receives 4 doubles per level
  * (f·0.5, c ← (c + 0.5)·0.5 − 0.5 per step from k).  Blocking; allocates and frees its own device memory. */

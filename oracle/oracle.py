@@ -54,6 +54,9 @@ def lib() -> C.CDLL:
             "oracle_median": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, _SV, C.c_int]),
             "oracle_reeval_f64": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                             C.POINTER(C.POINTER(C.c_double)), C.c_int]),
+            "oracle_select_neighbors": (C.c_int, [C.POINTER(_lib.SparseView), C.c_uint32, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_uint64, C.POINTER(_lib.NeighborParams), C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
             "oracle_mix64": (C.c_uint64, [C.c_uint64]),
             "oracle_rng_state": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                               C.c_uint64]),
@@ -235,3 +238,10 @@ def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[
                            vc.ctypes.data, vis.ctypes.data, stride, C.byref(n)), "fuse")
     k = int(n.value)
     return FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
+
+
+def select_neighbors(model, params, pair_stats: bool = False):
+    """PairStats::new + select_all / select_diverse + depth_ranges (crates/dense/src/neighbors.rs:44-186) on the CPU;
+    same inputs and outputs as cumulus3d_b200.neighbors.select_neighbors."""
+    from cumulus3d_b200 import neighbors
+    return neighbors.call(lib().oracle_select_neighbors, model, params, pair_stats)

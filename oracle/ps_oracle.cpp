@@ -34,6 +34,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <vector>
 
@@ -1454,6 +1455,182 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
   }
   *count = n_out;
   return n_out <= capacity ? PS_OK : PS_EINVAL;
+}
+
+// ---- neighbour views and depth ranges from sparse tracks (crates/dense/src/neighbors.rs:44-186) ----------------
+// DenseView::center (crates/dense/src/scene.rs:82-89): -(Rᵀ t).
+static void nb_center(const ps_sparse_view& v, double c[3]) {
+  for (int j = 0; j < 3; ++j) c[j] = -(v.r[0 * 3 + j] * v.t[0] + v.r[1 * 3 + j] * v.t[1] + v.r[2 * 3 + j] * v.t[2]);
+}
+// quantile_sorted (crates/dense/src/math.rs:126-135): linear interpolation between the order statistics around
+// q·(n-1).
+static double nb_quantile_sorted(const std::vector<double>& v, double q) {
+  if (v.empty()) return 0.0;
+  const double pos = q * (double)(v.size() - 1);
+  const size_t lo = (size_t)std::floor(pos);
+  const size_t hi = std::min(lo + 1, v.size() - 1);
+  const double f = pos - (double)lo;
+  return v[lo] + (v[hi] - v[lo]) * f;
+}
+// f64::powi as lowered for a run-time exponent: square-and-multiply over the exponent's bits, lowest bit first.
+static double nb_powi(double a, int b) {
+  const bool recip = b < 0;
+  double r = 1.0;
+  for (;;) {
+    if (b & 1) r *= a;
+    b /= 2;
+    if (b == 0) break;
+    a *= a;
+  }
+  return recip ? 1.0 / r : r;
+}
+
+void oracle_neighbor_params_default(ps_neighbor_params* out) {
+  out->num_views = 10;
+  out->direction_bins = 8;
+  out->min_triangulation_angle_deg = 1.0;
+  out->diversity_decay = 1.0;
+}
+
+int oracle_select_neighbors(const ps_sparse_view* views, uint32_t nv, const double* xyz, const uint32_t* toff,
+                            const uint32_t* tview, uint64_t np, const ps_neighbor_params* prm, uint32_t* sources,
+                            uint32_t* num_sources, double* depth_range, uint8_t* has_range, uint32_t* pair_count,
+                            double* pair_angle75) {
+  if (!views || !nv || !prm || !prm->num_views || !sources || !num_sources || (np && (!xyz || !toff || !tview)))
+    return PS_EINVAL;
+  for (uint64_t i = 0; i < np; ++i)
+    for (uint32_t k = toff[i]; k < toff[i + 1]; ++k)
+      if (tview[k] >= nv) return PS_EINVAL;
+  std::vector<std::array<double, 3>> centers(nv);
+  for (uint32_t v = 0; v < nv; ++v) nb_center(views[v], centers[v].data());
+  // PairStats::new (neighbors.rs:47-76): every pair of distinct entries of a track, counted and its triangulation
+  // angle min(a, pi - a) recorded in binary32
+  const size_t nn = (size_t)nv * nv;
+  std::vector<uint32_t> cnt(nn, 0);
+  std::vector<std::vector<float>> angs(nn);
+  for (uint64_t i = 0; i < np; ++i) {
+    const double* x = xyz + 3 * i;
+    for (uint32_t ii = toff[i]; ii < toff[i + 1]; ++ii)
+      for (uint32_t jj = toff[i]; jj < ii; ++jj) {
+        const uint32_t a = tview[ii], b = tview[jj];
+        if (a == b) continue;
+        const double* ca = centers[a].data();
+        const double* cb = centers[b].data();
+        const double u[3] = {ca[0] - x[0], ca[1] - x[1], ca[2] - x[2]};
+        const double w[3] = {cb[0] - x[0], cb[1] - x[1], cb[2] - x[2]};
+        const double nu = std::sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        const double nw = std::sqrt(w[0] * w[0] + w[1] * w[1] + w[2] * w[2]);
+        double ang = 0.0;
+        if (!(nu == 0.0 || nw == 0.0)) {
+          double c = (u[0] * w[0] + u[1] * w[1] + u[2] * w[2]) / (nu * nw);
+          if (c < -1.0) c = -1.0;
+          else if (c > 1.0) c = 1.0;
+          const double t = std::acos(c);
+          ang = std::fmin(t, M_PI - t);
+        }
+        const size_t key = (size_t)std::min(a, b) * nv + std::max(a, b);
+        cnt[key]++;
+        angs[key].push_back((float)ang);
+      }
+  }
+  std::vector<double> q75(nn, 0.0);
+  for (size_t k = 0; k < nn; ++k) {
+    if (!cnt[k]) continue;
+    std::vector<double> a(angs[k].begin(), angs[k].end());
+    std::sort(a.begin(), a.end());
+    q75[k] = nb_quantile_sorted(a, 0.75);
+  }
+  if (pair_count) memcpy(pair_count, cnt.data(), nn * sizeof(uint32_t));
+  if (pair_angle75) memcpy(pair_angle75, q75.data(), nn * sizeof(double));
+  // select (neighbors.rs:82-101) with the angle in radians (f64::to_radians: deg · (pi/180)), and select_diverse
+  // (neighbors.rs:108-150) when the decay is below 1 (densify.rs:224-240)
+  const double min_angle = prm->min_triangulation_angle_deg * (M_PI / 180.0);
+  const uint32_t maxn = prm->num_views;
+  const bool diverse = prm->diversity_decay < 1.0;
+  const size_t bins = std::max<uint32_t>(prm->direction_bins, 1);
+  for (uint32_t r = 0; r < nv; ++r) {
+    std::vector<std::pair<uint32_t, uint32_t>> cands;  // (count, view)
+    for (uint32_t o = 0; o < nv; ++o) {
+      if (o == r) continue;
+      const size_t key = (size_t)std::min(r, o) * nv + std::max(r, o);
+      if (!cnt[key]) continue;
+      if (min_angle > 0.0 && q75[key] < min_angle) continue;
+      cands.push_back({cnt[key], o});
+    }
+    std::sort(cands.begin(), cands.end(), [](const std::pair<uint32_t, uint32_t>& x, const std::pair<uint32_t, uint32_t>& y) {
+      return x.first != y.first ? x.first > y.first : x.second < y.second;
+    });
+    std::vector<uint32_t> out;
+    if (!diverse) {
+      for (size_t i = 0; i < cands.size() && out.size() < maxn; ++i) out.push_back(cands[i].second);
+    } else {
+      const ps_sparse_view& vr = views[r];
+      const double* cr = centers[r].data();
+      std::vector<size_t> bin(cands.size());
+      for (size_t i = 0; i < cands.size(); ++i) {
+        const double* co = centers[cands[i].second].data();
+        const double d[3] = {co[0] - cr[0], co[1] - cr[1], co[2] - cr[2]};
+        double b[3];
+        for (int k = 0; k < 3; ++k) b[k] = vr.r[k * 3 + 0] * d[0] + vr.r[k * 3 + 1] * d[1] + vr.r[k * 3 + 2] * d[2];
+        const double lat = std::sqrt(b[0] * b[0] + b[1] * b[1]);
+        if (lat < 0.3 * std::fabs(b[2])) {
+          bin[i] = bins;
+        } else {
+          const double a = std::atan2(b[1], b[0]) + M_PI;
+          bin[i] = std::min((size_t)(a / (2.0 * M_PI) * (double)bins), bins - 1);
+        }
+      }
+      std::vector<int> used(bins + 1, 0);
+      std::vector<char> taken(cands.size(), 0);
+      while (out.size() < maxn) {
+        bool any = false;
+        double bs = 0.0;
+        size_t bi = 0;
+        for (size_t i = 0; i < cands.size(); ++i) {
+          if (taken[i]) continue;
+          const double sc = (double)cands[i].first * nb_powi(prm->diversity_decay, used[bin[i]]);
+          if (!any || sc > bs) {
+            any = true;
+            bs = sc;
+            bi = i;
+          }
+        }
+        if (!any) break;
+        taken[bi] = 1;
+        used[bin[bi]]++;
+        out.push_back(cands[bi].second);
+      }
+    }
+    num_sources[r] = (uint32_t)out.size();
+    for (uint32_t k = 0; k < maxn; ++k) sources[(size_t)r * maxn + k] = k < out.size() ? out[k] : UINT32_MAX;
+  }
+  // depth_ranges / depth_range_of (neighbors.rs:160-186): positive depths of every observation (repeats included),
+  // the 1 % and 99 % order statistics (no interpolation) times 0.75 and 1.25
+  std::vector<std::vector<double>> lists(nv);
+  for (uint64_t i = 0; i < np; ++i) {
+    const double* x = xyz + 3 * i;
+    for (uint32_t k = toff[i]; k < toff[i + 1]; ++k) {
+      const ps_sparse_view& v = views[tview[k]];
+      const double d = v.r[6] * x[0] + v.r[7] * x[1] + v.r[8] * x[2] + v.t[2];
+      if (d > 0.0) lists[tview[k]].push_back(d);
+    }
+  }
+  for (uint32_t v = 0; v < nv; ++v) {
+    std::vector<double>& l = lists[v];
+    if (has_range) has_range[v] = l.empty() ? 0 : 1;
+    if (!depth_range) continue;
+    if (l.empty()) {
+      depth_range[2 * v] = depth_range[2 * v + 1] = 0.0;
+      continue;
+    }
+    std::sort(l.begin(), l.end());
+    const size_t n = l.size();
+    const double lo = l[std::min((size_t)std::floor((double)n * 0.01), n - 1)];
+    const double hi = l[std::min((size_t)std::floor((double)n * 0.99), n - 1)];
+    depth_range[2 * v] = 0.75 * lo;
+    depth_range[2 * v + 1] = 1.25 * hi;
+  }
+  return PS_OK;
 }
 
 }  // extern "C"

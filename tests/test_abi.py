@@ -43,7 +43,8 @@ STRUCTS = {
     "ps_kernel_input": _lib.KernelInput, "ps_view_state": _lib.ViewState, "ps_run_params": _lib.RunParams,
     "ps_depth_snapshot": _lib.DepthSnapshot, "ps_schedule": _lib.Schedule,
     "ps_multiscale_schedule": _lib.MultiscaleSchedule, "ps_post_params": _lib.PostParams,
-    "ps_fusion_params": _lib.FusionParams, "ps_fusion_view": _lib.FusionView,
+    "ps_fusion_params": _lib.FusionParams, "ps_fusion_view": _lib.FusionView, "ps_sparse_view": _lib.SparseView,
+    "ps_neighbor_params": _lib.NeighborParams,
 }
 
 

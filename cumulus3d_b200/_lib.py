@@ -87,9 +87,10 @@ class Schedule(C.Structure):
 
 
 class PostParams(C.Structure):
-    """PostParams (crates/dense/src/postproc.rs:41-74), speckle removal part."""
+    """PostParams (crates/dense/src/postproc.rs:41-74)."""
     _fields_ = [("remove_speckles", C.c_uint32), ("speckle_rel_depth", C.c_float), ("speckle_min_area_frac", C.c_double),
-                ("speckle_keep_cost", C.c_float)]
+                ("speckle_keep_cost", C.c_float), ("fill_holes", C.c_uint32), ("fill_max_frac", C.c_double),
+                ("fill_edge_step", C.c_float), ("fill_max_cost", C.c_float)]
 
 
 class FusionParams(C.Structure):
@@ -175,7 +176,7 @@ SIGNATURES = {
     "ps_post_params_default": (None, [C.POINTER(PostParams)]),
     "ps_fusion_params_default": (None, [C.POINTER(FusionParams)]),
     "ps_postprocess_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(PostParams),
-                                          C.POINTER(C.c_uint64)]),
+                                          C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ps_readout_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_fuse_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView), C.POINTER(FusionParams),
                                    C.POINTER(C.c_uint64)]),

@@ -379,6 +379,96 @@ __global__ void k_pyramid(const unsigned char* in, int w, int h, unsigned char* 
   out[(long long)Y * nw + X] = (unsigned char)fminf(fmaxf(roundf(v), 0.0f), 255.0f);
 }
 
+// ---------------------------------------------------------------------------------------------- hole filling
+// 8-bit gray value of an image-plane pixel: planes of 8-bit images hold the correctly rounded u/255, and
+// round(255·value) gives u back exactly for every u.
+__device__ __forceinline__ int fill_gray(const FillArgs& A, int x, int y) {
+  return (int)rintf(A.img[(long long)y * A.pitch + x] * 255.0f);
+}
+
+// The fill of every pixel from the unfilled state (postproc.rs:155-193): an invalid pixel with a run cost of at most
+// max_cost walks the 8 directions in the reference's order, up to maxd steps, stopping at the border or where the gray
+// value jumps by more than `step` from the previous pixel; the first valid pixel met ends a direction, and the one
+// with the smallest (|gray difference|, distance) over the directions (the earliest on ties) lends its plane through
+// plane_transfer (crates/dense/src/math.rs:146-154, binary64).
+__global__ void __launch_bounds__(256) k_fill_find(const FillArgs A) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)A.w * A.h) return;
+  const int y = (int)(i / A.w), x = (int)(i - (long long)y * A.w);
+  float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+  float oc = 0.f;
+  if (!(A.plane[i].w > 0.f) && !(A.cost[i] > A.max_cost)) {
+    const int ip = fill_gray(A, x, y);
+    const int dxs[8] = {1, -1, 0, 0, 1, -1, 1, -1}, dys[8] = {0, 0, 1, -1, 1, -1, -1, 1};
+    bool found = false;
+    int bd = 0, bs = 0;
+    long long bq = 0;
+    for (int d = 0; d < 8; ++d) {
+      int prev = ip;
+      for (int s = 1; s <= A.maxd; ++s) {
+        const int qx = x + dxs[d] * s, qy = y + dys[d] * s;
+        if (qx < 0 || qy < 0 || qx >= A.w || qy >= A.h) break;
+        const int iq = fill_gray(A, qx, qy);
+        if (abs(iq - prev) > A.step) break;
+        prev = iq;
+        const long long q = (long long)qy * A.w + qx;
+        if (A.plane[q].w > 0.f) {
+          const int diff = abs(iq - ip);
+          if (!found || diff < bd || (diff == bd && s < bs)) {
+            found = true;
+            bd = diff;
+            bs = s;
+            bq = q;
+          }
+          break;
+        }
+      }
+    }
+    if (found) {
+      const float4 pq = A.plane[bq];
+      const double qx = (double)(bq % A.w), qy = (double)(bq / A.w);
+      const double rq0 = (qx - A.k[2]) / A.k[0], rq1 = (qy - A.k[3]) / A.k[1];
+      const double rp0 = ((double)x - A.k[2]) / A.k[0], rp1 = ((double)y - A.k[3]) / A.k[1];
+      const double n0 = (double)pq.x, n1 = (double)pq.y, n2 = (double)pq.z;
+      const double num = n0 * rq0 + n1 * rq1 + n2 * 1.0;
+      const double den = n0 * rp0 + n1 * rp1 + n2 * 1.0;
+      if (!(den > -1e-6)) {
+        const double dd = (double)pq.w * num / den;
+        if (dd > 0.0 && isfinite(dd)) {
+          out = make_float4(pq.x, pq.y, pq.z, (float)dd);
+          oc = A.cost[bq];
+        }
+      }
+    }
+  }
+  A.tplane[i] = out;
+  A.tcost[i] = oc;
+}
+
+__global__ void __launch_bounds__(256) k_fill_apply(const FillArgs A) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool f = false;
+  if (i < (long long)A.w * A.h) {
+    const float4 t = A.tplane[i];
+    if (t.w > 0.f) {
+      A.plane[i] = t;
+      A.cost[i] = A.tcost[i];
+      f = true;
+    }
+  }
+  const unsigned m = __ballot_sync(0xffffffffu, f);
+  if ((threadIdx.x & 31) == 0 && m) atomicAdd(A.filled, (unsigned long long)__popc(m));
+}
+
+cudaError_t launch_fill_holes(const FillArgs& A, cudaStream_t st) {
+  const long long n = (long long)A.w * A.h;
+  if (n <= 0) return cudaSuccess;
+  const unsigned g = (unsigned)((n + 255) / 256);
+  k_fill_find<<<g, 256, 0, st>>>(A);
+  k_fill_apply<<<g, 256, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
 // Reference planes of a session: out[y·pitch + x] = lut[in[y·w + x]] (lut = the correctly rounded u/255 of the host,
 // so the plane has the bits the oracle's plane has).
 __global__ void k_u8_plane(const unsigned char* __restrict__ in, int w, int h, const float* __restrict__ lut,

@@ -62,6 +62,20 @@ struct FuseArgs {
   unsigned long long capacity;
 };
 
+// Hole filling of one view's readout planes (fill_holes, crates/dense/src/postproc.rs:139-201).
+struct FillArgs {
+  float4* plane;    // the view's readout planes (nx, ny, nz, d), filled in place
+  float* cost;      // the view's run costs in; filled pixels take their source pixel's cost
+  const float* img; // the view's image plane, row pitch `pitch` floats (gray = round(255·value))
+  float4* tplane;   // scratch per pixel: its fill (d = 0: none)
+  float* tcost;
+  unsigned long long* filled;
+  double k[4];
+  int w, h, pitch, maxd, step;
+  float max_cost;
+};
+cudaError_t launch_fill_holes(const FillArgs& A, cudaStream_t st);
+
 cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* launches);
 cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);

@@ -1682,7 +1682,7 @@ int ps_propose(ps_session* s, ps_net* net, uint32_t level, const uint32_t* views
     }
     grow(s, s->netin, s->netin_cap, in_need);
     grow(s, s->netout, s->netout_cap, out_need);
-    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 1);
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 2);  // two counters (post-processing uses both)
     cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
     for (size_t i = 0; i < n; ++i) {
       const uint32_t v = views[i];
@@ -1816,6 +1816,10 @@ void ps_post_params_default(ps_post_params* out) {
   out->speckle_rel_depth = 0.02f;
   out->speckle_min_area_frac = 2e-4;
   out->speckle_keep_cost = 0.2f;
+  out->fill_holes = 0;
+  out->fill_max_frac = 0.01;
+  out->fill_edge_step = 0.06f;
+  out->fill_max_cost = 1.0f;
 }
 
 void ps_fusion_params_default(ps_fusion_params* out) {
@@ -1834,17 +1838,20 @@ void ps_fusion_params_default(ps_fusion_params* out) {
 }
 
 int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
-                            uint64_t* removed) {
+                            const double* intrinsics, uint64_t* removed, uint64_t* filled) {
   return guard(s, [&] {
     if (!p) fail(PS_EINVAL, "params is NULL");
     check_views(s, views, n);
+    if (level >= (uint32_t)s->nl) fail(PS_EINVAL, "level out of range");
     Slot& sl = slot(s, (int)level);
     if (removed) *removed = 0;
-    if (!p->remove_speckles || n == 0) return;
+    if (filled) *filled = 0;
+    if (n == 0 || (!p->remove_speckles && !p->fill_holes)) return;
     if (!sl.spk) sl.spk = dalloc<int>(s, (size_t)std::max<long long>(sl.total, 1) * 5);
-    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 1);
-    cuda_ok(cudaMemsetAsync(s->pcount, 0, sizeof(unsigned long long), s->st), "memset");
+    if (!s->pcount) s->pcount = dalloc<unsigned long long>(s, 2);
+    cuda_ok(cudaMemsetAsync(s->pcount, 0, 2 * sizeof(unsigned long long), s->st), "memset");
     const size_t T = (size_t)std::max<long long>(sl.total, 1);
+    if (p->remove_speckles)
     for (auto [a, b] : batches(s, views, n, (int)level)) {
       ps_post::SpkArgs A;
       memset(&A, 0, sizeof A);
@@ -1868,11 +1875,46 @@ int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views
       cuda_ok(ps_post::launch_speckles(A, tiles, s->st, &nl), "speckle kernels");
       s->launches += nl;
     }
-    if (removed) {
-      unsigned long long c = 0;
-      cuda_ok(cudaMemcpyAsync(&c, s->pcount, sizeof c, cudaMemcpyDeviceToHost, s->st), "read count");
+    if (p->fill_holes) {
+      // scratch: a float4 fill plane and a cost per slot pixel in the speckle buffer (5 words per pixel)
+      float4* tplane = reinterpret_cast<float4*>(sl.spk);
+      float* tcost = reinterpret_cast<float*>(sl.spk + 4 * T);
+      for (size_t i = 0; i < n; ++i) {
+        const int v = (int)views[i];
+        const PsLevel& L = s->lvh[v * s->nl + (int)level];
+        ps_post::FillArgs F;
+        memset(&F, 0, sizeof F);
+        F.plane = sl.aux + sl.off[v];
+        F.cost = sl.cost + sl.off[v];
+        F.img = L.img;
+        F.pitch = L.pitch;
+        F.tplane = tplane + sl.off[v];
+        F.tcost = tcost + sl.off[v];
+        F.filled = s->pcount + 1;
+        F.w = s->W(v, (int)level);
+        F.h = s->H(v, (int)level);
+        if (intrinsics) {
+          for (int k = 0; k < 4; ++k) F.k[k] = intrinsics[4 * v + k];
+        } else {
+          F.k[0] = L.fx;
+          F.k[1] = L.fy;
+          F.k[2] = L.cx;
+          F.k[3] = L.cy;
+        }
+        const long long W = F.w, H = F.h;
+        F.maxd = (int)std::max<long long>((long long)std::round(std::sqrt((double)(W * W + H * H)) * p->fill_max_frac), 1);
+        F.step = (int)(p->fill_edge_step * 255.0f);
+        F.max_cost = p->fill_max_cost;
+        launched(s, ps_post::launch_fill_holes(F, s->st), "hole filling kernels");
+        s->launches += 1;  // two kernels per view (launched() counts one)
+      }
+    }
+    if (removed || filled) {
+      unsigned long long c[2] = {0, 0};
+      cuda_ok(cudaMemcpyAsync(c, s->pcount, sizeof c, cudaMemcpyDeviceToHost, s->st), "read counts");
       sync(s);
-      *removed = c;
+      if (removed) *removed = c[0];
+      if (filled) *filled = c[1];
     }
   });
 }

@@ -381,13 +381,23 @@ class PatchMatchSession:
         self._check(self.lib.ps_schedule_resident(self.h, _views(views), len(views), C.byref(sch)))
 
     # ---- post-processing and fusion ----------------------------------------------------------------------------
-    def postprocess_resident(self, level: int, views: Sequence[int], post=None, count: bool = True) -> Optional[int]:
-        """Speckle removal on the readout planes (PostParams; defaults of the reference when `post` is None)."""
+    def postprocess_resident(self, level: int, views: Sequence[int], post=None, count: bool = True,
+                             intrinsics=None, filled: bool = False):
+        """Speckle removal and (when enabled) hole filling on the readout planes (PostParams; defaults of the
+        reference when `post` is None).  `intrinsics`: (num_views, 4) float64 fx, fy, cx, cy of every session view
+        (the full-precision DenseView::k), or None for the level's.  Returns the erased pixel count (None without
+        `count`), or (erased, filled) with `filled`."""
         from .fusion import default_post
         p = post if post is not None else default_post()
-        n = C.c_uint64()
-        self._check(self.lib.ps_postprocess_resident(self.h, level, _views(views), len(views), C.byref(p),
-                                                     C.byref(n) if count else None))
+        n, f = C.c_uint64(), C.c_uint64()
+        kp = None
+        if intrinsics is not None:
+            k = np.ascontiguousarray(intrinsics, np.float64).reshape(-1, 4)
+            kp = k.ctypes.data_as(C.POINTER(C.c_double))
+        self._check(self.lib.ps_postprocess_resident(self.h, level, _views(views), len(views), C.byref(p), kp,
+                                                     C.byref(n) if count else None, C.byref(f) if filled else None))
+        if filled:
+            return int(n.value), int(f.value)
         return int(n.value) if count else None
 
     def readout_download(self, level: int, views: Sequence[int]) -> List[ViewState]:

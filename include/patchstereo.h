@@ -32,7 +32,7 @@ extern "C" {
 #endif
 
 #define PS_MAX_SOURCES 32 /* crates/cuda/src/kernels/patchmatch.cu:40 (MAXSRC) */
-#define PS_ABI_VERSION 2
+#define PS_ABI_VERSION 3
 
 /* Status codes.  Maps the reference's error kinds: Error::InvalidArgument -> PS_EINVAL,
  * Error::Invariant("CUDA: …") -> PS_ECUDA (crates/cuda/src/patchmatch.rs:234-236),
@@ -385,19 +385,31 @@ int ps_proposal_download(ps_session* s, uint32_t level, const uint32_t* views, s
                          float* const* conf);
 
 /* ---- post-processing and fusion of resident depth maps -------------------------------------------------------
- * PostParams (crates/dense/src/postproc.rs:41-74): speckle removal only (fill_holes is off by default there and is
- * not provided).  remove_speckles (postproc.rs:77-129) runs on the readout planes of `level` in place: 4-connected
- * components (|d_j - d_i| <= rel·min(d_i, d_j)) smaller than ceil(w·h·min_area_frac) whose lower median cost exceeds
- * keep_cost are erased.  Asynchronous unless `removed` is given (then it receives the erased pixel count). */
+ * PostParams (crates/dense/src/postproc.rs:41-74), applied to the readout planes of `level` in place, in the
+ * reference's order (crates/dense/src/densify.rs:455-461):
+ *  - remove_speckles (postproc.rs:77-129): 4-connected components (|d_j - d_i| <= rel·min(d_i, d_j)) smaller than
+ *    ceil(w·h·min_area_frac) whose lower median cost exceeds keep_cost are erased;
+ *  - fill_holes (postproc.rs:139-201, off by default): every invalid pixel whose run cost is at most fill_max_cost
+ *    walks the 8 directions up to round(diag·fill_max_frac) steps over the 8-bit gray image, stopping where the gray
+ *    value jumps by more than fill_edge_step·255, and takes the plane of the valid pixel it meets with the smallest
+ *    (gray difference, distance); filled pixels also take that pixel's cost (the slot's costs then hold the readout
+ *    costs, as DepthMapResult.cost does).  The gray value of a pixel is round(255·plane value), which is the 8-bit
+ *    input exactly for 8-bit images.  `intrinsics` (4 doubles fx, fy, cx, cy per session view, indexed by view;
+ *    may be NULL) gives the full-precision DenseView::k the reference's rays use; NULL uses the level's.
+ * Asynchronous unless `removed` / `filled` is given (then it receives the count). */
 typedef struct ps_post_params {
   uint32_t remove_speckles;     /* true */
   float speckle_rel_depth;      /* 0.02 */
   double speckle_min_area_frac; /* 2e-4 */
   float speckle_keep_cost;      /* 0.2 */
+  uint32_t fill_holes;          /* false */
+  double fill_max_frac;         /* 0.01 */
+  float fill_edge_step;         /* 0.06 */
+  float fill_max_cost;          /* 1.0 */
 } ps_post_params;
 void ps_post_params_default(ps_post_params* out);
 int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
-                            uint64_t* removed);
+                            const double* intrinsics, uint64_t* removed, uint64_t* filled);
 /* Downloads the current readout planes (after any post-processing) and final costs of `views` at `level` without
  * recomputing the readout. */
 int ps_readout_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* out);

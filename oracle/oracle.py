@@ -57,6 +57,9 @@ def lib() -> C.CDLL:
             "oracle_select_neighbors": (C.c_int, [C.POINTER(_lib.SparseView), C.c_uint32, C.c_void_p, C.c_void_p,
                                                   C.c_void_p, C.c_uint64, C.POINTER(_lib.NeighborParams), C.c_void_p,
                                                   C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+            "oracle_fill_holes": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                            C.POINTER(C.c_double), C.c_uint32, C.c_uint32, C.c_double, C.c_float,
+                                            C.c_float, C.POINTER(C.c_uint64)]),
             "oracle_mix64": (C.c_uint64, [C.c_uint64]),
             "oracle_rng_state": (C.c_uint64, [C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                               C.c_uint64]),
@@ -208,6 +211,23 @@ def remove_speckles(depth: np.ndarray, normal: np.ndarray, cost: np.ndarray, pos
     _chk(lib().oracle_remove_speckles(depth.ctypes.data, normal.ctypes.data, c.ctypes.data, w, h,
                                       post.speckle_rel_depth, post.speckle_min_area_frac, post.speckle_keep_cost,
                                       C.byref(n)), "remove_speckles")
+    return int(n.value)
+
+
+def fill_holes(depth: np.ndarray, normal: np.ndarray, cost: np.ndarray, raw_cost: np.ndarray, gray: np.ndarray, k,
+               post) -> int:
+    """fill_holes restated (depth (h, w), normal (h, w, 3) and cost updated in place); gray (h, w) uint8, k the view's
+    fx, fy, cx, cy.  Returns the filled pixel count."""
+    assert depth.dtype == np.float32 and normal.dtype == np.float32 and cost.dtype == np.float32
+    assert depth.flags.c_contiguous and normal.flags.c_contiguous and cost.flags.c_contiguous
+    h, w = depth.shape
+    rc_ = np.ascontiguousarray(raw_cost, np.float32)
+    g = np.ascontiguousarray(gray, np.uint8)
+    kk = (C.c_double * 4)(*[float(x) for x in k])
+    n = C.c_uint64()
+    _chk(lib().oracle_fill_holes(depth.ctypes.data, normal.ctypes.data, cost.ctypes.data, rc_.ctypes.data,
+                                 g.ctypes.data, kk, w, h, post.fill_max_frac, post.fill_edge_step, post.fill_max_cost,
+                                 C.byref(n)), "fill_holes")
     return int(n.value)
 
 

@@ -1215,6 +1215,77 @@ void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
 // row-major order over 4-neighbours with |d_j - d_i| <= rel·min(d_i, d_j); a component smaller than
 // ceil(w·h·frac) whose lower median cost (costs sorted by total order, element len/2) exceeds keep is erased
 // (depth 0, normal 0).  normal: 3 floats per pixel.
+// fill_holes (crates/dense/src/postproc.rs:139-201): every invalid pixel whose own (raw) cost is at most max_cost
+// walks the 8 directions up to maxd = max(round(diag · max_frac), 1) steps over the 8-bit gray image, stopping at the
+// border or where the gray value jumps by more than step = (int)(edge_step · 255) from the previous pixel, and takes
+// the valid pixel it meets with the smallest (|gray difference|, distance) (the first direction on ties); its plane
+// is transferred to the pixel (plane_transfer).  Fills read the unfilled state only and are applied at the end.
+int oracle_fill_holes(float* depth, float* normal, float* cost, const float* raw_cost, const uint8_t* gray,
+                      const double* k, uint32_t w, uint32_t h, double max_frac, float edge_step, float max_cost,
+                      uint64_t* filled) {
+  if (!depth || !normal || !cost || !raw_cost || !gray || !k) return PS_EINVAL;
+  const long long W = w, H = h;
+  const long long maxd = std::max<long long>((long long)std::round(std::sqrt((double)(W * W + H * H)) * max_frac), 1);
+  const int step = (int)(edge_step * 255.0f);
+  const size_t n = (size_t)w * h;
+  std::vector<char> valid(n);
+  for (size_t i = 0; i < n; ++i) valid[i] = depth[i] > 0.0f;
+  struct Fill {
+    size_t i;
+    float d, nx, ny, nz, c;
+  };
+  std::vector<Fill> fills;
+  static const int dirs[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {-1, -1}, {1, -1}, {-1, 1}};
+  for (long long y = 0; y < H; ++y)
+    for (long long x = 0; x < W; ++x) {
+      const size_t i = (size_t)(y * W + x);
+      if (valid[i] || raw_cost[i] > max_cost) continue;
+      const int ip = gray[i];
+      bool found = false;
+      int bdiff = 0;
+      long long bs = 0;
+      size_t bq = 0;
+      for (int d = 0; d < 8; ++d) {
+        int prev = ip;
+        for (long long st = 1; st <= maxd; ++st) {
+          const long long qx = x + dirs[d][0] * st, qy = y + dirs[d][1] * st;
+          if (qx < 0 || qy < 0 || qx >= W || qy >= H) break;
+          const size_t q = (size_t)(qy * W + qx);
+          const int iq = gray[q];
+          if (std::abs(iq - prev) > step) break;
+          prev = iq;
+          if (valid[q]) {
+            const int diff = std::abs(iq - ip);
+            if (!found || diff < bdiff || (diff == bdiff && st < bs)) {
+              found = true;
+              bdiff = diff;
+              bs = st;
+              bq = q;
+            }
+            break;
+          }
+        }
+      }
+      if (!found) continue;
+      const double nq[3] = {(double)normal[3 * bq], (double)normal[3 * bq + 1], (double)normal[3 * bq + 2]};
+      const double qx = (double)(bq % w), qy = (double)(bq / w);
+      const double rq[3] = {(qx - k[2]) / k[0], (qy - k[3]) / k[1], 1.0};
+      const double rp[3] = {((double)x - k[2]) / k[0], ((double)y - k[3]) / k[1], 1.0};
+      double dd;
+      if (oracle_plane_transfer((double)depth[bq], nq, rq, rp, &dd))
+        fills.push_back({i, (float)dd, normal[3 * bq], normal[3 * bq + 1], normal[3 * bq + 2], cost[bq]});
+    }
+  for (const Fill& f : fills) {
+    depth[f.i] = f.d;
+    normal[3 * f.i] = f.nx;
+    normal[3 * f.i + 1] = f.ny;
+    normal[3 * f.i + 2] = f.nz;
+    cost[f.i] = f.c;
+  }
+  if (filled) *filled = fills.size();
+  return PS_OK;
+}
+
 int oracle_remove_speckles(float* depth, float* normal, const float* cost, uint32_t w, uint32_t h, float rel,
                            double frac, float keep, uint64_t* removed) {
   if (!depth || !normal || !cost) return PS_EINVAL;

@@ -77,3 +77,36 @@ def test_fusion_bitwise_vs_oracle(pipeline):
                         [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views], views[1:], prm)
     assert n2 == len(want2)
     np.testing.assert_array_equal(s.fused_points().keys, want2.keys)
+
+
+@pytest.mark.parametrize("full_k", [True, False])
+def test_fill_holes_bitwise_vs_oracle(full_k):
+    """Speckle removal then hole filling (fill_holes, crates/dense/src/postproc.rs:139-201) on the device readout,
+    against the oracle on the same readout: planes, costs and counts equal bit for bit.  `full_k` passes the
+    cameras' binary64 intrinsics; otherwise the levels' binary32 ones (the oracle gets the same values)."""
+    wl = scenes.workload_small(160, 120, views=6, window_radius=3, seed=23, iters=2, sources=4, positions=2)
+    views = list(range(len(wl.cams)))
+    be = PatchMatchBackend(0, math="parity")
+    with be.begin(wl.input) as s:
+        s.schedule_resident(views, 2, 1, 1, graph=False)
+        before = s.readout_resident(views)
+        post = fusion.default_post()
+        post.speckle_min_area_frac = 0.002
+        post.fill_holes = 1
+        post.fill_max_frac = 0.05
+        ks = np.array([c.k for c in wl.cams], np.float64)
+        if not full_k:
+            ks = ks.astype(np.float32).astype(np.float64)
+        removed, filled = s.postprocess_resident(0, views, post, intrinsics=ks if full_k else None, filled=True)
+        got = s.readout_download(0, views)
+    be.close()
+    want_removed = want_filled = 0
+    for v, (g, st) in enumerate(zip(got, before)):
+        d, n, c = st.depth.copy(), st.normal.copy(), st.cost.copy()
+        want_removed += oracle.remove_speckles(d, n, c, post)
+        want_filled += oracle.fill_holes(d, n, c, st.cost, wl.input.views[v].levels[0].pixels, ks[v], post)
+        np.testing.assert_array_equal(g.depth, d)
+        np.testing.assert_array_equal(g.normal, n)
+        np.testing.assert_array_equal(g.cost, c)
+    assert (removed, filled) == (want_removed, want_filled)
+    assert filled > 0

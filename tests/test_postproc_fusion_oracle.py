@@ -40,6 +40,46 @@ def test_speckle_keeps_low_cost_components_and_defaults():
     assert oracle.remove_speckles(d, n, c, p) == 0  # ceil(1200·2e-4) = 1: off
 
 
+def test_fill_holes_known_answer():
+    """speckle_and_fill (crates/dense/src/postproc.rs:208-234): after the 2×2 speckle is erased, hole filling at
+    flat gray fills its 4 pixels and the 3×3 hole (13 pixels) with the surrounding depth 10."""
+    d, n, c, p = _speckle_case()
+    p.fill_holes = 1
+    p.fill_max_frac = 0.1
+    assert oracle.remove_speckles(d, n, c, p) == 4
+    assert d[5, 5] == 0.0
+    raw = np.full(d.shape, 0.3, np.float32)
+    gray = np.full(d.shape, 100, np.uint8)
+    assert oracle.fill_holes(d, n, c, raw, gray, (50.0, 50.0, 19.5, 14.5), p) == 13
+    assert abs(float(d[21, 21]) - 10.0) < 1e-4
+    assert (d > 0).all() and (n[21, 21] == np.float32([0, 0, -1])).all() and c[21, 21] == np.float32(0.5)
+
+
+def test_fill_holes_defaults_and_gates():
+    p = fusion.default_post()
+    assert (p.fill_holes, p.fill_max_frac, round(p.fill_edge_step, 6), p.fill_max_cost) == (0, 0.01, 0.06, 1.0)
+    d, n, c, p = _speckle_case()
+    p.fill_max_frac = 0.1
+    gray = np.full(d.shape, 100, np.uint8)
+    # a run cost above fill_max_cost keeps a hole pixel empty; a gray edge (jump > 0.06·255) stops the walk
+    raw = np.full(d.shape, 0.3, np.float32)
+    raw[21, 21] = 1.5
+    gray[:, 23:] = 200
+    gray[23:, :] = 200
+    gray[:20, :] = 200
+    gray[:, :20] = 200
+    filled = oracle.fill_holes(d, n, c, raw, gray, (50.0, 50.0, 19.5, 14.5), p)
+    assert d[21, 21] == 0.0
+    assert filled == 0  # every walk from the hole meets the edge before a valid pixel
+
+
+def test_gray_round_trip_of_unit_planes():
+    """The device derives a pixel's 8-bit gray as round(255·v) from the plane value v = correctly rounded u/255."""
+    u = np.arange(256, dtype=np.uint8)
+    v = scenes.unit_plane(u.reshape(16, 16)).ravel().astype(np.float32)
+    assert (np.rint(v * np.float32(255.0)).astype(np.int64) == np.arange(256)).all()
+
+
 def test_speckle_components_do_not_depend_on_scan_order():
     rng = np.random.default_rng(3)
     d = rng.choice([0.0, 10.0, 10.1, 13.0], size=(48, 64), p=[0.3, 0.3, 0.2, 0.2]).astype(np.float32)

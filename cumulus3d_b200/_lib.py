@@ -93,12 +93,17 @@ class PostParams(C.Structure):
                 ("fill_edge_step", C.c_float), ("fill_max_cost", C.c_float)]
 
 
+PS_FUSION_RESIDUAL_NONE, PS_FUSION_RESIDUAL_RELEASE, PS_FUSION_RESIDUAL_SECOND_PASS = 0, 1, 2
+
+
 class FusionParams(C.Structure):
-    """FusionParams of consistency fusion (crates/dense/src/params.rs:286-351)."""
+    """FusionParams of consistency fusion (crates/dense/src/params.rs:264-351), with the residual handling."""
     _fields_ = [("min_consistent_views", C.c_uint32), ("consistency_num_images", C.c_uint32), ("mark_used", C.c_uint32),
-                ("mark_radius", C.c_uint32), ("inverse_variance", C.c_uint32), ("reserved", C.c_uint32),
+                ("mark_radius", C.c_uint32), ("inverse_variance", C.c_uint32), ("residual", C.c_uint32),
                 ("sigma_px0", C.c_double), ("sigma_px_slope", C.c_double), ("max_reproj_error", C.c_double),
-                ("max_depth_error", C.c_double), ("max_normal_error_deg", C.c_double)]
+                ("max_depth_error", C.c_double), ("max_normal_error_deg", C.c_double),
+                ("residual_min_views", C.c_uint32), ("reserved", C.c_uint32), ("residual_depth_error", C.c_double),
+                ("residual_normal_error_deg", C.c_double), ("residual_min_dist_gsd", C.c_double)]
 
 
 class FusionView(C.Structure):
@@ -179,7 +184,7 @@ SIGNATURES = {
                                           C.POINTER(C.c_double), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ps_readout_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_fuse_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView), C.POINTER(FusionParams),
-                                   C.POINTER(C.c_uint64)]),
+                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_uint32]),
     "ps_build_pyramid": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.c_uint32,

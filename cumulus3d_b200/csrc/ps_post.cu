@@ -237,26 +237,27 @@ __device__ __forceinline__ double gray_u8(const FuseView& c, int col, int row) {
   return (double)(unsigned char)fminf(fmaxf(rintf(v), 0.0f), 255.0f);
 }
 
-__global__ void __launch_bounds__(256) k_fuse(FuseArgs A) {
-  const FuseView& cv = A.views[A.v];
-  const int col = blockIdx.x * 32 + threadIdx.x, row = blockIdx.y * 8 + threadIdx.y;
-  if (col >= cv.w || row >= cv.h) return;
-  const long long pix = (long long)row * cv.w + col;
-  const float4 q = A.plane[cv.off + pix];
-  if (!(q.w > 0.0f)) return;
-  if (A.mark_used && A.marks[cv.off + pix] != 0) return;
+// The agreement check of one reference pixel (ConsCtx::evaluate, crates/dense/src/fusion.rs:390-460) under the
+// tolerances of A: the weighted sums of the point and its agreeing (view, pixel) list; false when the normal sum
+// vanishes.
+struct FusePoint {
+  double sx[3], sn[3], sc[3], m, l;
+};
+__device__ bool fuse_eval(const FuseArgs& A, const FuseView& cv, int col, int row, float4 q, Hit* hits, int& nh,
+                          FusePoint& P) {
   const double d = (double)q.w;
   double x[3], nw[3];
   backproject(cv, (double)col, (double)row, d, x);
   normal_world(cv, q, nw);
-  const double w0 = inv_var(A, cv, d, A.cost[cv.off + pix]);
+  const double w0 = inv_var(A, cv, d, A.cost[cv.off + (long long)row * cv.w + col]);
   double sw = w0;
-  double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
-  double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
+  for (int k = 0; k < 3; ++k) {
+    P.sx[k] = x[k] * w0;
+    P.sn[k] = nw[k] * w0;
+  }
   const double c0 = gray_u8(cv, col, row);
-  double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
-  Hit hits[PS_FUSE_MAX_OVERLAP];
-  int nh = 0;
+  P.sc[0] = P.sc[1] = P.sc[2] = c0 * w0;
+  nh = 0;
   for (int i = 0; i < cv.nov; ++i) {
     const int o = cv.ov[i];
     const FuseView& oc = A.views[o];
@@ -281,18 +282,65 @@ __global__ void __launch_bounds__(256) k_fuse(FuseArgs A) {
     const double wo = inv_var(A, oc, od, A.cost[oc.off + opix]);
     sw += wo;
     for (int k = 0; k < 3; ++k) {
-      sx[k] += wo * xo[k];
-      sn[k] += wo * no[k];
-      sc[k] += wo * co;
+      P.sx[k] += wo * xo[k];
+      P.sn[k] += wo * no[k];
+      P.sc[k] += wo * co;
     }
     hits[nh].o = o;
     hits[nh].q = opix;
     nh++;
   }
-  if (nh < A.min_views) return;
-  const double m = sw;
-  const double l = sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
-  if (l < 1.1920928955078125e-07) return;  // f32::EPSILON
+  P.m = sw;
+  P.l = sqrt(P.sn[0] * P.sn[0] + P.sn[1] * P.sn[1] + P.sn[2] * P.sn[2]);
+  return !(P.l < 1.1920928955078125e-07);  // f32::EPSILON
+}
+
+// Writes one fused point (its slot from the shared counter): mean position, normalised normal, rounded colour, key
+// and the sorted, de-duplicated {v} ∪ hit views.
+__device__ void fuse_emit(const FuseArgs& A, const FuseView& cv, int v, int col, int row, const FusePoint& P,
+                          const Hit* hits, int nh) {
+  const unsigned long long slot = atomicAdd(A.count, 1ull);
+  if (slot >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
+  for (int k = 0; k < 3; ++k) {
+    A.pos[3 * slot + k] = (float)(P.sx[k] / P.m);
+    A.nrm[3 * slot + k] = (float)(P.sn[k] / P.l);
+    A.col[3 * slot + k] = (unsigned char)round(P.sc[k] / P.m);
+  }
+  A.key[slot] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
+                (unsigned long long)(col & 0xffff);
+  unsigned short* vis = A.vis + slot * A.vis_stride;
+  int nv = 0;
+  vis[nv++] = (unsigned short)v;
+  for (int i = 0; i < nh; ++i) {
+    const unsigned short o = (unsigned short)hits[i].o;
+    int j = nv;
+    bool dup = false;
+    for (int k = 0; k < nv; ++k) dup = dup || vis[k] == o;
+    if (dup) continue;
+    while (j > 0 && vis[j - 1] > o) {
+      vis[j] = vis[j - 1];
+      --j;
+    }
+    vis[j] = o;
+    nv++;
+  }
+  A.nvis[slot] = (unsigned char)nv;
+}
+
+// First pass (fusion.rs:243-333) of view A.v: one thread per reference pixel.
+__global__ void __launch_bounds__(256) k_fuse(FuseArgs A) {
+  const FuseView& cv = A.views[A.v];
+  const int col = blockIdx.x * 32 + threadIdx.x, row = blockIdx.y * 8 + threadIdx.y;
+  if (col >= cv.w || row >= cv.h) return;
+  const long long pix = (long long)row * cv.w + col;
+  const float4 q = A.plane[cv.off + pix];
+  if (!(q.w > 0.0f)) return;
+  if (A.mark_used && A.marks[cv.off + pix] != 0) return;
+  Hit hits[PS_FUSE_MAX_OVERLAP];
+  int nh;
+  FusePoint P;
+  const bool okp = fuse_eval(A, cv, col, row, q, hits, nh, P);
+  if (nh < A.min_views || !okp) return;
   if (A.mark_used) {
     for (int i = 0; i < nh; ++i) {
       const FuseView& oc = A.views[hits[i].o];
@@ -311,40 +359,190 @@ __global__ void __launch_bounds__(256) k_fuse(FuseArgs A) {
         }
     }
   }
-  const unsigned long long slot = atomicAdd(A.count, 1ull);
-  if (slot >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
-  A.pos[3 * slot + 0] = (float)(sx[0] / m);
-  A.pos[3 * slot + 1] = (float)(sx[1] / m);
-  A.pos[3 * slot + 2] = (float)(sx[2] / m);
-  A.nrm[3 * slot + 0] = (float)(sn[0] / l);
-  A.nrm[3 * slot + 1] = (float)(sn[1] / l);
-  A.nrm[3 * slot + 2] = (float)(sn[2] / l);
-  for (int k = 0; k < 3; ++k) A.col[3 * slot + k] = (unsigned char)round(sc[k] / m);
-  A.key[slot] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
-                (unsigned long long)(col & 0xffff);
-  // visibility: sorted, de-duplicated {v} ∪ hit views
-  unsigned short* vis = A.vis + slot * A.vis_stride;
-  int nv = 0;
-  vis[nv++] = (unsigned short)A.v;
-  for (int i = 0; i < nh; ++i) {
-    const unsigned short o = (unsigned short)hits[i].o;
-    int j = nv;
-    bool dup = false;
-    for (int k = 0; k < nv; ++k) dup = dup || vis[k] == o;
-    if (dup) continue;
-    while (j > 0 && vis[j - 1] > o) {
-      vis[j] = vis[j - 1];
-      --j;
-    }
-    vis[j] = o;
-    nv++;
+  if (A.consumed) {
+    A.consumed[cv.off + pix] = 1;
+    for (int i = 0; i < nh; ++i) A.consumed[A.views[hits[i].o].off + hits[i].q] = 1;
   }
-  A.nvis[slot] = (unsigned char)nv;
+  fuse_emit(A, cv, A.v, col, row, P, hits, nh);
+}
+
+// ---- second pass of leftover pixels (fusion.rs:540-627) ------------------------------------------------------
+__device__ __forceinline__ unsigned long long grid_mix(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+// Slot key of a cell (never 0, the empty marker).  Different cells may share a key; the distance test keeps the
+// result exact, since every point within the cell size lies in one of the 27 cells around.
+__device__ __forceinline__ unsigned long long grid_key(long long cx, long long cy, long long cz) {
+  const unsigned long long h =
+      grid_mix((unsigned long long)cx ^ grid_mix((unsigned long long)cy ^ grid_mix((unsigned long long)cz)));
+  return h ? h : 1ull;
+}
+__device__ __forceinline__ long long grid_cell(float x, double cell) { return (long long)floor((double)x / cell); }
+
+__global__ void __launch_bounds__(256) k_grid_insert(const float* pos, unsigned n, double cell,
+                                                     unsigned long long* keys, unsigned* heads, unsigned* next,
+                                                     unsigned cap, int* overflow) {
+  const unsigned i = blockIdx.x * 256u + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long key = grid_key(grid_cell(pos[3 * i], cell), grid_cell(pos[3 * i + 1], cell),
+                                          grid_cell(pos[3 * i + 2], cell));
+  unsigned slot = (unsigned)(key & (cap - 1));
+  for (unsigned t = 0; t < cap; ++t) {
+    const unsigned long long prev = atomicCAS(&keys[slot], 0ull, key);
+    if (prev == 0ull || prev == key) {
+      next[i] = atomicExch(&heads[slot], i);
+      return;
+    }
+    slot = (slot + 1u) & (cap - 1u);
+  }
+  atomicExch(overflow, 1);  // cannot happen: the table is at most half full
+}
+
+// GridIndex::any_within (fusion.rs:514-536): is a first-pass point within the cell size of x (binary64 distance)?
+__device__ bool grid_any_within(const FuseArgs& A, const float* x) {
+  const long long c0 = grid_cell(x[0], A.gcell), c1 = grid_cell(x[1], A.gcell), c2 = grid_cell(x[2], A.gcell);
+  const double rr = A.gcell * A.gcell;
+  for (int dz = -1; dz <= 1; ++dz)
+    for (int dy = -1; dy <= 1; ++dy)
+      for (int dx = -1; dx <= 1; ++dx) {
+        const unsigned long long key = grid_key(c0 + dx, c1 + dy, c2 + dz);
+        unsigned slot = (unsigned)(key & (A.gcap - 1));
+        for (unsigned t = 0; t < A.gcap; ++t) {
+          const unsigned long long k = A.gkeys[slot];
+          if (k == 0ull) break;
+          if (k == key) {
+            unsigned i = A.gheads[slot];
+            for (unsigned u = 0; u < A.gpoints && i != 0xffffffffu; ++u, i = A.gnext[i]) {
+              const double t0 = (double)A.pos[3 * i] - (double)x[0];
+              const double t1 = (double)A.pos[3 * i + 1] - (double)x[1];
+              const double t2 = (double)A.pos[3 * i + 2] - (double)x[2];
+              if ((t0 * t0 + t1 * t1) + t2 * t2 <= rr) return true;
+            }
+            break;
+          }
+          slot = (slot + 1u) & (A.gcap - 1u);
+        }
+      }
+  return false;
+}
+
+// Stage 1: a leftover pixel (valid, not consumed by the first pass) that agrees with residual_min_views views under
+// the second-pass tolerances and is not within the minimum distance of a first-pass point claims its own pixel and
+// its agreeing pixels with its candidate number (atomic minimum).  Stage 2: a candidate that owns its reference pixel
+// is emitted (only its own candidate writes its number there, so the test also says it was a candidate); its point
+// is evaluated again with the same inputs.
+__global__ void __launch_bounds__(256) k_fuse_second(FuseArgs A, int stage) {
+  const FuseView& cv = A.views[A.v];
+  const int col = blockIdx.x * 32 + threadIdx.x, row = blockIdx.y * 8 + threadIdx.y;
+  if (col >= cv.w || row >= cv.h) return;
+  const long long pix = (long long)row * cv.w + col;
+  const unsigned id = cv.idbase + (unsigned)pix;
+  if (stage == 2 && A.owner[cv.off + pix] != id) return;
+  const float4 q = A.plane[cv.off + pix];
+  if (!(q.w > 0.0f) || A.consumed[cv.off + pix] != 0) return;
+  Hit hits[PS_FUSE_MAX_OVERLAP];
+  int nh;
+  FusePoint P;
+  if (!fuse_eval(A, cv, col, row, q, hits, nh, P)) return;
+  if (nh < A.min_views) return;
+  if (stage == 1) {
+    if (A.gcap) {
+      const float x[3] = {(float)(P.sx[0] / P.m), (float)(P.sx[1] / P.m), (float)(P.sx[2] / P.m)};
+      if (grid_any_within(A, x)) return;
+    }
+    atomicMin(&A.owner[cv.off + pix], id);
+    for (int i = 0; i < nh; ++i) atomicMin(&A.owner[A.views[hits[i].o].off + hits[i].q], id);
+    return;
+  }
+  fuse_emit(A, cv, A.v, col, row, P, hits, nh);
+}
+
+// Every 97th valid depth of a view in row-major order (one CTA of 1024 threads walks the view in chunks with a block
+// scan of the valid flags), then the median of those samples over fx (quantile 0.5: the two middle order statistics,
+// interpolated in binary64) by bisection over order-preserving keys.
+__device__ __forceinline__ unsigned gsd_key(float f) { return __float_as_uint(f) | 0x80000000u; }  // f > 0
+__global__ void __launch_bounds__(1024) k_gsd(const float4* __restrict__ plane, const GsdView* __restrict__ views,
+                                              float* samples, unsigned* scount, double* gsd) {
+  __shared__ unsigned wsum[32];
+  __shared__ unsigned long long red[32];
+  const GsdView V = views[blockIdx.x];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  unsigned g = 0;  // valid pixels before the chunk (uniform)
+  for (int c0 = 0; c0 < V.npix; c0 += 1024) {
+    const int i = c0 + tid;
+    float d = 0.f;
+    const bool valid = i < V.npix && (d = plane[V.off + i].w) > 0.0f;
+    const unsigned b = __ballot_sync(0xffffffffu, valid);
+    if (lane == 0) wsum[warp] = __popc(b);
+    __syncthreads();
+    unsigned before = 0, total = 0;
+    for (int w = 0; w < 32; ++w) {
+      if (w < warp) before += wsum[w];
+      total += wsum[w];
+    }
+    const unsigned e = g + before + __popc(b & ((1u << lane) - 1u));
+    if (valid && e % 97u == 0u) samples[V.soff + e / 97u] = d;
+    g += total;
+    __syncthreads();
+  }
+  const unsigned m = (g + 96u) / 97u;
+  if (tid == 0) scount[blockIdx.x] = m;
+  if (m == 0) {
+    if (tid == 0) gsd[blockIdx.x] = __longlong_as_double(0x7ff8000000000000ll);  // NaN: no valid depth
+    return;
+  }
+  __syncthreads();
+  const float* seg = samples + V.soff;
+  const double pos = 0.5 * (double)(m - 1u);
+  const unsigned lo = (unsigned)floor(pos), hi = min(lo + 1u, m - 1u);
+  double val[2];
+  for (int s2 = 0; s2 < 2; ++s2) {
+    const unsigned k = s2 == 0 ? lo : hi;
+    unsigned a = 0u, bnd = 0xffffffffu;
+    while (a < bnd) {
+      const unsigned mid = a + (bnd - a) / 2u;
+      unsigned long long c = 0;
+      for (unsigned j = tid; j < m; j += 1024u) c += gsd_key(seg[j]) <= mid;
+      for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+      __syncthreads();
+      if (lane == 0) red[warp] = c;
+      __syncthreads();
+      unsigned long long tot = 0;
+      for (int w = 0; w < 32; ++w) tot += red[w];
+      if (tot >= (unsigned long long)k + 1ull) bnd = mid;
+      else a = mid + 1u;
+    }
+    val[s2] = (double)__uint_as_float(a & 0x7fffffffu);
+  }
+  if (tid == 0) gsd[blockIdx.x] = (val[0] + (val[1] - val[0]) * (pos - (double)lo)) / V.fx;
 }
 
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st) {
   const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
   k_fuse<<<g, b, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fuse_second(const FuseArgs& A, int w, int h, int stage, cudaStream_t st) {
+  const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+  k_fuse_second<<<g, b, 0, st>>>(A, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gsd(const float4* plane, const GsdView* views, int nviews, float* samples, unsigned* scount,
+                       double* gsd, cudaStream_t st) {
+  if (nviews <= 0) return cudaSuccess;
+  k_gsd<<<nviews, 1024, 0, st>>>(plane, views, samples, scount, gsd);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_insert(const float* pos, unsigned n, double cell, unsigned long long* keys, unsigned* heads,
+                               unsigned* next, unsigned cap, int* overflow, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  k_grid_insert<<<(n + 255) / 256, 256, 0, st>>>(pos, n, cell, keys, heads, next, cap, overflow);
   return cudaGetLastError();
 }
 

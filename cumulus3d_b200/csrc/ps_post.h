@@ -39,6 +39,7 @@ struct FuseView {
   long long off;         // slot offset of the view's depth map
   int w, h, pitch;
   unsigned image_id;
+  unsigned idbase;       // second pass: candidate number of the view's first pixel (prefix of the fused views' sizes)
   int nov;               // overlap views to check, in order
   int ov[PS_FUSE_MAX_OVERLAP];
 };
@@ -60,6 +61,22 @@ struct FuseArgs {
   int vis_stride;
   unsigned long long* count;
   unsigned long long capacity;
+  // second pass of leftover pixels (fusion.rs:540-627)
+  unsigned char* consumed;          // first pass: reference and agreeing pixels of adopted points (NULL: not kept)
+  unsigned* owner;                  // smallest candidate number claiming each slot pixel
+  const unsigned long long* gkeys;  // spatial hash of first-pass points (gcap slots, 0 = empty)
+  const unsigned* gheads;           // first point of each slot's chain (0xffffffff: none)
+  const unsigned* gnext;            // next point of the same slot
+  unsigned gcap, gpoints;           // gcap = 0: no distance test
+  double gcell;                     // cell size = minimum distance
+};
+
+// Median sampling of the ground sample distance (depth_gsd, fusion.rs:469-487), one CTA per view.
+struct GsdView {
+  long long off;       // slot offset of the view's readout planes
+  long long soff;      // first sample slot
+  int npix;
+  double fx;
 };
 
 // Hole filling of one view's readout planes (fill_holes, crates/dense/src/postproc.rs:139-201).
@@ -79,6 +96,14 @@ cudaError_t launch_fill_holes(const FillArgs& A, cudaStream_t st);
 cudaError_t launch_speckles(const SpkArgs& A, int ntiles, cudaStream_t st, int* launches);
 cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);
+// second pass: stage 1 (candidates claim their pixels) and stage 2 (owners of their reference pixel are emitted)
+cudaError_t launch_fuse_second(const FuseArgs& A, int w, int h, int stage, cudaStream_t st);
+// per view: every 97th valid depth in row-major order, then their median over fx (gsd[i]; NaN when the view has none)
+cudaError_t launch_gsd(const float4* plane, const GsdView* views, int nviews, float* samples, unsigned* scount,
+                       double* gsd, cudaStream_t st);
+// spatial hash of `n` points (positions x,y,z) with cells of size `cell` into a table of `cap` slots (a power of 2)
+cudaError_t launch_grid_insert(const float* pos, unsigned n, double cell, unsigned long long* keys, unsigned* heads,
+                               unsigned* next, unsigned cap, int* overflow, cudaStream_t st);
 cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g, cudaStream_t st);
 // 8-bit image (w × h, tight rows) -> f32 plane rows of `pitch` floats through a 256-entry table.
 cudaError_t launch_u8_plane(const unsigned char* in, int w, int h, const float* lut, float* out, int pitch,

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 #include <omp.h>
 #include <algorithm>
+#include <limits>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -94,12 +95,13 @@ struct Slot {
   std::vector<char> proposal_valid;
   int* spk = nullptr;          // speckle removal: parent, size, lo, hi, cnt per pixel (5 ints each, lazily)
   unsigned char* marks = nullptr;  // fusion "used" marks
+  unsigned char* consumed = nullptr;  // fusion second pass: pixels used by first-pass points
   float* cinit = nullptr;          // multi-scale driver: cost of the upsampled planes
 };
 
 // Fused point cloud of the last ps_fuse_resident call (device).
 struct FusedCloud {
-  unsigned long long cap = 0, count = 0;
+  unsigned long long cap = 0, count = 0, count1 = 0;  // count1: points of the first pass (they come first)
   int vis_stride = 0;
   float* pos = nullptr;
   float* nrm = nullptr;
@@ -979,6 +981,7 @@ int ps_end(ps_session* s) {
     dfree(s, sl.pconf);
     dfree(s, sl.spk);
     dfree(s, sl.marks);
+    dfree(s, sl.consumed);
     dfree(s, sl.cinit);
   }
   s->fused.release([s](void* q) { dfree(s, q); });
@@ -1835,6 +1838,11 @@ void ps_fusion_params_default(ps_fusion_params* out) {
   out->max_reproj_error = 2.0;
   out->max_depth_error = 0.01;
   out->max_normal_error_deg = 10.0;
+  out->residual = PS_FUSION_RESIDUAL_NONE;
+  out->residual_min_views = 2;
+  out->residual_depth_error = std::numeric_limits<double>::quiet_NaN();
+  out->residual_normal_error_deg = std::numeric_limits<double>::quiet_NaN();
+  out->residual_min_dist_gsd = 0.5;
 }
 
 int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
@@ -1920,9 +1928,11 @@ int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views
 }
 
 int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
-                     const ps_fusion_params* p, uint64_t* num_points) {
+                     const ps_fusion_params* p, uint64_t* num_points, uint64_t* num_residual) {
   return guard(s, [&] {
     if (!p || (n && !cams)) fail(PS_EINVAL, "params or cams is NULL");
+    if (p->residual > PS_FUSION_RESIDUAL_SECOND_PASS) fail(PS_EINVAL, "residual must be 0, 1 or 2");
+    const bool second = p->residual == PS_FUSION_RESIDUAL_SECOND_PASS;
     check_views(s, views, n);
     if (s->nv > 65535) fail(PS_EINVAL, "fusion supports at most 65535 views");
     if (p->consistency_num_images > PS_FUSE_MAX_OVERLAP)
@@ -2018,6 +2028,11 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     std::vector<uint32_t> order(views, views + n);
     std::sort(order.begin(), order.end());  // the reference walks views in index order
     order.erase(std::unique(order.begin(), order.end()), order.end());
+    if (second) {
+      if (!sl.consumed) sl.consumed = dalloc<unsigned char>(s, std::max<long long>(sl.total, 1));
+      cuda_ok(cudaMemsetAsync(sl.consumed, 0, std::max<long long>(sl.total, 1), s->st), "memset");
+      A.consumed = sl.consumed;
+    }
     for (uint32_t v : order) {
       A.v = (int)v;
       cuda_ok(ps_post::launch_fuse(A, s->W(v, l), s->H(v, l), s->st), "fusion kernel");
@@ -2026,8 +2041,107 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     unsigned long long cnt = 0;
     cuda_ok(cudaMemcpyAsync(&cnt, fc.counter, sizeof cnt, cudaMemcpyDeviceToHost, s->st), "read count");
     sync(s);
+    fc.count1 = std::min(cnt, fc.cap);
+    if (second) {
+      // ground sample distance (depth_gsd, fusion.rs:469-487) of the fused views, in index order
+      std::vector<ps_post::GsdView> gv(order.size());
+      long long soff = 0;
+      for (size_t i = 0; i < order.size(); ++i) {
+        const int v = (int)order[i];
+        gv[i].off = sl.off[v];
+        gv[i].npix = s->W(v, l) * s->H(v, l);
+        gv[i].soff = soff;
+        gv[i].fx = cams[v].k[0];
+        soff += (gv[i].npix + 96) / 97;
+      }
+      ps_post::GsdView* dgv = dalloc<ps_post::GsdView>(s, gv.size());
+      float* samples = dalloc<float>(s, std::max<long long>(soff, 1));
+      unsigned* scount = dalloc<unsigned>(s, gv.size());
+      double* dgsd = dalloc<double>(s, gv.size());
+      cuda_ok(cudaMemcpyAsync(dgv, gv.data(), gv.size() * sizeof(ps_post::GsdView), cudaMemcpyHostToDevice, s->st),
+              "upload gsd views");
+      launched(s, ps_post::launch_gsd(sl.aux, dgv, (int)gv.size(), samples, scount, dgsd, s->st), "gsd kernel");
+      std::vector<double> gs(gv.size());
+      cuda_ok(cudaMemcpyAsync(gs.data(), dgsd, gs.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st), "read gsd");
+      sync(s);
+      dfree(s, dgv);
+      dfree(s, samples);
+      dfree(s, scount);
+      dfree(s, dgsd);
+      std::vector<double> g2;
+      for (double x : gs)
+        if (!std::isnan(x)) g2.push_back(x);
+      double gsd = 0.0;
+      if (!g2.empty()) {  // median_in_place (crates/dense/src/math.rs:137-141)
+        std::sort(g2.begin(), g2.end());
+        const double pos = 0.5 * (double)(g2.size() - 1);
+        const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, g2.size() - 1);
+        gsd = g2[lo] + (g2[hi] - g2[lo]) * (pos - (double)lo);
+      }
+      const double min_dist = p->residual_min_dist_gsd * gsd;
+      // candidate numbers: prefix of the fused views' pixel counts in index order (fusion.rs:560-565)
+      std::vector<ps_post::FuseView> fv2 = fv;
+      unsigned long long base = 0;
+      for (int v = 0; v < s->nv; ++v) {
+        fv2[v].idbase = (unsigned)base;
+        if (used[v]) base += (unsigned long long)s->W(v, l) * s->H(v, l);
+      }
+      if (base >= 0xffffffffull) fail(PS_EINVAL, "second pass: more than 2^32 - 1 pixels");
+      cuda_ok(cudaMemcpyAsync(fc.views, fv2.data(), fv2.size() * sizeof(ps_post::FuseView), cudaMemcpyHostToDevice,
+                              s->st),
+              "upload fusion views");
+      unsigned* owner = dalloc<unsigned>(s, std::max<long long>(sl.total, 1));
+      cuda_ok(cudaMemsetAsync(owner, 0xff, std::max<long long>(sl.total, 1) * sizeof(unsigned), s->st), "memset");
+      unsigned long long* gkeys = nullptr;
+      unsigned *gheads = nullptr, *gnext = nullptr;
+      int* overflow = nullptr;
+      unsigned cap = 0;
+      const unsigned n1 = (unsigned)fc.count1;
+      if (min_dist > 0.0 && n1 > 0) {
+        cap = 1024;
+        while (cap < 2u * n1) cap <<= 1;
+        gkeys = dalloc<unsigned long long>(s, cap);
+        gheads = dalloc<unsigned>(s, cap);
+        gnext = dalloc<unsigned>(s, n1);
+        overflow = dalloc<int>(s, 1);
+        cuda_ok(cudaMemsetAsync(gkeys, 0, cap * sizeof(unsigned long long), s->st), "memset");
+        cuda_ok(cudaMemsetAsync(gheads, 0xff, cap * sizeof(unsigned), s->st), "memset");
+        cuda_ok(cudaMemsetAsync(overflow, 0, sizeof(int), s->st), "memset");
+        launched(s, ps_post::launch_grid_insert(fc.pos, n1, min_dist, gkeys, gheads, gnext, cap, overflow, s->st),
+                 "grid kernel");
+      }
+      ps_post::FuseArgs B = A;
+      B.depth_tol = std::isnan(p->residual_depth_error) ? 0.5 * p->max_depth_error : p->residual_depth_error;
+      B.cos_n = std::cos(ps_to_radians_f64(std::isnan(p->residual_normal_error_deg) ? 0.67 * p->max_normal_error_deg
+                                                                                    : p->residual_normal_error_deg));
+      B.min_views = (int)p->residual_min_views;
+      B.owner = owner;
+      B.gkeys = gkeys;
+      B.gheads = gheads;
+      B.gnext = gnext;
+      B.gcap = cap;
+      B.gpoints = n1;
+      B.gcell = min_dist;
+      for (int stage = 1; stage <= 2; ++stage)
+        for (uint32_t v : order) {
+          B.v = (int)v;
+          cuda_ok(ps_post::launch_fuse_second(B, s->W(v, l), s->H(v, l), stage, s->st), "second-pass kernel");
+          s->launches++;
+        }
+      int ovf = 0;
+      cuda_ok(cudaMemcpyAsync(&cnt, fc.counter, sizeof cnt, cudaMemcpyDeviceToHost, s->st), "read count");
+      if (overflow) cuda_ok(cudaMemcpyAsync(&ovf, overflow, sizeof ovf, cudaMemcpyDeviceToHost, s->st), "read flag");
+      sync(s);
+      dfree(s, owner);
+      dfree(s, gkeys);
+      dfree(s, gheads);
+      dfree(s, gnext);
+      dfree(s, overflow);
+      if (ovf) fail(PS_ECUDA, "second pass: spatial hash table full");
+    }
     fc.count = std::min(cnt, fc.cap);
     if (num_points) *num_points = fc.count;
+    if (num_residual) *num_residual = fc.count - fc.count1;
   });
 }
 
@@ -2051,10 +2165,12 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
       cuda_ok(cudaMemcpyAsync(vv.data(), fc.vis, 2 * n * fc.vis_stride, cudaMemcpyDeviceToHost, s->st), "download");
     }
     sync(s);
-    // points in the reference's order: ascending key (view, row, column)
+    // points in the reference's order: the first pass, then the second, each in ascending key (view, row, column)
     std::vector<size_t> idx(n);
     for (size_t i = 0; i < n; ++i) idx[i] = i;
-    std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
+    const size_t n1 = std::min<size_t>(fc.count1, n);
+    std::sort(idx.begin(), idx.begin() + n1, [&](size_t a, size_t b) { return k[a] < k[b]; });
+    std::sort(idx.begin() + n1, idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
     for (size_t j = 0; j < n; ++j) {
       const size_t i = idx[j];
       if (positions) memcpy(positions + 3 * j, &p[3 * i], 12);

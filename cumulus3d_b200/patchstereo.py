@@ -411,10 +411,11 @@ class PatchMatchSession:
         """Consistency fusion of the readout planes of `views`; `cams` is a fusion.FusionCams of every view."""
         from .fusion import default_fusion
         p = params if params is not None else default_fusion()
-        n = C.c_uint64()
+        n, r = C.c_uint64(), C.c_uint64()
         self._check(self.lib.ps_fuse_resident(self.h, level, _views(views), len(views), cams.table, C.byref(p),
-                                              C.byref(n)))
+                                              C.byref(n), C.byref(r)))
         self._fused = (int(n.value), int(p.consistency_num_images) + 1)
+        self.fused_residual = int(r.value)  # points added by the second pass (they come last)
         return int(n.value)
 
     def fused_points(self):

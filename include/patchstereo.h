@@ -413,19 +413,33 @@ int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views
 /* Downloads the current readout planes (after any post-processing) and final costs of `views` at `level` without
  * recomputing the readout. */
 int ps_readout_download(ps_session* s, uint32_t level, const uint32_t* views, size_t n, ps_view_state* out);
-/* FusionParams of consistency fusion (crates/dense/src/params.rs:286-351; residual handling "none"). */
+/* FusionParams of consistency fusion (crates/dense/src/params.rs:264-351) with its handling of leftover pixels
+ * (FusionResidual): none; release (the same result as none: fusion.rs:212-214 keeps marks only for adopted points);
+ * second pass (fusion.rs:215-218, 540-627): pixels that were neither the reference nor an agreeing pixel of a
+ * first-pass point are checked again with the residual tolerances (depth NaN = 0.5 × max_depth_error, normal NaN =
+ * 0.67 × max_normal_error_deg) and residual_min_views; a candidate within residual_min_dist_gsd × GSD of a first-pass
+ * point is dropped (GSD: the median over views of the median of every 97th valid depth over fx); candidates take
+ * their pixels with the smallest candidate number and only those that own their reference pixel are kept. */
+#define PS_FUSION_RESIDUAL_NONE 0u
+#define PS_FUSION_RESIDUAL_RELEASE 1u
+#define PS_FUSION_RESIDUAL_SECOND_PASS 2u
 typedef struct ps_fusion_params {
   uint32_t min_consistent_views;   /* 5 */
   uint32_t consistency_num_images; /* 12 (at most 32) */
   uint32_t mark_used;              /* true */
   uint32_t mark_radius;            /* 0 */
   uint32_t inverse_variance;       /* true */
-  uint32_t reserved;
+  uint32_t residual;               /* PS_FUSION_RESIDUAL_NONE */
   double sigma_px0;                /* 0.25 */
   double sigma_px_slope;           /* 1.0 */
   double max_reproj_error;         /* 2.0 px */
   double max_depth_error;          /* 0.01 relative */
   double max_normal_error_deg;     /* 10 */
+  uint32_t residual_min_views;       /* 2 */
+  uint32_t reserved;
+  double residual_depth_error;       /* NaN */
+  double residual_normal_error_deg;  /* NaN */
+  double residual_min_dist_gsd;      /* 0.5 */
 } ps_fusion_params;
 void ps_fusion_params_default(ps_fusion_params* out);
 /* Camera of one view for fusion (DenseView, crates/dense/src/scene.rs): world -> camera x_c = R x_w + t with R
@@ -443,12 +457,14 @@ typedef struct ps_fusion_view {
 } ps_fusion_view;
 /* Consistency fusion (crates/dense/src/fusion.rs:219-459) of the readout planes and final costs of `views` at
  * `level`; cams[v] for every session view v (only the listed views are used).  Views are fused in index order.  The
- * point cloud stays in the session; num_points receives its size.  Colours are the gray image value as u8. */
+ * point cloud stays in the session; num_points receives its size and num_residual (may be NULL) how many of them
+ * the second pass added (FusionOutput::residual).  Colours are the gray image value as u8. */
 int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
-                     const ps_fusion_params* p, uint64_t* num_points);
-/* The fused points in the reference's order (ascending point key (image_id << 32) | (row << 16) | col): positions
- * and normals 3 floats, colours 3 bytes, keys, the number of contributing views and their indices (ascending,
- * vis_stride >= consistency_num_images + 1 entries per point).  Any output may be NULL. */
+                     const ps_fusion_params* p, uint64_t* num_points, uint64_t* num_residual);
+/* The fused points in the reference's order: the first pass in ascending point key (image_id << 32) | (row << 16) |
+ * col, then the second-pass points in ascending key: positions and normals 3 floats, colours 3 bytes, keys, the
+ * number of contributing views and their indices (ascending, vis_stride >= consistency_num_images + 1 entries per
+ * point).  Any output may be NULL. */
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride);
 

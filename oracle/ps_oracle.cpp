@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <map>
 #include <vector>
 
 #include "../cumulus3d_b200/csrc/ps_consts.h"
@@ -1401,8 +1402,9 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
                 const float* const* depth, const float* const* normal, const float* const* cost,
                 const float* const* img, const uint8_t* used, const ps_fusion_params* p, int threads,
                 uint64_t capacity, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
-                uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count) {
+                uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count, uint64_t* residual_count) {
   if (!cams || !widths || !heights || !depth || !normal || !cost || !img || !used || !p || !count) return PS_EINVAL;
+  if (p->residual > PS_FUSION_RESIDUAL_SECOND_PASS) return PS_EINVAL;
   set_threads(threads);
   std::vector<FCam> fc(nviews);
   for (uint32_t v = 0; v < nviews; ++v) {
@@ -1413,20 +1415,88 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
     fc[v].w = (int)widths[v];
     fc[v].h = (int)heights[v];
   }
-  std::vector<std::vector<uint8_t>> marks(nviews);
+  const bool second = p->residual == PS_FUSION_RESIDUAL_SECOND_PASS;
+  std::vector<std::vector<uint8_t>> marks(nviews), consumed(nviews);
   for (uint32_t v = 0; v < nviews; ++v)
-    if (used[v]) marks[v].assign((size_t)fc[v].w * fc[v].h, 0);
-  const double cos_n = std::cos(ps_to_radians_f64(p->max_normal_error_deg));
+    if (used[v]) {
+      marks[v].assign((size_t)fc[v].w * fc[v].h, 0);
+      if (second) consumed[v].assign((size_t)fc[v].w * fc[v].h, 0);
+    }
+  std::vector<std::vector<int>> ovs(nviews);
+  for (uint32_t v = 0; v < nviews; ++v) {
+    if (!used[v]) continue;
+    for (uint32_t j = 0; j < cams[v].num_overlap && ovs[v].size() < p->consistency_num_images; ++j) {
+      const uint32_t o = cams[v].overlap[j];
+      if (o < nviews && used[o] && o != v) ovs[v].push_back((int)o);
+    }
+  }
   const double r2 = p->max_reproj_error * p->max_reproj_error;
-  uint64_t n_out = 0;
+  // ConsCtx::evaluate (fusion.rs:390-460): the weighted mean point of the reference pixel and the agreeing pixels of
+  // its overlap views under the tolerances (depth_tol, cos_n); false when the normal sum vanishes.
+  auto evaluate = [&](uint32_t v, int row, int col, double depth_tol, double cos_n,
+                      std::vector<std::pair<int, int>>& hits, FPoint& pt) -> bool {
+    const FCam& cv = fc[v];
+    const size_t pix = (size_t)row * cv.w + col;
+    const double d = (double)depth[v][pix];
+    double x[3], nw[3];
+    f_backproject(cv, (double)col, (double)row, d, x);
+    f_normal(cv, normal[v] + 3 * pix, nw);
+    const double w0 = f_inv_var(*p, cv, d, cost[v][pix]);
+    double sw = w0;
+    double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
+    double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
+    const double c0 = f_gray(img[v], cv, col, row);
+    double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
+    hits.clear();
+    for (int o : ovs[v]) {
+      const FCam& oc = fc[o];
+      double u, vv, z;
+      if (!f_project(oc, x, &u, &vv, &z)) continue;
+      const double cu = std::floor(u + 0.5), rv = std::floor(vv + 0.5);
+      if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
+      const size_t opix = (size_t)rv * oc.w + (size_t)cu;
+      const double od = (double)depth[o][opix];
+      if (od <= 0.0 || std::fabs(z - od) / od > depth_tol) continue;
+      double xo[3];
+      f_backproject(oc, cu, rv, od, xo);
+      double bu, bv, bz;
+      if (!f_project(cv, xo, &bu, &bv, &bz)) continue;
+      const double eu = bu - (double)col, ev = bv - (double)row;
+      if (eu * eu + ev * ev > r2) continue;
+      double no[3];
+      f_normal(oc, normal[o] + 3 * opix, no);
+      if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < cos_n) continue;
+      const double co = f_gray(img[o], oc, (int)cu, (int)rv);
+      const double wo = f_inv_var(*p, oc, od, cost[o][opix]);
+      sw += wo;
+      for (int k = 0; k < 3; ++k) {
+        sx[k] += wo * xo[k];
+        sn[k] += wo * no[k];
+        sc[k] += wo * co;
+      }
+      hits.push_back({o, (int)opix});
+    }
+    const double m = sw;
+    const double l = std::sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+    if (l < 1.1920928955078125e-07) return false;
+    for (int k = 0; k < 3; ++k) {
+      pt.pos[k] = (float)(sx[k] / m);
+      pt.nrm[k] = (float)(sn[k] / l);
+      pt.col[k] = (uint8_t)std::round(sc[k] / m);
+    }
+    pt.key = ((uint64_t)cams[v].image_id << 32) | ((uint64_t)(row & 0xffff) << 16) | (uint64_t)(col & 0xffff);
+    pt.vis.assign(1, (uint16_t)v);
+    for (auto& hq : hits) pt.vis.push_back((uint16_t)hq.first);
+    std::sort(pt.vis.begin(), pt.vis.end());
+    pt.vis.erase(std::unique(pt.vis.begin(), pt.vis.end()), pt.vis.end());
+    return true;
+  };
+  // first pass (fusion.rs:243-333): views in index order, pixels independent within a view
+  const double cos_n = std::cos(ps_to_radians_f64(p->max_normal_error_deg));
+  std::vector<FPoint> out1, out2;
   for (uint32_t v = 0; v < nviews; ++v) {
     if (!used[v]) continue;
     const FCam& cv = fc[v];
-    std::vector<int> ov;
-    for (uint32_t j = 0; j < cams[v].num_overlap && ov.size() < p->consistency_num_images; ++j) {
-      const uint32_t o = cams[v].overlap[j];
-      if (o < nviews && used[o] && o != v) ov.push_back((int)o);
-    }
     std::vector<std::vector<FPoint>> rows(cv.h);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int row = 0; row < cv.h; ++row) {
@@ -1435,49 +1505,9 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
         const size_t pix = (size_t)row * cv.w + col;
         if (depth[v][pix] <= 0.0f) continue;
         if (p->mark_used && __atomic_load_n(&marks[v][pix], __ATOMIC_RELAXED) != 0) continue;
-        const double d = (double)depth[v][pix];
-        double x[3], nw[3];
-        f_backproject(cv, (double)col, (double)row, d, x);
-        f_normal(cv, normal[v] + 3 * pix, nw);
-        const double w0 = f_inv_var(*p, cv, d, cost[v][pix]);
-        double sw = w0;
-        double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
-        double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
-        const double c0 = f_gray(img[v], cv, col, row);
-        double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
-        hits.clear();
-        for (int o : ov) {
-          const FCam& oc = fc[o];
-          double u, vv, z;
-          if (!f_project(oc, x, &u, &vv, &z)) continue;
-          const double cu = std::floor(u + 0.5), rv = std::floor(vv + 0.5);
-          if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
-          const size_t opix = (size_t)rv * oc.w + (size_t)cu;
-          const double od = (double)depth[o][opix];
-          if (od <= 0.0 || std::fabs(z - od) / od > p->max_depth_error) continue;
-          double xo[3];
-          f_backproject(oc, cu, rv, od, xo);
-          double bu, bv, bz;
-          if (!f_project(cv, xo, &bu, &bv, &bz)) continue;
-          const double eu = bu - (double)col, ev = bv - (double)row;
-          if (eu * eu + ev * ev > r2) continue;
-          double no[3];
-          f_normal(oc, normal[o] + 3 * opix, no);
-          if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < cos_n) continue;
-          const double co = f_gray(img[o], oc, (int)cu, (int)rv);
-          const double wo = f_inv_var(*p, oc, od, cost[o][opix]);
-          sw += wo;
-          for (int k = 0; k < 3; ++k) {
-            sx[k] += wo * xo[k];
-            sn[k] += wo * no[k];
-            sc[k] += wo * co;
-          }
-          hits.push_back({o, (int)opix});
-        }
-        if (hits.size() < p->min_consistent_views) continue;
-        const double m = sw;
-        const double l = std::sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
-        if (l < 1.1920928955078125e-07) continue;
+        FPoint pt;
+        const bool okp = evaluate(v, row, col, p->max_depth_error, cos_n, hits, pt);
+        if (hits.size() < p->min_consistent_views || !okp) continue;
         if (p->mark_used) {
           for (auto& hq : hits) {
             const FCam& oc = fc[hq.first];
@@ -1496,35 +1526,124 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
               }
           }
         }
-        FPoint pt;
-        for (int k = 0; k < 3; ++k) {
-          pt.pos[k] = (float)(sx[k] / m);
-          pt.nrm[k] = (float)(sn[k] / l);
-          pt.col[k] = (uint8_t)std::round(sc[k] / m);
+        if (second) {
+          __atomic_store_n(&consumed[v][pix], (uint8_t)1, __ATOMIC_RELAXED);
+          for (auto& hq : hits) __atomic_store_n(&consumed[hq.first][hq.second], (uint8_t)1, __ATOMIC_RELAXED);
         }
-        pt.key = ((uint64_t)cams[v].image_id << 32) | ((uint64_t)(row & 0xffff) << 16) | (uint64_t)(col & 0xffff);
-        pt.vis.push_back((uint16_t)v);
-        for (auto& hq : hits) pt.vis.push_back((uint16_t)hq.first);
-        std::sort(pt.vis.begin(), pt.vis.end());
-        pt.vis.erase(std::unique(pt.vis.begin(), pt.vis.end()), pt.vis.end());
         rows[row].push_back(std::move(pt));
       }
     }
     for (auto& r : rows)
-      for (auto& pt : r) {
-        if (n_out < capacity) {
-          if (positions) memcpy(positions + 3 * n_out, pt.pos, 12);
-          if (normals) memcpy(normals + 3 * n_out, pt.nrm, 12);
-          if (colors) memcpy(colors + 3 * n_out, pt.col, 3);
-          if (keys) keys[n_out] = pt.key;
-          if (vis_counts) vis_counts[n_out] = (uint8_t)pt.vis.size();
-          if (vis)
-            for (uint32_t t = 0; t < vis_stride; ++t) vis[n_out * vis_stride + t] = t < pt.vis.size() ? pt.vis[t] : 0;
-        }
-        n_out++;
-      }
+      for (auto& pt : r) out1.push_back(std::move(pt));
   }
+  if (second) {
+    // second_pass (fusion.rs:540-627)
+    const double dtol2 = std::isnan(p->residual_depth_error) ? 0.5 * p->max_depth_error : p->residual_depth_error;
+    const double ndeg2 =
+        std::isnan(p->residual_normal_error_deg) ? 0.67 * p->max_normal_error_deg : p->residual_normal_error_deg;
+    const double cos2 = std::cos(ps_to_radians_f64(ndeg2));
+    // depth_gsd (fusion.rs:469-487): per used view the median of every 97th valid depth (row-major) over fx, then
+    // the median of those; median = quantile_sorted(·, 0.5)
+    auto median = [](std::vector<double>& a) {
+      std::sort(a.begin(), a.end());
+      const double pos = 0.5 * (double)(a.size() - 1);
+      const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, a.size() - 1);
+      return a[lo] + (a[hi] - a[lo]) * (pos - (double)lo);
+    };
+    std::vector<double> gs;
+    for (uint32_t v = 0; v < nviews; ++v) {
+      if (!used[v]) continue;
+      std::vector<double> dd;
+      size_t k = 0;
+      for (size_t i = 0; i < (size_t)fc[v].w * fc[v].h; ++i)
+        if (depth[v][i] > 0.0f) {
+          if (k % 97 == 0) dd.push_back((double)depth[v][i]);
+          ++k;
+        }
+      if (dd.empty()) continue;
+      gs.push_back(median(dd) / fc[v].k[0]);
+    }
+    const double gsd = gs.empty() ? 0.0 : median(gs);
+    const double min_dist = p->residual_min_dist_gsd * gsd;
+    // exact neighbourhood test of first-pass points: cells of size min_dist, the 27 cells around
+    std::map<std::array<long long, 3>, std::vector<uint32_t>> grid;
+    auto cell_of = [&](const float* x) {
+      return std::array<long long, 3>{(long long)std::floor((double)x[0] / min_dist),
+                                      (long long)std::floor((double)x[1] / min_dist),
+                                      (long long)std::floor((double)x[2] / min_dist)};
+    };
+    if (min_dist > 0.0)
+      for (uint32_t i = 0; i < out1.size(); ++i) grid[cell_of(out1[i].pos)].push_back(i);
+    auto any_within = [&](const float* x) {
+      const auto c = cell_of(x);
+      const double rr = min_dist * min_dist;
+      for (long long dz = -1; dz <= 1; ++dz)
+        for (long long dy = -1; dy <= 1; ++dy)
+          for (long long dx = -1; dx <= 1; ++dx) {
+            auto it = grid.find({c[0] + dx, c[1] + dy, c[2] + dz});
+            if (it == grid.end()) continue;
+            for (uint32_t i : it->second) {
+              const float* q = out1[i].pos;
+              double d2 = 0.0;
+              for (int a2 = 0; a2 < 3; ++a2) {
+                const double t = (double)q[a2] - (double)x[a2];
+                d2 = d2 + t * t;
+              }
+              if (d2 <= rr) return true;
+            }
+          }
+      return false;
+    };
+    std::vector<uint64_t> offset(nviews + 1, 0);
+    for (uint32_t v = 0; v < nviews; ++v)
+      offset[v + 1] = offset[v] + (used[v] ? (uint64_t)fc[v].w * fc[v].h : 0);
+    if (offset[nviews] >= 0xffffffffull) return PS_EINVAL;
+    std::vector<std::vector<uint32_t>> owner(nviews);
+    for (uint32_t v = 0; v < nviews; ++v)
+      if (used[v]) owner[v].assign((size_t)fc[v].w * fc[v].h, 0xffffffffu);
+    struct Cand {
+      uint32_t v;
+      size_t pix;
+      FPoint pt;
+    };
+    std::vector<Cand> cands;
+    std::vector<std::pair<int, int>> hits;
+    for (uint32_t v = 0; v < nviews; ++v) {
+      if (!used[v]) continue;
+      const FCam& cv = fc[v];
+      for (int row = 0; row < cv.h; ++row)
+        for (int col = 0; col < cv.w; ++col) {
+          const size_t pix = (size_t)row * cv.w + col;
+          if (depth[v][pix] <= 0.0f || consumed[v][pix] != 0) continue;
+          FPoint pt;
+          if (!evaluate(v, row, col, dtol2, cos2, hits, pt)) continue;
+          if (hits.size() < p->residual_min_views) continue;
+          if (min_dist > 0.0 && any_within(pt.pos)) continue;
+          const uint32_t id = (uint32_t)(offset[v] + pix);
+          owner[v][pix] = std::min(owner[v][pix], id);
+          for (auto& hq : hits) owner[hq.first][hq.second] = std::min(owner[hq.first][hq.second], id);
+          cands.push_back({v, pix, std::move(pt)});
+        }
+    }
+    for (auto& c : cands)
+      if (owner[c.v][c.pix] == (uint32_t)(offset[c.v] + c.pix)) out2.push_back(std::move(c.pt));
+  }
+  uint64_t n_out = 0;
+  for (std::vector<FPoint>* part : {&out1, &out2})
+    for (auto& pt : *part) {
+      if (n_out < capacity) {
+        if (positions) memcpy(positions + 3 * n_out, pt.pos, 12);
+        if (normals) memcpy(normals + 3 * n_out, pt.nrm, 12);
+        if (colors) memcpy(colors + 3 * n_out, pt.col, 3);
+        if (keys) keys[n_out] = pt.key;
+        if (vis_counts) vis_counts[n_out] = (uint8_t)pt.vis.size();
+        if (vis)
+          for (uint32_t t = 0; t < vis_stride; ++t) vis[n_out * vis_stride + t] = t < pt.vis.size() ? pt.vis[t] : 0;
+      }
+      n_out++;
+    }
   *count = n_out;
+  if (residual_count) *residual_count = out2.size();
   return n_out <= capacity ? PS_OK : PS_EINVAL;
 }
 

@@ -79,6 +79,43 @@ def test_fusion_bitwise_vs_oracle(pipeline):
     np.testing.assert_array_equal(s.fused_points().keys, want2.keys)
 
 
+def test_second_pass_fusion_bitwise_vs_oracle(pipeline):
+    """FusionResidual::SecondPass (crates/dense/src/fusion.rs:540-627) on the device against the restatement: the
+    whole cloud (first pass, then the second-pass points) and the residual count equal; Release equals None."""
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    imgs = [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views]
+    args = ([st.depth for st in states], [st.normal for st in states], [st.cost for st in states], imgs, views)
+    prm = fusion.default_fusion(3)
+    prm.residual = 2
+    n = s.fuse_resident(0, views, fc, prm)
+    got = s.fused_points()
+    want = oracle.fuse(fc, *args, prm)
+    assert n == len(want) and s.fused_residual == want.residual > 0
+    np.testing.assert_array_equal(got.keys, want.keys)
+    np.testing.assert_array_equal(got.positions, want.positions)
+    np.testing.assert_array_equal(got.normals, want.normals)
+    np.testing.assert_array_equal(got.colors, want.colors)
+    np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
+    for i in range(len(want)):
+        assert got.visibility(i) == want.visibility(i)
+    # explicit residual tolerances and no distance rule
+    prm.residual_depth_error, prm.residual_normal_error_deg, prm.residual_min_dist_gsd = 0.004, 6.0, 0.0
+    n2 = s.fuse_resident(0, views, fc, prm)
+    want2 = oracle.fuse(fc, *args, prm)
+    assert n2 == len(want2) and s.fused_residual == want2.residual
+    np.testing.assert_array_equal(s.fused_points().keys, want2.keys)
+    rel = fusion.default_fusion(3)
+    rel.residual = 1
+    n_rel = s.fuse_resident(0, views, fc, rel)
+    n_none = s.fuse_resident(0, views, fc, fusion.default_fusion(3))
+    assert n_rel == n_none and s.fused_residual == 0
+
+
 @pytest.mark.parametrize("full_k", [True, False])
 def test_fill_holes_bitwise_vs_oracle(full_k):
     """Speckle removal then hole filling (fill_holes, crates/dense/src/postproc.rs:139-201) on the device readout,

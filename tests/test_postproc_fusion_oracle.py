@@ -151,3 +151,43 @@ def test_fusion_depth_tolerance(gt_scene):
     sc = _fuse_gt(wl, fc, scaled)
     merged = lambda cl: int(sum(1 for i in range(len(cl)) if 2 in cl.visibility(i) and cl.vis_counts[i] > 1))
     assert merged(sc) * 50 < merged(base)
+
+
+def _fuse_gt_noisy(wl, fc, prm, seed=5):
+    """Ground-truth maps with multiplicative depth noise, so the first pass leaves pixels for the second."""
+    rng = np.random.default_rng(seed)
+    d = [(g * (1.0 + rng.normal(0, 0.006, g.shape))).astype(np.float32) for g in wl.gt_depth]
+    n = [g.astype(np.float32) for g in wl.gt_normal]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    return oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), prm)
+
+
+def test_residual_release_equals_none_and_second_pass_appends(gt_scene):
+    """FusionResidual (crates/dense/src/fusion.rs:210-218): Release gives the None result; SecondPass keeps the
+    first-pass points as they are and appends its own, in ascending key, none of them within min_dist_gsd × GSD of a
+    first-pass point, each from a distinct reference pixel."""
+    wl, fc = gt_scene
+    base = fusion.default_fusion(3)
+    none = _fuse_gt_noisy(wl, fc, base)
+    rel = fusion.default_fusion(3)
+    rel.residual = 1
+    release = _fuse_gt_noisy(wl, fc, rel)
+    np.testing.assert_array_equal(release.keys, none.keys)
+    np.testing.assert_array_equal(release.positions, none.positions)
+    sp = fusion.default_fusion(3)
+    sp.residual = 2
+    two = _fuse_gt_noisy(wl, fc, sp)
+    n1 = len(two) - two.residual
+    assert n1 == len(none) and two.residual > 0
+    np.testing.assert_array_equal(two.keys[:n1], none.keys)
+    np.testing.assert_array_equal(two.positions[:n1], none.positions)
+    k2 = two.keys[n1:].astype(np.int64)
+    assert (np.diff(k2) > 0).all()
+    assert not np.isin(two.keys[n1:], none.keys).any()
+    assert (two.vis_counts[n1:] >= 3).all()  # reference + residual_min_views (2)
+    # the distance rule, with the GSD the restatement uses: the median over views of the median valid depth / fx
+    d1 = two.positions[:n1].astype(np.float64)
+    d2 = two.positions[n1:].astype(np.float64)
+    gsd_lo = 0.5 * min(np.median(g[g > 0]) / c.k[0] for g, c in zip(wl.gt_depth, wl.cams)) * 0.9
+    for x in d2[::7]:
+        assert np.min(np.sum((d1 - x) ** 2, axis=1)) > gsd_lo ** 2

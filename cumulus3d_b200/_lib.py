@@ -103,7 +103,9 @@ class FusionParams(C.Structure):
                 ("sigma_px0", C.c_double), ("sigma_px_slope", C.c_double), ("max_reproj_error", C.c_double),
                 ("max_depth_error", C.c_double), ("max_normal_error_deg", C.c_double),
                 ("residual_min_views", C.c_uint32), ("reserved", C.c_uint32), ("residual_depth_error", C.c_double),
-                ("residual_normal_error_deg", C.c_double), ("residual_min_dist_gsd", C.c_double)]
+                ("residual_normal_error_deg", C.c_double), ("residual_min_dist_gsd", C.c_double),
+                ("visibility_check_views", C.c_uint32), ("visibility_min_violations", C.c_uint32),
+                ("visibility_tau", C.c_double)]
 
 
 class FusionView(C.Structure):
@@ -185,6 +187,7 @@ SIGNATURES = {
     "ps_readout_download": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(ViewState)]),
     "ps_fuse_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView), C.POINTER(FusionParams),
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+    "ps_fused_visibility_removed": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_uint32]),
     "ps_build_pyramid": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.c_uint32,

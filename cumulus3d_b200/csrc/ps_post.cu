@@ -520,6 +520,61 @@ __global__ void __launch_bounds__(1024) k_gsd(const float4* __restrict__ plane, 
   if (tid == 0) gsd[blockIdx.x] = (val[0] + (val[1] - val[0]) * (pos - (double)lo)) / V.fx;
 }
 
+// One thread per fused point: the candidate views are the overlap lists of its contributing views in order,
+// de-duplicated and cut at `limit` (views that were not fused take their place in the count, as in the reference);
+// each fused candidate that sees the point in front of its camera at a pixel with a valid depth votes: a violation
+// when the point lies in front of that depth by more than tau, a support when it agrees within tau.  The point is
+// removed when it has at least min_violations violations and more violations than supports.
+__global__ void __launch_bounds__(256) k_visibility(const VisArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
+  if (i >= A.n) return;
+  const double x[3] = {(double)A.pos[3 * i], (double)A.pos[3 * i + 1], (double)A.pos[3 * i + 2]};
+  int cand[PS_VIS_MAX_CHECK];
+  int nc = 0;
+  bool full = false;
+  const unsigned short* vl = A.vis + i * A.vis_stride;
+  for (int a = 0; a < (int)A.nvis[i] && !full; ++a) {
+    const int v = vl[a];
+    if (v >= A.nviews) continue;
+    for (int j = A.ovoff[v]; j < A.ovoff[v + 1]; ++j) {
+      if (nc >= A.limit) {
+        full = true;
+        break;
+      }
+      const int o = A.ovlist[j];
+      bool dup = false;
+      for (int k = 0; k < nc; ++k) dup = dup || cand[k] == o;
+      if (!dup) cand[nc++] = o;
+    }
+  }
+  int viol = 0, sup = 0;
+  for (int k = 0; k < nc; ++k) {
+    const int v = cand[k];
+    if (v < 0 || v >= A.nviews || !A.used[v]) continue;
+    const FuseView& c = A.views[v];
+    const double* r = c.r;
+    const double cx = r[0] * x[0] + r[1] * x[1] + r[2] * x[2] + c.t[0];
+    const double cy = r[3] * x[0] + r[4] * x[1] + r[5] * x[2] + c.t[1];
+    const double cz = r[6] * x[0] + r[7] * x[1] + r[8] * x[2] + c.t[2];
+    if (cz <= 0.0) continue;
+    const double col = round(c.k[0] * cx / cz + c.k[2]), row = round(c.k[1] * cy / cz + c.k[3]);
+    if (col < 0.0 || row < 0.0 || col >= (double)c.w || row >= (double)c.h) continue;
+    const double dv = (double)A.plane[c.off + (long long)row * c.w + (long long)col].w;
+    if (dv <= 0.0) continue;
+    if (cz < dv * (1.0 - A.tau)) viol++;
+    else if (fabs(cz - dv) <= A.tau * dv) sup++;
+  }
+  const bool keep = !(viol >= A.min_violations && viol > sup);
+  A.keep[i] = keep ? 1 : 0;
+  if (!keep) atomicAdd(&A.removed[i < A.n1 ? 0 : 1], 1ull);
+}
+
+cudaError_t launch_visibility(const VisArgs& A, cudaStream_t st) {
+  if (A.n == 0) return cudaSuccess;
+  k_visibility<<<(unsigned)((A.n + 255) / 256), 256, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st) {
   const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
   k_fuse<<<g, b, 0, st>>>(A);

@@ -71,6 +71,26 @@ struct FuseArgs {
   double gcell;                     // cell size = minimum distance
 };
 
+// Free-space visibility filter of a fused cloud (filter_visibility, crates/dense/src/visibility.rs:106-151).
+#define PS_VIS_MAX_CHECK 64
+struct VisArgs {
+  const FuseView* views;        // camera and slot offset per session view
+  const float4* plane;          // readout planes (depth = w)
+  const unsigned char* used;    // per session view: fused
+  const int* ovoff;             // full overlap list of view v: ovlist[ovoff[v] .. ovoff[v+1])
+  const int* ovlist;
+  int nviews;
+  const float* pos;
+  const unsigned char* nvis;
+  const unsigned short* vis;
+  int vis_stride;
+  unsigned long long n, n1;     // points; the first n1 are from the first pass
+  int limit, min_violations;
+  double tau;
+  unsigned char* keep;
+  unsigned long long* removed;  // [0]: first-pass points removed, [1]: second-pass points removed
+};
+
 // Median sampling of the ground sample distance (depth_gsd, fusion.rs:469-487), one CTA per view.
 struct GsdView {
   long long off;       // slot offset of the view's readout planes
@@ -98,6 +118,7 @@ cudaError_t launch_count_valid(const SpkArgs& A, int ntiles, cudaStream_t st);
 cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st);
 // second pass: stage 1 (candidates claim their pixels) and stage 2 (owners of their reference pixel are emitted)
 cudaError_t launch_fuse_second(const FuseArgs& A, int w, int h, int stage, cudaStream_t st);
+cudaError_t launch_visibility(const VisArgs& A, cudaStream_t st);
 // per view: every 97th valid depth in row-major order, then their median over fx (gsd[i]; NaN when the view has none)
 cudaError_t launch_gsd(const float4* plane, const GsdView* views, int nviews, float* samples, unsigned* scount,
                        double* gsd, cudaStream_t st);

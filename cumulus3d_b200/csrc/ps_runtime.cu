@@ -102,6 +102,9 @@ struct Slot {
 // Fused point cloud of the last ps_fuse_resident call (device).
 struct FusedCloud {
   unsigned long long cap = 0, count = 0, count1 = 0;  // count1: points of the first pass (they come first)
+  // visibility filter: per emitted point 1 = kept (NULL: no filter ran), and the removed points of each pass
+  unsigned char* keep = nullptr;
+  unsigned long long removed1 = 0, removed2 = 0;
   int vis_stride = 0;
   float* pos = nullptr;
   float* nrm = nullptr;
@@ -113,6 +116,7 @@ struct FusedCloud {
   ps_post::FuseView* views = nullptr;
   template <typename Free>
   void release(Free&& free) {
+    free(keep);
     free(pos);
     free(nrm);
     free(col);
@@ -1843,6 +1847,9 @@ void ps_fusion_params_default(ps_fusion_params* out) {
   out->residual_depth_error = std::numeric_limits<double>::quiet_NaN();
   out->residual_normal_error_deg = std::numeric_limits<double>::quiet_NaN();
   out->residual_min_dist_gsd = 0.5;
+  out->visibility_check_views = 0;
+  out->visibility_min_violations = 2;
+  out->visibility_tau = 0.01;
 }
 
 int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
@@ -2140,8 +2147,71 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
       if (ovf) fail(PS_ECUDA, "second pass: spatial hash table full");
     }
     fc.count = std::min(cnt, fc.cap);
-    if (num_points) *num_points = fc.count;
-    if (num_residual) *num_residual = fc.count - fc.count1;
+    fc.removed1 = fc.removed2 = 0;
+    if (fc.keep) dfree(s, fc.keep);
+    fc.keep = nullptr;
+    const bool vis_on = p->visibility_check_views > 0 && p->visibility_tau > 0.0 && p->visibility_min_violations > 0;
+    if (vis_on && fc.count > 0) {
+      if (p->visibility_check_views > PS_VIS_MAX_CHECK) fail(PS_EINVAL, "visibility_check_views > 64");
+      // full overlap lists of the fused views (the candidate order of the filter)
+      std::vector<int> ovoff(s->nv + 1, 0), ovlist;
+      for (int v = 0; v < s->nv; ++v) {
+        ovoff[v] = (int)ovlist.size();
+        if (!used[v]) continue;
+        for (uint32_t j = 0; j < cams[v].num_overlap; ++j) ovlist.push_back((int)cams[v].overlap[j]);
+      }
+      ovoff[s->nv] = (int)ovlist.size();
+      std::vector<unsigned char> used8(used.begin(), used.end());
+      int* dovoff = dalloc<int>(s, ovoff.size());
+      int* dovlist = dalloc<int>(s, std::max<size_t>(ovlist.size(), 1));
+      unsigned char* dused = dalloc<unsigned char>(s, std::max(s->nv, 1));
+      unsigned long long* drem = dalloc<unsigned long long>(s, 2);
+      fc.keep = dalloc<unsigned char>(s, fc.count);
+      cuda_ok(cudaMemcpyAsync(dovoff, ovoff.data(), ovoff.size() * sizeof(int), cudaMemcpyHostToDevice, s->st), "upload");
+      if (!ovlist.empty())
+        cuda_ok(cudaMemcpyAsync(dovlist, ovlist.data(), ovlist.size() * sizeof(int), cudaMemcpyHostToDevice, s->st),
+                "upload");
+      cuda_ok(cudaMemcpyAsync(dused, used8.data(), used8.size(), cudaMemcpyHostToDevice, s->st), "upload");
+      cuda_ok(cudaMemsetAsync(drem, 0, 2 * sizeof(unsigned long long), s->st), "memset");
+      ps_post::VisArgs V;
+      memset(&V, 0, sizeof V);
+      V.views = fc.views;
+      V.plane = sl.aux;
+      V.used = dused;
+      V.ovoff = dovoff;
+      V.ovlist = dovlist;
+      V.nviews = s->nv;
+      V.pos = fc.pos;
+      V.nvis = fc.nvis;
+      V.vis = fc.vis;
+      V.vis_stride = fc.vis_stride;
+      V.n = fc.count;
+      V.n1 = fc.count1;
+      V.limit = (int)p->visibility_check_views;
+      V.min_violations = (int)p->visibility_min_violations;
+      V.tau = p->visibility_tau;
+      V.keep = fc.keep;
+      V.removed = drem;
+      launched(s, ps_post::launch_visibility(V, s->st), "visibility kernel");
+      unsigned long long rem[2] = {0, 0};
+      cuda_ok(cudaMemcpyAsync(rem, drem, sizeof rem, cudaMemcpyDeviceToHost, s->st), "read counts");
+      sync(s);
+      fc.removed1 = rem[0];
+      fc.removed2 = rem[1];
+      dfree(s, dovoff);
+      dfree(s, dovlist);
+      dfree(s, dused);
+      dfree(s, drem);
+    }
+    if (num_points) *num_points = fc.count - fc.removed1 - fc.removed2;
+    if (num_residual) *num_residual = fc.count - fc.count1 - fc.removed2;
+  });
+}
+
+int ps_fused_visibility_removed(ps_session* s, uint64_t* removed) {
+  return guard(s, [&] {
+    if (!removed) fail(PS_EINVAL, "removed is NULL");
+    *removed = s->fused.removed1 + s->fused.removed2;
   });
 }
 
@@ -2149,8 +2219,10 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride) {
   return guard(s, [&] {
     FusedCloud& fc = s->fused;
-    const size_t n = fc.count;
-    if (capacity < n) fail(PS_EINVAL, "capacity " + std::to_string(capacity) + " < " + std::to_string(n) + " points");
+    const size_t n = fc.count;  // emitted points (before the visibility filter)
+    const size_t kept = n - fc.removed1 - fc.removed2;
+    if (capacity < kept)
+      fail(PS_EINVAL, "capacity " + std::to_string(capacity) + " < " + std::to_string(kept) + " points");
     if (vis && (int)vis_stride < fc.vis_stride) fail(PS_EINVAL, "vis_stride too small");
     std::vector<float> p(3 * n), q(3 * n);
     std::vector<unsigned char> c(3 * n), nv(n);
@@ -2164,14 +2236,22 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
       cuda_ok(cudaMemcpyAsync(nv.data(), fc.nvis, n, cudaMemcpyDeviceToHost, s->st), "download");
       cuda_ok(cudaMemcpyAsync(vv.data(), fc.vis, 2 * n * fc.vis_stride, cudaMemcpyDeviceToHost, s->st), "download");
     }
+    std::vector<unsigned char> keep(n, 1);
+    if (n && fc.keep) cuda_ok(cudaMemcpyAsync(keep.data(), fc.keep, n, cudaMemcpyDeviceToHost, s->st), "download");
     sync(s);
-    // points in the reference's order: the first pass, then the second, each in ascending key (view, row, column)
-    std::vector<size_t> idx(n);
-    for (size_t i = 0; i < n; ++i) idx[i] = i;
+    // points in the reference's order: the first pass, then the second, each in ascending key (view, row, column),
+    // without the points the visibility filter removed
     const size_t n1 = std::min<size_t>(fc.count1, n);
-    std::sort(idx.begin(), idx.begin() + n1, [&](size_t a, size_t b) { return k[a] < k[b]; });
-    std::sort(idx.begin() + n1, idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
-    for (size_t j = 0; j < n; ++j) {
+    std::vector<size_t> idx;
+    idx.reserve(kept);
+    for (size_t i = 0; i < n1; ++i)
+      if (keep[i]) idx.push_back(i);
+    const size_t k1 = idx.size();
+    for (size_t i = n1; i < n; ++i)
+      if (keep[i]) idx.push_back(i);
+    std::sort(idx.begin(), idx.begin() + k1, [&](size_t a, size_t b) { return k[a] < k[b]; });
+    std::sort(idx.begin() + k1, idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
+    for (size_t j = 0; j < idx.size(); ++j) {
       const size_t i = idx[j];
       if (positions) memcpy(positions + 3 * j, &p[3 * i], 12);
       if (normals) memcpy(normals + 3 * j, &q[3 * i], 12);

@@ -416,6 +416,9 @@ class PatchMatchSession:
                                               C.byref(n), C.byref(r)))
         self._fused = (int(n.value), int(p.consistency_num_images) + 1)
         self.fused_residual = int(r.value)  # points added by the second pass (they come last)
+        vr = C.c_uint64()
+        self._check(self.lib.ps_fused_visibility_removed(self.h, C.byref(vr)))
+        self.fused_visibility_removed = int(vr.value)
         return int(n.value)
 
     def fused_points(self):

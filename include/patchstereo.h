@@ -440,6 +440,14 @@ typedef struct ps_fusion_params {
   double residual_depth_error;       /* NaN */
   double residual_normal_error_deg;  /* NaN */
   double residual_min_dist_gsd;      /* 0.5 */
+  /* free-space visibility filter of the fused cloud (VisibilityParams, crates/dense/src/visibility.rs:50-72,
+   * applied as crates/dense/src/densify.rs:544-551 does): a point is projected into up to visibility_check_views
+   * candidate views (the overlap lists of its contributing views in order, de-duplicated; at most 64; 0 = off) and
+   * removed when at least visibility_min_violations of them see a valid depth beyond it by more than tau (relative)
+   * and those outnumber the views that agree within tau. */
+  uint32_t visibility_check_views;    /* 0 */
+  uint32_t visibility_min_violations; /* 2 */
+  double visibility_tau;              /* 0.01 */
 } ps_fusion_params;
 void ps_fusion_params_default(ps_fusion_params* out);
 /* Camera of one view for fusion (DenseView, crates/dense/src/scene.rs): world -> camera x_c = R x_w + t with R
@@ -461,6 +469,8 @@ typedef struct ps_fusion_view {
  * the second pass added (FusionOutput::residual).  Colours are the gray image value as u8. */
 int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
                      const ps_fusion_params* p, uint64_t* num_points, uint64_t* num_residual);
+/* Points the visibility filter removed from the last fused cloud (FusionOutput::visibility_removed). */
+int ps_fused_visibility_removed(ps_session* s, uint64_t* removed);
 /* The fused points in the reference's order: the first pass in ascending point key (image_id << 32) | (row << 16) |
  * col, then the second-pass points in ascending key: positions and normals 3 floats, colours 3 bytes, keys, the
  * number of contributing views and their indices (ascending, vis_stride >= consistency_num_images + 1 entries per

@@ -46,7 +46,7 @@ def lib() -> C.CDLL:
                                       C.POINTER(C.c_void_p), C.POINTER(C.c_void_p), C.c_void_p,
                                       C.POINTER(_lib.FusionParams), C.c_int, C.c_uint64, C.c_void_p, C.c_void_p,
                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
-                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+                                      C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int]),
             "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
@@ -252,13 +252,14 @@ def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[
     key = np.empty(cap, np.uint64)
     vc = np.empty(cap, np.uint8)
     vis = np.empty((cap, stride), np.uint16)
-    n, r = C.c_uint64(), C.c_uint64()
+    n, r, vr = C.c_uint64(), C.c_uint64(), C.c_uint64()
     _chk(lib().oracle_fuse(nv, cams.table, ws, hs, dp, np_, cp, ip, used.ctypes.data, C.byref(params),
                            _threads(threads), cap, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data, key.ctypes.data,
-                           vc.ctypes.data, vis.ctypes.data, stride, C.byref(n), C.byref(r)), "fuse")
+                           vc.ctypes.data, vis.ctypes.data, stride, C.byref(n), C.byref(r), C.byref(vr)), "fuse")
     k = int(n.value)
     out = FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
     out.residual = int(r.value)  # points of the second pass (the last ones)
+    out.visibility_removed = int(vr.value)
     return out
 
 

@@ -1402,7 +1402,8 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
                 const float* const* depth, const float* const* normal, const float* const* cost,
                 const float* const* img, const uint8_t* used, const ps_fusion_params* p, int threads,
                 uint64_t capacity, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
-                uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count, uint64_t* residual_count) {
+                uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count, uint64_t* residual_count,
+                uint64_t* visibility_removed) {
   if (!cams || !widths || !heights || !depth || !normal || !cost || !img || !used || !p || !count) return PS_EINVAL;
   if (p->residual > PS_FUSION_RESIDUAL_SECOND_PASS) return PS_EINVAL;
   set_threads(threads);
@@ -1628,6 +1629,52 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
     for (auto& c : cands)
       if (owner[c.v][c.pix] == (uint32_t)(offset[c.v] + c.pix)) out2.push_back(std::move(c.pt));
   }
+  // filter_visibility (crates/dense/src/visibility.rs:106-151) over both passes' points, order kept
+  uint64_t vis_removed = 0;
+  if (p->visibility_check_views > 0 && p->visibility_tau > 0.0 && p->visibility_min_violations > 0) {
+    for (std::vector<FPoint>* part : {&out1, &out2}) {
+      std::vector<FPoint> kept;
+      for (auto& pt : *part) {
+        const double x[3] = {(double)pt.pos[0], (double)pt.pos[1], (double)pt.pos[2]};
+        std::vector<int> cand;
+        bool full = false;
+        for (uint16_t v : pt.vis) {
+          if (full) break;
+          if (v >= nviews) continue;
+          for (uint32_t j = 0; j < cams[v].num_overlap; ++j) {
+            if (cand.size() >= p->visibility_check_views) {
+              full = true;
+              break;
+            }
+            const int o = (int)cams[v].overlap[j];
+            if (std::find(cand.begin(), cand.end(), o) == cand.end()) cand.push_back(o);
+          }
+        }
+        int viol = 0, sup = 0;
+        for (int v : cand) {
+          if (v < 0 || v >= (int)nviews || !used[v]) continue;
+          const FCam& c = fc[v];
+          const double cx = c.r[0] * x[0] + c.r[1] * x[1] + c.r[2] * x[2] + c.t[0];
+          const double cy = c.r[3] * x[0] + c.r[4] * x[1] + c.r[5] * x[2] + c.t[1];
+          const double cz = c.r[6] * x[0] + c.r[7] * x[1] + c.r[8] * x[2] + c.t[2];
+          if (cz <= 0.0) continue;
+          const double col = std::round(c.k[0] * cx / cz + c.k[2]), row = std::round(c.k[1] * cy / cz + c.k[3]);
+          if (col < 0.0 || row < 0.0 || col >= (double)c.w || row >= (double)c.h) continue;
+          const double dv = (double)depth[v][(size_t)row * c.w + (size_t)col];
+          if (dv <= 0.0) continue;
+          if (cz < dv * (1.0 - p->visibility_tau)) viol++;
+          else if (std::fabs(cz - dv) <= p->visibility_tau * dv) sup++;
+        }
+        if (viol >= (int)p->visibility_min_violations && viol > sup) {
+          vis_removed++;
+          continue;
+        }
+        kept.push_back(std::move(pt));
+      }
+      *part = std::move(kept);
+    }
+  }
+  if (visibility_removed) *visibility_removed = vis_removed;
   uint64_t n_out = 0;
   for (std::vector<FPoint>* part : {&out1, &out2})
     for (auto& pt : *part) {

@@ -116,6 +116,32 @@ def test_second_pass_fusion_bitwise_vs_oracle(pipeline):
     assert n_rel == n_none and s.fused_residual == 0
 
 
+@pytest.mark.parametrize("residual", [0, 2])
+def test_visibility_filter_bitwise_vs_oracle(pipeline, residual):
+    """filter_visibility (crates/dense/src/visibility.rs:106-151) on the device cloud against the restatement: the
+    kept points (both passes) and the removed count equal."""
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    imgs = [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views]
+    prm = fusion.default_fusion(2)
+    prm.residual = residual
+    prm.visibility_check_views, prm.visibility_min_violations, prm.visibility_tau = 8, 1, 0.002
+    n = s.fuse_resident(0, views, fc, prm)
+    got = s.fused_points()
+    want = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
+                       imgs, views, prm)
+    assert s.fused_visibility_removed == want.visibility_removed > 0
+    assert n == len(want) and s.fused_residual == want.residual
+    np.testing.assert_array_equal(got.keys, want.keys)
+    np.testing.assert_array_equal(got.positions, want.positions)
+    np.testing.assert_array_equal(got.normals, want.normals)
+    np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
+
+
 @pytest.mark.parametrize("full_k", [True, False])
 def test_fill_holes_bitwise_vs_oracle(full_k):
     """Speckle removal then hole filling (fill_holes, crates/dense/src/postproc.rs:139-201) on the device readout,

@@ -191,3 +191,64 @@ def test_residual_release_equals_none_and_second_pass_appends(gt_scene):
     gsd_lo = 0.5 * min(np.median(g[g > 0]) / c.k[0] for g, c in zip(wl.gt_depth, wl.cams)) * 0.9
     for x in d2[::7]:
         assert np.min(np.sum((d1 - x) ** 2, axis=1)) > gsd_lo ** 2
+
+
+def _visibility_keep_py(cloud, depths, fc_views, used, limit, tau, min_viol):
+    """filter_visibility (crates/dense/src/visibility.rs:106-151) restated in Python: the keep flag of every point."""
+    keep = []
+    for i in range(len(cloud)):
+        x = cloud.positions[i].astype(np.float64)
+        cand = []
+        full = False
+        for v in cloud.visibility(i):
+            if full:
+                break
+            for o in fc_views[v]["overlap"]:
+                if len(cand) >= limit:
+                    full = True
+                    break
+                if o not in cand:
+                    cand.append(o)
+        viol = sup = 0
+        for v in cand:
+            if not used[v]:
+                continue
+            c = fc_views[v]
+            pc = c["r"] @ x + c["t"]
+            if pc[2] <= 0:
+                continue
+            col = np.round(c["k"][0] * pc[0] / pc[2] + c["k"][2])
+            row = np.round(c["k"][1] * pc[1] / pc[2] + c["k"][3])
+            h, w = depths[v].shape
+            if col < 0 or row < 0 or col >= w or row >= h:
+                continue
+            dv = float(depths[v][int(row), int(col)])
+            if dv <= 0:
+                continue
+            if pc[2] < dv * (1 - tau):
+                viol += 1
+            elif abs(pc[2] - dv) <= tau * dv:
+                sup += 1
+        keep.append(not (viol >= min_viol and viol > sup))
+    return np.array(keep, bool)
+
+
+def test_visibility_filter_matches_independent_restatement(gt_scene):
+    """Four of six views see 5 % too far: points fused from the other two violate free space in those four."""
+    wl, fc = gt_scene
+    d = [g.astype(np.float32) for g in wl.gt_depth]
+    for v in (2, 3, 4, 5):
+        d[v] = d[v] * np.float32(1.05)
+    n = [g.astype(np.float32) for g in wl.gt_normal]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    prm = fusion.default_fusion(1)
+    base = oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), prm)
+    prm.visibility_check_views, prm.visibility_min_violations, prm.visibility_tau = 8, 2, 0.01
+    filt = oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), prm)
+    views = []
+    for v, cam in enumerate(wl.cams):
+        views.append({"k": cam.k, "r": cam.r, "t": cam.t, "overlap": [int(o) for o in fc.overlap[v]]})
+    keep = _visibility_keep_py(base, d, views, [True] * len(d), 8, 0.01, 2)
+    assert filt.visibility_removed == int((~keep).sum()) > 0
+    np.testing.assert_array_equal(filt.keys, base.keys[keep])
+    np.testing.assert_array_equal(filt.positions, base.positions[keep])

@@ -105,7 +105,9 @@ class FusionParams(C.Structure):
                 ("residual_min_views", C.c_uint32), ("reserved", C.c_uint32), ("residual_depth_error", C.c_double),
                 ("residual_normal_error_deg", C.c_double), ("residual_min_dist_gsd", C.c_double),
                 ("visibility_check_views", C.c_uint32), ("visibility_min_violations", C.c_uint32),
-                ("visibility_tau", C.c_double)]
+                ("visibility_tau", C.c_double), ("smooth_iterations", C.c_uint32), ("reserved2", C.c_uint32),
+                ("smooth_radius_gsd", C.c_double), ("smooth_sigma_range_gsd", C.c_double),
+                ("smooth_normal_deg", C.c_double)]
 
 
 class FusionView(C.Structure):

@@ -9,6 +9,10 @@
 //    (ln2/2)^8/8! ~ 5e-9 relative; measured error is about 1 ulp.  Results below 2^-126·(e^-0.35) are flushed
 //    to +0 (arguments below -87.33); arguments above 88.0 return +inf.  All call sites in this project pass
 //    arguments <= 0.
+//  * ps_exp64: binary64 e^x by the same scheme: x = k·ln2 + r with ln2 split into a head of 32 significant bits
+//    (k·ln2_hi exact for |k| < 2^21) and a tail, both products folded with fma; the degree-13 Taylor polynomial of
+//    e^r on |r| <= ln2/2 (truncation below 2^-57 relative) by Horner's rule with fma; scaling by 2^k through the
+//    exponent field (in two steps below 2^-1022).  Arguments above 709 give +inf, below -745.2 give +0.
 //  * ps_sincosf: Cody–Waite reduction by pi/2 (three-part split of pi/2 folded with fma, valid for |x| < 1e5),
 //    then Taylor polynomials of degree 9 (sin) and 10 (cos) on |r| <= pi/4 (truncation error < 2e-9), with the
 //    quadrant selecting sign and swap.
@@ -63,6 +67,44 @@ PS_HD float ps_expf(float x) {
   p = fmaf(p, r, 1.0f);
   int ki = (int)k;                                // k in [-126, 127]
   return p * ps_u2f((uint32_t)(ki + 127) << 23);
+}
+
+PS_HD double ps_u2d(uint64_t u) {
+#if defined(__CUDA_ARCH__)
+  return __longlong_as_double((long long)u);
+#else
+  double f;
+  memcpy(&f, &u, sizeof f);
+  return f;
+#endif
+}
+
+PS_HD double ps_exp64(double x) {
+  if (!(x == x)) return x;
+  if (x > 709.0) return ps_u2d(0x7ff0000000000000ull);
+  if (x < -745.2) return 0.0;
+  const double ln2_hi = 0.6931471803691238;     // ln 2 to 32 significant bits
+  const double ln2_lo = 1.9082149292705877e-10;  // ln 2 - ln2_hi
+  const double k = rint(x * 1.4426950408889634);
+  double r = fma(-k, ln2_hi, x);
+  r = fma(-k, ln2_lo, r);
+  double p = 1.6059043836821613e-10;  // 1/13!
+  p = fma(p, r, 2.08767569878681e-09);
+  p = fma(p, r, 2.505210838544172e-08);
+  p = fma(p, r, 2.755731922398589e-07);
+  p = fma(p, r, 2.7557319223985893e-06);
+  p = fma(p, r, 2.48015873015873e-05);
+  p = fma(p, r, 0.0001984126984126984);
+  p = fma(p, r, 0.001388888888888889);
+  p = fma(p, r, 0.008333333333333333);
+  p = fma(p, r, 0.041666666666666664);
+  p = fma(p, r, 0.16666666666666666);
+  p = fma(p, r, 0.5);
+  p = fma(p, r, 1.0);
+  p = fma(p, r, 1.0);
+  const int ki = (int)k;  // -1075 .. 1023
+  if (ki >= -1022) return p * ps_u2d((uint64_t)(ki + 1023) << 52);
+  return (p * ps_u2d((uint64_t)(ki + 1023 + 600) << 52)) * ps_u2d((uint64_t)(1023 - 600) << 52);
 }
 
 PS_HD void ps_sincosf(float x, float* s, float* c) {

@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include "ps_post.h"
+#include "ps_fmath.h"
 
 namespace ps_post {
 
@@ -572,6 +573,141 @@ __global__ void __launch_bounds__(256) k_visibility(const VisArgs A) {
 cudaError_t launch_visibility(const VisArgs& A, cudaStream_t st) {
   if (A.n == 0) return cudaSuccess;
   k_visibility<<<(unsigned)((A.n + 255) / 256), 256, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+// ---- smoothing along normals ------------------------------------------------------------------------------------
+// Cells of size r, packed 21 bits per axis (offset by 2^20) plus one so that 0 marks an empty slot.
+#define PS_SM_LIM ((1ll << 20) - 2)
+__device__ __forceinline__ unsigned long long sm_code(long long cx, long long cy, long long cz) {
+  return ((unsigned long long)(cx + (1ll << 20)) << 42 | (unsigned long long)(cy + (1ll << 20)) << 21 |
+          (unsigned long long)(cz + (1ll << 20))) + 1ull;
+}
+__device__ __forceinline__ bool sm_cell(const SmoothArgs& A, unsigned long long i, long long* c) {
+  for (int a = 0; a < 3; ++a) {
+    const double f = floor((double)A.pos[3 * i + a] / A.r);
+    if (!(f >= (double)-PS_SM_LIM && f <= (double)PS_SM_LIM)) return false;
+    c[a] = (long long)f;
+  }
+  return true;
+}
+__device__ __forceinline__ unsigned long long sm_order(const SmoothArgs& A, unsigned u) {
+  return ((unsigned long long)(u >= A.n1) << 63) | A.key[u];
+}
+__device__ __forceinline__ int sm_find(const SmoothArgs& A, unsigned long long code) {
+  unsigned slot = (unsigned)(grid_mix(code) & (A.cap - 1u));
+  for (unsigned t = 0; t < A.cap; ++t) {
+    const unsigned long long k = A.hkeys[slot];
+    if (k == code) return (int)slot;
+    if (k == 0ull) return -1;
+    slot = (slot + 1u) & (A.cap - 1u);
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(256) k_sm_insert(const SmoothArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
+  if (i >= A.n || (A.keep && !A.keep[i])) return;
+  long long c[3];
+  if (!sm_cell(A, i, c)) {
+    atomicExch(A.flag, 1);
+    return;
+  }
+  const unsigned long long code = sm_code(c[0], c[1], c[2]);
+  unsigned slot = (unsigned)(grid_mix(code) & (A.cap - 1u));
+  for (unsigned t = 0; t < A.cap; ++t) {
+    const unsigned long long prev = atomicCAS(&A.hkeys[slot], 0ull, code);
+    if (prev == 0ull || prev == code) {
+      A.pslot[i] = slot;
+      atomicAdd(&A.hcnt[slot], 1u);
+      return;
+    }
+    slot = (slot + 1u) & (A.cap - 1u);
+  }
+  atomicExch(A.flag, 1);  // cannot happen: the table is at most half full
+}
+__global__ void __launch_bounds__(256) k_sm_alloc(const SmoothArgs A) {
+  const unsigned s = blockIdx.x * 256u + threadIdx.x;
+  if (s < A.cap && A.hcnt[s]) A.hstart[s] = atomicAdd(A.total, A.hcnt[s]);
+}
+__global__ void __launch_bounds__(256) k_sm_scatter(const SmoothArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
+  if (i >= A.n || (A.keep && !A.keep[i])) return;
+  long long c[3];
+  if (!sm_cell(A, i, c)) return;
+  const unsigned s = A.pslot[i];
+  A.list[A.hstart[s] + atomicAdd(&A.hcur[s], 1u)] = (unsigned)i;
+}
+// each cell's points in cloud order (first pass before second, then ascending key): insertion sort per cell
+__global__ void __launch_bounds__(256) k_sm_sort(const SmoothArgs A) {
+  const unsigned s = blockIdx.x * 256u + threadIdx.x;
+  if (s >= A.cap || !A.hcnt[s]) return;
+  unsigned* l = A.list + A.hstart[s];
+  const unsigned m = A.hcnt[s];
+  for (unsigned a = 1; a < m; ++a) {
+    const unsigned u = l[a];
+    const unsigned long long ku = sm_order(A, u);
+    unsigned b = a;
+    while (b > 0 && sm_order(A, l[b - 1]) > ku) {
+      l[b] = l[b - 1];
+      --b;
+    }
+    l[b] = u;
+  }
+}
+__device__ __forceinline__ void sm_normal(const SmoothArgs& A, unsigned long long i, double* n) {
+  const double m[3] = {(double)A.nrm[3 * i], (double)A.nrm[3 * i + 1], (double)A.nrm[3 * i + 2]};
+  const double l = sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  for (int a = 0; a < 3; ++a) n[a] = l > 1e-12 ? m[a] / l : 0.0;
+}
+// The move of one point: neighbours in the 27 cells around (z, then y, then x offsets; each cell in cloud order)
+// within r, other than the point, whose normal is within the angle, weigh exp(-d²/(2(r/2)²) - dn²/(2σ²)); the point
+// moves along its normal by Σ w·dn / (1 + Σ w).
+__global__ void __launch_bounds__(256) k_sm_step(const SmoothArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
+  if (i >= A.n || (A.keep && !A.keep[i])) return;
+  long long c[3];
+  if (!sm_cell(A, i, c)) return;
+  const double pi[3] = {(double)A.pos[3 * i], (double)A.pos[3 * i + 1], (double)A.pos[3 * i + 2]};
+  double ni[3];
+  sm_normal(A, i, ni);
+  double t = 0.0;
+  if (!(ni[0] == 0.0 && ni[1] == 0.0 && ni[2] == 0.0)) {
+    double sw = 1.0, swd = 0.0;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int s = sm_find(A, sm_code(c[0] + dx, c[1] + dy, c[2] + dz));
+          if (s < 0) continue;
+          const unsigned* l = A.list + A.hstart[s];
+          for (unsigned q = 0; q < A.hcnt[s]; ++q) {
+            const unsigned j = l[q];
+            const double dv[3] = {(double)A.pos[3 * j] - pi[0], (double)A.pos[3 * j + 1] - pi[1],
+                                  (double)A.pos[3 * j + 2] - pi[2]};
+            const double d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+            if (d2 > A.r2 || j == (unsigned)i) continue;
+            double nj[3];
+            sm_normal(A, j, nj);
+            if (ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2] < A.cos_n) continue;
+            const double dn = ni[0] * dv[0] + ni[1] * dv[1] + ni[2] * dv[2];
+            const double w = ps_exp64(-d2 * A.inv_2ss - dn * dn * A.inv_2sr);
+            sw += w;
+            swd += w * dn;
+          }
+        }
+    t = swd / sw;
+  }
+  for (int a = 0; a < 3; ++a) A.pos2[3 * i + a] = (float)(pi[a] + t * ni[a]);
+}
+
+cudaError_t launch_smooth_pass(const SmoothArgs& A, cudaStream_t st) {
+  if (A.n == 0) return cudaSuccess;
+  const unsigned gp = (unsigned)((A.n + 255) / 256), gs = (A.cap + 255) / 256;
+  k_sm_insert<<<gp, 256, 0, st>>>(A);
+  k_sm_alloc<<<gs, 256, 0, st>>>(A);
+  k_sm_scatter<<<gp, 256, 0, st>>>(A);
+  k_sm_sort<<<gs, 256, 0, st>>>(A);
+  k_sm_step<<<gp, 256, 0, st>>>(A);
   return cudaGetLastError();
 }
 

@@ -91,6 +91,28 @@ struct VisArgs {
   unsigned long long* removed;  // [0]: first-pass points removed, [1]: second-pass points removed
 };
 
+// Bilateral smoothing of a fused cloud along its normals (smooth_along_normals, crates/dense/src/smooth.rs:143-220).
+struct SmoothArgs {
+  float* pos;                         // cloud positions (read)
+  float* pos2;                        // next positions (written)
+  const float* nrm;
+  const unsigned char* keep;          // visibility mask (NULL: every point)
+  const unsigned long long* key;      // point keys; with the pass they give the cloud order
+  unsigned long long n, n1;           // points; the first n1 are from the first pass
+  double r, r2, inv_2ss, inv_2sr, cos_n;
+  unsigned long long* hkeys;          // cell table (cap slots, 0 = empty)
+  unsigned* hcnt;
+  unsigned* hstart;
+  unsigned* hcur;
+  unsigned cap;
+  unsigned* list;                     // points grouped by cell, each group in cloud order
+  unsigned* pslot;                    // cell slot of each point
+  unsigned* total;
+  int* flag;                          // set when a cell is out of range or the table is full
+};
+// one Jacobi pass: cells, grouping, ordering, and the moves into pos2
+cudaError_t launch_smooth_pass(const SmoothArgs& A, cudaStream_t st);
+
 // Median sampling of the ground sample distance (depth_gsd, fusion.rs:469-487), one CTA per view.
 struct GsdView {
   long long off;       // slot offset of the view's readout planes

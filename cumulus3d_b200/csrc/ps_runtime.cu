@@ -1850,6 +1850,10 @@ void ps_fusion_params_default(ps_fusion_params* out) {
   out->visibility_check_views = 0;
   out->visibility_min_violations = 2;
   out->visibility_tau = 0.01;
+  out->smooth_iterations = 0;
+  out->smooth_radius_gsd = 1.0;
+  out->smooth_sigma_range_gsd = 0.25;
+  out->smooth_normal_deg = 30.0;
 }
 
 int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_post_params* p,
@@ -2049,8 +2053,8 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     cuda_ok(cudaMemcpyAsync(&cnt, fc.counter, sizeof cnt, cudaMemcpyDeviceToHost, s->st), "read count");
     sync(s);
     fc.count1 = std::min(cnt, fc.cap);
-    if (second) {
-      // ground sample distance (depth_gsd, fusion.rs:469-487) of the fused views, in index order
+    // ground sample distance (depth_gsd, fusion.rs:469-487) of the fused views, in index order
+    auto fused_gsd = [&]() {
       std::vector<ps_post::GsdView> gv(order.size());
       long long soff = 0;
       for (size_t i = 0; i < order.size(); ++i) {
@@ -2085,6 +2089,10 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
         const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, g2.size() - 1);
         gsd = g2[lo] + (g2[hi] - g2[lo]) * (pos - (double)lo);
       }
+      return gsd;
+    };
+    if (second) {
+      const double gsd = fused_gsd();
       const double min_dist = p->residual_min_dist_gsd * gsd;
       // candidate numbers: prefix of the fused views' pixel counts in index order (fusion.rs:560-565)
       std::vector<ps_post::FuseView> fv2 = fv;
@@ -2202,6 +2210,62 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
       dfree(s, dovlist);
       dfree(s, dused);
       dfree(s, drem);
+    }
+    // smooth_along_normals (crates/dense/src/smooth.rs:143-220) of the kept points, as densify.rs:552-556 runs it
+    const bool smooth_on = p->smooth_iterations > 0 && p->smooth_radius_gsd > 0.0 && p->smooth_sigma_range_gsd > 0.0;
+    if (smooth_on && fc.count > 0) {
+      const double gsd = fused_gsd();
+      if (gsd > 0.0) {
+        ps_post::SmoothArgs M;
+        memset(&M, 0, sizeof M);
+        M.r = p->smooth_radius_gsd * gsd;
+        M.r2 = M.r * M.r;
+        M.inv_2ss = 1.0 / (2.0 * ((0.5 * M.r) * (0.5 * M.r)));
+        const double sr = p->smooth_sigma_range_gsd * gsd;
+        M.inv_2sr = 1.0 / (2.0 * (sr * sr));
+        M.cos_n = std::cos(ps_to_radians_f64(p->smooth_normal_deg));
+        M.n = fc.count;
+        M.n1 = fc.count1;
+        M.nrm = fc.nrm;
+        M.keep = fc.keep;
+        M.key = fc.key;
+        unsigned cap = 1024;
+        while (cap < 2ull * fc.count) cap <<= 1;
+        M.cap = cap;
+        M.hkeys = dalloc<unsigned long long>(s, cap);
+        M.hcnt = dalloc<unsigned>(s, cap);
+        M.hstart = dalloc<unsigned>(s, cap);
+        M.hcur = dalloc<unsigned>(s, cap);
+        M.list = dalloc<unsigned>(s, fc.count);
+        M.pslot = dalloc<unsigned>(s, fc.count);
+        M.total = dalloc<unsigned>(s, 1);
+        M.flag = dalloc<int>(s, 1);
+        float* pos2 = dalloc<float>(s, 3 * fc.count);
+        cuda_ok(cudaMemcpyAsync(pos2, fc.pos, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
+        cuda_ok(cudaMemsetAsync(M.flag, 0, sizeof(int), s->st), "memset");
+        float* cur = fc.pos;
+        float* nxt = pos2;
+        for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
+          cuda_ok(cudaMemsetAsync(M.hkeys, 0, cap * sizeof(unsigned long long), s->st), "memset");
+          cuda_ok(cudaMemsetAsync(M.hcnt, 0, cap * sizeof(unsigned), s->st), "memset");
+          cuda_ok(cudaMemsetAsync(M.hcur, 0, cap * sizeof(unsigned), s->st), "memset");
+          cuda_ok(cudaMemsetAsync(M.total, 0, sizeof(unsigned), s->st), "memset");
+          M.pos = cur;
+          M.pos2 = nxt;
+          cuda_ok(ps_post::launch_smooth_pass(M, s->st), "smoothing kernels");
+          s->launches += 5;
+          std::swap(cur, nxt);
+        }
+        if (cur != fc.pos)
+          cuda_ok(cudaMemcpyAsync(fc.pos, cur, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
+        int flag = 0;
+        cuda_ok(cudaMemcpyAsync(&flag, M.flag, sizeof flag, cudaMemcpyDeviceToHost, s->st), "read flag");
+        sync(s);
+        for (void* q : {(void*)M.hkeys, (void*)M.hcnt, (void*)M.hstart, (void*)M.hcur, (void*)M.list, (void*)M.pslot,
+                        (void*)M.total, (void*)M.flag, (void*)pos2})
+          dfree(s, q);
+        if (flag) fail(PS_EINVAL, "smoothing: a point lies more than 2^20 smoothing radii from the origin");
+      }
     }
     if (num_points) *num_points = fc.count - fc.removed1 - fc.removed2;
     if (num_residual) *num_residual = fc.count - fc.count1 - fc.removed2;

@@ -448,6 +448,17 @@ typedef struct ps_fusion_params {
   uint32_t visibility_check_views;    /* 0 */
   uint32_t visibility_min_violations; /* 2 */
   double visibility_tau;              /* 0.01 */
+  /* bilateral smoothing of the fused points along their normals after the visibility filter (SmoothParams,
+   * crates/dense/src/smooth.rs:51-75, applied as densify.rs:552-556 does): smooth_iterations Jacobi passes (0 = off);
+   * neighbours within radius = smooth_radius_gsd × GSD whose normal is within smooth_normal_deg move a point along
+   * its normal by the weighted mean offset, weights exp(-d²/(2(r/2)²) - dn²/(2σ²)), σ = smooth_sigma_range_gsd × GSD.
+   * The exponential is a fixed binary64 sequence (not the platform's), the same in the CPU restatement.  Cells of the
+   * radius must stay within ±2^20 of the origin on every axis. */
+  uint32_t smooth_iterations;     /* 0 */
+  uint32_t reserved2;
+  double smooth_radius_gsd;       /* 1.0 */
+  double smooth_sigma_range_gsd;  /* 0.25 */
+  double smooth_normal_deg;       /* 30 */
 } ps_fusion_params;
 void ps_fusion_params_default(ps_fusion_params* out);
 /* Camera of one view for fusion (DenseView, crates/dense/src/scene.rs): world -> camera x_c = R x_w + t with R

@@ -78,6 +78,7 @@ def lib() -> C.CDLL:
             "oracle_pyramid_step": (None, [C.c_void_p, C.c_size_t, C.c_size_t, C.POINTER(C.c_double), C.c_void_p,
                                            C.POINTER(C.c_double)]),
             "oracle_expf": (C.c_float, [C.c_float]),
+            "oracle_exp64": (C.c_double, [C.c_double]),
             "oracle_sincosf": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         }
         for n, (r, a) in sig.items():

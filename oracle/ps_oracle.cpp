@@ -1208,6 +1208,7 @@ void oracle_pyramid_step(const uint8_t* src, size_t w, size_t h, const double* k
   kout[3] = (k[3] + 0.5) * 0.5 - 0.5;
 }
 float oracle_expf(float x) { return ps_expf(x); }
+double oracle_exp64(double x) { return ps_exp64(x); }
 void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
 
 
@@ -1675,6 +1676,87 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
     }
   }
   if (visibility_removed) *visibility_removed = vis_removed;
+  // smooth_along_normals (crates/dense/src/smooth.rs:143-220) over the cloud in its order (first pass, then second)
+  if (p->smooth_iterations > 0 && p->smooth_radius_gsd > 0.0 && p->smooth_sigma_range_gsd > 0.0) {
+    std::vector<FPoint*> cl;
+    for (auto& pt : out1) cl.push_back(&pt);
+    for (auto& pt : out2) cl.push_back(&pt);
+    auto median = [](std::vector<double>& a) {
+      std::sort(a.begin(), a.end());
+      const double pos = 0.5 * (double)(a.size() - 1);
+      const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, a.size() - 1);
+      return a[lo] + (a[hi] - a[lo]) * (pos - (double)lo);
+    };
+    std::vector<double> gs;  // scene_gsd (fusion.rs:463-487)
+    for (uint32_t v = 0; v < nviews; ++v) {
+      if (!used[v]) continue;
+      std::vector<double> dd;
+      size_t k = 0;
+      for (size_t i = 0; i < (size_t)fc[v].w * fc[v].h; ++i)
+        if (depth[v][i] > 0.0f) {
+          if (k % 97 == 0) dd.push_back((double)depth[v][i]);
+          ++k;
+        }
+      if (!dd.empty()) gs.push_back(median(dd) / fc[v].k[0]);
+    }
+    const double gsd = gs.empty() ? 0.0 : median(gs);
+    const size_t n = cl.size();
+    if (gsd > 0.0 && n > 0) {
+      const double r = p->smooth_radius_gsd * gsd;
+      const double r2 = r * r;
+      const double inv_2ss = 1.0 / (2.0 * ((0.5 * r) * (0.5 * r)));
+      const double sr = p->smooth_sigma_range_gsd * gsd;
+      const double inv_2sr = 1.0 / (2.0 * (sr * sr));
+      const double cos_n = std::cos(ps_to_radians_f64(p->smooth_normal_deg));
+      std::vector<std::array<double, 3>> nrm(n);
+      for (size_t i = 0; i < n; ++i) {
+        const double m[3] = {(double)cl[i]->nrm[0], (double)cl[i]->nrm[1], (double)cl[i]->nrm[2]};
+        const double l = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+        nrm[i] = l > 1e-12 ? std::array<double, 3>{m[0] / l, m[1] / l, m[2] / l} : std::array<double, 3>{0.0, 0.0, 0.0};
+      }
+      for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
+        std::map<std::array<long long, 3>, std::vector<uint32_t>> grid;  // cell -> points in cloud order
+        std::vector<std::array<long long, 3>> cell(n);
+        for (size_t i = 0; i < n; ++i) {
+          for (int a = 0; a < 3; ++a) cell[i][a] = (long long)std::floor((double)cl[i]->pos[a] / r);
+          grid[cell[i]].push_back((uint32_t)i);
+        }
+        std::vector<std::array<float, 3>> next(n);
+#pragma omp parallel for schedule(dynamic, 256)
+        for (long long ii = 0; ii < (long long)n; ++ii) {
+          const size_t i = (size_t)ii;
+          const double pi[3] = {(double)cl[i]->pos[0], (double)cl[i]->pos[1], (double)cl[i]->pos[2]};
+          const auto& ni = nrm[i];
+          double t = 0.0;
+          if (!(ni[0] == 0.0 && ni[1] == 0.0 && ni[2] == 0.0)) {
+            double sw = 1.0, swd = 0.0;
+            for (long long dz = -1; dz <= 1; ++dz)
+              for (long long dy = -1; dy <= 1; ++dy)
+                for (long long dx = -1; dx <= 1; ++dx) {
+                  auto g = grid.find({cell[i][0] + dx, cell[i][1] + dy, cell[i][2] + dz});
+                  if (g == grid.end()) continue;
+                  for (uint32_t j : g->second) {
+                    const double dv[3] = {(double)cl[j]->pos[0] - pi[0], (double)cl[j]->pos[1] - pi[1],
+                                          (double)cl[j]->pos[2] - pi[2]};
+                    const double d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+                    if (d2 > r2 || j == i) continue;
+                    const auto& nj = nrm[j];
+                    if (ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2] < cos_n) continue;
+                    const double dn = ni[0] * dv[0] + ni[1] * dv[1] + ni[2] * dv[2];
+                    const double w = ps_exp64(-d2 * inv_2ss - dn * dn * inv_2sr);
+                    sw += w;
+                    swd += w * dn;
+                  }
+                }
+            t = swd / sw;
+          }
+          for (int a = 0; a < 3; ++a) next[i][a] = (float)(pi[a] + t * ni[a]);
+        }
+        for (size_t i = 0; i < n; ++i)
+          for (int a = 0; a < 3; ++a) cl[i]->pos[a] = next[i][a];
+      }
+    }
+  }
   uint64_t n_out = 0;
   for (std::vector<FPoint>* part : {&out1, &out2})
     for (auto& pt : *part) {

@@ -142,6 +142,36 @@ def test_visibility_filter_bitwise_vs_oracle(pipeline, residual):
     np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
 
 
+@pytest.mark.parametrize("full", [False, True])
+def test_smoothing_bitwise_vs_oracle(pipeline, full):
+    """smooth_along_normals (crates/dense/src/smooth.rs:143-220) of the device cloud against the restatement (the
+    same binary64 exponential on both sides): positions equal bit for bit; `full` adds the second pass and the
+    visibility filter before it."""
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    imgs = [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views]
+    prm = fusion.default_fusion(2)
+    prm.smooth_iterations, prm.smooth_radius_gsd = 2, 2.0
+    if full:
+        prm.residual = 2
+        prm.visibility_check_views, prm.visibility_min_violations, prm.visibility_tau = 8, 1, 0.002
+    n = s.fuse_resident(0, views, fc, prm)
+    got = s.fused_points()
+    want = oracle.fuse(fc, [st.depth for st in states], [st.normal for st in states], [st.cost for st in states],
+                       imgs, views, prm)
+    assert n == len(want) > 0
+    np.testing.assert_array_equal(got.keys, want.keys)
+    np.testing.assert_array_equal(got.positions, want.positions)
+    np.testing.assert_array_equal(got.normals, want.normals)
+    prm.smooth_iterations = 0
+    s.fuse_resident(0, views, fc, prm)
+    assert (s.fused_points().positions != got.positions).any()  # the smoothing moved points
+
+
 @pytest.mark.parametrize("full_k", [True, False])
 def test_fill_holes_bitwise_vs_oracle(full_k):
     """Speckle removal then hole filling (fill_holes, crates/dense/src/postproc.rs:139-201) on the device readout,

@@ -252,3 +252,50 @@ def test_visibility_filter_matches_independent_restatement(gt_scene):
     assert filt.visibility_removed == int((~keep).sum()) > 0
     np.testing.assert_array_equal(filt.keys, base.keys[keep])
     np.testing.assert_array_equal(filt.positions, base.positions[keep])
+
+
+def test_exp64_is_faithful():
+    """The smoothing weights' exponential (a fixed binary64 sequence shared by the engine and the restatement) is
+    within 1 ulp of the platform's over the arguments the weights take and beyond."""
+    import math
+    xs = np.concatenate([np.linspace(-745.0, 0.0, 20001), -np.logspace(-12, 2, 4001), np.linspace(0.0, 700.0, 2001)])
+    worst = 0
+    for x in xs:
+        a, b = oracle.lib().oracle_exp64(float(x)), math.exp(float(x))
+        if b == 0.0 or not math.isfinite(b):
+            continue
+        worst = max(worst, abs(int(np.float64(a).view(np.int64)) - int(np.float64(b).view(np.int64))))
+    assert worst <= 1
+
+
+def test_smoothing_moves_points_along_normals_toward_the_surface(gt_scene):
+    """smooth_along_normals (crates/dense/src/smooth.rs:143-220): keys and normals stay, every point moves along its
+    own normal only, and noisy depths end up closer to the true surface."""
+    wl, fc = gt_scene
+    rng = np.random.default_rng(9)
+    d = [(g * (1.0 + rng.normal(0, 0.002, g.shape))).astype(np.float32) for g in wl.gt_depth]
+    n = [g.astype(np.float32) for g in wl.gt_normal]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    prm = fusion.default_fusion(2)
+    prm.max_depth_error = 0.02
+    base = oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), prm)
+    prm.smooth_iterations, prm.smooth_radius_gsd = 2, 3.0
+    sm = oracle.fuse(fc, d, n, c, list(wl.images), range(len(d)), prm)
+    np.testing.assert_array_equal(sm.keys, base.keys)
+    np.testing.assert_array_equal(sm.normals, base.normals)
+    mv = sm.positions.astype(np.float64) - base.positions.astype(np.float64)
+    nn = base.normals.astype(np.float64)
+    nn /= np.linalg.norm(nn, axis=1, keepdims=True)
+    tang = mv - (mv * nn).sum(1, keepdims=True) * nn
+    assert np.abs(tang).max() < 1e-4 and np.abs(mv).max() > 0
+
+    def err(cloud):
+        e = []
+        keys = cloud.keys.astype(np.int64)
+        for i in range(0, len(cloud), 11):
+            v, row, col = int(keys[i] >> 32), int((keys[i] >> 16) & 0xFFFF), int(keys[i] & 0xFFFF)
+            pc = wl.cams[v].r @ cloud.positions[i].astype(np.float64) + wl.cams[v].t
+            e.append(abs(pc[2] - wl.gt_depth[v][row, col]))
+        return float(np.median(e))
+
+    assert err(sm) < 0.8 * err(base)

@@ -250,6 +250,8 @@ def bench_ours(args, rank, world, local):
     if args.latency or args.workload == "c5":
         res["latency"] = view_latency(wl, sess, stream, mine)
     res["hbm_high_water_gb"] = round(max(hbm) / 1e9, 2)
+    if not shard_job:
+        res["fusion_all_options"] = fusion_options_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
     sess.close()
     # ---- e2e through the host-buffer C ABI (session begin uploads the images) ----
     if not args.no_e2e:
@@ -342,6 +344,52 @@ def fusion_stage(args, wl, sess, mine, check=True, label="plain"):
         out["oracle_points"] = len(ref)
         out["oracle_s"] = round(time.perf_counter() - t1, 2)
         out["oracle_cores"] = os.cpu_count() or 1
+    return out
+
+
+def fusion_options_stage(wl, sess, mine, check=True, check_views=6):
+    """Every post-processing and fusion option of the reference at once on the final maps: speckle removal, hole
+    filling, consistency fusion with the second pass of leftover pixels, the visibility filter (8 views, 2 violations,
+    1 %) and one smoothing pass, timed through the C ABI over all views.  With `check`, the device fuses the first
+    `check_views` views again and the CPU oracle must give the same cloud bit for bit."""
+    from cumulus3d_b200 import fusion
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    post = fusion.default_post()
+    post.fill_holes = 1
+    prm = fusion.default_fusion(3)
+    prm.residual = 2
+    prm.visibility_check_views, prm.visibility_min_violations, prm.visibility_tau = 8, 2, 0.01
+    prm.smooth_iterations = 1
+    ks = np.array([c.k for c in wl.cams], np.float64)
+    sess.readout_resident(mine, download=False)
+    sess.synchronize()
+    t0 = time.perf_counter()
+    removed, filled = sess.postprocess_resident(0, mine, post, intrinsics=ks, filled=True)
+    n = sess.fuse_resident(0, mine, fc, prm)
+    dt = time.perf_counter() - t0
+    out = {"points": n, "second_pass_points": sess.fused_residual,
+           "visibility_removed": sess.fused_visibility_removed, "speckle_pixels_removed": removed,
+           "pixels_filled": filled, "ms": round(dt * 1e3, 2),
+           "params": "speckles and hole filling (PostParams defaults, fill on); consistency fusion min 3 views with "
+                     "the second pass (ResidualParams defaults); visibility filter 8 views / 2 violations / 1 %; "
+                     "1 smoothing pass (SmoothParams defaults)"}
+    if check:
+        from oracle import oracle
+        from cumulus3d_b200 import scenes
+        sub = list(mine[:check_views])
+        n_sub = sess.fuse_resident(0, sub, fc, prm)
+        got = sess.fused_points()
+        st = sess.readout_download(0, mine)
+        imgs = [scenes.unit_plane(kv.levels[0].pixels) if kv.levels[0].pixels.dtype == np.uint8
+                else kv.levels[0].pixels for kv in wl.input.views]
+        t1 = time.perf_counter()
+        ref = oracle.fuse(fc, [x.depth for x in st], [x.normal for x in st], [x.cost for x in st], imgs, sub, prm)
+        out["check"] = {"views": len(sub), "points": n_sub, "oracle_points": len(ref),
+                        "oracle_s": round(time.perf_counter() - t1, 2),
+                        "equal": bool(len(ref) == n_sub and np.array_equal(ref.keys, got.keys)
+                                      and np.array_equal(ref.positions, got.positions)
+                                      and np.array_equal(ref.normals, got.normals))}
     return out
 
 

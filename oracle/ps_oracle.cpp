@@ -37,6 +37,7 @@
 #include <array>
 #include <cmath>
 #include <map>
+#include <unordered_map>
 #include <vector>
 
 #include "../cumulus3d_b200/csrc/ps_consts.h"
@@ -1608,12 +1609,21 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
       size_t pix;
       FPoint pt;
     };
-    std::vector<Cand> cands;
-    std::vector<std::pair<int, int>> hits;
+    // stage 1 in parallel over rows (the ownership is an atomic minimum, so the order does not matter); candidates
+    // are collected per row and visited in (view, row, column) order afterwards
+    auto fetch_min = [](uint32_t* a, uint32_t v) {
+      uint32_t cur = __atomic_load_n(a, __ATOMIC_RELAXED);
+      while (v < cur && !__atomic_compare_exchange_n(a, &cur, v, true, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {
+      }
+    };
+    std::vector<std::vector<std::vector<Cand>>> cands(nviews);
     for (uint32_t v = 0; v < nviews; ++v) {
       if (!used[v]) continue;
       const FCam& cv = fc[v];
-      for (int row = 0; row < cv.h; ++row)
+      cands[v].resize(cv.h);
+#pragma omp parallel for schedule(dynamic, 4)
+      for (int row = 0; row < cv.h; ++row) {
+        std::vector<std::pair<int, int>> hits;
         for (int col = 0; col < cv.w; ++col) {
           const size_t pix = (size_t)row * cv.w + col;
           if (depth[v][pix] <= 0.0f || consumed[v][pix] != 0) continue;
@@ -1622,13 +1632,16 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
           if (hits.size() < p->residual_min_views) continue;
           if (min_dist > 0.0 && any_within(pt.pos)) continue;
           const uint32_t id = (uint32_t)(offset[v] + pix);
-          owner[v][pix] = std::min(owner[v][pix], id);
-          for (auto& hq : hits) owner[hq.first][hq.second] = std::min(owner[hq.first][hq.second], id);
-          cands.push_back({v, pix, std::move(pt)});
+          fetch_min(&owner[v][pix], id);
+          for (auto& hq : hits) fetch_min(&owner[hq.first][hq.second], id);
+          cands[v][row].push_back({v, pix, std::move(pt)});
         }
+      }
     }
-    for (auto& c : cands)
-      if (owner[c.v][c.pix] == (uint32_t)(offset[c.v] + c.pix)) out2.push_back(std::move(c.pt));
+    for (auto& cv : cands)
+      for (auto& cr : cv)
+        for (auto& c : cr)
+          if (owner[c.v][c.pix] == (uint32_t)(offset[c.v] + c.pix)) out2.push_back(std::move(c.pt));
   }
   // filter_visibility (crates/dense/src/visibility.rs:106-151) over both passes' points, order kept
   uint64_t vis_removed = 0;
@@ -1715,11 +1728,16 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
         nrm[i] = l > 1e-12 ? std::array<double, 3>{m[0] / l, m[1] / l, m[2] / l} : std::array<double, 3>{0.0, 0.0, 0.0};
       }
       for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
-        std::map<std::array<long long, 3>, std::vector<uint32_t>> grid;  // cell -> points in cloud order
+        // cell -> points in cloud order (cells packed 21 bits per axis around 2^20; the device requires that range)
+        auto pack = [](long long x, long long y, long long z) {
+          return ((uint64_t)(x + (1ll << 20)) << 42) | ((uint64_t)(y + (1ll << 20)) << 21) | (uint64_t)(z + (1ll << 20));
+        };
+        std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
+        grid.reserve(n);
         std::vector<std::array<long long, 3>> cell(n);
         for (size_t i = 0; i < n; ++i) {
           for (int a = 0; a < 3; ++a) cell[i][a] = (long long)std::floor((double)cl[i]->pos[a] / r);
-          grid[cell[i]].push_back((uint32_t)i);
+          grid[pack(cell[i][0], cell[i][1], cell[i][2])].push_back((uint32_t)i);
         }
         std::vector<std::array<float, 3>> next(n);
 #pragma omp parallel for schedule(dynamic, 256)
@@ -1733,7 +1751,7 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
             for (long long dz = -1; dz <= 1; ++dz)
               for (long long dy = -1; dy <= 1; ++dy)
                 for (long long dx = -1; dx <= 1; ++dx) {
-                  auto g = grid.find({cell[i][0] + dx, cell[i][1] + dy, cell[i][2] + dz});
+                  auto g = grid.find(pack(cell[i][0] + dx, cell[i][1] + dy, cell[i][2] + dz));
                   if (g == grid.end()) continue;
                   for (uint32_t j : g->second) {
                     const double dv[3] = {(double)cl[j]->pos[0] - pi[0], (double)cl[j]->pos[1] - pi[1],

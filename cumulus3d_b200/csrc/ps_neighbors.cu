@@ -10,7 +10,7 @@
 // Layout: the pairs of n views are a dense n×n table indexed min(a,b)·n + max(a,b) (n <= 4096).  Pass 0 counts the
 // pairs of every track, a one-CTA scan turns the counts into segment offsets (and lists the non-empty pairs in
 // ascending order), pass 1 writes each pair's angles into its segment, and one CTA per non-empty pair finds the two
-// order statistics around 0.75·(m-1) exactly (bisection over order-preserving keys; no sort).  Depth observations
+// order statistics around 0.75·(m-1) exactly (radix select over order-preserving keys; no sort).  Depth observations
 // follow the same count / scan / scatter / order-statistic scheme per view.  One CTA per view then selects its
 // sources: candidates gated by the 75th-percentile angle, repeatedly the best by (score, shared count, lower index).
 #include <cuda_runtime.h>
@@ -142,17 +142,6 @@ __global__ void __launch_bounds__(1024) k_nb_scan(const unsigned* __restrict__ c
   }
 }
 
-__device__ __forceinline__ unsigned long long block_sum(unsigned long long v, unsigned long long* red) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();  // red may still be read from the previous call
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  unsigned long long s = 0;
-  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
-  return s;
-}
-
 // Order-preserving unsigned keys of binary32 / binary64 values (negative values reversed below the positives).
 __device__ __forceinline__ unsigned key32(float f) {
   const unsigned u = __float_as_uint(f);
@@ -169,29 +158,42 @@ __device__ __forceinline__ double unkey64(unsigned long long k) {
   return __longlong_as_double((long long)((k >> 63) ? (k & 0x7fffffffffffffffull) : ~k));
 }
 
-// The k-th smallest (0-based) of seg[0..m): the smallest key with more than k keys at or below it, by bisection
-// (32 or 64 halvings of the key range, each one pass over the segment).  Every thread of the CTA returns it.
-__device__ float kth32(const float* seg, unsigned m, unsigned k, unsigned long long* red) {
-  unsigned lo = 0u, hi = 0xffffffffu;
-  while (lo < hi) {
-    const unsigned mid = lo + (hi - lo) / 2u;
-    unsigned long long c = 0;
-    for (unsigned i = threadIdx.x; i < m; i += blockDim.x) c += key32(seg[i]) <= mid;
-    if (block_sum(c, red) >= (unsigned long long)k + 1ull) hi = mid;
-    else lo = mid + 1u;
+// The k-th smallest (0-based) of seg[0..m) by radix select over the order-preserving keys: 8-bit digits from the
+// most significant; each pass counts, in a shared histogram, the digit of every key that agrees with the digits
+// chosen so far, and takes the digit whose running count passes k (4 passes for binary32, 8 for binary64).  Every
+// thread of the CTA returns it.
+template <typename T, typename K, typename KeyFn>
+__device__ K radix_kth(const T* seg, unsigned m, unsigned k, KeyFn key, unsigned* hist, K* chosen) {
+  constexpr int NB = (int)sizeof(K) * 8;
+  K prefix = 0, mask = 0;
+  unsigned rank = k;
+  for (int shift = NB - 8; shift >= 0; shift -= 8) {
+    for (int d = threadIdx.x; d < 256; d += blockDim.x) hist[d] = 0u;
+    __syncthreads();
+    for (unsigned i = threadIdx.x; i < m; i += blockDim.x) {
+      const K kk = key(seg[i]);
+      if ((kk & mask) == prefix) atomicAdd(&hist[(unsigned)(kk >> shift) & 255u], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      unsigned cum = 0, d = 0;
+      for (; d < 255u && cum + hist[d] <= rank; ++d) cum += hist[d];
+      chosen[0] = (K)d;
+      chosen[1] = (K)(rank - cum);
+    }
+    __syncthreads();
+    prefix |= chosen[0] << shift;
+    mask |= (K)255 << shift;
+    rank = (unsigned)chosen[1];
+    __syncthreads();
   }
-  return unkey32(lo);
+  return prefix;
 }
-__device__ double kth64(const double* seg, unsigned m, unsigned k, unsigned long long* red) {
-  unsigned long long lo = 0ull, hi = ~0ull;
-  while (lo < hi) {
-    const unsigned long long mid = lo + (hi - lo) / 2ull;
-    unsigned long long c = 0;
-    for (unsigned i = threadIdx.x; i < m; i += blockDim.x) c += key64(seg[i]) <= mid;
-    if (block_sum(c, red) >= (unsigned long long)k + 1ull) hi = mid;
-    else lo = mid + 1ull;
-  }
-  return unkey64(lo);
+__device__ float kth32(const float* seg, unsigned m, unsigned k, unsigned* hist, unsigned* chosen) {
+  return unkey32(radix_kth<float, unsigned>(seg, m, k, [](float f) { return key32(f); }, hist, chosen));
+}
+__device__ double kth64(const double* seg, unsigned m, unsigned k, unsigned* hist, unsigned long long* chosen) {
+  return unkey64(radix_kth<double, unsigned long long>(seg, m, k, [](double f) { return key64(f); }, hist, chosen));
 }
 
 // quantile_sorted(angles, 0.75) of every non-empty pair (crates/dense/src/math.rs:126-135): the order statistics at
@@ -199,7 +201,8 @@ __device__ double kth64(const double* seg, unsigned m, unsigned k, unsigned long
 __global__ void __launch_bounds__(NB_NT) k_nb_q75(const unsigned* __restrict__ nz, const unsigned* __restrict__ cnt,
                                                   const unsigned long long* __restrict__ off,
                                                   const float* __restrict__ ang, double* q75) {
-  __shared__ unsigned long long red[NB_NT / 32];
+  __shared__ unsigned hist[256];
+  __shared__ unsigned chosen[2];
   const unsigned key = nz[blockIdx.x];
   const unsigned m = cnt[key];
   const float* seg = ang + off[key];
@@ -207,8 +210,8 @@ __global__ void __launch_bounds__(NB_NT) k_nb_q75(const unsigned* __restrict__ n
   const unsigned lo = (unsigned)floor(pos);
   const unsigned hi = min(lo + 1u, m - 1u);
   const double f = pos - (double)lo;
-  const double vlo = (double)kth32(seg, m, lo, red);
-  const double vhi = hi == lo ? vlo : (double)kth32(seg, m, hi, red);
+  const double vlo = (double)kth32(seg, m, lo, hist, chosen);
+  const double vhi = hi == lo ? vlo : (double)kth32(seg, m, hi, hist, chosen);
   if (threadIdx.x == 0) q75[key] = vlo + (vhi - vlo) * f;
 }
 
@@ -217,7 +220,8 @@ __global__ void __launch_bounds__(NB_NT) k_nb_q75(const unsigned* __restrict__ n
 __global__ void __launch_bounds__(NB_NT) k_nb_range(const unsigned* __restrict__ cnt,
                                                     const unsigned long long* __restrict__ off,
                                                     const double* __restrict__ dep, double* range, uint8_t* has) {
-  __shared__ unsigned long long red[NB_NT / 32];
+  __shared__ unsigned hist[256];
+  __shared__ unsigned long long chosen[2];
   const int v = blockIdx.x;
   const unsigned n = cnt[v];
   if (n == 0) {
@@ -230,8 +234,8 @@ __global__ void __launch_bounds__(NB_NT) k_nb_range(const unsigned* __restrict__
   const double* seg = dep + off[v];
   const unsigned ilo = min((unsigned)floor((double)n * 0.01), n - 1u);
   const unsigned ihi = min((unsigned)floor((double)n * 0.99), n - 1u);
-  const double lo = kth64(seg, n, ilo, red);
-  const double hi = kth64(seg, n, ihi, red);
+  const double lo = kth64(seg, n, ilo, hist, chosen);
+  const double hi = kth64(seg, n, ihi, hist, chosen);
   if (threadIdx.x == 0) {
     has[v] = 1;
     range[2 * v] = 0.75 * lo;

@@ -403,7 +403,7 @@ def neighbors_stage(wl, sess, mine, local, check=True):
     from cumulus3d_b200 import scenes
     from cumulus3d_b200.neighbors import NeighborParams, select_neighbors
     st = sess.readout_download(0, mine)
-    depth = np.stack([x.depth for x in st])
+    depth = [x.depth for x in st]  # one map per view (views may differ in size)
     model = scenes.sparse_model([wl.cams[v] for v in mine], depth, 20000, seed=11)
     prm = NeighborParams()
     select_neighbors(model, prm, local)  # warm-up (module load)

@@ -187,3 +187,15 @@ def test_invalid_tracks_are_rejected_before_any_device_work():
     with pytest.raises(_lib.PsError) as e:
         neighbors.call(lib.ps_select_neighbors, m, NeighborParams(0, 1.0), False, 0)
     assert e.value.code == _lib.PS_EINVAL
+
+
+def test_sparse_model_of_views_of_different_sizes():
+    """Tracks from depth maps of different sizes (one map per view, not a stacked array)."""
+    from cumulus3d_b200 import scenes
+    cams = scenes.formation(64, 48, 1, prefix="a") + scenes.formation(96, 72, 1, prefix="b", y0=1.0)
+    depth = [np.full((c.height, c.width), 30.0, np.float32) for c in cams]
+    m = scenes.sparse_model(cams, depth, 200, seed=1, rel_tol=0.5)
+    assert m.num_views == len(cams) and len(m.track_offsets) == m.xyz.shape[0] + 1
+    assert int(m.track_offsets[-1]) == m.track_views.size and m.track_views.max() < len(cams)
+    r = oracle.select_neighbors(m, NeighborParams(2, 0.0))
+    assert len(r.sources) == len(cams)

@@ -4,7 +4,7 @@ A BF16 encoder-decoder (``ps_net_*`` in include/patchstereo.h, kernels in csrc/p
 a confidence per pixel from the reference image and a 32-plane NCC sweep volume (``ps_sweep_volume``).  A photometric
 run that starts with ``random_init = PS_INIT_PROPOSAL`` takes the proposed plane wherever the confidence reached the
 threshold and the ordinary seeded random draw everywhere else, so plain PatchStereo initialisation is the per-pixel
-fallback and plain PatchStereo itself is the judge of the result.
+fallback, and the PatchStereo iterations that follow decide every pixel's final plane.
 
 Training data are the engine's own outputs: seeded synthetic terrains seen through the 1920×1080 camera formation of
 the aerial workloads, cut into 256×256 reference crops (a crop is the same camera with a shifted principal point)

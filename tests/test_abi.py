@@ -117,3 +117,39 @@ def test_defaults_match_reference():
     o = _lib.Options()
     _lib.engine().ps_options_default(C.byref(o))
     assert (o.math_mode, o.max_batch, o.batch_pixels, o.checked, o.tuning) == (0, 64, 0, 0, 0)
+
+
+def test_post_fusion_and_neighbour_defaults_match_reference():
+    """PostParams (crates/dense/src/postproc.rs:61-74), FusionParams with ResidualParams / VisibilityParams /
+    SmoothParams (crates/dense/src/params.rs:278-351, visibility.rs:60-64, smooth.rs:67-71) and NeighborOptions
+    (params.rs:366-369) defaults."""
+    import math
+    lib = _lib.engine()
+    post = _lib.PostParams()
+    lib.ps_post_params_default(C.byref(post))
+    assert (post.remove_speckles, post.fill_holes) == (1, 0)
+    for name, want in [("speckle_rel_depth", 0.02), ("speckle_min_area_frac", 2e-4), ("speckle_keep_cost", 0.2),
+                       ("fill_max_frac", 0.01), ("fill_edge_step", 0.06), ("fill_max_cost", 1.0)]:
+        assert abs(getattr(post, name) - want) < 1e-7, name
+    f = _lib.FusionParams()
+    lib.ps_fusion_params_default(C.byref(f))
+    assert (f.min_consistent_views, f.consistency_num_images, f.mark_used, f.mark_radius, f.inverse_variance,
+            f.residual, f.residual_min_views) == (5, 12, 1, 0, 1, _lib.PS_FUSION_RESIDUAL_NONE, 2)
+    assert math.isnan(f.residual_depth_error) and math.isnan(f.residual_normal_error_deg)
+    assert f.residual_min_dist_gsd == 0.5
+    assert (f.visibility_check_views, f.visibility_min_violations, f.visibility_tau) == (0, 2, 0.01)
+    assert (f.smooth_iterations, f.smooth_radius_gsd, f.smooth_sigma_range_gsd, f.smooth_normal_deg) == \
+        (0, 1.0, 0.25, 30.0)
+    nb = _lib.NeighborParams()
+    lib.ps_neighbor_params_default(C.byref(nb))
+    assert (nb.num_views, nb.direction_bins, nb.min_triangulation_angle_deg, nb.diversity_decay) == (10, 8, 1.0, 1.0)
+
+
+def test_reciprocal_check_validates_its_range_without_device():
+    lib = _lib.engine()
+    bad = C.c_uint64()
+    assert lib.ps_check_reciprocal(0, -127, 0, C.byref(bad), None) == _lib.PS_EINVAL
+    assert lib.ps_check_reciprocal(0, 0, 128, C.byref(bad), None) == _lib.PS_EINVAL
+    assert lib.ps_check_reciprocal(0, 5, 4, C.byref(bad), None) == _lib.PS_EINVAL
+    assert lib.ps_check_reciprocal(0, 0, 1, None, None) == _lib.PS_EINVAL
+    assert lib.ps_fused_visibility_removed(None, C.byref(bad)) == _lib.PS_EINVAL

@@ -110,6 +110,14 @@ class FusionParams(C.Structure):
                 ("smooth_normal_deg", C.c_double)]
 
 
+class ScoreFusionParams(C.Structure):
+    """ScoreFusionOptions of score fusion (crates/dense/src/fusion_score.rs:56-103)."""
+    _fields_ = [("sigma_e_px", C.c_double), ("sigma_theta_deg", C.c_double), ("lambda", C.c_double),
+                ("tau", C.c_double), ("depth_error", C.c_double), ("normal_error_deg", C.c_double),
+                ("num_neighbors", C.c_uint32), ("mark_used", C.c_uint32), ("inverse_variance", C.c_uint32),
+                ("reserved", C.c_uint32), ("sigma_px0", C.c_double), ("sigma_px_slope", C.c_double)]
+
+
 class FusionView(C.Structure):
     _fields_ = [("k", C.c_double * 4), ("r", C.c_double * 9), ("t", C.c_double * 3), ("baseline", C.c_double),
                 ("image_id", C.c_uint32), ("num_overlap", C.c_uint32), ("overlap", C.POINTER(C.c_uint32))]
@@ -190,6 +198,9 @@ SIGNATURES = {
     "ps_fuse_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView), C.POINTER(FusionParams),
                                    C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "ps_fused_visibility_removed": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "ps_score_fusion_params_default": (None, [C.POINTER(ScoreFusionParams)]),
+    "ps_fuse_scored_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView),
+                                          C.POINTER(ScoreFusionParams), C.POINTER(C.c_uint64)]),
     "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_uint32]),
     "ps_build_pyramid": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.c_uint32,

@@ -13,6 +13,10 @@
 //    (k·ln2_hi exact for |k| < 2^21) and a tail, both products folded with fma; the degree-13 Taylor polynomial of
 //    e^r on |r| <= ln2/2 (truncation below 2^-57 relative) by Horner's rule with fma; scaling by 2^k through the
 //    exponent field (in two steps below 2^-1022).  Arguments above 709 give +inf, below -745.2 give +0.
+//  * ps_acos64: binary64 arc cosine on [-1, 1]: acos x = pi/2 - asin x for |x| <= 1/2, 2·asin(sqrt((1 - x)/2)) above
+//    and pi - 2·asin(sqrt((1 + x)/2)) below (1 ∓ x and the halving are exact there); asin y on |y| <= 1/2 by its Taylor
+//    series y·Σ c_n y^(2n), c_n = (2n)!/(4^n (n!)^2 (2n+1)), 28 terms by Horner's rule with fma (truncation below
+//    2^-60 relative).
 //  * ps_sincosf: Cody–Waite reduction by pi/2 (three-part split of pi/2 folded with fma, valid for |x| < 1e5),
 //    then Taylor polynomials of degree 9 (sin) and 10 (cos) on |r| <= pi/4 (truncation error < 2e-9), with the
 //    quadrant selecting sign and swap.
@@ -105,6 +109,45 @@ PS_HD double ps_exp64(double x) {
   const int ki = (int)k;  // -1075 .. 1023
   if (ki >= -1022) return p * ps_u2d((uint64_t)(ki + 1023) << 52);
   return (p * ps_u2d((uint64_t)(ki + 1023 + 600) << 52)) * ps_u2d((uint64_t)(1023 - 600) << 52);
+}
+
+PS_HD double ps_asin_half64(double y) {  // |y| <= 1/2
+  const double y2 = y * y;
+  double p = 0.0019650336162772837;
+  p = fma(p, y2, 0.0020776610325181676);
+  p = fma(p, y2, 0.0022014739737101384);
+  p = fma(p, y2, 0.002338091892111975);
+  p = fma(p, y2, 0.0024894486782468836);
+  p = fma(p, y2, 0.00265787063820729);
+  p = fma(p, y2, 0.002846178401108942);
+  p = fma(p, y2, 0.0030578216492580306);
+  p = fma(p, y2, 0.003297059503473485);
+  p = fma(p, y2, 0.0035692053938259347);
+  p = fma(p, y2, 0.003880964558837669);
+  p = fma(p, y2, 0.004240907093679363);
+  p = fma(p, y2, 0.004660143486915096);
+  p = fma(p, y2, 0.005153309682319905);
+  p = fma(p, y2, 0.005740037670841924);
+  p = fma(p, y2, 0.006447210311889649);
+  p = fma(p, y2, 0.0073125258735988454);
+  p = fma(p, y2, 0.008390335809616815);
+  p = fma(p, y2, 0.009761609529194078);
+  p = fma(p, y2, 0.011551800896139705);
+  p = fma(p, y2, 0.01396484375);
+  p = fma(p, y2, 0.017352764423076924);
+  p = fma(p, y2, 0.022372159090909092);
+  p = fma(p, y2, 0.030381944444444444);
+  p = fma(p, y2, 0.044642857142857144);
+  p = fma(p, y2, 0.075);
+  p = fma(p, y2, 0.16666666666666666);
+  return fma(y * y2, p, y);
+}
+
+PS_HD double ps_acos64(double x) {
+  if (!(x == x)) return x;
+  if (x > 0.5) return 2.0 * ps_asin_half64(sqrt((1.0 - x) * 0.5));
+  if (x < -0.5) return 3.141592653589793 - 2.0 * ps_asin_half64(sqrt((1.0 + x) * 0.5));
+  return 1.5707963267948966 - ps_asin_half64(x);
 }
 
 PS_HD void ps_sincosf(float x, float* s, float* c) {

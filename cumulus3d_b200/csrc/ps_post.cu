@@ -296,20 +296,8 @@ __device__ bool fuse_eval(const FuseArgs& A, const FuseView& cv, int col, int ro
   return !(P.l < 1.1920928955078125e-07);  // f32::EPSILON
 }
 
-// Writes one fused point (its slot from the shared counter): mean position, normalised normal, rounded colour, key
-// and the sorted, de-duplicated {v} ∪ hit views.
-__device__ void fuse_emit(const FuseArgs& A, const FuseView& cv, int v, int col, int row, const FusePoint& P,
-                          const Hit* hits, int nh) {
-  const unsigned long long slot = atomicAdd(A.count, 1ull);
-  if (slot >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
-  for (int k = 0; k < 3; ++k) {
-    A.pos[3 * slot + k] = (float)(P.sx[k] / P.m);
-    A.nrm[3 * slot + k] = (float)(P.sn[k] / P.l);
-    A.col[3 * slot + k] = (unsigned char)round(P.sc[k] / P.m);
-  }
-  A.key[slot] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
-                (unsigned long long)(col & 0xffff);
-  unsigned short* vis = A.vis + slot * A.vis_stride;
+// The sorted, de-duplicated {v} ∪ hit views into vis; returns their number.
+__device__ int write_vis(unsigned short* vis, int v, const Hit* hits, int nh) {
   int nv = 0;
   vis[nv++] = (unsigned short)v;
   for (int i = 0; i < nh; ++i) {
@@ -325,7 +313,23 @@ __device__ void fuse_emit(const FuseArgs& A, const FuseView& cv, int v, int col,
     vis[j] = o;
     nv++;
   }
-  A.nvis[slot] = (unsigned char)nv;
+  return nv;
+}
+
+// Writes one fused point (its slot from the shared counter): mean position, normalised normal, rounded colour, key
+// and the sorted, de-duplicated {v} ∪ hit views.
+__device__ void fuse_emit(const FuseArgs& A, const FuseView& cv, int v, int col, int row, const FusePoint& P,
+                          const Hit* hits, int nh) {
+  const unsigned long long slot = atomicAdd(A.count, 1ull);
+  if (slot >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
+  for (int k = 0; k < 3; ++k) {
+    A.pos[3 * slot + k] = (float)(P.sx[k] / P.m);
+    A.nrm[3 * slot + k] = (float)(P.sn[k] / P.l);
+    A.col[3 * slot + k] = (unsigned char)round(P.sc[k] / P.m);
+  }
+  A.key[slot] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
+                (unsigned long long)(col & 0xffff);
+  A.nvis[slot] = (unsigned char)write_vis(A.vis + slot * A.vis_stride, v, hits, nh);
 }
 
 // First pass (fusion.rs:243-333) of view A.v: one thread per reference pixel.
@@ -459,6 +463,194 @@ __global__ void __launch_bounds__(256) k_fuse_second(FuseArgs A, int stage) {
     return;
   }
   fuse_emit(A, cv, A.v, col, row, P, hits, nh);
+}
+
+// ---- score fusion (crates/dense/src/fusion_score.rs:196-435) -------------------------------------------------
+// Comparisons spelled as the CPU restatement's std::min / std::max, so that NaN inputs take the same branch there.
+__device__ __forceinline__ double sc_clamp(double x, double lo, double hi) {
+  x = x < lo ? lo : x;
+  return hi < x ? hi : x;
+}
+// camera centre -Rᵀ t (DenseView::center, crates/dense/src/scene.rs:82-89)
+__device__ __forceinline__ void sc_centre(const FuseView& c, double* o) {
+  for (int j = 0; j < 3; ++j) o[j] = -(c.r[0 * 3 + j] * c.t[0] + c.r[1 * 3 + j] * c.t[1] + c.r[2 * 3 + j] * c.t[2]);
+}
+// inv_var (fusion_score.rs:161-171)
+__device__ __forceinline__ double sc_inv_var(const ScoreArgs& A, const FuseView& c, double d, float cost) {
+  if (!A.inverse_variance || !(c.baseline > 0.0)) return 1.0;
+  float cc = cost < 0.0f ? 0.0f : cost;
+  cc = 2.0f < cc ? 2.0f : cc;
+  const double spx = A.sigma0 + A.slope * (double)cc;
+  const double sd = d * d * spx / (c.k[0] * c.baseline);
+  const double v = sd * sd;
+  return 1.0 / (v < 1e-300 ? 1e-300 : v);
+}
+// IEEE total order of binary32 as an unsigned key (f32::total_cmp)
+__device__ __forceinline__ unsigned sc_total_key(float f) {
+  const unsigned k = __float_as_uint(f);
+  return (k & 0x80000000u) ? ~k : (k | 0x80000000u);
+}
+
+// view_candidates (fusion_score.rs:196-303): one thread per reference pixel of view A.v.  The reference walks its
+// pixels in order; here each candidate takes the next free record and its candidate number restores the order.
+__global__ void __launch_bounds__(256) k_score(const ScoreArgs A) {
+  const FuseView& cv = A.views[A.v];
+  const int col = blockIdx.x * 32 + threadIdx.x, row = blockIdx.y * 8 + threadIdx.y;
+  if (col >= cv.w || row >= cv.h) return;
+  const long long pix = (long long)row * cv.w + col;
+  const float4 q = A.plane[cv.off + pix];
+  const double d = (double)q.w;
+  if (!(d > 0.0)) return;
+  double x[3], nw[3], cr[3];
+  backproject(cv, (double)col, (double)row, d, x);
+  normal_world(cv, q, nw);
+  sc_centre(cv, cr);
+  const double rr[3] = {x[0] - cr[0], x[1] - cr[1], x[2] - cr[2]};
+  const double l_ref = sqrt(rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2]);
+  const float cost0 = A.cost[cv.off + pix];
+  const double s_ref = sc_clamp(1.0 - (double)cost0, 0.0, 1.0);
+  const double w0 = s_ref * sc_inv_var(A, cv, d, cost0);
+  double sum_s = s_ref, sum_p = 0.0, sw = w0, sx[3], sn[3], sc[3];
+  for (int k = 0; k < 3; ++k) {
+    sx[k] = x[k] * w0;
+    sn[k] = nw[k] * w0;
+  }
+  const double c0 = gray_u8(cv, col, row);
+  sc[0] = sc[1] = sc[2] = c0 * w0;
+  Hit hits[PS_FUSE_MAX_OVERLAP];
+  int nh = 0;
+  for (int i = 0; i < cv.nov; ++i) {
+    const int j = cv.ov[i];
+    const FuseView& oc = A.views[j];
+    double u, vv, z;
+    if (!project(oc, x, &u, &vv, &z)) continue;
+    const double cu = floor(u + 0.5), rv = floor(vv + 0.5);
+    if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
+    const int opix = (int)rv * oc.w + (int)cu;
+    const float4 oq = A.plane[oc.off + opix];
+    const double od = (double)oq.w;
+    if (od <= 0.0) continue;
+    const float ocost = A.cost[oc.off + opix];
+    const double cj = sc_clamp(1.0 - (double)ocost, 0.0, 1.0);
+    if (fabs(z - od) / od > A.depth_tol) {
+      if (z < od * (1.0 - A.depth_tol)) sum_p += cj;  // free-space violation
+      continue;
+    }
+    double no[3];
+    normal_world(oc, oq, no);
+    if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < A.cos_n) continue;
+    double xo[3];
+    backproject(oc, cu, rv, od, xo);
+    double bu, bv, bz;
+    if (!project(cv, xo, &bu, &bv, &bz)) continue;
+    const double eu = bu - (double)col, ev = bv - (double)row;
+    const double e2 = eu * eu + ev * ev;
+    double cj3[3];
+    sc_centre(oc, cj3);
+    const double rj[3] = {x[0] - cj3[0], x[1] - cj3[1], x[2] - cj3[2]};
+    const double cos_t = sc_clamp((rr[0] * rj[0] + rr[1] * rj[1] + rr[2] * rj[2]) /
+                                      (l_ref * sqrt(rj[0] * rj[0] + rj[1] * rj[1] + rj[2] * rj[2])),
+                                  -1.0, 1.0);
+    const double th = ps_acos64(cos_t);
+    const double sj = cj * ps_exp64(-e2 * A.k_e) * (1.0 - ps_exp64(-th * th * A.k_t));
+    sum_s += sj;
+    if (sj <= 0.0) continue;
+    const double wo = sj * sc_inv_var(A, oc, od, ocost);
+    const double co = gray_u8(oc, (int)cu, (int)rv);
+    sw += wo;
+    for (int k = 0; k < 3; ++k) {
+      sx[k] += wo * xo[k];
+      sn[k] += wo * no[k];
+      sc[k] += wo * co;
+    }
+    hits[nh].o = j;
+    hits[nh].q = opix;
+    nh++;
+  }
+  const double score = sum_s - A.lambda * sum_p;
+  if (score < A.tau || sw <= 0.0 || !isfinite(sw)) return;
+  const double l = sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+  if (l < 1.1920928955078125e-07) return;  // f32::EPSILON
+  const unsigned long long c = atomicAdd(A.count, 1ull);
+  if (c >= A.capacity) return;  // cannot happen: capacity = valid pixels of the fused views
+  for (int k = 0; k < 3; ++k) {
+    A.pos[3 * c + k] = (float)(sx[k] / sw);
+    A.nrm[3 * c + k] = (float)(sn[k] / l);
+    A.col[3 * c + k] = (unsigned char)sc_clamp(round(sc[k] / sw), 0.0, 255.0);
+  }
+  A.key[c] = ((unsigned long long)cv.image_id << 32) | ((unsigned long long)(row & 0xffff) << 16) |
+             (unsigned long long)(col & 0xffff);
+  A.nvis[c] = (unsigned char)write_vis(A.vis + c * A.vis_stride, A.v, hits, nh);
+  const unsigned g = cv.idbase + (unsigned)pix;
+  A.gid[c] = g;
+  A.prio[c] = ((unsigned long long)(~sc_total_key((float)score)) << 32) | (unsigned long long)(g + 1u);
+  unsigned* px = A.pix + c * A.pix_stride;
+  px[0] = (unsigned)(cv.off + pix);
+  for (int i = 0; i < nh; ++i) px[1 + i] = (unsigned)(A.views[hits[i].o].off + hits[i].q);
+  A.npix[c] = (unsigned char)(1 + nh);
+  A.state[c] = A.mark_used ? 2 : 1;
+}
+
+__global__ void k_score_init(const ScoreArgs A, unsigned n) {
+  const unsigned i = blockIdx.x * 256u + threadIdx.x;
+  if (i == 0) *A.ncur = n;
+  if (i < n) const_cast<unsigned*>(A.active)[i] = i;
+}
+
+// Adoption rounds (fusion_score.rs:352-414), one kernel per phase.  Phase 1: every undecided candidate frees its
+// pixels that are not locked, and one that touches a locked pixel is rejected (the reference rejects it in the next
+// phase; locks change only in phase 3, so both see the same locks).
+__global__ void __launch_bounds__(256) k_score_reset(const ScoreArgs A) {
+  const unsigned n = *A.ncur;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *A.nnext = 0;
+  for (unsigned t = blockIdx.x * 256u + threadIdx.x; t < n; t += gridDim.x * 256u) {
+    const unsigned c = A.active[t];
+    const unsigned* px = A.pix + (size_t)c * A.pix_stride;
+    const int np = A.npix[c];
+    bool locked = false;
+    for (int i = 0; i < np; ++i) {
+      unsigned long long* cl = A.claim + px[i];
+      if (*cl == PS_SCORE_LOCKED)
+        locked = true;
+      else
+        *cl = PS_SCORE_FREE;
+    }
+    if (locked) A.state[c] = 0;
+  }
+}
+// Phase 2: the undecided candidates claim their pixels by their priority (atomic minimum).
+__global__ void __launch_bounds__(256) k_score_claim(const ScoreArgs A) {
+  const unsigned n = *A.ncur;
+  for (unsigned t = blockIdx.x * 256u + threadIdx.x; t < n; t += gridDim.x * 256u) {
+    const unsigned c = A.active[t];
+    if (A.state[c] != 2) continue;
+    const unsigned* px = A.pix + (size_t)c * A.pix_stride;
+    const unsigned long long pr = A.prio[c];
+    const int np = A.npix[c];
+    for (int i = 0; i < np; ++i) atomicMin(A.claim + px[i], pr);
+  }
+}
+// Phase 3: a candidate that holds all its pixels is adopted and locks them; the other undecided ones go to the next
+// round.  A pixel that holds this candidate's priority is claimed by no adopted candidate but this one, so the locks
+// written meanwhile by others never touch it: adoption and locking can share the launch.
+__global__ void __launch_bounds__(256) k_score_adopt(const ScoreArgs A) {
+  const unsigned n = *A.ncur;
+  for (unsigned t = blockIdx.x * 256u + threadIdx.x; t < n; t += gridDim.x * 256u) {
+    const unsigned c = A.active[t];
+    if (A.state[c] != 2) continue;
+    const unsigned* px = A.pix + (size_t)c * A.pix_stride;
+    const unsigned long long pr = A.prio[c];
+    const int np = A.npix[c];
+    bool all = true;
+    for (int i = 0; i < np; ++i) all = all && A.claim[px[i]] == pr;
+    if (all) {
+      A.state[c] = 1;
+      for (int i = 0; i < np; ++i) A.claim[px[i]] = PS_SCORE_LOCKED;
+      atomicAdd(A.adopted, 1ull);
+    } else {
+      A.next[atomicAdd(A.nnext, 1u)] = c;
+    }
+  }
 }
 
 // Every 97th valid depth of a view in row-major order (one CTA of 1024 threads walks the view in chunks with a block
@@ -720,6 +912,24 @@ cudaError_t launch_fuse(const FuseArgs& A, int w, int h, cudaStream_t st) {
 cudaError_t launch_fuse_second(const FuseArgs& A, int w, int h, int stage, cudaStream_t st) {
   const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
   k_fuse_second<<<g, b, 0, st>>>(A, stage);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_score_candidates(const ScoreArgs& A, int w, int h, cudaStream_t st) {
+  const dim3 b(32, 8), g((w + 31) / 32, (h + 7) / 8);
+  k_score<<<g, b, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_score_init(const ScoreArgs& A, unsigned n, cudaStream_t st) {
+  k_score_init<<<(n + 255) / 256 + (n == 0), 256, 0, st>>>(A, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_score_round(const ScoreArgs& A, int blocks, cudaStream_t st) {
+  k_score_reset<<<blocks, 256, 0, st>>>(A);
+  k_score_claim<<<blocks, 256, 0, st>>>(A);
+  k_score_adopt<<<blocks, 256, 0, st>>>(A);
   return cudaGetLastError();
 }
 

@@ -71,6 +71,49 @@ struct FuseArgs {
   double gcell;                     // cell size = minimum distance
 };
 
+// Score fusion (fuse_scored, crates/dense/src/fusion_score.rs:196-435).  Candidates are appended in any order; each
+// carries its candidate number gid = idbase + pixel, whose order is the output order, and its priority
+// (~total_order(score) << 32) | (gid + 1), smaller first, so that score descends and ties go to (view, pixel) order.
+#define PS_SCORE_FREE 0xffffffffffffffffull
+#define PS_SCORE_LOCKED 0ull
+struct ScoreArgs {
+  const FuseView* views;  // camera, slot offset, candidate numbering and overlap list per session view
+  int v;                  // reference view of a candidate launch
+  const float4* plane;    // readout planes of the level (slot layout)
+  const float* cost;
+  int inverse_variance, mark_used;
+  double sigma0, slope, depth_tol, cos_n, k_e, k_t, lambda, tau;
+  // candidates (capacity entries)
+  float* pos;
+  float* nrm;
+  unsigned char* col;
+  unsigned long long* key;
+  unsigned char* nvis;
+  unsigned short* vis;
+  int vis_stride;
+  unsigned* gid;
+  unsigned long long* prio;
+  unsigned* pix;          // pix_stride slot pixels per candidate: its reference pixel, then its agreeing pixels
+  unsigned char* npix;
+  int pix_stride;
+  unsigned char* state;   // 2 undecided, 1 adopted, 0 rejected
+  unsigned long long* count;
+  unsigned long long capacity;
+  // adoption rounds (fusion_score.rs:352-414)
+  unsigned long long* claim;  // per slot pixel: PS_SCORE_FREE, PS_SCORE_LOCKED or the smallest claiming priority
+  const unsigned* active;     // undecided candidates of this round (*ncur of them)
+  unsigned* next;             // undecided candidates after it (*nnext)
+  unsigned* ncur;
+  unsigned* nnext;
+  unsigned long long* adopted;
+};
+// candidates of view A.v (one thread per pixel)
+cudaError_t launch_score_candidates(const ScoreArgs& A, int w, int h, cudaStream_t st);
+// active = 0 .. n-1, *ncur = n
+cudaError_t launch_score_init(const ScoreArgs& A, unsigned n, cudaStream_t st);
+// one adoption round over *ncur active candidates (three launches; `blocks` CTAs of 256 threads each)
+cudaError_t launch_score_round(const ScoreArgs& A, int blocks, cudaStream_t st);
+
 // Free-space visibility filter of a fused cloud (filter_visibility, crates/dense/src/visibility.rs:106-151).
 #define PS_VIS_MAX_CHECK 64
 struct VisArgs {

@@ -105,6 +105,10 @@ struct FusedCloud {
   // visibility filter: per emitted point 1 = kept (NULL: no filter ran), and the removed points of each pass
   unsigned char* keep = nullptr;
   unsigned long long removed1 = 0, removed2 = 0;
+  // score fusion: candidates that lost to a higher-priority one (keep = 0), and each point's candidate number, whose
+  // order is the output order (NULL: key order per pass)
+  unsigned long long rejected = 0;
+  unsigned* gid = nullptr;
   int vis_stride = 0;
   float* pos = nullptr;
   float* nrm = nullptr;
@@ -117,6 +121,7 @@ struct FusedCloud {
   template <typename Free>
   void release(Free&& free) {
     free(keep);
+    free(gid);
     free(pos);
     free(nrm);
     free(col);
@@ -1938,6 +1943,29 @@ int ps_postprocess_resident(ps_session* s, uint32_t level, const uint32_t* views
   });
 }
 
+namespace {
+// Valid pixels (depth > 0) of the readout planes of `views` at level l.
+unsigned long long count_valid(ps_session* s, const uint32_t* views, size_t n, int l) {
+  Slot& sl = slot(s, l);
+  FusedCloud& fc = s->fused;
+  if (!fc.counter) fc.counter = dalloc<unsigned long long>(s, 1);
+  cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
+  for (auto [a, b] : batches(s, views, n, l)) {
+    ps_post::SpkArgs A;
+    memset(&A, 0, sizeof A);
+    A.plane = sl.aux;
+    A.valid = fc.counter;
+    const int tiles = spk_items(s, A, views, a, b, l, 0.0);
+    cuda_ok(ps_post::launch_count_valid(A, tiles, s->st), "count kernel");
+    s->launches++;
+  }
+  unsigned long long valid = 0;
+  cuda_ok(cudaMemcpyAsync(&valid, fc.counter, sizeof valid, cudaMemcpyDeviceToHost, s->st), "read count");
+  sync(s);
+  return valid;
+}
+}  // namespace
+
 int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
                      const ps_fusion_params* p, uint64_t* num_points, uint64_t* num_residual) {
   return guard(s, [&] {
@@ -1982,20 +2010,7 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     if (!fc.views) fc.views = dalloc<ps_post::FuseView>(s, std::max(s->nv, 1));
     cuda_ok(cudaMemcpyAsync(fc.views, fv.data(), fv.size() * sizeof(ps_post::FuseView), cudaMemcpyHostToDevice, s->st),
             "upload fusion views");
-    // capacity: valid pixels of the fused views
-    cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
-    for (auto [a, b] : batches(s, views, n, l)) {
-      ps_post::SpkArgs A;
-      memset(&A, 0, sizeof A);
-      A.plane = sl.aux;
-      A.valid = fc.counter;
-      const int tiles = spk_items(s, A, views, a, b, l, 0.0);
-      cuda_ok(ps_post::launch_count_valid(A, tiles, s->st), "count kernel");
-      s->launches++;
-    }
-    unsigned long long valid = 0;
-    cuda_ok(cudaMemcpyAsync(&valid, fc.counter, sizeof valid, cudaMemcpyDeviceToHost, s->st), "read count");
-    sync(s);
+    const unsigned long long valid = count_valid(s, views, n, l);  // capacity
     const int stride = (int)p->consistency_num_images + 1;
     if (valid > fc.cap || stride != fc.vis_stride) {
       fc.release([s](void* q) { dfree(s, q); });
@@ -2155,9 +2170,11 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
       if (ovf) fail(PS_ECUDA, "second pass: spatial hash table full");
     }
     fc.count = std::min(cnt, fc.cap);
-    fc.removed1 = fc.removed2 = 0;
+    fc.removed1 = fc.removed2 = fc.rejected = 0;
     if (fc.keep) dfree(s, fc.keep);
     fc.keep = nullptr;
+    if (fc.gid) dfree(s, fc.gid);
+    fc.gid = nullptr;
     const bool vis_on = p->visibility_check_views > 0 && p->visibility_tau > 0.0 && p->visibility_min_violations > 0;
     if (vis_on && fc.count > 0) {
       if (p->visibility_check_views > PS_VIS_MAX_CHECK) fail(PS_EINVAL, "visibility_check_views > 64");
@@ -2279,12 +2296,180 @@ int ps_fused_visibility_removed(ps_session* s, uint64_t* removed) {
   });
 }
 
+void ps_score_fusion_params_default(ps_score_fusion_params* o) {
+  if (!o) return;
+  memset(o, 0, sizeof *o);
+  o->sigma_e_px = 1.0;
+  o->sigma_theta_deg = 2.0;
+  o->lambda = 1.0;
+  o->tau = 2.0;
+  o->depth_error = 0.01;
+  o->normal_error_deg = 10.0;
+  o->num_neighbors = 12;
+  o->mark_used = 1;
+  o->inverse_variance = 1;
+  o->sigma_px0 = 0.25;
+  o->sigma_px_slope = 1.0;
+}
+
+// fuse_scored (crates/dense/src/fusion_score.rs:314-435): candidates per view (one launch per fused view, in index
+// order), then with mark_used the adoption rounds until no candidate is undecided (the host reads the undecided count
+// every few rounds; a round adopts at least the highest-priority undecided candidate, so rounds <= candidates).
+int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
+                            const ps_score_fusion_params* p, uint64_t* num_points) {
+  return guard(s, [&] {
+    if (!p || (n && !cams)) fail(PS_EINVAL, "params or cams is NULL");
+    check_views(s, views, n);
+    if (s->nv > 65535) fail(PS_EINVAL, "fusion supports at most 65535 views");
+    if (p->num_neighbors > PS_FUSE_MAX_OVERLAP) fail(PS_EINVAL, "num_neighbors > " + std::to_string(PS_FUSE_MAX_OVERLAP));
+    const int l = (int)level;
+    Slot& sl = slot(s, l);
+    if (sl.total >= 0xffffffffLL) fail(PS_EINVAL, "score fusion: more than 2^32 - 1 pixels in the level");
+    std::vector<char> used(s->nv, 0);
+    for (size_t i = 0; i < n; ++i) used[views[i]] = 1;
+    // camera table: overlap lists without the view itself and unused or out-of-range views, first num_neighbors
+    // (fusion_score.rs:324-330); candidate numbers in (view, pixel) order over the fused views
+    std::vector<ps_post::FuseView> fv(s->nv);
+    unsigned long long base = 0;
+    for (int v = 0; v < s->nv; ++v) {
+      ps_post::FuseView& f = fv[v];
+      memset(&f, 0, sizeof f);
+      f.off = sl.off[v];
+      f.w = s->W(v, l);
+      f.h = s->H(v, l);
+      const PsLevel& L = s->lvh[v * s->nl + l];
+      f.img = L.img;
+      f.pitch = L.pitch;
+      f.idbase = (unsigned)base;
+      if (!used[v]) continue;
+      base += (unsigned long long)f.w * f.h;
+      const ps_fusion_view& c = cams[v];
+      memcpy(f.k, c.k, sizeof f.k);
+      memcpy(f.r, c.r, sizeof f.r);
+      memcpy(f.t, c.t, sizeof f.t);
+      f.baseline = c.baseline;
+      f.image_id = c.image_id;
+      if (c.num_overlap && !c.overlap) fail(PS_EINVAL, "overlap is NULL");
+      for (uint32_t j = 0; j < c.num_overlap && f.nov < (int)p->num_neighbors; ++j) {
+        const uint32_t o = c.overlap[j];
+        if (o < (uint32_t)s->nv && (int)o != v && used[o]) f.ov[f.nov++] = (int)o;
+      }
+    }
+    if (base >= 0xfffffffeull) fail(PS_EINVAL, "score fusion: more than 2^32 - 2 pixels");
+    FusedCloud& fc = s->fused;
+    if (!fc.views) fc.views = dalloc<ps_post::FuseView>(s, std::max(s->nv, 1));
+    cuda_ok(cudaMemcpyAsync(fc.views, fv.data(), fv.size() * sizeof(ps_post::FuseView), cudaMemcpyHostToDevice, s->st),
+            "upload fusion views");
+    const unsigned long long valid = count_valid(s, views, n, l);  // capacity
+    const int stride = (int)p->num_neighbors + 1;
+    if (valid > fc.cap || stride != fc.vis_stride) {
+      fc.release([s](void* q) { dfree(s, q); });
+      const size_t c = std::max<unsigned long long>(valid, 1);
+      fc.pos = dalloc<float>(s, 3 * c);
+      fc.nrm = dalloc<float>(s, 3 * c);
+      fc.col = dalloc<unsigned char>(s, 3 * c);
+      fc.key = dalloc<unsigned long long>(s, c);
+      fc.nvis = dalloc<unsigned char>(s, c);
+      fc.vis = dalloc<unsigned short>(s, c * stride);
+      fc.cap = c;
+      fc.vis_stride = stride;
+    }
+    if (fc.keep) dfree(s, fc.keep);
+    if (fc.gid) dfree(s, fc.gid);
+    fc.keep = dalloc<unsigned char>(s, fc.cap);
+    fc.gid = dalloc<unsigned>(s, fc.cap);
+    fc.count = fc.count1 = fc.removed1 = fc.removed2 = fc.rejected = 0;
+    ps_post::ScoreArgs A;
+    memset(&A, 0, sizeof A);
+    A.views = fc.views;
+    A.plane = sl.aux;
+    A.cost = sl.cost;
+    A.inverse_variance = p->inverse_variance ? 1 : 0;
+    A.mark_used = p->mark_used ? 1 : 0;
+    A.sigma0 = p->sigma_px0;
+    A.slope = p->sigma_px_slope;
+    A.depth_tol = p->depth_error;
+    A.cos_n = std::cos(ps_to_radians_f64(p->normal_error_deg));
+    A.k_e = 1.0 / (2.0 * p->sigma_e_px * p->sigma_e_px);
+    const double st = ps_to_radians_f64(p->sigma_theta_deg);
+    A.k_t = 1.0 / (2.0 * st * st);
+    A.lambda = p->lambda;
+    A.tau = p->tau;
+    A.pos = fc.pos;
+    A.nrm = fc.nrm;
+    A.col = fc.col;
+    A.key = fc.key;
+    A.nvis = fc.nvis;
+    A.vis = fc.vis;
+    A.vis_stride = stride;
+    A.gid = fc.gid;
+    A.state = fc.keep;
+    A.count = fc.counter;
+    A.capacity = fc.cap;
+    A.prio = dalloc<unsigned long long>(s, fc.cap);
+    A.pix = dalloc<unsigned>(s, fc.cap * stride);
+    A.npix = dalloc<unsigned char>(s, fc.cap);
+    A.pix_stride = stride;
+    std::vector<uint32_t> order(views, views + n);
+    std::sort(order.begin(), order.end());
+    order.erase(std::unique(order.begin(), order.end()), order.end());
+    cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
+    for (uint32_t v : order) {
+      A.v = (int)v;
+      launched(s, ps_post::launch_score_candidates(A, s->W(v, l), s->H(v, l), s->st), "score fusion kernel");
+    }
+    unsigned long long cand = 0;
+    cuda_ok(cudaMemcpyAsync(&cand, fc.counter, sizeof cand, cudaMemcpyDeviceToHost, s->st), "read count");
+    sync(s);
+    cand = std::min(cand, fc.cap);
+    unsigned long long adopted = cand;
+    if (p->mark_used && cand > 0) {
+      A.claim = dalloc<unsigned long long>(s, sl.total);
+      unsigned* lists = dalloc<unsigned>(s, 2 * cand);
+      unsigned* counts = dalloc<unsigned>(s, 2);
+      A.adopted = dalloc<unsigned long long>(s, 1);
+      cuda_ok(cudaMemsetAsync(A.claim, 0xff, sl.total * sizeof(unsigned long long), s->st), "memset");
+      cuda_ok(cudaMemsetAsync(A.adopted, 0, sizeof(unsigned long long), s->st), "memset");
+      A.active = lists;
+      A.ncur = counts;
+      launched(s, ps_post::launch_score_init(A, (unsigned)cand, s->st), "score fusion kernel");
+      const int blocks = (int)std::min<unsigned long long>((cand + 255) / 256, 148ull * 16);
+      unsigned left = 1;
+      for (unsigned long long r = 0; left > 0; ++r) {
+        if (r > cand + 8) fail(PS_ECUDA, "score fusion: adoption rounds did not finish");
+        A.active = lists + (r & 1) * cand;
+        A.next = lists + ((r + 1) & 1) * cand;
+        A.ncur = counts + (r & 1);
+        A.nnext = counts + ((r + 1) & 1);
+        cuda_ok(ps_post::launch_score_round(A, blocks, s->st), "score fusion rounds");
+        s->launches += 3;
+        if (r % 4 == 3 || r < 4) {
+          cuda_ok(cudaMemcpyAsync(&left, A.nnext, sizeof left, cudaMemcpyDeviceToHost, s->st), "read count");
+          sync(s);
+        }
+      }
+      cuda_ok(cudaMemcpyAsync(&adopted, A.adopted, sizeof adopted, cudaMemcpyDeviceToHost, s->st), "read count");
+      sync(s);
+      dfree(s, A.claim);
+      dfree(s, lists);
+      dfree(s, counts);
+      dfree(s, A.adopted);
+    }
+    dfree(s, A.prio);
+    dfree(s, A.pix);
+    dfree(s, A.npix);
+    fc.count = fc.count1 = cand;
+    fc.rejected = cand - adopted;
+    if (num_points) *num_points = adopted;
+  });
+}
+
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride) {
   return guard(s, [&] {
     FusedCloud& fc = s->fused;
     const size_t n = fc.count;  // emitted points (before the visibility filter)
-    const size_t kept = n - fc.removed1 - fc.removed2;
+    const size_t kept = n - fc.removed1 - fc.removed2 - fc.rejected;
     if (capacity < kept)
       fail(PS_EINVAL, "capacity " + std::to_string(capacity) + " < " + std::to_string(kept) + " points");
     if (vis && (int)vis_stride < fc.vis_stride) fail(PS_EINVAL, "vis_stride too small");
@@ -2302,6 +2487,8 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
     }
     std::vector<unsigned char> keep(n, 1);
     if (n && fc.keep) cuda_ok(cudaMemcpyAsync(keep.data(), fc.keep, n, cudaMemcpyDeviceToHost, s->st), "download");
+    std::vector<unsigned> gid(fc.gid ? n : 0);
+    if (n && fc.gid) cuda_ok(cudaMemcpyAsync(gid.data(), fc.gid, 4 * n, cudaMemcpyDeviceToHost, s->st), "download");
     sync(s);
     // points in the reference's order: the first pass, then the second, each in ascending key (view, row, column),
     // without the points the visibility filter removed
@@ -2313,8 +2500,12 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
     const size_t k1 = idx.size();
     for (size_t i = n1; i < n; ++i)
       if (keep[i]) idx.push_back(i);
-    std::sort(idx.begin(), idx.begin() + k1, [&](size_t a, size_t b) { return k[a] < k[b]; });
-    std::sort(idx.begin() + k1, idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
+    if (fc.gid) {  // score fusion: (view, pixel) order
+      std::sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return gid[a] < gid[b]; });
+    } else {
+      std::sort(idx.begin(), idx.begin() + k1, [&](size_t a, size_t b) { return k[a] < k[b]; });
+      std::sort(idx.begin() + k1, idx.end(), [&](size_t a, size_t b) { return k[a] < k[b]; });
+    }
     for (size_t j = 0; j < idx.size(); ++j) {
       const size_t i = idx[j];
       if (positions) memcpy(positions + 3 * j, &p[3 * i], 12);

@@ -35,6 +35,19 @@ def default_fusion(min_consistent_views: Optional[int] = None) -> _lib.FusionPar
     return p
 
 
+def default_score_fusion(**overrides) -> _lib.ScoreFusionParams:
+    """ScoreFusionOptions::default() (crates/dense/src/fusion_score.rs:81-97); keyword arguments override fields
+    (`lambda_` for the penalty coefficient, the field `lambda`)."""
+    p = _lib.ScoreFusionParams()
+    _lib.engine().ps_score_fusion_params_default(C.byref(p))
+    for k, v in overrides.items():
+        k = "lambda" if k == "lambda_" else k
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p
+
+
 def median_interp(v: Sequence[float]) -> float:
     """median_in_place (crates/dense/src/math.rs:126-141): sorted, linear interpolation at 0.5·(n-1)."""
     if len(v) == 0:

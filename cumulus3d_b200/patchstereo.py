@@ -421,6 +421,19 @@ class PatchMatchSession:
         self.fused_visibility_removed = int(vr.value)
         return int(n.value)
 
+    def fuse_scored_resident(self, level: int, views: Sequence[int], cams, params=None) -> int:
+        """Score fusion (fuse_scored, crates/dense/src/fusion_score.rs:314-435) of the readout planes of `views`;
+        `cams` is a fusion.FusionCams of every view.  fused_points() then gives the points in (view, pixel) order."""
+        from .fusion import default_score_fusion
+        p = params if params is not None else default_score_fusion()
+        n = C.c_uint64()
+        self._check(self.lib.ps_fuse_scored_resident(self.h, level, _views(views), len(views), cams.table,
+                                                     C.byref(p), C.byref(n)))
+        self._fused = (int(n.value), int(p.num_neighbors) + 1)
+        self.fused_residual = 0
+        self.fused_visibility_removed = 0
+        return int(n.value)
+
     def fused_points(self):
         from .fusion import FusedCloud
         n, stride = getattr(self, "_fused", (0, 1))

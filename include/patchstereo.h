@@ -482,6 +482,34 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
                      const ps_fusion_params* p, uint64_t* num_points, uint64_t* num_residual);
 /* Points the visibility filter removed from the last fused cloud (FusionOutput::visibility_removed). */
 int ps_fused_visibility_removed(ps_session* s, uint64_t* removed);
+
+/* ScoreFusionOptions (crates/dense/src/fusion_score.rs:56-103).  Score fusion (fuse_scored, fusion_score.rs:314-435):
+ * every valid reference pixel is lifted to a point and checked against up to num_neighbors overlap views; a view that
+ * agrees in depth and normal contributes c_j·exp(-e²/(2σ_e²))·(1 - exp(-θ²/(2σ_θ²))) (c_j = clamp(1 - cost, 0, 1),
+ * e the round-trip reprojection error, θ the angle of the two viewing rays), a view whose surface lies behind the
+ * point by more than depth_error costs λ·c_j, and the reference contributes its own c; points scoring at least tau
+ * are candidates (weighted means of position, normal, colour).  With mark_used, candidates whose pixels overlap keep
+ * only the higher priority (score descending, then view and pixel ascending).  The exponentials and the arc cosine
+ * are fixed binary64 sequences shared with the CPU restatement. */
+typedef struct ps_score_fusion_params {
+  double sigma_e_px;        /* 1.0 */
+  double sigma_theta_deg;   /* 2.0 */
+  double lambda;            /* 1.0 */
+  double tau;               /* 2.0 */
+  double depth_error;       /* 0.01 */
+  double normal_error_deg;  /* 10 */
+  uint32_t num_neighbors;   /* 12 (at most 32) */
+  uint32_t mark_used;       /* true */
+  uint32_t inverse_variance; /* true */
+  uint32_t reserved;
+  double sigma_px0;         /* 0.25 */
+  double sigma_px_slope;    /* 1.0 */
+} ps_score_fusion_params;
+void ps_score_fusion_params_default(ps_score_fusion_params* out);
+/* Score fusion of the readout planes and final costs of `views` at `level` (cams as for ps_fuse_resident); the
+ * cloud replaces the session's fused cloud (ps_fused_points reads it; its order is the reference's: ascending key). */
+int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
+                            const ps_score_fusion_params* p, uint64_t* num_points);
 /* The fused points in the reference's order: the first pass in ascending point key (image_id << 32) | (row << 16) |
  * col, then the second-pass points in ascending key: positions and normals 3 floats, colours 3 bytes, keys, the
  * number of contributing views and their indices (ascending, vis_stride >= consistency_num_images + 1 entries per

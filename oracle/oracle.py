@@ -78,7 +78,13 @@ def lib() -> C.CDLL:
             "oracle_pyramid_step": (None, [C.c_void_p, C.c_size_t, C.c_size_t, C.POINTER(C.c_double), C.c_void_p,
                                            C.POINTER(C.c_double)]),
             "oracle_expf": (C.c_float, [C.c_float]),
+            "oracle_fuse_scored": (C.c_int, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
+                                             C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.POINTER(_lib.ScoreFusionParams), C.c_int, C.c_uint64,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_uint32, C.POINTER(C.c_uint64)]),
             "oracle_exp64": (C.c_double, [C.c_double]),
+            "oracle_acos64": (C.c_double, [C.c_double]),
             "oracle_sincosf": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
         }
         for n, (r, a) in sig.items():
@@ -262,6 +268,34 @@ def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[
     out.residual = int(r.value)  # points of the second pass (the last ones)
     out.visibility_removed = int(vr.value)
     return out
+
+
+def fuse_scored(cams, depths, normals, costs, images, views, params, threads: Optional[int] = None):
+    """Score fusion restated (fuse_scored, crates/dense/src/fusion_score.rs:314-435); inputs as for fuse.  Returns a
+    fusion.FusedCloud in the reference's point order: (view, pixel) ascending."""
+    from cumulus3d_b200.fusion import FusedCloud
+    nv = len(depths)
+    ws = (C.c_uint32 * nv)(*[d.shape[1] for d in depths])
+    hs = (C.c_uint32 * nv)(*[d.shape[0] for d in depths])
+    keep = [np.ascontiguousarray(a, np.float32) for a in list(depths) + list(normals) + list(costs) + list(images)]
+    ptr = lambda arrs: (C.c_void_p * nv)(*[a.ctypes.data for a in arrs])
+    dp, np_, cp, ip = (ptr(keep[i * nv:(i + 1) * nv]) for i in range(4))
+    used = np.zeros(nv, np.uint8)
+    used[list(views)] = 1
+    cap = int(sum(int((d > 0).sum()) for d in depths)) + 1
+    stride = int(params.num_neighbors) + 1
+    pos = np.empty((cap, 3), np.float32)
+    nrm = np.empty((cap, 3), np.float32)
+    col = np.empty((cap, 3), np.uint8)
+    key = np.empty(cap, np.uint64)
+    vc = np.empty(cap, np.uint8)
+    vis = np.empty((cap, stride), np.uint16)
+    n = C.c_uint64()
+    _chk(lib().oracle_fuse_scored(nv, cams.table, ws, hs, dp, np_, cp, ip, used.ctypes.data, C.byref(params),
+                                  _threads(threads), cap, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data,
+                                  key.ctypes.data, vc.ctypes.data, vis.ctypes.data, stride, C.byref(n)), "fuse_scored")
+    k = int(n.value)
+    return FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
 
 
 def select_neighbors(model, params, pair_stats: bool = False):

@@ -1210,6 +1210,7 @@ void oracle_pyramid_step(const uint8_t* src, size_t w, size_t h, const double* k
 }
 float oracle_expf(float x) { return ps_expf(x); }
 double oracle_exp64(double x) { return ps_exp64(x); }
+double oracle_acos64(double x) { return ps_acos64(x); }
 void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
 
 
@@ -1968,6 +1969,187 @@ int oracle_select_neighbors(const ps_sparse_view* views, uint32_t nv, const doub
     depth_range[2 * v + 1] = 1.25 * hi;
   }
   return PS_OK;
+}
+
+// ---- score fusion (crates/dense/src/fusion_score.rs:196-435) -------------------------------------------------
+// Candidates per reference pixel (view_candidates, fusion_score.rs:196-303) in (view, pixel) order; with mark_used the
+// greedy choice in priority order (score descending, then view and pixel ascending): a candidate is adopted when none
+// of its pixels (its own and its agreeing pixels) was taken by an adopted candidate before it, which is the result the
+// reference's claim rounds reach (fusion_score.rs:352-414).  The exponentials and the arc cosine are ps_exp64 /
+// ps_acos64, as in the engine.
+int oracle_fuse_scored(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* widths, const uint32_t* heights,
+                       const float* const* depth, const float* const* normal, const float* const* cost,
+                       const float* const* img, const uint8_t* used, const ps_score_fusion_params* p, int threads,
+                       uint64_t capacity, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
+                       uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count) {
+  if (!cams || !widths || !heights || !depth || !normal || !cost || !img || !used || !p || !count) return PS_EINVAL;
+  set_threads(threads);
+  std::vector<FCam> fc(nviews);
+  std::vector<std::array<double, 3>> ctr(nviews);
+  for (uint32_t v = 0; v < nviews; ++v) {
+    memcpy(fc[v].k, cams[v].k, sizeof fc[v].k);
+    memcpy(fc[v].r, cams[v].r, sizeof fc[v].r);
+    memcpy(fc[v].t, cams[v].t, sizeof fc[v].t);
+    fc[v].baseline = cams[v].baseline;
+    fc[v].w = (int)widths[v];
+    fc[v].h = (int)heights[v];
+    for (int j = 0; j < 3; ++j)
+      ctr[v][j] = -(fc[v].r[0 * 3 + j] * fc[v].t[0] + fc[v].r[1 * 3 + j] * fc[v].t[1] + fc[v].r[2 * 3 + j] * fc[v].t[2]);
+  }
+  std::vector<std::vector<int>> ovs(nviews);
+  for (uint32_t v = 0; v < nviews; ++v) {
+    if (!used[v]) continue;
+    for (uint32_t j = 0; j < cams[v].num_overlap && ovs[v].size() < p->num_neighbors; ++j) {
+      const uint32_t o = cams[v].overlap[j];
+      if (o != v && o < nviews && used[o]) ovs[v].push_back((int)o);
+    }
+  }
+  const double cos_n = std::cos(ps_to_radians_f64(p->normal_error_deg));
+  const double k_e = 1.0 / (2.0 * p->sigma_e_px * p->sigma_e_px);
+  const double st = ps_to_radians_f64(p->sigma_theta_deg);
+  const double k_t = 1.0 / (2.0 * st * st);
+  auto conf = [&](int v, size_t pix) { return std::min(std::max(1.0 - (double)cost[v][pix], 0.0), 1.0); };
+  auto ivar = [&](int v, size_t pix, double d) {
+    if (!p->inverse_variance || !(fc[v].baseline > 0.0)) return 1.0;
+    const double spx = p->sigma_px0 + p->sigma_px_slope * (double)std::min(std::max(cost[v][pix], 0.0f), 2.0f);
+    const double sd = d * d * spx / (fc[v].k[0] * fc[v].baseline);
+    return 1.0 / std::max(sd * sd, 1e-300);
+  };
+  struct SCand {
+    uint32_t v, pix;
+    float score;
+    FPoint pt;
+    std::vector<std::pair<int, int>> hits;
+  };
+  std::vector<SCand> cands;
+  for (uint32_t v = 0; v < nviews; ++v) {
+    if (!used[v]) continue;
+    const FCam& cv = fc[v];
+    std::vector<std::vector<SCand>> rows(cv.h);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int row = 0; row < cv.h; ++row) {
+      for (int col = 0; col < cv.w; ++col) {
+        const size_t pix = (size_t)row * cv.w + col;
+        const double d = (double)depth[v][pix];
+        if (!(d > 0.0)) continue;  // NaN depths are invalid too (the reference's casts of NaN are undefined)
+        double x[3], nw[3];
+        f_backproject(cv, (double)col, (double)row, d, x);
+        f_normal(cv, normal[v] + 3 * pix, nw);
+        const double rr[3] = {x[0] - ctr[v][0], x[1] - ctr[v][1], x[2] - ctr[v][2]};
+        const double l_ref = std::sqrt(rr[0] * rr[0] + rr[1] * rr[1] + rr[2] * rr[2]);
+        const double s_ref = conf((int)v, pix);
+        const double w0 = s_ref * ivar((int)v, pix, d);
+        double sum_s = s_ref, sum_p = 0.0, sw = w0;
+        double sx[3] = {x[0] * w0, x[1] * w0, x[2] * w0};
+        double sn[3] = {nw[0] * w0, nw[1] * w0, nw[2] * w0};
+        const double c0 = f_gray(img[v], cv, col, row);
+        double sc[3] = {c0 * w0, c0 * w0, c0 * w0};
+        std::vector<std::pair<int, int>> hits;
+        for (int j : ovs[v]) {
+          const FCam& oc = fc[j];
+          double u, vv, z;
+          if (!f_project(oc, x, &u, &vv, &z)) continue;
+          const double cu = std::floor(u + 0.5), rv = std::floor(vv + 0.5);
+          if (cu < 0.0 || rv < 0.0 || cu >= (double)oc.w || rv >= (double)oc.h) continue;
+          const size_t opix = (size_t)rv * oc.w + (size_t)cu;
+          const double od = (double)depth[j][opix];
+          if (od <= 0.0) continue;
+          const double cj = conf(j, opix);
+          if (std::fabs(z - od) / od > p->depth_error) {
+            if (z < od * (1.0 - p->depth_error)) sum_p += cj;
+            continue;
+          }
+          double no[3];
+          f_normal(oc, normal[j] + 3 * opix, no);
+          if (no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < cos_n) continue;
+          double xo[3];
+          f_backproject(oc, cu, rv, od, xo);
+          double bu, bv, bz;
+          if (!f_project(cv, xo, &bu, &bv, &bz)) continue;
+          const double eu = bu - (double)col, ev = bv - (double)row;
+          const double e2 = eu * eu + ev * ev;
+          const double rj[3] = {x[0] - ctr[j][0], x[1] - ctr[j][1], x[2] - ctr[j][2]};
+          double cos_t = (rr[0] * rj[0] + rr[1] * rj[1] + rr[2] * rj[2]) /
+                         (l_ref * std::sqrt(rj[0] * rj[0] + rj[1] * rj[1] + rj[2] * rj[2]));
+          cos_t = std::min(std::max(cos_t, -1.0), 1.0);
+          const double th = ps_acos64(cos_t);
+          const double sj = cj * ps_exp64(-e2 * k_e) * (1.0 - ps_exp64(-th * th * k_t));
+          sum_s += sj;
+          if (sj <= 0.0) continue;
+          const double wo = sj * ivar(j, opix, od);
+          const double co = f_gray(img[j], oc, (int)cu, (int)rv);
+          sw += wo;
+          for (int k = 0; k < 3; ++k) {
+            sx[k] += wo * xo[k];
+            sn[k] += wo * no[k];
+            sc[k] += wo * co;
+          }
+          hits.push_back({j, (int)opix});
+        }
+        const double score = sum_s - p->lambda * sum_p;
+        if (score < p->tau || sw <= 0.0 || !std::isfinite(sw)) continue;
+        const double l = std::sqrt(sn[0] * sn[0] + sn[1] * sn[1] + sn[2] * sn[2]);
+        if (l < 1.1920928955078125e-07) continue;
+        SCand c;
+        c.v = v;
+        c.pix = (uint32_t)pix;
+        c.score = (float)score;
+        for (int k = 0; k < 3; ++k) {
+          c.pt.pos[k] = (float)(sx[k] / sw);
+          c.pt.nrm[k] = (float)(sn[k] / l);
+          c.pt.col[k] = (uint8_t)std::min(std::max(std::round(sc[k] / sw), 0.0), 255.0);
+        }
+        c.pt.key = ((uint64_t)cams[v].image_id << 32) | ((uint64_t)(row & 0xffff) << 16) | (uint64_t)(col & 0xffff);
+        c.pt.vis.assign(1, (uint16_t)v);
+        for (auto& hq : hits) c.pt.vis.push_back((uint16_t)hq.first);
+        std::sort(c.pt.vis.begin(), c.pt.vis.end());
+        c.pt.vis.erase(std::unique(c.pt.vis.begin(), c.pt.vis.end()), c.pt.vis.end());
+        c.hits = std::move(hits);
+        rows[row].push_back(std::move(c));
+      }
+    }
+    for (auto& r : rows)
+      for (auto& c : r) cands.push_back(std::move(c));
+  }
+  std::vector<char> accepted(cands.size(), p->mark_used ? 0 : 1);
+  if (p->mark_used && !cands.empty()) {
+    std::vector<size_t> order(cands.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = i;  // (view, pixel) order already
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+      const uint32_t ka = ps_f2u(cands[a].score), kb = ps_f2u(cands[b].score);
+      const uint32_t oa = (ka & 0x80000000u) ? ~ka : (ka | 0x80000000u), ob = (kb & 0x80000000u) ? ~kb : (kb | 0x80000000u);
+      return oa > ob;  // score descending in total order; ties keep (view, pixel) order
+    });
+    std::vector<std::vector<char>> taken(nviews);
+    for (uint32_t v = 0; v < nviews; ++v)
+      if (used[v]) taken[v].assign((size_t)fc[v].w * fc[v].h, 0);
+    for (size_t g : order) {
+      const SCand& c = cands[g];
+      bool free = !taken[c.v][c.pix];
+      for (auto& hq : c.hits) free = free && !taken[hq.first][hq.second];
+      if (!free) continue;
+      accepted[g] = 1;
+      taken[c.v][c.pix] = 1;
+      for (auto& hq : c.hits) taken[hq.first][hq.second] = 1;
+    }
+  }
+  uint64_t n_out = 0;
+  for (size_t g = 0; g < cands.size(); ++g) {
+    if (!accepted[g]) continue;
+    const FPoint& pt = cands[g].pt;
+    if (n_out < capacity) {
+      if (positions) memcpy(positions + 3 * n_out, pt.pos, 12);
+      if (normals) memcpy(normals + 3 * n_out, pt.nrm, 12);
+      if (colors) memcpy(colors + 3 * n_out, pt.col, 3);
+      if (keys) keys[n_out] = pt.key;
+      if (vis_counts) vis_counts[n_out] = (uint8_t)pt.vis.size();
+      if (vis)
+        for (uint32_t t = 0; t < vis_stride; ++t) vis[n_out * vis_stride + t] = t < pt.vis.size() ? pt.vis[t] : 0;
+    }
+    n_out++;
+  }
+  *count = n_out;
+  return n_out <= capacity ? PS_OK : PS_EINVAL;
 }
 
 }  // extern "C"

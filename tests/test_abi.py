@@ -44,7 +44,7 @@ STRUCTS = {
     "ps_depth_snapshot": _lib.DepthSnapshot, "ps_schedule": _lib.Schedule,
     "ps_multiscale_schedule": _lib.MultiscaleSchedule, "ps_post_params": _lib.PostParams,
     "ps_fusion_params": _lib.FusionParams, "ps_fusion_view": _lib.FusionView, "ps_sparse_view": _lib.SparseView,
-    "ps_neighbor_params": _lib.NeighborParams,
+    "ps_neighbor_params": _lib.NeighborParams, "ps_score_fusion_params": _lib.ScoreFusionParams,
 }
 
 
@@ -143,6 +143,11 @@ def test_post_fusion_and_neighbour_defaults_match_reference():
     nb = _lib.NeighborParams()
     lib.ps_neighbor_params_default(C.byref(nb))
     assert (nb.num_views, nb.direction_bins, nb.min_triangulation_angle_deg, nb.diversity_decay) == (10, 8, 1.0, 1.0)
+    sf = _lib.ScoreFusionParams()
+    lib.ps_score_fusion_params_default(C.byref(sf))  # ScoreFusionOptions (crates/dense/src/fusion_score.rs:81-97)
+    assert (sf.sigma_e_px, sf.sigma_theta_deg, getattr(sf, "lambda"), sf.tau, sf.depth_error, sf.normal_error_deg,
+            sf.num_neighbors, sf.mark_used, sf.inverse_variance, sf.sigma_px0, sf.sigma_px_slope) == \
+        (1.0, 2.0, 1.0, 2.0, 0.01, 10.0, 12, 1, 1, 0.25, 1.0)
 
 
 def test_reciprocal_check_validates_its_range_without_device():

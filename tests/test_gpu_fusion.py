@@ -116,6 +116,35 @@ def test_second_pass_fusion_bitwise_vs_oracle(pipeline):
     assert n_rel == n_none and s.fused_residual == 0
 
 
+@pytest.mark.parametrize("opts", [{}, {"mark_used": 0}, {"tau": 0.5, "num_neighbors": 3},
+                                  {"tau": 1.5, "lambda_": 0.0, "inverse_variance": 0}])
+def test_score_fusion_bitwise_vs_oracle(pipeline, opts):
+    """fuse_scored (crates/dense/src/fusion_score.rs:314-435) on the device against the restatement: candidates,
+    adoption under mark_used and the (view, pixel) output order (image ids descend with the view index here, so key
+    order would differ)."""
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src, image_ids=[1000 - v for v in range(len(wl.cams))])
+    imgs = [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views]
+    args = ([st.depth for st in states], [st.normal for st in states], [st.cost for st in states], imgs)
+    prm = fusion.default_score_fusion(**opts)
+    for vs in (views, views[1:]):
+        n = s.fuse_scored_resident(0, vs, fc, prm)
+        got = s.fused_points()
+        want = oracle.fuse_scored(fc, *args, vs, prm)
+        assert n == len(want) > 0
+        np.testing.assert_array_equal(got.keys, want.keys)
+        np.testing.assert_array_equal(got.positions, want.positions)
+        np.testing.assert_array_equal(got.normals, want.normals)
+        np.testing.assert_array_equal(got.colors, want.colors)
+        np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
+        for i in range(len(want)):
+            assert got.visibility(i) == want.visibility(i)
+
+
 @pytest.mark.parametrize("residual", [0, 2])
 def test_visibility_filter_bitwise_vs_oracle(pipeline, residual):
     """filter_visibility (crates/dense/src/visibility.rs:106-151) on the device cloud against the restatement: the

@@ -252,6 +252,7 @@ def bench_ours(args, rank, world, local):
     res["hbm_high_water_gb"] = round(max(hbm) / 1e9, 2)
     if not shard_job:
         res["fusion_all_options"] = fusion_options_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
+        res["score_fusion"] = score_fusion_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
     sess.close()
     # ---- e2e through the host-buffer C ABI (session begin uploads the images) ----
     if not args.no_e2e:
@@ -388,6 +389,43 @@ def fusion_options_stage(wl, sess, mine, check=True, check_views=6):
                 else kv.levels[0].pixels for kv in wl.input.views]
         t1 = time.perf_counter()
         ref = oracle.fuse(fc, [x.depth for x in st], [x.normal for x in st], [x.cost for x in st], imgs, sub, prm)
+        out["check"] = {"views": len(sub), "points": n_sub, "oracle_points": len(ref),
+                        "oracle_s": round(time.perf_counter() - t1, 2),
+                        "equal": bool(len(ref) == n_sub and np.array_equal(ref.keys, got.keys)
+                                      and np.array_equal(ref.positions, got.positions)
+                                      and np.array_equal(ref.normals, got.normals))}
+    return out
+
+
+def score_fusion_stage(wl, sess, mine, check=True, check_views=6):
+    """Score fusion (fuse_scored, ScoreFusionOptions defaults: tau 2, λ 1, mark_used) of the final maps through the C
+    ABI over all views, after one untimed run; with `check`, the device fuses the first `check_views` views again and
+    the CPU oracle must give the same cloud bit for bit."""
+    from cumulus3d_b200 import fusion
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    prm = fusion.default_score_fusion()
+    sess.readout_resident(mine, download=False)
+    sess.postprocess_resident(0, mine)
+    sess.fuse_scored_resident(0, mine, fc, prm)  # warm-up, untimed
+    sess.synchronize()
+    t0 = time.perf_counter()
+    n = sess.fuse_scored_resident(0, mine, fc, prm)
+    dt = time.perf_counter() - t0
+    out = {"points": n, "ms": round(dt * 1e3, 2),
+           "what": "candidates, claim rounds (mark_used) and the count, on the speckle-filtered final maps"}
+    if check:
+        from oracle import oracle
+        from cumulus3d_b200 import scenes
+        sub = list(mine[:check_views])
+        n_sub = sess.fuse_scored_resident(0, sub, fc, prm)
+        got = sess.fused_points()
+        st = sess.readout_download(0, mine)
+        imgs = [scenes.unit_plane(kv.levels[0].pixels) if kv.levels[0].pixels.dtype == np.uint8
+                else kv.levels[0].pixels for kv in wl.input.views]
+        t1 = time.perf_counter()
+        ref = oracle.fuse_scored(fc, [x.depth for x in st], [x.normal for x in st], [x.cost for x in st], imgs, sub,
+                                 prm)
         out["check"] = {"views": len(sub), "points": n_sub, "oracle_points": len(ref),
                         "oracle_s": round(time.perf_counter() - t1, 2),
                         "equal": bool(len(ref) == n_sub and np.array_equal(ref.keys, got.keys)

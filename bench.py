@@ -252,7 +252,7 @@ def bench_ours(args, rank, world, local):
     res["hbm_high_water_gb"] = round(max(hbm) / 1e9, 2)
     if not shard_job:
         res["fusion_all_options"] = fusion_options_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
-        try:  # a later addition: its failure must not cost the line
+        try:  # an error in this leg is reported in the line instead of ending the run
             res["score_fusion"] = score_fusion_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
         except Exception as e:  # noqa: BLE001
             res["score_fusion"] = {"error": f"{type(e).__name__}: {e}"}

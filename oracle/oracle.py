@@ -83,6 +83,12 @@ def lib() -> C.CDLL:
                                              C.c_void_p, C.POINTER(_lib.ScoreFusionParams), C.c_int, C.c_uint64,
                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                              C.c_uint32, C.POINTER(C.c_uint64)]),
+            "oracle_smooth": (C.c_double, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_uint32, C.c_double,
+                                           C.c_double, C.c_double, C.c_int]),
+            "oracle_filter_visibility": (C.c_int64, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
+                                                     C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
+                                                     C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_uint32,
+                                                     C.c_uint32, C.c_double, C.c_void_p]),
             "oracle_exp64": (C.c_double, [C.c_double]),
             "oracle_acos64": (C.c_double, [C.c_double]),
             "oracle_sincosf": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
@@ -268,6 +274,45 @@ def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[
     out.residual = int(r.value)  # points of the second pass (the last ones)
     out.visibility_removed = int(vr.value)
     return out
+
+
+def filter_visibility(cams, depths, views, positions, visibility, check_views: int, min_violations: int,
+                      tau: float):
+    """filter_visibility (crates/dense/src/visibility.rs:106-151) on a bare cloud: cams a fusion.FusionCams (its
+    overlap lists are the candidate order), depths one map per view (only `views` count), visibility one list of view
+    indices per point.  Returns the keep mask (bool per point)."""
+    nv = len(depths)
+    ws = (C.c_uint32 * nv)(*[d.shape[1] for d in depths])
+    hs = (C.c_uint32 * nv)(*[d.shape[0] for d in depths])
+    keepalive = [np.ascontiguousarray(d, np.float32) for d in depths]
+    dp = (C.c_void_p * nv)(*[a.ctypes.data for a in keepalive])
+    used = np.zeros(nv, np.uint8)
+    used[list(views)] = 1
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+    n = pos.shape[0]
+    stride = max([len(v) for v in visibility] + [1])
+    vc = np.array([len(v) for v in visibility], np.uint8)
+    vis = np.zeros((n, stride), np.uint16)
+    for i, v in enumerate(visibility):
+        vis[i, :len(v)] = v
+    keep = np.empty(n, np.uint8)
+    r = lib().oracle_filter_visibility(nv, cams.table, ws, hs, dp, used.ctypes.data, pos.ctypes.data, vc.ctypes.data,
+                                       vis.ctypes.data, stride, n, check_views, min_violations, tau, keep.ctypes.data)
+    if r < 0:
+        raise RuntimeError("oracle_filter_visibility: invalid arguments")
+    return keep.astype(bool)
+
+
+def smooth(positions, normals, gsd: float, iterations: int, radius_gsd: float, sigma_range_gsd: float,
+           normal_deg: float, threads: Optional[int] = None):
+    """smooth_along_normals (crates/dense/src/smooth.rs:143-220) on a bare cloud: returns (new positions, the median
+    absolute displacement of the last pass)."""
+    pos = np.ascontiguousarray(positions, np.float32).copy()
+    nrm = np.ascontiguousarray(normals, np.float32)
+    assert pos.shape == nrm.shape and pos.ndim == 2 and pos.shape[1] == 3
+    d = lib().oracle_smooth(pos.ctypes.data, nrm.ctypes.data, pos.shape[0], gsd, iterations, radius_gsd,
+                            sigma_range_gsd, normal_deg, _threads(threads))
+    return pos, float(d)
 
 
 def fuse_scored(cams, depths, normals, costs, images, views, params, threads: Optional[int] = None):

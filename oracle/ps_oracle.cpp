@@ -1399,6 +1399,121 @@ struct FPoint {
   uint64_t key;
   std::vector<uint16_t> vis;
 };
+// filter_visibility's test of one point (crates/dense/src/visibility.rs:117-138): candidate views are the overlap
+// lists of its views in order, de-duplicated, cut at check_views; a view whose depth lies behind the point by more
+// than tau is a violation, one within tau a support.
+bool visibility_violated(const float* pos, const uint16_t* vis, size_t nvis, uint32_t nviews,
+                         const ps_fusion_view* cams, const std::vector<FCam>& fc, const float* const* depth,
+                         const uint8_t* used, uint32_t check_views, uint32_t min_violations, double tau) {
+  const double x[3] = {(double)pos[0], (double)pos[1], (double)pos[2]};
+  std::vector<int> cand;
+  bool full = false;
+  for (size_t t = 0; t < nvis; ++t) {
+    const uint16_t v = vis[t];
+    if (full) break;
+    if (v >= nviews) continue;
+    for (uint32_t j = 0; j < cams[v].num_overlap; ++j) {
+      if (cand.size() >= check_views) {
+        full = true;
+        break;
+      }
+      const int o = (int)cams[v].overlap[j];
+      if (std::find(cand.begin(), cand.end(), o) == cand.end()) cand.push_back(o);
+    }
+  }
+  int viol = 0, sup = 0;
+  for (int v : cand) {
+    if (v < 0 || v >= (int)nviews || !used[v]) continue;
+    const FCam& c = fc[v];
+    const double cx = c.r[0] * x[0] + c.r[1] * x[1] + c.r[2] * x[2] + c.t[0];
+    const double cy = c.r[3] * x[0] + c.r[4] * x[1] + c.r[5] * x[2] + c.t[1];
+    const double cz = c.r[6] * x[0] + c.r[7] * x[1] + c.r[8] * x[2] + c.t[2];
+    if (cz <= 0.0) continue;
+    const double col = std::round(c.k[0] * cx / cz + c.k[2]), row = std::round(c.k[1] * cy / cz + c.k[3]);
+    if (col < 0.0 || row < 0.0 || col >= (double)c.w || row >= (double)c.h) continue;
+    const double dv = (double)depth[v][(size_t)row * c.w + (size_t)col];
+    if (dv <= 0.0) continue;
+    if (cz < dv * (1.0 - tau))
+      viol++;
+    else if (std::fabs(cz - dv) <= tau * dv)
+      sup++;
+  }
+  return viol >= (int)min_violations && viol > sup;
+}
+
+// smooth_along_normals (crates/dense/src/smooth.rs:143-220) over points in cloud order: Jacobi passes; each point
+// sums its neighbours within the radius in the order of the 27 cells around it ((z, y, x) offsets), each cell's points
+// in cloud order.  Returns the median absolute displacement of the last pass (0 when nothing ran).
+double smooth_points(std::vector<float*>& pos, const std::vector<const float*>& nrm3, double gsd, uint32_t iterations,
+                     double radius_gsd, double sigma_range_gsd, double normal_deg) {
+  const size_t n = pos.size();
+  if (!(iterations > 0 && radius_gsd > 0.0 && sigma_range_gsd > 0.0) || gsd <= 0.0 || n == 0) return 0.0;
+  const double r = radius_gsd * gsd;
+  const double r2 = r * r;
+  const double inv_2ss = 1.0 / (2.0 * ((0.5 * r) * (0.5 * r)));
+  const double sr = sigma_range_gsd * gsd;
+  const double inv_2sr = 1.0 / (2.0 * (sr * sr));
+  const double cos_n = std::cos(ps_to_radians_f64(normal_deg));
+  std::vector<std::array<double, 3>> nrm(n);
+  for (size_t i = 0; i < n; ++i) {
+    const double m[3] = {(double)nrm3[i][0], (double)nrm3[i][1], (double)nrm3[i][2]};
+    const double l = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    nrm[i] = l > 1e-12 ? std::array<double, 3>{m[0] / l, m[1] / l, m[2] / l} : std::array<double, 3>{0.0, 0.0, 0.0};
+  }
+  double last = 0.0;
+  for (uint32_t it = 0; it < iterations; ++it) {
+    // cell -> points in cloud order (cells packed 21 bits per axis around 2^20; the device requires that range)
+    auto pack = [](long long x, long long y, long long z) {
+      return ((uint64_t)(x + (1ll << 20)) << 42) | ((uint64_t)(y + (1ll << 20)) << 21) | (uint64_t)(z + (1ll << 20));
+    };
+    std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
+    grid.reserve(n);
+    std::vector<std::array<long long, 3>> cell(n);
+    for (size_t i = 0; i < n; ++i) {
+      for (int a = 0; a < 3; ++a) cell[i][a] = (long long)std::floor((double)pos[i][a] / r);
+      grid[pack(cell[i][0], cell[i][1], cell[i][2])].push_back((uint32_t)i);
+    }
+    std::vector<std::array<float, 3>> next(n);
+    std::vector<double> disp(n);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long long ii = 0; ii < (long long)n; ++ii) {
+      const size_t i = (size_t)ii;
+      const double pi[3] = {(double)pos[i][0], (double)pos[i][1], (double)pos[i][2]};
+      const auto& ni = nrm[i];
+      double t = 0.0;
+      if (!(ni[0] == 0.0 && ni[1] == 0.0 && ni[2] == 0.0)) {
+        double sw = 1.0, swd = 0.0;
+        for (long long dz = -1; dz <= 1; ++dz)
+          for (long long dy = -1; dy <= 1; ++dy)
+            for (long long dx = -1; dx <= 1; ++dx) {
+              auto g = grid.find(pack(cell[i][0] + dx, cell[i][1] + dy, cell[i][2] + dz));
+              if (g == grid.end()) continue;
+              for (uint32_t j : g->second) {
+                const double dv[3] = {(double)pos[j][0] - pi[0], (double)pos[j][1] - pi[1], (double)pos[j][2] - pi[2]};
+                const double d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
+                if (d2 > r2 || j == i) continue;
+                const auto& nj = nrm[j];
+                if (ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2] < cos_n) continue;
+                const double dn = ni[0] * dv[0] + ni[1] * dv[1] + ni[2] * dv[2];
+                const double w = ps_exp64(-d2 * inv_2ss - dn * dn * inv_2sr);
+                sw += w;
+                swd += w * dn;
+              }
+            }
+        t = swd / sw;
+      }
+      for (int a = 0; a < 3; ++a) next[i][a] = (float)(pi[a] + t * ni[a]);
+      disp[i] = std::fabs(t);
+    }
+    for (size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) pos[i][a] = next[i][a];
+    std::sort(disp.begin(), disp.end());  // median_in_place (crates/dense/src/math.rs:126-141)
+    const double q = 0.5 * (double)(n - 1);
+    const size_t lo = (size_t)std::floor(q), hi = std::min(lo + 1, n - 1);
+    last = disp[lo] + (disp[hi] - disp[lo]) * (q - (double)lo);
+  }
+  return last;
+}
 }  // namespace
 
 int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* widths, const uint32_t* heights,
@@ -1650,37 +1765,8 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
     for (std::vector<FPoint>* part : {&out1, &out2}) {
       std::vector<FPoint> kept;
       for (auto& pt : *part) {
-        const double x[3] = {(double)pt.pos[0], (double)pt.pos[1], (double)pt.pos[2]};
-        std::vector<int> cand;
-        bool full = false;
-        for (uint16_t v : pt.vis) {
-          if (full) break;
-          if (v >= nviews) continue;
-          for (uint32_t j = 0; j < cams[v].num_overlap; ++j) {
-            if (cand.size() >= p->visibility_check_views) {
-              full = true;
-              break;
-            }
-            const int o = (int)cams[v].overlap[j];
-            if (std::find(cand.begin(), cand.end(), o) == cand.end()) cand.push_back(o);
-          }
-        }
-        int viol = 0, sup = 0;
-        for (int v : cand) {
-          if (v < 0 || v >= (int)nviews || !used[v]) continue;
-          const FCam& c = fc[v];
-          const double cx = c.r[0] * x[0] + c.r[1] * x[1] + c.r[2] * x[2] + c.t[0];
-          const double cy = c.r[3] * x[0] + c.r[4] * x[1] + c.r[5] * x[2] + c.t[1];
-          const double cz = c.r[6] * x[0] + c.r[7] * x[1] + c.r[8] * x[2] + c.t[2];
-          if (cz <= 0.0) continue;
-          const double col = std::round(c.k[0] * cx / cz + c.k[2]), row = std::round(c.k[1] * cy / cz + c.k[3]);
-          if (col < 0.0 || row < 0.0 || col >= (double)c.w || row >= (double)c.h) continue;
-          const double dv = (double)depth[v][(size_t)row * c.w + (size_t)col];
-          if (dv <= 0.0) continue;
-          if (cz < dv * (1.0 - p->visibility_tau)) viol++;
-          else if (std::fabs(cz - dv) <= p->visibility_tau * dv) sup++;
-        }
-        if (viol >= (int)p->visibility_min_violations && viol > sup) {
+        if (visibility_violated(pt.pos, pt.vis.data(), pt.vis.size(), nviews, cams, fc, depth, used,
+                                p->visibility_check_views, p->visibility_min_violations, p->visibility_tau)) {
           vis_removed++;
           continue;
         }
@@ -1714,67 +1800,14 @@ int oracle_fuse(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* wid
       if (!dd.empty()) gs.push_back(median(dd) / fc[v].k[0]);
     }
     const double gsd = gs.empty() ? 0.0 : median(gs);
-    const size_t n = cl.size();
-    if (gsd > 0.0 && n > 0) {
-      const double r = p->smooth_radius_gsd * gsd;
-      const double r2 = r * r;
-      const double inv_2ss = 1.0 / (2.0 * ((0.5 * r) * (0.5 * r)));
-      const double sr = p->smooth_sigma_range_gsd * gsd;
-      const double inv_2sr = 1.0 / (2.0 * (sr * sr));
-      const double cos_n = std::cos(ps_to_radians_f64(p->smooth_normal_deg));
-      std::vector<std::array<double, 3>> nrm(n);
-      for (size_t i = 0; i < n; ++i) {
-        const double m[3] = {(double)cl[i]->nrm[0], (double)cl[i]->nrm[1], (double)cl[i]->nrm[2]};
-        const double l = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
-        nrm[i] = l > 1e-12 ? std::array<double, 3>{m[0] / l, m[1] / l, m[2] / l} : std::array<double, 3>{0.0, 0.0, 0.0};
-      }
-      for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
-        // cell -> points in cloud order (cells packed 21 bits per axis around 2^20; the device requires that range)
-        auto pack = [](long long x, long long y, long long z) {
-          return ((uint64_t)(x + (1ll << 20)) << 42) | ((uint64_t)(y + (1ll << 20)) << 21) | (uint64_t)(z + (1ll << 20));
-        };
-        std::unordered_map<uint64_t, std::vector<uint32_t>> grid;
-        grid.reserve(n);
-        std::vector<std::array<long long, 3>> cell(n);
-        for (size_t i = 0; i < n; ++i) {
-          for (int a = 0; a < 3; ++a) cell[i][a] = (long long)std::floor((double)cl[i]->pos[a] / r);
-          grid[pack(cell[i][0], cell[i][1], cell[i][2])].push_back((uint32_t)i);
-        }
-        std::vector<std::array<float, 3>> next(n);
-#pragma omp parallel for schedule(dynamic, 256)
-        for (long long ii = 0; ii < (long long)n; ++ii) {
-          const size_t i = (size_t)ii;
-          const double pi[3] = {(double)cl[i]->pos[0], (double)cl[i]->pos[1], (double)cl[i]->pos[2]};
-          const auto& ni = nrm[i];
-          double t = 0.0;
-          if (!(ni[0] == 0.0 && ni[1] == 0.0 && ni[2] == 0.0)) {
-            double sw = 1.0, swd = 0.0;
-            for (long long dz = -1; dz <= 1; ++dz)
-              for (long long dy = -1; dy <= 1; ++dy)
-                for (long long dx = -1; dx <= 1; ++dx) {
-                  auto g = grid.find(pack(cell[i][0] + dx, cell[i][1] + dy, cell[i][2] + dz));
-                  if (g == grid.end()) continue;
-                  for (uint32_t j : g->second) {
-                    const double dv[3] = {(double)cl[j]->pos[0] - pi[0], (double)cl[j]->pos[1] - pi[1],
-                                          (double)cl[j]->pos[2] - pi[2]};
-                    const double d2 = dv[0] * dv[0] + dv[1] * dv[1] + dv[2] * dv[2];
-                    if (d2 > r2 || j == i) continue;
-                    const auto& nj = nrm[j];
-                    if (ni[0] * nj[0] + ni[1] * nj[1] + ni[2] * nj[2] < cos_n) continue;
-                    const double dn = ni[0] * dv[0] + ni[1] * dv[1] + ni[2] * dv[2];
-                    const double w = ps_exp64(-d2 * inv_2ss - dn * dn * inv_2sr);
-                    sw += w;
-                    swd += w * dn;
-                  }
-                }
-            t = swd / sw;
-          }
-          for (int a = 0; a < 3; ++a) next[i][a] = (float)(pi[a] + t * ni[a]);
-        }
-        for (size_t i = 0; i < n; ++i)
-          for (int a = 0; a < 3; ++a) cl[i]->pos[a] = next[i][a];
-      }
+    std::vector<float*> ppos;
+    std::vector<const float*> pnrm;
+    for (FPoint* q : cl) {
+      ppos.push_back(q->pos);
+      pnrm.push_back(q->nrm);
     }
+    smooth_points(ppos, pnrm, gsd, p->smooth_iterations, p->smooth_radius_gsd, p->smooth_sigma_range_gsd,
+                  p->smooth_normal_deg);
   }
   uint64_t n_out = 0;
   for (std::vector<FPoint>* part : {&out1, &out2})
@@ -1969,6 +2002,50 @@ int oracle_select_neighbors(const ps_sparse_view* views, uint32_t nv, const doub
     depth_range[2 * v + 1] = 1.25 * hi;
   }
   return PS_OK;
+}
+
+// filter_visibility (crates/dense/src/visibility.rs:106-151) on a bare cloud: keep[i] = 0 for the removed points;
+// returns their number (0 when the filter is off: check_views, min_violations and tau must all be positive).
+int64_t oracle_filter_visibility(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* widths,
+                                 const uint32_t* heights, const float* const* depth, const uint8_t* used,
+                                 const float* positions, const uint8_t* vis_counts, const uint16_t* vis,
+                                 uint32_t vis_stride, uint64_t n, uint32_t check_views, uint32_t min_violations,
+                                 double tau, uint8_t* keep) {
+  if (!cams || !widths || !heights || !depth || !used || (n && (!positions || !vis_counts || !vis || !keep)))
+    return -1;
+  std::vector<FCam> fc(nviews);
+  for (uint32_t v = 0; v < nviews; ++v) {
+    memcpy(fc[v].k, cams[v].k, sizeof fc[v].k);
+    memcpy(fc[v].r, cams[v].r, sizeof fc[v].r);
+    memcpy(fc[v].t, cams[v].t, sizeof fc[v].t);
+    fc[v].w = (int)widths[v];
+    fc[v].h = (int)heights[v];
+  }
+  const bool on = check_views > 0 && tau > 0.0 && min_violations > 0;
+  int64_t removed = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    const bool out = on && visibility_violated(positions + 3 * i, vis + i * vis_stride,
+                                               std::min<uint32_t>(vis_counts[i], vis_stride), nviews, cams, fc, depth,
+                                               used, check_views, min_violations, tau);
+    keep[i] = out ? 0 : 1;
+    removed += out;
+  }
+  return removed;
+}
+
+// smooth_along_normals on a bare cloud (positions updated in place); returns the median absolute displacement of the
+// last pass, as the reference does.
+double oracle_smooth(float* positions, const float* normals, uint64_t n, double gsd, uint32_t iterations,
+                     double radius_gsd, double sigma_range_gsd, double normal_deg, int threads) {
+  if ((!positions || !normals) && n) return -1.0;
+  set_threads(threads);
+  std::vector<float*> ppos(n);
+  std::vector<const float*> pnrm(n);
+  for (uint64_t i = 0; i < n; ++i) {
+    ppos[i] = positions + 3 * i;
+    pnrm[i] = normals + 3 * i;
+  }
+  return smooth_points(ppos, pnrm, gsd, iterations, radius_gsd, sigma_range_gsd, normal_deg);
 }
 
 // ---- score fusion (crates/dense/src/fusion_score.rs:196-435) -------------------------------------------------

@@ -299,3 +299,83 @@ def test_smoothing_moves_points_along_normals_toward_the_surface(gt_scene):
         return float(np.median(e))
 
     assert err(sm) < 0.8 * err(base)
+
+
+def _mix64(z):
+    """mix64 (crates/dense/src/math.rs:40-47): the splitmix64 finalizer."""
+    m = (1 << 64) - 1
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & m
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & m
+    return z ^ (z >> 31)
+
+
+def _noisy_plane(n, noise):
+    """noisy_plane of crates/dense/src/smooth.rs:231-245: points uniform on [0, 4]² with z uniform in ±noise, normals
+    +z, from the reference's mix64 sequence."""
+    s = 0x12345678
+    vals = np.empty(3 * n)
+    for i in range(3 * n):
+        s = _mix64((s + 0x9E3779B97F4A7C15) & ((1 << 64) - 1))
+        vals[i] = (s >> 11) / float(1 << 53)
+    v = vals.reshape(n, 3)
+    pos = np.stack([v[:, 0] * 4.0, v[:, 1] * 4.0, (v[:, 2] - 0.5) * 2.0 * noise], 1).astype(np.float32)
+    return pos, np.tile(np.float32([0, 0, 1]), (n, 1))
+
+
+def test_smoothing_thins_a_noisy_plane_without_moving_tangentially():
+    """thins_a_noisy_plane_without_moving_tangentially (crates/dense/src/smooth.rs:252-263)."""
+    pos, nrm = _noisy_plane(20000, 0.01)
+    out, disp = oracle.smooth(pos, nrm, 0.05, 1, 4.0, 1.0, 30.0)
+    rms = lambda p: float(np.sqrt(np.mean(p[:, 2].astype(np.float64) ** 2)))
+    assert disp > 0.0
+    assert rms(out) < 0.5 * rms(pos)
+    np.testing.assert_array_equal(out[:, :2], pos[:, :2])
+
+
+def test_smoothing_keeps_a_step_and_respects_normals():
+    """keeps_a_step_and_respects_normals (crates/dense/src/smooth.rs:265-284): two sheets 0.5 apart stay apart under
+    the range term; smoothing off leaves a cloud untouched."""
+    lower, nrm = _noisy_plane(10000, 0.0)
+    upper = lower.copy()
+    upper[:, 2] = 0.5
+    out, _ = oracle.smooth(np.concatenate([lower, upper]), np.concatenate([nrm, nrm]), 0.05, 2, 12.0, 0.5, 30.0)
+    assert (np.abs(out[:10000, 2]) < 1e-4).all()
+    assert (np.abs(out[10000:, 2] - 0.5) < 1e-4).all()
+    c, cn = _noisy_plane(100, 0.01)
+    same, d = oracle.smooth(c, cn, 0.05, 0, 1.0, 0.25, 30.0)  # SmoothParams::default(): 0 iterations
+    assert d == 0.0
+    np.testing.assert_array_equal(same, c)
+
+
+def _floater_cloud(wl):
+    """setup() of crates/dense/src/visibility.rs:170-189 on this package's scene: five pixels near the middle of view
+    0 lifted at their true depth and at 80 % of it (the reference's half depth leaves this scene's narrower frames),
+    each point seen by view 0 only; every other view overlaps."""
+    cam = wl.cams[0]
+    h, w = wl.gt_depth[0].shape
+    pix = [(w // 2 + dx, h // 2 + dy) for dx, dy in ((-20, -10), (0, 0), (20, 10), (-10, 15), (10, -15))]
+    pts = []
+    for frac in (1.0, 0.8):
+        for col, row in pix:
+            d = float(wl.gt_depth[0][row, col])
+            c = np.array([(col - cam.k[2]) / cam.k[0] * d * frac, (row - cam.k[3]) / cam.k[1] * d * frac, d * frac])
+            pts.append(cam.r.T @ (c - cam.t))
+    n = len(wl.cams)
+    overlap = [[o for o in range(n) if o != v] for v in range(n)]
+    return np.array(pts, np.float32), [[0]] * len(pts), overlap
+
+
+def test_visibility_removes_floaters_and_keeps_surface(gt_scene):
+    """removes_floaters_and_keeps_plane and default_params_leave_cloud_unchanged (crates/dense/src/visibility.rs:196-
+    220): with 8 views, 2 violations and 1 % the five floaters go and the five surface points stay; the default
+    parameters (check_views 0) keep everything."""
+    wl, _ = gt_scene
+    pts, vis, overlap = _floater_cloud(wl)
+    fc = fusion.FusionCams(wl.cams, [list(kv.sources) for kv in wl.input.views], overlap=overlap)
+    depth = [g.astype(np.float32) for g in wl.gt_depth]
+    keep = oracle.filter_visibility(fc, depth, range(len(depth)), pts, vis, 8, 2, 0.01)
+    assert keep.tolist() == [True] * 5 + [False] * 5
+    p = fusion.default_fusion()
+    keep = oracle.filter_visibility(fc, depth, range(len(depth)), pts, vis, p.visibility_check_views,
+                                    p.visibility_min_violations, p.visibility_tau)
+    assert keep.all()

@@ -153,6 +153,40 @@ def test_fusion_depth_tolerance(gt_scene):
     assert merged(sc) * 50 < merged(base)
 
 
+def _rotated_normals(normals, deg):
+    """Every normal turned by exactly `deg` (Rodrigues rotation about an axis perpendicular to it)."""
+    n = normals.astype(np.float64)
+    k = np.cross(n, np.array([1.0, 0.0, 0.0]))
+    k /= np.linalg.norm(k, axis=-1, keepdims=True)
+    a = np.radians(deg)
+    return (n * np.cos(a) + np.cross(k, n) * np.sin(a)).astype(np.float32)
+
+
+def test_fusion_normal_tolerance_and_marks(gt_scene):
+    """fusion_depth_and_normal_tolerances (normal half) and consistency_fusion_of_true_maps (crates/dense/tests/
+    host_parts.rs:163-196, :231-250): one view's normals turned by 15° stop merging at the 10° tolerance, by 8° they
+    still merge; without marks the same surface is emitted again per view (more points)."""
+    wl, fc = gt_scene
+    d = [g.astype(np.float32) for g in wl.gt_depth]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    prm = fusion.default_fusion(3)
+
+    def run(normals, p=prm):
+        return oracle.fuse(fc, d, normals, c, list(wl.images), range(len(d)), p)
+
+    merged = lambda cl: int(sum(1 for i in range(len(cl)) if 2 in cl.visibility(i) and cl.vis_counts[i] > 1))
+    n0 = [g.astype(np.float32) for g in wl.gt_normal]
+    base = run(n0)
+    for deg, far in ((15.0, True), (8.0, False)):
+        nr = [g.copy() for g in n0]
+        nr[2] = _rotated_normals(nr[2], deg)
+        m = merged(run(nr))
+        assert (m * 20 < merged(base)) if far else (m * 2 > merged(base)), deg
+    nomark = fusion.default_fusion(3)
+    nomark.mark_used = 0
+    assert len(run(n0, nomark)) > len(base)
+
+
 def _fuse_gt_noisy(wl, fc, prm, seed=5):
     """Ground-truth maps with multiplicative depth noise, so the first pass leaves pixels for the second."""
     rng = np.random.default_rng(seed)
@@ -191,6 +225,40 @@ def test_residual_release_equals_none_and_second_pass_appends(gt_scene):
     gsd_lo = 0.5 * min(np.median(g[g > 0]) / c.k[0] for g, c in zip(wl.gt_depth, wl.cams)) * 0.9
     for x in d2[::7]:
         assert np.min(np.sum((d1 - x) ** 2, axis=1)) > gsd_lo ** 2
+
+
+def test_fusion_keys_unique_reproducible_and_thread_independent(gt_scene):
+    """fusion_keys_are_unique_and_reproducible and second_pass_is_deterministic (crates/dense/tests/
+    residual_fusion.rs:154-200): consistency fusion, its second pass and score fusion give unique keys whose view
+    and pixel exist, the same cloud on 1, 3 and all threads, and the same keys when run again."""
+    wl, fc = gt_scene
+    rng = np.random.default_rng(5)
+    d = [(g * (1.0 + rng.normal(0, 0.006, g.shape))).astype(np.float32) for g in wl.gt_depth]
+    n = [g.astype(np.float32) for g in wl.gt_normal]
+    c = [np.full(g.shape, 0.3, np.float32) for g in d]
+    sp = fusion.default_fusion(3)
+    sp.residual = 2
+    args = (fc, d, n, c, list(wl.images), range(len(d)))
+    runs = {"consistency": lambda t: oracle.fuse(*args, fusion.default_fusion(3), t),
+            "second pass": lambda t: oracle.fuse(*args, sp, t),
+            "score": lambda t: oracle.fuse_scored(*args, fusion.default_score_fusion(), t)}
+    for name, run in runs.items():
+        a = run(None)
+        assert len(a) > 500, name
+        assert len(set(a.keys.tolist())) == len(a), name
+        for t in (1, 3):
+            b = run(t)
+            np.testing.assert_array_equal(a.keys, b.keys, name)
+            np.testing.assert_array_equal(a.positions, b.positions, name)
+            np.testing.assert_array_equal(a.normals, b.normals, name)
+            np.testing.assert_array_equal(a.colors, b.colors, name)
+            np.testing.assert_array_equal(a.vis, b.vis, name)
+        keys = a.keys.astype(np.int64)
+        img, row, col = keys >> 32, (keys >> 16) & 0xFFFF, keys & 0xFFFF
+        assert ((img >= 0) & (img < len(d))).all(), name  # image ids here are the view indices
+        h = np.array([g.shape[0] for g in d])[img]
+        w = np.array([g.shape[1] for g in d])[img]
+        assert ((row < h) & (col < w)).all(), name
 
 
 def _visibility_keep_py(cloud, depths, fc_views, used, limit, tau, min_viol):

@@ -2296,20 +2296,20 @@ int ps_fused_visibility_removed(ps_session* s, uint64_t* removed) {
   });
 }
 
-void ps_score_fusion_params_default(ps_score_fusion_params* o) {
-  if (!o) return;
-  memset(o, 0, sizeof *o);
-  o->sigma_e_px = 1.0;
-  o->sigma_theta_deg = 2.0;
-  o->lambda = 1.0;
-  o->tau = 2.0;
-  o->depth_error = 0.01;
-  o->normal_error_deg = 10.0;
-  o->num_neighbors = 12;
-  o->mark_used = 1;
-  o->inverse_variance = 1;
-  o->sigma_px0 = 0.25;
-  o->sigma_px_slope = 1.0;
+void ps_score_fusion_params_default(ps_score_fusion_params* out) {
+  if (!out) return;
+  memset(out, 0, sizeof *out);
+  out->sigma_e_px = 1.0;
+  out->sigma_theta_deg = 2.0;
+  out->lambda = 1.0;
+  out->tau = 2.0;
+  out->depth_error = 0.01;
+  out->normal_error_deg = 10.0;
+  out->num_neighbors = 12;
+  out->mark_used = 1;
+  out->inverse_variance = 1;
+  out->sigma_px0 = 0.25;
+  out->sigma_px_slope = 1.0;
 }
 
 // fuse_scored (crates/dense/src/fusion_score.rs:314-435): candidates per view (one launch per fused view, in index

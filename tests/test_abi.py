@@ -98,6 +98,13 @@ def test_null_arguments_rejected_without_device():
     assert lib.ps_net_train_step(None, None, None, 1, 8, 8, 25.0, 60.0, 0.0, 0.0, None, None) == _lib.PS_EINVAL
     assert lib.ps_sweep_volume(None, 0, 0, None, 0) == _lib.PS_EINVAL
     assert lib.ps_propose(None, None, 0, None, 0, 0.5, None) == _lib.PS_EINVAL
+    # post-processing and fusion entry points
+    assert lib.ps_postprocess_resident(None, 0, None, 0, None, None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_fuse_resident(None, 0, None, 0, None, None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_fuse_scored_resident(None, 0, None, 0, None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_fused_points(None, 0, None, None, None, None, None, None, 0) == _lib.PS_EINVAL
+    assert lib.ps_fused_visibility_removed(None, None) == _lib.PS_EINVAL
+    lib.ps_score_fusion_params_default(None)  # NULL is ignored, as by the other *_default functions
 
 
 def test_defaults_match_reference():

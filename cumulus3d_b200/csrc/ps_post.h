@@ -4,7 +4,7 @@
 
 #include "ps_types.h"
 
-#define PS_FUSE_MAX_OVERLAP 32  // overlap views checked per reference pixel (consistency_num_images is at most this)
+#define PS_FUSE_MAX_OVERLAP 32  // overlap views checked per reference pixel (consistency_num_images and num_neighbors)
 
 namespace ps_post {
 

@@ -108,6 +108,7 @@ class FusedCloud:
     keys: np.ndarray       # (n,) u64
     vis_counts: np.ndarray  # (n,) u8
     vis: np.ndarray        # (n, stride) u16, first vis_counts entries valid (ascending view indices)
+    residual: int = 0      # the last `residual` points come from the second pass of leftover pixels
 
     def __len__(self) -> int:
         return int(self.positions.shape[0])
@@ -115,8 +116,32 @@ class FusedCloud:
     def visibility(self, i: int) -> List[int]:
         return [int(x) for x in self.vis[i, : self.vis_counts[i]]]
 
+    def num_residual(self) -> int:
+        """DenseOutput::num_residual (crates/dense/src/densify.rs:155-158)."""
+        return int(self.residual)
+
     def write_ply(self, path) -> None:
+        """DenseOutput::write_ply (crates/dense/src/densify.rs:143-153): creates the parent folder."""
+        _parent_dir(path)
         write_ply(path, self.positions, self.normals, self.colors)
+
+    def write_residual_ply(self, path) -> bool:
+        """DenseOutput::write_residual_ply (crates/dense/src/densify.rs:160-180): only the second-pass points; False
+        without writing when there are none."""
+        r = self.num_residual()
+        if r == 0:
+            return False
+        _parent_dir(path)
+        n = len(self)
+        write_ply(path, self.positions[n - r:], self.normals[n - r:], self.colors[n - r:])
+        return True
+
+
+def _parent_dir(path) -> None:
+    import pathlib
+    parent = pathlib.Path(path).parent
+    if str(parent):
+        parent.mkdir(parents=True, exist_ok=True)
 
 
 def write_ply(path, positions: np.ndarray, normals: Optional[np.ndarray] = None,

@@ -445,7 +445,7 @@ class PatchMatchSession:
         vis = np.empty((n, stride), np.uint16)
         self._check(self.lib.ps_fused_points(self.h, n, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data,
                                              key.ctypes.data, nv.ctypes.data, vis.ctypes.data, stride))
-        return FusedCloud(pos, nrm, col, key, nv, vis)
+        return FusedCloud(pos, nrm, col, key, nv, vis, getattr(self, "fused_residual", 0))
 
     def schedule_multiscale(self, views: Sequence[int], photometric_iters: int = 6, photometric_iters_upper: int = 3,
                             geometric_rounds: int = 2, geometric_iters: int = 2, jbu_sigma_spatial: float = 1.0,

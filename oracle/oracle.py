@@ -270,8 +270,7 @@ def fuse(cams, depths, normals, costs, images, views, params, threads: Optional[
                            _threads(threads), cap, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data, key.ctypes.data,
                            vc.ctypes.data, vis.ctypes.data, stride, C.byref(n), C.byref(r), C.byref(vr)), "fuse")
     k = int(n.value)
-    out = FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
-    out.residual = int(r.value)  # points of the second pass (the last ones)
+    out = FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k], int(r.value))
     out.visibility_removed = int(vr.value)
     return out
 

@@ -261,6 +261,31 @@ def test_fusion_keys_unique_reproducible_and_thread_independent(gt_scene):
         assert ((row < h) & (col < w)).all(), name
 
 
+def test_residual_ply_holds_the_second_pass_points(gt_scene, tmp_path):
+    """DenseOutput::write_ply / write_residual_ply (crates/dense/src/densify.rs:143-180): the parent folder is
+    created; the residual file holds exactly the second-pass points; without them nothing is written."""
+    wl, fc = gt_scene
+    sp = fusion.default_fusion(3)
+    sp.residual = 2
+    cl = _fuse_gt_noisy(wl, fc, sp)
+    r = cl.num_residual()
+    assert r > 0
+    f = tmp_path / "out" / "dense" / "residual.ply"
+    assert cl.write_residual_ply(f)
+    b = f.read_bytes()
+    body = b[b.index(b"end_header\n") + len(b"end_header\n"):]
+    rec = np.frombuffer(body, dtype=np.dtype([("p", "<f4", 3), ("n", "<f4", 3), ("c", "u1", 3)]))
+    assert len(rec) == r and f"element vertex {r}\n".encode() in b
+    np.testing.assert_array_equal(rec["p"], cl.positions[len(cl) - r:])
+    np.testing.assert_array_equal(rec["c"], cl.colors[len(cl) - r:])
+    cl.write_ply(tmp_path / "x" / "all.ply")
+    a = (tmp_path / "x" / "all.ply").read_bytes()
+    assert len(a) - (a.index(b"end_header\n") + len(b"end_header\n")) == 27 * len(cl)
+    none = _fuse_gt_noisy(wl, fc, fusion.default_fusion(3))
+    assert none.num_residual() == 0
+    assert not none.write_residual_ply(tmp_path / "none.ply") and not (tmp_path / "none.ply").exists()
+
+
 def _visibility_keep_py(cloud, depths, fc_views, used, limit, tau, min_viol):
     """filter_visibility (crates/dense/src/visibility.rs:106-151) restated in Python: the keep flag of every point."""
     keep = []

@@ -507,13 +507,15 @@ typedef struct ps_score_fusion_params {
 } ps_score_fusion_params;
 void ps_score_fusion_params_default(ps_score_fusion_params* out);
 /* Score fusion of the readout planes and final costs of `views` at `level` (cams as for ps_fuse_resident); the
- * cloud replaces the session's fused cloud (ps_fused_points reads it; its order is the reference's: ascending key). */
+ * cloud replaces the session's fused cloud (ps_fused_points reads it, in the reference's order: view index, then
+ * pixel).  num_points: the adopted points. */
 int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
                             const ps_score_fusion_params* p, uint64_t* num_points);
-/* The fused points in the reference's order: the first pass in ascending point key (image_id << 32) | (row << 16) |
- * col, then the second-pass points in ascending key: positions and normals 3 floats, colours 3 bytes, keys, the
- * number of contributing views and their indices (ascending, vis_stride >= consistency_num_images + 1 entries per
- * point).  Any output may be NULL. */
+/* The fused points in the reference's order: after ps_fuse_resident the first pass in ascending point key
+ * (image_id << 32) | (row << 16) | col, then the second-pass points in ascending key; after ps_fuse_scored_resident
+ * (view index, pixel) order.  Positions and normals 3 floats, colours 3 bytes, keys, the number of contributing views
+ * and their indices (ascending; vis_stride >= consistency_num_images + 1, or num_neighbors + 1, entries per point).
+ * Any output may be NULL. */
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride);
 

@@ -286,13 +286,55 @@ def _greedy(pixsets, ranks):
     return out
 
 
+def _device_rounds(pixsets, ranks, rng):
+    """The engine's form of the rounds (k_score_reset / k_score_claim / k_score_adopt): rejection in the reset phase,
+    adoption and locking in one phase, the undecided ones compacted into the next round's list in completion order.
+    Threads of a phase run one at a time in a random order, each thread's steps interleaved with nothing: every
+    pixel's final claim is the same for any order, and the adopt phase's outcome must not depend on it."""
+    FREE, LOCKED = 1 << 64, 0
+    claim = {}
+    state = [2] * len(pixsets)  # 2 undecided, 1 adopted, 0 rejected
+    active = list(range(len(pixsets)))
+    while active:
+        for g in rng.permutation(active).tolist():  # reset: free unlocked pixels, reject on a locked one
+            locked = False
+            for q in pixsets[g]:
+                if claim.get(q, FREE) == LOCKED:
+                    locked = True
+                else:
+                    claim[q] = FREE
+            if locked:
+                state[g] = 0
+        for g in rng.permutation(active).tolist():  # claim: atomic minimum
+            if state[g] == 2:
+                for q in pixsets[g]:
+                    claim[q] = min(claim.get(q, FREE), ranks[g])
+        nxt = []
+        for g in rng.permutation(active).tolist():  # adopt and lock
+            if state[g] != 2:
+                continue
+            if all(claim[q] == ranks[g] for q in pixsets[g]):
+                state[g] = 1
+                for q in pixsets[g]:
+                    claim[q] = LOCKED
+            else:
+                nxt.append(g)
+        active = nxt
+    return [x == 1 for x in state]
+
+
 @pytest.mark.parametrize("seed", range(8))
 def test_claim_rounds_equal_greedy_selection(seed):
+    """The reference's rounds and the engine's form of them both choose what greedy selection in priority order
+    chooses, on random pixel sets with many overlaps, for several thread orders."""
     rng = np.random.default_rng(seed)
     n, universe = 400, 300 + 100 * seed
     pixsets = [sorted(set(rng.integers(0, universe, size=int(rng.integers(1, 6))).tolist())) for _ in range(n)]
     ranks = (rng.permutation(n) + 1).tolist()
-    assert _rounds(pixsets, ranks) == _greedy(pixsets, ranks)
+    want = _greedy(pixsets, ranks)
+    assert _rounds(pixsets, ranks) == want
+    for k in range(3):
+        assert _device_rounds(pixsets, ranks, np.random.default_rng(100 * seed + k)) == want
 
 
 def test_acos64_is_faithful():

@@ -93,3 +93,21 @@ def test_fp64_reevaluation_close_to_fp32(small):
     ok = (c32 < 1.5) & (c64 < 1.5)
     assert ok.mean() > 0.5
     assert np.median(np.abs(c32[ok] - c64[ok])) < 1e-5
+
+
+@pytest.mark.parametrize("case", ["radius20", "sources32"])
+def test_oracle_runs_at_the_abi_limits(case):
+    """The limits the reference validates (crates/cuda/src/patchmatch.rs:292-294, :366-371): window radius 20 (a
+    41×41 window larger than the image) and 32 sources.  The restatement runs there, with finite costs in [0, 2]
+    positive depths and unit normals."""
+    if case == "radius20":
+        wl = scenes.workload_small(32, 24, views=3, window_radius=20, seed=5, sources=2)
+    else:
+        wl = scenes.workload_small(24, 16, views=33, window_radius=1, seed=6, sources=32, positions=11)
+        assert all(len(kv.sources) == 32 for kv in wl.input.views)
+    st = [ViewState.new(c.width, c.height) for c in wl.cams]
+    oracle.run(wl.input, wl.views, st, RunParams(0, False, True, 1, 1))
+    for s in st:
+        assert np.isfinite(s.cost).all() and (s.cost >= 0).all() and (s.cost <= 2).all()
+        assert np.isfinite(s.depth).all() and (s.depth > 0).all()
+        assert np.allclose(np.linalg.norm(s.normal, axis=-1), 1.0, atol=1e-4)

@@ -80,9 +80,10 @@ def lib() -> C.CDLL:
             "oracle_expf": (C.c_float, [C.c_float]),
             "oracle_fuse_scored": (C.c_int, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
                                              C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                             C.c_void_p, C.POINTER(_lib.ScoreFusionParams), C.c_int, C.c_uint64,
-                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
-                                             C.c_uint32, C.POINTER(C.c_uint64)]),
+                                             C.c_void_p, C.POINTER(_lib.ScoreFusionParams),
+                                             C.POINTER(_lib.FusionParams), C.c_int, C.c_uint64, C.c_void_p,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                             C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
             "oracle_smooth": (C.c_double, [C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_uint32, C.c_double,
                                            C.c_double, C.c_double, C.c_int]),
             "oracle_filter_visibility": (C.c_int64, [C.c_uint32, C.POINTER(_lib.FusionView), C.POINTER(C.c_uint32),
@@ -314,9 +315,11 @@ def smooth(positions, normals, gsd: float, iterations: int, radius_gsd: float, s
     return pos, float(d)
 
 
-def fuse_scored(cams, depths, normals, costs, images, views, params, threads: Optional[int] = None):
-    """Score fusion restated (fuse_scored, crates/dense/src/fusion_score.rs:314-435); inputs as for fuse.  Returns a
-    fusion.FusedCloud in the reference's point order: (view, pixel) ascending."""
+def fuse_scored(cams, depths, normals, costs, images, views, params, threads: Optional[int] = None, post=None):
+    """Score fusion restated (fuse_scored, crates/dense/src/fusion_score.rs:314-435); inputs as for fuse.  With
+    `post` (a FusionParams), its visibility filter and smoothing follow, as fuse_depth_maps_with runs them
+    (crates/dense/src/densify.rs:535-556).  Returns a fusion.FusedCloud in the reference's point order: (view, pixel)
+    ascending; `.visibility_removed` counts the points the filter removed."""
     from cumulus3d_b200.fusion import FusedCloud
     nv = len(depths)
     ws = (C.c_uint32 * nv)(*[d.shape[1] for d in depths])
@@ -334,12 +337,15 @@ def fuse_scored(cams, depths, normals, costs, images, views, params, threads: Op
     key = np.empty(cap, np.uint64)
     vc = np.empty(cap, np.uint8)
     vis = np.empty((cap, stride), np.uint16)
-    n = C.c_uint64()
+    n, vr = C.c_uint64(), C.c_uint64()
     _chk(lib().oracle_fuse_scored(nv, cams.table, ws, hs, dp, np_, cp, ip, used.ctypes.data, C.byref(params),
-                                  _threads(threads), cap, pos.ctypes.data, nrm.ctypes.data, col.ctypes.data,
-                                  key.ctypes.data, vc.ctypes.data, vis.ctypes.data, stride, C.byref(n)), "fuse_scored")
+                                  None if post is None else C.byref(post), _threads(threads), cap, pos.ctypes.data,
+                                  nrm.ctypes.data, col.ctypes.data, key.ctypes.data, vc.ctypes.data, vis.ctypes.data,
+                                  stride, C.byref(n), C.byref(vr)), "fuse_scored")
     k = int(n.value)
-    return FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
+    out = FusedCloud(pos[:k], nrm[:k], col[:k], key[:k], vc[:k], vis[:k])
+    out.visibility_removed = int(vr.value)
+    return out
 
 
 def select_neighbors(model, params, pair_stats: bool = False):

@@ -1441,6 +1441,30 @@ bool visibility_violated(const float* pos, const uint16_t* vis, size_t nvis, uin
   return viol >= (int)min_violations && viol > sup;
 }
 
+// scene_gsd (crates/dense/src/fusion.rs:463-487): per used view the median of every 97th valid depth over fx, then
+// the median over views (medians interpolated at 0.5·(n-1)); 0 without valid depths.
+double scene_gsd(uint32_t nviews, const std::vector<FCam>& fc, const float* const* depth, const uint8_t* used) {
+  auto median = [](std::vector<double>& a) {
+    std::sort(a.begin(), a.end());
+    const double pos = 0.5 * (double)(a.size() - 1);
+    const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, a.size() - 1);
+    return a[lo] + (a[hi] - a[lo]) * (pos - (double)lo);
+  };
+  std::vector<double> gs;
+  for (uint32_t v = 0; v < nviews; ++v) {
+    if (!used[v]) continue;
+    std::vector<double> dd;
+    size_t k = 0;
+    for (size_t i = 0; i < (size_t)fc[v].w * fc[v].h; ++i)
+      if (depth[v][i] > 0.0f) {
+        if (k % 97 == 0) dd.push_back((double)depth[v][i]);
+        ++k;
+      }
+    if (!dd.empty()) gs.push_back(median(dd) / fc[v].k[0]);
+  }
+  return gs.empty() ? 0.0 : median(gs);
+}
+
 // smooth_along_normals (crates/dense/src/smooth.rs:143-220) over points in cloud order: Jacobi passes; each point
 // sums its neighbours within the radius in the order of the 27 cells around it ((z, y, x) offsets), each cell's points
 // in cloud order.  Returns the median absolute displacement of the last pass (0 when nothing ran).
@@ -2056,9 +2080,10 @@ double oracle_smooth(float* positions, const float* normals, uint64_t n, double 
 // ps_acos64, as in the engine.
 int oracle_fuse_scored(uint32_t nviews, const ps_fusion_view* cams, const uint32_t* widths, const uint32_t* heights,
                        const float* const* depth, const float* const* normal, const float* const* cost,
-                       const float* const* img, const uint8_t* used, const ps_score_fusion_params* p, int threads,
-                       uint64_t capacity, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
-                       uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride, uint64_t* count) {
+                       const float* const* img, const uint8_t* used, const ps_score_fusion_params* p,
+                       const ps_fusion_params* post, int threads, uint64_t capacity, float* positions, float* normals,
+                       uint8_t* colors, uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride,
+                       uint64_t* count, uint64_t* visibility_removed) {
   if (!cams || !widths || !heights || !depth || !normal || !cost || !img || !used || !p || !count) return PS_EINVAL;
   set_threads(threads);
   std::vector<FCam> fc(nviews);
@@ -2209,6 +2234,31 @@ int oracle_fuse_scored(uint32_t nviews, const ps_fusion_view* cams, const uint32
       taken[c.v][c.pix] = 1;
       for (auto& hq : c.hits) taken[hq.first][hq.second] = 1;
     }
+  }
+  // fuse_depth_maps_with (crates/dense/src/densify.rs:535-556): the visibility filter, then the smoothing, on the
+  // adopted points in their order, with the fusion's overlap lists and the scene GSD of the fused views
+  uint64_t vis_removed = 0;
+  if (post && post->visibility_check_views > 0 && post->visibility_tau > 0.0 && post->visibility_min_violations > 0)
+    for (size_t g = 0; g < cands.size(); ++g) {
+      if (!accepted[g]) continue;
+      const FPoint& pt = cands[g].pt;
+      if (visibility_violated(pt.pos, pt.vis.data(), pt.vis.size(), nviews, cams, fc, depth, used,
+                              post->visibility_check_views, post->visibility_min_violations, post->visibility_tau)) {
+        accepted[g] = 0;
+        vis_removed++;
+      }
+    }
+  if (visibility_removed) *visibility_removed = vis_removed;
+  if (post && post->smooth_iterations > 0) {
+    std::vector<float*> ppos;
+    std::vector<const float*> pnrm;
+    for (size_t g = 0; g < cands.size(); ++g)
+      if (accepted[g]) {
+        ppos.push_back(cands[g].pt.pos);
+        pnrm.push_back(cands[g].pt.nrm);
+      }
+    smooth_points(ppos, pnrm, scene_gsd(nviews, fc, depth, used), post->smooth_iterations, post->smooth_radius_gsd,
+                  post->smooth_sigma_range_gsd, post->smooth_normal_deg);
   }
   uint64_t n_out = 0;
   for (size_t g = 0; g < cands.size(); ++g) {

@@ -347,3 +347,37 @@ def test_acos64_is_faithful():
         a, b = oracle.lib().oracle_acos64(float(x)), math.acos(float(x))
         worst = max(worst, abs(int(np.float64(a).view(np.int64)) - int(np.float64(b).view(np.int64))))
     assert worst <= 1
+
+
+def test_visibility_and_smoothing_after_score_fusion(scene):
+    """fuse_depth_maps_with (crates/dense/src/densify.rs:535-556) runs the visibility filter and then the smoothing
+    on the score-fusion cloud: the restatement's composed run equals the standalone filter and smoother applied to
+    the plain score cloud (overlap lists of the fusion, scene GSD of the fused views)."""
+    wl, fc = scene
+    rng = np.random.default_rng(8)
+    depth = [(g * (1.0 + rng.normal(0, 0.003, g.shape))).astype(np.float32) for g in wl.gt_depth]
+    for v in (1, 4):
+        depth[v] = depth[v] * np.float32(0.96)  # floaters in front of the surface the other views see
+    normal = [g.astype(np.float32) for g in wl.gt_normal]
+    cost = [np.full(g.shape, 0.2, np.float32) for g in depth]
+    imgs = list(wl.images)
+    views = range(len(depth))
+    sp = fusion.default_score_fusion(tau=0.5, lambda_=0.0)  # no penalty: the floaters stay candidates
+    post = fusion.default_fusion()
+    post.visibility_check_views, post.visibility_min_violations, post.visibility_tau = 8, 1, 0.01
+    post.smooth_iterations, post.smooth_radius_gsd, post.smooth_sigma_range_gsd = 2, 3.0, 0.5
+    plain = oracle.fuse_scored(fc, depth, normal, cost, imgs, views, sp)
+    both = oracle.fuse_scored(fc, depth, normal, cost, imgs, views, sp, post=post)
+    keep = oracle.filter_visibility(fc, depth, views, plain.positions, [plain.visibility(i) for i in range(len(plain))],
+                                    8, 1, 0.01)
+    assert 0 < both.visibility_removed == int((~keep).sum()) < len(plain)
+    np.testing.assert_array_equal(both.keys, plain.keys[keep])
+    np.testing.assert_array_equal(both.normals, plain.normals[keep])
+    gs = []
+    for g, c in zip(depth, wl.cams):
+        s = g.ravel()[g.ravel() > 0][::97].astype(np.float64)
+        gs.append(fusion.median_interp(s) / c.k[0])
+    smoothed, _ = oracle.smooth(plain.positions[keep], plain.normals[keep], fusion.median_interp(gs), 2, 3.0, 0.5,
+                                post.smooth_normal_deg)
+    np.testing.assert_array_equal(both.positions, smoothed)
+    assert not np.array_equal(smoothed, plain.positions[keep])

@@ -200,7 +200,8 @@ SIGNATURES = {
     "ps_fused_visibility_removed": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "ps_score_fusion_params_default": (None, [C.POINTER(ScoreFusionParams)]),
     "ps_fuse_scored_resident": (C.c_int, [_P, C.c_uint32, _U32P, C.c_size_t, C.POINTER(FusionView),
-                                          C.POINTER(ScoreFusionParams), C.POINTER(C.c_uint64)]),
+                                          C.POINTER(ScoreFusionParams), C.POINTER(FusionParams),
+                                          C.POINTER(C.c_uint64)]),
     "ps_fused_points": (C.c_int, [_P, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_void_p, C.c_uint32]),
     "ps_build_pyramid": (C.c_int, [C.c_int, C.c_void_p, C.c_uint32, C.c_uint32, C.POINTER(C.c_double), C.c_uint32,

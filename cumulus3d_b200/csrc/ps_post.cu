@@ -721,6 +721,7 @@ __global__ void __launch_bounds__(1024) k_gsd(const float4* __restrict__ plane, 
 __global__ void __launch_bounds__(256) k_visibility(const VisArgs A) {
   const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
   if (i >= A.n) return;
+  if (A.masked && A.keep[i] == 0) return;
   const double x[3] = {(double)A.pos[3 * i], (double)A.pos[3 * i + 1], (double)A.pos[3 * i + 2]};
   int cand[PS_VIS_MAX_CHECK];
   int nc = 0;
@@ -784,6 +785,7 @@ __device__ __forceinline__ bool sm_cell(const SmoothArgs& A, unsigned long long 
   return true;
 }
 __device__ __forceinline__ unsigned long long sm_order(const SmoothArgs& A, unsigned u) {
+  if (A.gid) return (unsigned long long)A.gid[u];
   return ((unsigned long long)(u >= A.n1) << 63) | A.key[u];
 }
 __device__ __forceinline__ int sm_find(const SmoothArgs& A, unsigned long long code) {
@@ -830,7 +832,8 @@ __global__ void __launch_bounds__(256) k_sm_scatter(const SmoothArgs A) {
   const unsigned s = A.pslot[i];
   A.list[A.hstart[s] + atomicAdd(&A.hcur[s], 1u)] = (unsigned)i;
 }
-// each cell's points in cloud order (first pass before second, then ascending key): insertion sort per cell
+// each cell's points in cloud order (first pass before second, then ascending key; or ascending candidate number):
+// insertion sort per cell
 __global__ void __launch_bounds__(256) k_sm_sort(const SmoothArgs A) {
   const unsigned s = blockIdx.x * 256u + threadIdx.x;
   if (s >= A.cap || !A.hcnt[s]) return;

@@ -131,6 +131,7 @@ struct VisArgs {
   int limit, min_violations;
   double tau;
   unsigned char* keep;
+  int masked;                   // 1: only points whose keep entry is set are tested (the others stay out, uncounted)
   unsigned long long* removed;  // [0]: first-pass points removed, [1]: second-pass points removed
 };
 
@@ -141,6 +142,7 @@ struct SmoothArgs {
   const float* nrm;
   const unsigned char* keep;          // visibility mask (NULL: every point)
   const unsigned long long* key;      // point keys; with the pass they give the cloud order
+  const unsigned* gid;                // candidate numbers (score fusion): the cloud order instead (NULL: keys)
   unsigned long long n, n1;           // points; the first n1 are from the first pass
   double r, r2, inv_2ss, inv_2sr, cos_n;
   unsigned long long* hkeys;          // cell table (cap slots, 0 = empty)

@@ -1964,6 +1964,166 @@ unsigned long long count_valid(ps_session* s, const uint32_t* views, size_t n, i
   sync(s);
   return valid;
 }
+
+// Ground sample distance (depth_gsd, crates/dense/src/fusion.rs:469-487) of the fused views `order` (ascending).
+double fused_gsd(ps_session* s, Slot& sl, const std::vector<uint32_t>& order, const ps_fusion_view* cams, int l) {
+  std::vector<ps_post::GsdView> gv(order.size());
+  long long soff = 0;
+  for (size_t i = 0; i < order.size(); ++i) {
+    const int v = (int)order[i];
+    gv[i].off = sl.off[v];
+    gv[i].npix = s->W(v, l) * s->H(v, l);
+    gv[i].soff = soff;
+    gv[i].fx = cams[v].k[0];
+    soff += (gv[i].npix + 96) / 97;
+  }
+  ps_post::GsdView* dgv = dalloc<ps_post::GsdView>(s, gv.size());
+  float* samples = dalloc<float>(s, std::max<long long>(soff, 1));
+  unsigned* scount = dalloc<unsigned>(s, gv.size());
+  double* dgsd = dalloc<double>(s, gv.size());
+  cuda_ok(cudaMemcpyAsync(dgv, gv.data(), gv.size() * sizeof(ps_post::GsdView), cudaMemcpyHostToDevice, s->st),
+          "upload gsd views");
+  launched(s, ps_post::launch_gsd(sl.aux, dgv, (int)gv.size(), samples, scount, dgsd, s->st), "gsd kernel");
+  std::vector<double> gs(gv.size());
+  cuda_ok(cudaMemcpyAsync(gs.data(), dgsd, gs.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st), "read gsd");
+  sync(s);
+  dfree(s, dgv);
+  dfree(s, samples);
+  dfree(s, scount);
+  dfree(s, dgsd);
+  std::vector<double> g2;
+  for (double x : gs)
+    if (!std::isnan(x)) g2.push_back(x);
+  double gsd = 0.0;
+  if (!g2.empty()) {  // median_in_place (crates/dense/src/math.rs:137-141)
+    std::sort(g2.begin(), g2.end());
+    const double pos = 0.5 * (double)(g2.size() - 1);
+    const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, g2.size() - 1);
+    gsd = g2[lo] + (g2[hi] - g2[lo]) * (pos - (double)lo);
+  }
+  return gsd;
+}
+
+// filter_visibility (crates/dense/src/visibility.rs:106-151) of the fused cloud, when p turns it on.  masked: only the
+// points whose keep entry is set are tested (the others stay out and are not counted); otherwise every point is, and
+// the keep mask is made here.
+void fused_visibility(ps_session* s, Slot& sl, FusedCloud& fc, const ps_fusion_view* cams,
+                      const std::vector<char>& used, const ps_fusion_params* p, bool masked) {
+  const bool vis_on = p->visibility_check_views > 0 && p->visibility_tau > 0.0 && p->visibility_min_violations > 0;
+  if (!vis_on || fc.count == 0) return;
+  if (p->visibility_check_views > PS_VIS_MAX_CHECK) fail(PS_EINVAL, "visibility_check_views > 64");
+  // full overlap lists of the fused views (the candidate order of the filter)
+  std::vector<int> ovoff(s->nv + 1, 0), ovlist;
+  for (int v = 0; v < s->nv; ++v) {
+    ovoff[v] = (int)ovlist.size();
+    if (!used[v]) continue;
+    for (uint32_t j = 0; j < cams[v].num_overlap; ++j) ovlist.push_back((int)cams[v].overlap[j]);
+  }
+  ovoff[s->nv] = (int)ovlist.size();
+  std::vector<unsigned char> used8(used.begin(), used.end());
+  int* dovoff = dalloc<int>(s, ovoff.size());
+  int* dovlist = dalloc<int>(s, std::max<size_t>(ovlist.size(), 1));
+  unsigned char* dused = dalloc<unsigned char>(s, std::max(s->nv, 1));
+  unsigned long long* drem = dalloc<unsigned long long>(s, 2);
+  if (!masked) fc.keep = dalloc<unsigned char>(s, fc.count);
+  cuda_ok(cudaMemcpyAsync(dovoff, ovoff.data(), ovoff.size() * sizeof(int), cudaMemcpyHostToDevice, s->st), "upload");
+  if (!ovlist.empty())
+    cuda_ok(cudaMemcpyAsync(dovlist, ovlist.data(), ovlist.size() * sizeof(int), cudaMemcpyHostToDevice, s->st),
+            "upload");
+  cuda_ok(cudaMemcpyAsync(dused, used8.data(), used8.size(), cudaMemcpyHostToDevice, s->st), "upload");
+  cuda_ok(cudaMemsetAsync(drem, 0, 2 * sizeof(unsigned long long), s->st), "memset");
+  ps_post::VisArgs V;
+  memset(&V, 0, sizeof V);
+  V.views = fc.views;
+  V.plane = sl.aux;
+  V.used = dused;
+  V.ovoff = dovoff;
+  V.ovlist = dovlist;
+  V.nviews = s->nv;
+  V.pos = fc.pos;
+  V.nvis = fc.nvis;
+  V.vis = fc.vis;
+  V.vis_stride = fc.vis_stride;
+  V.n = fc.count;
+  V.n1 = fc.count1;
+  V.limit = (int)p->visibility_check_views;
+  V.min_violations = (int)p->visibility_min_violations;
+  V.tau = p->visibility_tau;
+  V.keep = fc.keep;
+  V.masked = masked ? 1 : 0;
+  V.removed = drem;
+  launched(s, ps_post::launch_visibility(V, s->st), "visibility kernel");
+  unsigned long long rem[2] = {0, 0};
+  cuda_ok(cudaMemcpyAsync(rem, drem, sizeof rem, cudaMemcpyDeviceToHost, s->st), "read counts");
+  sync(s);
+  fc.removed1 = rem[0];
+  fc.removed2 = rem[1];
+  dfree(s, dovoff);
+  dfree(s, dovlist);
+  dfree(s, dused);
+  dfree(s, drem);
+}
+
+// smooth_along_normals (crates/dense/src/smooth.rs:143-220) of the kept points, as densify.rs:552-556 runs it, when p
+// turns it on; the neighbour order is the cloud order (candidate numbers after score fusion).
+void fused_smoothing(ps_session* s, Slot& sl, FusedCloud& fc, const std::vector<uint32_t>& order,
+                     const ps_fusion_view* cams, int l, const ps_fusion_params* p) {
+  const bool smooth_on = p->smooth_iterations > 0 && p->smooth_radius_gsd > 0.0 && p->smooth_sigma_range_gsd > 0.0;
+  if (!smooth_on || fc.count == 0) return;
+  const double gsd = fused_gsd(s, sl, order, cams, l);
+  if (gsd > 0.0) {
+    ps_post::SmoothArgs M;
+    memset(&M, 0, sizeof M);
+    M.r = p->smooth_radius_gsd * gsd;
+    M.r2 = M.r * M.r;
+    M.inv_2ss = 1.0 / (2.0 * ((0.5 * M.r) * (0.5 * M.r)));
+    const double sr = p->smooth_sigma_range_gsd * gsd;
+    M.inv_2sr = 1.0 / (2.0 * (sr * sr));
+    M.cos_n = std::cos(ps_to_radians_f64(p->smooth_normal_deg));
+    M.n = fc.count;
+    M.n1 = fc.count1;
+    M.nrm = fc.nrm;
+    M.keep = fc.keep;
+    M.key = fc.key;
+    M.gid = fc.gid;
+    unsigned cap = 1024;
+    while (cap < 2ull * fc.count) cap <<= 1;
+    M.cap = cap;
+    M.hkeys = dalloc<unsigned long long>(s, cap);
+    M.hcnt = dalloc<unsigned>(s, cap);
+    M.hstart = dalloc<unsigned>(s, cap);
+    M.hcur = dalloc<unsigned>(s, cap);
+    M.list = dalloc<unsigned>(s, fc.count);
+    M.pslot = dalloc<unsigned>(s, fc.count);
+    M.total = dalloc<unsigned>(s, 1);
+    M.flag = dalloc<int>(s, 1);
+    float* pos2 = dalloc<float>(s, 3 * fc.count);
+    cuda_ok(cudaMemcpyAsync(pos2, fc.pos, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
+    cuda_ok(cudaMemsetAsync(M.flag, 0, sizeof(int), s->st), "memset");
+    float* cur = fc.pos;
+    float* nxt = pos2;
+    for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
+      cuda_ok(cudaMemsetAsync(M.hkeys, 0, cap * sizeof(unsigned long long), s->st), "memset");
+      cuda_ok(cudaMemsetAsync(M.hcnt, 0, cap * sizeof(unsigned), s->st), "memset");
+      cuda_ok(cudaMemsetAsync(M.hcur, 0, cap * sizeof(unsigned), s->st), "memset");
+      cuda_ok(cudaMemsetAsync(M.total, 0, sizeof(unsigned), s->st), "memset");
+      M.pos = cur;
+      M.pos2 = nxt;
+      cuda_ok(ps_post::launch_smooth_pass(M, s->st), "smoothing kernels");
+      s->launches += 5;
+      std::swap(cur, nxt);
+    }
+    if (cur != fc.pos)
+      cuda_ok(cudaMemcpyAsync(fc.pos, cur, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
+    int flag = 0;
+    cuda_ok(cudaMemcpyAsync(&flag, M.flag, sizeof flag, cudaMemcpyDeviceToHost, s->st), "read flag");
+    sync(s);
+    for (void* q : {(void*)M.hkeys, (void*)M.hcnt, (void*)M.hstart, (void*)M.hcur, (void*)M.list, (void*)M.pslot,
+                    (void*)M.total, (void*)M.flag, (void*)pos2})
+      dfree(s, q);
+    if (flag) fail(PS_EINVAL, "smoothing: a point lies more than 2^20 smoothing radii from the origin");
+  }
+}
 }  // namespace
 
 int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
@@ -2068,46 +2228,8 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     cuda_ok(cudaMemcpyAsync(&cnt, fc.counter, sizeof cnt, cudaMemcpyDeviceToHost, s->st), "read count");
     sync(s);
     fc.count1 = std::min(cnt, fc.cap);
-    // ground sample distance (depth_gsd, fusion.rs:469-487) of the fused views, in index order
-    auto fused_gsd = [&]() {
-      std::vector<ps_post::GsdView> gv(order.size());
-      long long soff = 0;
-      for (size_t i = 0; i < order.size(); ++i) {
-        const int v = (int)order[i];
-        gv[i].off = sl.off[v];
-        gv[i].npix = s->W(v, l) * s->H(v, l);
-        gv[i].soff = soff;
-        gv[i].fx = cams[v].k[0];
-        soff += (gv[i].npix + 96) / 97;
-      }
-      ps_post::GsdView* dgv = dalloc<ps_post::GsdView>(s, gv.size());
-      float* samples = dalloc<float>(s, std::max<long long>(soff, 1));
-      unsigned* scount = dalloc<unsigned>(s, gv.size());
-      double* dgsd = dalloc<double>(s, gv.size());
-      cuda_ok(cudaMemcpyAsync(dgv, gv.data(), gv.size() * sizeof(ps_post::GsdView), cudaMemcpyHostToDevice, s->st),
-              "upload gsd views");
-      launched(s, ps_post::launch_gsd(sl.aux, dgv, (int)gv.size(), samples, scount, dgsd, s->st), "gsd kernel");
-      std::vector<double> gs(gv.size());
-      cuda_ok(cudaMemcpyAsync(gs.data(), dgsd, gs.size() * sizeof(double), cudaMemcpyDeviceToHost, s->st), "read gsd");
-      sync(s);
-      dfree(s, dgv);
-      dfree(s, samples);
-      dfree(s, scount);
-      dfree(s, dgsd);
-      std::vector<double> g2;
-      for (double x : gs)
-        if (!std::isnan(x)) g2.push_back(x);
-      double gsd = 0.0;
-      if (!g2.empty()) {  // median_in_place (crates/dense/src/math.rs:137-141)
-        std::sort(g2.begin(), g2.end());
-        const double pos = 0.5 * (double)(g2.size() - 1);
-        const size_t lo = (size_t)std::floor(pos), hi = std::min(lo + 1, g2.size() - 1);
-        gsd = g2[lo] + (g2[hi] - g2[lo]) * (pos - (double)lo);
-      }
-      return gsd;
-    };
     if (second) {
-      const double gsd = fused_gsd();
+      const double gsd = fused_gsd(s, sl, order, cams, l);
       const double min_dist = p->residual_min_dist_gsd * gsd;
       // candidate numbers: prefix of the fused views' pixel counts in index order (fusion.rs:560-565)
       std::vector<ps_post::FuseView> fv2 = fv;
@@ -2175,115 +2297,8 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
     fc.keep = nullptr;
     if (fc.gid) dfree(s, fc.gid);
     fc.gid = nullptr;
-    const bool vis_on = p->visibility_check_views > 0 && p->visibility_tau > 0.0 && p->visibility_min_violations > 0;
-    if (vis_on && fc.count > 0) {
-      if (p->visibility_check_views > PS_VIS_MAX_CHECK) fail(PS_EINVAL, "visibility_check_views > 64");
-      // full overlap lists of the fused views (the candidate order of the filter)
-      std::vector<int> ovoff(s->nv + 1, 0), ovlist;
-      for (int v = 0; v < s->nv; ++v) {
-        ovoff[v] = (int)ovlist.size();
-        if (!used[v]) continue;
-        for (uint32_t j = 0; j < cams[v].num_overlap; ++j) ovlist.push_back((int)cams[v].overlap[j]);
-      }
-      ovoff[s->nv] = (int)ovlist.size();
-      std::vector<unsigned char> used8(used.begin(), used.end());
-      int* dovoff = dalloc<int>(s, ovoff.size());
-      int* dovlist = dalloc<int>(s, std::max<size_t>(ovlist.size(), 1));
-      unsigned char* dused = dalloc<unsigned char>(s, std::max(s->nv, 1));
-      unsigned long long* drem = dalloc<unsigned long long>(s, 2);
-      fc.keep = dalloc<unsigned char>(s, fc.count);
-      cuda_ok(cudaMemcpyAsync(dovoff, ovoff.data(), ovoff.size() * sizeof(int), cudaMemcpyHostToDevice, s->st), "upload");
-      if (!ovlist.empty())
-        cuda_ok(cudaMemcpyAsync(dovlist, ovlist.data(), ovlist.size() * sizeof(int), cudaMemcpyHostToDevice, s->st),
-                "upload");
-      cuda_ok(cudaMemcpyAsync(dused, used8.data(), used8.size(), cudaMemcpyHostToDevice, s->st), "upload");
-      cuda_ok(cudaMemsetAsync(drem, 0, 2 * sizeof(unsigned long long), s->st), "memset");
-      ps_post::VisArgs V;
-      memset(&V, 0, sizeof V);
-      V.views = fc.views;
-      V.plane = sl.aux;
-      V.used = dused;
-      V.ovoff = dovoff;
-      V.ovlist = dovlist;
-      V.nviews = s->nv;
-      V.pos = fc.pos;
-      V.nvis = fc.nvis;
-      V.vis = fc.vis;
-      V.vis_stride = fc.vis_stride;
-      V.n = fc.count;
-      V.n1 = fc.count1;
-      V.limit = (int)p->visibility_check_views;
-      V.min_violations = (int)p->visibility_min_violations;
-      V.tau = p->visibility_tau;
-      V.keep = fc.keep;
-      V.removed = drem;
-      launched(s, ps_post::launch_visibility(V, s->st), "visibility kernel");
-      unsigned long long rem[2] = {0, 0};
-      cuda_ok(cudaMemcpyAsync(rem, drem, sizeof rem, cudaMemcpyDeviceToHost, s->st), "read counts");
-      sync(s);
-      fc.removed1 = rem[0];
-      fc.removed2 = rem[1];
-      dfree(s, dovoff);
-      dfree(s, dovlist);
-      dfree(s, dused);
-      dfree(s, drem);
-    }
-    // smooth_along_normals (crates/dense/src/smooth.rs:143-220) of the kept points, as densify.rs:552-556 runs it
-    const bool smooth_on = p->smooth_iterations > 0 && p->smooth_radius_gsd > 0.0 && p->smooth_sigma_range_gsd > 0.0;
-    if (smooth_on && fc.count > 0) {
-      const double gsd = fused_gsd();
-      if (gsd > 0.0) {
-        ps_post::SmoothArgs M;
-        memset(&M, 0, sizeof M);
-        M.r = p->smooth_radius_gsd * gsd;
-        M.r2 = M.r * M.r;
-        M.inv_2ss = 1.0 / (2.0 * ((0.5 * M.r) * (0.5 * M.r)));
-        const double sr = p->smooth_sigma_range_gsd * gsd;
-        M.inv_2sr = 1.0 / (2.0 * (sr * sr));
-        M.cos_n = std::cos(ps_to_radians_f64(p->smooth_normal_deg));
-        M.n = fc.count;
-        M.n1 = fc.count1;
-        M.nrm = fc.nrm;
-        M.keep = fc.keep;
-        M.key = fc.key;
-        unsigned cap = 1024;
-        while (cap < 2ull * fc.count) cap <<= 1;
-        M.cap = cap;
-        M.hkeys = dalloc<unsigned long long>(s, cap);
-        M.hcnt = dalloc<unsigned>(s, cap);
-        M.hstart = dalloc<unsigned>(s, cap);
-        M.hcur = dalloc<unsigned>(s, cap);
-        M.list = dalloc<unsigned>(s, fc.count);
-        M.pslot = dalloc<unsigned>(s, fc.count);
-        M.total = dalloc<unsigned>(s, 1);
-        M.flag = dalloc<int>(s, 1);
-        float* pos2 = dalloc<float>(s, 3 * fc.count);
-        cuda_ok(cudaMemcpyAsync(pos2, fc.pos, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
-        cuda_ok(cudaMemsetAsync(M.flag, 0, sizeof(int), s->st), "memset");
-        float* cur = fc.pos;
-        float* nxt = pos2;
-        for (uint32_t it = 0; it < p->smooth_iterations; ++it) {
-          cuda_ok(cudaMemsetAsync(M.hkeys, 0, cap * sizeof(unsigned long long), s->st), "memset");
-          cuda_ok(cudaMemsetAsync(M.hcnt, 0, cap * sizeof(unsigned), s->st), "memset");
-          cuda_ok(cudaMemsetAsync(M.hcur, 0, cap * sizeof(unsigned), s->st), "memset");
-          cuda_ok(cudaMemsetAsync(M.total, 0, sizeof(unsigned), s->st), "memset");
-          M.pos = cur;
-          M.pos2 = nxt;
-          cuda_ok(ps_post::launch_smooth_pass(M, s->st), "smoothing kernels");
-          s->launches += 5;
-          std::swap(cur, nxt);
-        }
-        if (cur != fc.pos)
-          cuda_ok(cudaMemcpyAsync(fc.pos, cur, 12 * fc.count, cudaMemcpyDeviceToDevice, s->st), "copy");
-        int flag = 0;
-        cuda_ok(cudaMemcpyAsync(&flag, M.flag, sizeof flag, cudaMemcpyDeviceToHost, s->st), "read flag");
-        sync(s);
-        for (void* q : {(void*)M.hkeys, (void*)M.hcnt, (void*)M.hstart, (void*)M.hcur, (void*)M.list, (void*)M.pslot,
-                        (void*)M.total, (void*)M.flag, (void*)pos2})
-          dfree(s, q);
-        if (flag) fail(PS_EINVAL, "smoothing: a point lies more than 2^20 smoothing radii from the origin");
-      }
-    }
+    fused_visibility(s, sl, fc, cams, used, p, false);
+    fused_smoothing(s, sl, fc, order, cams, l, p);
     if (num_points) *num_points = fc.count - fc.removed1 - fc.removed2;
     if (num_residual) *num_residual = fc.count - fc.count1 - fc.removed2;
   });
@@ -2314,9 +2329,10 @@ void ps_score_fusion_params_default(ps_score_fusion_params* out) {
 
 // fuse_scored (crates/dense/src/fusion_score.rs:314-435): candidates per view (one launch per fused view, in index
 // order), then with mark_used the adoption rounds until no candidate is undecided (the host reads the undecided count
-// every few rounds; a round adopts at least the highest-priority undecided candidate, so rounds <= candidates).
+// every few rounds; a round adopts at least the highest-priority undecided candidate, so rounds <= candidates); then
+// the visibility filter and the smoothing of `post` on the adopted points.
 int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
-                            const ps_score_fusion_params* p, uint64_t* num_points) {
+                            const ps_score_fusion_params* p, const ps_fusion_params* post, uint64_t* num_points) {
   return guard(s, [&] {
     if (!p || (n && !cams)) fail(PS_EINVAL, "params or cams is NULL");
     check_views(s, views, n);
@@ -2460,7 +2476,11 @@ int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views
     dfree(s, A.npix);
     fc.count = fc.count1 = cand;
     fc.rejected = cand - adopted;
-    if (num_points) *num_points = adopted;
+    if (post) {  // fuse_depth_maps_with (crates/dense/src/densify.rs:535-556): on the adopted points
+      fused_visibility(s, sl, fc, cams, used, post, true);
+      fused_smoothing(s, sl, fc, order, cams, l, post);
+    }
+    if (num_points) *num_points = adopted - fc.removed1;
   });
 }
 

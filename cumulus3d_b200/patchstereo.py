@@ -421,17 +421,22 @@ class PatchMatchSession:
         self.fused_visibility_removed = int(vr.value)
         return int(n.value)
 
-    def fuse_scored_resident(self, level: int, views: Sequence[int], cams, params=None) -> int:
+    def fuse_scored_resident(self, level: int, views: Sequence[int], cams, params=None, post=None) -> int:
         """Score fusion (fuse_scored, crates/dense/src/fusion_score.rs:314-435) of the readout planes of `views`;
-        `cams` is a fusion.FusionCams of every view.  fused_points() then gives the points in (view, pixel) order."""
+        `cams` is a fusion.FusionCams of every view.  `post` (a FusionParams) adds its visibility filter and smoothing
+        after the fusion, as fuse_depth_maps_with does.  fused_points() then gives the points in (view, pixel)
+        order."""
         from .fusion import default_score_fusion
         p = params if params is not None else default_score_fusion()
         n = C.c_uint64()
         self._check(self.lib.ps_fuse_scored_resident(self.h, level, _views(views), len(views), cams.table,
-                                                     C.byref(p), C.byref(n)))
+                                                     C.byref(p), None if post is None else C.byref(post),
+                                                     C.byref(n)))
         self._fused = (int(n.value), int(p.num_neighbors) + 1)
         self.fused_residual = 0
-        self.fused_visibility_removed = 0
+        vr = C.c_uint64()
+        self._check(self.lib.ps_fused_visibility_removed(self.h, C.byref(vr)))
+        self.fused_visibility_removed = int(vr.value)
         return int(n.value)
 
     def fused_points(self):

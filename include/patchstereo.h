@@ -508,9 +508,11 @@ typedef struct ps_score_fusion_params {
 void ps_score_fusion_params_default(ps_score_fusion_params* out);
 /* Score fusion of the readout planes and final costs of `views` at `level` (cams as for ps_fuse_resident); the
  * cloud replaces the session's fused cloud (ps_fused_points reads it, in the reference's order: view index, then
- * pixel).  num_points: the adopted points. */
+ * pixel).  `post` (nullable; only its visibility_* and smooth_* fields are read) adds the visibility filter and the
+ * smoothing after the fusion, as fuse_depth_maps_with does (crates/dense/src/densify.rs:535-556).  num_points: the
+ * adopted points the visibility filter kept. */
 int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views, size_t n, const ps_fusion_view* cams,
-                            const ps_score_fusion_params* p, uint64_t* num_points);
+                            const ps_score_fusion_params* p, const ps_fusion_params* post, uint64_t* num_points);
 /* The fused points in the reference's order: after ps_fuse_resident the first pass in ascending point key
  * (image_id << 32) | (row << 16) | col, then the second-pass points in ascending key; after ps_fuse_scored_resident
  * (view index, pixel) order.  Positions and normals 3 floats, colours 3 bytes, keys, the number of contributing views

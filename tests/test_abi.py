@@ -101,7 +101,7 @@ def test_null_arguments_rejected_without_device():
     # post-processing and fusion entry points
     assert lib.ps_postprocess_resident(None, 0, None, 0, None, None, None, None) == _lib.PS_EINVAL
     assert lib.ps_fuse_resident(None, 0, None, 0, None, None, None, None) == _lib.PS_EINVAL
-    assert lib.ps_fuse_scored_resident(None, 0, None, 0, None, None, None) == _lib.PS_EINVAL
+    assert lib.ps_fuse_scored_resident(None, 0, None, 0, None, None, None, None) == _lib.PS_EINVAL
     assert lib.ps_fused_points(None, 0, None, None, None, None, None, None, 0) == _lib.PS_EINVAL
     assert lib.ps_fused_visibility_removed(None, None) == _lib.PS_EINVAL
     lib.ps_score_fusion_params_default(None)  # NULL is ignored, as by the other *_default functions

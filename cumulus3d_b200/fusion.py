@@ -154,3 +154,18 @@ def write_ply(path, positions: np.ndarray, normals: Optional[np.ndarray] = None,
                                     None if nrm is None else nrm.ctypes.data, None if col is None else col.ctypes.data)
     if rc != _lib.PS_OK:
         raise _lib.PsError(rc, f"ps_write_ply({path}) failed")
+
+
+def fuse_depth_maps_with(session, level: int, views: Sequence[int], cams: FusionCams,
+                         params: Optional[_lib.FusionParams] = None,
+                         score: Optional[_lib.ScoreFusionParams] = None) -> FusedCloud:
+    """fuse_depth_maps_with (crates/dense/src/densify.rs:505-556) on a session's resident readout planes: score fusion
+    when `score` is given, else consistency fusion with `params`; the visibility filter and the smoothing of `params`
+    follow either one.  `cams` carries the overlap lists (PairStats::select(v, lim, 0.0) in the reference, lim =
+    score.num_neighbors or params.consistency_num_images)."""
+    p = params if params is not None else default_fusion()
+    if score is not None:
+        session.fuse_scored_resident(level, views, cams, score, post=p)
+    else:
+        session.fuse_resident(level, views, cams, p)
+    return session.fused_points()

@@ -472,3 +472,25 @@ def test_visibility_removes_floaters_and_keeps_surface(gt_scene):
     keep = oracle.filter_visibility(fc, depth, range(len(depth)), pts, vis, p.visibility_check_views,
                                     p.visibility_min_violations, p.visibility_tau)
     assert keep.all()
+
+
+def test_fuse_depth_maps_with_dispatch():
+    """fusion.fuse_depth_maps_with picks the fusion as the reference's does (score options present: score fusion with
+    the fusion parameters' visibility and smoothing after it; otherwise consistency fusion)."""
+    calls = []
+
+    class Session:
+        def fuse_resident(self, level, views, cams, p):
+            calls.append(("consistency", level, list(views), p.min_consistent_views))
+
+        def fuse_scored_resident(self, level, views, cams, s, post=None):
+            calls.append(("score", level, list(views), s.tau, post.smooth_iterations))
+
+        def fused_points(self):
+            return "cloud"
+
+    prm = fusion.default_fusion(4)
+    prm.smooth_iterations = 2
+    assert fusion.fuse_depth_maps_with(Session(), 1, [0, 2], None, prm) == "cloud"
+    assert fusion.fuse_depth_maps_with(Session(), 0, [1], None, prm, fusion.default_score_fusion(tau=3.0)) == "cloud"
+    assert calls == [("consistency", 1, [0, 2], 4), ("score", 0, [1], 3.0, 2)]

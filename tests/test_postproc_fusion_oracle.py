@@ -535,3 +535,113 @@ def test_smoothing_equals_direct_restatement():
     np.testing.assert_allclose(got, cur, rtol=0, atol=2e-6)
     assert np.abs(got - pos).max() > 1e-3  # it moved
     np.testing.assert_array_equal(got[::50], pos[::50])
+
+
+def _consistency_point_py(fc, depth, normal, cost, imgs, p, v, row, col):
+    """ConsCtx::evaluate (crates/dense/src/fusion.rs:390-459) for one pixel in Python floats: None or (position,
+    normal, colour, sorted views), under FusionParams p (the first consistency_num_images used partners)."""
+    import math
+    T = fc.table
+    R = lambda c: [list(T[c].r[3 * i:3 * i + 3]) for i in range(3)]
+
+    def project(c, x):
+        r, t, k = R(c), list(T[c].t), list(T[c].k)
+        cz = r[2][0] * x[0] + r[2][1] * x[1] + r[2][2] * x[2] + t[2]
+        if cz <= 0.0:
+            return None
+        cx = r[0][0] * x[0] + r[0][1] * x[1] + r[0][2] * x[2] + t[0]
+        cy = r[1][0] * x[0] + r[1][1] * x[1] + r[1][2] * x[2] + t[1]
+        return k[0] * cx / cz + k[2], k[1] * cy / cz + k[3], cz
+
+    def world(c, q):
+        r = R(c)
+        return [r[0][i] * q[0] + r[1][i] * q[1] + r[2][i] * q[2] for i in range(3)]
+
+    def backproject(c, cl, rw, d):
+        k, t = list(T[c].k), list(T[c].t)
+        cc = [(cl - k[2]) / k[0] * d, (rw - k[3]) / k[1] * d, d]
+        return world(c, [cc[0] - t[0], cc[1] - t[1], cc[2] - t[2]])
+
+    def inv_var(c, y, x, d):
+        if not p.inverse_variance or not T[c].baseline > 0.0:
+            return 1.0
+        spx = p.sigma_px0 + p.sigma_px_slope * float(min(max(cost[c][y, x], np.float32(0)), np.float32(2)))
+        sd = d * d * spx / (T[c].k[0] * T[c].baseline)
+        return 1.0 / max(sd * sd, 1e-300)
+
+    def gray(c, x, y):
+        return float(np.rint(np.float32(imgs[c][y, x]) * np.float32(255.0)))
+
+    d = float(depth[v][row, col])
+    x = backproject(v, float(col), float(row), d)
+    nw = world(v, [float(q) for q in normal[v][row, col]])
+    w0 = inv_var(v, row, col, d)
+    sw, sx, sn, sc = w0, [a * w0 for a in x], [a * w0 for a in nw], [gray(v, col, row) * w0] * 3
+    views = {v}
+    hits = 0
+    cos_n = math.cos(math.radians(p.max_normal_error_deg))
+    for o in [o for o in fc.overlap[v] if o != v][:p.consistency_num_images]:
+        pr = project(o, x)
+        if pr is None:
+            continue
+        cu, rv = math.floor(pr[0] + 0.5), math.floor(pr[1] + 0.5)
+        h, w = depth[o].shape
+        if cu < 0 or rv < 0 or cu >= w or rv >= h:
+            continue
+        od = float(depth[o][rv, cu])
+        if od <= 0.0 or abs(pr[2] - od) / od > p.max_depth_error:
+            continue
+        xo = backproject(o, float(cu), float(rv), od)
+        bp = project(v, xo)
+        if bp is None or (bp[0] - col) ** 2 + (bp[1] - row) ** 2 > p.max_reproj_error ** 2:
+            continue
+        no = world(o, [float(q) for q in normal[o][rv, cu]])
+        if no[0] * nw[0] + no[1] * nw[1] + no[2] * nw[2] < cos_n:
+            continue
+        wo = inv_var(o, rv, cu, od)
+        co = gray(o, cu, rv)
+        sw += wo
+        for k in range(3):
+            sx[k] += wo * xo[k]
+            sn[k] += wo * no[k]
+            sc[k] += wo * co
+        views.add(o)
+        hits += 1
+    ln = math.sqrt(sn[0] ** 2 + sn[1] ** 2 + sn[2] ** 2)
+    if hits < p.min_consistent_views or ln < 1.1920928955078125e-07:
+        return None
+    return [a / sw for a in sx], [a / ln for a in sn], [math.floor(a / sw + 0.5) for a in sc], sorted(views)
+
+
+def test_consistency_points_equal_independent_restatement(gt_scene):
+    """Without marks every pixel is fused on its own: a sample of pixels of every view restated in Python, with
+    noisy depths, varying costs (inverse-variance weights) and the default tolerances."""
+    wl, fc = gt_scene
+    rng = np.random.default_rng(21)
+    depth = [(g * (1.0 + rng.normal(0, 0.003, g.shape))).astype(np.float32) for g in wl.gt_depth]
+    normal = [g.astype(np.float32) for g in wl.gt_normal]
+    cost = [rng.uniform(0.0, 1.2, g.shape).astype(np.float32) for g in depth]
+    imgs = list(wl.images)
+    p = fusion.default_fusion(2)
+    p.mark_used = 0
+    cl = oracle.fuse(fc, depth, normal, cost, imgs, range(len(depth)), p)
+    by_key = {int(k): i for i, k in enumerate(cl.keys)}
+    checked = found = 0
+    for v in range(len(depth)):
+        h, w = depth[v].shape
+        for pix in range(v, h * w, 41):
+            row, col = divmod(pix, w)
+            if not depth[v][row, col] > 0:
+                continue
+            want = _consistency_point_py(fc, depth, normal, cost, imgs, p, v, row, col)
+            got = by_key.get((v << 32) | (row << 16) | col)
+            assert (got is None) == (want is None), (v, row, col)
+            checked += 1
+            if want is None:
+                continue
+            found += 1
+            np.testing.assert_allclose(cl.positions[got], want[0], rtol=1e-6, atol=1e-6)
+            np.testing.assert_allclose(cl.normals[got], want[1], rtol=1e-5, atol=1e-6)
+            assert np.all(np.abs(cl.colors[got].astype(int) - np.array(want[2], int)) <= 1)
+            assert cl.visibility(got) == want[3]
+    assert checked > 2000 and found > 500

@@ -381,3 +381,28 @@ def test_visibility_and_smoothing_after_score_fusion(scene):
                                 post.smooth_normal_deg)
     np.testing.assert_array_equal(both.positions, smoothed)
     assert not np.array_equal(smoothed, plain.positions[keep])
+
+
+def test_views_of_different_sizes():
+    """Views of two sizes over one terrain (the reference fuses any mix of view sizes): both fusions keep every key
+    inside its own view and put the points of true maps on the surface."""
+    a = scenes.formation(96, 72, 1, prefix="a")
+    b = scenes.formation(128, 96, 1, prefix="b", y0=2.0)
+    cams = a + b
+    ext = scenes._extent(cams)
+    ia, da, na = scenes.render(a, 4, extent=ext)
+    ib, db, nb = scenes.render(b, 4, extent=ext)
+    imgs, depth, normal = list(ia) + list(ib), list(da) + list(db), list(na) + list(nb)
+    fc = fusion.FusionCams(cams, [[j for j in range(len(cams)) if j != i][:3] for i in range(len(cams))])
+    cost = [np.zeros(d.shape, np.float32) for d in depth]
+    wl = type("W", (), {"cams": cams, "gt_depth": depth})
+    for cl in (oracle.fuse(fc, depth, normal, cost, imgs, range(len(cams)), fusion.default_fusion(2)),
+               oracle.fuse_scored(fc, depth, normal, cost, imgs, range(len(cams)),
+                                  fusion.default_score_fusion(inverse_variance=0))):
+        assert len(cl) > 2000
+        keys = cl.keys.astype(np.int64)
+        v, row, col = keys >> 32, (keys >> 16) & 0xFFFF, keys & 0xFFFF
+        assert ((row < np.array([d.shape[0] for d in depth])[v]) & (col < np.array([d.shape[1] for d in depth])[v])).all()
+        assert set(v.tolist()) == set(range(len(cams)))
+        err = _ref_error(wl, cl)
+        assert np.median(err) < 0.002 and np.quantile(err, 0.99) < 0.01

@@ -6,8 +6,10 @@ All variants of the half-step kernel produce the same bits, so the choice only a
 * window-weight cache: on or off;
 * source sampling: loads from the bordered plane, or a texture gather.
 
-The tuner times each candidate on a prefix of the caller's own views (a photometric run of one red-black iteration,
-kernel time from the session's CUDA events) and returns the fastest tuning word.  Results are cached in a JSON file
+The tuner times each candidate on a prefix of the caller's own views and returns the fastest tuning word: a
+photometric run of two red-black iterations from random init brings the planes near convergence (the state most
+half steps of a schedule see, and the one the staged source boxes are built for), then one more iteration continuing
+from it is timed (kernel time from the session's CUDA events).  Results are cached in a JSON file
 keyed by (GPU name, window radius, window step, math mode, image size class).
 """
 from __future__ import annotations
@@ -20,7 +22,7 @@ from typing import Dict, Optional, Sequence
 from . import _lib
 from .patchstereo import KernelInput, PatchMatchBackend, RunParams
 
-CANDIDATES = (0, 2, 3, 4, 6, 7)  # see PS_TUNE_* in include/patchstereo.h
+CANDIDATES = (0, 2, 3, 4, 6, 7, 8, 10, 16, 18)  # see PS_TUNE_* in include/patchstereo.h
 DEFAULT_CACHE = pathlib.Path(os.environ.get("PS_AUTOTUNE_CACHE",
                                             pathlib.Path(__file__).resolve().parent / "_autotune_cache.json"))
 
@@ -56,12 +58,12 @@ def tune(inp: KernelInput, device: int = 0, math: str = "parity", views: Optiona
     for t in candidates:
         be = PatchMatchBackend(device, math=math, tuning=t)
         with be.begin(inp) as s:
-            p = RunParams(inp.num_levels - 1, False, True, 1, 1)
-            s.run_resident(vs, p)  # warm-up (module load, texture setup)
+            lvl = inp.num_levels - 1
+            s.run_resident(vs, RunParams(lvl, False, True, 2, 1))  # warm-up (module load, textures), converging
             s.synchronize()
             s.set_profiling(True)
             s.reset_stats()
-            s.run_resident(vs, p)
+            s.run_resident(vs, RunParams(lvl, False, False, 1, 2))
             times[t] = s.kernel_stats(_lib.PS_KERNEL_HALF)["ms"]
         be.close()
     best = min(times, key=times.get)

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "ps_fmath.h"
+#include "ps_pairs.h"
 #include "ps_types.h"
 
 #ifndef PS_FAST
@@ -159,12 +160,18 @@ struct RefStats {
 // (a = 0, 2, …) and odd rows (a = 1, 3, …) accumulate separately, in ascending row order, and the NCC uses
 // even + odd.  With G = 2 lanes per pixel, lane g sums the rows of parity g and the two partial sums meet through
 // one shuffle (pmask = the pair's lanes); with G = 1 one thread keeps both partial sums.
+//
+// Weight-cache layouts: per tap (a, b) one float per thread, stride NT between taps.  The legacy layout keeps row a at
+// wc + a·wn·NT.  The row-pair layout (PW) used by the f32x2 tap loops puts the weights of rows 2p and 2p+1 of the
+// same column next to each other (one 8-byte load per tap pair): wc + (p·wn + b)·2·NT + (a & 1) with wc = base +
+// 2·thread, and the last row of an odd window at wl + b·NT.
 struct RefWin {
   const float* t;
   int tw;
   float* wc;
   int g;
   unsigned pmask;
+  float* wl;
 };
 
 // Row-parity partial sums -> total (even + odd; IEEE addition is commutative, so both lanes get the same bits).
@@ -179,7 +186,7 @@ __device__ __forceinline__ float pair_total(const RefWin& rw, const float* part)
 }
 
 // ref_stats (patchmatch.cu:199-223).  Weights w_k = exp(-(dx²+dy²)/(2σs²) - (Ic-Ik)²/(2σc²)); 0 outside the image.
-template <int WR, int WS, bool CW, int NT, int G = 1>
+template <int WR, int WS, bool CW, int NT, int G = 1, bool PW = false>
 __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) {
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
@@ -191,13 +198,24 @@ __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) 
     const int dy = -wr + a * ws;
     const int pa = G == 2 ? 0 : (a & 1);
     const float* trow = rw.t + dy * rw.tw;
-    float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+    float* wrow;
+    int wst = NT;
+    if constexpr (PW) {
+      if (a < (wn & ~1)) {
+        wrow = rw.wc + (a >> 1) * wn * NT * 2 + (a & 1);
+        wst = 2 * NT;
+      } else {
+        wrow = rw.wl;
+      }
+    } else {
+      wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+    }
     auto tap = [&](int b) {
       const int dx = -wr + b * ws;
       float ik = trow[dx];
       float d = s.ic - ik;
       float w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
-      if (CW) wrow[b * NT] = w;
+      if (CW) wrow[b * wst] = w;
       float wi = w * ik;
       W[pa] = W[pa] + w;
       S[pa] = S[pa] + wi;
@@ -277,7 +295,7 @@ __device__ __forceinline__ float ncc_finish(const RefStats& rs, float Sst, float
 // a correctly rounded function of an affine expression, and rounding is monotone), so the smallest zz of the window
 // is at one of its four corner taps.  When all four are in front, every tap is, and the taps run without the
 // per-tap test and selects; otherwise a guarded loop handles each tap (the same bits either way).
-template <int WR, int WS, bool CW, int NT, bool TEX, int G>
+template <int WR, int WS, bool CW, int NT, bool TEX, int G, bool PW = false>
 __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
                                             const float* H, int x, int y) {
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
@@ -302,9 +320,15 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
     SSs[pa] = fmaf(wsv, sv, SSs[pa]);
     IS[pa] = fmaf(wsv, ik, IS[pa]);
   };
-  auto weight = [&](const float* wrow, int b, int dx, int dy, float ik) {
+  // weights of row a start at wrow(a), stride wst(a) between taps (legacy or row-pair cache layout)
+  auto wrow_of = [&](int a) -> const float* {
+    if constexpr (PW) return a < (wn & ~1) ? rw.wc + (a >> 1) * wn * NT * 2 + (a & 1) : rw.wl;
+    else return rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+  };
+  auto wst_of = [&](int a) { return (PW && a < (wn & ~1)) ? 2 * NT : NT; };
+  auto weight = [&](const float* wrow, int wst, int b, int dx, int dy, float ik) {
     if constexpr (CW) {
-      return wrow[b * NT];
+      return wrow[b * wst];
     } else {
       const float d = rs.ic - ik;
       return m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
@@ -320,12 +344,13 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
       const float ry = fmaf(H[4], sy, H[5]);
       const float rz = fmaf(H[7], sy, H[8]);
       const float* trow = rw.t + dy * rw.tw;
-      const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+      const float* wrow = wrow_of(a);
+      const int wst = wst_of(a);
       auto tap = [&](int b) {
         const int dx = -wr + b * ws;
         const float sx = fx + (float)dx;
         const float ik = trow[dx];
-        const float w = weight(wrow, b, dx, dy, ik);
+        const float w = weight(wrow, wst, b, dx, dy, ik);
         const float izz = m_rcp(fmaf(H[6], sx, rz));
         accumulate(pa, w, sample(fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz), ik);
       };
@@ -347,13 +372,14 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
       const float ry = fmaf(H[4], sy, H[5]);
       const float rz = fmaf(H[7], sy, H[8]);
       const float* trow = rw.t + dy * rw.tw;
-      const float* wrow = rw.wc + (G == 2 ? (a >> 1) : a) * wn * NT;
+      const float* wrow = wrow_of(a);
+      const int wst = wst_of(a);
 #pragma unroll 1
       for (int b = 0; b < wn; ++b) {
         const int dx = -wr + b * ws;
         const float sx = fx + (float)dx;
         const float ik = trow[dx];
-        const float w = weight(wrow, b, dx, dy, ik);
+        const float w = weight(wrow, wst, b, dx, dy, ik);
         // the reciprocal is replaced by 0 behind the camera so the discarded fetch coordinates stay finite
         const float zz = fmaf(H[6], sx, rz);
         const bool front = zz > 1e-8f;
@@ -372,6 +398,272 @@ __device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, cons
   if (!ncc_begin(rs, S, H, (float)x, (float)y)) return 2.0f;
   nwin++;
   return ncc_window<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y);
+}
+
+// ================================================================================ row-pair tap loops (f32x2)
+// The window sums with rows 2p (even) and 2p+1 (odd) in the two halves of f32x2 pairs.  The even-row and odd-row
+// partial sums of the parity contract advance in exactly the order of ncc_window, so the bits are the same, and each
+// pair operation takes one issue slot for two taps.  Sources are sampled by plane loads, a texture gather, or the
+// warp's staged source box (shared memory).
+enum { SMP_LOAD = 0, SMP_TEX = 1, SMP_BOX = 2 };
+
+// The warp's staged box: box[r·PS_BOX_P + c] holds texel (gx0 + c, gy0 + r) of the source (0 outside the image);
+// mx = 1.5·2^23 - gx0 and my = 1.5·2^23 - gy0.
+struct BoxRef {
+  const float* box;
+  float mx, my;
+};
+
+// Reciprocal of a pair given nz = -z: m_rcp lane by lane (rcp.approx, then the FMA correction as pair operations).
+__device__ __forceinline__ float2 m_rcp2(float2 nz) {
+  float2 r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.x) : "f"(-nz.x));
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r.y) : "f"(-nz.y));
+#if PS_FAST
+  return r;
+#else
+  return v_fma(r, v_fma(nz, r, v_splat(1.0f)), r);
+#endif
+}
+
+// Bilinear samples of a pair of taps: the arithmetic of src_sample lane by lane, with the footprint from the plane,
+// the texture or the box.  Box addressing: F = (u + mx) rounded toward -inf is floor(u) - gx0 + 1.5·2^23 exactly (u
+// lies within the box, |gx0| < 2^15), so floor(u) = F - mx exactly and the bits of F are bits(1.5·2^23) + the box
+// column; the box offset is therefore bits(Fv)·P + bits(Fu) - (P + 1)·bits(1.5·2^23), taken mod 2^32.
+constexpr unsigned kBoxBias = 0u - (unsigned)(PS_BOX_P + 1) * 0x4B400000u;
+
+template <int SMP>
+__device__ __forceinline__ float2 sample_pair(const PsLevel& S, const BoxRef& bx, float2 u, float2 v) {
+  float2 ax, ay, p00, p10, p01, p11;
+  if constexpr (SMP == SMP_BOX) {
+    const float2 mx = v_splat(bx.mx), my = v_splat(bx.my);
+    const float2 fu = v_add_rm(u, mx), fv = v_add_rm(v, my);
+    ax = v_sub(u, v_sub(fu, mx));
+    ay = v_sub(v, v_sub(fv, my));
+    const float* qa = bx.box + ((unsigned)__float_as_int(fv.x) * PS_BOX_P + (unsigned)__float_as_int(fu.x) + kBoxBias);
+    const float* qb = bx.box + ((unsigned)__float_as_int(fv.y) * PS_BOX_P + (unsigned)__float_as_int(fu.y) + kBoxBias);
+    p00 = make_float2(qa[0], qb[0]);
+    p10 = make_float2(qa[1], qb[1]);
+    p01 = make_float2(qa[PS_BOX_P], qb[PS_BOX_P]);
+    p11 = make_float2(qa[PS_BOX_P + 1], qb[PS_BOX_P + 1]);
+  } else {
+    const float2 xf = make_float2(floorf(u.x), floorf(u.y)), yf = make_float2(floorf(v.x), floorf(v.y));
+    ax = v_sub(u, xf);
+    ay = v_sub(v, yf);
+    if constexpr (SMP == SMP_TEX) {
+      const float4 qa = gather_red_offset11(S.tex, xf.x, yf.x), qb = gather_red_offset11(S.tex, xf.y, yf.y);
+      p00 = make_float2(qa.w, qb.w);
+      p10 = make_float2(qa.z, qb.z);
+      p01 = make_float2(qa.x, qb.x);
+      p11 = make_float2(qa.y, qb.y);
+    } else {
+      const float wf = (float)S.w, hf = (float)S.h;
+      const float* pa = S.img + f2i_exact(fminf(fmaxf(yf.x, -2.0f), hf)) * S.pitch + f2i_exact(fminf(fmaxf(xf.x, -2.0f), wf));
+      const float* pb = S.img + f2i_exact(fminf(fmaxf(yf.y, -2.0f), hf)) * S.pitch + f2i_exact(fminf(fmaxf(xf.y, -2.0f), wf));
+      p00 = make_float2(__ldg(pa), __ldg(pb));
+      p10 = make_float2(__ldg(pa + 1), __ldg(pb + 1));
+      p01 = make_float2(__ldg(pa + S.pitch), __ldg(pb + S.pitch));
+      p11 = make_float2(__ldg(pa + S.pitch + 1), __ldg(pb + S.pitch + 1));
+    }
+  }
+  const float2 top = v_fma(ax, v_sub(p10, p00), p00);
+  const float2 bot = v_fma(ax, v_sub(p11, p01), p01);
+  return v_fma(ay, v_sub(bot, top), top);
+}
+
+template <int SMP>
+__device__ __forceinline__ float sample_one(const PsLevel& S, const BoxRef& bx, float u, float v) {
+  if constexpr (SMP == SMP_BOX) {
+    const float fu = __fadd_rd(u, bx.mx), fv = __fadd_rd(v, bx.my);
+    const float ax = u - (fu - bx.mx), ay = v - (fv - bx.my);
+    const float* q = bx.box + ((unsigned)__float_as_int(fv) * PS_BOX_P + (unsigned)__float_as_int(fu) + kBoxBias);
+    const float p00 = q[0], p10 = q[1], p01 = q[PS_BOX_P], p11 = q[PS_BOX_P + 1];
+    const float top = fmaf(ax, p10 - p00, p00);
+    const float bot = fmaf(ax, p11 - p01, p01);
+    return fmaf(ay, bot - top, top);
+  } else if constexpr (SMP == SMP_TEX) {
+    return src_sample_tex(S.tex, u, v);
+  } else {
+    return src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u, v);
+  }
+}
+
+// Window sums of a window whose four corner taps lie in front of the source camera (every tap then does), with the
+// row-pair weight cache.  Rows 2p / 2p+1 go through the pair loop; the last row of an odd window is scalar and adds
+// into the even-row sums, as in ncc_window.
+template <int WR, int WS, int NT, int SMP>
+__device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefStats& rs, const PsLevel& S, const float* H,
+                                                  int x, int y, const BoxRef& bx) {
+  constexpr int wr = WR, ws = WS, wn = (2 * WR) / WS + 1, np = wn / 2;
+  const float fx = (float)x, fy = (float)y;
+  float2 Ss = v_splat(0.f), SSs = v_splat(0.f), IS = v_splat(0.f);
+  const float2 h0 = v_splat(H[0]), h1 = v_splat(H[1]), h2 = v_splat(H[2]), h3 = v_splat(H[3]), h4 = v_splat(H[4]),
+               h5 = v_splat(H[5]), nh6 = v_splat(-H[6]), nh7 = v_splat(-H[7]), nh8 = v_splat(-H[8]);
+#pragma unroll 1
+  for (int p = 0; p < np; ++p) {
+    const int dy = -wr + 2 * p * ws;
+    const float2 sy = make_float2(fy + (float)dy, fy + (float)(dy + ws));
+    const float2 rx = v_fma(h1, sy, h2), ry = v_fma(h4, sy, h5), nrz = v_fma(nh7, sy, nh8);
+    const float* t0 = rw.t + dy * rw.tw;
+    const float* t1 = t0 + ws * rw.tw;
+    const float* wp = rw.wc + p * wn * NT * 2;
+#pragma unroll
+    for (int b = 0; b < wn; ++b) {
+      const int dx = -wr + b * ws;
+      const float2 sx = v_splat(fx + (float)dx);
+      const float2 ik = make_float2(t0[dx], t1[dx]);
+      const float2 w = *reinterpret_cast<const float2*>(wp + b * NT * 2);
+      const float2 izz = m_rcp2(v_fma(nh6, sx, nrz));
+      const float2 sv = sample_pair<SMP>(S, bx, v_mul(v_fma(h0, sx, rx), izz), v_mul(v_fma(h3, sx, ry), izz));
+      const float2 wsv = v_mul(w, sv);
+      Ss = v_add(Ss, wsv);
+      SSs = v_fma(wsv, sv, SSs);
+      IS = v_fma(wsv, ik, IS);
+    }
+  }
+  if constexpr ((wn & 1) != 0) {
+    const int dy = -wr + (wn - 1) * ws;
+    const float sy = fy + (float)dy;
+    const float rx = fmaf(H[1], sy, H[2]), ry = fmaf(H[4], sy, H[5]), rz = fmaf(H[7], sy, H[8]);
+    const float* t0 = rw.t + dy * rw.tw;
+#pragma unroll
+    for (int b = 0; b < wn; ++b) {
+      const int dx = -wr + b * ws;
+      const float sx = fx + (float)dx;
+      const float ik = t0[dx];
+      const float w = rw.wl[b * NT];
+      const float izz = m_rcp(fmaf(H[6], sx, rz));
+      const float sv = sample_one<SMP>(S, bx, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
+      const float wsv = w * sv;
+      Ss.x = Ss.x + wsv;
+      SSs.x = fmaf(wsv, sv, SSs.x);
+      IS.x = fmaf(wsv, ik, IS.x);
+    }
+  }
+  return ncc_finish(rs, Ss.x + Ss.y, SSs.x + SSs.y, IS.x + IS.y);
+}
+
+// Corner test of ncc_window: the four corner taps in front of the source camera.
+template <int WR>
+__device__ __forceinline__ bool window_front(const float* H, float fx, float fy) {
+  const float sx0 = fx + (float)(-WR), sx1 = fx + (float)WR;
+  const float rz0 = fmaf(H[7], fy + (float)(-WR), H[8]), rz1 = fmaf(H[7], fy + (float)WR, H[8]);
+  return fmaf(H[6], sx0, rz0) > 1e-8f && fmaf(H[6], sx1, rz0) > 1e-8f && fmaf(H[6], sx0, rz1) > 1e-8f &&
+         fmaf(H[6], sx1, rz1) > 1e-8f;
+}
+
+// One lane's window with the row-pair loops (the prologue must have passed): pair loop when the window is wholly in
+// front, otherwise the guarded loop of ncc_window on the row-pair cache.
+template <int WR, int WS, int NT, bool TEX>
+__device__ __forceinline__ float ncc_window_lane(const PsRun& P, const RefWin& rw, const RefStats& rs,
+                                                 const PsLevel& S, const float* H, int x, int y) {
+  if (window_front<WR>(H, (float)x, (float)y))
+    return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD>(rw, rs, S, H, x, y, BoxRef{nullptr, 0.f, 0.f});
+  return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
+}
+
+// What the warp's box holds: texels [ox, ox + PS_BOX_P) × [oy, oy + PS_BOX_H) of the plane at src (warp-uniform).
+struct BoxState {
+  const float* src;
+  int ox, oy;
+};
+
+// Warp-collective NCC cost (every lane of the warp calls it; `act` marks the lanes that want this window).
+//
+// The lanes' windows usually overlap in the source (neighbouring pixels, similar planes), so the warp stages the
+// union of their footprints into its shared-memory box once and every tap reads its 2×2 texels from there instead of
+// the texture unit.  Footprint bound: the tap position is a projective function of the tap with a positive
+// denominator over the window, so its exact value lies between the values at the four corner taps.  The computed
+// positions differ from the exact ones by at most 2^-23·(Tu + |u|·Tz)/zmin + 2^-23·|u| (Tu, Tz the sums of the
+// magnitudes of the homography terms at the window's extreme coordinates); with Tu, Tv, (|u|+|v|+1)·Tz ≤ 2^14·zmin
+// and |u|, |v| < 2^14 that is below 2^-7, so the texels [floor(umin - 1/64), floor(umax + 1/64) + 1] of the computed
+// corner positions cover every texel a tap reads.  The box is reused while the requested footprints fit inside it;
+// a restage centres the box on the request and copies it with 16-byte cp.async chunks.  Windows that fail the bound,
+// a request wider than PS_BOX_P - 3 or taller than PS_BOX_H texels, or fewer than PS_STAGE_MIN_LANES active lanes use
+// the per-lane loops.  All paths give the same bits.
+template <int WR, int WS, int NT, bool TEX>
+__device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
+                                               const float* H, int x, int y, bool act, int& nwin, float* box,
+                                               BoxState& bs) {
+  const float fx = (float)x, fy = (float)y;
+  act = act && ncc_begin(rs, S, H, fx, fy);
+  const unsigned am = __ballot_sync(0xffffffffu, act);
+  if (am == 0u) return 2.0f;
+  if (act) nwin++;
+  bool front = false, fits = false;
+  int lx = 0x7fffffff, ly = 0x7fffffff, hx = -0x7fffffff, hy = -0x7fffffff;
+  if (act) {
+    const float sx0 = fx + (float)(-WR), sx1 = fx + (float)WR, sy0 = fy + (float)(-WR), sy1 = fy + (float)WR;
+    const float rz0 = fmaf(H[7], sy0, H[8]), rz1 = fmaf(H[7], sy1, H[8]);
+    const float z00 = fmaf(H[6], sx0, rz0), z10 = fmaf(H[6], sx1, rz0);
+    const float z01 = fmaf(H[6], sx0, rz1), z11 = fmaf(H[6], sx1, rz1);
+    front = z00 > 1e-8f && z10 > 1e-8f && z01 > 1e-8f && z11 > 1e-8f;
+    if (front) {
+      const float rx0 = fmaf(H[1], sy0, H[2]), rx1 = fmaf(H[1], sy1, H[2]);
+      const float ry0 = fmaf(H[4], sy0, H[5]), ry1 = fmaf(H[4], sy1, H[5]);
+      const float i00 = m_rcp(z00), i10 = m_rcp(z10), i01 = m_rcp(z01), i11 = m_rcp(z11);
+      const float u00 = fmaf(H[0], sx0, rx0) * i00, u10 = fmaf(H[0], sx1, rx0) * i10;
+      const float u01 = fmaf(H[0], sx0, rx1) * i01, u11 = fmaf(H[0], sx1, rx1) * i11;
+      const float v00 = fmaf(H[3], sx0, ry0) * i00, v10 = fmaf(H[3], sx1, ry0) * i10;
+      const float v01 = fmaf(H[3], sx0, ry1) * i01, v11 = fmaf(H[3], sx1, ry1) * i11;
+      const float umin = fminf(fminf(u00, u10), fminf(u01, u11)), umax = fmaxf(fmaxf(u00, u10), fmaxf(u01, u11));
+      const float vmin = fminf(fminf(v00, v10), fminf(v01, v11)), vmax = fmaxf(fmaxf(v00, v10), fmaxf(v01, v11));
+      const float zmin = fminf(fminf(z00, z10), fminf(z01, z11));
+      const float mx = fmaxf(fabsf(sx0), fabsf(sx1)), my = fmaxf(fabsf(sy0), fabsf(sy1));
+      const float tu = fabsf(H[0]) * mx + fabsf(H[1]) * my + fabsf(H[2]);
+      const float tv = fabsf(H[3]) * mx + fabsf(H[4]) * my + fabsf(H[5]);
+      const float tz = fabsf(H[6]) * mx + fabsf(H[7]) * my + fabsf(H[8]);
+      const float ua = fmaxf(fabsf(umin), fabsf(umax)), va = fmaxf(fabsf(vmin), fabsf(vmax));
+      const float lim = 16384.0f * zmin;
+      fits = zmin < 1e30f && tu <= lim && tv <= lim && (ua + va + 1.0f) * tz <= lim && ua < 16384.0f && va < 16384.0f;
+      if (fits) {
+        lx = (int)floorf(umin - 0.015625f);
+        hx = (int)floorf(umax + 0.015625f) + 1;
+        ly = (int)floorf(vmin - 0.015625f);
+        hy = (int)floorf(vmax + 0.015625f) + 1;
+      }
+    }
+  }
+  if (__all_sync(0xffffffffu, !act || fits) && __popc(am) >= PS_STAGE_MIN_LANES) {
+    const int gx0 = __reduce_min_sync(0xffffffffu, lx), gx1 = __reduce_max_sync(0xffffffffu, hx);
+    const int gy0 = __reduce_min_sync(0xffffffffu, ly), gy1 = __reduce_max_sync(0xffffffffu, hy);
+    if (gx1 - gx0 + 1 <= PS_BOX_P - 3 && gy1 - gy0 + 1 <= PS_BOX_H) {
+      if (!(S.img == bs.src && gx0 >= bs.ox && gx1 < bs.ox + PS_BOX_P && gy0 >= bs.oy && gy1 < bs.oy + PS_BOX_H)) {
+        // Restage, centred on the request: origin x ≡ 2 (mod 4), so every 16-byte chunk of a plane row is aligned
+        // (rows start 2 floats after a 128-byte boundary); chunks outside the plane's allocated rows are zero-filled,
+        // inside they read the image or its zero border and padding.
+        const int xlo = gx1 - (PS_BOX_P - 1), ylo = gy1 - (PS_BOX_H - 1);
+        int ox = (xlo + gx0) >> 1;
+        ox -= (ox - 2) & 3;
+        if (ox < xlo) ox += 4;
+        const int oy = (ylo + gy0) >> 1;
+        __syncwarp();  // every lane is done with the previous box
+        const int lane = threadIdx.x & 31;
+        const unsigned sbase = (unsigned)__cvta_generic_to_shared(box);
+#pragma unroll 2
+        for (int i = lane; i < PS_BOX_H * (PS_BOX_P / 4); i += 32) {
+          const int r = i / (PS_BOX_P / 4), q = i - r * (PS_BOX_P / 4);
+          const int X = ox + 4 * q, Y = oy + r;
+          const bool in = Y >= -PS_BORDER && Y < S.h + PS_BORDER && X >= -PS_BORDER && X + 4 <= S.pitch - PS_BORDER;
+          const float* src = in ? S.img + (long long)Y * S.pitch + X : S.img - PS_BORDER;  // aligned; 0 bytes read
+          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + 4u * (unsigned)(r * PS_BOX_P + 4 * q)),
+                       "l"(src), "r"(in ? 16 : 0)
+                       : "memory");
+        }
+        asm volatile("cp.async.wait_all;\n" ::: "memory");
+        __syncwarp();
+        bs.src = S.img;
+        bs.ox = ox;
+        bs.oy = oy;
+      }
+      return act ? ncc_window_pairs<WR, WS, NT, SMP_BOX>(
+                       rw, rs, S, H, x, y, BoxRef{box, 12582912.0f - (float)bs.ox, 12582912.0f - (float)bs.oy})
+                 : 2.0f;
+    }
+  }
+  if (!act) return 2.0f;
+  if (front) return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD>(rw, rs, S, H, x, y, BoxRef{nullptr, 0.f, 0.f});
+  return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
 }
 
 // Forward/backward reprojection error through the source snapshot (patchmatch.cu:292-314); INF on failure.
@@ -514,25 +806,38 @@ __device__ __forceinline__ void count_windows(const PsRun& P, int nwin) {
 
 // Half-step tile geometry for G lanes per pixel: G = 1 -> 32 × 8 pixels (a warp = 16 active columns × 2 rows);
 // G = 2 -> 16 × 8 pixels (a warp = 8 active columns × 2 rows × 2 lanes).  The shared tile's row pitch is padded so
-// that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.
+// that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.  The staged mode's
+// warp (8 active columns × 4 rows) needs a pitch ≡ 8 (mod 16): its rows 0 and 2 (and 1 and 3) then fall 16 banks
+// apart, and the checkerboard puts odd rows on the other bank parity.
 __host__ __device__ constexpr int half_pw(int G) { return G == 2 ? PS_HALF2_PW : PS_HALF_PW; }
 __host__ __device__ constexpr int half_tw(int G, int wr) {
   return G == 2 ? (((PS_HALF2_PW + 2 * wr) + 15) / 32) * 32 + 16 : PS_HALF_PW + 2 * wr;
 }
+__host__ __device__ constexpr int half_tw_staged(int wr) { return ((PS_HALF_PW + 2 * wr + 7) / 16) * 16 + 8; }
 
+// Half-step variants (all give the same bits):
+//   MODE 0: one lane (G = 1) or two lanes (G = 2) per pixel, scalar tap loops;
+//   MODE 1: one lane per pixel, row-pair f32x2 tap loops on the row-pair weight cache;
+//   MODE 2: MODE 1 plus the warp-collective staged source boxes (ncc_cost_warp).  No lane leaves early: lanes
+//           outside the image work on a clamped pixel with every window inactive and write nothing, and every loop
+//           that contains a window evaluation runs the same trip count on all lanes.
 // G = 1: two CTAs per SM with the weight cache (~90 KB each for a 13×13 window), four without it.
 // G = 2: the two lanes of a pixel split the window rows, so each thread caches half the weights: four CTAs per SM.
-template <int WR, int WS, bool CW, bool TEX, int G>
+template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
 __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_HALF_NT;
   constexpr int PW = half_pw(G);
+  constexpr bool PAIRW = MODE >= 1;
+  constexpr bool COLL = MODE == 2;
+  static_assert(MODE == 0 || (CW && G == 1 && WR != 0), "row-pair modes need the weight cache, one lane, a fixed window");
   extern __shared__ float sm[];
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
-  const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
+  const int TW = COLL ? half_tw_staged(wr) : half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
   float* tile = sm;
   float* wcache = sm + ((TW * TH + 31) & ~31);
   float* wvs = wcache + (CW ? ((wn + G - 1) / G) * wn * NT : 0);
+  float* boxes = wvs + P.maxsrc * NT;
 
   const int ii = find_item(P, blockIdx.x);
   const PsItem& it = P.items[ii];
@@ -552,17 +857,34 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int gl = G == 2 ? (lane & 1) : 0;
-  const int row = 2 * warp + (lane >> 4), col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
-  const int y = y0 + row;
-  const int x = x0 + 2 * col + ((y + P.color) & 1);
-  if (x >= w || y >= h) return;  // both lanes of a pixel leave together
+  int row, col;
+  if constexpr (COLL) {
+    row = 4 * (warp >> 1) + (lane >> 3);
+    col = 8 * (warp & 1) + (lane & 7);
+  } else {
+    row = 2 * warp + (lane >> 4);
+    col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
+  }
+  int y = y0 + row;
+  int x = x0 + 2 * col + ((y + P.color) & 1);
+  const bool live = x < w && y < h;
+  if constexpr (!COLL) {
+    if (!live) return;  // both lanes of a pixel leave together
+  } else {
+    y = min(y, h - 1);
+    x = min(x, w - 1);
+    row = y - y0;
+  }
+  float* box = boxes + warp * (PS_BOX_P * PS_BOX_H);
+  BoxState bs{nullptr, 0, 0};
 
   RefWin rw;
   rw.t = tile + (row + wr) * TW + (x - x0 + wr);
   rw.tw = TW;
-  rw.wc = wcache + threadIdx.x;
+  rw.wc = wcache + (PAIRW ? 2 * threadIdx.x : threadIdx.x);
   rw.g = gl;
   rw.pmask = G == 2 ? (3u << (lane & ~1)) : 0u;
+  rw.wl = wcache + (wn & ~1) * wn * NT + threadIdx.x;
   float* wv = wvs + threadIdx.x;
 
   const PsView& vd = P.views[it.view];
@@ -609,9 +931,22 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
     }
   }
 
-  // 2. View traversal: voting, weighting, aggregation.
+  // One NCC window of this pixel (the homography H is valid where hok): per lane, or warp-collective in MODE 2.
   int nwin = 0;
-  const RefStats rs = ref_stats<WR, WS, CW, NT, G>(P, rw);
+  const RefStats rs = ref_stats<WR, WS, CW, NT, G, PAIRW>(P, rw);
+  auto window = [&](const PsLevel& S, const float* H, bool hok) -> float {
+    if constexpr (COLL) {
+      return ncc_cost_warp<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y, hok, nwin, box, bs);
+    } else if constexpr (MODE == 1) {
+      if (!hok || !ncc_begin(rs, S, H, (float)x, (float)y)) return 2.0f;
+      nwin++;
+      return ncc_window_lane<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y);
+    } else {
+      return hok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.0f;
+    }
+  };
+
+  // 2. View traversal: voting, weighting, aggregation.
   const int vprev = P.bview[base + pix];
   float num[9], numf[9];
 #pragma unroll
@@ -633,13 +968,18 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[0], H);
       prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
-      if (!(prior > 0.f)) continue;
+    }
+    const bool use = prior > 0.f && live;
+    if constexpr (COLL) {
+      if (!__any_sync(0xffffffffu, use)) continue;
+    } else {
+      if (!use) continue;
     }
 #pragma unroll 1
     for (int i = 0; i < 9; ++i) {
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[i], H);
-      const float mi = ok ? ncc_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, S, H, x, y, nwin) : 2.f;
+      const float mi = window(S, H, ok && use);
       const float gi = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[i].w), P.gmax) : 0.f;
 #pragma unroll
       for (int q = 0; q < 9; ++q)
@@ -648,6 +988,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
           gg[q] = gi;
         }
     }
+    if (!use) continue;
     int good = 0, bad = 0;
     float conf = 0.f;
 #pragma unroll
@@ -732,33 +1073,42 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
       default: return qprior;
     }
   };
+  int ncw = ncand;
+  if constexpr (COLL) ncw = (int)__reduce_max_sync(0xffffffffu, (unsigned)ncand);
 #pragma unroll 1
-  for (int c = 0; c < ncand; ++c) {
+  for (int c = 0; c < ncw; ++c) {
     const float4 cd = candidate(c);
-    float cc;
-    if (den > 0.f) {
-      float nm = 0.f;
+    const bool run = c < ncand && den > 0.f && live;
+    float nm = 0.f;
+    if (!COLL || __any_sync(0xffffffffu, run)) {
 #pragma unroll 1
       for (int j = 0; j < nsrc; ++j) {
         const float wj = wv[j * NT];
-        if (!(wj > 0.f)) continue;
+        const bool aj = run && wj > 0.f;
+        if constexpr (COLL) {
+          if (!__any_sync(0xffffffffu, aj)) continue;
+        } else {
+          if (!aj) continue;
+        }
         const PsPair& pr = prs[j];
         const PsLPair lp = lps[j];
         const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
-        float g = 0.f;
-        const float mm = pair_cost<WR, WS, CW, NT, TEX, G>(P, rw, rs, R, S, pr, lp, x, y, cd, &g, nwin);
-        nm += wj * (mm + P.lambda * g);
+        float H[9];
+        const bool hok = homography(R, lp, (float)x, (float)y, cd, H);
+        const float mm = window(S, H, aj && hok);
+        if (aj) {
+          const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, cd.w), P.gmax) : 0.f;
+          nm += wj * (mm + P.lambda * g);
+        }
       }
-      cc = nm / den;
-    } else {
-      cc = 2.f;
     }
-    if (cc < bcost) {
+    const float cc = den > 0.f ? nm / den : 2.f;
+    if (c < ncand && cc < bcost) {
       bcost = cc;
       best = cd;
     }
   }
-  if (gl == 0) {
+  if (gl == 0 && live) {
     pl[pix] = best;
     P.cost[base + pix] = bcost;
     P.bview[base + pix] = (unsigned char)vbest;
@@ -1246,11 +1596,11 @@ static cudaError_t init_constants() {
   return e;
 }
 
-size_t half_smem(int wr, int ws, bool cw, int maxsrc, int G) {
+size_t half_smem(int wr, int ws, bool cw, int maxsrc, int G, int mode) {
   const int wn = (2 * wr) / ws + 1;
-  const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
+  const int TW = mode == 2 ? half_tw_staged(wr) : half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
   size_t f = ((TW * TH + 31) & ~31) + (cw ? (size_t)((wn + G - 1) / G) * wn * PS_HALF_NT : 0) +
-             (size_t)maxsrc * PS_HALF_NT;
+             (size_t)maxsrc * PS_HALF_NT + (mode == 2 ? (size_t)(PS_HALF_NT / 32) * PS_BOX_P * PS_BOX_H : 0);
   return f * sizeof(float);
 }
 size_t eval_smem(int wr, int ws, bool cw) {
@@ -1261,7 +1611,7 @@ size_t eval_smem(int wr, int ws, bool cw) {
 }
 
 // Whether the weight cache fits (<= 200 KB of shared memory per CTA with the largest source count).
-static bool use_cache(int wr, int ws) { return half_smem(wr, ws, true, PS_MAXSRC, 1) <= 200 * 1024; }
+static bool use_cache(int wr, int ws) { return half_smem(wr, ws, true, PS_MAXSRC, 1, 0) <= 200 * 1024; }
 
 template <typename K>
 static cudaError_t launch(K kern, int ncta, int nt, size_t smem, cudaStream_t st, const PsRun& P) {
@@ -1273,8 +1623,21 @@ static cudaError_t launch(K kern, int ncta, int nt, size_t smem, cudaStream_t st
   return cudaGetLastError();
 }
 
-// Lanes per pixel of the half-step kernel for a tuning word (PS_TUNE_ONE_LANE selects 1, default 2).
-int half_lanes(unsigned tuning) { return (tuning & 0x4u) ? 1 : 2; }
+// Half-step mode of a tuning word: 2 = staged source boxes (PS_TUNE_STAGED), 1 = row-pair loops (PS_TUNE_ROW_PAIRS),
+// 0 = scalar loops.  The row-pair modes need one lane per pixel, the weight cache and a compiled window; otherwise the
+// scalar kernel runs (same bits).
+static int half_mode(unsigned tuning, int wr, int ws) {
+  if (!(tuning & 0x18u) || (tuning & 0x1u) || !use_cache(wr, ws)) return 0;
+  bool compiled = false;
+#define PS_CASE(a, b) compiled = compiled || (wr == a && ws == b);
+  PS_SPECS(PS_CASE)
+#undef PS_CASE
+  if (!compiled) return 0;
+  return (tuning & 0x10u) ? 2 : 1;
+}
+
+// Lanes per pixel of the half-step kernel for a tuning word (PS_TUNE_ONE_LANE or a row-pair mode selects 1, default 2).
+int half_lanes(unsigned tuning) { return (tuning & 0x1Cu) ? 1 : 2; }
 
 template <int A, int B, int G>
 static cudaError_t launch_half_g(const PsRun& P, bool cw, bool tex, size_t smem, cudaStream_t st) {
@@ -1283,14 +1646,29 @@ static cudaError_t launch_half_g(const PsRun& P, bool cw, bool tex, size_t smem,
   return tex ? launch(k_half<A, B, false, true, G>, P.ntiles, PS_HALF_NT, smem, st, P)
              : launch(k_half<A, B, false, false, G>, P.ntiles, PS_HALF_NT, smem, st, P);
 }
+template <int A, int B>
+static cudaError_t launch_half_pairs(const PsRun& P, int mode, bool tex, size_t smem, cudaStream_t st) {
+  if (mode == 2) return tex ? launch(k_half<A, B, true, true, 1, 2>, P.ntiles, PS_HALF_NT, smem, st, P)
+                            : launch(k_half<A, B, true, false, 1, 2>, P.ntiles, PS_HALF_NT, smem, st, P);
+  return tex ? launch(k_half<A, B, true, true, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P)
+             : launch(k_half<A, B, true, false, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P);
+}
 
 cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st) {
   cudaError_t e = init_constants();
   if (e != cudaSuccess) return e;
-  const bool cw = use_cache(P.wr, P.ws) && !(tuning & 0x1u);
   const bool tex = (tuning & 0x2u) != 0;
+  const int mode = half_mode(tuning, P.wr, P.ws);
+  if (mode != 0) {
+    const size_t smem = half_smem(P.wr, P.ws, true, P.maxsrc, 1, mode);
+#define PS_CASE(a, b) \
+    if (P.wr == a && P.ws == b) return launch_half_pairs<a, b>(P, mode, tex, smem, st);
+    PS_SPECS(PS_CASE)
+#undef PS_CASE
+  }
+  const bool cw = use_cache(P.wr, P.ws) && !(tuning & 0x1u);
   const int G = half_lanes(tuning);
-  const size_t smem = half_smem(P.wr, P.ws, cw, P.maxsrc, G);
+  const size_t smem = half_smem(P.wr, P.ws, cw, P.maxsrc, G, 0);
 #define PS_CASE(a, b)                                                                \
   if (P.wr == a && P.ws == b)                                                        \
     return G == 2 ? launch_half_g<a, b, 2>(P, cw, tex, smem, st) : launch_half_g<a, b, 1>(P, cw, tex, smem, st);

@@ -14,6 +14,11 @@
 #define PS_HALF_PW 32
 #define PS_HALF2_PW 16  // two lanes per pixel: a warp = 8 active columns × 2 rows × 2 lanes
 #define PS_HALF_PH 8
+// Staged-source half step (PS_TUNE_STAGED): a warp covers 8 active columns × 4 rows of the 32 × 8 tile and stages
+// the union of its lanes' source footprints of one window into a PS_BOX_P × PS_BOX_H box of shared memory.
+#define PS_BOX_P 40
+#define PS_BOX_H 24
+#define PS_STAGE_MIN_LANES 4
 // Evaluate / filter CTA: 128 threads covering 32 × 4 pixels (a warp is one row).
 #define PS_EVAL_NT 128
 #define PS_EVAL_PW 32

@@ -72,7 +72,9 @@ typedef struct ps_options {
 #define PS_TUNE_NO_WEIGHT_CACHE 0x1u /* recompute window weights per tap (more CTAs per SM, more exp work) */
 #define PS_TUNE_TEX_GATHER 0x2u      /* fetch each bilinear 2×2 footprint with one texture gather (same bits) */
 #define PS_TUNE_ONE_LANE 0x4u        /* one thread per pixel (default: two lanes per pixel split the window rows) */
-#define PS_TUNE_VALID_MASK 0x7u
+#define PS_TUNE_ROW_PAIRS 0x8u       /* one thread per pixel, window rows 2p and 2p+1 as packed f32x2 pairs */
+#define PS_TUNE_STAGED 0x10u         /* row pairs, and each warp stages its sources' footprints in shared memory */
+#define PS_TUNE_VALID_MASK 0x1Fu
 
 /* PmParams (crates/dense/src/params.rs:76-124, defaults :126-154). */
 typedef struct ps_pm_params {

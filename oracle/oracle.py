@@ -93,6 +93,8 @@ def lib() -> C.CDLL:
             "oracle_exp64": (C.c_double, [C.c_double]),
             "oracle_acos64": (C.c_double, [C.c_double]),
             "oracle_sincosf": (None, [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+            "oracle_box_footprint_check": (C.c_int, [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int,
+                                                     C.POINTER(C.c_int)]),
         }
         for n, (r, a) in sig.items():
             f = getattr(o, n)

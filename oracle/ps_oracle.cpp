@@ -36,6 +36,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <unordered_map>
 #include <vector>
@@ -1212,6 +1213,79 @@ float oracle_expf(float x) { return ps_expf(x); }
 double oracle_exp64(double x) { return ps_exp64(x); }
 double oracle_acos64(double x) { return ps_acos64(x); }
 void oracle_sincosf(float x, float* s, float* c) { ps_sincosf(x, s, c); }
+
+// Footprint bound of the engine's staged source boxes (the half step with PS_TUNE_STAGED; no reference counterpart:
+// it decides only where the kernel reads texels from, never a value).  Restates the kernel's per-lane rule: the
+// corner taps of the window at (x, y) (radius wr) must be in front of the source (1e-8 < z, zmin < 1e30) and the homography
+// terms bounded (Tu, Tv, (|u|+|v|+1)·Tz <= 2^14·zmin, |u|, |v| < 2^14); the lane's texel range is then
+// [floor(umin - 1/64), floor(umax + 1/64) + 1] × the same for v.  Returns -1 when the rule rejects the window,
+// otherwise the number of taps (window step ws) whose 2×2 texels fall outside that range or whose box address,
+// computed as the kernel does (F = u + (1.5·2^23 - lo) rounded toward -inf), differs from floor(u) - lo.  The tap
+// positions use the parity build's operation sequence (correctly rounded reciprocal).  range = {lx, hx, ly, hy}.
+int oracle_box_footprint_check(const float* H, int x, int y, int wr, int ws, int* range) {
+  const float fx = (float)x, fy = (float)y;
+  const float sx0 = fx + (float)(-wr), sx1 = fx + (float)wr, sy0 = fy + (float)(-wr), sy1 = fy + (float)wr;
+  const float rz0 = std::fma(H[7], sy0, H[8]), rz1 = std::fma(H[7], sy1, H[8]);
+  const float z00 = std::fma(H[6], sx0, rz0), z10 = std::fma(H[6], sx1, rz0);
+  const float z01 = std::fma(H[6], sx0, rz1), z11 = std::fma(H[6], sx1, rz1);
+  if (!(z00 > 1e-8f && z10 > 1e-8f && z01 > 1e-8f && z11 > 1e-8f)) return -1;
+  const float rx0 = std::fma(H[1], sy0, H[2]), rx1 = std::fma(H[1], sy1, H[2]);
+  const float ry0 = std::fma(H[4], sy0, H[5]), ry1 = std::fma(H[4], sy1, H[5]);
+  const float i00 = 1.0f / z00, i10 = 1.0f / z10, i01 = 1.0f / z01, i11 = 1.0f / z11;
+  const float u00 = std::fma(H[0], sx0, rx0) * i00, u10 = std::fma(H[0], sx1, rx0) * i10;
+  const float u01 = std::fma(H[0], sx0, rx1) * i01, u11 = std::fma(H[0], sx1, rx1) * i11;
+  const float v00 = std::fma(H[3], sx0, ry0) * i00, v10 = std::fma(H[3], sx1, ry0) * i10;
+  const float v01 = std::fma(H[3], sx0, ry1) * i01, v11 = std::fma(H[3], sx1, ry1) * i11;
+  const float umin = std::fmin(std::fmin(u00, u10), std::fmin(u01, u11));
+  const float umax = std::fmax(std::fmax(u00, u10), std::fmax(u01, u11));
+  const float vmin = std::fmin(std::fmin(v00, v10), std::fmin(v01, v11));
+  const float vmax = std::fmax(std::fmax(v00, v10), std::fmax(v01, v11));
+  const float zmin = std::fmin(std::fmin(z00, z10), std::fmin(z01, z11));
+  const float mx = std::fmax(std::fabs(sx0), std::fabs(sx1)), my = std::fmax(std::fabs(sy0), std::fabs(sy1));
+  const float tu = std::fabs(H[0]) * mx + std::fabs(H[1]) * my + std::fabs(H[2]);
+  const float tv = std::fabs(H[3]) * mx + std::fabs(H[4]) * my + std::fabs(H[5]);
+  const float tz = std::fabs(H[6]) * mx + std::fabs(H[7]) * my + std::fabs(H[8]);
+  const float ua = std::fmax(std::fabs(umin), std::fabs(umax)), va = std::fmax(std::fabs(vmin), std::fabs(vmax));
+  const float lim = 16384.0f * zmin;
+  if (!(zmin < 1e30f && tu <= lim && tv <= lim && (ua + va + 1.0f) * tz <= lim && ua < 16384.0f && va < 16384.0f))
+    return -1;
+  const int lx = (int)std::floor(umin - 0.015625f), hx = (int)std::floor(umax + 0.015625f) + 1;
+  const int ly = (int)std::floor(vmin - 0.015625f), hy = (int)std::floor(vmax + 0.015625f) + 1;
+  range[0] = lx;
+  range[1] = hx;
+  range[2] = ly;
+  range[3] = hy;
+  const float mxb = 12582912.0f - (float)lx, myb = 12582912.0f - (float)ly;
+  uint32_t mbits;
+  const float mag = 12582912.0f;
+  std::memcpy(&mbits, &mag, 4);
+  const int wn = (2 * wr) / ws + 1;
+  int bad = 0;
+  for (int a = 0; a < wn; ++a) {
+    const int dy = -wr + a * ws;
+    const float sy = fy + (float)dy;
+    const float rx = std::fma(H[1], sy, H[2]), ry = std::fma(H[4], sy, H[5]), rz = std::fma(H[7], sy, H[8]);
+    for (int b = 0; b < wn; ++b) {
+      const int dx = -wr + b * ws;
+      const float sx = fx + (float)dx;
+      const float izz = 1.0f / std::fma(H[6], sx, rz);
+      const float u = std::fma(H[0], sx, rx) * izz, v = std::fma(H[3], sx, ry) * izz;
+      const float xf = std::floor(u), yf = std::floor(v);
+      if (!(xf >= (float)lx && xf + 1.0f <= (float)hx && yf >= (float)ly && yf + 1.0f <= (float)hy)) {
+        bad++;
+        continue;
+      }
+      // u + mxb and v + myb are exact in binary64; rounding toward -inf onto the integer grid of [2^23, 2^24)
+      const float Fu = (float)std::floor((double)u + (double)mxb), Fv = (float)std::floor((double)v + (double)myb);
+      uint32_t bu, bv;
+      std::memcpy(&bu, &Fu, 4);
+      std::memcpy(&bv, &Fv, 4);
+      if ((int)(bu - mbits) != (int)xf - lx || (int)(bv - mbits) != (int)yf - ly || Fu - mxb != xf || Fv - myb != yf)
+        bad++;
+    }
+  }
+  return bad;
+}
 
 
 // ================================================================================================ post-processing

@@ -31,7 +31,7 @@ class _FakeSession:
         pass
 
     def kernel_stats(self, kind):
-        return {"ms": {0: 5.0, 2: 4.0, 3: 3.5, 4: 2.5, 6: 3.0, 7: 2.75}[self.tuning]}
+        return {"ms": {0: 5.0, 2: 4.0, 3: 3.5, 4: 2.5, 6: 3.0, 7: 2.75, 8: 2.6, 10: 2.7, 16: 2.9, 18: 2.8}[self.tuning]}
 
 
 class _FakeBackend:
@@ -70,9 +70,10 @@ def test_picks_fastest_and_caches(fake, tmp_path):
     r = autotune.tune(inp, cache=cache, max_views=4)
     assert r["tuning"] == 4 and not r["cached"]
     assert set(r["ms"]) == {str(t) for t in autotune.CANDIDATES}
-    # every candidate ran a warm-up and a timed run of one iteration on the first 4 views
+    # every candidate ran a converging warm-up of two iterations, then a timed iteration, on the first 4 views
     assert sorted({t for t, _, _ in fake.log}) == sorted(autotune.CANDIDATES)
-    assert all(v == (0, 1, 2, 3) and it == 1 for _, v, it in fake.log)
+    assert all(v == (0, 1, 2, 3) for _, v, _ in fake.log)
+    assert [it for _, _, it in fake.log] == [2, 1] * len(autotune.CANDIDATES)
     assert len(fake.log) == 2 * len(autotune.CANDIDATES)
     stored = json.loads(cache.read_text())
     assert stored[r["key"]]["tuning"] == 4

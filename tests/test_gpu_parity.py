@@ -141,9 +141,10 @@ def test_bit_reproducible(backend):
         _assert_same(x, y, "rerun")
 
 
-@pytest.mark.parametrize("tuning", [1, 2, 3, 4, 5, 6, 7])
+@pytest.mark.parametrize("tuning", [1, 2, 3, 4, 5, 6, 7, 8, 10, 16, 18])
 def test_half_step_variants_bitwise_equal(tuning):
-    """Every half-step kernel variant (weight cache off, texture gather, one lane per pixel) gives the oracle's bits."""
+    """Every half-step kernel variant (weight cache off, texture gather, one lane per pixel, row-pair f32x2 loops,
+    staged source boxes) gives the oracle's bits."""
     from cumulus3d_b200.patchstereo import PatchMatchBackend
     wl = scenes.workload_small(72, 56, window_radius=6, seed=13)
     p = RunParams(0, False, True, 2, 1)
@@ -155,6 +156,28 @@ def test_half_step_variants_bitwise_equal(tuning):
     oracle.run(wl.input, wl.views, cpu, p)
     for i in range(len(gpu)):
         _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning}")
+
+
+@pytest.mark.parametrize("tuning", [8, 10, 16, 18])
+@pytest.mark.parametrize("wr,ws", [(3, 1), (5, 1), (5, 2), (6, 1)])
+def test_row_pair_and_staged_variants_converged(tuning, wr, ws):
+    """The row-pair and staged-box variants on every compiled window, over a photometric run long enough for the
+    planes to converge (so that warps' footprints overlap and the staged boxes are used), then a geometric run."""
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    wl = scenes.workload_small(128, 96, views=3, window_radius=wr, window_step=ws, seed=31 + wr)
+    p1 = RunParams(0, False, True, 4, 1)
+    p2 = RunParams(0, True, False, 1, 2)
+    gpu, cpu = _states(wl), _states(wl)
+    be = PatchMatchBackend(0, math="parity", tuning=tuning)
+    with be.begin(wl.input) as s:
+        s.run(wl.views, gpu, p1)
+        snap = DepthSnapshot(1, 0, [g.depth.copy() for g in gpu])
+        s.run(wl.views, gpu, p2, snap)
+    be.close()
+    oracle.run(wl.input, wl.views, cpu, p1)
+    oracle.run(wl.input, wl.views, cpu, p2, snap)
+    for i in range(len(gpu)):
+        _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning} wr={wr} ws={ws}")
 
 
 def test_batched_mixed_sizes_equal_single_view_runs(backend):

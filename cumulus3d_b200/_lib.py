@@ -187,6 +187,7 @@ SIGNATURES = {
     "ps_kernel_stats": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_uint64)]),
     "ps_reset_stats": (C.c_int, [_P]),
+    "ps_kernel_staged_stats": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64)]),
     "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ps_check_reciprocal": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),
     # post-processing, fusion, output

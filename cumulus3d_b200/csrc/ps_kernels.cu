@@ -408,9 +408,9 @@ __device__ __forceinline__ float ncc_cost(const PsRun& P, const RefWin& rw, cons
 enum { SMP_LOAD = 0, SMP_TEX = 1, SMP_BOX = 2 };
 
 // The warp's staged box: box[r·PS_BOX_P + c] holds texel (gx0 + c, gy0 + r) of the source (0 outside the image);
-// mx = 1.5·2^23 - gx0 and my = 1.5·2^23 - gy0.
+// mx = 1.5·2^23 - gx0 and my = 1.5·2^23 - gy0; the taps address it with 32-bit shared-memory addresses.
 struct BoxRef {
-  const float* box;
+  unsigned sbase;  // shared address of the box minus 4·(P + 1)·bits(1.5·2^23), mod 2^32
   float mx, my;
 };
 
@@ -430,45 +430,44 @@ __device__ __forceinline__ float2 m_rcp2(float2 nz) {
 // the texture or the box.  Box addressing: F = (u + mx) rounded toward -inf is floor(u) - gx0 + 1.5·2^23 exactly (u
 // lies within the box, |gx0| < 2^15), so floor(u) = F - mx exactly and the bits of F are bits(1.5·2^23) + the box
 // column; the box offset is therefore bits(Fv)·P + bits(Fu) - (P + 1)·bits(1.5·2^23), taken mod 2^32.
-constexpr unsigned kBoxBias = 0u - (unsigned)(PS_BOX_P + 1) * 0x4B400000u;
+constexpr unsigned kBoxBias = 0u - 4u * (unsigned)(PS_BOX_P + 1) * 0x4B400000u;
+
+__device__ __forceinline__ float lds(unsigned a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"(a));
+  return v;
+}
+template <int OFF>
+__device__ __forceinline__ float lds_off(unsigned a) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1+%2];" : "=f"(v) : "r"(a), "n"(OFF));
+  return v;
+}
 
 template <int SMP>
 __device__ __forceinline__ float2 sample_pair(const PsLevel& S, const BoxRef& bx, float2 u, float2 v) {
-  float2 ax, ay, p00, p10, p01, p11;
   if constexpr (SMP == SMP_BOX) {
     const float2 mx = v_splat(bx.mx), my = v_splat(bx.my);
     const float2 fu = v_add_rm(u, mx), fv = v_add_rm(v, my);
-    ax = v_sub(u, v_sub(fu, mx));
-    ay = v_sub(v, v_sub(fv, my));
-    const float* qa = bx.box + ((unsigned)__float_as_int(fv.x) * PS_BOX_P + (unsigned)__float_as_int(fu.x) + kBoxBias);
-    const float* qb = bx.box + ((unsigned)__float_as_int(fv.y) * PS_BOX_P + (unsigned)__float_as_int(fu.y) + kBoxBias);
-    p00 = make_float2(qa[0], qb[0]);
-    p10 = make_float2(qa[1], qb[1]);
-    p01 = make_float2(qa[PS_BOX_P], qb[PS_BOX_P]);
-    p11 = make_float2(qa[PS_BOX_P + 1], qb[PS_BOX_P + 1]);
+    const float2 ax = v_sub(u, v_sub(fu, mx));
+    const float2 ay = v_sub(v, v_sub(fv, my));
+    // byte address = base + 4·(bits(Fv)·P + bits(Fu)) with the constant part folded into bx.sbase
+    const unsigned qa = (unsigned)__float_as_int(fv.x) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu.x);
+    const unsigned qb = (unsigned)__float_as_int(fv.y) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu.y);
+    const float2 p00 = make_float2(lds(qa), lds(qb));
+    const float2 p10 = make_float2(lds_off<4>(qa), lds_off<4>(qb));
+    const float2 p01 = make_float2(lds_off<4 * PS_BOX_P>(qa), lds_off<4 * PS_BOX_P>(qb));
+    const float2 p11 = make_float2(lds_off<4 * PS_BOX_P + 4>(qa), lds_off<4 * PS_BOX_P + 4>(qb));
+    const float2 top = v_fma(ax, v_sub(p10, p00), p00);
+    const float2 bot = v_fma(ax, v_sub(p11, p01), p01);
+    return v_fma(ay, v_sub(bot, top), top);
+  } else if constexpr (SMP == SMP_TEX) {
+    // scalar per lane: the gather's four texels feed the bilinear directly (no repacking into pairs)
+    return make_float2(src_sample_tex(S.tex, u.x, v.x), src_sample_tex(S.tex, u.y, v.y));
   } else {
-    const float2 xf = make_float2(floorf(u.x), floorf(u.y)), yf = make_float2(floorf(v.x), floorf(v.y));
-    ax = v_sub(u, xf);
-    ay = v_sub(v, yf);
-    if constexpr (SMP == SMP_TEX) {
-      const float4 qa = gather_red_offset11(S.tex, xf.x, yf.x), qb = gather_red_offset11(S.tex, xf.y, yf.y);
-      p00 = make_float2(qa.w, qb.w);
-      p10 = make_float2(qa.z, qb.z);
-      p01 = make_float2(qa.x, qb.x);
-      p11 = make_float2(qa.y, qb.y);
-    } else {
-      const float wf = (float)S.w, hf = (float)S.h;
-      const float* pa = S.img + f2i_exact(fminf(fmaxf(yf.x, -2.0f), hf)) * S.pitch + f2i_exact(fminf(fmaxf(xf.x, -2.0f), wf));
-      const float* pb = S.img + f2i_exact(fminf(fmaxf(yf.y, -2.0f), hf)) * S.pitch + f2i_exact(fminf(fmaxf(xf.y, -2.0f), wf));
-      p00 = make_float2(__ldg(pa), __ldg(pb));
-      p10 = make_float2(__ldg(pa + 1), __ldg(pb + 1));
-      p01 = make_float2(__ldg(pa + S.pitch), __ldg(pb + S.pitch));
-      p11 = make_float2(__ldg(pa + S.pitch + 1), __ldg(pb + S.pitch + 1));
-    }
+    return make_float2(src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.x, v.x),
+                       src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.y, v.y));
   }
-  const float2 top = v_fma(ax, v_sub(p10, p00), p00);
-  const float2 bot = v_fma(ax, v_sub(p11, p01), p01);
-  return v_fma(ay, v_sub(bot, top), top);
 }
 
 template <int SMP>
@@ -476,8 +475,8 @@ __device__ __forceinline__ float sample_one(const PsLevel& S, const BoxRef& bx, 
   if constexpr (SMP == SMP_BOX) {
     const float fu = __fadd_rd(u, bx.mx), fv = __fadd_rd(v, bx.my);
     const float ax = u - (fu - bx.mx), ay = v - (fv - bx.my);
-    const float* q = bx.box + ((unsigned)__float_as_int(fv) * PS_BOX_P + (unsigned)__float_as_int(fu) + kBoxBias);
-    const float p00 = q[0], p10 = q[1], p01 = q[PS_BOX_P], p11 = q[PS_BOX_P + 1];
+    const unsigned q = (unsigned)__float_as_int(fv) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu);
+    const float p00 = lds(q), p10 = lds_off<4>(q), p01 = lds_off<4 * PS_BOX_P>(q), p11 = lds_off<4 * PS_BOX_P + 4>(q);
     const float top = fmaf(ax, p10 - p00, p00);
     const float bot = fmaf(ax, p11 - p01, p01);
     return fmaf(ay, bot - top, top);
@@ -490,8 +489,9 @@ __device__ __forceinline__ float sample_one(const PsLevel& S, const BoxRef& bx, 
 
 // Window sums of a window whose four corner taps lie in front of the source camera (every tap then does), with the
 // row-pair weight cache.  Rows 2p / 2p+1 go through the pair loop; the last row of an odd window is scalar and adds
-// into the even-row sums, as in ncc_window.
-template <int WR, int WS, int NT, int SMP>
+// into the even-row sums, as in ncc_window.  UNROLL unrolls the pair loop over the window columns (the staged path);
+// the rolled form keeps the fallback's code small (instruction-cache footprint of the staged kernel).
+template <int WR, int WS, int NT, int SMP, bool UNROLL>
 __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefStats& rs, const PsLevel& S, const float* H,
                                                   int x, int y, const BoxRef& bx) {
   constexpr int wr = WR, ws = WS, wn = (2 * WR) / WS + 1, np = wn / 2;
@@ -507,18 +507,31 @@ __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefSta
     const float* t0 = rw.t + dy * rw.tw;
     const float* t1 = t0 + ws * rw.tw;
     const float* wp = rw.wc + p * wn * NT * 2;
-#pragma unroll
-    for (int b = 0; b < wn; ++b) {
-      const int dx = -wr + b * ws;
-      const float2 sx = v_splat(fx + (float)dx);
+    auto tap = [&](int dx, float sxf, const float* wq) {
+      const float2 sx = v_splat(sxf);
       const float2 ik = make_float2(t0[dx], t1[dx]);
-      const float2 w = *reinterpret_cast<const float2*>(wp + b * NT * 2);
+      const float2 w = *reinterpret_cast<const float2*>(wq);
       const float2 izz = m_rcp2(v_fma(nh6, sx, nrz));
       const float2 sv = sample_pair<SMP>(S, bx, v_mul(v_fma(h0, sx, rx), izz), v_mul(v_fma(h3, sx, ry), izz));
       const float2 wsv = v_mul(w, sv);
       Ss = v_add(Ss, wsv);
       SSs = v_fma(wsv, sv, SSs);
       IS = v_fma(wsv, ik, IS);
+    };
+    if constexpr (UNROLL) {
+#pragma unroll
+      for (int b = 0; b < wn; ++b) tap(-wr + b * ws, fx + (float)(-wr + b * ws), wp + b * NT * 2);
+    } else {
+      int dx = -wr;
+      float sxf = fx + (float)(-wr);
+      const float* wq = wp;
+#pragma unroll 1
+      for (int b = 0; b < wn; ++b) {
+        tap(dx, sxf, wq);
+        dx += ws;
+        sxf += (float)ws;
+        wq += NT * 2;
+      }
     }
   }
   if constexpr ((wn & 1) != 0) {
@@ -526,10 +539,7 @@ __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefSta
     const float sy = fy + (float)dy;
     const float rx = fmaf(H[1], sy, H[2]), ry = fmaf(H[4], sy, H[5]), rz = fmaf(H[7], sy, H[8]);
     const float* t0 = rw.t + dy * rw.tw;
-#pragma unroll
-    for (int b = 0; b < wn; ++b) {
-      const int dx = -wr + b * ws;
-      const float sx = fx + (float)dx;
+    auto tap = [&](int b, int dx, float sx) {
       const float ik = t0[dx];
       const float w = rw.wl[b * NT];
       const float izz = m_rcp(fmaf(H[6], sx, rz));
@@ -538,6 +548,19 @@ __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefSta
       Ss.x = Ss.x + wsv;
       SSs.x = fmaf(wsv, sv, SSs.x);
       IS.x = fmaf(wsv, ik, IS.x);
+    };
+    if constexpr (UNROLL) {
+#pragma unroll
+      for (int b = 0; b < wn; ++b) tap(b, -wr + b * ws, fx + (float)(-wr + b * ws));
+    } else {
+      int dx = -wr;
+      float sx = fx + (float)(-wr);
+#pragma unroll 1
+      for (int b = 0; b < wn; ++b) {
+        tap(b, dx, sx);
+        dx += ws;
+        sx += (float)ws;
+      }
     }
   }
   return ncc_finish(rs, Ss.x + Ss.y, SSs.x + SSs.y, IS.x + IS.y);
@@ -557,8 +580,9 @@ __device__ __forceinline__ bool window_front(const float* H, float fx, float fy)
 template <int WR, int WS, int NT, bool TEX>
 __device__ __forceinline__ float ncc_window_lane(const PsRun& P, const RefWin& rw, const RefStats& rs,
                                                  const PsLevel& S, const float* H, int x, int y) {
+  constexpr int smp = TEX ? SMP_TEX : SMP_LOAD;
   if (window_front<WR>(H, (float)x, (float)y))
-    return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD>(rw, rs, S, H, x, y, BoxRef{nullptr, 0.f, 0.f});
+    return ncc_window_pairs<WR, WS, NT, smp, true>(rw, rs, S, H, x, y, BoxRef{0u, 0.f, 0.f});
   return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
 }
 
@@ -566,6 +590,10 @@ __device__ __forceinline__ float ncc_window_lane(const PsRun& P, const RefWin& r
 struct BoxState {
   const float* src;
   int ox, oy;
+  // profiling: this lane's windows read from the box, restages (counted on every lane), and this lane's windows left
+  // to the per-lane loops because the footprint bound failed, the warp's request was too wide or too tall, or too few
+  // lanes were active
+  int nstaged, nrestage, nbound, nwide, ntall, nfew;
 };
 
 // Warp-collective NCC cost (every lane of the warp calls it; `act` marks the lanes that want this window).
@@ -624,10 +652,21 @@ __device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw,
       }
     }
   }
-  if (__all_sync(0xffffffffu, !act || fits) && __popc(am) >= PS_STAGE_MIN_LANES) {
+  const bool allfit = __all_sync(0xffffffffu, !act || fits);
+  const bool many = __popc(am) >= PS_STAGE_MIN_LANES;
+  if (P.stage_count && act) {
+    bs.nbound += !allfit;
+    bs.nfew += allfit && !many;
+  }
+  if (allfit && many) {
     const int gx0 = __reduce_min_sync(0xffffffffu, lx), gx1 = __reduce_max_sync(0xffffffffu, hx);
     const int gy0 = __reduce_min_sync(0xffffffffu, ly), gy1 = __reduce_max_sync(0xffffffffu, hy);
-    if (gx1 - gx0 + 1 <= PS_BOX_P - 3 && gy1 - gy0 + 1 <= PS_BOX_H) {
+    const bool narrow = gx1 - gx0 + 1 <= PS_BOX_P - 3, low = gy1 - gy0 + 1 <= PS_BOX_H;
+    if (P.stage_count && act) {
+      bs.nwide += !narrow;
+      bs.ntall += narrow && !low;
+    }
+    if (narrow && low) {
       if (!(S.img == bs.src && gx0 >= bs.ox && gx1 < bs.ox + PS_BOX_P && gy0 >= bs.oy && gy1 < bs.oy + PS_BOX_H)) {
         // Restage, centred on the request: origin x ≡ 2 (mod 4), so every 16-byte chunk of a plane row is aligned
         // (rows start 2 floats after a 128-byte boundary); chunks outside the plane's allocated rows are zero-filled,
@@ -655,14 +694,19 @@ __device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw,
         bs.src = S.img;
         bs.ox = ox;
         bs.oy = oy;
+        bs.nrestage++;
       }
-      return act ? ncc_window_pairs<WR, WS, NT, SMP_BOX>(
-                       rw, rs, S, H, x, y, BoxRef{box, 12582912.0f - (float)bs.ox, 12582912.0f - (float)bs.oy})
+      if (act) bs.nstaged++;
+      return act ? ncc_window_pairs<WR, WS, NT, SMP_BOX, true>(
+                       rw, rs, S, H, x, y,
+                       BoxRef{(unsigned)__cvta_generic_to_shared(box) + kBoxBias, 12582912.0f - (float)bs.ox,
+                              12582912.0f - (float)bs.oy})
                  : 2.0f;
     }
   }
   if (!act) return 2.0f;
-  if (front) return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD>(rw, rs, S, H, x, y, BoxRef{nullptr, 0.f, 0.f});
+  if (front)
+    return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD, true>(rw, rs, S, H, x, y, BoxRef{0u, 0.f, 0.f});
   return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
 }
 
@@ -806,100 +850,23 @@ __device__ __forceinline__ void count_windows(const PsRun& P, int nwin) {
 
 // Half-step tile geometry for G lanes per pixel: G = 1 -> 32 × 8 pixels (a warp = 16 active columns × 2 rows);
 // G = 2 -> 16 × 8 pixels (a warp = 8 active columns × 2 rows × 2 lanes).  The shared tile's row pitch is padded so
-// that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.  The staged mode's
-// warp (8 active columns × 4 rows) needs a pitch ≡ 8 (mod 16): its rows 0 and 2 (and 1 and 3) then fall 16 banks
-// apart, and the checkerboard puts odd rows on the other bank parity.
+// that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.  The staged kernel's
+// warp (4 active columns × 8 rows) needs a pitch ≡ 4 or 12 (mod 16): its same-parity rows then fall 8 banks apart
+// and the checkerboard puts the other rows on the other bank parity.
 __host__ __device__ constexpr int half_pw(int G) { return G == 2 ? PS_HALF2_PW : PS_HALF_PW; }
 __host__ __device__ constexpr int half_tw(int G, int wr) {
   return G == 2 ? (((PS_HALF2_PW + 2 * wr) + 15) / 32) * 32 + 16 : PS_HALF_PW + 2 * wr;
 }
-__host__ __device__ constexpr int half_tw_staged(int wr) { return ((PS_HALF_PW + 2 * wr + 7) / 16) * 16 + 8; }
+__host__ __device__ constexpr int half_tw_staged(int wr) { return ((PS_HALF_PW + 2 * wr + 3) / 8) * 8 + 4; }
 
-// Half-step variants (all give the same bits):
-//   MODE 0: one lane (G = 1) or two lanes (G = 2) per pixel, scalar tap loops;
-//   MODE 1: one lane per pixel, row-pair f32x2 tap loops on the row-pair weight cache;
-//   MODE 2: MODE 1 plus the warp-collective staged source boxes (ncc_cost_warp).  No lane leaves early: lanes
-//           outside the image work on a clamped pixel with every window inactive and write nothing, and every loop
-//           that contains a window evaluation runs the same trip count on all lanes.
-// G = 1: two CTAs per SM with the weight cache (~90 KB each for a 13×13 window), four without it.
-// G = 2: the two lanes of a pixel split the window rows, so each thread caches half the weights: four CTAs per SM.
-template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
-__global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
-  constexpr int NT = PS_HALF_NT;
-  constexpr int PW = half_pw(G);
-  constexpr bool PAIRW = MODE >= 1;
-  constexpr bool COLL = MODE == 2;
-  static_assert(MODE == 0 || (CW && G == 1 && WR != 0), "row-pair modes need the weight cache, one lane, a fixed window");
-  extern __shared__ float sm[];
-  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
-  const int wn = (2 * wr) / ws + 1;
-  const int TW = COLL ? half_tw_staged(wr) : half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
-  float* tile = sm;
-  float* wcache = sm + ((TW * TH + 31) & ~31);
-  float* wvs = wcache + (CW ? ((wn + G - 1) / G) * wn * NT : 0);
-  float* boxes = wvs + P.maxsrc * NT;
+// ---------------------------------------------------------------------------- per-pixel PatchMatch logic
+// Shared by the half-step kernels; each helper is the reference's step verbatim (patchmatch.cu line ranges cited).
 
-  const int ii = find_item(P, blockIdx.x);
-  const PsItem& it = P.items[ii];
-  const int w = it.w, h = it.h;
-  const int tiles_x = (w + PW - 1) / PW;
-  const int tl = blockIdx.x - it.tile0;
-  const int x0 = (tl % tiles_x) * PW, y0 = (tl / tiles_x) * PS_HALF_PH;
-  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
-  {
-    const int ox = x0 - wr, oy = y0 - wr;
-    for (int i = threadIdx.x; i < TW * TH; i += NT) {
-      int tx = i % TW, ty = i / TW;
-      int gx = ox + tx, gy = oy + ty;
-      tile[i] = (gx >= 0 && gy >= 0 && gx < w && gy < h) ? R.img[gy * R.pitch + gx] : 0.f;
-    }
-  }
-  __syncthreads();
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int gl = G == 2 ? (lane & 1) : 0;
-  int row, col;
-  if constexpr (COLL) {
-    row = 4 * (warp >> 1) + (lane >> 3);
-    col = 8 * (warp & 1) + (lane & 7);
-  } else {
-    row = 2 * warp + (lane >> 4);
-    col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
-  }
-  int y = y0 + row;
-  int x = x0 + 2 * col + ((y + P.color) & 1);
-  const bool live = x < w && y < h;
-  if constexpr (!COLL) {
-    if (!live) return;  // both lanes of a pixel leave together
-  } else {
-    y = min(y, h - 1);
-    x = min(x, w - 1);
-    row = y - y0;
-  }
-  float* box = boxes + warp * (PS_BOX_P * PS_BOX_H);
-  BoxState bs{nullptr, 0, 0};
-
-  RefWin rw;
-  rw.t = tile + (row + wr) * TW + (x - x0 + wr);
-  rw.tw = TW;
-  rw.wc = wcache + (PAIRW ? 2 * threadIdx.x : threadIdx.x);
-  rw.g = gl;
-  rw.pmask = G == 2 ? (3u << (lane & ~1)) : 0u;
-  rw.wl = wcache + (wn & ~1) * wn * NT + threadIdx.x;
-  float* wv = wvs + threadIdx.x;
-
-  const PsView& vd = P.views[it.view];
-  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
-  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
-  const int nsrc = vd.nsrc;
-  const long long base = it.off;
-  const int pix = y * w + x;
-  float4* pl = P.plane + base;
-  const float* co = P.cost + base;
-  const float3 ray = pixel_ray(R, x, y);
-
-  // 1. Candidates: current + 8 regions.
-  float4 hyp[9];
-  hyp[0] = pl[pix];
+// 1. Candidates: the current plane and the best-cost neighbour of each of the 8 regions, transferred onto this
+// pixel's ray (patchmatch.cu:477-511).
+__device__ __forceinline__ void propagation_candidates(const PsLevel& R, const float4* pl, const float* co, int x, int y,
+                                                       int w, int h, float3 ray, float4* hyp) {
+  hyp[0] = pl[y * w + x];
 #pragma unroll 1
   for (int r = 0; r < 8; ++r) {
     const int k0 = r < 4 ? r * 7 : 28 + (r - 4) * 11;
@@ -930,14 +897,202 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
       }
     }
   }
+}
 
-  // One NCC window of this pixel (the homography H is valid where hok): per lane, or warp-collective in MODE 2.
+// 2. View selection and aggregation (patchmatch.cu:513-594): per source, votes over the 8 propagated hypotheses,
+// the view weight, and the weighted cost sums of the 9 hypotheses; then the aggregated argmin.
+struct ViewAgg {
+  float num[9], numf[9];
+  float den, denf, wbest;
+  int vbest;
+};
+__device__ __forceinline__ void agg_init(ViewAgg& a) {
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    a.num[i] = 0.f;
+    a.numf[i] = 0.f;
+  }
+  a.den = 0.f;
+  a.wbest = 0.f;
+  a.denf = 0.f;
+  a.vbest = 255;
+}
+// Source j with prior > 0: m, gg = photometric costs and truncated geometric errors of the 9 hypotheses; writes the
+// view weight (or -prior) to *wvj.
+__device__ __forceinline__ void agg_source(const PsRun& P, ViewAgg& a, const float* m, const float* gg, float prior,
+                                           int j, int vprev, float* wvj) {
+  int good = 0, bad = 0;
+  float conf = 0.f;
+#pragma unroll
+  for (int i = 1; i < 9; ++i) {
+    if (m[i] < P.tau_good) {
+      good++;
+      conf += m_exp(-m[i] * m[i] * P.inv2beta2);
+    }
+    if (m[i] > P.tau_bad) bad++;
+  }
+  const bool adopt = good > P.n1 && bad < P.n2;
+  const bool isprev = j == vprev;
+  const float wp = adopt ? (isprev ? 2.f : 1.f) * conf / (float)good : (isprev ? P.prev_w : 0.f);
+  const float w2 = wp * prior;
+  *wvj = w2 > 0.f ? w2 : -prior;
+#pragma unroll
+  for (int i = 0; i < 9; ++i) a.numf[i] += prior * (m[i] + P.lambda * gg[i]);
+  a.denf += prior;
+  if (w2 > 0.f) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) a.num[i] += w2 * (m[i] + P.lambda * gg[i]);
+    a.den += w2;
+    if (w2 > a.wbest) {
+      a.wbest = w2;
+      a.vbest = j;
+    }
+  }
+}
+// Aggregated costs, the prior-weighted fallback (view weights become the priors, den = denf), the argmin (earliest on
+// ties); returns the best hypothesis and its cost.
+__device__ __forceinline__ void agg_finish(ViewAgg& a, const float4* hyp, int nsrc, float* wv, int wstride,
+                                           float4& best, float& bcost) {
+  float agg[9];
+  int bi9 = 0;
+  if (a.den > 0.f) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = a.num[i] / a.den;
+  } else if (a.denf > 0.f) {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = a.numf[i] / a.denf;
+    for (int j = 0; j < nsrc; ++j) wv[j * wstride] = -wv[j * wstride];
+    a.den = a.denf;
+  } else {
+#pragma unroll
+    for (int i = 0; i < 9; ++i) agg[i] = 2.f;
+  }
+  float bagg = agg[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i)
+    if (agg[i] < bagg) {
+      bagg = agg[i];
+      bi9 = i;
+    }
+  best = hyp[0];
+#pragma unroll
+  for (int i = 1; i < 9; ++i)
+    if (i == bi9) best = hyp[i];
+  bcost = bagg;
+}
+
+// 3. Refinement candidates (patchmatch.cu:596-628) and 4. the coarse-scale candidate (:629-653).  The draws come from
+// the per-pixel RNG in the reference's order; a best plane with d <= 0 takes the random depth.
+struct Refine {
+  float3 n0, n_r, n_p;
+  float d_r, d_p, bw;
+  float4 qprior;
+  int ncand;
+};
+// has_prior / qprior: the coarse-scale candidate (does not depend on the traversal).
+__device__ __forceinline__ void refine_prior(const PsRun& P, long long g, float var, float3 ray, Refine& r) {
+  bool has_prior = false;
+  r.qprior = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (P.use_prior && var < P.weak_var) {
+    r.qprior = P.prior[g];
+    has_prior = r.qprior.w > 0.f && dot3(make_float3(r.qprior.x, r.qprior.y, r.qprior.z), ray) < 0.f;
+  }
+  r.ncand = has_prior ? 7 : 6;
+}
+__device__ __forceinline__ void refine_draw(const PsRun& P, const PsView& vd, int pix, float3 ray, float4& best,
+                                            Refine& r) {
+  u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, P.t, P.color, (u64)pix);
+  r.d_r = random_depth(st, vd.dmin, vd.dmax);
+  r.n_r = random_normal(st, ray);
+  const float uu = 2.f * rnd(st) - 1.f;
+  const float inv = best.w > 0.f ? (1.f / best.w) * (1.f + uu * P.eps) : -1.f;
+  r.d_p = inv > 0.f ? 1.f / inv : r.d_r;
+  if (!(best.w > 0.f)) best.w = r.d_r;
+  r.n0 = make_float3(best.x, best.y, best.z);
+  r.n_p = perturb_normal(st, r.n0, ray, P.phi);
+  r.bw = best.w;
+}
+__device__ __forceinline__ float4 refine_candidate(const Refine& r, int c) {
+  switch (c) {
+    case 0: return make_float4(r.n0.x, r.n0.y, r.n0.z, r.d_r);
+    case 1: return make_float4(r.n_r.x, r.n_r.y, r.n_r.z, r.bw);
+    case 2: return make_float4(r.n_r.x, r.n_r.y, r.n_r.z, r.d_r);
+    case 3: return make_float4(r.n0.x, r.n0.y, r.n0.z, r.d_p);
+    case 4: return make_float4(r.n_p.x, r.n_p.y, r.n_p.z, r.bw);
+    case 5: return make_float4(r.n_p.x, r.n_p.y, r.n_p.z, r.d_p);
+    default: return r.qprior;
+  }
+}
+
+// Half-step variants (all give the same bits):
+//   k_half MODE 0: one lane (G = 1) or two lanes (G = 2) per pixel, scalar tap loops;
+//   k_half MODE 1: one lane per pixel, row-pair f32x2 tap loops on the row-pair weight cache;
+//   k_half_st:     row pairs plus the warp-collective staged source boxes (ncc_cost_warp).
+// G = 1: two CTAs per SM with the weight cache (~90 KB each for a 13×13 window), four without it.
+// G = 2: the two lanes of a pixel split the window rows, so each thread caches half the weights: four CTAs per SM.
+template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
+__global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_HALF_NT;
+  constexpr int PW = half_pw(G);
+  constexpr bool PAIRW = MODE >= 1;
+  static_assert(MODE == 0 || (MODE == 1 && CW && G == 1 && WR != 0), "row pairs need the weight cache, one lane, a fixed window");
+  extern __shared__ float sm[];
+  const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
+  const int wn = (2 * wr) / ws + 1;
+  const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
+  float* tile = sm;
+  float* wcache = sm + ((TW * TH + 31) & ~31);
+  float* wvs = wcache + (CW ? ((wn + G - 1) / G) * wn * NT : 0);
+
+  const int ii = find_item(P, blockIdx.x);
+  const PsItem& it = P.items[ii];
+  const int w = it.w, h = it.h;
+  const int tiles_x = (w + PW - 1) / PW;
+  const int tl = blockIdx.x - it.tile0;
+  const int x0 = (tl % tiles_x) * PW, y0 = (tl / tiles_x) * PS_HALF_PH;
+  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
+  {
+    const int ox = x0 - wr, oy = y0 - wr;
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+      int tx = i % TW, ty = i / TW;
+      int gx = ox + tx, gy = oy + ty;
+      tile[i] = (gx >= 0 && gy >= 0 && gx < w && gy < h) ? R.img[gy * R.pitch + gx] : 0.f;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gl = G == 2 ? (lane & 1) : 0;
+  const int row = 2 * warp + (lane >> 4), col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
+  const int y = y0 + row;
+  const int x = x0 + 2 * col + ((y + P.color) & 1);
+  if (x >= w || y >= h) return;  // both lanes of a pixel leave together
+
+  RefWin rw;
+  rw.t = tile + (row + wr) * TW + (x - x0 + wr);
+  rw.tw = TW;
+  rw.wc = wcache + (PAIRW ? 2 * threadIdx.x : threadIdx.x);
+  rw.g = gl;
+  rw.pmask = G == 2 ? (3u << (lane & ~1)) : 0u;
+  rw.wl = wcache + (wn & ~1) * wn * NT + threadIdx.x;
+  float* wv = wvs + threadIdx.x;
+
+  const PsView& vd = P.views[it.view];
+  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
+  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
+  const int nsrc = vd.nsrc;
+  const long long base = it.off;
+  const int pix = y * w + x;
+  float4* pl = P.plane + base;
+  const float3 ray = pixel_ray(R, x, y);
+
+  float4 hyp[9];
+  propagation_candidates(R, pl, P.cost + base, x, y, w, h, ray, hyp);
+
+  // One NCC window of this pixel (the homography H is valid where hok).
   int nwin = 0;
   const RefStats rs = ref_stats<WR, WS, CW, NT, G, PAIRW>(P, rw);
   auto window = [&](const PsLevel& S, const float* H, bool hok) -> float {
-    if constexpr (COLL) {
-      return ncc_cost_warp<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y, hok, nwin, box, bs);
-    } else if constexpr (MODE == 1) {
+    if constexpr (MODE == 1) {
       if (!hok || !ncc_begin(rs, S, H, (float)x, (float)y)) return 2.0f;
       nwin++;
       return ncc_window_lane<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y);
@@ -948,14 +1103,8 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
 
   // 2. View traversal: voting, weighting, aggregation.
   const int vprev = P.bview[base + pix];
-  float num[9], numf[9];
-#pragma unroll
-  for (int i = 0; i < 9; ++i) {
-    num[i] = 0.f;
-    numf[i] = 0.f;
-  }
-  float den = 0.f, wbest = 0.f, denf = 0.f;
-  int vbest = 255;
+  ViewAgg ag;
+  agg_init(ag);
 #pragma unroll 1
   for (int j = 0; j < nsrc; ++j) {
     const PsPair& pr = prs[j];
@@ -968,18 +1117,13 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[0], H);
       prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
-    }
-    const bool use = prior > 0.f && live;
-    if constexpr (COLL) {
-      if (!__any_sync(0xffffffffu, use)) continue;
-    } else {
-      if (!use) continue;
+      if (!(prior > 0.f)) continue;
     }
 #pragma unroll 1
     for (int i = 0; i < 9; ++i) {
       float H[9];
       const bool ok = homography(R, lp, (float)x, (float)y, hyp[i], H);
-      const float mi = window(S, H, ok && use);
+      const float mi = window(S, H, ok);
       const float gi = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hyp[i].w), P.gmax) : 0.f;
 #pragma unroll
       for (int q = 0; q < 9; ++q)
@@ -988,132 +1132,217 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
           gg[q] = gi;
         }
     }
-    if (!use) continue;
-    int good = 0, bad = 0;
-    float conf = 0.f;
-#pragma unroll
-    for (int i = 1; i < 9; ++i) {
-      if (m[i] < P.tau_good) {
-        good++;
-        conf += m_exp(-m[i] * m[i] * P.inv2beta2);
-      }
-      if (m[i] > P.tau_bad) bad++;
-    }
-    const bool adopt = good > P.n1 && bad < P.n2;
-    const bool isprev = j == vprev;
-    const float wp = adopt ? (isprev ? 2.f : 1.f) * conf / (float)good : (isprev ? P.prev_w : 0.f);
-    const float w2 = wp * prior;
-    wv[j * NT] = w2 > 0.f ? w2 : -prior;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) numf[i] += prior * (m[i] + P.lambda * gg[i]);
-    denf += prior;
-    if (w2 > 0.f) {
-#pragma unroll
-      for (int i = 0; i < 9; ++i) num[i] += w2 * (m[i] + P.lambda * gg[i]);
-      den += w2;
-      if (w2 > wbest) {
-        wbest = w2;
-        vbest = j;
-      }
-    }
+    agg_source(P, ag, m, gg, prior, j, vprev, wv + j * NT);
   }
-  float agg[9];
-  int bi9 = 0;
-  if (den > 0.f) {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) agg[i] = num[i] / den;
-  } else if (denf > 0.f) {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) agg[i] = numf[i] / denf;
-    for (int j = 0; j < nsrc; ++j) wv[j * NT] = -wv[j * NT];
-    den = denf;
-  } else {
-#pragma unroll
-    for (int i = 0; i < 9; ++i) agg[i] = 2.f;
-  }
-  float bagg = agg[0];
-#pragma unroll
-  for (int i = 1; i < 9; ++i)
-    if (agg[i] < bagg) {
-      bagg = agg[i];
-      bi9 = i;
-    }
-  float4 best = hyp[0];
-#pragma unroll
-  for (int i = 1; i < 9; ++i)
-    if (i == bi9) best = hyp[i];
-  float bcost = bagg;
+  float4 best;
+  float bcost;
+  agg_finish(ag, hyp, nsrc, wv, NT, best, bcost);
 
   // 3. Refinement, 6 hypotheses (patchmatch.cu:596-628), then 4. the coarse-scale candidate (:629-653).
-  u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, P.t, P.color, (u64)pix);
-  const float d_r = random_depth(st, vd.dmin, vd.dmax);
-  const float3 n_r = random_normal(st, ray);
-  const float uu = 2.f * rnd(st) - 1.f;
-  const float inv = best.w > 0.f ? (1.f / best.w) * (1.f + uu * P.eps) : -1.f;
-  const float d_p = inv > 0.f ? 1.f / inv : d_r;
-  if (!(best.w > 0.f)) best.w = d_r;
-  const float3 n0 = make_float3(best.x, best.y, best.z);
-  const float3 n_p = perturb_normal(st, n0, ray, P.phi);
-  const float bw = best.w;
-  bool has_prior = false;
-  float4 qprior = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (P.use_prior && rs.var < P.weak_var) {
-    qprior = P.prior[base + pix];
-    has_prior = qprior.w > 0.f && dot3(make_float3(qprior.x, qprior.y, qprior.z), ray) < 0.f;
-  }
-  const int ncand = has_prior ? 7 : 6;
-  auto candidate = [&](int c) {
-    switch (c) {
-      case 0: return make_float4(n0.x, n0.y, n0.z, d_r);
-      case 1: return make_float4(n_r.x, n_r.y, n_r.z, bw);
-      case 2: return make_float4(n_r.x, n_r.y, n_r.z, d_r);
-      case 3: return make_float4(n0.x, n0.y, n0.z, d_p);
-      case 4: return make_float4(n_p.x, n_p.y, n_p.z, bw);
-      case 5: return make_float4(n_p.x, n_p.y, n_p.z, d_p);
-      default: return qprior;
-    }
-  };
-  int ncw = ncand;
-  if constexpr (COLL) ncw = (int)__reduce_max_sync(0xffffffffu, (unsigned)ncand);
+  Refine rf;
+  refine_prior(P, base + pix, rs.var, ray, rf);
+  refine_draw(P, vd, pix, ray, best, rf);
 #pragma unroll 1
-  for (int c = 0; c < ncw; ++c) {
-    const float4 cd = candidate(c);
-    const bool run = c < ncand && den > 0.f && live;
-    float nm = 0.f;
-    if (!COLL || __any_sync(0xffffffffu, run)) {
+  for (int c = 0; c < rf.ncand; ++c) {
+    const float4 cd = refine_candidate(rf, c);
+    float cc;
+    if (ag.den > 0.f) {
+      float nm = 0.f;
 #pragma unroll 1
       for (int j = 0; j < nsrc; ++j) {
         const float wj = wv[j * NT];
-        const bool aj = run && wj > 0.f;
-        if constexpr (COLL) {
-          if (!__any_sync(0xffffffffu, aj)) continue;
-        } else {
-          if (!aj) continue;
-        }
+        if (!(wj > 0.f)) continue;
         const PsPair& pr = prs[j];
         const PsLPair lp = lps[j];
         const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
         float H[9];
         const bool hok = homography(R, lp, (float)x, (float)y, cd, H);
-        const float mm = window(S, H, aj && hok);
-        if (aj) {
-          const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, cd.w), P.gmax) : 0.f;
-          nm += wj * (mm + P.lambda * g);
-        }
+        const float mm = window(S, H, hok);
+        const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, cd.w), P.gmax) : 0.f;
+        nm += wj * (mm + P.lambda * g);
       }
+      cc = nm / ag.den;
+    } else {
+      cc = 2.f;
     }
-    const float cc = den > 0.f ? nm / den : 2.f;
-    if (c < ncand && cc < bcost) {
+    if (cc < bcost) {
       bcost = cc;
       best = cd;
     }
   }
-  if (gl == 0 && live) {
+  if (gl == 0) {
     pl[pix] = best;
     P.cost[base + pix] = bcost;
-    P.bview[base + pix] = (unsigned char)vbest;
+    P.bview[base + pix] = (unsigned char)ag.vbest;
   }
   count_windows(P, gl == 0 ? nwin : 0);
+}
+
+// Staged-source half step.  One lane per pixel; a warp covers an 8 × 8 pixel block of the 32 × 8 tile.  Every
+// window of every lane goes through ncc_cost_warp, which the whole warp calls together, so no lane leaves early
+// (lanes outside the image work on a clamped pixel with every window inactive and write nothing) and the pixel's
+// windows run as one job list with a single window call site: first the traversal jobs (source j, hypothesis i) in
+// the reference's order, then the refinement jobs (candidate c, source j).  The arithmetic and the order of every
+// sum are those of k_half, so the bits are the same.
+template <int WR, int WS, bool TEX>
+__global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant__ PsRun P) {
+  constexpr int NT = PS_HALF_NT;
+  constexpr int wr = WR, wn = (2 * WR) / WS + 1;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ float sm[];
+  const int TW = half_tw_staged(wr), TH = PS_HALF_PH + 2 * wr;
+  float* tile = sm;
+  float* wcache = sm + ((TW * TH + 31) & ~31);
+  float* wvs = wcache + wn * wn * NT;
+  float* boxes = wvs + P.maxsrc * NT;
+
+  const int ii = find_item(P, blockIdx.x);
+  const PsItem& it = P.items[ii];
+  const int w = it.w, h = it.h;
+  const int tiles_x = (w + PS_HALF_PW - 1) / PS_HALF_PW;
+  const int tl = blockIdx.x - it.tile0;
+  const int x0 = (tl % tiles_x) * PS_HALF_PW, y0 = (tl / tiles_x) * PS_HALF_PH;
+  const PsLevel R = P.lv[it.view * P.nlevels + P.level];
+  {
+    const int ox = x0 - wr, oy = y0 - wr;
+    for (int i = threadIdx.x; i < TW * TH; i += NT) {
+      int tx = i % TW, ty = i / TW;
+      int gx = ox + tx, gy = oy + ty;
+      tile[i] = (gx >= 0 && gy >= 0 && gx < w && gy < h) ? R.img[gy * R.pitch + gx] : 0.f;
+    }
+  }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int y = y0 + (lane >> 2);
+  int x = x0 + 2 * (4 * warp + (lane & 3)) + ((y + P.color) & 1);
+  const bool live = x < w && y < h;
+  y = min(y, h - 1);
+  x = min(x, w - 1);
+  float* box = boxes + warp * (PS_BOX_P * PS_BOX_H);
+  BoxState bs{nullptr, 0, 0, 0, 0, 0, 0, 0, 0};
+
+  RefWin rw;
+  rw.t = tile + (y - y0 + wr) * TW + (x - x0 + wr);
+  rw.tw = TW;
+  rw.wc = wcache + 2 * threadIdx.x;
+  rw.g = 0;
+  rw.pmask = 0u;
+  rw.wl = wcache + (wn & ~1) * wn * NT + threadIdx.x;
+  float* wv = wvs + threadIdx.x;
+
+  const PsView& vd = P.views[it.view];
+  const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
+  const PsLPair* lps = P.lpairs + ((size_t)it.view * P.nlevels + P.level) * PS_MAXSRC;
+  const int nsrc = vd.nsrc;
+  const long long base = it.off;
+  const int pix = y * w + x;
+  float4* pl = P.plane + base;
+  const float3 ray = pixel_ray(R, x, y);
+  const float fx = (float)x, fy = (float)y;
+
+  float4 hyp[9];
+  propagation_candidates(R, pl, P.cost + base, x, y, w, h, ray, hyp);
+  int nwin = 0;
+  const RefStats rs = ref_stats<WR, WS, true, NT, 1, true>(P, rw);
+  const int vprev = P.bview[base + pix];
+  Refine rf;
+  refine_prior(P, base + pix, rs.var, ray, rf);
+
+  const int nA = nsrc * 9;
+  const int nB = (int)__reduce_max_sync(FULL, (unsigned)rf.ncand) * nsrc;
+  ViewAgg ag;
+  agg_init(ag);
+  float m[9], gg[9];
+  float prior = 0.f, nm = 0.f;
+  bool use = false;
+  float4 best = hyp[0];
+  float bcost = 2.f;
+#pragma unroll 1
+  for (int k = 0;; ++k) {
+    if (k == nA) {  // end of the traversal: aggregate, then the refinement draws
+      agg_finish(ag, hyp, nsrc, wv, NT, best, bcost);
+      refine_draw(P, vd, pix, ray, best, rf);
+    }
+    if (k == nA + nB) break;
+    const bool trav = k < nA;
+    int j, i = 0, c = 0;
+    if (trav) {
+      j = k / 9;
+      i = k - 9 * j;
+    } else {
+      c = (k - nA) / nsrc;
+      j = (k - nA) - c * nsrc;
+    }
+    const PsPair& pr = prs[j];
+    const PsLPair lp = lps[j];
+    const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
+    float4 hv;
+    bool act;
+    float wj = 0.f;
+    if (trav) {
+      if (i == 0) {
+        wv[j * NT] = 0.f;
+        float H[9];
+        const bool ok = homography(R, lp, fx, fy, hyp[0], H);
+        prior = view_prior(P, R, pr, H, ok, x, y, hyp[0], wr);
+        use = prior > 0.f && live;
+      }
+      hv = hyp[i];
+      act = use;
+    } else {
+      hv = refine_candidate(rf, c);
+      wj = wv[j * NT];
+      act = c < rf.ncand && ag.den > 0.f && live && wj > 0.f;
+    }
+    float mv = 2.f;
+    if (__any_sync(FULL, act)) {
+      float H[9];
+      const bool hok = homography(R, lp, fx, fy, hv, H);
+      mv = ncc_cost_warp<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y, act && hok, nwin, box, bs);
+    }
+    if (trav) {
+      const float gv = (P.geometric && use) ? fminf(geo_error(P, R, S, pr, x, y, hv.w), P.gmax) : 0.f;
+#pragma unroll
+      for (int q = 0; q < 9; ++q)
+        if (q == i) {
+          m[q] = mv;
+          gg[q] = gv;
+        }
+      if (i == 8 && use) agg_source(P, ag, m, gg, prior, j, vprev, wv + j * NT);
+    } else {
+      if (act) {
+        const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hv.w), P.gmax) : 0.f;
+        nm += wj * (mv + P.lambda * g);
+      }
+      if (j == nsrc - 1) {
+        const float cc = ag.den > 0.f ? nm / ag.den : 2.f;
+        if (c < rf.ncand && cc < bcost) {
+          bcost = cc;
+          best = hv;
+        }
+        nm = 0.f;
+      }
+    }
+  }
+  if (live) {
+    pl[pix] = best;
+    P.cost[base + pix] = bcost;
+    P.bview[base + pix] = (unsigned char)ag.vbest;
+  }
+  count_windows(P, nwin);
+  if (P.stage_count) {
+    const unsigned c0 = __reduce_add_sync(FULL, (unsigned)bs.nstaged), c2 = __reduce_add_sync(FULL, (unsigned)bs.nbound);
+    const unsigned c3 = __reduce_add_sync(FULL, (unsigned)bs.nwide), c4 = __reduce_add_sync(FULL, (unsigned)bs.ntall);
+    const unsigned c5 = __reduce_add_sync(FULL, (unsigned)bs.nfew);
+    if (lane == 0) {
+      atomicAdd(P.stage_count, (unsigned long long)c0);
+      atomicAdd(P.stage_count + 1, (unsigned long long)bs.nrestage);
+      atomicAdd(P.stage_count + 2, (unsigned long long)c2);
+      atomicAdd(P.stage_count + 3, (unsigned long long)c3);
+      atomicAdd(P.stage_count + 4, (unsigned long long)c4);
+      atomicAdd(P.stage_count + 5, (unsigned long long)c5);
+    }
+  }
 }
 
 // ================================================================================ run start / evaluate (patchmatch.cu:661-692)
@@ -1648,8 +1877,8 @@ static cudaError_t launch_half_g(const PsRun& P, bool cw, bool tex, size_t smem,
 }
 template <int A, int B>
 static cudaError_t launch_half_pairs(const PsRun& P, int mode, bool tex, size_t smem, cudaStream_t st) {
-  if (mode == 2) return tex ? launch(k_half<A, B, true, true, 1, 2>, P.ntiles, PS_HALF_NT, smem, st, P)
-                            : launch(k_half<A, B, true, false, 1, 2>, P.ntiles, PS_HALF_NT, smem, st, P);
+  if (mode == 2) return tex ? launch(k_half_st<A, B, true>, P.ntiles, PS_HALF_NT, smem, st, P)
+                            : launch(k_half_st<A, B, false>, P.ntiles, PS_HALF_NT, smem, st, P);
   return tex ? launch(k_half<A, B, true, true, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P)
              : launch(k_half<A, B, true, false, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P);
 }

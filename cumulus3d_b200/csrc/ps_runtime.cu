@@ -207,7 +207,7 @@ struct ps_session {
   unsigned tuning = 0;
   // profiling
   bool profiling = false;
-  unsigned long long* counters = nullptr;  // NCC windows per kernel kind (device)
+  unsigned long long* counters = nullptr;  // NCC windows per kernel kind, then PS_STAGE_STATS counters per kind
   struct Pending {
     int kind;
     cudaEvent_t a, b;
@@ -417,10 +417,12 @@ template <typename F>
 void timed_launch(ps_session* s, int kind, PsRun& P, F&& f, const char* what) {
   if (!s->profiling) {
     P.ncc_count = nullptr;
+    P.stage_count = nullptr;
     launched(s, f(P), what);
     return;
   }
   P.ncc_count = s->counters + kind;
+  P.stage_count = s->counters + PS_KERNEL_KINDS + PS_STAGE_STATS * kind;
   ps_session::Pending pd;
   pd.kind = kind;
   pd.persistent = false;
@@ -913,8 +915,8 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
       sync(s);  // the pinned staging buffer is reused by the next call
       dfree(s, d8);
     }
-    s->counters = dalloc<unsigned long long>(s, PS_KERNEL_KINDS);
-    cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
+    s->counters = dalloc<unsigned long long>(s, (1 + PS_STAGE_STATS) * PS_KERNEL_KINDS);
+    cuda_ok(cudaMemsetAsync(s->counters, 0, (1 + PS_STAGE_STATS) * PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     s->lvh = lvh;
     s->lv = dalloc<PsLevel>(s, lvh.size());
     cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
@@ -2628,6 +2630,19 @@ int ps_kernel_stats(ps_session* s, uint32_t kind, double* total_ms, uint64_t* la
   });
 }
 
+int ps_kernel_staged_stats(ps_session* s, uint32_t kind, uint64_t* stats) {
+  return guard(s, [&] {
+    if (kind >= PS_KERNEL_KINDS) fail(PS_EINVAL, "kernel kind out of range");
+    if (!stats) fail(PS_EINVAL, "stats is NULL");
+    unsigned long long c[PS_STAGE_STATS];
+    cuda_ok(cudaMemcpyAsync(c, s->counters + PS_KERNEL_KINDS + PS_STAGE_STATS * kind, sizeof c,
+                            cudaMemcpyDeviceToHost, s->st),
+            "read counters");
+    sync(s);
+    for (int k = 0; k < PS_STAGE_STATS; ++k) stats[k] = c[k];
+  });
+}
+
 int ps_reset_stats(ps_session* s) {
   return guard(s, [&] {
     collect_events(s);
@@ -2635,7 +2650,7 @@ int ps_reset_stats(ps_session* s) {
       s->kind_ms[k] = 0;
       s->kind_launches[k] = 0;
     }
-    cuda_ok(cudaMemsetAsync(s->counters, 0, PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
+    cuda_ok(cudaMemsetAsync(s->counters, 0, (1 + PS_STAGE_STATS) * PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     sync(s);
   });
 }

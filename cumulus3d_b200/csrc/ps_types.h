@@ -14,11 +14,13 @@
 #define PS_HALF_PW 32
 #define PS_HALF2_PW 16  // two lanes per pixel: a warp = 8 active columns × 2 rows × 2 lanes
 #define PS_HALF_PH 8
-// Staged-source half step (PS_TUNE_STAGED): a warp covers 8 active columns × 4 rows of the 32 × 8 tile and stages
-// the union of its lanes' source footprints of one window into a PS_BOX_P × PS_BOX_H box of shared memory.
-#define PS_BOX_P 40
-#define PS_BOX_H 24
+// Staged-source half step (PS_TUNE_STAGED): a warp covers an 8 × 8 pixel block (4 active columns × 8 rows) of the
+// 32 × 8 tile and stages the union of its lanes' source footprints of one window into a PS_BOX_P × PS_BOX_H box of
+// shared memory.  The pitch is ≡ 4 (mod 16) so that the warp's ideal access pattern is free of bank conflicts.
+#define PS_BOX_P 36
+#define PS_BOX_H 32
 #define PS_STAGE_MIN_LANES 4
+#define PS_STAGE_STATS 8  // profiling counters of the staged half step per kernel kind
 // Evaluate / filter CTA: 128 threads covering 32 × 4 pixels (a warp is one row).
 #define PS_EVAL_NT 128
 #define PS_EVAL_PW 32
@@ -101,6 +103,7 @@ struct PsRun {
   int need_min;              // readout threshold: min_num_consistent
   int mode;                  // evaluate: 1 = run start (init + cost + clear best view), 0 = cost only
   unsigned long long* ncc_count;  // when set, kernels add the number of NCC window evaluations they performed
+  unsigned long long* stage_count;  // when set (staged half step): PS_STAGE_STATS counters, see ps_kernel_staged_stats
   const float4* proposal;  // run start with random init: planes with d > 0 replace the random draw (learned init)
   unsigned short* netin;   // plane sweep: bf16 network input [rows][netin_pitch][PS_NET_CH_IN] of the run's one view
   int netin_pitch;         // pixels per row of netin

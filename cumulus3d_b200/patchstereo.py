@@ -516,7 +516,10 @@ class PatchMatchSession:
     def kernel_stats(self, kind: int) -> dict:
         ms, n, w = C.c_double(), C.c_uint64(), C.c_uint64()
         self._check(self.lib.ps_kernel_stats(self.h, kind, C.byref(ms), C.byref(n), C.byref(w)))
-        return {"ms": ms.value, "launches": n.value, "ncc_windows": w.value}
+        st = (C.c_uint64 * 8)()
+        self._check(self.lib.ps_kernel_staged_stats(self.h, kind, st))
+        return {"ms": ms.value, "launches": n.value, "ncc_windows": w.value, "staged_windows": st[0],
+                "box_restages": st[1], "unstaged": {"bound": st[2], "wide": st[3], "tall": st[4], "few_lanes": st[5]}}
 
     def reset_stats(self) -> None:
         self._check(self.lib.ps_reset_stats(self.h))

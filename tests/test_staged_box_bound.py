@@ -97,15 +97,24 @@ def _place(g0, g1, size, align):
     return o
 
 
+def _box_dims():
+    import pathlib
+    import re
+    hdr = (pathlib.Path(__file__).resolve().parent.parent / "cumulus3d_b200" / "csrc" / "ps_types.h").read_text()
+    return (int(re.search(r"#define PS_BOX_P (\d+)", hdr).group(1)), int(re.search(r"#define PS_BOX_H (\d+)", hdr).group(1)))
+
+
 def test_box_placement_contains_every_admissible_request():
-    """Every request the kernel stages (at most PS_BOX_P - 3 = 37 wide, PS_BOX_H = 24 tall) lies inside the placed
-    box, and the x origin keeps the 16-byte chunk alignment."""
+    """Every request the kernel stages (at most PS_BOX_P - 3 wide, PS_BOX_H tall) lies inside the placed box, and the
+    x origin keeps the 16-byte chunk alignment; the pitch is a whole number of 16-byte chunks."""
+    bp, bh = _box_dims()
+    assert bp % 4 == 0
     for g0 in range(-70, 70):
-        for width in range(1, 38):
+        for width in range(1, bp - 2):
             g1 = g0 + width - 1
-            o = _place(g0, g1, 40, True)
-            assert (o - 2) % 4 == 0 and o <= g0 and g1 <= o + 39, (g0, g1, o)
-        for height in range(1, 25):
+            o = _place(g0, g1, bp, True)
+            assert (o - 2) % 4 == 0 and o <= g0 and g1 <= o + bp - 1, (g0, g1, o)
+        for height in range(1, bh + 1):
             g1 = g0 + height - 1
-            o = _place(g0, g1, 24, False)
-            assert o <= g0 and g1 <= o + 23, (g0, g1, o)
+            o = _place(g0, g1, bh, False)
+            assert o <= g0 and g1 <= o + bh - 1, (g0, g1, o)

@@ -80,8 +80,8 @@ def build_engine(force: bool = False, verbose: bool = False) -> pathlib.Path:
 def build_synth(force: bool = False) -> pathlib.Path:
     src = CSRC / "ps_synth.cpp"
     if force or _newer(SYNTH, [src]):
-        subprocess.run(["g++", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17", str(src),
-                        "-o", str(SYNTH)], check=True)
+        subprocess.run(["g++", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared",
+                        "-std=c++17", str(src), "-o", str(SYNTH)], check=True)
     return SYNTH
 
 

@@ -96,6 +96,41 @@ def build_pyramid_device(gray: np.ndarray, k: Sequence[float], levels: int, devi
     return [LevelImage(outs[i], tuple(ko[4 * i:4 * i + 4])) for i in range(levels)]
 
 
+DEFAULT_SEED = 0x005EED0FDE75  # DensifyOptions::base().seed (crates/dense/src/params.rs:423)
+
+
+def fast_filter():
+    """FilterParams with the fast profile's tuning (crates/dense/src/params.rs:452-459)."""
+    from . import _lib
+    f = _lib.default_filter()
+    f.min_ncc, f.geom_max_cost, f.min_num_consistent, f.median_filter = 0.2, 0.5, 3, 0
+    return f
+
+
+def kernel_input(cams, gray: Sequence[np.ndarray], sources: Sequence[Sequence[int]],
+                 ranges: Sequence[Optional[tuple]], *, pm=None, filt=None, seed: int = DEFAULT_SEED,
+                 max_levels: int = 3, min_level_size: int = 64) -> KernelInput:
+    """The KernelInput compute_depth_maps assembles (crates/dense/src/densify.rs:277-312): the level count from the
+    smallest image side, every view's 8-bit pyramid (coarsest first), key = FNV-1a of the image name, its sources with
+    their pair geometry (binary32 and binary64), the depth range ((1, 2) where the view observes no point).  pm
+    defaults to PmParams::default() (the fast profile's window), filt to the fast profile's filter."""
+    from . import _lib
+    from .patchstereo import KernelView, PairGeometry
+    from .scenes import fnv1a, pair_geometry
+    min_side = min(min(c.width, c.height) for c in cams)
+    nl = num_levels(min_side, max(max_levels, 1), max(min_level_size, 8))
+    views = []
+    for v, cam in enumerate(cams):
+        p64 = np.stack([pair_geometry(cam, cams[j]) for j in sources[v]]) if sources[v] else np.zeros((0, 15))
+        pairs = [PairGeometry(p[:9].astype(np.float32), p[9:12].astype(np.float32), p[12:15].astype(np.float32))
+                 for p in p64]
+        dmin, dmax = ranges[v] if ranges[v] is not None else (1.0, 2.0)
+        views.append(KernelView(fnv1a(cam.name.encode()), build_pyramid(np.asarray(gray[v], np.uint8), cam.k, nl),
+                                list(sources[v]), pairs, float(dmin), float(dmax), p64))
+    return KernelInput(views, nl, pm if pm is not None else _lib.default_pm(),
+                       filt if filt is not None else fast_filter(), seed)
+
+
 def readout(states: Sequence[ViewState], counts: Sequence[np.ndarray], nsrc: Sequence[int],
             min_num_consistent: int) -> List[ViewState]:
     """Readout threshold (densify.rs:441-454): depth/normal zeroed where count < max(1, min(min_num_consistent, nsrc)).

@@ -39,6 +39,12 @@ class _SynthScene(C.Structure):
 _synth = None
 
 
+class _RefSceneConfig(C.Structure):
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("focal", C.c_double), ("grid_x", C.c_int),
+                ("grid_y", C.c_int), ("spacing", C.c_double), ("altitude", C.c_double), ("seed", C.c_uint64),
+                ("num_points", C.c_int), ("num_boxes", C.c_int), ("boxes", (C.c_double * 6) * 8)]
+
+
 def _synth_lib():
     global _synth
     if _synth is None:
@@ -48,6 +54,10 @@ def _synth_lib():
         _synth.synth_render.restype = C.c_int
         _synth.synth_render.argtypes = [C.POINTER(_SynthScene), C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int,
                                         C.c_void_p, C.c_void_p, C.c_void_p]
+        _synth.synth_reference_scene.restype = C.c_int
+        _synth.synth_reference_scene.argtypes = [C.POINTER(_RefSceneConfig), C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.POINTER(C.c_int)]
     return _synth
 
 
@@ -336,3 +346,86 @@ def workload_c5(seed: int = 5, views: Optional[int] = None, with_gt: bool = Fals
     src = nearest_sources(cams, 5)
     inp = kernel_input(cams, list(img), src, (20.0, 60.0), window_radius=6, window_step=1)
     return Workload("c5_3840x2160_48views_boxes", cams, img, dep, nrm, inp, 2, 1, 1)
+
+
+# ---------------------------------------------------------------------------------------------- reference test scene
+# SynthConfig::default() (crates/dense/src/synthetic.rs:108-121).
+REFERENCE_BOXES = (((-3.0, -2.0, 0.0), (1.0, 2.5, 4.0)), ((3.0, 2.0, 0.0), (6.0, 5.0, 2.0)))
+
+
+@dataclass
+class ReferenceScene:
+    """The reference's synthetic accuracy scene: views in its order (name synth_{j}_{i}.png, image id = index + 1),
+    8-bit gray images, ground-truth camera-z depth and camera-frame normals, and the sparse model."""
+    cams: List[Camera]
+    gray: np.ndarray       # (n, h, w) uint8
+    gt_depth: np.ndarray   # (n, h, w) float32, 0 where the ray misses
+    gt_normal: np.ndarray  # (n, h, w, 3) float32
+    model: "object"        # neighbors.SparseModel
+    boxes: Tuple[Tuple[Tuple[float, float, float], Tuple[float, float, float]], ...]
+
+    @property
+    def image_ids(self) -> List[int]:
+        return [i + 1 for i in range(len(self.cams))]
+
+    def surface_distance(self, p) -> float:
+        """SynthScene::surface_distance (synthetic.rs:292-308): distance to the floor or the nearest box surface."""
+        best = abs(p[2])
+        for mn, mx in self.boxes:
+            inside = all(mn[a] <= p[a] <= mx[a] for a in range(3))
+            if inside:
+                dd = min(min(p[a] - mn[a], mx[a] - p[a]) for a in range(3))
+            else:
+                q = [max(mn[a] - p[a], 0.0, p[a] - mx[a]) for a in range(3)]
+                dd = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2])
+            best = min(best, dd)
+        return best
+
+    def surface_distances(self, pts: np.ndarray) -> np.ndarray:
+        """surface_distance of every row of pts (n, 3), vectorised."""
+        p = np.asarray(pts, np.float64)
+        best = np.abs(p[:, 2])
+        for mn, mx in self.boxes:
+            mn, mx = np.asarray(mn), np.asarray(mx)
+            inside = np.all((p >= mn) & (p <= mx), axis=1)
+            din = np.min(np.minimum(p - mn, mx - p), axis=1)
+            q = np.maximum(np.maximum(mn - p, 0.0), p - mx)
+            dout = np.sqrt((q * q).sum(1))
+            best = np.minimum(best, np.where(inside, din, dout))
+        return best
+
+
+def reference_scene(width: int = 384, height: int = 288, focal: float = 300.0, grid=(3, 3), spacing: float = 3.0,
+                    altitude: float = 20.0, boxes=REFERENCE_BOXES, seed: int = 11,
+                    num_points: int = 3000) -> ReferenceScene:
+    """make_scene(&SynthConfig) (crates/dense/src/synthetic.rs:190-290), rendered by csrc/ps_synth.cpp."""
+    from .neighbors import SparseModel
+    cfg = _RefSceneConfig(width, height, focal, grid[0], grid[1], spacing, altitude, seed, num_points, len(boxes))
+    for b, (mn, mx) in enumerate(boxes):
+        for a in range(3):
+            cfg.boxes[b][a] = mn[a]
+            cfg.boxes[b][3 + a] = mx[a]
+    n = grid[0] * grid[1]
+    cams = np.zeros((n, 16), np.float64)
+    gray = np.zeros((n, height, width), np.uint8)
+    dep = np.zeros((n, height, width), np.float32)
+    nrm = np.zeros((n, height, width, 3), np.float32)
+    pts = np.zeros((num_points, 3), np.float64)
+    off = np.zeros(num_points + 1, np.uint32)
+    tv = np.zeros(max(num_points * n, 1), np.uint32)
+    npts = C.c_int(0)
+    rc = _synth_lib().synth_reference_scene(C.byref(cfg), cams.ctypes.data, gray.ctypes.data, dep.ctypes.data,
+                                            nrm.ctypes.data, pts.ctypes.data, off.ctypes.data, tv.ctypes.data,
+                                            C.byref(npts))
+    if rc != 0:
+        raise RuntimeError("synth_reference_scene failed")
+    m = npts.value
+    cam_list = []
+    for v in range(n):
+        j, i = divmod(v, grid[0])
+        c = cams[v]
+        cam_list.append(Camera(f"synth_{j}_{i}.png", tuple(float(x) for x in c[:4]), c[4:13].reshape(3, 3).copy(),
+                               c[13:16].copy(), width, height))
+    views = np.array([np.concatenate([c.r.ravel(), c.t]) for c in cam_list], np.float64)
+    model = SparseModel(views, np.ascontiguousarray(pts[:m]), off[: m + 1].copy(), tv[: off[m]].copy())
+    return ReferenceScene(cam_list, gray, dep, nrm, model, tuple(boxes))

@@ -24,8 +24,21 @@ def test_thread_count_does_not_change_bits(small):
         assert np.array_equal(x.cost, y.cost)
 
 
+def test_reference_acceptance_gate():
+    """The reference's own acceptance gate (crates/cuda/tests/patchmatch_gpu.rs:96-98 and :118-132) on its own
+    synthetic scene (crates/dense/src/synthetic.rs, restated in csrc/ps_synth.cpp), run by the oracle through the whole
+    fast-profile flow: median depth error < 0.005, median normal error < 3°, valid > 0.5, and a fused cloud of more
+    than 10 000 points on the scene's surfaces."""
+    import reference_gate as rg
+    g = rg.setup(oracle.select_neighbors)
+    assert g.input.num_levels == 3 and all(len(s) == 8 for s in g.sources)
+    depths, normals, _, cloud = rg.run_oracle(g)
+    rg.check(rg.accuracy(g.scene, depths, normals), rg.fusion_stats(g.scene, cloud.positions))
+
+
 def test_converges_to_ground_truth(small):
-    """Accuracy gate in the spirit of crates/cuda/tests/patchmatch_gpu.rs:96-98 on the centre view."""
+    """A raw single-level run (no filter, no post-processing, 2 sources) on a terrain scene converges toward the ground
+    truth on the centre view; the reference's own thresholds apply to its full flow (test_reference_acceptance_gate)."""
     st = [ViewState.new(c.width, c.height) for c in small.cams]
     oracle.run(small.input, small.views, st, RunParams(0, False, True, 4, 1))
     gt, gn = small.gt_depth[1], small.gt_normal[1]

@@ -125,6 +125,20 @@ def make_workload(args, rank: int, shard_job: bool):
     return scenes.workload_c2(seed=2 + seed_shift, with_gt=False, views=args.views)
 
 
+def bench_config(wl, world: int, shard_job: bool, math: str) -> dict:
+    """The `config` of the line, the same in both arms (the reference arm times this workload on the CPU oracle)."""
+    wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
+    views_total = len(wl.cams) * (1 if shard_job else world)
+    return {"workload": wl.name, "views": views_total, "sizes": sorted({f"{c.width}x{c.height}" for c in wl.cams}),
+            "window": f"{wn}x{wn}", "sources": sorted({len(v.sources) for v in wl.input.views}),
+            "megapixels_per_job": round(wl.pixels() / 1e6, 2),
+            "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x{wl.geometric_iters} geometric",
+            "math": math, "inputs": "8-bit gray images, seeded synthetic terrain",
+            "l2": "inputs larger than L2 (24 f32 images + 1.2 GB of resident per-pixel state)",
+            "parallelism": (f"one job's views sharded over {world} ranks" if shard_job else
+                            f"{world} independent job(s), one per GPU")}
+
+
 def bench_ours(args, rank, world, local):
     import torch
     from cumulus3d_b200 import _lib, densify, scenes
@@ -216,15 +230,9 @@ def bench_ours(args, rank, world, local):
         "unit": "views/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms_step, 3), "higher_is_better": True, "scaling": "strong" if shard_job else "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain renderer, no dataset)",
-        "config": {"workload": wl.name, "views": views_total, "sizes": sorted({f"{c.width}x{c.height}" for c in wl.cams}),
-                   "window": f"{wn}x{wn}", "sources": sorted({len(v.sources) for v in wl.input.views}),
-                   "megapixels_per_job": round(wl.pixels() / 1e6, 2),
-                   "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x"
-                   f"{wl.geometric_iters} geometric", "math": args.math, "tuning": args.tuning,
-                   "autotune": None if tuned is None else {"half_ms": tuned["ms"], "cached": tuned["cached"]},
-                   "l2": "inputs larger than L2 (24 f32 images + 1.2 GB of resident per-pixel state)",
-                   "parallelism": (f"one job's views sharded over {world} ranks" if shard_job else
-                                   f"{world} independent job(s), one per GPU")},
+        "config": bench_config(wl, world, shard_job, args.math),
+        "kernel": {"tuning": args.tuning,
+                   "autotune": None if tuned is None else {"half_ms": tuned["ms"], "cached": tuned["cached"]}},
         "mpix_iter_per_s": round(mpix_iter, 2),
         "roofline": {"bound": "fp32", "kernel": "k_half", "achieved": round(achieved, 3),
                      "peak": round(fp32_peak, 2), "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4),
@@ -572,8 +580,14 @@ def ms_step_ratio(plain_ms, other_ms):
 
 
 def e2e_leg(args, wl, be, mine, world, rank, local, multi, views_total):
+    """The whole job through the host-buffer C ABI: ps_begin (image upload), the schedule with host states in and out
+    of every call, then (one job per rank) speckle removal and consistency fusion (min 3 views) of the read-out maps
+    and the download of the fused cloud."""
     import torch
-    from cumulus3d_b200 import densify
+    from cumulus3d_b200 import densify, fusion
+    fc = fusion.FusionCams(wl.cams, [list(kv.sources) for kv in wl.input.views])
+    prm = fusion.default_fusion(3)
+    cloud_bytes = [0]
 
     def run_once():
         with be.begin(wl.input) as s:
@@ -584,6 +598,12 @@ def e2e_leg(args, wl, be, mine, world, rank, local, multi, views_total):
             else:
                 densify.schedule_host(s, wl.input, mine, wl.photometric_iters, wl.geometric_rounds,
                                       wl.geometric_iters)
+                s.readout_resident(mine, download=False)
+                s.postprocess_resident(0, mine)
+                s.fuse_resident(0, mine, fc, prm)
+                cl = s.fused_points()
+                cloud_bytes[0] = int(cl.positions.nbytes + cl.normals.nbytes + cl.colors.nbytes + cl.keys.nbytes +
+                                     cl.vis_counts.nbytes + cl.vis.nbytes)
     for _ in range(max(1, min(args.warmup, 2))):
         run_once()
     torch.cuda.synchronize()
@@ -603,10 +623,13 @@ def e2e_leg(args, wl, be, mine, world, rank, local, multi, views_total):
     runs = 1 + wl.geometric_rounds
     h2d = imgs + npx * (16 * wl.geometric_rounds + 4 * len(wl.cams) / max(len(mine), 1) * (wl.geometric_rounds + 1)
                         + 16)
-    d2h = npx * (20 * runs + 1)
+    d2h = npx * (20 * runs + 1) + cloud_bytes[0]
     return {"value": round(views_total / dt, 3), "unit": "views/s", "ms_per_step": round(dt * 1e3, 2),
             "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
-            "path": "ps_begin + ps_run/ps_filter with host ViewState buffers (include/patchstereo.h)",
+            "path": "ps_begin + ps_run/ps_filter with host ViewState buffers, then ps_postprocess_resident + "
+                    "ps_fuse_resident + ps_fused_points (include/patchstereo.h)" if not multi else
+                    "ps_begin + ps_run/ps_filter with host ViewState buffers (include/patchstereo.h)",
+            "fused_cloud_bytes": cloud_bytes[0],
             "timer": "host wall clock around whole steps, max over ranks"}
 
 
@@ -648,11 +671,77 @@ def c_px(wl):
     return wl.cams[0].width * wl.cams[0].height
 
 
+def write_reference_workload(path: str) -> None:
+    """Renders the drone-scale workload and stores what the reference arm needs (cameras, 8-bit images, sources, the
+    ground-truth depth of view 0 and its sources) in an .npz.  Runs in a child process of the reference arm, so that
+    the arm's own process maps only the CPU oracle's library."""
+    from cumulus3d_b200 import scenes
+    wl = scenes.workload_c2(with_gt=True)
+    keep = [0] + list(wl.input.views[0].sources)
+    np.savez(path, names=np.array([c.name for c in wl.cams]), k=np.array([c.k for c in wl.cams], np.float64),
+             r=np.array([c.r for c in wl.cams]), t=np.array([c.t for c in wl.cams]),
+             size=np.array([(c.width, c.height) for c in wl.cams]),
+             gray=np.stack([kv.levels[0].pixels for kv in wl.input.views]),
+             src_off=np.cumsum([0] + [len(kv.sources) for kv in wl.input.views]),
+             src=np.array([j for kv in wl.input.views for j in kv.sources], np.int64),
+             gt_views=np.array(keep), gt=np.stack([wl.gt_depth[v] for v in keep]),
+             iters=np.array([wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters]),
+             window=np.array([wl.input.pm.window_radius, wl.input.pm.window_step]), name=np.array(wl.name))
+
+
+def load_reference_workload(path: str):
+    """The workload written by write_reference_workload, rebuilt without the renderer or the engine library."""
+    from cumulus3d_b200 import scenes
+    z = np.load(path)
+    cams = [scenes.Camera(str(n), tuple(float(x) for x in k), r, t, int(sz[0]), int(sz[1]))
+            for n, k, r, t, sz in zip(z["names"], z["k"], z["r"], z["t"], z["size"])]
+    off = z["src_off"]
+    src = [[int(j) for j in z["src"][off[i]:off[i + 1]]] for i in range(len(cams))]
+    inp = scenes.kernel_input(cams, list(z["gray"]), src, (25.0, 60.0), window_radius=int(z["window"][0]),
+                              window_step=int(z["window"][1]))
+    it = [int(x) for x in z["iters"]]
+    wl = scenes.Workload(str(z["name"]), cams, None, None, None, inp, it[0], it[1], it[2])
+    gt = {int(v): z["gt"][i] for i, v in enumerate(z["gt_views"])}
+    return wl, gt
+
+
+def cpu_whole_view(wl, gt, threads=None):
+    """Times the CPU oracle on the whole of view 0 through its full per-view schedule: run start and the photometric
+    iterations, the geometric rounds, the filter.  The snapshot holds view 0's own depth map and the ground truth of
+    its sources (their own maps would need their schedules first; the geometric cost does not depend on the values).
+    Returns seconds."""
+    from cumulus3d_b200.patchstereo import DepthSnapshot, RunParams, ViewState
+    from oracle import oracle
+    c = wl.cams[0]
+    st = [ViewState.new(c.width, c.height)]
+    t0 = time.perf_counter()
+    oracle.run(wl.input, [0], st, RunParams(0, False, True, wl.photometric_iters, 1), threads=threads)
+    for r in range(wl.geometric_rounds):
+        maps = [None] * len(wl.cams)
+        for v, d in gt.items():
+            maps[v] = d
+        maps[0] = st[0].depth.copy()
+        oracle.run(wl.input, [0], st, RunParams(0, True, False, wl.geometric_iters, 2 + r),
+                   DepthSnapshot(1 + r, 0, maps), threads=threads)
+    maps = [None] * len(wl.cams)
+    for v, d in gt.items():
+        maps[v] = d
+    maps[0] = st[0].depth.copy()
+    oracle.filter(wl.input, [0], st, DepthSnapshot(1 + wl.geometric_rounds, 0, maps), threads=threads)
+    return time.perf_counter() - t0
+
+
 def bench_reference(args, rank, world):
+    """The reference arm: the CPU oracle (the restatement of the reference's PatchStereo, all host cores) on the
+    same workload and config.  Each step times a band of full-width rows of view 0 and extrapolates to the per-view
+    schedule; one whole view through its full schedule is timed once and reported beside it with their ratio."""
     if rank != 0:
         return None
-    from cumulus3d_b200 import scenes
-    wl = scenes.workload_c2(with_gt=False)
+    import tempfile
+    tmp = tempfile.mkdtemp(prefix="ps_ref_")
+    path = os.path.join(tmp, "workload.npz")
+    subprocess.run([sys.executable, os.path.abspath(__file__), "--write-reference-workload", path], check=True)
+    wl, gt = load_reference_workload(path)
     cores = os.cpu_count() or 1
     for _ in range(args.warmup):
         cpu_sample(wl, cores, band=0.03)
@@ -662,19 +751,27 @@ def bench_reference(args, rank, world):
         per.append(cpu_sample(wl, cores)[2])
     wall = time.perf_counter() - t0
     per_view = statistics.median(per)
+    whole = None if args.no_whole_view else cpu_whole_view(wl, gt, cores)
     value = 1.0 / per_view
-    wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
-    return {"impl": "reference", "metric": "PatchStereo views/s (drone-scale workload, 1 B200 per rank)",
-            "value": round(value, 5), "unit": "views/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(wall / args.steps * 1e3, 1), "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain renderer, no dataset)",
-            "config": {"workload": "c2_1920x1080_24views_w13_6it_geo", "window": f"{wn}x{wn}", "sources": 4},
-            "cpu_baseline": {"value": round(value, 5), "unit": "views/s", "cores": cores, "kind": "port",
-                             "sample": "per step: the CPU oracle (all cores) on the top eighth of view 0's rows "
-                                       "(evaluate pass + one iteration), scaled by pixel count and extrapolated to "
-                                       "the full per-view schedule; the reference ships no CPU PatchStereo and its "
-                                       "Rust/CUDA code cannot be built here"},
-            "e2e": {"value": round(value, 5), "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    res = {"impl": "reference", "metric": "PatchStereo views/s (drone-scale workload, 1 B200 per rank)",
+           "value": round(value, 5), "unit": "views/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(wall / args.steps * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain renderer, no dataset)",
+           "config": bench_config(wl, world, False, "parity"),
+           "cpu_baseline": {"value": round(value, 5), "unit": "views/s", "cores": cores, "kind": "port",
+                            "sample": "per step: the CPU oracle (all cores) on the top eighth of view 0's rows "
+                                      "(evaluate pass + one iteration), scaled by pixel count and extrapolated to "
+                                      "the full per-view schedule; the reference ships no CPU PatchStereo and its "
+                                      "Rust/CUDA code cannot be built here"},
+           "e2e": {"value": round(value, 5), "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if whole is not None:
+        res["whole_view"] = {"seconds": round(whole, 2), "views_per_s": round(1.0 / whole, 5),
+                             "band_estimate_over_whole": round(value * whole, 3),
+                             "what": "view 0 at full size through run start, the photometric iterations, the "
+                                     "geometric rounds and the filter on all cores, timed once"}
+    os.remove(path)
+    os.rmdir(tmp)
+    return res
 
 
 def main():
@@ -702,7 +799,13 @@ def main():
                     help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
     ap.add_argument("--learned-iters", type=int, default=3,
                     help="photometric iterations of the learned-init schedule")
+    ap.add_argument("--no-whole-view", action="store_true",
+                    help="reference arm: skip the single whole-view timing of the CPU oracle")
+    ap.add_argument("--write-reference-workload", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.write_reference_workload:
+        write_reference_workload(args.write_reference_workload)
+        return
     if args.warmup < 3:
         args.warmup = 3
     rank, world, local = dist_env()

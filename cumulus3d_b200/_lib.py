@@ -256,16 +256,24 @@ def engine() -> C.CDLL:
     return _engine
 
 
+# PmParams::default() (crates/dense/src/params.rs:126-154) and FilterParams::default() (:209-220), the values
+# ps_pm_params_default / ps_filter_params_default return (a CPU test keeps them equal).  Plain Python, so that building
+# an input never loads the engine library (the CPU oracle's users, such as the benchmark's reference arm, rely on it).
+_PM_DEFAULTS = dict(window_radius=5, window_step=2, sigma_spatial=-1.0, sigma_color=0.2, tau0=0.8, tau_alpha=90.0,
+                    tau1=1.2, beta=0.3, n1=2, n2=3, prev_view_weight=0.2, min_triangulation_angle_deg=1.0,
+                    incident_angle_sigma=0.9, geom_lambda=0.2, geom_max_cost=3.0, top_k=3, eps0_photometric=0.2,
+                    eps0_geometric=0.05, phi0_photometric_deg=30.0, phi0_geometric_deg=10.0, eps_min=0.005,
+                    phi_min_deg=1.0, weak_texture_var=0.0)
+_FILTER_DEFAULTS = dict(min_ncc=0.1, min_triangulation_angle_deg=3.0, min_num_consistent=2, geom_max_cost=1.0,
+                        ncc_sigma=0.6, median_filter=1)
+
+
 def default_pm() -> PmParams:
-    p = PmParams()
-    engine().ps_pm_params_default(C.byref(p))
-    return p
+    return PmParams(**_PM_DEFAULTS)
 
 
 def default_filter() -> FilterParams:
-    p = FilterParams()
-    engine().ps_filter_params_default(C.byref(p))
-    return p
+    return FilterParams(**_FILTER_DEFAULTS)
 
 
 class PsError(RuntimeError):

@@ -124,6 +124,11 @@ def test_defaults_match_reference():
     o = _lib.Options()
     _lib.engine().ps_options_default(C.byref(o))
     assert (o.math_mode, o.max_batch, o.batch_pixels, o.checked, o.tuning) == (0, 64, 0, 0, 0)
+    # the Python defaults (which never load the engine) are the engine's exported defaults, field for field
+    epm, efl = _lib.PmParams(), _lib.FilterParams()
+    _lib.engine().ps_pm_params_default(C.byref(epm))
+    _lib.engine().ps_filter_params_default(C.byref(efl))
+    assert bytes(epm) == bytes(pm) and bytes(efl) == bytes(fl)
 
 
 def test_post_fusion_and_neighbour_defaults_match_reference():

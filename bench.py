@@ -9,7 +9,7 @@ snapshots, host counts) inside the timed region.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--math parity|fast] [--impl ours|reference]
 
 N > 1 (torchrun): by default every rank runs its own 24-view job (a differently seeded scene) with no collective in
-the data path ("scaling": "weak"); with --shard-job the views of ONE job are sharded over ranks (contiguous blocks)
+the data path ("scaling": "weak"); with --shard-job the views of ONE job are sharded over ranks (by pixel count)
 and the geometric round's snapshot is exchanged per owner rank over NCCL into every GPU's own snapshot buffer
 ("scaling": "strong").  `--impl reference` times the CPU
 oracle (this project's C++ restatement of the reference kernel; the reference has no CPU path of its own) on the
@@ -104,13 +104,6 @@ def dist_env():
     return rank, world, local
 
 
-def shard(n_views: int, rank: int, world: int):
-    """Contiguous view blocks, sizes differing by at most one (uniform view sizes, so pixel-balanced)."""
-    base, extra = divmod(n_views, world)
-    start = rank * base + min(rank, extra)
-    return list(range(start, start + base + (1 if rank < extra else 0)))
-
-
 def make_workload(args, rank: int, shard_job: bool):
     """The benchmark workload: c2 (drone scale, the metric's configuration; default), c1 (640×480, 3 views) or c3
     (64 views of mixed sizes from 4 terrains, 2-8 sources each)."""
@@ -151,7 +144,11 @@ def bench_ours(args, rank, world, local):
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     shard_job = world > 1 and args.shard_job
     wl = make_workload(args, rank, shard_job)
-    mine = shard(len(wl.cams), rank, world) if shard_job else list(range(len(wl.cams)))
+    if shard_job:
+        from cumulus3d_b200.multigpu import shard_lpt, view_pixels
+        mine = shard_lpt(view_pixels(wl.input), world)[rank]
+    else:
+        mine = list(range(len(wl.cams)))
     wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
     tuned = None
     if args.tuning < 0:  # autotune the half-step variant on a prefix of this job's views (outside the timed region)
@@ -165,7 +162,7 @@ def bench_ours(args, rank, world, local):
     exchange = None
     if shard_job:
         from cumulus3d_b200.multigpu import SnapshotExchange
-        exchange = SnapshotExchange(sess, wl.input, world, rank, shard)
+        exchange = SnapshotExchange(sess, wl.input, world, rank)
 
     def step():
         if exchange is None:  # one CUDA-graph launch per step (captured during the first warm-up step)

@@ -28,6 +28,8 @@ class Options(C.Structure):
 
 
 PS_TUNE_NO_WEIGHT_CACHE, PS_TUNE_TEX_GATHER, PS_TUNE_ONE_LANE = 0x1, 0x2, 0x4
+PS_TUNE_ROW_PAIRS, PS_TUNE_STAGED = 0x8, 0x10
+PS_INJECT_NONE, PS_INJECT_DEVICE_ALLOC, PS_INJECT_UPLOAD = 0, 1, 2
 PS_KERNEL_HALF, PS_KERNEL_EVAL, PS_KERNEL_FILTER, PS_KERNEL_OTHER, PS_KERNEL_SWEEP, PS_KERNEL_NET = range(6)
 PS_KERNEL_KINDS = 6
 
@@ -141,7 +143,7 @@ class NeighborParams(C.Structure):
 
 class DepthSnapshot(C.Structure):
     _fields_ = [("id", C.c_uint64), ("level", C.c_uint32), ("num_maps", C.c_uint32),
-                ("maps", C.POINTER(C.POINTER(C.c_float)))]
+                ("maps", C.POINTER(C.POINTER(C.c_float))), ("map_lengths", C.POINTER(C.c_uint64))]
 
 
 # Every exported symbol of include/patchstereo.h with (restype, argtypes).
@@ -187,6 +189,7 @@ SIGNATURES = {
     "ps_kernel_stats": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint64),
                                   C.POINTER(C.c_uint64)]),
     "ps_reset_stats": (C.c_int, [_P]),
+    "ps_backend_inject_failure": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32]),
     "ps_kernel_staged_stats": (C.c_int, [_P, C.c_uint32, C.POINTER(C.c_uint64)]),
     "ps_measure_fp32_peak": (C.c_int, [C.c_int, C.POINTER(C.c_double)]),
     "ps_check_reciprocal": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)]),

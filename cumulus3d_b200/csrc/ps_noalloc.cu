@@ -14,10 +14,15 @@
 //    whole input into it and reads only what it copied, so nothing has to start at zero; calls whose work overlaps
 //    on the GPU (two streams at once) race on the array;
 //  * the first call on a device looks the array's device address up (cudaGetSymbolAddress) with that device
-//    current; make that first call before any stream capture.
+//    current; make that first call before any stream capture.  The address is kept for the life of the process,
+//    so it is no longer valid after the caller resets the device (cudaDeviceReset);
+//  * `planes` must be device (or managed) memory of `device`: anything else is rejected before any device work;
+//  * the call makes `device` current only while it runs and restores the caller's current device before it returns;
+//  * it does not run while the calling thread has a CUDA error pending (it returns PS_ECUDA and leaves that error
+//    for its owner), so a launch failure it reports is its own.
 //
 // The arithmetic is the parity build's (this file is compiled with --fmad=false and IEEE division), so the output
-// has the same bits as ps_median_filter on the same planes.
+// has the same bits as ps_median_filter of a parity-math session on the same planes.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -46,10 +51,12 @@ struct Intr {
 // 5×5 median plane filter (the rule of crates/dense/src/upsample.rs:192-238 as the GPU kernel states it in
 // crates/cuda/src/kernels/patchmatch.cu:805-849): lower median of the depths the valid neighbour planes give on
 // this pixel's ray, ties by index; invalid pixels pass through.  Reads `in` (the scratch copy), writes `out`.
+// One thread per pixel over a 1-D grid (any image shape within the pixel limit fits the grid's x dimension).
 __global__ void __launch_bounds__(256) k_median_noalloc(const float4* __restrict__ in, float4* __restrict__ out, int w,
                                                         int h, Intr K) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y;
-  if (x >= w || y >= h) return;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (long long)w * h) return;
+  const int x = (int)(i % w), y = (int)(i / w);
   const float4 self = in[y * w + x];
   if (!(self.w > 0.f)) {
     out[y * w + x] = self;
@@ -90,17 +97,16 @@ __global__ void __launch_bounds__(256) k_median_noalloc(const float4* __restrict
 
 }  // namespace
 
-extern "C" int ps_median_filter_inplace_noalloc(int device, float* planes, uint32_t width, uint32_t height,
-                                                const float* k, void* stream) {
-  if (!planes || !k || width == 0 || height == 0) return PS_EINVAL;
-  if (((uintptr_t)planes & 15u) != 0) return PS_EINVAL;  // float4 planes
-  if ((uint64_t)width * height > PS_NOALLOC_MAX_PIXELS) return PS_EINVAL;
-  if (!(k[0] != 0.0f) || !(k[1] != 0.0f)) return PS_EINVAL;
-  if (device < 0 || device >= kMaxDevices) return PS_ENODEV;
-  if (cudaSetDevice(device) != cudaSuccess) {
-    cudaGetLastError();
-    return PS_ENODEV;
+namespace {
+
+// Runs the filter with `device` current (the caller restores its own current device).
+int median_noalloc_on(int device, float* planes, uint32_t width, uint32_t height, const float* k, void* stream) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, planes) != cudaSuccess) {
+    cudaGetLastError();  // the query's own error
+    return PS_EINVAL;
   }
+  if (!((a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == device)) return PS_EINVAL;
   float4* scratch = nullptr;
   {
     std::lock_guard<std::mutex> g(g_mu);
@@ -122,8 +128,34 @@ extern "C" int ps_median_filter_inplace_noalloc(int device, float* planes, uint3
   }
   Intr K;
   for (int i = 0; i < 4; ++i) K.k[i] = k[i];
-  const dim3 b(32, 8), g((width + 31) / 32, (height + 7) / 8);
-  k_median_noalloc<<<g, b, 0, st>>>(scratch, (float4*)planes, (int)width, (int)height, K);
+  k_median_noalloc<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(scratch, (float4*)planes, (int)width, (int)height, K);
   if (cudaGetLastError() != cudaSuccess) return PS_ECUDA;
   return PS_OK;
+}
+
+}  // namespace
+
+extern "C" int ps_median_filter_inplace_noalloc(int device, float* planes, uint32_t width, uint32_t height,
+                                                const float* k, void* stream) {
+  if (!planes || !k || width == 0 || height == 0) return PS_EINVAL;
+  if (((uintptr_t)planes & 15u) != 0) return PS_EINVAL;  // float4 planes
+  if ((uint64_t)width * height > PS_NOALLOC_MAX_PIXELS) return PS_EINVAL;
+  if (!(k[0] != 0.0f) || !(k[1] != 0.0f)) return PS_EINVAL;
+  if (device < 0 || device >= kMaxDevices) return PS_ENODEV;
+  if (cudaPeekAtLastError() != cudaSuccess) return PS_ECUDA;  // the caller's pending error stays pending
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  if (cudaSetDevice(device) != cudaSuccess) {
+    cudaGetLastError();
+    return PS_ENODEV;
+  }
+  const int rc = median_noalloc_on(device, planes, width, height, k, stream);
+  if (prev != device && cudaSetDevice(prev) != cudaSuccess) {
+    cudaGetLastError();
+    return rc == PS_OK ? PS_ECUDA : rc;
+  }
+  return rc;
 }

@@ -155,6 +155,9 @@ struct ps_backend {
     bool u8;
   };
   std::vector<CachedArray> arrays;
+  // host-side failure injection (ps_backend_inject_failure): kind and the successes left before the failure
+  uint32_t inject_kind = PS_INJECT_NONE;
+  uint32_t inject_after = 0;
 };
 
 struct ps_session {
@@ -262,10 +265,24 @@ int guard(ps_session* s, F&& f) {
   }
 }
 
+// An armed injected failure of `kind` (ps_backend_inject_failure): counts the operation down and fails it when the
+// count is spent, before anything is issued to the device.
+void maybe_inject(ps_session* s, uint32_t kind, const char* what) {
+  ps_backend* be = s->be;
+  if (!be || be->inject_kind != kind) return;
+  if (be->inject_after > 0) {
+    be->inject_after--;
+    return;
+  }
+  be->inject_kind = PS_INJECT_NONE;
+  fail(kind == PS_INJECT_DEVICE_ALLOC ? PS_ENOMEM : PS_ECUDA, std::string("injected failure: ") + what);
+}
+
 // Session device memory: from the backend's pool in the session stream's order (plain cudaMalloc when the device
 // offers no pool).  Every use of a buffer is on the session stream.
 template <typename T>
 T* dalloc(ps_session* s, size_t n) {
+  maybe_inject(s, PS_INJECT_DEVICE_ALLOC, "device allocation");
   void* p = nullptr;
   const size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
   if (s->be && s->be->pool) cuda_ok(cudaMallocFromPoolAsync(&p, bytes, s->be->pool, s->st), "cudaMallocFromPoolAsync");
@@ -492,6 +509,7 @@ void check_state(ps_session* s, int v, int level, const ps_view_state& st) {
 void upload_planes(ps_session* s, const uint32_t* views, size_t a, size_t b, const ps_view_state* states,
                    int level, bool with_prior, float4* dst_base = nullptr) {
   Slot& sl = slot(s, level);
+  maybe_inject(s, PS_INJECT_UPLOAD, "upload states");
   size_t total = 0;
   for (size_t i = a; i < b; ++i) total += (size_t)states[i].width * states[i].height;
   float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * sizeof(float4) * (with_prior ? 2 : 1));
@@ -592,11 +610,14 @@ void ensure_snapshot(ps_session* s, const ps_depth_snapshot* snap) {
   std::vector<long long> offs(s->nv, -1);
   size_t total = 0;
   for (int v = 0; v < s->nv; ++v) {
-    if ((uint32_t)v < snap->num_maps && snap->maps && snap->maps[v]) {
+    const uint64_t need = (uint64_t)s->W(v, l) * s->H(v, l);
+    if ((uint32_t)v < snap->num_maps && snap->maps && snap->maps[v] &&
+        (!snap->map_lengths || snap->map_lengths[v] == need)) {
       offs[v] = (long long)total;
-      total += (size_t)s->W(v, l) * s->H(v, l);
+      total += (size_t)need;
     }
   }
+  maybe_inject(s, PS_INJECT_UPLOAD, "upload snapshot");
   if (total > s->snap_cap) {
     realloc_snapshot(s, total);
   }
@@ -725,6 +746,14 @@ const char* ps_backend_last_error(const ps_backend* be) { return be ? be->err.c_
 const char* ps_last_error(const ps_session* s) { return s ? s->err.c_str() : "session is NULL"; }
 uint64_t ps_launch_count(const ps_session* s) { return s ? s->launches : 0; }
 
+int ps_backend_inject_failure(ps_backend* be, uint32_t kind, uint32_t after) {
+  if (!be || kind > PS_INJECT_UPLOAD) return PS_EINVAL;
+  std::lock_guard<std::mutex> g(be->mu);
+  be->inject_kind = kind;
+  be->inject_after = after;
+  return PS_OK;
+}
+
 int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
   if (!be || !in || !out) return PS_EINVAL;
   *out = nullptr;
@@ -833,6 +862,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
           memcpy(dst + (size_t)y * li.width, (const unsigned char*)li.pixels + y * stride, li.width);
       }
       d8 = dalloc<unsigned char>(s, u8_total + 256 * sizeof(float));
+      maybe_inject(s, PS_INJECT_UPLOAD, "upload 8-bit images");
       cuda_ok(cudaMemcpyAsync(d8, stage, u8_total + 256 * sizeof(float), cudaMemcpyHostToDevice, s->st),
               "upload 8-bit images");
     }
@@ -848,6 +878,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
                    "image plane kernel");
         } else {
           const size_t stride = li.stride ? li.stride : li.width;
+          maybe_inject(s, PS_INJECT_UPLOAD, "upload image");
           cuda_ok(cudaMemcpy2DAsync(dst, pitch * sizeof(float), li.pixels, stride * sizeof(float),
                                     li.width * sizeof(float), li.height, cudaMemcpyHostToDevice, s->st),
                   "upload image");

@@ -192,13 +192,16 @@ def c_snapshot(snap: Optional[DepthSnapshot], keep: list):
         return None
     n = len(snap.maps)
     maps = (FP * max(n, 1))()
+    lens = (C.c_uint64 * max(n, 1))()
     for v, m in enumerate(snap.maps):
         if m is not None:
             a = np.ascontiguousarray(m, np.float32)
             keep.append(a)
             maps[v] = _fptr(a)
+            lens[v] = a.size
     keep.append(maps)
-    s = _lib.DepthSnapshot(snap.id, snap.level, n, maps)
+    keep.append(lens)
+    s = _lib.DepthSnapshot(snap.id, snap.level, n, maps, C.cast(lens, C.POINTER(C.c_uint64)))
     keep.append(s)
     return C.byref(s)
 
@@ -245,6 +248,13 @@ class PatchMatchBackend:
         if rc != _lib.PS_OK:
             raise PsError(rc, self.lib.ps_backend_last_error(self.h).decode())
         return PatchMatchSession(self, s, inp)
+
+    def inject_failure(self, kind: int, after: int = 0) -> None:
+        """Arms one host-side failure (ps_backend_inject_failure): after `after` more operations of `kind`
+        (_lib.PS_INJECT_DEVICE_ALLOC or PS_INJECT_UPLOAD) succeed, the next one fails; PS_INJECT_NONE disarms."""
+        rc = self.lib.ps_backend_inject_failure(self.h, kind, after)
+        if rc != _lib.PS_OK:
+            raise PsError(rc, "ps_backend_inject_failure")
 
     def close(self):
         if self.h:

@@ -32,7 +32,7 @@ extern "C" {
 #endif
 
 #define PS_MAX_SOURCES 32 /* crates/cuda/src/kernels/patchmatch.cu:40 (MAXSRC) */
-#define PS_ABI_VERSION 3
+#define PS_ABI_VERSION 4
 
 /* Status codes.  Maps the reference's error kinds: Error::InvalidArgument -> PS_EINVAL,
  * Error::Invariant("CUDA: …") -> PS_ECUDA (crates/cuda/src/patchmatch.rs:234-236),
@@ -185,10 +185,24 @@ typedef struct ps_depth_snapshot {
   uint32_t level;
   uint32_t num_maps;
   const float* const* maps;
+  /* optional (NULL = every map has its level's width*height elements): the element count of every map; a map whose
+   * count differs from its level's width*height is left out of the snapshot, as the reference leaves it out
+   * (crates/cuda/src/patchmatch.rs:573-604, the Vec lengths of DepthSnapshot::maps) */
+  const uint64_t* map_lengths;
 } ps_depth_snapshot;
 
 typedef struct ps_backend ps_backend;
 typedef struct ps_session ps_session;
+
+/* ---- host-side failure injection (no counterpart in the reference; for tests of the error paths) ----------
+ * Arms one failure on the backend: after `after` more operations of `kind` succeed, the next one fails as a device
+ * would (PS_INJECT_DEVICE_ALLOC: a device allocation, reported as PS_ENOMEM; PS_INJECT_UPLOAD: a host-to-device copy
+ * of images, states or snapshots, reported as PS_ECUDA), then the injection disarms itself.  PS_INJECT_NONE disarms.
+ * Nothing reaches the GPU: the failing operation is refused on the host before it is issued. */
+#define PS_INJECT_NONE 0u
+#define PS_INJECT_DEVICE_ALLOC 1u
+#define PS_INJECT_UPLOAD 2u
+int ps_backend_inject_failure(ps_backend* be, uint32_t kind, uint32_t after);
 
 /* ---- defaults and diagnostics ------------------------------------------------------------------------------ */
 int ps_abi_version(void);
@@ -305,14 +319,17 @@ void* ps_session_stream(const ps_session* s);
 /* ---- allocation-free median filter (no counterpart in the reference) ---------------------------------------
  * For callers that own device buffers but may not allocate device memory (a host framework's memory pool owns every
  * allocation, a fixed budget forbids growth after start-up, or a real-time loop must not allocate).  Filters the
- * caller's planes in place: `planes` is device memory, 16-byte aligned, width*height float4 (nx, ny, nz, d), and
- * k = fx, fy, cx, cy of the image.  Same rule and same bits as ps_median_filter.  Instead of a session buffer, the
- * input copy lives in a static device array of PS_NOALLOC_MAX_PIXELS planes (32 MiB, reserved on every GPU that
- * loads the library until exit); larger images are rejected with PS_EINVAL.  No cudaMalloc or cudaFree is called.
- * All calls on a device share that array and it keeps the last call's contents (a call reads only what it copied,
- * so nothing needs clearing); calls that overlap on the GPU race on it.  The first call on a device looks up the
- * array's address with that device current; make it before any stream capture.  Asynchronous on `stream`
- * (a cudaStream_t, NULL = default stream). */
+ * caller's planes in place: `planes` is device (or managed) memory of `device`, 16-byte aligned, width*height float4
+ * (nx, ny, nz, d), and k = fx, fy, cx, cy of the image; other pointers are rejected with PS_EINVAL before any device
+ * work.  Same rule as ps_median_filter, and the same bits as the median filter of a parity-math session.  Instead of
+ * a session buffer, the input copy lives in a static device array of PS_NOALLOC_MAX_PIXELS planes (32 MiB, reserved
+ * on every GPU that loads the library until exit); larger images are rejected with PS_EINVAL.  No cudaMalloc or
+ * cudaFree is called.  All calls on a device share that array and it keeps the last call's contents (a call reads
+ * only what it copied, so nothing needs clearing); calls that overlap on the GPU race on it.  The first call on a
+ * device looks up the array's address with that device current; make it before any stream capture; the address is
+ * kept, so it is stale after the caller resets that device.  The caller's current device is restored before the
+ * call returns.  While the calling thread has a CUDA error pending the call does nothing and returns PS_ECUDA,
+ * leaving that error pending.  Asynchronous on `stream` (a cudaStream_t, NULL = default stream). */
 #define PS_NOALLOC_MAX_PIXELS (1u << 21)
 int ps_median_filter_inplace_noalloc(int device, float* planes, uint32_t width, uint32_t height, const float* k,
                                      void* stream);

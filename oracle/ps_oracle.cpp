@@ -759,6 +759,8 @@ std::vector<std::vector<float>> snapshot_maps(const Scene& sc, const ps_depth_sn
   for (size_t v = 0; v < sc.v.size(); ++v)
     if (v < snap->num_maps && snap->maps && snap->maps[v]) {
       const Img& L = sc.L((int)v, (int)snap->level);
+      // a map of another size is left out (crates/cuda/src/patchmatch.rs:573-604)
+      if (snap->map_lengths && snap->map_lengths[v] != (uint64_t)L.w * L.h) continue;
       m[v].assign(snap->maps[v], snap->maps[v] + (size_t)L.w * L.h);
     }
   return m;

@@ -21,16 +21,23 @@ from cumulus3d_b200.patchstereo import KernelInput, KernelView, LevelImage, Patc
 pytestmark = pytest.mark.gpu
 
 
-def _noalloc(planes_dev: torch.Tensor, w: int, h: int, k) -> int:
+def _noalloc(planes_dev, w: int, h: int, k, stream=None) -> int:
     kk = (C.c_float * 4)(*[float(x) for x in k])
-    return _lib.engine().ps_median_filter_inplace_noalloc(0, C.c_void_p(planes_dev.data_ptr()), w, h, kk, None)
+    ptr = planes_dev.data_ptr() if isinstance(planes_dev, torch.Tensor) else planes_dev
+    return _lib.engine().ps_median_filter_inplace_noalloc(0, C.c_void_p(ptr), w, h, kk,
+                                                          None if stream is None else C.c_void_p(stream))
 
 
-def _run_noalloc(state: ViewState, k) -> ViewState:
+def _run_noalloc(state: ViewState, k, stream: "torch.cuda.Stream" = None) -> ViewState:
     planes = np.ascontiguousarray(state.planes(), np.float32)
     dev = torch.from_numpy(planes).cuda()
-    assert _noalloc(dev, state.width, state.height, k) == _lib.PS_OK
     torch.cuda.synchronize()
+    if stream is None:
+        assert _noalloc(dev, state.width, state.height, k) == _lib.PS_OK
+        torch.cuda.synchronize()
+    else:
+        assert _noalloc(dev, state.width, state.height, k, stream.cuda_stream) == _lib.PS_OK
+        stream.synchronize()
     out = dev.cpu().numpy()
     res = state.copy()
     res.normal[...] = out[..., :3]
@@ -50,6 +57,46 @@ def test_noalloc_median_equals_session_median_twice():
         got = _run_noalloc(states[v], wl.cams[v].k)
         np.testing.assert_array_equal(got.depth, want[v].depth)
         np.testing.assert_array_equal(got.normal, want[v].normal)
+    # on a stream of the caller's own (ordered after that stream's earlier work), twice in a row
+    side = torch.cuda.Stream()
+    for v in (2, 1):
+        got = _run_noalloc(states[v], wl.cams[v].k, side)
+        np.testing.assert_array_equal(got.depth, want[v].depth)
+        np.testing.assert_array_equal(got.normal, want[v].normal)
+
+
+def test_noalloc_rejects_memory_it_cannot_filter():
+    """Host memory (or memory of another device) is rejected before any device work, and the caller's current device
+    is unchanged afterwards."""
+    w, h = 16, 8
+    k = (20.0, 20.0, 7.5, 3.5)
+    host = np.zeros((h, w, 4), np.float32)
+    dev_before = torch.cuda.current_device()
+    assert _noalloc(host.ctypes.data, w, h, k) == _lib.PS_EINVAL
+    assert torch.cuda.current_device() == dev_before
+    dev = torch.zeros((h, w, 4), dtype=torch.float32, device="cuda")
+    assert _noalloc(dev, w, h, k) == _lib.PS_OK
+    torch.cuda.synchronize()
+    assert torch.cuda.current_device() == dev_before
+
+
+def test_noalloc_tall_image():
+    """A two-column image taller than a session accepts (sessions take sides up to 32768) and taller than 65535
+    blocks of 8 rows: the entry point's one-dimensional launch covers it.  The reference is the CPU restatement of the
+    median filter, which the parity tests hold equal to the session's."""
+    from oracle import oracle
+    w, h = 2, 1 << 20
+    k = (500.0, 500.0, 0.5, h / 2.0)
+    s = ViewState.new(w, h)
+    rng = np.random.default_rng(3)
+    n = rng.normal(0.0, 0.1, (h, w, 3)).astype(np.float32) + np.float32([0.0, 0.0, -1.0])
+    s.normal[...] = n / np.linalg.norm(n, axis=-1, keepdims=True)
+    s.depth[...] = rng.uniform(25.0, 60.0, (h, w)).astype(np.float32)
+    inp = KernelInput([KernelView(1, [LevelImage(np.zeros((h, w), np.float32), k)], [], [], 20.0, 80.0)], 1)
+    want = oracle.median(inp, 0, [0], [s])[0]
+    got = _run_noalloc(s, k)
+    np.testing.assert_array_equal(got.depth, want.depth)
+    np.testing.assert_array_equal(got.normal, want.normal)
 
 
 def test_noalloc_median_full_hd_and_size_limit():

@@ -151,6 +151,7 @@ def bench_ours(args, rank, world, local):
         mine = list(range(len(wl.cams)))
     wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
     tuned = None
+    args.tuning_was_auto = args.tuning < 0
     if args.tuning < 0:  # autotune the half-step variant on a prefix of this job's views (outside the timed region)
         from cumulus3d_b200.autotune import tune
         tuned = tune(wl.input, local, args.math, views=mine)
@@ -257,6 +258,11 @@ def bench_ours(args, rank, world, local):
     res["hbm_high_water_gb"] = round(max(hbm) / 1e9, 2)
     if not shard_job:
         res["fusion_all_options"] = fusion_options_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
+    if not args.no_c3 and args.workload == "c2" and not shard_job:
+        try:  # an error in this leg is reported in the line instead of ending the run
+            res["c3"] = c3_leg(args, local, fp32_peak, check=rank == 0 and not args.no_check)
+        except Exception as e:  # noqa: BLE001
+            res["c3"] = {"error": f"{type(e).__name__}: {e}"}
         try:  # an error in this leg is reported in the line instead of ending the run
             res["score_fusion"] = score_fusion_stage(wl, sess, mine, check=rank == 0 and not args.no_check)
         except Exception as e:  # noqa: BLE001
@@ -274,6 +280,78 @@ def bench_ours(args, rank, world, local):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+    return res
+
+
+def c3_leg(args, local, fp32_peak, check=True, subset_per_size=2):
+    """The batched uneven workload (64 views of 4 sizes from 4 terrains, 2-8 sources each) in one session: one
+    warm-up schedule (graph capture), one timed schedule (CUDA events on the session stream), the half step's
+    roofline, and a bitwise check of the ragged batching: a subset with `subset_per_size` views of every size runs
+    once with all views in each launch and once with one view per launch, in fresh sessions; the maps must agree."""
+    import torch
+    from cumulus3d_b200 import _lib, scenes
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    t0 = time.time()
+    wl = scenes.workload_c3(seed=3)
+    gen_s = time.time() - t0
+    tuning = args.tuning
+    tuned = None
+    if getattr(args, "c3_tuning", -1) >= 0:
+        tuning = args.c3_tuning
+    elif args.tuning_was_auto:
+        from cumulus3d_b200.autotune import tune
+        tuned = tune(wl.input, local, args.math)
+        tuning = tuned["tuning"]
+    views = list(range(len(wl.cams)))
+    wn = 2 * wl.input.pm.window_radius // wl.input.pm.window_step + 1
+    be = PatchMatchBackend(local, math=args.math, tuning=tuning)
+    sess = be.begin(wl.input)
+    stream = torch.cuda.ExternalStream(sess.stream(), device=local)
+    sess.set_profiling(True)
+    run = lambda: sess.schedule_resident(views, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters)
+    run()
+    sess.synchronize()
+    sess.reset_stats()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    run()
+    e1.record(stream)
+    sess.synchronize()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    half = sess.kernel_stats(_lib.PS_KERNEL_HALF)
+    sess.close()
+    half_ms = half["ms"] / max(half["launches"], 1)
+    taps = half["ncc_windows"] * wn * wn / max(half["launches"], 1)
+    achieved = taps * FLOP_PER_TAP_CACHED / (half_ms / 1e3) / 1e12
+    res = {"workload": wl.name, "views": len(views), "megapixels": round(wl.pixels() / 1e6, 2),
+           "sizes": sorted({f"{c.width}x{c.height}" for c in wl.cams}),
+           "sources": sorted({len(v.sources) for v in wl.input.views}),
+           "iterations": f"{wl.photometric_iters} photometric + {wl.geometric_rounds}x{wl.geometric_iters} geometric",
+           "value": round(len(views) / (ms / 1e3), 3), "unit": "views/s", "ms_per_step": round(ms, 2),
+           "timed_steps": 1, "warmup": 1, "tuning": tuning,
+           "autotune": None if tuned is None else {"half_ms": tuned["ms"], "cached": tuned["cached"], "key": tuned["key"]},
+           "roofline": {"bound": "fp32", "kernel": "k_half", "achieved": round(achieved, 3), "peak": round(fp32_peak, 2),
+                        "unit": "TFLOP/s", "frac": round(achieved / fp32_peak, 4), "launch_ms": round(half_ms, 3)},
+           "scene_s": round(gen_s, 1)}
+    if check:
+        sizes = {}
+        for v in views:
+            sizes.setdefault((wl.cams[v].width, wl.cams[v].height), []).append(v)
+        sub = sorted(v for vs in sizes.values() for v in vs[:subset_per_size])
+        maps = []
+        for mb in (64, 1):
+            b2 = PatchMatchBackend(local, math=args.math, tuning=tuning, max_batch=mb)
+            with b2.begin(wl.input) as s2:
+                s2.schedule_resident(sub, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters)
+                maps.append(s2.readout_download(0, sub))
+            b2.close()
+        equal = all(np.array_equal(a.depth, b.depth) and np.array_equal(a.normal, b.normal) and
+                    np.array_equal(a.cost, b.cost) for a, b in zip(*maps))
+        res["batch_check"] = {"views": sub, "equal": bool(equal),
+                              "what": "the subset batched into every launch vs one view per launch (max_batch 1), "
+                                      "fresh sessions, depth/normal/cost bitwise"}
+    be.close()
     return res
 
 
@@ -481,7 +559,7 @@ def net_flop_per_pixel():
 def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, local):
     """The learned-init schedule on the same resident session: ps_propose (plane sweep + proposal network + decode)
     then the schedule with `--learned-iters` photometric iterations from the proposals (random init where the
-    confidence is below 0.5), the same geometric round, filter and readout.  Timed like the plain step; accuracy is
+    confidence is below 0.5), a geometric round of `--learned-geo-iters` iterations, filter and readout.  Timed like the plain step; accuracy is
     the agreement of the final filtered depth with the plain schedule's (within 1 % depth on the pixels the plain
     result keeps), next to the plain schedule's agreement with itself under another RNG seed and to a plain schedule
     shortened to the same iteration count."""
@@ -491,6 +569,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     proposal.set_conv_path(args.conv_path)
     net = proposal.ProposalNet(local, weights=args.weights or proposal.DEFAULT_WEIGHTS)
     k = args.learned_iters
+    gi = args.learned_geo_iters
     # final depth maps of every view, flattened into one vector (views may differ in size)
     plain_depth = np.concatenate([o.depth.ravel() for o in sess.readout_resident(mine)])  # the last plain step's
 
@@ -512,8 +591,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
 
     def learned_step():
         sess.propose(net, 0, mine, proposal.CONF_THRESHOLD, count=False)
-        sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters, graph=not args.no_graph,
-                               proposal=True)
+        sess.schedule_resident(mine, k, wl.geometric_rounds, gi, graph=not args.no_graph, proposal=True)
 
     sess.set_profiling(True)  # per-launch events for the sweep and network shares
     sess.reset_stats()
@@ -523,8 +601,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     sess.set_profiling(False)
     learned_depth = depth()
     learned_fused = fusion_stage(args, wl, sess, mine, check=False)["points"]
-    ms_short = timed(lambda: sess.schedule_resident(mine, k, wl.geometric_rounds, wl.geometric_iters,
-                                                     graph=not args.no_graph), 1, 2)
+    ms_short = timed(lambda: sess.schedule_resident(mine, k, wl.geometric_rounds, gi, graph=not args.no_graph), 1, 2)
     short_depth = depth()
     short_fused = fusion_stage(args, wl, sess, mine, check=False)["points"]
     sess.schedule_resident(mine, wl.photometric_iters, wl.geometric_rounds, wl.geometric_iters, run_id_base=101,
@@ -546,7 +623,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
     n = len(mine)
     return {
         "schedule": f"propose (plane sweep + network + decode) + {k} photometric from the proposal + "
-                    f"{wl.geometric_rounds}x{wl.geometric_iters} geometric + filter",
+                    f"{wl.geometric_rounds}x{gi} geometric + filter",
         "value": round(n / (ms_learned / 1e3), 3), "unit": "views/s", "ms_per_step": round(ms_learned, 2),
         "vs_plain": round(ms_step_ratio(plain_ms, ms_learned), 3),
         "propose_ms_per_view": round((net_stats["ms"] + sweep_stats["ms"]) / max(net_stats["launches"], 1), 3),
@@ -791,10 +868,14 @@ def main():
     ap.add_argument("--no-check", action="store_true",
                     help="skip the CPU oracle checks (fused point count, FP64 re-evaluation)")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-init schedule")
+    ap.add_argument("--no-c3", action="store_true", help="skip the batched uneven (64 mixed views) leg")
+    ap.add_argument("--c3-tuning", type=int, default=-1, help="half-step variant of the c3 leg; -1 = autotune")
     ap.add_argument("--weights", default=None, help="proposal network parameters (.npz; default: the committed ones)")
     ap.add_argument("--conv-path", default="auto", choices=["auto", "mma", "tcgen05"],
                     help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
-    ap.add_argument("--learned-iters", type=int, default=3,
+    ap.add_argument("--learned-geo-iters", type=int, default=1,
+                    help="iterations of the learned schedule's geometric round (the plain schedule's is 2)")
+    ap.add_argument("--learned-iters", type=int, default=1,
                     help="photometric iterations of the learned-init schedule")
     ap.add_argument("--no-whole-view", action="store_true",
                     help="reference arm: skip the single whole-view timing of the CPU oracle")

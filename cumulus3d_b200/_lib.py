@@ -28,8 +28,8 @@ class Options(C.Structure):
 
 
 PS_TUNE_NO_WEIGHT_CACHE, PS_TUNE_TEX_GATHER, PS_TUNE_ONE_LANE = 0x1, 0x2, 0x4
-PS_TUNE_ROW_PAIRS, PS_TUNE_STAGED = 0x8, 0x10
-PS_INJECT_NONE, PS_INJECT_DEVICE_ALLOC, PS_INJECT_UPLOAD = 0, 1, 2
+PS_TUNE_ROW_PAIRS, PS_TUNE_STAGED, PS_TUNE_PERSISTENT, PS_TUNE_TMA = 0x8, 0x10, 0x20, 0x40
+PS_INJECT_NONE, PS_INJECT_DEVICE_ALLOC, PS_INJECT_UPLOAD, PS_INJECT_CHECK_PROBE, PS_INJECT_QUEUE_STALL = 0, 1, 2, 3, 4
 PS_KERNEL_HALF, PS_KERNEL_EVAL, PS_KERNEL_FILTER, PS_KERNEL_OTHER, PS_KERNEL_SWEEP, PS_KERNEL_NET = range(6)
 PS_KERNEL_KINDS = 6
 

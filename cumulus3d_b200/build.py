@@ -1,7 +1,8 @@
 """Builds the native libraries in-tree.
 
-* ``cumulus3d_b200/libpatchstereo.so`` — the engine: CUDA kernels for sm_100a (parity and fast builds of the same
-  source) + the host runtime and C ABI (include/patchstereo.h).  CUDA runtime linked statically; no PyTorch.
+* ``cumulus3d_b200/libpatchstereo.so`` — the engine: CUDA kernels for sm_100a (parity, fast and bounds-checked
+  builds of the same source) + the host runtime and C ABI (include/patchstereo.h).  CUDA runtime linked statically;
+  no PyTorch.
 * ``cumulus3d_b200/libps_synth.so`` — the synthetic scene renderer (host code).
 * ``oracle/_build/libps_oracle.so`` — the CPU oracle (test infrastructure), via oracle/Makefile.
 
@@ -49,6 +50,7 @@ def build_engine(force: bool = False, verbose: bool = False) -> pathlib.Path:
     specs = [
         ("k_parity.o", CSRC / "ps_kernels.cu", PARITY),
         ("k_fast.o", CSRC / "ps_kernels.cu", FAST),
+        ("k_checked.o", CSRC / "ps_kernels.cu", PARITY + ["-DPS_CHECKED=1"]),
         ("runtime.o", CSRC / "ps_runtime.cu", ["-Xcompiler", "-fopenmp"]),
         ("noalloc.o", CSRC / "ps_noalloc.cu", PARITY),
         ("cnn.o", CSRC / "ps_cnn.cu", []),

@@ -1,11 +1,14 @@
 // PatchStereo kernels for sm_100a.
 //
-// Compiled twice into libpatchstereo.so:
+// Compiled three times into libpatchstereo.so:
 //   PS_FAST=0 (namespace ps_parity): --fmad=false, IEEE division and square root, the project's own exp/sincos
 //            (ps_fmath.h) and fma only where written out.  Bitwise equal to the CPU oracle (oracle/ps_oracle.cpp),
 //            which follows the same operation sequence.
 //   PS_FAST=1 (namespace ps_fast):   --use_fast_math, hardware reciprocal / exp / rsqrt in the hot loops
 //            ("the kernel may use approximate division and exponential", crates/dense/src/kernel.rs:73-74).
+//   PS_CHECKED=1 (namespace ps_checked): the parity build plus bounds tests on every data-dependent index (tile,
+//            staged box, source plane, state arrays, source view, snapshot); a failed test skips the access and
+//            records the first violation in PsRun.fault (see PsCheckSite), which the runtime reports as PS_EFAULT.
 //
 // The rules are those of the reference kernel crates/cuda/src/kernels/patchmatch.cu (cited per function) and of
 // crates/dense/src/kernel.rs:36-74.  The B200 layout differs from the reference:
@@ -21,6 +24,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <algorithm>
 #include "ps_fmath.h"
 #include "ps_pairs.h"
 #include "ps_types.h"
@@ -28,8 +32,16 @@
 #ifndef PS_FAST
 #define PS_FAST 0
 #endif
+#ifndef PS_CHECKED
+#define PS_CHECKED 0
+#endif
+#if PS_FAST && PS_CHECKED
+#error "the bounds-checked build uses the parity math"
+#endif
 #if PS_FAST
 #define PS_NS ps_fast
+#elif PS_CHECKED
+#define PS_NS ps_checked
 #else
 #define PS_NS ps_parity
 #endif
@@ -37,6 +49,26 @@
 typedef unsigned long long u64;
 
 namespace PS_NS {
+
+// ------------------------------------------------------------------------------------------- bounds tests
+// PS_IN(fault, site, idx, lo, hi): lo <= idx < hi.  In the checked build a failure records (site, idx) once per launch
+// (the first failure wins) and the caller skips the access; in the other builds the test is absent (true, and the
+// arguments are not evaluated).
+#if PS_CHECKED
+__device__ __noinline__ void chk_record(unsigned long long* fault, unsigned site, long long idx) {
+  if (fault)
+    atomicCAS(fault, 0ull, ((unsigned long long)site << 56) | ((unsigned long long)idx & 0x00FFFFFFFFFFFFFFull));
+}
+__device__ __forceinline__ bool chk_in(unsigned long long* fault, unsigned site, long long idx, long long lo,
+                                       long long hi) {
+  if (idx >= lo && idx < hi) return true;
+  chk_record(fault, site, idx);
+  return false;
+}
+#define PS_IN(fault, site, idx, lo, hi) chk_in((fault), (site), (long long)(idx), (long long)(lo), (long long)(hi))
+#else
+#define PS_IN(fault, site, idx, lo, hi) true
+#endif
 
 // ------------------------------------------------------------------------------------------- math policy
 __device__ __forceinline__ float m_rcp(float x) {
@@ -117,11 +149,18 @@ __device__ __forceinline__ int f2i_exact(float v) {
   return __float_as_int(v + 12582912.0f) - 0x4B400000;
 }
 __device__ __forceinline__ float src_sample(const float* __restrict__ img, int pitch, float wf, float hf, float u,
-                                            float v) {
+                                            float v, unsigned long long* fault = nullptr) {
   float xf = floorf(u), yf = floorf(v);
   float ax = u - xf, ay = v - yf;
   float xc = fminf(fmaxf(xf, -2.0f), wf);
   float yc = fminf(fmaxf(yf, -2.0f), hf);
+#if PS_CHECKED
+  // the 2 × 2 footprint inside the bordered plane: columns [-PS_BORDER, pitch - PS_BORDER), rows [-PS_BORDER,
+  // h + PS_BORDER)
+  if (!PS_IN(fault, PS_SITE_PLANE, f2i_exact(xc), -PS_BORDER, pitch - PS_BORDER - 1) ||
+      !PS_IN(fault, PS_SITE_PLANE, f2i_exact(yc), -PS_BORDER, (int)hf + PS_BORDER - 1))
+    return 0.f;
+#endif
   const float* p = img + f2i_exact(yc) * pitch + f2i_exact(xc);
   float p00 = __ldg(p), p10 = __ldg(p + 1), p01 = __ldg(p + pitch), p11 = __ldg(p + pitch + 1);
   float top = fmaf(ax, p10 - p00, p00);
@@ -172,7 +211,28 @@ struct RefWin {
   int g;
   unsigned pmask;
   float* wl;
+#if PS_CHECKED
+  const float* tbase;  // the tile and its size in floats
+  int tn;
+  unsigned long long* fault;
+#endif
 };
+
+// Bounds of the tile a RefWin reads (checked build only).
+__device__ __forceinline__ void refwin_bounds(RefWin& rw, const float* tile, int n, const PsRun& P) {
+#if PS_CHECKED
+  rw.tbase = tile;
+  rw.tn = n;
+  rw.fault = P.fault;
+#endif
+}
+// Reference intensity at p inside the tile.
+__device__ __forceinline__ float tile_at(const RefWin& rw, const float* p) {
+#if PS_CHECKED
+  if (!PS_IN(rw.fault, PS_SITE_TILE, p - rw.tbase, 0, rw.tn)) return 0.f;
+#endif
+  return *p;
+}
 
 // Row-parity partial sums -> total (even + odd; IEEE addition is commutative, so both lanes get the same bits).
 template <int G>
@@ -191,7 +251,7 @@ __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) 
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
   RefStats s;
-  s.ic = rw.t[0];
+  s.ic = tile_at(rw, rw.t);
   float W[2] = {0.f, 0.f}, S[2] = {0.f, 0.f}, SS[2] = {0.f, 0.f};
 #pragma unroll 1
   for (int a = (G == 2 ? rw.g : 0); a < wn; a += G) {
@@ -212,7 +272,7 @@ __device__ __forceinline__ RefStats ref_stats(const PsRun& P, const RefWin& rw) 
     }
     auto tap = [&](int b) {
       const int dx = -wr + b * ws;
-      float ik = trow[dx];
+      float ik = tile_at(rw, trow + dx);
       float d = s.ic - ik;
       float w = m_exp(-(float)(dx * dx + dy * dy) * P.inv2s - d * d * P.inv2c);
       if (CW) wrow[b * wst] = w;
@@ -312,7 +372,7 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
                          fmaf(H[6], sx0, rz1) > 1e-8f && fmaf(H[6], sx1, rz1) > 1e-8f;
   auto sample = [&](float uf, float vf) {
     if constexpr (TEX) return src_sample_tex(tex, uf, vf);
-    else return src_sample(img, pitch, wf, hf, uf, vf);
+    else return src_sample(img, pitch, wf, hf, uf, vf, P.fault);
   };
   auto accumulate = [&](int pa, float w, float sv, float ik) {
     const float wsv = w * sv;
@@ -349,7 +409,7 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
       auto tap = [&](int b) {
         const int dx = -wr + b * ws;
         const float sx = fx + (float)dx;
-        const float ik = trow[dx];
+        const float ik = tile_at(rw, trow + dx);
         const float w = weight(wrow, wst, b, dx, dy, ik);
         const float izz = m_rcp(fmaf(H[6], sx, rz));
         accumulate(pa, w, sample(fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz), ik);
@@ -378,7 +438,7 @@ __device__ __forceinline__ float ncc_window(const PsRun& P, const RefWin& rw, co
       for (int b = 0; b < wn; ++b) {
         const int dx = -wr + b * ws;
         const float sx = fx + (float)dx;
-        const float ik = trow[dx];
+        const float ik = tile_at(rw, trow + dx);
         const float w = weight(wrow, wst, b, dx, dy, ik);
         // the reciprocal is replaced by 0 behind the camera so the discarded fetch coordinates stay finite
         const float zz = fmaf(H[6], sx, rz);
@@ -412,7 +472,28 @@ enum { SMP_LOAD = 0, SMP_TEX = 1, SMP_BOX = 2 };
 struct BoxRef {
   unsigned sbase;  // shared address of the box minus 4·(P + 1)·bits(1.5·2^23), mod 2^32
   float mx, my;
+#if PS_CHECKED
+  unsigned box;  // shared address of the box
+  unsigned long long* fault;
+#endif
 };
+// A BoxRef for the samplers that do not read a box (plane loads, texture).
+__device__ __forceinline__ BoxRef no_box(const PsRun& P) {
+  BoxRef b{0u, 0.f, 0.f};
+#if PS_CHECKED
+  b.box = 0u;
+  b.fault = P.fault;
+#endif
+  return b;
+}
+// Checked build: the box texel q (byte address) and its 2 × 2 footprint inside the box.
+__device__ __forceinline__ bool box_in(const BoxRef& bx, unsigned q) {
+#if PS_CHECKED
+  return PS_IN(bx.fault, PS_SITE_BOX, (long long)((q - bx.box) >> 2), 0, PS_BOX_P * PS_BOX_H - PS_BOX_P - 1);
+#else
+  return true;
+#endif
+}
 
 // Reciprocal of a pair given nz = -z: m_rcp lane by lane (rcp.approx, then the FMA correction as pair operations).
 __device__ __forceinline__ float2 m_rcp2(float2 nz) {
@@ -454,6 +535,9 @@ __device__ __forceinline__ float2 sample_pair(const PsLevel& S, const BoxRef& bx
     // byte address = base + 4·(bits(Fv)·P + bits(Fu)) with the constant part folded into bx.sbase
     const unsigned qa = (unsigned)__float_as_int(fv.x) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu.x);
     const unsigned qb = (unsigned)__float_as_int(fv.y) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu.y);
+#if PS_CHECKED
+    if (!box_in(bx, qa) || !box_in(bx, qb)) return make_float2(0.f, 0.f);
+#endif
     const float2 p00 = make_float2(lds(qa), lds(qb));
     const float2 p10 = make_float2(lds_off<4>(qa), lds_off<4>(qb));
     const float2 p01 = make_float2(lds_off<4 * PS_BOX_P>(qa), lds_off<4 * PS_BOX_P>(qb));
@@ -462,11 +546,17 @@ __device__ __forceinline__ float2 sample_pair(const PsLevel& S, const BoxRef& bx
     const float2 bot = v_fma(ax, v_sub(p11, p01), p01);
     return v_fma(ay, v_sub(bot, top), top);
   } else if constexpr (SMP == SMP_TEX) {
-    // scalar per lane: the gather's four texels feed the bilinear directly (no repacking into pairs)
+    // scalar per lane: the gather's four texels feed the bilinear directly (no repacking into pairs); floorf, not the
+    // FMA-pipe add.rm floor of the box path, which measured 5 % slower here (more registers in the unrolled loop)
     return make_float2(src_sample_tex(S.tex, u.x, v.x), src_sample_tex(S.tex, u.y, v.y));
   } else {
-    return make_float2(src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.x, v.x),
-                       src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.y, v.y));
+#if PS_CHECKED
+    unsigned long long* const fault = bx.fault;
+#else
+    unsigned long long* const fault = nullptr;
+#endif
+    return make_float2(src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.x, v.x, fault),
+                       src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u.y, v.y, fault));
   }
 }
 
@@ -476,6 +566,9 @@ __device__ __forceinline__ float sample_one(const PsLevel& S, const BoxRef& bx, 
     const float fu = __fadd_rd(u, bx.mx), fv = __fadd_rd(v, bx.my);
     const float ax = u - (fu - bx.mx), ay = v - (fv - bx.my);
     const unsigned q = (unsigned)__float_as_int(fv) * (4u * PS_BOX_P) + bx.sbase + 4u * (unsigned)__float_as_int(fu);
+#if PS_CHECKED
+    if (!box_in(bx, q)) return 0.f;
+#endif
     const float p00 = lds(q), p10 = lds_off<4>(q), p01 = lds_off<4 * PS_BOX_P>(q), p11 = lds_off<4 * PS_BOX_P + 4>(q);
     const float top = fmaf(ax, p10 - p00, p00);
     const float bot = fmaf(ax, p11 - p01, p01);
@@ -483,7 +576,11 @@ __device__ __forceinline__ float sample_one(const PsLevel& S, const BoxRef& bx, 
   } else if constexpr (SMP == SMP_TEX) {
     return src_sample_tex(S.tex, u, v);
   } else {
+#if PS_CHECKED
+    return src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u, v, bx.fault);
+#else
     return src_sample(S.img, S.pitch, (float)S.w, (float)S.h, u, v);
+#endif
   }
 }
 
@@ -509,7 +606,7 @@ __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefSta
     const float* wp = rw.wc + p * wn * NT * 2;
     auto tap = [&](int dx, float sxf, const float* wq) {
       const float2 sx = v_splat(sxf);
-      const float2 ik = make_float2(t0[dx], t1[dx]);
+      const float2 ik = make_float2(tile_at(rw, t0 + dx), tile_at(rw, t1 + dx));
       const float2 w = *reinterpret_cast<const float2*>(wq);
       const float2 izz = m_rcp2(v_fma(nh6, sx, nrz));
       const float2 sv = sample_pair<SMP>(S, bx, v_mul(v_fma(h0, sx, rx), izz), v_mul(v_fma(h3, sx, ry), izz));
@@ -540,7 +637,7 @@ __device__ __forceinline__ float ncc_window_pairs(const RefWin& rw, const RefSta
     const float rx = fmaf(H[1], sy, H[2]), ry = fmaf(H[4], sy, H[5]), rz = fmaf(H[7], sy, H[8]);
     const float* t0 = rw.t + dy * rw.tw;
     auto tap = [&](int b, int dx, float sx) {
-      const float ik = t0[dx];
+      const float ik = tile_at(rw, t0 + dx);
       const float w = rw.wl[b * NT];
       const float izz = m_rcp(fmaf(H[6], sx, rz));
       const float sv = sample_one<SMP>(S, bx, fmaf(H[0], sx, rx) * izz, fmaf(H[3], sx, ry) * izz);
@@ -582,14 +679,59 @@ __device__ __forceinline__ float ncc_window_lane(const PsRun& P, const RefWin& r
                                                  const PsLevel& S, const float* H, int x, int y) {
   constexpr int smp = TEX ? SMP_TEX : SMP_LOAD;
   if (window_front<WR>(H, (float)x, (float)y))
-    return ncc_window_pairs<WR, WS, NT, smp, true>(rw, rs, S, H, x, y, BoxRef{0u, 0.f, 0.f});
+    return ncc_window_pairs<WR, WS, NT, smp, true>(rw, rs, S, H, x, y, no_box(P));
   return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
 }
+
+// ------------------------------------------------------------------------------------------- TMA staging
+// Tensor maps (built by the runtime for PS_TUNE_TMA) describe each bordered image plane as a 2-D f32 tensor of
+// pitch × (h + 2·PS_BORDER) elements whose origin is the plane's allocation (texel (-PS_BORDER, -PS_BORDER)), so a
+// texel (X, Y) is element (X + PS_BORDER, Y + PS_BORDER); elements outside the tensor read 0, like the border.  Per
+// (view, level) the table holds two maps: the reference tile box (PsRun.tma_tile_w × PS_HALF_PH + 2·wr) and the
+// source box (PS_BOX_P × PS_BOX_H).  Loads are plain 2-D tiled loads into this CTA's shared memory (no multicast),
+// completed on an mbarrier with a byte count.
+__device__ __forceinline__ const void* tmap(const PsRun& P, int view, int which) {
+  return (const unsigned char*)P.tmaps + ((size_t)(view * P.nlevels + P.level) * 2 + which) * 128;
+}
+__device__ __forceinline__ void mbar_init(unsigned bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+}
+// One thread: expect `bytes` on the barrier and start the 2-D load of the box at element (x, y) (x·4 must be a
+// multiple of 16) into shared memory at dst (128-byte aligned).
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const void* map, int x, int y, unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+// Bounded wait for the barrier's phase `parity` to complete.  After PS_TMA_SPIN_LIMIT polls the error word (when
+// set) is marked, the wait is repeated once more with the same bound (the copy may still land), and false returns;
+// the caller's data is then unreliable and the run reports PS_ETIMEOUT.
+#define PS_TMA_SPIN_LIMIT (1u << 20)
+__device__ __forceinline__ bool mbar_wait(const PsRun& P, unsigned bar, unsigned parity) {
+  for (int round = 0; round < 2; ++round) {
+    for (unsigned i = 0; i < PS_TMA_SPIN_LIMIT; ++i) {
+      unsigned done;
+      asm volatile(
+          "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+          : "=r"(done)
+          : "r"(bar), "r"(parity)
+          : "memory");
+      if (done) return round == 0;
+    }
+    if (round == 0 && P.queue) atomicCAS(P.queue + 1, 0u, 2u);
+  }
+  return false;
+}
+// Shared-memory reads of a buffer made by the generic proxy are ordered before a following TMA write into it.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // What the warp's box holds: texels [ox, ox + PS_BOX_P) × [oy, oy + PS_BOX_H) of the plane at src (warp-uniform).
 struct BoxState {
   const float* src;
   int ox, oy;
+  unsigned bar, phase;  // TMA staging: the warp's mbarrier (shared address) and its next phase parity
   // profiling: this lane's windows read from the box, restages (counted on every lane), and this lane's windows left
   // to the per-lane loops because the footprint bound failed, the warp's request was too wide or too tall, or too few
   // lanes were active
@@ -609,9 +751,9 @@ struct BoxState {
 // a restage centres the box on the request and copies it with 16-byte cp.async chunks.  Windows that fail the bound,
 // a request wider than PS_BOX_P - 3 or taller than PS_BOX_H texels, or fewer than PS_STAGE_MIN_LANES active lanes use
 // the per-lane loops.  All paths give the same bits.
-template <int WR, int WS, int NT, bool TEX>
+template <int WR, int WS, int NT, bool TEX, bool TMA>
 __device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& S,
-                                               const float* H, int x, int y, bool act, int& nwin, float* box,
+                                               int src, const float* H, int x, int y, bool act, int& nwin, float* box,
                                                BoxState& bs) {
   const float fx = (float)x, fy = (float)y;
   act = act && ncc_begin(rs, S, H, fx, fy);
@@ -679,17 +821,28 @@ __device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw,
         __syncwarp();  // every lane is done with the previous box
         const int lane = threadIdx.x & 31;
         const unsigned sbase = (unsigned)__cvta_generic_to_shared(box);
+        if constexpr (TMA) {
+          // one 2-D tensor load of the whole box (x = ox + PS_BORDER ≡ 0 mod 4: 16-byte aligned); outside the
+          // plane's tensor the box reads 0, as the cp.async path's zero-filled chunks do
+          if (lane == 0) {
+            fence_proxy_async();
+            tma_load_2d(sbase, tmap(P, src, 1), ox + PS_BORDER, oy + PS_BORDER, bs.bar, PS_BOX_P * PS_BOX_H * 4u);
+          }
+          mbar_wait(P, bs.bar, bs.phase);
+          bs.phase ^= 1u;
+        } else {
 #pragma unroll 2
-        for (int i = lane; i < PS_BOX_H * (PS_BOX_P / 4); i += 32) {
-          const int r = i / (PS_BOX_P / 4), q = i - r * (PS_BOX_P / 4);
-          const int X = ox + 4 * q, Y = oy + r;
-          const bool in = Y >= -PS_BORDER && Y < S.h + PS_BORDER && X >= -PS_BORDER && X + 4 <= S.pitch - PS_BORDER;
-          const float* src = in ? S.img + (long long)Y * S.pitch + X : S.img - PS_BORDER;  // aligned; 0 bytes read
-          asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + 4u * (unsigned)(r * PS_BOX_P + 4 * q)),
-                       "l"(src), "r"(in ? 16 : 0)
-                       : "memory");
+          for (int i = lane; i < PS_BOX_H * (PS_BOX_P / 4); i += 32) {
+            const int r = i / (PS_BOX_P / 4), q = i - r * (PS_BOX_P / 4);
+            const int X = ox + 4 * q, Y = oy + r;
+            const bool in = Y >= -PS_BORDER && Y < S.h + PS_BORDER && X >= -PS_BORDER && X + 4 <= S.pitch - PS_BORDER;
+            const float* srcp = in ? S.img + (long long)Y * S.pitch + X : S.img - PS_BORDER;  // aligned; 0 bytes read
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sbase + 4u * (unsigned)(r * PS_BOX_P + 4 * q)),
+                         "l"(srcp), "r"(in ? 16 : 0)
+                         : "memory");
+          }
+          asm volatile("cp.async.wait_all;\n" ::: "memory");
         }
-        asm volatile("cp.async.wait_all;\n" ::: "memory");
         __syncwarp();
         bs.src = S.img;
         bs.ox = ox;
@@ -697,16 +850,17 @@ __device__ __forceinline__ float ncc_cost_warp(const PsRun& P, const RefWin& rw,
         bs.nrestage++;
       }
       if (act) bs.nstaged++;
-      return act ? ncc_window_pairs<WR, WS, NT, SMP_BOX, true>(
-                       rw, rs, S, H, x, y,
-                       BoxRef{(unsigned)__cvta_generic_to_shared(box) + kBoxBias, 12582912.0f - (float)bs.ox,
-                              12582912.0f - (float)bs.oy})
-                 : 2.0f;
+      BoxRef bx{(unsigned)__cvta_generic_to_shared(box) + kBoxBias, 12582912.0f - (float)bs.ox, 12582912.0f - (float)bs.oy};
+#if PS_CHECKED
+      bx.box = (unsigned)__cvta_generic_to_shared(box);
+      bx.fault = P.fault;
+#endif
+      return act ? ncc_window_pairs<WR, WS, NT, SMP_BOX, true>(rw, rs, S, H, x, y, bx) : 2.0f;
     }
   }
   if (!act) return 2.0f;
   if (front)
-    return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD, true>(rw, rs, S, H, x, y, BoxRef{0u, 0.f, 0.f});
+    return ncc_window_pairs<WR, WS, NT, TEX ? SMP_TEX : SMP_LOAD, true>(rw, rs, S, H, x, y, no_box(P));
   return ncc_window<WR, WS, true, NT, TEX, 1, true>(P, rw, rs, S, H, x, y);
 }
 
@@ -724,6 +878,7 @@ __device__ float geo_error(const PsRun& P, const PsLevel& R, const PsLevel& S, c
   float u = S.fx * xj / zj + S.cx, v = S.fy * yj / zj + S.cy;
   float uf = floorf(u + 0.5f), vf = floorf(v + 0.5f);
   if (!(uf >= 0.f && vf >= 0.f && uf < (float)S.w && vf < (float)S.h)) return PS_INF_ERR;
+  if (!PS_IN(P.fault, PS_SITE_SNAPSHOT, off + (long long)vf * S.w + (long long)uf, 0, P.snap_pixels)) return PS_INF_ERR;
   float dj = __ldg(P.snap + off + (long long)vf * S.w + (long long)uf);
   if (!(dj > 0.f)) return PS_INF_ERR;
   float3 Yj = make_float3((u - S.cx) / S.fx * dj, (v - S.cy) / S.fy * dj, dj);
@@ -839,6 +994,25 @@ __device__ __forceinline__ int find_item(const PsRun& P, int cta) {
   return lo;
 }
 
+// Checked build: the item's view, its pixels in the state arrays, its source count and source views; the self-test
+// probe (PsRun.probe) tests one index past the end of the state arrays here, so no access follows it.  CTA-uniform,
+// so a kernel may return on false before its first barrier.  Always true in the other builds.
+__device__ __forceinline__ bool item_ok(const PsRun& P, const PsItem& it) {
+#if PS_CHECKED
+  if (P.probe && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0)
+    (void)PS_IN(P.fault, PS_SITE_PROBE, P.state_pixels, 0, P.state_pixels);
+  if (!PS_IN(P.fault, PS_SITE_SOURCE, it.view, 0, P.nviews_all)) return false;
+  if (!PS_IN(P.fault, PS_SITE_STATE, it.off, 0, P.state_pixels) ||
+      !PS_IN(P.fault, PS_SITE_STATE, it.off + (long long)it.w * it.h - 1, 0, P.state_pixels))
+    return false;
+  const int nsrc = P.views[it.view].nsrc;
+  if (!PS_IN(P.fault, PS_SITE_SOURCE, nsrc, 0, PS_MAXSRC + 1)) return false;
+  for (int j = 0; j < nsrc; ++j)
+    if (!PS_IN(P.fault, PS_SITE_SOURCE, P.pairs[(size_t)it.view * PS_MAXSRC + j].src, 0, P.nviews_all)) return false;
+#endif
+  return true;
+}
+
 // ================================================================================ half step (patchmatch.cu:439-657)
 // Warp-aggregated add of the per-thread NCC window count (threads that already returned do not take part).
 __device__ __forceinline__ void count_windows(const PsRun& P, int nwin) {
@@ -857,7 +1031,7 @@ __host__ __device__ constexpr int half_pw(int G) { return G == 2 ? PS_HALF2_PW :
 __host__ __device__ constexpr int half_tw(int G, int wr) {
   return G == 2 ? (((PS_HALF2_PW + 2 * wr) + 15) / 32) * 32 + 16 : PS_HALF_PW + 2 * wr;
 }
-__host__ __device__ constexpr int half_tw_staged(int wr) { return ((PS_HALF_PW + 2 * wr + 3) / 8) * 8 + 4; }
+__host__ __device__ constexpr int half_tw_staged(int wr) { return PS_HALF_ST_TW(wr); }
 
 // ---------------------------------------------------------------------------- per-pixel PatchMatch logic
 // Shared by the half-step kernels; each helper is the reference's step verbatim (patchmatch.cu line ranges cited).
@@ -917,15 +1091,26 @@ __device__ __forceinline__ void agg_init(ViewAgg& a) {
   a.denf = 0.f;
   a.vbest = 255;
 }
+// The values that change between the half steps of a run: iteration, colour and the iteration's constants
+// (patchmatch.rs:752-799: tau_good, eps and phi follow the iteration).  A launch per half step takes them from its
+// PsRun; the persistent kernel from the run's phase table.
+struct HalfPhase {
+  int t, color;
+  float tau_good, eps, phi;
+};
+__device__ __forceinline__ HalfPhase launch_phase(const PsRun& P) {
+  return HalfPhase{P.t, P.color, P.tau_good, P.eps, P.phi};
+}
+
 // Source j with prior > 0: m, gg = photometric costs and truncated geometric errors of the 9 hypotheses; writes the
 // view weight (or -prior) to *wvj.
-__device__ __forceinline__ void agg_source(const PsRun& P, ViewAgg& a, const float* m, const float* gg, float prior,
-                                           int j, int vprev, float* wvj) {
+__device__ __forceinline__ void agg_source(const PsRun& P, float tau_good, ViewAgg& a, const float* m, const float* gg,
+                                           float prior, int j, int vprev, float* wvj) {
   int good = 0, bad = 0;
   float conf = 0.f;
 #pragma unroll
   for (int i = 1; i < 9; ++i) {
-    if (m[i] < P.tau_good) {
+    if (m[i] < tau_good) {
       good++;
       conf += m_exp(-m[i] * m[i] * P.inv2beta2);
     }
@@ -999,17 +1184,17 @@ __device__ __forceinline__ void refine_prior(const PsRun& P, long long g, float 
   }
   r.ncand = has_prior ? 7 : 6;
 }
-__device__ __forceinline__ void refine_draw(const PsRun& P, const PsView& vd, int pix, float3 ray, float4& best,
-                                            Refine& r) {
-  u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, P.t, P.color, (u64)pix);
+__device__ __forceinline__ void refine_draw(const PsRun& P, const HalfPhase& ph, const PsView& vd, int pix, float3 ray,
+                                            float4& best, Refine& r) {
+  u64 st = rng_state(P.seed, vd.key, P.level, P.run_id, ph.t, ph.color, (u64)pix);
   r.d_r = random_depth(st, vd.dmin, vd.dmax);
   r.n_r = random_normal(st, ray);
   const float uu = 2.f * rnd(st) - 1.f;
-  const float inv = best.w > 0.f ? (1.f / best.w) * (1.f + uu * P.eps) : -1.f;
+  const float inv = best.w > 0.f ? (1.f / best.w) * (1.f + uu * ph.eps) : -1.f;
   r.d_p = inv > 0.f ? 1.f / inv : r.d_r;
   if (!(best.w > 0.f)) best.w = r.d_r;
   r.n0 = make_float3(best.x, best.y, best.z);
-  r.n_p = perturb_normal(st, r.n0, ray, P.phi);
+  r.n_p = perturb_normal(st, r.n0, ray, ph.phi);
   r.bw = best.w;
 }
 __device__ __forceinline__ float4 refine_candidate(const Refine& r, int c) {
@@ -1030,13 +1215,13 @@ __device__ __forceinline__ float4 refine_candidate(const Refine& r, int c) {
 //   k_half_st:     row pairs plus the warp-collective staged source boxes (ncc_cost_warp).
 // G = 1: two CTAs per SM with the weight cache (~90 KB each for a 13×13 window), four without it.
 // G = 2: the two lanes of a pixel split the window rows, so each thread caches half the weights: four CTAs per SM.
-template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
-__global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
+// One half-step tile: CTA `cta` of the launch's flattened tile list, in phase `ph`, with dynamic shared memory sm.
+template <int WR, int WS, bool CW, bool TEX, int G, int MODE>
+__device__ __forceinline__ void half_tile(const PsRun& P, const HalfPhase& ph, int cta, float* sm) {
   constexpr int NT = PS_HALF_NT;
   constexpr int PW = half_pw(G);
   constexpr bool PAIRW = MODE >= 1;
   static_assert(MODE == 0 || (MODE == 1 && CW && G == 1 && WR != 0), "row pairs need the weight cache, one lane, a fixed window");
-  extern __shared__ float sm[];
   const int wr = WR ? WR : P.wr, ws = WR ? WS : P.ws;
   const int wn = (2 * wr) / ws + 1;
   const int TW = half_tw(G, wr), TH = PS_HALF_PH + 2 * wr;
@@ -1044,11 +1229,12 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
   float* wcache = sm + ((TW * TH + 31) & ~31);
   float* wvs = wcache + (CW ? ((wn + G - 1) / G) * wn * NT : 0);
 
-  const int ii = find_item(P, blockIdx.x);
+  const int ii = find_item(P, cta);
   const PsItem& it = P.items[ii];
+  if (!item_ok(P, it)) return;
   const int w = it.w, h = it.h;
   const int tiles_x = (w + PW - 1) / PW;
-  const int tl = blockIdx.x - it.tile0;
+  const int tl = cta - it.tile0;
   const int x0 = (tl % tiles_x) * PW, y0 = (tl / tiles_x) * PS_HALF_PH;
   const PsLevel R = P.lv[it.view * P.nlevels + P.level];
   {
@@ -1064,12 +1250,13 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
   const int gl = G == 2 ? (lane & 1) : 0;
   const int row = 2 * warp + (lane >> 4), col = G == 2 ? ((lane >> 1) & 7) : (lane & 15);
   const int y = y0 + row;
-  const int x = x0 + 2 * col + ((y + P.color) & 1);
+  const int x = x0 + 2 * col + ((y + ph.color) & 1);
   if (x >= w || y >= h) return;  // both lanes of a pixel leave together
 
   RefWin rw;
   rw.t = tile + (row + wr) * TW + (x - x0 + wr);
   rw.tw = TW;
+  refwin_bounds(rw, tile, TW * TH, P);
   rw.wc = wcache + (PAIRW ? 2 * threadIdx.x : threadIdx.x);
   rw.g = gl;
   rw.pmask = G == 2 ? (3u << (lane & ~1)) : 0u;
@@ -1132,7 +1319,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
           gg[q] = gi;
         }
     }
-    agg_source(P, ag, m, gg, prior, j, vprev, wv + j * NT);
+    agg_source(P, ph.tau_good, ag, m, gg, prior, j, vprev, wv + j * NT);
   }
   float4 best;
   float bcost;
@@ -1141,7 +1328,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
   // 3. Refinement, 6 hypotheses (patchmatch.cu:596-628), then 4. the coarse-scale candidate (:629-653).
   Refine rf;
   refine_prior(P, base + pix, rs.var, ray, rf);
-  refine_draw(P, vd, pix, ray, best, rf);
+  refine_draw(P, ph, vd, pix, ray, best, rf);
 #pragma unroll 1
   for (int c = 0; c < rf.ncand; ++c) {
     const float4 cd = refine_candidate(rf, c);
@@ -1178,19 +1365,98 @@ __global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(con
   count_windows(P, gl == 0 ? nwin : 0);
 }
 
+template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
+__global__ void __launch_bounds__(PS_HALF_NT, (CW && G == 1) ? 2 : 4) k_half(const __grid_constant__ PsRun P) {
+  extern __shared__ float sm[];
+  half_tile<WR, WS, CW, TEX, G, MODE>(P, launch_phase(P), blockIdx.x, sm);
+}
+
+// ================================================================================ persistent half step (PS_TUNE_PERSISTENT)
+// Bounded wait of one thread until *ctr >= need (acquire at GPU scope, so the CTA's loads after the following barrier
+// see the counted tiles' stores).  Gives up when another CTA has already given up (error word set) or after
+// PS_QUEUE_SPIN_LIMIT polls, setting the error word; returns whether the count was reached.
+__device__ __forceinline__ bool queue_wait(const PsRun& P, const unsigned* ctr, unsigned need) {
+  for (unsigned spins = 0;; ++spins) {
+    unsigned v, e;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(ctr) : "memory");
+    if (v >= need) return true;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(e) : "l"(P.queue + 1) : "memory");
+    if (e != 0u) return false;
+    if (spins >= PS_QUEUE_SPIN_LIMIT) {
+      atomicCAS(P.queue + 1, 0u, 1u);
+      return false;
+    }
+    __nanosleep(256);
+  }
+}
+
+// Every half step of a run in one launch.  Items (phase k, tile c) are handed out in the order k·ntiles + c from the
+// queue counter, so all tiles of phase k precede those of phase k + 1; before a tile of phase k > 0 runs, its CTA
+// waits until every tile of phase k - 1 of the same view is done (the tile reads the other colour's planes that
+// phase k - 1 wrote, and overwrites planes that phase k - 1 read).  A CTA only dequeues when it is running and only
+// waits on items dequeued before its own, so the smallest unfinished item never waits: the queue cannot deadlock,
+// whatever the grid size.  When a wait gives up, the tile is skipped (its count is still added, so nothing waits on
+// it) and the run reports PS_ETIMEOUT; every later wait returns at once.  The tiles compute exactly what the
+// per-half-step launches compute, so the results are the same bits.
+template <int WR, int WS, bool TEX>
+__global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_q(const __grid_constant__ PsRun P) {
+  extern __shared__ float sm[];
+  __shared__ int s_item, s_go;
+  const int total = P.ntiles * P.nphases;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const int i = (int)atomicAdd(P.queue, 1u);
+      int go = 1;
+      if (i < total) {
+        const int k = i / P.ntiles, cta = i - k * P.ntiles;
+        if (k > 0) {
+          const int ii = find_item(P, cta);
+          const int next = ii + 1 < P.nitems ? P.items[ii + 1].tile0 : P.ntiles;
+          const unsigned need = (unsigned)(next - P.items[ii].tile0) + (P.qstall ? 1u : 0u);
+          go = queue_wait(P, P.queue + 2 + (size_t)(k - 1) * P.nitems + ii, need) ? 1 : 0;
+        }
+      }
+      s_item = i;
+      s_go = go;
+    }
+    __syncthreads();
+    const int i = s_item;
+    if (i >= total) return;
+    const int k = i / P.ntiles, cta = i - k * P.ntiles;
+    if (s_go) {
+      const PsPhase& q = P.phases[k];
+      half_tile<WR, WS, true, TEX, 1, 1>(P, HalfPhase{q.t, q.color, q.tau_good, q.eps, q.phi}, cta, sm);
+    }
+    __syncthreads();  // the tile's stores (and its reads of s_item) are done
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(P.queue + 2 + (size_t)k * P.nitems + find_item(P, cta), 1u);
+    }
+  }
+}
+
 // Staged-source half step.  One lane per pixel; a warp covers an 8 × 8 pixel block of the 32 × 8 tile.  Every
 // window of every lane goes through ncc_cost_warp, which the whole warp calls together, so no lane leaves early
 // (lanes outside the image work on a clamped pixel with every window inactive and write nothing) and the pixel's
 // windows run as one job list with a single window call site: first the traversal jobs (source j, hypothesis i) in
 // the reference's order, then the refinement jobs (candidate c, source j).  The arithmetic and the order of every
 // sum are those of k_half, so the bits are the same.
-template <int WR, int WS, bool TEX>
+//
+// TMA (PS_TUNE_TMA): the reference tile and the source boxes arrive by 2-D tensor loads on mbarriers instead of the
+// tile copy loop and the cp.async chunks.  The tile then starts tma_xo(wr) ≥ wr columns left of the CTA's first
+// column (so its first element is 16-byte aligned) and reads the plane's zero border, padding and out-of-tensor zeros
+// where the copy loop writes zeros outside the image: the same values.
+__host__ __device__ constexpr int tma_xo(int wr) { return wr + ((PS_BORDER - wr) & 3); }
+template <int WR, int WS, bool TEX, bool TMA>
 __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_HALF_NT;
   constexpr int wr = WR, wn = (2 * WR) / WS + 1;
+  constexpr int XO = TMA ? tma_xo(WR) : WR;  // tile columns left of the CTA's first column
   constexpr unsigned FULL = 0xffffffffu;
-  extern __shared__ float sm[];
+  extern __shared__ __align__(128) float sm[];
+  __shared__ __align__(8) unsigned long long bars[1 + PS_HALF_NT / 32];
   const int TW = half_tw_staged(wr), TH = PS_HALF_PH + 2 * wr;
+  static_assert(!TMA || PS_HALF_PW + tma_xo(WR) + WR <= half_tw_staged(WR), "TMA tile wider than the tile pitch");
   float* tile = sm;
   float* wcache = sm + ((TW * TH + 31) & ~31);
   float* wvs = wcache + wn * wn * NT;
@@ -1198,12 +1464,30 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
 
   const int ii = find_item(P, blockIdx.x);
   const PsItem& it = P.items[ii];
+  if (!item_ok(P, it)) return;
   const int w = it.w, h = it.h;
   const int tiles_x = (w + PS_HALF_PW - 1) / PS_HALF_PW;
   const int tl = blockIdx.x - it.tile0;
   const int x0 = (tl % tiles_x) * PS_HALF_PW, y0 = (tl / tiles_x) * PS_HALF_PH;
   const PsLevel R = P.lv[it.view * P.nlevels + P.level];
-  {
+  if constexpr (TMA) {
+    // the tensor loads need 128-byte aligned destinations: the tile (the start of dynamic shared memory) and the
+    // boxes (whole multiples of 128 bytes after it); otherwise nothing is loaded and the run fails (error word 3)
+    if (((unsigned)__cvta_generic_to_shared(sm) & 127u) != 0u) {
+      if (threadIdx.x == 0 && P.queue) atomicCAS(P.queue + 1, 0u, 3u);
+      return;
+    }
+    const unsigned bar0 = (unsigned)__cvta_generic_to_shared(bars);
+    if (threadIdx.x == 0) {
+      for (int b = 0; b < 1 + PS_HALF_NT / 32; ++b) mbar_init(bar0 + 8u * b);
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      fence_proxy_async();
+      tma_load_2d((unsigned)__cvta_generic_to_shared(tile), tmap(P, it.view, 0), x0 - XO + PS_BORDER,
+                  y0 - wr + PS_BORDER, bar0, (unsigned)(TW * TH * 4));
+    }
+    __syncthreads();  // barriers initialised
+    mbar_wait(P, bar0, 0u);
+  } else {
     const int ox = x0 - wr, oy = y0 - wr;
     for (int i = threadIdx.x; i < TW * TH; i += NT) {
       int tx = i % TW, ty = i / TW;
@@ -1214,16 +1498,18 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int y = y0 + (lane >> 2);
-  int x = x0 + 2 * (4 * warp + (lane & 3)) + ((y + P.color) & 1);
+  const HalfPhase ph = launch_phase(P);
+  int x = x0 + 2 * (4 * warp + (lane & 3)) + ((y + ph.color) & 1);
   const bool live = x < w && y < h;
   y = min(y, h - 1);
   x = min(x, w - 1);
   float* box = boxes + warp * (PS_BOX_P * PS_BOX_H);
-  BoxState bs{nullptr, 0, 0, 0, 0, 0, 0, 0, 0};
+  BoxState bs{nullptr, 0, 0, (unsigned)__cvta_generic_to_shared(bars) + 8u * (1 + warp), 0u, 0, 0, 0, 0, 0, 0};
 
   RefWin rw;
-  rw.t = tile + (y - y0 + wr) * TW + (x - x0 + wr);
+  rw.t = tile + (y - y0 + wr) * TW + (x - x0 + XO);
   rw.tw = TW;
+  refwin_bounds(rw, tile, TW * TH, P);
   rw.wc = wcache + 2 * threadIdx.x;
   rw.g = 0;
   rw.pmask = 0u;
@@ -1261,7 +1547,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
   for (int k = 0;; ++k) {
     if (k == nA) {  // end of the traversal: aggregate, then the refinement draws
       agg_finish(ag, hyp, nsrc, wv, NT, best, bcost);
-      refine_draw(P, vd, pix, ray, best, rf);
+      refine_draw(P, ph, vd, pix, ray, best, rf);
     }
     if (k == nA + nB) break;
     const bool trav = k < nA;
@@ -1298,7 +1584,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
     if (__any_sync(FULL, act)) {
       float H[9];
       const bool hok = homography(R, lp, fx, fy, hv, H);
-      mv = ncc_cost_warp<WR, WS, NT, TEX>(P, rw, rs, S, H, x, y, act && hok, nwin, box, bs);
+      mv = ncc_cost_warp<WR, WS, NT, TEX, TMA>(P, rw, rs, S, pr.src, H, x, y, act && hok, nwin, box, bs);
     }
     if (trav) {
       const float gv = (P.geometric && use) ? fminf(geo_error(P, R, S, pr, x, y, hv.w), P.gmax) : 0.f;
@@ -1308,7 +1594,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
           m[q] = mv;
           gg[q] = gv;
         }
-      if (i == 8 && use) agg_source(P, ag, m, gg, prior, j, vprev, wv + j * NT);
+      if (i == 8 && use) agg_source(P, ph.tau_good, ag, m, gg, prior, j, vprev, wv + j * NT);
     } else {
       if (act) {
         const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, hv.w), P.gmax) : 0.f;
@@ -1386,6 +1672,7 @@ struct EvalCtx {
 __device__ __forceinline__ bool eval_tile(const PsRun& P, float* tile, int wr, EvalCtx& e) {
   const int ii = find_item(P, blockIdx.x);
   const PsItem& it = P.items[ii];
+  if (!item_ok(P, it)) return false;
   e.it = &it;
   e.w = it.w;
   e.h = it.h;
@@ -1423,6 +1710,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
     rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
   }
   rw.tw = TW;
+  refwin_bounds(rw, sm, TW * TH, P);
   rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
   const PsItem& it = *e.it;
   const PsView& vd = P.views[it.view];
@@ -1483,6 +1771,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__
     rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
   }
   rw.tw = TW;
+  refwin_bounds(rw, sm, TW * TH, P);
   rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
   const PsView& vd = P.views[e.it->view];
   const PsLPair* lps = P.lpairs + ((size_t)e.it->view * P.nlevels + P.level) * PS_MAXSRC;
@@ -1491,7 +1780,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__
   const RefStats rs = ref_stats<WR, WS, true, NT>(P, rw);
   const float inear = 1.0f / vd.dmin, ifar = 1.0f / vd.dmax;
   unsigned short* out = P.netin + ((long long)y * P.netin_pitch + x) * PS_NET_CH_IN;
-  out[0] = bf16_bits(rw.t[0]);
+  out[0] = bf16_bits(tile_at(rw, rw.t));
   int nwin = 0;
 #pragma unroll 1
   for (int k = 0; k < PS_SWEEP_PLANES; ++k) {
@@ -1533,6 +1822,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant_
     rw.t = sm + (y - y0 + wr) * TW + (x - x0 + wr);
   }
   rw.tw = TW;
+  refwin_bounds(rw, sm, TW * TH, P);
   rw.wc = sm + ((TW * TH + 31) & ~31) + threadIdx.x;
   const PsView& vd = P.views[it.view];
   const PsPair* prs = P.pairs + (size_t)it.view * PS_MAXSRC;
@@ -1580,6 +1870,7 @@ struct SimpleCtx {
 __device__ __forceinline__ bool simple_px(const PsRun& P, SimpleCtx& c) {
   const int ii = find_item(P, blockIdx.x);
   const PsItem& it = P.items[ii];
+  if (!item_ok(P, it)) return false;
   const int tiles_x = (it.w + PS_SIMPLE_BX - 1) / PS_SIMPLE_BX;
   const int tl = blockIdx.x - it.tile0;
   c.x = (tl % tiles_x) * PS_SIMPLE_BX + (int)threadIdx.x;
@@ -1877,10 +2168,50 @@ static cudaError_t launch_half_g(const PsRun& P, bool cw, bool tex, size_t smem,
 }
 template <int A, int B>
 static cudaError_t launch_half_pairs(const PsRun& P, int mode, bool tex, size_t smem, cudaStream_t st) {
-  if (mode == 2) return tex ? launch(k_half_st<A, B, true>, P.ntiles, PS_HALF_NT, smem, st, P)
-                            : launch(k_half_st<A, B, false>, P.ntiles, PS_HALF_NT, smem, st, P);
+  if (mode == 2) {
+    if (P.tmaps) return tex ? launch(k_half_st<A, B, true, true>, P.ntiles, PS_HALF_NT, smem, st, P)
+                            : launch(k_half_st<A, B, false, true>, P.ntiles, PS_HALF_NT, smem, st, P);
+    return tex ? launch(k_half_st<A, B, true, false>, P.ntiles, PS_HALF_NT, smem, st, P)
+               : launch(k_half_st<A, B, false, false>, P.ntiles, PS_HALF_NT, smem, st, P);
+  }
   return tex ? launch(k_half<A, B, true, true, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P)
              : launch(k_half<A, B, true, false, 1, 1>, P.ntiles, PS_HALF_NT, smem, st, P);
+}
+
+// Whether the persistent kernel runs a run's half steps for this tuning word and window: the row-pair mode with
+// PS_TUNE_PERSISTENT.
+bool half_run_ok(unsigned tuning, int wr, int ws) { return (tuning & 0x20u) && half_mode(tuning, wr, ws) == 1; }
+
+// The persistent half step: as many CTAs as fit on the device at once (or fewer when there are fewer items).
+template <int A, int B>
+static cudaError_t launch_half_q(const PsRun& P, bool tex, size_t smem, cudaStream_t st) {
+  void (*kern)(PsRun) = tex ? k_half_q<A, B, true> : k_half_q<A, B, false>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, PS_HALF_NT, smem)) != cudaSuccess) return e;
+  const long long total = (long long)P.ntiles * P.nphases;
+  const long long grid = std::min<long long>(total, (long long)std::max(per, 1) * sms);
+  if (grid <= 0) return cudaSuccess;
+  kern<<<(int)grid, PS_HALF_NT, smem, st>>>(P);
+  return cudaGetLastError();
+}
+
+// Every half step of P's phase table in one launch (half_run_ok must hold); P.queue must be zeroed on the stream.
+cudaError_t launch_half_run(const PsRun& P, unsigned tuning, cudaStream_t st) {
+  cudaError_t e = init_constants();
+  if (e != cudaSuccess) return e;
+  if (!half_run_ok(tuning, P.wr, P.ws) || !P.queue || P.nphases < 1 || P.nphases > PS_MAX_PHASES)
+    return cudaErrorInvalidValue;
+  const bool tex = (tuning & 0x2u) != 0;
+  const size_t smem = half_smem(P.wr, P.ws, true, P.maxsrc, 1, 1);
+#define PS_CASE(a, b) \
+  if (P.wr == a && P.ws == b) return launch_half_q<a, b>(P, tex, smem, st);
+  PS_SPECS(PS_CASE)
+#undef PS_CASE
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st) {

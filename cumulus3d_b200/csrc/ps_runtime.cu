@@ -9,6 +9,8 @@
 //     keeps everything on the device (ps_run_resident, ps_snapshot_capture, ps_filter_resident) never copies states;
 //   * the FP64 homography setup A = K_j R K^-1, b = K_j t runs on the device once per session;
 //   * the batch table rides in the kernel parameters, tiles of all views of a batch are flattened into one grid.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <omp.h>
 #include <algorithm>
@@ -30,6 +32,8 @@
 #define PS_DECLARE_LAUNCHERS(NS)                                                                           \
   namespace NS {                                                                                           \
   cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st);                               \
+  bool half_run_ok(unsigned tuning, int wr, int ws);                                                       \
+  cudaError_t launch_half_run(const PsRun& P, unsigned tuning, cudaStream_t st);                           \
   int half_lanes(unsigned tuning);                                                                         \
   cudaError_t launch_eval(const PsRun& P, cudaStream_t st);                                                \
   cudaError_t launch_filter(const PsRun& P, cudaStream_t st);                                              \
@@ -47,6 +51,7 @@
   }
 PS_DECLARE_LAUNCHERS(ps_parity)
 PS_DECLARE_LAUNCHERS(ps_fast)
+PS_DECLARE_LAUNCHERS(ps_checked)
 
 namespace {
 
@@ -61,15 +66,21 @@ struct Launchers {
   int (*half_lanes)(unsigned);
   cudaError_t (*sweep)(const PsRun&, bool, cudaStream_t);
   cudaError_t (*restore)(const PsRun&, const float4*, const float*, float, cudaStream_t);
+  bool (*half_run_ok)(unsigned, int, int);
+  cudaError_t (*half_run)(const PsRun&, unsigned, cudaStream_t);
 };
 const Launchers kParity = {ps_parity::launch_half,     ps_parity::launch_eval,   ps_parity::launch_filter,
                            ps_parity::launch_upsample, ps_parity::launch_median, ps_parity::launch_snapshot,
                            ps_parity::launch_readout,  ps_parity::half_lanes,    ps_parity::launch_sweep,
-                           ps_parity::launch_restore};
+                           ps_parity::launch_restore, ps_parity::half_run_ok, ps_parity::launch_half_run};
 const Launchers kFast = {ps_fast::launch_half,     ps_fast::launch_eval,   ps_fast::launch_filter,
                          ps_fast::launch_upsample, ps_fast::launch_median, ps_fast::launch_snapshot,
                          ps_fast::launch_readout,  ps_fast::half_lanes,    ps_fast::launch_sweep,
-                         ps_fast::launch_restore};
+                         ps_fast::launch_restore, ps_fast::half_run_ok, ps_fast::launch_half_run};
+const Launchers kChecked = {ps_checked::launch_half,     ps_checked::launch_eval,   ps_checked::launch_filter,
+                            ps_checked::launch_upsample, ps_checked::launch_median, ps_checked::launch_snapshot,
+                            ps_checked::launch_readout,  ps_checked::half_lanes,    ps_checked::launch_sweep,
+                            ps_checked::launch_restore, ps_checked::half_run_ok, ps_checked::launch_half_run};
 
 struct PsError {
   int code;
@@ -165,6 +176,10 @@ struct ps_session {
   std::string err;
   cudaStream_t st = nullptr;
   const Launchers* L = &kParity;
+  unsigned long long* fault = nullptr;  // checked build: the kernels' fault word (device), else null
+  unsigned* qbuf = nullptr;             // persistent half step: queue counter, error word, per-phase done counts
+  CUtensorMap* tmaps = nullptr;         // TMA staging: two maps per (view, level) plane (tile box, source box)
+  bool q_used = false;                  // a persistent launch was issued since the last check of its error word
   int nv = 0, nl = 0;
   ps_pm_params pm{};
   ps_filter_params fl{};
@@ -278,6 +293,52 @@ void maybe_inject(ps_session* s, uint32_t kind, const char* what) {
   fail(kind == PS_INJECT_DEVICE_ALLOC ? PS_ENOMEM : PS_ECUDA, std::string("injected failure: ") + what);
 }
 
+const char* site_name(unsigned site) {
+  switch (site) {
+    case PS_SITE_TILE: return "reference tile";
+    case PS_SITE_BOX: return "staged source box";
+    case PS_SITE_PLANE: return "source plane";
+    case PS_SITE_STATE: return "state arrays";
+    case PS_SITE_SOURCE: return "source view index";
+    case PS_SITE_SNAPSHOT: return "depth snapshot";
+    case PS_SITE_PROBE: return "self-test probe";
+    default: return "unknown site";
+  }
+}
+
+// Bounded waits (persistent queue, TMA barriers): after the stream has drained, a set error word (1 = queue, 2 = TMA)
+// means a wait gave up; the word is cleared and the call fails with PS_ETIMEOUT.  An armed queue stall
+// (PS_INJECT_QUEUE_STALL) is spent.
+void check_queue(ps_session* s) {
+  if (!s->q_used) return;
+  s->q_used = false;
+  if (s->be && s->be->inject_kind == PS_INJECT_QUEUE_STALL) s->be->inject_kind = PS_INJECT_NONE;
+  unsigned e = 0;
+  cuda_ok(cudaMemcpy(&e, s->qbuf + 1, sizeof e, cudaMemcpyDeviceToHost), "read queue error word");
+  if (!e) return;
+  cuda_ok(cudaMemset(s->qbuf + 1, 0, sizeof e), "clear queue error word");
+  if (e == 3u) fail(PS_ECUDA, "staged half step: shared memory not aligned for TMA loads (nothing was loaded)");
+  fail(PS_ETIMEOUT, e == 2u ? "staged half step: a wait for a TMA tile load gave up"
+                            : "persistent half step: a wait for the previous half step's tiles gave up");
+}
+
+// Checked build: after the stream has drained, a non-zero fault word means a kernel skipped an out-of-bounds access.
+// The word is cleared (so the session stays usable) and the call fails with PS_EFAULT naming the first violation.
+// An armed self-test probe (PS_INJECT_CHECK_PROBE) is spent here.
+void check_fault(ps_session* s) {
+  if (!s->fault) return;
+  unsigned long long w = 0;
+  cuda_ok(cudaMemcpy(&w, s->fault, sizeof w, cudaMemcpyDeviceToHost), "read fault word");
+  if (s->be && s->be->inject_kind == PS_INJECT_CHECK_PROBE) s->be->inject_kind = PS_INJECT_NONE;
+  if (!w) return;
+  cuda_ok(cudaMemset(s->fault, 0, sizeof w), "clear fault word");
+  const unsigned site = (unsigned)(w >> 56);
+  long long idx = (long long)(w & 0x00FFFFFFFFFFFFFFull);
+  if (idx & 0x0080000000000000ll) idx -= 0x0100000000000000ll;  // sign of the 56-bit index
+  fail(PS_EFAULT, std::string("checked build: out-of-bounds index ") + std::to_string(idx) + " (" + site_name(site) +
+                      "); the access was skipped");
+}
+
 // Session device memory: from the backend's pool in the session stream's order (plain cudaMalloc when the device
 // offers no pool).  Every use of a buffer is on the session stream.
 template <typename T>
@@ -359,6 +420,42 @@ std::vector<std::pair<size_t, size_t>> batches(ps_session* s, const uint32_t* vi
   return out;
 }
 
+// TMA staging: two tensor maps per (view, level) plane over the session's image buffer (see tmap() in the kernels):
+// map 0 with the reference tile's box (PS_HALF_ST_TW(wr) × PS_HALF_PH + 2·wr), map 1 with the source box
+// (PS_BOX_P × PS_BOX_H).  The tensor is the whole bordered plane, pitch × (h + 2·PS_BORDER) f32 elements from its
+// 128-byte aligned allocation; elements outside it read 0.
+void build_tensor_maps(ps_session* s, const std::vector<PsLevel>& lvh, const std::vector<size_t>& offs,
+                       const std::vector<size_t>& pitches) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      fail(PS_ECUDA, "cuTensorMapEncodeTiled is not available");
+    encode = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  }
+  const int wr = s->pm.window_radius;
+  const cuuint32_t boxes[2][2] = {{(cuuint32_t)PS_HALF_ST_TW(wr), (cuuint32_t)(PS_HALF_PH + 2 * wr)},
+                                  {(cuuint32_t)PS_BOX_P, (cuuint32_t)PS_BOX_H}};
+  std::vector<CUtensorMap> maps(lvh.size() * 2);
+  for (size_t i = 0; i < lvh.size(); ++i) {
+    void* base = s->img + offs[i];
+    if (((uintptr_t)base & 127u) || (pitches[i] * sizeof(float)) % 16) fail(PS_EINVAL, "plane not aligned for TMA");
+    const cuuint64_t dims[2] = {(cuuint64_t)pitches[i], (cuuint64_t)(lvh[i].h + 2 * PS_BORDER)};
+    const cuuint64_t strides[1] = {(cuuint64_t)(pitches[i] * sizeof(float))};
+    const cuuint32_t es[2] = {1, 1};
+    for (int k = 0; k < 2; ++k)
+      if (encode(&maps[2 * i + k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base, dims, strides, boxes[k], es,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        fail(PS_ECUDA, "cuTensorMapEncodeTiled failed");
+  }
+  s->tmaps = dalloc<CUtensorMap>(s, maps.size());
+  cuda_ok(cudaMemcpyAsync(s->tmaps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice, s->st),
+          "upload tensor maps");
+}
+
 PsRun base_params(ps_session* s, int level) {
   PsRun P;
   memset(&P, 0, sizeof P);
@@ -398,6 +495,12 @@ PsRun base_params(ps_session* s, int level) {
   P.filter_gmax = s->cs.filter_gmax;
   P.weak_var = s->cs.weak_var;
   P.need_min = (int)s->fl.min_num_consistent;
+  P.fault = s->fault;
+  P.state_pixels = sl.total;
+  P.snap_pixels = (long long)s->snap_cap;
+  P.nviews_all = s->nv;
+  P.probe = s->fault && s->be && s->be->inject_kind == PS_INJECT_CHECK_PROBE && !s->capturing;
+  P.queue = s->qbuf;  // word 1 is the error word of every bounded wait (queue, TMA)
   return P;
 }
 
@@ -458,6 +561,8 @@ void timed_launch(ps_session* s, int kind, PsRun& P, F&& f, const char* what) {
 void collect_events(ps_session* s) {
   if (s->pending.empty()) return;
   cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize");
+  check_fault(s);
+  check_queue(s);
   for (auto& pd : s->pending) {
     float ms = 0.f;
     cuda_ok(cudaEventElapsedTime(&ms, pd.a, pd.b), "cudaEventElapsedTime");
@@ -470,7 +575,11 @@ void collect_events(ps_session* s) {
   s->pending.clear();
 }
 
-void sync(ps_session* s) { cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize"); }
+void sync(ps_session* s) {
+  cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize");
+  check_fault(s);
+  check_queue(s);
+}
 
 // Destroys every captured schedule graph: they hold device addresses of a buffer about to be replaced.
 void drop_graphs(ps_session* s) {
@@ -654,6 +763,31 @@ void run_batch(ps_session* s, const uint32_t* views, size_t a, size_t b, const p
   PsRun H = P;
   set_items(s, H, views, a, b, (int)p->level, s->L->half_lanes(s->tuning) == 2 ? PS_HALF2_PW : PS_HALF_PW,
             PS_HALF_PH);
+  if (s->L->half_run_ok(s->tuning, H.wr, H.ws)) {
+    // persistent kernel: up to PS_MAX_PHASES half steps per launch, over a zeroed queue
+    for (uint32_t t0 = 0; t0 < p->iterations; t0 += PS_MAX_PHASES / 2) {
+      const uint32_t n = std::min<uint32_t>(p->iterations - t0, PS_MAX_PHASES / 2);
+      H.nphases = (int)(2 * n);
+      for (uint32_t k = 0; k < 2 * n; ++k) {
+        PsPhase& q = H.phases[k];
+        q.t = (int)(t0 + k / 2);
+        q.color = (int)(k & 1);
+        ps_iter_consts(&s->pm, P.geometric, q.t, &q.tau_good, &q.eps, &q.phi);
+      }
+      H.queue = s->qbuf;
+      H.qstall = s->be && s->be->inject_kind == PS_INJECT_QUEUE_STALL && !s->capturing;
+      // the queue counter and the done counts; the error word (qbuf[1]) keeps what earlier launches set
+      cuda_ok(cudaMemsetAsync(s->qbuf, 0, sizeof(unsigned), s->st), "memset queue");
+      cuda_ok(cudaMemsetAsync(s->qbuf + 2, 0, (size_t)H.nphases * H.nitems * sizeof(unsigned), s->st),
+              "memset queue");
+      timed_launch(s, PS_KERNEL_HALF, H, [&](const PsRun& q) { return s->L->half_run(q, s->tuning, s->st); },
+                   "persistent half-step kernel");
+      s->q_used = true;
+    }
+    return;
+  }
+  H.tmaps = s->tmaps;
+  if (s->tmaps) s->q_used = true;  // the TMA waits report through the error word
   for (uint32_t t = 0; t < p->iterations; ++t) {
     H.t = (int)t;
     ps_iter_consts(&s->pm, P.geometric, (int)t, &H.tau_good, &H.eps, &H.phi);
@@ -707,11 +841,13 @@ int ps_backend_create(int device, const ps_options* opts, ps_backend** out) {
   be->device = device;
   ps_options_default(&be->opts);
   if (opts) be->opts = *opts;
-  if (be->opts.math_mode > PS_MATH_FAST || be->opts.checked || (be->opts.tuning & ~PS_TUNE_VALID_MASK)) {
+  if (be->opts.math_mode > PS_MATH_FAST || be->opts.checked > 1 ||
+      (be->opts.checked && be->opts.math_mode == PS_MATH_FAST) || (be->opts.tuning & ~PS_TUNE_VALID_MASK)) {
     delete be;
     return PS_EINVAL;
   }
-  be->name = std::string("b200(") + prop.name + (be->opts.math_mode == PS_MATH_FAST ? ", fast)" : ", parity)");
+  be->name = std::string("b200(") + prop.name +
+             (be->opts.checked ? ", parity, checked)" : be->opts.math_mode == PS_MATH_FAST ? ", fast)" : ", parity)");
   cudaMemPoolProps pp;
   memset(&pp, 0, sizeof pp);
   pp.allocType = cudaMemAllocationTypePinned;
@@ -747,7 +883,8 @@ const char* ps_last_error(const ps_session* s) { return s ? s->err.c_str() : "se
 uint64_t ps_launch_count(const ps_session* s) { return s ? s->launches : 0; }
 
 int ps_backend_inject_failure(ps_backend* be, uint32_t kind, uint32_t after) {
-  if (!be || kind > PS_INJECT_UPLOAD) return PS_EINVAL;
+  if (!be || kind > PS_INJECT_QUEUE_STALL) return PS_EINVAL;
+  if (kind == PS_INJECT_CHECK_PROBE && !be->opts.checked) return PS_EINVAL;
   std::lock_guard<std::mutex> g(be->mu);
   be->inject_kind = kind;
   be->inject_after = after;
@@ -789,7 +926,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     s->fl = in->filter;
     s->seed = in->seed;
     s->cs = ps_session_consts(&s->pm, &s->fl);
-    s->L = be->opts.math_mode == PS_MATH_FAST ? &kFast : &kParity;
+    s->L = be->opts.checked ? &kChecked : (be->opts.math_mode == PS_MATH_FAST ? &kFast : &kParity);
     s->tuning = be->opts.tuning;
     s->w.assign(s->nv * s->nl, 0);
     s->h.assign(s->nv * s->nl, 0);
@@ -828,6 +965,12 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     // module constants are set here, outside any stream capture (their copy is synchronous)
     cuda_ok(ps_parity::prepare(), "module constants");
     cuda_ok(ps_fast::prepare(), "module constants");
+    s->qbuf = dalloc<unsigned>(s, 2 + (size_t)PS_MAX_PHASES * PS_MAX_ITEMS);
+    if (be->opts.checked) {
+      cuda_ok(ps_checked::prepare(), "module constants");
+      s->fault = dalloc<unsigned long long>(s, 1);
+      cuda_ok(cudaMemsetAsync(s->fault, 0, sizeof(unsigned long long), s->st), "memset");
+    }
     // images: normalised f32 planes with a zero border.  8-bit images travel as bytes through the pinned staging
     // buffer and are expanded on the device with a table of the correctly rounded u/255 (the oracle's plane values);
     // f32 images are copied row by row into the bordered plane.
@@ -949,6 +1092,7 @@ int ps_begin(ps_backend* be, const ps_kernel_input* in, ps_session** out) {
     s->counters = dalloc<unsigned long long>(s, (1 + PS_STAGE_STATS) * PS_KERNEL_KINDS);
     cuda_ok(cudaMemsetAsync(s->counters, 0, (1 + PS_STAGE_STATS) * PS_KERNEL_KINDS * sizeof(unsigned long long), s->st), "memset");
     s->lvh = lvh;
+    if ((s->tuning & PS_TUNE_TMA) && (s->tuning & PS_TUNE_STAGED)) build_tensor_maps(s, lvh, offs, pitches);
     s->lv = dalloc<PsLevel>(s, lvh.size());
     cuda_ok(cudaMemcpyAsync(s->lv, lvh.data(), lvh.size() * sizeof(PsLevel), cudaMemcpyHostToDevice, s->st), "upload levels");
     // pairs, views, FP64 pair tables
@@ -1041,6 +1185,9 @@ int ps_end(ps_session* s) {
   dfree(s, s->has64);
   dfree(s, s->snap);
   dfree(s, s->snap_off);
+  dfree(s, s->qbuf);
+  dfree(s, s->tmaps);
+  dfree(s, s->fault);
   for (cudaTextureObject_t t : s->texs) cudaDestroyTextureObject(t);
   if (s->be) {  // arrays no session reused are freed; this session's arrays wait for the next one
     for (auto& c : s->be->arrays) cudaFreeArray(c.a);

@@ -223,7 +223,7 @@ class PatchMatchBackend:
     """CudaPatchMatch equivalent (crates/cuda/src/patchmatch.rs:91-298) on one B200."""
 
     def __init__(self, device: int = 0, math: str = "parity", max_batch: int = 64, batch_pixels: int = 0,
-                 tuning: int = 0):
+                 tuning: int = 0, checked: bool = False):
         self.lib = _lib.engine()
         o = _lib.Options()
         self.lib.ps_options_default(C.byref(o))
@@ -231,6 +231,7 @@ class PatchMatchBackend:
         o.max_batch = max_batch
         o.batch_pixels = batch_pixels
         o.tuning = tuning
+        o.checked = int(bool(checked))
         self.device = device
         h = C.c_void_p()
         rc = self.lib.ps_backend_create(device, C.byref(o), C.byref(h))
@@ -251,7 +252,9 @@ class PatchMatchBackend:
 
     def inject_failure(self, kind: int, after: int = 0) -> None:
         """Arms one host-side failure (ps_backend_inject_failure): after `after` more operations of `kind`
-        (_lib.PS_INJECT_DEVICE_ALLOC or PS_INJECT_UPLOAD) succeed, the next one fails; PS_INJECT_NONE disarms."""
+        (_lib.PS_INJECT_DEVICE_ALLOC or PS_INJECT_UPLOAD) succeed, the next one fails; PS_INJECT_NONE disarms.
+        PS_INJECT_CHECK_PROBE (checked backends): the next synchronising call fails with PS_EFAULT from the kernels'
+        own bounds test of one out-of-range index (no access is made)."""
         rc = self.lib.ps_backend_inject_failure(self.h, kind, after)
         if rc != _lib.PS_OK:
             raise PsError(rc, "ps_backend_inject_failure")

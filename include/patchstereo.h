@@ -32,7 +32,7 @@ extern "C" {
 #endif
 
 #define PS_MAX_SOURCES 32 /* crates/cuda/src/kernels/patchmatch.cu:40 (MAXSRC) */
-#define PS_ABI_VERSION 4
+#define PS_ABI_VERSION 5
 
 /* Status codes.  Maps the reference's error kinds: Error::InvalidArgument -> PS_EINVAL,
  * Error::Invariant("CUDA: …") -> PS_ECUDA (crates/cuda/src/patchmatch.rs:234-236),
@@ -64,7 +64,11 @@ typedef struct ps_options {
   uint32_t math_mode;    /* ps_math_mode */
   uint32_t max_batch;    /* views per launch; 0 = 64 (reference default) */
   uint64_t batch_pixels; /* pixel budget per launch; 0 = unbounded (HBM holds every view of a job) */
-  uint32_t checked;      /* reserved (bounds-checked build); must be 0 */
+  uint32_t checked;      /* 1 = bounds-checked kernels (parity math; not with PS_MATH_FAST): every data-dependent index
+                            is tested before its access, a failed test skips the access and the next synchronising
+                            call fails with PS_EFAULT naming the first violation; the results are those of the parity
+                            build.  The half step, evaluate, filter, upsample, median, readout and snapshot kernels are
+                            checked; post-processing, fusion, neighbours and the network are not. */
   uint32_t tuning;       /* half-step kernel variant, PS_TUNE_* flags; 0 = defaults (the autotuner sets these) */
 } ps_options;
 
@@ -74,7 +78,12 @@ typedef struct ps_options {
 #define PS_TUNE_ONE_LANE 0x4u        /* one thread per pixel (default: two lanes per pixel split the window rows) */
 #define PS_TUNE_ROW_PAIRS 0x8u       /* one thread per pixel, window rows 2p and 2p+1 as packed f32x2 pairs */
 #define PS_TUNE_STAGED 0x10u         /* row pairs, and each warp stages its sources' footprints in shared memory */
-#define PS_TUNE_VALID_MASK 0x1Fu
+#define PS_TUNE_PERSISTENT 0x20u     /* with PS_TUNE_ROW_PAIRS: one persistent launch per run over a device work queue of
+                                        (half step, tile) items with bounded per-view waits between half steps; a
+                                        wait that gives up fails the call with PS_ETIMEOUT */
+#define PS_TUNE_TMA 0x40u            /* with PS_TUNE_STAGED: the reference tile and the source boxes arrive by 2-D TMA
+                                        tensor loads (cp.async.bulk.tensor, no multicast) on mbarriers */
+#define PS_TUNE_VALID_MASK 0x7Fu
 
 /* PmParams (crates/dense/src/params.rs:76-124, defaults :126-154). */
 typedef struct ps_pm_params {
@@ -202,6 +211,15 @@ typedef struct ps_session ps_session;
 #define PS_INJECT_NONE 0u
 #define PS_INJECT_DEVICE_ALLOC 1u
 #define PS_INJECT_UPLOAD 2u
+/* Checked backends only: the kernels launched until the next synchronising call each test one index past the end of
+ * the state arrays (the test fails, no access is made), so that call fails with PS_EFAULT ("self-test probe"); the
+ * probe is then spent.  Captured schedules (CUDA graphs) do not carry it.  `after` is ignored. */
+#define PS_INJECT_CHECK_PROBE 3u
+/* Persistent half step (PS_TUNE_PERSISTENT): the launches until the next synchronising call make every wait of their
+ * queue need one tile more than exists, so the first wait runs out its bounded spin (about a second), the others
+ * return at once, and that call fails with PS_ETIMEOUT; the stall is then spent.  Not carried by captured schedules.
+ * `after` is ignored. */
+#define PS_INJECT_QUEUE_STALL 4u
 int ps_backend_inject_failure(ps_backend* be, uint32_t kind, uint32_t after);
 
 /* ---- defaults and diagnostics ------------------------------------------------------------------------------ */

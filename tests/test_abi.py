@@ -89,7 +89,7 @@ def test_null_arguments_rejected_without_device():
     assert lib.ps_end(None) == _lib.PS_EINVAL
     assert lib.ps_run(None, None, 0, None, None, None) == _lib.PS_EINVAL
     assert lib.ps_last_error(None) == b"session is NULL"
-    assert lib.ps_abi_version() == 4
+    assert lib.ps_abi_version() == 5
     # learned-proposal entry points
     assert lib.ps_net_create(0, 1, None) == _lib.PS_EINVAL
     assert lib.ps_net_num_params(None) == 0

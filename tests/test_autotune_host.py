@@ -31,7 +31,8 @@ class _FakeSession:
         pass
 
     def kernel_stats(self, kind):
-        return {"ms": {0: 5.0, 2: 4.0, 3: 3.5, 4: 2.5, 6: 3.0, 7: 2.75, 8: 2.6, 10: 2.7, 16: 2.9, 18: 2.8}[self.tuning]}
+        return {"ms": {0: 5.0, 2: 4.0, 3: 3.5, 4: 2.5, 6: 3.0, 7: 2.75, 8: 2.6, 10: 2.7, 16: 2.9, 18: 2.8, 42: 2.65,
+                       90: 2.85}[self.tuning]}
 
 
 class _FakeBackend:
@@ -59,9 +60,28 @@ def fake(monkeypatch):
 
 def test_key_size_classes():
     small = scenes.workload_small(96, 72).input
-    assert autotune._key("G", small, "parity") == "G|r3|s1|parity|S"
+    assert autotune._key("G", small, "parity") == "G|r3|s1|parity|S|n2"
     c1 = scenes.workload_c1().input
-    assert autotune._key("G", c1, "fast").endswith("|r5|s1|fast|S")  # 0.31 Mpix
+    assert autotune._key("G", c1, "fast").endswith("|r5|s1|fast|S|n2")  # 0.31 Mpix, 2 sources
+
+
+def test_key_of_a_mixed_batch_names_every_size_class_and_the_source_count():
+    """A batch of several image sizes keys on all of its size classes (not on its first view's) and on its largest
+    source count; the tuner's views include one of every size class."""
+    inp = scenes.workload_small(96, 72, views=4).input
+    big = scenes.workload_small(1024, 768, views=2).input
+    inp.views = inp.views + big.views
+    inp.views[-1].sources = list(range(5))
+    assert autotune._key("G", inp, "parity") == "G|r3|s1|parity|MS|n5"
+
+
+def test_tuning_views_cover_every_size_class(fake, tmp_path):
+    inp = scenes.workload_small(96, 72, views=6).input
+    n = len(inp.views)
+    big = scenes.workload_small(1024, 768, views=1).input
+    inp.views = inp.views + big.views
+    autotune.tune(inp, cache=tmp_path / "t.json", max_views=2, candidates=(0,))
+    assert fake.log[0][1] == (0, n)
 
 
 def test_picks_fastest_and_caches(fake, tmp_path):

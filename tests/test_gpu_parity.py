@@ -204,7 +204,8 @@ def test_bit_reproducible(backend):
         _assert_same(x, y, "rerun")
 
 
-@pytest.mark.parametrize("tuning", [1, 2, 3, 4, 5, 6, 7, 8, 10, 16, 18])
+# 42: row pairs + gather in the persistent kernel; 88 / 90: staged boxes loaded by TMA (without / with the gather)
+@pytest.mark.parametrize("tuning", [1, 2, 3, 4, 5, 6, 7, 8, 10, 16, 18, 42, 88, 90])
 def test_half_step_variants_bitwise_equal(tuning):
     """Every half-step kernel variant (weight cache off, texture gather, one lane per pixel, row-pair f32x2 loops,
     staged source boxes) gives the oracle's bits."""
@@ -221,7 +222,7 @@ def test_half_step_variants_bitwise_equal(tuning):
         _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning}")
 
 
-@pytest.mark.parametrize("tuning", [8, 10, 16, 18])
+@pytest.mark.parametrize("tuning", [8, 10, 16, 18, 42, 88, 90])
 @pytest.mark.parametrize("wr,ws", [(3, 1), (5, 1), (5, 2), (6, 1)])
 def test_row_pair_and_staged_variants_converged(tuning, wr, ws):
     """The row-pair and staged-box variants on every compiled window, over a photometric run long enough for the

@@ -590,7 +590,7 @@ def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, lo
         return e0.elapsed_time(e1) / steps
 
     def learned_step():
-        sess.propose(net, 0, mine, proposal.CONF_THRESHOLD, count=False)
+        sess.propose(net, 0, mine, args.learned_conf, count=False)
         sess.schedule_resident(mine, k, wl.geometric_rounds, gi, graph=not args.no_graph, proposal=True)
 
     sess.set_profiling(True)  # per-launch events for the sweep and network shares
@@ -707,38 +707,53 @@ def e2e_leg(args, wl, be, mine, world, rank, local, multi, views_total):
             "timer": "host wall clock around whole steps, max over ranks"}
 
 
-def cpu_sample(wl, threads=None, band=0.125):
-    """Times the CPU oracle on a band of rows (`band` of the height) of view 0: the run-start evaluate pass alone,
-    then evaluate + one red-black iteration; both scale to the full view by pixel count.  Returns full-view
-    estimates (t_eval, t_iter, per-view schedule time)."""
-    from cumulus3d_b200.patchstereo import RunParams, ViewState
+def _snapshot_maps(wl, st0, gt):
+    """Snapshot maps for view 0's geometric rounds: its own map, and its sources' ground truth when known (else view
+    0's map again; the geometric term's cost does not depend on the values)."""
+    maps = [None] * len(wl.cams)
+    for v in range(len(wl.cams)):
+        if gt is not None and v in gt:
+            maps[v] = gt[v]
+        elif (wl.cams[v].width, wl.cams[v].height) == (wl.cams[0].width, wl.cams[0].height):
+            maps[v] = st0.depth
+    maps[0] = st0.depth.copy()
+    return maps
+
+
+def cpu_sample(wl, threads=None, index=0, nbands=16, gt=None):
+    """Times the CPU oracle on band `index` of `nbands` equal bands of full-width rows of view 0, through the whole
+    per-view schedule: run start and the photometric iterations, the geometric rounds, the filter.  Scaled to the full
+    view by pixel count.  The cost per row varies over the image (the top rows of the drone views cost about a third
+    more than the average), so an estimate of the whole view averages the bands of a full cycle of indices.  Returns
+    (per-view seconds, rows)."""
+    from cumulus3d_b200.patchstereo import DepthSnapshot, RunParams, ViewState
     from oracle import oracle
-    v = [0]
     c = wl.cams[0]
-    rows = (0, max(8, int(c.height * band)))
-    scale = c.height / rows[1]
+    k = index % nbands
+    rows = (c.height * k // nbands, c.height * (k + 1) // nbands)
+    scale = c.height / (rows[1] - rows[0])
     st = [ViewState.new(c.width, c.height)]
     t0 = time.perf_counter()
-    oracle.run(wl.input, v, st, RunParams(0, False, True, 0, 1), threads=threads, rows=rows)
-    t_eval = (time.perf_counter() - t0) * scale
-    st = [ViewState.new(c.width, c.height)]
-    t0 = time.perf_counter()
-    oracle.run(wl.input, v, st, RunParams(0, False, True, 1, 1), threads=threads, rows=rows)
-    t_run = (time.perf_counter() - t0) * scale
-    t_iter = max(t_run - t_eval, 1e-9)
-    per_view = wl.iterations() * t_iter + (2 + wl.geometric_rounds) * t_eval
-    return t_eval, t_iter, per_view, rows
+    oracle.run(wl.input, [0], st, RunParams(0, False, True, wl.photometric_iters, 1), threads=threads, rows=rows)
+    for r in range(wl.geometric_rounds):
+        snap = DepthSnapshot(1 + r, 0, _snapshot_maps(wl, st[0], gt))
+        oracle.run(wl.input, [0], st, RunParams(0, True, False, wl.geometric_iters, 2 + r), snap, threads=threads,
+                   rows=rows)
+    oracle.filter(wl.input, [0], st, DepthSnapshot(1 + wl.geometric_rounds, 0, _snapshot_maps(wl, st[0], gt)),
+                  threads=threads, rows=rows)
+    return (time.perf_counter() - t0) * scale, rows
 
 
-def cpu_baseline(wl, args):
+def cpu_baseline(wl, args, nbands=16, picks=(1, 5, 9, 13)):
     cores = os.cpu_count() or 1
-    t_eval, t_iter, per_view, rows = cpu_sample(wl, cores)
+    est = [cpu_sample(wl, cores, k, nbands)[0] for k in picks]
+    per_view = sum(est) / len(est)
     return {"value": round(1.0 / per_view, 5), "unit": "views/s", "cores": cores, "kind": "port",
-            "sample": f"oracle (C++ restatement, OpenMP, all cores) on rows {rows[0]}-{rows[1]} of view 0 "
-                      f"(random init, evaluate pass, one red-black iteration), scaled by pixel count to a full view "
-                      f"(evaluate {t_eval:.2f} s, iteration {t_iter:.2f} s) and extrapolated to the per-view schedule "
-                      f"({wl.iterations()} iterations + {2 + wl.geometric_rounds} evaluate/filter passes)",
-            "mpix_iter_per_s": round(c_px(wl) / t_iter / 1e6, 3)}
+            "sample": f"oracle (C++ restatement, OpenMP, all cores) on bands {list(picks)} of {nbands} equal bands of "
+                      f"full-width rows of view 0, each through the whole per-view schedule ({wl.photometric_iters} "
+                      f"photometric + {wl.geometric_rounds}x{wl.geometric_iters} geometric iterations + filter) and "
+                      f"scaled by pixel count to a full view; the mean of the four",
+            "mpix_iter_per_s": round(c_px(wl) * wl.iterations() / per_view / 1e6, 3)}
 
 
 def c_px(wl):
@@ -782,8 +797,7 @@ def load_reference_workload(path: str):
 def cpu_whole_view(wl, gt, threads=None):
     """Times the CPU oracle on the whole of view 0 through its full per-view schedule: run start and the photometric
     iterations, the geometric rounds, the filter.  The snapshot holds view 0's own depth map and the ground truth of
-    its sources (their own maps would need their schedules first; the geometric cost does not depend on the values).
-    Returns seconds."""
+    its sources (_snapshot_maps; their own maps would need their schedules first).  Returns seconds."""
     from cumulus3d_b200.patchstereo import DepthSnapshot, RunParams, ViewState
     from oracle import oracle
     c = wl.cams[0]
@@ -791,24 +805,19 @@ def cpu_whole_view(wl, gt, threads=None):
     t0 = time.perf_counter()
     oracle.run(wl.input, [0], st, RunParams(0, False, True, wl.photometric_iters, 1), threads=threads)
     for r in range(wl.geometric_rounds):
-        maps = [None] * len(wl.cams)
-        for v, d in gt.items():
-            maps[v] = d
-        maps[0] = st[0].depth.copy()
         oracle.run(wl.input, [0], st, RunParams(0, True, False, wl.geometric_iters, 2 + r),
-                   DepthSnapshot(1 + r, 0, maps), threads=threads)
-    maps = [None] * len(wl.cams)
-    for v, d in gt.items():
-        maps[v] = d
-    maps[0] = st[0].depth.copy()
-    oracle.filter(wl.input, [0], st, DepthSnapshot(1 + wl.geometric_rounds, 0, maps), threads=threads)
+                   DepthSnapshot(1 + r, 0, _snapshot_maps(wl, st[0], gt)), threads=threads)
+    oracle.filter(wl.input, [0], st, DepthSnapshot(1 + wl.geometric_rounds, 0, _snapshot_maps(wl, st[0], gt)),
+                  threads=threads)
     return time.perf_counter() - t0
 
 
 def bench_reference(args, rank, world):
     """The reference arm: the CPU oracle (the restatement of the reference's PatchStereo, all host cores) on the
-    same workload and config.  Each step times a band of full-width rows of view 0 and extrapolates to the per-view
-    schedule; one whole view through its full schedule is timed once and reported beside it with their ratio."""
+    same workload and config.  Step i times band i mod 16 of full-width rows of view 0 (a sixteenth of its height)
+    through the whole per-view schedule, scaled by pixel count, and the value is the mean of the steps' estimates
+    (16 steps cover the view once); one whole view through the same schedule is timed once and reported beside it
+    with their ratio."""
     if rank != 0:
         return None
     import tempfile
@@ -817,14 +826,14 @@ def bench_reference(args, rank, world):
     subprocess.run([sys.executable, os.path.abspath(__file__), "--write-reference-workload", path], check=True)
     wl, gt = load_reference_workload(path)
     cores = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        cpu_sample(wl, cores, band=0.03)
+    for i in range(args.warmup):
+        cpu_sample(wl, cores, i, 64, gt=gt)
     per = []
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        per.append(cpu_sample(wl, cores)[2])
+    for i in range(args.steps):  # step i times band i mod 16; 16 steps cover the whole view once
+        per.append(cpu_sample(wl, cores, i, 16, gt=gt)[0])
     wall = time.perf_counter() - t0
-    per_view = statistics.median(per)
+    per_view = statistics.fmean(per)
     whole = None if args.no_whole_view else cpu_whole_view(wl, gt, cores)
     value = 1.0 / per_view
     res = {"impl": "reference", "metric": "PatchStereo views/s (drone-scale workload, 1 B200 per rank)",
@@ -833,9 +842,10 @@ def bench_reference(args, rank, world):
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded terrain renderer, no dataset)",
            "config": bench_config(wl, world, False, "parity"),
            "cpu_baseline": {"value": round(value, 5), "unit": "views/s", "cores": cores, "kind": "port",
-                            "sample": "per step: the CPU oracle (all cores) on the top eighth of view 0's rows "
-                                      "(evaluate pass + one iteration), scaled by pixel count and extrapolated to "
-                                      "the full per-view schedule; the reference ships no CPU PatchStereo and its "
+                            "sample": "step i: the CPU oracle (all cores) on band i mod 16 of view 0's rows (a "
+                                      "sixteenth of the height) through the whole per-view schedule (photometric "
+                                      "iterations, geometric rounds, filter), scaled by pixel count; value = 1 / the "
+                                      "mean of the steps' estimates; the reference ships no CPU PatchStereo and its "
                                       "Rust/CUDA code cannot be built here"},
            "e2e": {"value": round(value, 5), "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if whole is not None:
@@ -875,6 +885,8 @@ def main():
                     help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
     ap.add_argument("--learned-geo-iters", type=int, default=1,
                     help="iterations of the learned schedule's geometric round (the plain schedule's is 2)")
+    ap.add_argument("--learned-conf", type=float, default=0.5,
+                    help="confidence threshold of the proposals (random init below it)")
     ap.add_argument("--learned-iters", type=int, default=1,
                     help="photometric iterations of the learned-init schedule")
     ap.add_argument("--no-whole-view", action="store_true",

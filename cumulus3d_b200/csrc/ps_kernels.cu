@@ -1398,11 +1398,18 @@ __device__ __forceinline__ bool queue_wait(const PsRun& P, const unsigned* ctr, 
 // whatever the grid size.  When a wait gives up, the tile is skipped (its count is still added, so nothing waits on
 // it) and the run reports PS_ETIMEOUT; every later wait returns at once.  The tiles compute exactly what the
 // per-half-step launches compute, so the results are the same bits.
+//
+// A CTA that has seen phase k - 1 of a view complete (an acquire) needs no second wait for it: its later loads see
+// those stores.  It remembers the last completed phase per view (s_seen), so a CTA waits about once per view and
+// phase instead of once per tile.
 template <int WR, int WS, bool TEX>
 __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_q(const __grid_constant__ PsRun P) {
   extern __shared__ float sm[];
   __shared__ int s_item, s_go;
+  __shared__ int s_seen[PS_MAX_ITEMS];
   const int total = P.ntiles * P.nphases;
+  if (threadIdx.x < PS_MAX_ITEMS) s_seen[threadIdx.x] = -1;
+  __syncthreads();
   for (;;) {
     if (threadIdx.x == 0) {
       const int i = (int)atomicAdd(P.queue, 1u);
@@ -1411,9 +1418,12 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_q(const __grid_constant_
         const int k = i / P.ntiles, cta = i - k * P.ntiles;
         if (k > 0) {
           const int ii = find_item(P, cta);
-          const int next = ii + 1 < P.nitems ? P.items[ii + 1].tile0 : P.ntiles;
-          const unsigned need = (unsigned)(next - P.items[ii].tile0) + (P.qstall ? 1u : 0u);
-          go = queue_wait(P, P.queue + 2 + (size_t)(k - 1) * P.nitems + ii, need) ? 1 : 0;
+          if (s_seen[ii] < k - 1 || P.qstall) {
+            const int next = ii + 1 < P.nitems ? P.items[ii + 1].tile0 : P.ntiles;
+            const unsigned need = (unsigned)(next - P.items[ii].tile0) + (P.qstall ? 1u : 0u);
+            go = queue_wait(P, P.queue + 2 + (size_t)(k - 1) * P.nitems + ii, need) ? 1 : 0;
+            if (go) s_seen[ii] = k - 1;
+          }
         }
       }
       s_item = i;

@@ -338,10 +338,11 @@ def agreement(depth: np.ndarray, ref: np.ndarray, mask: Optional[np.ndarray] = N
 
 
 def evaluate_gain(net: ProposalNet, n_scenes: int = 6, seed: int = 90000, crop: int = 256, iters: int = 2,
-                  plain_iters: int = 6, depth_range=(25.0, 60.0), device: int = 0) -> dict:
+                  plain_iters: int = 6, depth_range=(25.0, 60.0), device: int = 0,
+                  threshold: float = CONF_THRESHOLD) -> dict:
     """Held-out crop scenes: agreement (within 1 % depth) with the plain `plain_iters`-iteration result, on pixels
     where that result's cost is below LABEL_MAX_COST, of (a) `iters` iterations from random init and (b) `iters`
-    iterations from the learned proposal (random init where the confidence is below CONF_THRESHOLD)."""
+    iterations from the learned proposal (random init where the confidence is below `threshold`)."""
     grp = [crop_scene(seed + i, crop, depth_range) for i in range(n_scenes)]
     inp, refs = crop_input(grp, depth_range)
     be = PatchMatchBackend(device, math="parity")
@@ -351,11 +352,11 @@ def evaluate_gain(net: ProposalNet, n_scenes: int = 6, seed: int = 90000, crop: 
     with be.begin(inp) as s:
         s.run(refs, plain, RunParams(0, False, True, plain_iters, 1))
         s.run(refs, rnd, RunParams(0, False, True, iters, 1))
-        proposed = s.propose(net, 0, refs, CONF_THRESHOLD)
+        proposed = s.propose(net, 0, refs, threshold)
         s.run(refs, lrn, RunParams(0, False, _lib.PS_INIT_PROPOSAL, iters, 1))
     be.close()
     a_r = [agreement(r.depth, p.depth, p.cost < LABEL_MAX_COST) for r, p in zip(rnd, plain)]
     a_l = [agreement(l.depth, p.depth, p.cost < LABEL_MAX_COST) for l, p in zip(lrn, plain)]
     return {"random": float(np.nanmean(a_r)), "learned": float(np.nanmean(a_l)),
             "proposed_fraction": proposed / float(len(refs) * crop * crop), "iters": iters,
-            "plain_iters": plain_iters, "scenes": n_scenes}
+            "plain_iters": plain_iters, "scenes": n_scenes, "threshold": threshold}

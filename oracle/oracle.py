@@ -50,6 +50,8 @@ def lib() -> C.CDLL:
             "oracle_evaluate": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
                                           C.POINTER(C.POINTER(C.c_float)), C.c_int]),
             "oracle_filter": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)), C.c_int]),
+            "oracle_filter_rows": (C.c_int, [_KI, _U32P, C.c_size_t, _SV, _SNAP, C.POINTER(C.POINTER(C.c_uint8)),
+                                             C.c_int, C.c_int, C.c_int]),
             "oracle_upsample": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_float, C.c_float, _SV, C.c_int]),
             "oracle_median": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, _SV, C.c_int]),
             "oracle_reeval_f64": (C.c_int, [_KI, C.c_uint32, _U32P, C.c_size_t, _SV, C.c_uint32, _SNAP,
@@ -154,12 +156,15 @@ def evaluate(inp: KernelInput, level: int, views: Sequence[int], states: List[Vi
 
 
 def filter(inp: KernelInput, views: Sequence[int], states: List[ViewState], snapshot: DepthSnapshot,
-           threads: Optional[int] = None) -> List[np.ndarray]:
+           threads: Optional[int] = None, rows=None) -> List[np.ndarray]:
+    """pm_filter restated: per-pixel consistent-source counts.  `rows` = (y0, y1) restricts the work to a band of
+    rows (timing samples only; the other rows of the counts are 0)."""
     ci, keep = CInput(inp), []
-    outs = [np.empty((s.height, s.width), np.uint8) for s in states]
+    outs = [np.zeros((s.height, s.width), np.uint8) for s in states]
     op = (C.POINTER(C.c_uint8) * max(len(outs), 1))(*[o.ctypes.data_as(C.POINTER(C.c_uint8)) for o in outs])
-    _chk(lib().oracle_filter(C.byref(ci.c), _views(views), len(views), c_states(states, keep),
-                             c_snapshot(snapshot, keep), op, _threads(threads)), "filter")
+    y0, y1 = rows if rows is not None else (0, 0)
+    _chk(lib().oracle_filter_rows(C.byref(ci.c), _views(views), len(views), c_states(states, keep),
+                                  c_snapshot(snapshot, keep), op, _threads(threads), int(y0), int(y1)), "filter")
     return outs
 
 

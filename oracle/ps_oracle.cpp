@@ -804,18 +804,27 @@ int oracle_run_init(const ps_kernel_input* in, const uint32_t* views, size_t n, 
     r.color = 0;
     r.tau_good = r.eps = r.phi = 0;
     r.proposal = (p->random_init == PS_INIT_PROPOSAL && proposals) ? proposals[i] : nullptr;
+    // work items of CHUNK columns of one row (pixels of one colour are independent, so the split changes no bits;
+    // small items keep the threads balanced on a narrow band)
+    constexpr int CHUNK = 64;
     const int ya = std::max(y0, 0), yb = y1 > 0 ? std::min(y1, st.h) : st.h;
+    const int cx = (st.w + CHUNK - 1) / CHUNK;
+    const long long items = (long long)std::max(yb - ya, 0) * cx;
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int y = ya; y < yb; ++y)
-      for (int x = 0; x < st.w; ++x) eval_pixel(r, st, x, y, 1, p->random_init);
+    for (long long k = 0; k < items; ++k) {
+      const int y = ya + (int)(k / cx), xa = (int)(k % cx) * CHUNK, xb = std::min(xa + CHUNK, st.w);
+      for (int x = xa; x < xb; ++x) eval_pixel(r, st, x, y, 1, p->random_init);
+    }
     for (uint32_t t = 0; t < p->iterations; ++t) {
       r.t = (int)t;
       ps_iter_consts(&sc.pm, p->geometric, (int)t, &r.tau_good, &r.eps, &r.phi);
       for (int color = 0; color < 2; ++color) {
         r.color = color;
 #pragma omp parallel for schedule(dynamic, 1)
-        for (int y = ya; y < yb; ++y)
-          for (int x = ((y + color) & 1); x < st.w; x += 2) half_pixel(r, st, x, y);
+        for (long long k = 0; k < items; ++k) {
+          const int y = ya + (int)(k / cx), xa = (int)(k % cx) * CHUNK, xb = std::min(xa + CHUNK, st.w);
+          for (int x = xa + ((y + color) & 1); x < xb; x += 2) half_pixel(r, st, x, y);
+        }
       }
     }
     from_state(st, states[i]);
@@ -906,8 +915,10 @@ int oracle_evaluate(const ps_kernel_input* in, uint32_t level, const uint32_t* v
   return PS_OK;
 }
 
-int oracle_filter(const ps_kernel_input* in, const uint32_t* views, size_t n, const ps_view_state* states,
-                  const ps_depth_snapshot* snap, uint8_t* const* out, int threads) {
+// Rows [y0, y1) only (y1 <= 0: all rows; the other rows of `out` are left as they are): the timing sample of the
+// CPU baseline filters the same band of rows it ran.
+int oracle_filter_rows(const ps_kernel_input* in, const uint32_t* views, size_t n, const ps_view_state* states,
+                       const ps_depth_snapshot* snap, uint8_t* const* out, int threads, int y0, int y1) {
   Scene sc;
   if (!load_scene(in, sc) || !snap) return PS_EINVAL;
   set_threads(threads);
@@ -922,11 +933,22 @@ int oracle_filter(const ps_kernel_input* in, const uint32_t* views, size_t n, co
     r.geometric = 1;
     r.topk = sc.cs.topk;
     r.snap = &maps;
+    constexpr int CHUNK = 64;
+    const int ya = y1 > 0 ? std::max(0, y0) : 0, yb = y1 > 0 ? std::min(st.h, y1) : st.h;
+    const int cx = (st.w + CHUNK - 1) / CHUNK;
+    const long long items = (long long)std::max(yb - ya, 0) * cx;
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int y = 0; y < st.h; ++y)
-      for (int x = 0; x < st.w; ++x) out[i][y * st.w + x] = (uint8_t)filter_pixel(r, st, x, y);
+    for (long long k = 0; k < items; ++k) {
+      const int y = ya + (int)(k / cx), xa = (int)(k % cx) * CHUNK, xb = std::min(xa + CHUNK, st.w);
+      for (int x = xa; x < xb; ++x) out[i][y * st.w + x] = (uint8_t)filter_pixel(r, st, x, y);
+    }
   }
   return PS_OK;
+}
+
+int oracle_filter(const ps_kernel_input* in, const uint32_t* views, size_t n, const ps_view_state* states,
+                  const ps_depth_snapshot* snap, uint8_t* const* out, int threads) {
+  return oracle_filter_rows(in, views, n, states, snap, out, threads, 0, 0);
 }
 
 // pm_upsample (patchmatch.cu:741-801), binary32.

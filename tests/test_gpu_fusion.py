@@ -145,6 +145,39 @@ def test_score_fusion_bitwise_vs_oracle(pipeline, opts):
             assert got.visibility(i) == want.visibility(i)
 
 
+@pytest.mark.parametrize("smooth", [0, 2])
+def test_score_fusion_with_visibility_and_smoothing_bitwise_vs_oracle(pipeline, smooth):
+    """fuse_depth_maps_with(.., Some(score)) with its off-by-default steps on (crates/dense/src/densify.rs:535-556):
+    the visibility filter over the adopted points, then `smooth` smoothing passes along normals, against the
+    restatement of the same steps.  The filter must remove points and the smoothing must move some."""
+    wl, views, s = pipeline
+    s.readout_resident(views, download=False)
+    s.postprocess_resident(0, views)
+    states = s.readout_download(0, views)
+    src = [list(kv.sources) for kv in wl.input.views]
+    fc = fusion.FusionCams(wl.cams, src)
+    imgs = [scenes.unit_plane(kv.levels[0].pixels) for kv in wl.input.views]
+    args = ([st.depth for st in states], [st.normal for st in states], [st.cost for st in states], imgs)
+    prm = fusion.default_score_fusion()
+    post = fusion.default_fusion(2)
+    post.visibility_check_views, post.visibility_min_violations, post.visibility_tau = 8, 1, 0.002
+    post.smooth_iterations, post.smooth_radius_gsd = smooth, 2.0
+    n = s.fuse_scored_resident(0, views, fc, prm, post=post)
+    got = s.fused_points()
+    want = oracle.fuse_scored(fc, *args, views, prm, post=post)
+    assert n == len(want) > 0
+    assert s.fused_visibility_removed == want.visibility_removed > 0
+    np.testing.assert_array_equal(got.keys, want.keys)
+    np.testing.assert_array_equal(got.positions, want.positions)
+    np.testing.assert_array_equal(got.normals, want.normals)
+    np.testing.assert_array_equal(got.vis_counts, want.vis_counts)
+    if smooth:
+        plain = fusion.default_fusion(2)
+        plain.visibility_check_views, plain.visibility_min_violations, plain.visibility_tau = 8, 1, 0.002
+        s.fuse_scored_resident(0, views, fc, prm, post=plain)
+        assert (s.fused_points().positions != got.positions).any()  # the smoothing moved points
+
+
 @pytest.mark.parametrize("residual", [0, 2])
 def test_visibility_filter_bitwise_vs_oracle(pipeline, residual):
     """filter_visibility (crates/dense/src/visibility.rs:106-151) on the device cloud against the restatement: the

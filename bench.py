@@ -559,7 +559,7 @@ def net_flop_per_pixel():
 def learned_leg(args, wl, sess, stream, mine, plain_value, plain_ms, barrier, local):
     """The learned-init schedule on the same resident session: ps_propose (plane sweep + proposal network + decode)
     then the schedule with `--learned-iters` photometric iterations from the proposals (random init where the
-    confidence is below 0.5), a geometric round of `--learned-geo-iters` iterations, filter and readout.  Timed like the plain step; accuracy is
+    confidence is below `--learned-conf`), a geometric round of `--learned-geo-iters` iterations, filter and readout.  Timed like the plain step; accuracy is
     the agreement of the final filtered depth with the plain schedule's (within 1 % depth on the pixels the plain
     result keeps), next to the plain schedule's agreement with itself under another RNG seed and to a plain schedule
     shortened to the same iteration count."""
@@ -885,9 +885,9 @@ def main():
                     help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
     ap.add_argument("--learned-geo-iters", type=int, default=1,
                     help="iterations of the learned schedule's geometric round (the plain schedule's is 2)")
-    ap.add_argument("--learned-conf", type=float, default=0.5,
+    ap.add_argument("--learned-conf", type=float, default=0.3,
                     help="confidence threshold of the proposals (random init below it)")
-    ap.add_argument("--learned-iters", type=int, default=1,
+    ap.add_argument("--learned-iters", type=int, default=2,
                     help="photometric iterations of the learned-init schedule")
     ap.add_argument("--no-whole-view", action="store_true",
                     help="reference arm: skip the single whole-view timing of the CPU oracle")

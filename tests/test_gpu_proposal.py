@@ -235,15 +235,15 @@ def test_learned_init_beats_random_init_on_held_out_scenes(seed):
     """The gain of the committed network: on held-out crop scenes (seeds far from the training set's 1000-1599),
     one photometric iteration from the learned proposal agrees with the converged plain result (6 iterations, within
     1 % depth, on the pixels that result trusts) on clearly more pixels than one iteration from random init.  Both
-    start from the same seeded draws; the proposal replaces them where the network's confidence reaches 0.5.
-    Measured on a B200: 79.5 % vs 73.9 % (seed 90000) and 78.6 % vs 74.0 % (seed 91000)."""
+    start from the same seeded draws; the proposal replaces them where the network's confidence reaches
+    CONF_THRESHOLD (0.3).  Measured on a B200 (seed 90000): 92.5 % vs 73.9 %, proposals on 84 % of the pixels."""
     net = proposal.ProposalNet(0, weights=proposal.DEFAULT_WEIGHTS)
     try:
         g = proposal.evaluate_gain(net, n_scenes=8, seed=seed, iters=1)
     finally:
         net.close()
-    assert g["proposed_fraction"] > 0.1, g
-    assert g["learned"] >= g["random"] + 0.02, g
+    assert g["proposed_fraction"] > 0.5, g
+    assert g["learned"] >= g["random"] + 0.08, g
 
 
 def test_sweep_with_ground_normals_bitwise_vs_oracle():

@@ -1022,6 +1022,15 @@ __device__ __forceinline__ void count_windows(const PsRun& P, int nwin) {
   if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s) atomicAdd(P.ncc_count, (unsigned long long)s);
 }
 
+// Profiling: refinement windows skipped because the candidate's partial cost had reached the best cost (the
+// half-step kernels' early exit), into staged-statistics slot 6 of the launch's kind.
+__device__ __forceinline__ void count_skipped(const PsRun& P, int n) {
+  if (!P.stage_count) return;
+  const unsigned m = __activemask();
+  const unsigned s = __reduce_add_sync(m, (unsigned)n);
+  if ((int)(threadIdx.x & 31) == __ffs(m) - 1 && s) atomicAdd(P.stage_count + 6, (unsigned long long)s);
+}
+
 // Half-step tile geometry for G lanes per pixel: G = 1 -> 32 × 8 pixels (a warp = 16 active columns × 2 rows);
 // G = 2 -> 16 × 8 pixels (a warp = 8 active columns × 2 rows × 2 lanes).  The shared tile's row pitch is padded so
 // that the lanes of one warp read 32 distinct banks: even for G = 1, ≡ 16 (mod 32) for G = 2.  The staged kernel's
@@ -1326,7 +1335,12 @@ __device__ __forceinline__ void half_tile(const PsRun& P, const HalfPhase& ph, i
   agg_finish(ag, hyp, nsrc, wv, NT, best, bcost);
 
   // 3. Refinement, 6 hypotheses (patchmatch.cu:596-628), then 4. the coarse-scale candidate (:629-653).
+  // A candidate's cost nm / den only grows as sources are added (every term wj·(mm + λ·g) is finite and ≥ 0, and
+  // round-to-nearest addition and division by den > 0 are monotone), so once the partial cost reaches bcost the
+  // candidate cannot be adopted (the test is cc < bcost) and its remaining windows are skipped: same decisions,
+  // same bits.
   Refine rf;
+  int nskip = 0;
   refine_prior(P, base + pix, rs.var, ray, rf);
   refine_draw(P, ph, vd, pix, ray, best, rf);
 #pragma unroll 1
@@ -1335,10 +1349,16 @@ __device__ __forceinline__ void half_tile(const PsRun& P, const HalfPhase& ph, i
     float cc;
     if (ag.den > 0.f) {
       float nm = 0.f;
+      bool beaten = false;
 #pragma unroll 1
-      for (int j = 0; j < nsrc; ++j) {
+      for (int j = 0; j < nsrc; ++j) {  // no break: the warp's lanes keep stepping through the sources together
         const float wj = wv[j * NT];
         if (!(wj > 0.f)) continue;
+        beaten = beaten || nm / ag.den >= bcost;
+        if (beaten) {
+          nskip++;
+          continue;
+        }
         const PsPair& pr = prs[j];
         const PsLPair lp = lps[j];
         const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
@@ -1348,7 +1368,7 @@ __device__ __forceinline__ void half_tile(const PsRun& P, const HalfPhase& ph, i
         const float g = P.geometric ? fminf(geo_error(P, R, S, pr, x, y, cd.w), P.gmax) : 0.f;
         nm += wj * (mm + P.lambda * g);
       }
-      cc = nm / ag.den;
+      cc = beaten ? bcost : nm / ag.den;
     } else {
       cc = 2.f;
     }
@@ -1363,6 +1383,7 @@ __device__ __forceinline__ void half_tile(const PsRun& P, const HalfPhase& ph, i
     P.bview[base + pix] = (unsigned char)ag.vbest;
   }
   count_windows(P, gl == 0 ? nwin : 0);
+  count_skipped(P, gl == 0 ? nskip : 0);
 }
 
 template <int WR, int WS, bool CW, bool TEX, int G, int MODE = 0>
@@ -1550,6 +1571,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
   agg_init(ag);
   float m[9], gg[9];
   float prior = 0.f, nm = 0.f;
+  int nskip = 0;
   bool use = false;
   float4 best = hyp[0];
   float bcost = 2.f;
@@ -1588,7 +1610,12 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
     } else {
       hv = refine_candidate(rf, c);
       wj = wv[j * NT];
+      // the candidate's partial cost already reaches bcost: its remaining windows cannot change the outcome
       act = c < rf.ncand && ag.den > 0.f && live && wj > 0.f;
+      if (act && nm / ag.den >= bcost) {
+        act = false;
+        nskip++;
+      }
     }
     float mv = 2.f;
     if (__any_sync(FULL, act)) {
@@ -1626,6 +1653,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
     P.bview[base + pix] = (unsigned char)ag.vbest;
   }
   count_windows(P, nwin);
+  count_skipped(P, nskip);
   if (P.stage_count) {
     const unsigned c0 = __reduce_add_sync(FULL, (unsigned)bs.nstaged), c2 = __reduce_add_sync(FULL, (unsigned)bs.nbound);
     const unsigned c3 = __reduce_add_sync(FULL, (unsigned)bs.nwide), c4 = __reduce_add_sync(FULL, (unsigned)bs.ntall);

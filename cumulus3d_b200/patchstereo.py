@@ -532,7 +532,8 @@ class PatchMatchSession:
         st = (C.c_uint64 * 8)()
         self._check(self.lib.ps_kernel_staged_stats(self.h, kind, st))
         return {"ms": ms.value, "launches": n.value, "ncc_windows": w.value, "staged_windows": st[0],
-                "box_restages": st[1], "unstaged": {"bound": st[2], "wide": st[3], "tall": st[4], "few_lanes": st[5]}}
+                "box_restages": st[1], "unstaged": {"bound": st[2], "wide": st[3], "tall": st[4], "few_lanes": st[5]},
+                "skipped_windows": st[6]}
 
     def reset_stats(self) -> None:
         self._check(self.lib.ps_reset_stats(self.h))

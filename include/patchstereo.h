@@ -615,7 +615,9 @@ int ps_reset_stats(ps_session* s);
 /* With profiling on, the staged half step (PS_TUNE_STAGED) also counts, into stats[8]: [0] NCC windows whose taps
  * read a warp's staged source box, [1] box restages (per warp), and the windows left to the per-lane loops because
  * [2] a footprint was not bounded, [3] the warp's footprint union was too wide or [4] too tall for the box, or [5] too
- * few lanes were active; [6], [7] are 0.  All are 0 for the other variants and kernel kinds. */
+ * few lanes were active (0 for the other variants and kernel kinds).  Every half-step variant counts into [6] the
+ * refinement windows it skipped because the candidate's partial cost had already reached the best cost (the result
+ * is the same as evaluating them).  [7] is 0. */
 int ps_kernel_staged_stats(ps_session* s, uint32_t kind, uint64_t* stats);
 /* Measured FP32 FMA throughput of the device (TFLOP/s, FMA = 2 FLOP) from a register-resident FFMA loop. */
 int ps_measure_fp32_peak(int device, double* tflops);

@@ -244,6 +244,29 @@ def test_row_pair_and_staged_variants_converged(tuning, wr, ws):
         _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning} wr={wr} ws={ws}")
 
 
+@pytest.mark.parametrize("tuning", [0, 10, 18, 42])
+def test_refinement_early_exit_skips_windows_and_keeps_bits(tuning):
+    """A refinement candidate whose partial cost (sum over the sources so far / den) already reaches the best cost is
+    rejected without its remaining windows: the kernels count the skipped windows, and the results still equal the
+    oracle, which evaluates every window."""
+    from cumulus3d_b200 import _lib
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    wl = scenes.workload_small(128, 96, views=4, window_radius=6, seed=44)
+    p = RunParams(0, False, True, 4, 1)
+    gpu, cpu = _states(wl), _states(wl)
+    be = PatchMatchBackend(0, math="parity", tuning=tuning)
+    with be.begin(wl.input) as s:
+        s.set_profiling(True)
+        s.run(wl.views, gpu, p)
+        st = s.kernel_stats(_lib.PS_KERNEL_HALF)
+    be.close()
+    oracle.run(wl.input, wl.views, cpu, p)
+    for i in range(len(gpu)):
+        _assert_same(gpu[i], cpu[i], f"view {i} tuning={tuning}")
+    assert st["skipped_windows"] > 0, st
+    assert st["ncc_windows"] > st["skipped_windows"], st
+
+
 def test_batched_mixed_sizes_equal_single_view_runs(backend):
     """One flattened launch over views of uneven sizes and source counts gives each view the bits of a run of that
     view alone (the batched configuration's per-view check)."""

@@ -178,6 +178,9 @@ struct ps_session {
   const Launchers* L = &kParity;
   unsigned long long* fault = nullptr;  // checked build: the kernels' fault word (device), else null
   unsigned* qbuf = nullptr;             // persistent half step: queue counter, error word, per-phase done counts
+  std::vector<cudaEvent_t> xfer;        // per-view copy events of the host-state transfers (pack/unpack overlap)
+  cudaStream_t up = nullptr, down = nullptr;  // copy streams of the pipelined host-state runs
+  std::vector<cudaEvent_t> stage_ev;          // their chunk events
   CUtensorMap* tmaps = nullptr;         // TMA staging: two maps per (view, level) plane (tile box, source box)
   bool q_used = false;                  // a persistent launch was issued since the last check of its error word
   int nv = 0, nl = 0;
@@ -558,6 +561,15 @@ void timed_launch(ps_session* s, int kind, PsRun& P, F&& f, const char* what) {
   s->kind_launches[kind]++;
 }
 
+// At least n copy events for the host-state transfers.
+void xfer_events(ps_session* s, size_t n) {
+  while (s->xfer.size() < n) {
+    cudaEvent_t e;
+    cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    s->xfer.push_back(e);
+  }
+}
+
 void collect_events(ps_session* s) {
   if (s->pending.empty()) return;
   cuda_ok(cudaStreamSynchronize(s->st), "cudaStreamSynchronize");
@@ -622,25 +634,21 @@ void upload_planes(ps_session* s, const uint32_t* views, size_t a, size_t b, con
   size_t total = 0;
   for (size_t i = a; i < b; ++i) total += (size_t)states[i].width * states[i].height;
   float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * sizeof(float4) * (with_prior ? 2 : 1));
+  for (size_t i = a; i < b; ++i) {  // every view is checked before any copy is issued
+    check_state(s, (int)views[i], level, states[i]);
+    if (!states[i].depth || !states[i].normal) fail(PS_EINVAL, "state depth/normal is NULL");
+  }
   size_t o = 0;
-  std::vector<size_t> so;
-  for (size_t i = a; i < b; ++i) {
+  float4* dst = dst_base ? dst_base : sl.plane;
+  for (size_t i = a; i < b; ++i) {  // each view's copy starts as soon as it is packed, while the next view is packed
     const ps_view_state& st = states[i];
-    check_state(s, (int)views[i], level, st);
-    if (!st.depth || !st.normal) fail(PS_EINVAL, "state depth/normal is NULL");
-    so.push_back(o);
     const long long n = (long long)st.width * st.height;
     float4* q = stage + o;
 #pragma omp parallel for schedule(static) if (n > 65536)
     for (long long p = 0; p < n; ++p) q[p] = make_float4(st.normal[3 * p], st.normal[3 * p + 1], st.normal[3 * p + 2], st.depth[p]);
-    o += (size_t)n;
-  }
-  float4* dst = dst_base ? dst_base : sl.plane;
-  for (size_t i = a; i < b; ++i) {
-    const size_t n = (size_t)states[i].width * states[i].height;
-    cuda_ok(cudaMemcpyAsync(dst + sl.off[views[i]], stage + so[i - a], n * sizeof(float4), cudaMemcpyHostToDevice,
-                            s->st),
+    cuda_ok(cudaMemcpyAsync(dst + sl.off[views[i]], q, (size_t)n * sizeof(float4), cudaMemcpyHostToDevice, s->st),
             "upload planes");
+    o += (size_t)n;
   }
   if (with_prior) {
     float4* pst = stage + total;
@@ -671,11 +679,16 @@ void download_states(ps_session* s, const uint32_t* views, size_t a, size_t b, p
   for (size_t i = a; i < b; ++i) total += (size_t)s->W(views[i], level) * s->H(views[i], level);
   float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * (sizeof(float4) + sizeof(float)));
   float* cst = (float*)(stage + total);
+  for (size_t i = a; i < b; ++i) {  // every view is checked before any copy is issued
+    check_state(s, (int)views[i], level, states[i]);
+    if (planes && (!states[i].depth || !states[i].normal)) fail(PS_EINVAL, "state depth/normal is NULL");
+    if (costs && !states[i].cost) fail(PS_EINVAL, "state cost is NULL");
+  }
   size_t o = 0;
   std::vector<size_t> so;
+  xfer_events(s, b - a);
   for (size_t i = a; i < b; ++i) {
     const int v = (int)views[i];
-    check_state(s, v, level, states[i]);
     const size_t n = (size_t)s->W(v, level) * s->H(v, level);
     so.push_back(o);
     if (planes)
@@ -685,15 +698,16 @@ void download_states(ps_session* s, const uint32_t* views, size_t a, size_t b, p
     if (costs)
       cuda_ok(cudaMemcpyAsync(cst + o, sl.cost + sl.off[v], n * sizeof(float), cudaMemcpyDeviceToHost, s->st),
               "download cost");
+    cuda_ok(cudaEventRecord(s->xfer[i - a], s->st), "cudaEventRecord");
     o += n;
   }
-  sync(s);
+  // each view is unpacked as soon as its own copies are done, while the later views' copies run
   for (size_t i = a; i < b; ++i) {
+    cuda_ok(cudaEventSynchronize(s->xfer[i - a]), "cudaEventSynchronize");
     ps_view_state& st = states[i];
     const long long n = (long long)st.width * st.height;
     const float4* q = stage + so[i - a];
     if (planes) {
-      if (!st.depth || !st.normal) fail(PS_EINVAL, "state depth/normal is NULL");
 #pragma omp parallel for schedule(static) if (n > 65536)
       for (long long p = 0; p < n; ++p) {
         st.normal[3 * p] = q[p].x;
@@ -703,10 +717,10 @@ void download_states(ps_session* s, const uint32_t* views, size_t a, size_t b, p
       }
     }
     if (costs) {
-      if (!st.cost) fail(PS_EINVAL, "state cost is NULL");
       memcpy(st.cost, cst + so[i - a], n * sizeof(float));
     }
   }
+  sync(s);  // fault and error words
 }
 
 // Uploads a host snapshot (re-uploaded only when its id or level changes, cf. Session::ensure_snapshot,
@@ -1187,6 +1201,7 @@ int ps_end(ps_session* s) {
   dfree(s, s->snap_off);
   dfree(s, s->qbuf);
   dfree(s, s->tmaps);
+  for (cudaEvent_t e : s->xfer) cudaEventDestroy(e);
   dfree(s, s->fault);
   for (cudaTextureObject_t t : s->texs) cudaDestroyTextureObject(t);
   if (s->be) {  // arrays no session reused are freed; this session's arrays wait for the next one
@@ -1218,7 +1233,12 @@ int ps_end(ps_session* s) {
   } else if (s->pin) {
     cudaFreeHost(s->pin);
   }
+  if (s->up) cudaStreamSynchronize(s->up);
+  if (s->down) cudaStreamSynchronize(s->down);
   if (s->st) cudaStreamDestroy(s->st);
+  if (s->up) cudaStreamDestroy(s->up);
+  if (s->down) cudaStreamDestroy(s->down);
+  for (cudaEvent_t e : s->stage_ev) cudaEventDestroy(e);
   cudaGetLastError();
   if (s->be) {
     std::lock_guard<std::mutex> g(s->be->mu);
@@ -1267,6 +1287,113 @@ int ps_run_resident(ps_session* s, const uint32_t* views, size_t n, const ps_run
   });
 }
 
+namespace {
+// Host-state runs of at least this many pixels are pipelined (run_pipelined); smaller ones gain nothing from it.
+constexpr size_t kPipelinePixels = size_t(1) << 22;
+
+// A photometric or geometric run of views[a, b) with host states, pipelined: the views go in up to three chunks of
+// about equal pixel count, and while chunk k runs on the session stream, chunk k + 1's states are packed on the host
+// and copied in on one copy stream, and chunk k - 1's results are copied out on the other and unpacked.  Views are
+// independent within a run, so the chunks compute exactly what one launch over all of them computes.
+void run_pipelined(ps_session* s, const uint32_t* views, size_t a, size_t b, ps_view_state* states,
+                   const ps_run_params* p) {
+  const int level = (int)p->level;
+  Slot& sl = slot(s, level);
+  const bool upload = !p->random_init;
+  std::vector<size_t> px(b - a);
+  size_t total = 0;
+  for (size_t i = a; i < b; ++i) {
+    check_state(s, (int)views[i], level, states[i]);
+    if (!states[i].depth || !states[i].normal || !states[i].cost) fail(PS_EINVAL, "state depth/normal/cost is NULL");
+    px[i - a] = (size_t)states[i].width * states[i].height;
+    total += px[i - a];
+  }
+  // chunk boundaries by pixel count
+  std::vector<size_t> cut{a};
+  const int K = (int)std::min<size_t>(3, b - a);
+  size_t acc = 0;
+  for (size_t i = a; i < b; ++i) {
+    acc += px[i - a];
+    if (cut.size() < (size_t)K && i + 1 < b && acc * K >= total * cut.size()) cut.push_back(i + 1);
+  }
+  cut.push_back(b);
+  const int nk = (int)cut.size() - 1;
+  if (upload) maybe_inject(s, PS_INJECT_UPLOAD, "upload states");
+  // pinned staging: [uploads (float4)][downloads (float4)][costs (float)]
+  float4* stage = (float4*)pinned(s, std::max<size_t>(total, 1) * (2 * sizeof(float4) + sizeof(float)));
+  float4* upst = stage;
+  float4* dnst = stage + total;
+  float* cst = (float*)(stage + 2 * total);
+  std::vector<size_t> so(b - a);
+  for (size_t i = a, o = 0; i < b; ++i) {
+    so[i - a] = o;
+    o += px[i - a];
+  }
+  if (!s->up) cuda_ok(cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking), "cudaStreamCreate");
+  if (!s->down) cuda_ok(cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking), "cudaStreamCreate");
+  while (s->stage_ev.size() < (size_t)(2 * nk)) {
+    cudaEvent_t e;
+    cuda_ok(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+    s->stage_ev.push_back(e);
+  }
+  xfer_events(s, b - a);
+  auto pack_upload = [&](int k) {
+    for (size_t i = cut[k]; i < cut[k + 1]; ++i) {
+      const ps_view_state& st = states[i];
+      const long long n = (long long)px[i - a];
+      float4* q = upst + so[i - a];
+#pragma omp parallel for schedule(static) if (n > 65536)
+      for (long long q2 = 0; q2 < n; ++q2)
+        q[q2] = make_float4(st.normal[3 * q2], st.normal[3 * q2 + 1], st.normal[3 * q2 + 2], st.depth[q2]);
+      cuda_ok(cudaMemcpyAsync(sl.plane + sl.off[views[i]], q, (size_t)n * sizeof(float4), cudaMemcpyHostToDevice,
+                              s->up),
+              "upload planes");
+    }
+    cuda_ok(cudaEventRecord(s->stage_ev[2 * k], s->up), "cudaEventRecord");
+    cuda_ok(cudaStreamWaitEvent(s->st, s->stage_ev[2 * k], 0), "cudaStreamWaitEvent");
+  };
+  auto download = [&](int k) {
+    cuda_ok(cudaStreamWaitEvent(s->down, s->stage_ev[2 * k + 1], 0), "cudaStreamWaitEvent");
+    for (size_t i = cut[k]; i < cut[k + 1]; ++i) {
+      const size_t n = px[i - a];
+      cuda_ok(cudaMemcpyAsync(dnst + so[i - a], sl.plane + sl.off[views[i]], n * sizeof(float4),
+                              cudaMemcpyDeviceToHost, s->down),
+              "download planes");
+      cuda_ok(cudaMemcpyAsync(cst + so[i - a], sl.cost + sl.off[views[i]], n * sizeof(float), cudaMemcpyDeviceToHost,
+                              s->down),
+              "download cost");
+      cuda_ok(cudaEventRecord(s->xfer[i - a], s->down), "cudaEventRecord");
+    }
+  };
+  auto unpack = [&](int k) {
+    for (size_t i = cut[k]; i < cut[k + 1]; ++i) {
+      cuda_ok(cudaEventSynchronize(s->xfer[i - a]), "cudaEventSynchronize");
+      ps_view_state& st = states[i];
+      const long long n = (long long)px[i - a];
+      const float4* q = dnst + so[i - a];
+#pragma omp parallel for schedule(static) if (n > 65536)
+      for (long long q2 = 0; q2 < n; ++q2) {
+        st.normal[3 * q2] = q[q2].x;
+        st.normal[3 * q2 + 1] = q[q2].y;
+        st.normal[3 * q2 + 2] = q[q2].z;
+        st.depth[q2] = q[q2].w;
+      }
+      memcpy(st.cost, cst + so[i - a], (size_t)n * sizeof(float));
+    }
+  };
+  for (int k = 0; k < nk; ++k) {
+    if (upload) pack_upload(k);
+    run_batch(s, views, cut[k], cut[k + 1], p, false);
+    cuda_ok(cudaEventRecord(s->stage_ev[2 * k + 1], s->st), "cudaEventRecord");
+    download(k);
+    if (k > 0) unpack(k - 1);  // chunk k runs meanwhile
+  }
+  unpack(nk - 1);
+  cuda_ok(cudaStreamSynchronize(s->up), "cudaStreamSynchronize");
+  sync(s);  // fault and error words
+}
+}  // namespace
+
 int ps_run(ps_session* s, const uint32_t* views, size_t n, ps_view_state* states, const ps_run_params* p,
            const ps_depth_snapshot* snapshot) {
   return guard(s, [&] {
@@ -1280,6 +1407,12 @@ int ps_run(ps_session* s, const uint32_t* views, size_t n, ps_view_state* states
     Slot& sl = slot(s, level);
     for (auto [a, b] : batches(s, views, n, level)) {
       for (size_t i = a; i < b; ++i) check_state(s, (int)views[i], level, states[i]);
+      size_t px = 0;
+      for (size_t i = a; i < b; ++i) px += (size_t)states[i].width * states[i].height;
+      if (!p->use_prior && p->random_init != PS_INIT_PROPOSAL && b - a >= 2 && px >= kPipelinePixels) {
+        run_pipelined(s, views, a, b, states, p);
+        continue;
+      }
       bool all_prior = true;
       for (size_t i = a; i < b; ++i) all_prior = all_prior && states[i].prior != nullptr;
       if (!p->random_init || (p->use_prior && all_prior)) {

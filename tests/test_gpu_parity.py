@@ -129,6 +129,37 @@ def test_resident_path_equals_host_path(backend):
         _assert_same(a, b, "resident")
 
 
+def test_pipelined_host_runs_equal_resident_runs(backend):
+    """Host-state runs of at least 2^22 pixels go through the pipelined path (chunks of views whose state copies and
+    host packing overlap the other chunks' runs on two copy streams).  A photometric run from random init and a
+    continuation that uploads the states must give the resident path's bits, and a geometric run must give the bits
+    of one-view runs (the unpipelined path) from the same states and snapshot."""
+    wl = scenes.workload_small(1280, 960, views=4, window_radius=5, seed=61)
+    p1 = RunParams(0, False, True, 2, 1)
+    p2 = RunParams(0, False, False, 1, 2)
+    p3 = RunParams(0, True, False, 1, 3)
+    host = _states(wl)
+    with backend.begin(wl.input) as s:
+        s.run(wl.views, host, p1)
+        s.run(wl.views, host, p2)
+        mid_host = [h.copy() for h in host]
+        snap = DepthSnapshot(1, 0, [h.depth.copy() for h in host])
+        s.run(wl.views, host, p3, snap)
+    with backend.begin(wl.input) as s:
+        s.run_resident(wl.views, p1)
+        s.run_resident(wl.views, p2)
+        mid = s.download(0, wl.views)
+    for a, b in zip(mid_host, mid):
+        _assert_same(a, b, "pipelined photometric runs")
+    ref = [m.copy() for m in mid]
+    with backend.begin(wl.input) as s:
+        for v in wl.views:
+            one = [ref[v]]
+            s.run([v], one, p3, snap)
+    for a, b in zip(host, ref):
+        _assert_same(a, b, "pipelined geometric run")
+
+
 def test_c1_bitwise_vs_oracle(backend):
     """The small drone configuration exactly: 3 × 640×480 8-bit views, each a reference with the other two as
     sources, depth 25-60 m, 11×11 window, 5 red-black iterations from random init; all three views equal the oracle

@@ -1089,6 +1089,135 @@ cudaError_t launch_u8_plane(const unsigned char* in, int w, int h, const float* 
   return cudaGetLastError();
 }
 
+// ------------------------------------------------------------------------------------------- fused cloud order
+// Cell of point i (see CloudOrderArgs), or -1 when the point was not kept or its key names no fused view.
+__device__ __forceinline__ long long cloud_cell(const CloudOrderArgs& A, unsigned long long i) {
+  if (A.keep && !A.keep[i]) return -1;
+  if (A.gid) return A.gid[i] < A.cells ? (long long)A.gid[i] : -1;
+  const unsigned long long k = A.key[i];
+  const unsigned id = (unsigned)(k >> 32);
+  const int row = (int)((k >> 16) & 0xffffu), col = (int)(k & 0xffffu);
+  if (A.nids <= 0) return -1;
+  int lo = 0, hi = A.nids - 1;
+  while (lo < hi) {  // the fused views' image ids are ascending and distinct
+    const int mid = (lo + hi) >> 1;
+    if (A.ids[mid] < id) lo = mid + 1;
+    else hi = mid;
+  }
+  if (A.ids[lo] != id || col >= A.width[lo]) return -1;
+  const unsigned long long cell = A.base[lo] + (unsigned long long)row * A.width[lo] + col;
+  if (cell >= A.cells) return -1;  // never for keys the fusion kernels write; the grid's bound all the same
+  const unsigned long long pass = i < A.count1 ? 0ull : 1ull;
+  return (long long)(pass * A.cells + cell);
+}
+
+__global__ void __launch_bounds__(256) k_cloud_mark(CloudOrderArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const long long c = cloud_cell(A, i);
+  if (c >= 0) A.rank[c] = 1u;
+}
+
+__global__ void __launch_bounds__(256) k_cloud_scatter(CloudOrderArgs A) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= A.n) return;
+  const long long c = cloud_cell(A, i);
+  if (c < 0) return;
+  const unsigned long long j = A.rank[c];
+  if (A.opos)
+    for (int k = 0; k < 3; ++k) A.opos[3 * j + k] = A.pos[3 * i + k];
+  if (A.onrm)
+    for (int k = 0; k < 3; ++k) A.onrm[3 * j + k] = A.nrm[3 * i + k];
+  if (A.ocol)
+    for (int k = 0; k < 3; ++k) A.ocol[3 * j + k] = A.col[3 * i + k];
+  if (A.okey) A.okey[j] = A.key[i];
+  if (A.onvis) A.onvis[j] = A.nvis[i];
+  if (A.ovis)
+    for (int t = 0; t < A.ovis_stride; ++t)
+      A.ovis[j * A.ovis_stride + t] = t < A.vis_stride && t < A.nvis[i] ? A.vis[i * A.vis_stride + t] : 0;
+}
+
+cudaError_t launch_cloud_mark(const CloudOrderArgs& A, cudaStream_t st) {
+  if (!A.n) return cudaSuccess;
+  k_cloud_mark<<<(unsigned)((A.n + 255) / 256), 256, 0, st>>>(A);
+  return cudaGetLastError();
+}
+cudaError_t launch_cloud_scatter(const CloudOrderArgs& A, cudaStream_t st) {
+  if (!A.n) return cudaSuccess;
+  k_cloud_scatter<<<(unsigned)((A.n + 255) / 256), 256, 0, st>>>(A);
+  return cudaGetLastError();
+}
+
+// Exclusive prefix sum: blocks of 1024 threads scan 4096 entries each (4 consecutive entries per thread, then a
+// warp-shuffle scan of the thread sums and of the warp totals), write their totals; the totals are scanned the same
+// way (recursively), and every entry adds its block's prefix.  The sums count points, so 32 bits suffice.
+constexpr int kScanBlock = 4096;
+
+__global__ void __launch_bounds__(1024) k_scan_block(unsigned* data, unsigned long long n, unsigned* sums) {
+  __shared__ unsigned warp_tot[32];
+  const unsigned long long b0 = (unsigned long long)blockIdx.x * kScanBlock;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  unsigned v[4], s = 0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const unsigned long long i = b0 + 4ull * t + k;
+    v[k] = i < n ? data[i] : 0u;
+    s += v[k];
+  }
+  unsigned inc = s;  // inclusive scan of the thread sums within the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += u;
+  }
+  if (lane == 31) warp_tot[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const unsigned w = warp_tot[lane];
+    unsigned wi = w;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned u = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += u;
+    }
+    warp_tot[lane] = wi - w;  // exclusive prefix of the warp totals
+    if (lane == 31) sums[blockIdx.x] = wi;
+  }
+  __syncthreads();
+  unsigned run = warp_tot[warp] + inc - s;  // exclusive prefix of this thread's first entry within the block
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const unsigned long long i = b0 + 4ull * t + k;
+    if (i < n) data[i] = run;
+    run += v[k];
+  }
+}
+
+__global__ void __launch_bounds__(256) k_scan_add(unsigned* data, unsigned long long n, const unsigned* sums) {
+  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) data[i] += sums[i / kScanBlock];
+}
+
+size_t scan_scratch(size_t n) {
+  size_t total = 0;
+  while (n > 1) {
+    n = (n + kScanBlock - 1) / kScanBlock;
+    total += n;
+  }
+  return total + 1;
+}
+
+cudaError_t scan_exclusive(unsigned* data, size_t n, unsigned* tmp, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const size_t nb = (n + kScanBlock - 1) / kScanBlock;
+  k_scan_block<<<(unsigned)nb, 1024, 0, st>>>(data, n, tmp);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || nb == 1) return e;
+  if ((e = scan_exclusive(tmp, nb, tmp + nb, st)) != cudaSuccess) return e;
+  k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(data, n, tmp);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g,
                            cudaStream_t st) {
   const dim3 b(32, 8), gr((w / 2 + 31) / 32, (h / 2 + 7) / 8);

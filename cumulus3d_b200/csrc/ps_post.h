@@ -194,6 +194,41 @@ cudaError_t launch_grid_insert(const float* pos, unsigned n, double cell, unsign
                                unsigned* next, unsigned cap, int* overflow, cudaStream_t st);
 cudaError_t launch_pyramid(const unsigned char* in, int w, int h, unsigned char* out, const float* g, cudaStream_t st);
 // 8-bit image (w × h, tight rows) -> f32 plane rows of `pitch` floats through a 256-entry table.
+// Output order of a fused cloud on the device.  Every kept point owns one cell of a grid of `cells` cells per pass,
+// laid out in output order: consistency fusion: pass (first, second) × the fused views in ascending image id × the
+// view's pixels row-major, which is ascending key within a pass; score fusion: its candidate number (one pass).  The
+// exclusive prefix sum of the occupied cells is each point's output index.
+struct CloudOrderArgs {
+  unsigned long long n, count1;    // emitted points; the first count1 are the first pass
+  unsigned long long cells;        // cells per pass
+  const unsigned char* keep;       // per point 1 = kept (NULL: all)
+  const unsigned* gid;             // score fusion: candidate number = cell (NULL: consistency fusion, cell from key)
+  const unsigned long long* key;
+  const unsigned* ids;             // consistency fusion: the fused views' image ids, ascending and distinct
+  const unsigned long long* base;  // their first cell
+  const int* width;                // their widths
+  int nids;
+  unsigned* rank;                  // passes·cells entries: occupancy, then exclusive ranks
+  const float* pos;                // the cloud as emitted
+  const float* nrm;
+  const unsigned char* col;
+  const unsigned char* nvis;
+  const unsigned short* vis;
+  int vis_stride;
+  float* opos;                     // the cloud in output order (any of opos..ovis may be NULL)
+  float* onrm;
+  unsigned char* ocol;
+  unsigned long long* okey;
+  unsigned char* onvis;
+  unsigned short* ovis;
+  int ovis_stride;
+};
+cudaError_t launch_cloud_mark(const CloudOrderArgs& A, cudaStream_t st);
+cudaError_t launch_cloud_scatter(const CloudOrderArgs& A, cudaStream_t st);
+// In-place exclusive prefix sum of n unsigned ints; `tmp` holds scan_scratch(n) entries.
+size_t scan_scratch(size_t n);
+cudaError_t scan_exclusive(unsigned* data, size_t n, unsigned* tmp, cudaStream_t st);
+
 cudaError_t launch_u8_plane(const unsigned char* in, int w, int h, const float* lut, float* out, int pitch,
                             cudaStream_t st);
 

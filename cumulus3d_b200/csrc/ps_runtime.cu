@@ -129,6 +129,13 @@ struct FusedCloud {
   unsigned short* vis = nullptr;
   unsigned long long* counter = nullptr;
   ps_post::FuseView* views = nullptr;
+  // output order on the device (ps_fused_points): cells per pass and, for consistency fusion, the fused views in
+  // ascending image id with their first cell and width; `ordered` is false when two fused views share an image id
+  unsigned long long cells = 0;
+  std::vector<unsigned> ids;
+  std::vector<unsigned long long> bases;
+  std::vector<int> widths;
+  bool ordered = false;
   template <typename Free>
   void release(Free&& free) {
     free(keep);
@@ -2497,6 +2504,24 @@ int ps_fuse_resident(ps_session* s, uint32_t level, const uint32_t* views, size_
       fc.cap = c;
       fc.vis_stride = stride;
     }
+    {  // key order = the fused views in ascending image id, row-major within a view
+      std::vector<std::pair<unsigned, int>> iv;
+      for (int v = 0; v < s->nv; ++v)
+        if (used[v]) iv.push_back({cams[v].image_id, v});
+      std::sort(iv.begin(), iv.end());
+      fc.ids.clear();
+      fc.bases.clear();
+      fc.widths.clear();
+      fc.cells = 0;
+      fc.ordered = true;
+      for (size_t i = 0; i < iv.size(); ++i) {
+        if (i && iv[i].first == iv[i - 1].first) fc.ordered = false;
+        fc.ids.push_back(iv[i].first);
+        fc.bases.push_back(fc.cells);
+        fc.widths.push_back(s->W(iv[i].second, l));
+        fc.cells += (unsigned long long)s->W(iv[i].second, l) * s->H(iv[i].second, l);
+      }
+    }
     if (!sl.marks) sl.marks = dalloc<unsigned char>(s, std::max<long long>(sl.total, 1));
     cuda_ok(cudaMemsetAsync(sl.marks, 0, std::max<long long>(sl.total, 1), s->st), "memset");
     cuda_ok(cudaMemsetAsync(fc.counter, 0, sizeof(unsigned long long), s->st), "memset");
@@ -2691,6 +2716,7 @@ int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views
             "upload fusion views");
     const unsigned long long valid = count_valid(s, views, n, l);  // capacity
     const int stride = (int)p->num_neighbors + 1;
+    const unsigned long long score_cells = base;  // candidate numbers run over the fused views' pixels
     if (valid > fc.cap || stride != fc.vis_stride) {
       fc.release([s](void* q) { dfree(s, q); });
       const size_t c = std::max<unsigned long long>(valid, 1);
@@ -2708,6 +2734,11 @@ int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views
     fc.keep = dalloc<unsigned char>(s, fc.cap);
     fc.gid = dalloc<unsigned>(s, fc.cap);
     fc.count = fc.count1 = fc.removed1 = fc.removed2 = fc.rejected = 0;
+    fc.ids.clear();
+    fc.bases.clear();
+    fc.widths.clear();
+    fc.cells = score_cells;
+    fc.ordered = true;
     ps_post::ScoreArgs A;
     memset(&A, 0, sizeof A);
     A.views = fc.views;
@@ -2797,6 +2828,89 @@ int ps_fuse_scored_resident(ps_session* s, uint32_t level, const uint32_t* views
   });
 }
 
+namespace {
+// The fused cloud in output order, ordered on the device (CloudOrderArgs in csrc/ps_post.h): every kept point marks
+// its cell of the output-order grid, an exclusive prefix sum of the marks gives each point's output index, the points
+// are scattered into output buffers, and those are copied into the caller's arrays.  Returns false (nothing written)
+// when the marks do not count exactly `kept` points, so the caller falls back to ordering on the host.
+bool fused_points_device(ps_session* s, size_t kept, float* positions, float* normals, uint8_t* colors, uint64_t* keys,
+                         uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride) {
+  FusedCloud& fc = s->fused;
+  const size_t n = fc.count;
+  const size_t ncell = (fc.gid ? 1 : 2) * (size_t)fc.cells;
+  if (ncell >= 0xffffffffull) return false;  // 32-bit ranks
+  std::vector<void*> tmp;
+  auto get = [&](size_t bytes) {
+    void* p = dalloc<unsigned char>(s, std::max<size_t>(bytes, 1));
+    tmp.push_back(p);
+    return p;
+  };
+  ps_post::CloudOrderArgs A;
+  memset(&A, 0, sizeof A);
+  A.n = n;
+  A.count1 = std::min<size_t>(fc.count1, n);
+  A.cells = fc.cells;
+  A.keep = fc.keep;
+  A.gid = fc.gid;
+  A.key = fc.key;
+  A.pos = fc.pos;
+  A.nrm = fc.nrm;
+  A.col = fc.col;
+  A.nvis = fc.nvis;
+  A.vis = fc.vis;
+  A.vis_stride = fc.vis_stride;
+  A.rank = (unsigned*)get((ncell + 1) * sizeof(unsigned));
+  unsigned* scratch = (unsigned*)get(ps_post::scan_scratch(ncell + 1) * sizeof(unsigned));
+  if (!fc.gid) {
+    A.nids = (int)fc.ids.size();
+    unsigned* ids = (unsigned*)get(fc.ids.size() * sizeof(unsigned));
+    unsigned long long* base = (unsigned long long*)get(fc.bases.size() * sizeof(unsigned long long));
+    int* width = (int*)get(fc.widths.size() * sizeof(int));
+    cuda_ok(cudaMemcpyAsync(ids, fc.ids.data(), fc.ids.size() * sizeof(unsigned), cudaMemcpyHostToDevice, s->st),
+            "upload cloud order");
+    cuda_ok(cudaMemcpyAsync(base, fc.bases.data(), fc.bases.size() * sizeof(unsigned long long),
+                            cudaMemcpyHostToDevice, s->st),
+            "upload cloud order");
+    cuda_ok(cudaMemcpyAsync(width, fc.widths.data(), fc.widths.size() * sizeof(int), cudaMemcpyHostToDevice, s->st),
+            "upload cloud order");
+    A.ids = ids;
+    A.base = base;
+    A.width = width;
+  }
+  if (positions) A.opos = (float*)get(kept * 12);
+  if (normals) A.onrm = (float*)get(kept * 12);
+  if (colors) A.ocol = (unsigned char*)get(kept * 3);
+  if (keys) A.okey = (unsigned long long*)get(kept * 8);
+  if (vis_counts) A.onvis = (unsigned char*)get(kept);
+  if (vis) {
+    A.ovis = (unsigned short*)get(kept * vis_stride * sizeof(unsigned short));
+    A.ovis_stride = (int)vis_stride;
+  }
+  cuda_ok(cudaMemsetAsync(A.rank, 0, (ncell + 1) * sizeof(unsigned), s->st), "memset");
+  launched(s, ps_post::launch_cloud_mark(A, s->st), "cloud order kernel");
+  launched(s, ps_post::scan_exclusive(A.rank, ncell + 1, scratch, s->st), "scan kernel");
+  unsigned occupied = 0;
+  cuda_ok(cudaMemcpyAsync(&occupied, A.rank + ncell, sizeof occupied, cudaMemcpyDeviceToHost, s->st), "read count");
+  sync(s);
+  bool ok = occupied == kept;
+  if (ok) {
+    launched(s, ps_post::launch_cloud_scatter(A, s->st), "cloud scatter kernel");
+    auto down = [&](void* dst, const void* src, size_t bytes) {
+      if (dst && bytes) cuda_ok(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s->st), "download cloud");
+    };
+    down(positions, A.opos, kept * 12);
+    down(normals, A.onrm, kept * 12);
+    down(colors, A.ocol, kept * 3);
+    down(keys, A.okey, kept * 8);
+    down(vis_counts, A.onvis, kept);
+    down(vis, A.ovis, kept * vis_stride * sizeof(unsigned short));
+    sync(s);
+  }
+  for (void* p : tmp) dfree(s, p);
+  return ok;
+}
+}  // namespace
+
 int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* normals, uint8_t* colors,
                     uint64_t* keys, uint8_t* vis_counts, uint16_t* vis, uint32_t vis_stride) {
   return guard(s, [&] {
@@ -2806,6 +2920,8 @@ int ps_fused_points(ps_session* s, uint64_t capacity, float* positions, float* n
     if (capacity < kept)
       fail(PS_EINVAL, "capacity " + std::to_string(capacity) + " < " + std::to_string(kept) + " points");
     if (vis && (int)vis_stride < fc.vis_stride) fail(PS_EINVAL, "vis_stride too small");
+    if (fc.ordered && n && fused_points_device(s, kept, positions, normals, colors, keys, vis_counts, vis, vis_stride))
+      return;
     std::vector<float> p(3 * n), q(3 * n);
     std::vector<unsigned char> c(3 * n), nv(n);
     std::vector<unsigned long long> k(n);

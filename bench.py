@@ -896,7 +896,7 @@ def main():
                     help="network convolution kernels (auto: tcgen05 for cout >= 64, mma.sync below)")
     ap.add_argument("--learned-geo-iters", type=int, default=1,
                     help="iterations of the learned schedule's geometric round (the plain schedule's is 2)")
-    ap.add_argument("--learned-conf", type=float, default=0.3,
+    ap.add_argument("--learned-conf", type=float, default=0.15,
                     help="confidence threshold of the proposals (random init below it)")
     ap.add_argument("--learned-iters", type=int, default=2,
                     help="photometric iterations of the learned-init schedule")

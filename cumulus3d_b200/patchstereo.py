@@ -490,7 +490,7 @@ class PatchMatchSession:
         a = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
         self._check(self.lib.ps_set_sweep_normals(self.h, a.ctypes.data))
 
-    def propose(self, net, level: int, views: Sequence[int], conf_threshold: float = 0.3,
+    def propose(self, net, level: int, views: Sequence[int], conf_threshold: float = 0.15,
                 count: bool = True) -> Optional[int]:
         """Sweep + network + decode into the session's proposal store; returns the number of proposed pixels."""
         n = C.c_uint64()

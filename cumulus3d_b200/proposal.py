@@ -38,7 +38,7 @@ NUM_PARAMS = sum(co * 9 * ci + co for ci, co in LAYERS)
 WEIGHTS_DIR = pathlib.Path(__file__).resolve().parent / "weights"
 DEFAULT_WEIGHTS = WEIGHTS_DIR / "proposal_aerial.npz"
 LABEL_MAX_COST = 0.6
-CONF_THRESHOLD = 0.3
+CONF_THRESHOLD = 0.15
 
 
 def split_params(flat: np.ndarray):

@@ -1671,7 +1671,7 @@ __global__ void __launch_bounds__(PS_HALF_NT, 2) k_half_st(const __grid_constant
 
 // ================================================================================ run start / evaluate (patchmatch.cu:661-692)
 // Top-K mean cost (patchmatch.cu:327-345).
-template <int WR, int WS, bool CW, int NT>
+template <int WR, int WS, bool CW, int NT, bool TEX = false>
 __device__ float topk_cost(const PsRun& P, const RefWin& rw, const RefStats& rs, const PsLevel& R, const PsPair* prs,
                            const PsLPair* lps, int nsrc, int x, int y, float4 h, int& nwin) {
   float b0 = 1e30f, b1 = 1e30f, b2 = 1e30f;
@@ -1681,7 +1681,7 @@ __device__ float topk_cost(const PsRun& P, const RefWin& rw, const RefStats& rs,
     const PsLPair lp = lps[j];
     const PsLevel S = P.lv[pr.src * P.nlevels + P.level];
     float g = 0.f;
-    float c = pair_cost<WR, WS, CW, NT>(P, rw, rs, R, S, pr, lp, x, y, h, &g, nwin);
+    float c = pair_cost<WR, WS, CW, NT, TEX>(P, rw, rs, R, S, pr, lp, x, y, h, &g, nwin);
     if (P.geometric) c += P.lambda * g;
     if (c < b0) {
       b2 = b1;
@@ -1731,7 +1731,8 @@ __device__ __forceinline__ bool eval_tile(const PsRun& P, float* tile, int wr, E
   return e.x < it.w && e.y < it.h;
 }
 
-template <int WR, int WS, bool CW>
+// TEX: the source samples through the planes' texture gathers (same bits as the plane loads).
+template <int WR, int WS, bool CW, bool TEX>
 __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_EVAL_NT;
   extern __shared__ float sm[];
@@ -1773,7 +1774,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_eval(const __grid_constant__ 
   int nwin = 0;
   if (h.w > 0.f) {
     const RefStats rs = ref_stats<WR, WS, CW, NT>(P, rw);
-    c = topk_cost<WR, WS, CW, NT>(P, rw, rs, e.R, prs, lps, vd.nsrc, x, y, h, nwin);
+    c = topk_cost<WR, WS, CW, NT, TEX>(P, rw, rs, e.R, prs, lps, vd.nsrc, x, y, h, nwin);
   }
   P.cost[base + pix] = c;
   if (P.mode == 1) P.bview[base + pix] = 255;
@@ -1842,7 +1843,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_sweep(const __grid_constant__
 }
 
 // ================================================================================ final readout (patchmatch.cu:695-737)
-template <int WR, int WS, bool CW>
+template <int WR, int WS, bool CW, bool TEX>
 __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant__ PsRun P) {
   constexpr int NT = PS_EVAL_NT;
   extern __shared__ float sm[];
@@ -1889,7 +1890,7 @@ __global__ void __launch_bounds__(PS_EVAL_NT, 2) k_filter(const __grid_constant_
       float H[9];
       const PsLPair lp = lps[j];
       if (!homography(e.R, lp, (float)x, (float)y, h, H)) continue;
-      const float m = ncc_cost<WR, WS, CW, NT>(P, rw, rs, S, H, x, y, nwin);
+      const float m = ncc_cost<WR, WS, CW, NT, TEX>(P, rw, rs, S, H, x, y, nwin);
       const float ee = P.ncc_norm * m_exp(-m * m * P.inv2ncc);
       if (ee / (ee + 0.5f) < P.q_min) continue;
       if (geo_error(P, e.R, S, pr, x, y, h.w) > P.filter_gmax) continue;
@@ -2275,26 +2276,32 @@ cudaError_t launch_half(const PsRun& P, unsigned tuning, cudaStream_t st) {
   return G == 2 ? launch_half_g<0, 1, 2>(P, cw, tex, smem, st) : launch_half_g<0, 1, 1>(P, cw, tex, smem, st);
 }
 
-cudaError_t launch_eval(const PsRun& P, cudaStream_t st) {
+// tex: the session built texture objects for its planes (PS_TUNE_TEX_GATHER); the specialised windows then sample
+// through them, the generic kernels keep the plane loads.
+cudaError_t launch_eval(const PsRun& P, bool tex, cudaStream_t st) {
   const bool cw = use_cache(P.wr, P.ws);
   const size_t smem = eval_smem(P.wr, P.ws, cw);
-#define PS_CASE(a, b) \
-  if (P.wr == a && P.ws == b) return launch(k_eval<a, b, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+#define PS_CASE(a, b)                                                                                  \
+  if (P.wr == a && P.ws == b)                                                                          \
+    return tex ? launch(k_eval<a, b, true, true>, P.ntiles, PS_EVAL_NT, smem, st, P)                   \
+               : launch(k_eval<a, b, true, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
   PS_SPECS(PS_CASE)
 #undef PS_CASE
-  if (cw) return launch(k_eval<0, 1, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
-  return launch(k_eval<0, 1, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  if (cw) return launch(k_eval<0, 1, true, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  return launch(k_eval<0, 1, false, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
 }
 
-cudaError_t launch_filter(const PsRun& P, cudaStream_t st) {
+cudaError_t launch_filter(const PsRun& P, bool tex, cudaStream_t st) {
   const bool cw = use_cache(P.wr, P.ws);
   const size_t smem = eval_smem(P.wr, P.ws, cw);
-#define PS_CASE(a, b) \
-  if (P.wr == a && P.ws == b) return launch(k_filter<a, b, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
+#define PS_CASE(a, b)                                                                                  \
+  if (P.wr == a && P.ws == b)                                                                          \
+    return tex ? launch(k_filter<a, b, true, true>, P.ntiles, PS_EVAL_NT, smem, st, P)                 \
+               : launch(k_filter<a, b, true, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
   PS_SPECS(PS_CASE)
 #undef PS_CASE
-  if (cw) return launch(k_filter<0, 1, true>, P.ntiles, PS_EVAL_NT, smem, st, P);
-  return launch(k_filter<0, 1, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  if (cw) return launch(k_filter<0, 1, true, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
+  return launch(k_filter<0, 1, false, false>, P.ntiles, PS_EVAL_NT, smem, st, P);
 }
 
 cudaError_t launch_upsample(const PsRun& P, cudaStream_t st) {

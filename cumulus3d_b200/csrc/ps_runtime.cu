@@ -35,8 +35,8 @@
   bool half_run_ok(unsigned tuning, int wr, int ws);                                                       \
   cudaError_t launch_half_run(const PsRun& P, unsigned tuning, cudaStream_t st);                           \
   int half_lanes(unsigned tuning);                                                                         \
-  cudaError_t launch_eval(const PsRun& P, cudaStream_t st);                                                \
-  cudaError_t launch_filter(const PsRun& P, cudaStream_t st);                                              \
+  cudaError_t launch_eval(const PsRun& P, bool tex, cudaStream_t st);                                      \
+  cudaError_t launch_filter(const PsRun& P, bool tex, cudaStream_t st);                                    \
   cudaError_t launch_upsample(const PsRun& P, cudaStream_t st);                                            \
   cudaError_t launch_median(const PsRun& P, cudaStream_t st);                                              \
   cudaError_t launch_snapshot(const PsRun& P, float* snap, cudaStream_t st);                               \
@@ -57,8 +57,8 @@ namespace {
 
 struct Launchers {
   cudaError_t (*half)(const PsRun&, unsigned, cudaStream_t);
-  cudaError_t (*eval)(const PsRun&, cudaStream_t);
-  cudaError_t (*filter)(const PsRun&, cudaStream_t);
+  cudaError_t (*eval)(const PsRun&, bool, cudaStream_t);
+  cudaError_t (*filter)(const PsRun&, bool, cudaStream_t);
   cudaError_t (*upsample)(const PsRun&, cudaStream_t);
   cudaError_t (*median)(const PsRun&, cudaStream_t);
   cudaError_t (*snapshot)(const PsRun&, float*, cudaStream_t);
@@ -780,7 +780,7 @@ void run_batch(ps_session* s, const uint32_t* views, size_t a, size_t b, const p
     P.proposal = sl.proposal;
   }
   set_items(s, P, views, a, b, (int)p->level, PS_EVAL_PW, PS_EVAL_PH);
-  timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+  timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "evaluate kernel");
   PsRun H = P;
   set_items(s, H, views, a, b, (int)p->level, s->L->half_lanes(s->tuning) == 2 ? PS_HALF2_PW : PS_HALF_PW,
             PS_HALF_PH);
@@ -1458,7 +1458,7 @@ int ps_evaluate(ps_session* s, uint32_t level, const uint32_t* views, size_t n, 
       P.geometric = geometric ? 1 : 0;
       P.mode = 0;
       set_items(s, P, views, a, b, (int)level, PS_EVAL_PW, PS_EVAL_PH);
-      timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+      timed_launch(s, PS_KERNEL_EVAL, P, [&](const PsRun& q) { return s->L->eval(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "evaluate kernel");
       for (size_t i = a; i < b; ++i) {
         if (!out_cost[i]) fail(PS_EINVAL, "out_cost entry is NULL");
         cuda_ok(cudaMemcpyAsync(out_cost[i], sl.cost + sl.off[views[i]],
@@ -1484,7 +1484,7 @@ int ps_filter(ps_session* s, const uint32_t* views, size_t n, const ps_view_stat
       PsRun P = base_params(s, level);
       P.geometric = 1;
       set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
-      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "filter kernel");
       for (size_t i = a; i < b; ++i) {
         if (!out_counts[i]) fail(PS_EINVAL, "out_counts entry is NULL");
         cuda_ok(cudaMemcpyAsync(out_counts[i], sl.count + sl.off[views[i]],
@@ -1616,7 +1616,7 @@ int ps_filter_resident(ps_session* s, const uint32_t* views, size_t n, uint8_t* 
       PsRun P = base_params(s, level);
       P.geometric = 1;
       set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
-      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+      timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "filter kernel");
       if (out_counts) {
         for (size_t i = a; i < b; ++i)
           if (out_counts[i])
@@ -1676,7 +1676,7 @@ void enqueue_schedule(ps_session* s, const uint32_t* views, size_t n, const ps_s
     PsRun P = base_params(s, level);
     P.geometric = 1;
     set_items(s, P, views, a, b, level, PS_EVAL_PW, PS_EVAL_PH);
-    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "filter kernel");
     PsRun Q = base_params(s, level);
     set_items(s, Q, views, a, b, level, PS_SIMPLE_BX, PS_SIMPLE_BY);
     launched(s, s->L->readout(Q, sl.aux, s->st), "readout kernel");
@@ -1714,7 +1714,7 @@ void enqueue_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps
         launched(s, s->L->upsample(U, s->st), "upsample kernel");
         PsRun E = base_params(s, l);  // c_init: top-K photometric cost of the upsampled planes
         set_items(s, E, views, a, b, l, PS_EVAL_PW, PS_EVAL_PH);
-        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "evaluate kernel");
       }
       for (size_t i = 0; i < n; ++i) {  // keep the upsampled planes and their cost
         const size_t np = (size_t)s->W(views[i], l) * s->H(views[i], l), o = (size_t)sl.off[views[i]];
@@ -1729,7 +1729,7 @@ void enqueue_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps
       for (auto [a, b] : batches(s, views, n, l)) {
         PsRun E = base_params(s, l);  // c_photo
         set_items(s, E, views, a, b, l, PS_EVAL_PW, PS_EVAL_PH);
-        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->st); }, "evaluate kernel");
+        timed_launch(s, PS_KERNEL_EVAL, E, [&](const PsRun& q) { return s->L->eval(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "evaluate kernel");
         PsRun R = base_params(s, l);
         set_items(s, R, views, a, b, l, PS_SIMPLE_BX, PS_SIMPLE_BY);
         launched(s, s->L->restore(R, sl.aux, sl.cinit, m->restorer_threshold, s->st), "restore kernel");
@@ -1759,7 +1759,7 @@ void enqueue_multiscale(ps_session* s, const uint32_t* views, size_t n, const ps
     PsRun P = base_params(s, top);
     P.geometric = 1;
     set_items(s, P, views, a, b, top, PS_EVAL_PW, PS_EVAL_PH);
-    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->st); }, "filter kernel");
+    timed_launch(s, PS_KERNEL_FILTER, P, [&](const PsRun& q) { return s->L->filter(q, s->tuning & PS_TUNE_TEX_GATHER, s->st); }, "filter kernel");
     PsRun Q = base_params(s, top);
     set_items(s, Q, views, a, b, top, PS_SIMPLE_BX, PS_SIMPLE_BY);
     launched(s, s->L->readout(Q, st.aux, s->st), "readout kernel");

@@ -76,6 +76,36 @@ def test_evaluate_photometric_parity(backend):
         np.testing.assert_array_equal(a, b)
 
 
+@pytest.mark.parametrize("wr,ws", [(3, 1), (5, 1), (5, 2), (6, 1), (4, 1)])
+def test_evaluate_and_filter_through_texture_gathers(wr, ws):
+    """A session with texture objects (PS_TUNE_TEX_GATHER) samples the sources of the run-start evaluate, the
+    evaluate call and the filter through texture gathers at the specialised windows (the generic window keeps the
+    plane loads): the same bits as the oracle for photometric and geometric top-K costs and the filter counts."""
+    from cumulus3d_b200 import _lib
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    wl = scenes.workload_small(96, 64, views=3, window_radius=wr, window_step=ws, seed=70 + wr)
+    p1 = RunParams(0, False, True, 2, 1)
+    gpu, cpu = _states(wl), _states(wl)
+    be = PatchMatchBackend(0, math="parity", tuning=_lib.PS_TUNE_ROW_PAIRS | _lib.PS_TUNE_TEX_GATHER)
+    with be.begin(wl.input) as s:
+        s.run(wl.views, gpu, p1)
+        oracle.run(wl.input, wl.views, cpu, p1)
+        for i in range(3):
+            _assert_same(gpu[i], cpu[i], f"run view {i}")
+        snap = DepthSnapshot(1, 0, [g.depth.copy() for g in gpu])
+        for geometric in (False, True):
+            ge = s.evaluate(0, wl.views, gpu, geometric, snap if geometric else None)
+            ce = oracle.evaluate(wl.input, 0, wl.views, cpu, geometric, snap if geometric else None)
+            for a, b in zip(ge, ce):
+                np.testing.assert_array_equal(a, b)
+        gf = s.filter(wl.views, gpu, snap)
+        cf = oracle.filter(wl.input, wl.views, cpu, snap)
+        for a, b in zip(gf, cf):
+            np.testing.assert_array_equal(a, b)
+        assert sum(int(a.sum()) for a in gf) > 0
+    be.close()
+
+
 def test_ragged_batch_and_subset(backend):
     """Views of different sizes in one launch, and a subset of views in a different order."""
     wl = scenes.workload_small(64, 48, views=3, window_radius=3, seed=9)

@@ -220,10 +220,16 @@ def bench_ours(args, rank, world, local):
     # the same time over the windows the reference evaluates: the evaluated ones plus those the early exit skips
     achieved_all = (taps_per_launch + skipped_per_launch * wn * wn) * FLOP_PER_TAP_CACHED / (half_launch_ms / 1e3) / 1e12
     traffic = None
+    data_stage = None
     try:
         with open(os.path.join(ROOT, "profiles", "k_half_traffic.json")) as f:
             tr = json.load(f)
         traffic = tr["bytes_per_window"] * half["ncc_windows"] / max(half["launches"], 1)
+        ds = tr.get("l1_data_stage")
+        if ds:  # the binding resource, from the ncu capture (not measured by this run)
+            data_stage = {"resource": "L1 data stage (texture gathers + shared-memory loads)", "busy": ds["busy"],
+                          "texture_pipe": ds["texture_pipe_busy"], "lsu_pipe": ds["lsu_pipe_busy"],
+                          "source": "ncu capture of one 6-view launch, profiles/k_half_c2_drone.md"}
     except Exception:
         pass
     res = {
@@ -242,6 +248,7 @@ def bench_ours(args, rank, world, local):
                      "launch_ms": round(half_launch_ms, 3), "traffic": traffic,
                      "skipped_windows_per_launch": round(skipped_per_launch),
                      "frac_all_windows": round(achieved_all / fp32_peak, 4),
+                     "binding_resource": data_stage,
                      "note": "achieved counts the NCC windows evaluated; refinement windows of candidates whose partial "
                              "cost already reached the best cost are skipped (same result), and frac_all_windows "
                              "counts them as the reference, which evaluates them, does"},

@@ -1,6 +1,7 @@
 """The C ABI library (CPU only: no compute calls).
 
-* libpatchstereo.so loads and exports every function declared in include/patchstereo.h;
+* libpatchstereo.so loads and exports every function declared in include/patchstereo.h, and the integration guide
+  names each of them;
 * the ctypes mirror has the same struct sizes and field offsets as a C compilation of the header;
 * without a GPU, backend creation fails with PS_ENODEV (no CPU fallback exists);
 * parameter defaults equal the reference's PmParams::default / FilterParams::default
@@ -35,6 +36,13 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     # the ctypes table covers the same set
     assert set(names) == set(_lib.SIGNATURES), set(names) ^ set(_lib.SIGNATURES)
+
+
+def test_integration_guide_names_every_declared_function():
+    """The integration guide is where a maintainer writing the binding looks each entry point up."""
+    guide = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    missing = [n for n in declared_functions() if not re.search(r"\b" + n + r"\b", guide)]
+    assert not missing, missing
 
 
 STRUCTS = {

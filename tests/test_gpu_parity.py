@@ -106,6 +106,39 @@ def test_evaluate_and_filter_through_texture_gathers(wr, ws):
     be.close()
 
 
+@pytest.mark.parametrize("tuning", [6, 10, 42])
+def test_f32_images_through_texture_gathers(tuning):
+    """f32 images (PS_IMAGE_F32) in a session with texture objects: the f32 texture arrays hold the planes' values, so
+    the half steps, the run-start evaluate, the evaluate call and the filter all give the oracle's bits."""
+    from cumulus3d_b200.patchstereo import PatchMatchBackend
+    wl = scenes.workload_small(96, 64, views=3, window_radius=5, seed=83)
+    inp = scenes.kernel_input(wl.cams, [np.asarray(im, np.float32) for im in wl.images],
+                              [list(v.sources) for v in wl.input.views], (25.0, 60.0), window_radius=5,
+                              window_step=1, gray8=False)
+    assert inp.views[0].levels[0].pixels.dtype == np.float32
+    p1 = RunParams(0, False, True, 2, 1)
+    p2 = RunParams(0, True, False, 1, 2)
+    gpu, cpu = _states(wl), _states(wl)
+    be = PatchMatchBackend(0, math="parity", tuning=tuning)
+    with be.begin(inp) as s:
+        s.run(wl.views, gpu, p1)
+        oracle.run(inp, wl.views, cpu, p1)
+        snap = DepthSnapshot(1, 0, [g.depth.copy() for g in gpu])
+        s.run(wl.views, gpu, p2, snap)
+        oracle.run(inp, wl.views, cpu, p2, snap)
+        for i in range(3):
+            _assert_same(gpu[i], cpu[i], f"f32 view {i} tuning={tuning}")
+        ge = s.evaluate(0, wl.views, gpu, True, snap)
+        ce = oracle.evaluate(inp, 0, wl.views, cpu, True, snap)
+        for a, b in zip(ge, ce):
+            np.testing.assert_array_equal(a, b)
+        gf = s.filter(wl.views, gpu, snap)
+        cf = oracle.filter(inp, wl.views, cpu, snap)
+        for a, b in zip(gf, cf):
+            np.testing.assert_array_equal(a, b)
+    be.close()
+
+
 def test_ragged_batch_and_subset(backend):
     """Views of different sizes in one launch, and a subset of views in a different order."""
     wl = scenes.workload_small(64, 48, views=3, window_radius=3, seed=9)
